@@ -1,0 +1,1186 @@
+/* oracle.c -- CPU restatement of the deterministic synchronous multilevel
+ * schedule (TEST INFRASTRUCTURE; see oracle.h).  Plain C, single threaded,
+ * written for clarity: dense scratch arrays, no clever data structures.
+ *
+ * Reference citations are paths inside the KaHIP source tree.
+ */
+#include "oracle.h"
+
+#include <limits.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+enum {
+    TAG_CSUB = 1, TAG_CTIE = 2, TAG_RSUB = 3, TAG_RTIE = 4, TAG_RPRIO = 5,
+    TAG_BTIE = 6, TAG_BCLS = 7, TAG_BPRIO = 8, TAG_IP = 9, TAG_IPM = 10
+};
+
+#define BAL_CLASSES 256
+
+static void* xcalloc(size_t n, size_t s) {
+    void* p = calloc(n ? n : 1, s);
+    if (!p) abort();
+    return p;
+}
+static void* xmalloc(size_t n) {
+    void* p = malloc(n ? n : 1);
+    if (!p) abort();
+    return p;
+}
+
+/* ------------------------------------------------------------------ hashing */
+
+uint64_t or_mix64(uint64_t z) {
+    /* splitmix64 output function (Steele, Lea & Flood 2014) */
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+uint64_t or_stream(int seed, int tag, int level, int round) {
+    uint64_t s = or_mix64((uint64_t)(uint32_t)seed ^ ((uint64_t)(uint32_t)tag << 40));
+    s = or_mix64(s ^ (uint64_t)(uint32_t)level);
+    return or_mix64(s ^ (uint64_t)(uint32_t)round);
+}
+
+uint32_t or_hash(uint64_t stream, uint32_t x) {
+    return (uint32_t)(or_mix64(stream ^ (uint64_t)x) >> 32);
+}
+
+/* ------------------------------------------------------------------- knobs */
+
+void or_derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, int mode,
+                     or_knobs* o) {
+    memset(o, 0, sizeof(*o));
+    o->k = k;
+    o->imbalance = imbalance;
+    o->seed = seed;
+    o->mode = mode;
+    /* app/balance_configuration.h:19-24: W = sum of node weights (NodeWeight) */
+    uint32_t W = 0;
+    for (int v = 0; v < n; ++v) W += vwgt ? (uint32_t)vwgt[v] : 1u;
+    o->total_weight = W;
+    /* interface/kaHIP_interface.cpp:115 then balance_configuration.h:40-47 */
+    double imbalance_pct = 100 * imbalance;
+    double epsilon = imbalance_pct / 100.0;
+    double per_block = ceil(W / (double)k);
+    if (imbalance_pct == 0) {
+        o->upper_bound = (uint32_t)((1 + epsilon + 0.01) * per_block);
+        o->final_bound = (uint32_t)per_block;
+    } else {
+        o->upper_bound = (uint32_t)((1 + epsilon) * per_block);
+        o->final_bound = o->upper_bound;
+    }
+    /* stop_rules.h:46-56 (simple_stop_rule, work_load = W) */
+    double x = 60;
+    double ns = (double)n / (2.0 * x * k);
+    if (ns < 60.0 * k) ns = 60.0 * k;
+    o->num_stop = (uint32_t)ns;
+    o->max_vertex_weight = (uint32_t)(1.5 * W / o->num_stop);
+    /* size_constraint_label_propagation.cpp:57 -- ceil(U / cluster_coarsening_factor)
+     * with cf = 18 (app/configuration.h:422), capped so that no coarse node
+     * exceeds max_vertex_weight (the matching bound of the fast/eco presets). */
+    uint32_t cb = (uint32_t)ceil(o->upper_bound / 18.0);
+    if (o->max_vertex_weight + 1u < cb) cb = o->max_vertex_weight + 1u;
+    o->cluster_bound = cb;
+    int fast = (mode == 0 || mode == 3);
+    o->lpc_rounds = fast ? 5 : 10;
+    o->lpc_subrounds = 4;
+    o->ref_rounds = fast ? 10 : 25;
+    o->ref_subrounds = 4;
+    o->ref_classes = 16;
+    o->bal_iters = 64;
+    o->ip_reps = fast ? 1 : 3;
+    o->ip_tries = 4;
+    o->ip_fm_passes = fast ? 3 : 6;
+    o->ip_fm_stall = 100;
+    o->max_levels = 48;
+}
+
+/* ----------------------------------------------------------------- metrics */
+
+long long or_edge_cut(const or_graph* g, const int* part) {
+    /* quality_metrics.cpp:23-37 (64-bit accumulation) */
+    long long cut = 0;
+    for (int v = 0; v < g->n; ++v)
+        for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e)
+            if (part[v] != part[g->adjncy[e]]) cut += g->adjwgt[e];
+    return cut / 2;
+}
+
+void or_block_weights(const or_graph* g, const int* part, int k, uint32_t* bw) {
+    memset(bw, 0, sizeof(uint32_t) * (size_t)k);
+    for (int v = 0; v < g->n; ++v) bw[part[v]] += (uint32_t)g->vwgt[v];
+}
+
+double or_balance_ratio(const or_graph* g, const int* part, int k) {
+    /* quality_metrics.cpp:265-288 */
+    uint32_t* bw = xcalloc((size_t)k, sizeof(uint32_t));
+    double total = 0;
+    for (int v = 0; v < g->n; ++v) { bw[part[v]] += (uint32_t)g->vwgt[v]; total += g->vwgt[v]; }
+    double per = ceil(total / (double)k), mx = -1;
+    for (int b = 0; b < k; ++b) if (bw[b] > mx) mx = bw[b];
+    free(bw);
+    return mx / per;
+}
+
+void or_rate_expansion_star_2(const or_graph* g, double* rating) {
+    /* edge_ratings.cpp:316-328: 1.0*w*w / (c(u)*c(v)), denominator as a
+     * 32-bit unsigned product */
+    for (int v = 0; v < g->n; ++v) {
+        uint32_t cv = (uint32_t)g->vwgt[v];
+        for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) {
+            uint32_t cu = (uint32_t)g->vwgt[g->adjncy[e]];
+            int w = g->adjwgt[e];
+            rating[e] = 1.0 * w * w / (uint32_t)(cu * cv);
+        }
+    }
+}
+
+/* --------------------------------------------------- neighbourhood scratch */
+
+typedef struct {
+    uint32_t* acc;  /* dense accumulator indexed by label */
+    int* touched;   /* labels with a live entry */
+    int ntouched;
+} or_acc;
+
+static void acc_init(or_acc* a, int labels, int maxdeg) {
+    a->acc = xcalloc((size_t)labels, sizeof(uint32_t));
+    a->touched = xmalloc(sizeof(int) * (size_t)(maxdeg + 1));
+    a->ntouched = 0;
+}
+static void acc_free(or_acc* a) { free(a->acc); free(a->touched); }
+
+/* conn[b] = sum of w(v,u) over neighbours u with lab[u] == b.  A label is
+ * recorded as touched the first time an edge to it is seen, so zero-weight
+ * edges still make their label a candidate. */
+static void acc_gather(or_acc* a, const or_graph* g, int v, const int* lab, char* seen) {
+    a->ntouched = 0;
+    for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) {
+        int b = lab[g->adjncy[e]];
+        if (!seen[b]) { seen[b] = 1; a->touched[a->ntouched++] = b; }
+        a->acc[b] += (uint32_t)g->adjwgt[e];
+    }
+}
+static void acc_clear(or_acc* a, char* seen) {
+    for (int i = 0; i < a->ntouched; ++i) { a->acc[a->touched[i]] = 0; seen[a->touched[i]] = 0; }
+    a->ntouched = 0;
+}
+
+static int max_degree(const or_graph* g) {
+    int d = 0;
+    for (int v = 0; v < g->n; ++v) if (g->xadj[v + 1] - g->xadj[v] > d) d = g->xadj[v + 1] - g->xadj[v];
+    return d;
+}
+
+/* Candidate order shared by clustering and refinement: higher connection
+ * wins; the current label wins ties against everything; among other labels
+ * the smaller hash(tie stream, label) wins, then the smaller label.
+ * (The reference breaks ties with a coin flip, random_functions.h:152-155.) */
+static int beats(uint32_t cb, int b, uint32_t ca, int a, int own, uint64_t ks_tie) {
+    if (cb != ca) return cb > ca;
+    if (a == own) return 0;
+    uint32_t hb = or_hash(ks_tie, (uint32_t)b), ha = or_hash(ks_tie, (uint32_t)a);
+    if (hb != ha) return hb < ha;
+    return b < a;
+}
+
+/* ----------------------------------------------------------- LP clustering */
+
+/* One node's choice.  Rules of size_constraint_label_propagation.cpp:160-190:
+ * start from the own cluster with its connection, move to a neighbouring
+ * cluster b with a strictly larger connection when
+ * cluster_weight[b] + c(v) < bound (:175); the own cluster is always
+ * allowed. */
+static int cluster_choice(const or_graph* g, int v, const int* label, const uint32_t* cw,
+                          uint32_t bound, or_acc* a, char* seen, uint64_t ks_tie) {
+    acc_gather(a, g, v, label, seen);
+    int own = label[v];
+    uint32_t cv = (uint32_t)g->vwgt[v];
+    int best = own;
+    uint32_t bestc = seen[own] ? a->acc[own] : 0;
+    for (int i = 0; i < a->ntouched; ++i) {
+        int b = a->touched[i];
+        if (b == own) continue;
+        uint32_t c = a->acc[b];
+        if (c == 0) continue;
+        if (!((uint64_t)cw[b] + cv < bound)) continue;
+        if (beats(c, b, bestc, best, own, ks_tie)) { best = b; bestc = c; }
+    }
+    acc_clear(a, seen);
+    return best;
+}
+
+void or_lp_cluster(const or_graph* g, const or_knobs* kn, int level, int* label) {
+    const int n = g->n;
+    uint32_t* cw = xmalloc(sizeof(uint32_t) * (size_t)(n ? n : 1));
+    int* prop = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    uint64_t* incoming = xcalloc((size_t)n, sizeof(uint64_t));
+    int* minv = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    char* seen = xcalloc((size_t)n, 1);
+    or_acc a;
+    acc_init(&a, n, max_degree(g));
+    for (int v = 0; v < n; ++v) { label[v] = v; cw[v] = (uint32_t)g->vwgt[v]; minv[v] = INT_MAX; }
+    const uint32_t S = (uint32_t)kn->lpc_subrounds;
+    for (int r = 0; r < kn->lpc_rounds; ++r) {
+        uint64_t ks_sub = or_stream(kn->seed, TAG_CSUB, level, r);
+        uint64_t ks_tie = or_stream(kn->seed, TAG_CTIE, level, r);
+        for (uint32_t s = 0; s < S; ++s) {
+            /* 1. every active node decides against the state at sub-round start */
+            for (int v = 0; v < n; ++v) {
+                prop[v] = -1;
+                if (or_hash(ks_sub, (uint32_t)v) % S != s) continue;
+                int b = cluster_choice(g, v, label, cw, kn->cluster_bound, &a, seen, ks_tie);
+                if (b != label[v]) prop[v] = b;
+            }
+            /* 2. admission: all proposals into b if they fit together,
+             *    otherwise only the one of the smallest node id (which fits
+             *    on its own by the test in cluster_choice) */
+            for (int v = 0; v < n; ++v) {
+                int b = prop[v];
+                if (b < 0) continue;
+                incoming[b] += (uint32_t)g->vwgt[v];
+                if (v < minv[b]) minv[b] = v;
+            }
+            for (int v = 0; v < n; ++v) {
+                int b = prop[v];
+                if (b < 0) continue;
+                int ok = ((uint64_t)cw[b] + incoming[b] < kn->cluster_bound) || minv[b] == v;
+                if (!ok) prop[v] = -2 - b; /* rejected, remember target for reset */
+            }
+            /* 3. apply */
+            for (int v = 0; v < n; ++v) {
+                int b = prop[v];
+                if (b == -1) continue;
+                int t = b >= 0 ? b : -2 - b;
+                incoming[t] = 0;
+                minv[t] = INT_MAX;
+                if (b < 0) continue;
+                cw[label[v]] -= (uint32_t)g->vwgt[v];
+                cw[b] += (uint32_t)g->vwgt[v];
+                label[v] = b;
+            }
+        }
+    }
+    acc_free(&a);
+    free(cw); free(prop); free(incoming); free(minv); free(seen);
+}
+
+int or_lp_cluster_seq(const or_graph* g, uint32_t bound, int rounds, const int* order, int* label) {
+    const int n = g->n;
+    uint32_t* cw = xmalloc(sizeof(uint32_t) * (size_t)(n ? n : 1));
+    char* seen = xcalloc((size_t)n, 1);
+    or_acc a;
+    acc_init(&a, n, max_degree(g));
+    for (int v = 0; v < n; ++v) { label[v] = v; cw[v] = (uint32_t)g->vwgt[v]; }
+    for (int r = 0; r < rounds; ++r)
+        for (int i = 0; i < n; ++i) {
+            int v = order[i];
+            int b = cluster_choice(g, v, label, cw, bound, &a, seen, 0);
+            cw[label[v]] -= (uint32_t)g->vwgt[v];
+            cw[b] += (uint32_t)g->vwgt[v];
+            label[v] = b;
+        }
+    /* remap_cluster_ids, size_constraint_label_propagation.cpp:207-232 */
+    int* remap = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    for (int v = 0; v < n; ++v) remap[v] = -1;
+    int nc = 0;
+    for (int v = 0; v < n; ++v) {
+        if (remap[label[v]] < 0) remap[label[v]] = nc++;
+        label[v] = remap[label[v]];
+    }
+    free(remap);
+    acc_free(&a);
+    free(cw); free(seen);
+    return nc;
+}
+
+/* ------------------------------------------------------------- contraction */
+
+static int cmp_int(const void* x, const void* y) {
+    int a = *(const int*)x, b = *(const int*)y;
+    return (a > b) - (a < b);
+}
+
+int or_contract(const or_graph* g, const int* label, int* cmap, int* cxadj, int* cadjncy,
+                int* cadjwgt, int* cvwgt) {
+    const int n = g->n;
+    /* coarse ids in order of each cluster's smallest member = order of first
+     * appearance, as remap_cluster_ids (size_constraint_label_propagation.cpp:
+     * 207-232) and the matching leaders (random_matching.cpp:104-110) number them */
+    int* cid = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    for (int v = 0; v < n; ++v) cid[v] = -1;
+    int nc = 0;
+    for (int v = 0; v < n; ++v) {
+        if (cid[label[v]] < 0) cid[label[v]] = nc++;
+        cmap[v] = cid[label[v]];
+    }
+    free(cid);
+    for (int c = 0; c < nc; ++c) cvwgt[c] = 0;
+    for (int v = 0; v < n; ++v) cvwgt[cmap[v]] += g->vwgt[v];
+    /* members of each coarse node */
+    int* start = xcalloc((size_t)nc + 1, sizeof(int));
+    int* mem = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    for (int v = 0; v < n; ++v) start[cmap[v] + 1]++;
+    for (int c = 0; c < nc; ++c) start[c + 1] += start[c];
+    {
+        int* fill = xmalloc(sizeof(int) * (size_t)(nc ? nc : 1));
+        for (int c = 0; c < nc; ++c) fill[c] = start[c];
+        for (int v = 0; v < n; ++v) mem[fill[cmap[v]]++] = v;
+        free(fill);
+    }
+    /* contraction.h:60-82 / complete_boundary.h:538-556: drop edges inside a
+     * coarse node, sum the weights of parallel edges.  Rows are emitted
+     * sorted by target. */
+    uint32_t* acc = xcalloc((size_t)nc, sizeof(uint32_t));
+    char* seen = xcalloc((size_t)nc, 1);
+    int* touched = xmalloc(sizeof(int) * (size_t)(nc ? nc : 1));
+    int pos = 0;
+    for (int c = 0; c < nc; ++c) {
+        cxadj[c] = pos;
+        int nt = 0;
+        for (int i = start[c]; i < start[c + 1]; ++i) {
+            int v = mem[i];
+            for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) {
+                int t = cmap[g->adjncy[e]];
+                if (t == c) continue;
+                if (!seen[t]) { seen[t] = 1; touched[nt++] = t; }
+                acc[t] += (uint32_t)g->adjwgt[e];
+            }
+        }
+        qsort(touched, (size_t)nt, sizeof(int), cmp_int);
+        for (int i = 0; i < nt; ++i) {
+            int t = touched[i];
+            cadjncy[pos] = t;
+            cadjwgt[pos] = (int)acc[t];
+            ++pos;
+            acc[t] = 0;
+            seen[t] = 0;
+        }
+    }
+    cxadj[nc] = pos;
+    free(start); free(mem); free(acc); free(seen); free(touched);
+    return nc;
+}
+
+/* ---------------------------------------------------------- LP refinement */
+
+/* One node's choice, label_propagation_refinement.cpp:49-78: start from the
+ * own block (connection counts only if the own block is within the bound,
+ * :68), move to a neighbouring block with a strictly larger connection whose
+ * weight stays below the bound (:67). */
+static int refine_choice(const or_graph* g, int v, const int* part, const uint32_t* bw,
+                         uint32_t bound, or_acc* a, char* seen, uint64_t ks_tie) {
+    acc_gather(a, g, v, part, seen);
+    int own = part[v];
+    uint32_t cv = (uint32_t)g->vwgt[v];
+    int own_ok = bw[own] <= bound;
+    int best = own;
+    uint32_t bestc = (own_ok && seen[own]) ? a->acc[own] : 0;
+    for (int i = 0; i < a->ntouched; ++i) {
+        int b = a->touched[i];
+        if (b == own) continue;
+        uint32_t c = a->acc[b];
+        if (c == 0) continue;
+        if (!((uint64_t)bw[b] + cv < bound)) continue;
+        /* when the own block is infeasible bestc starts at 0 < c, so the
+         * "own wins ties" rule of beats() only applies to a feasible own block */
+        if (beats(c, b, bestc, best, own, ks_tie)) { best = b; bestc = c; }
+    }
+    acc_clear(a, seen);
+    return best;
+}
+
+/* Threshold admission into capacity-limited targets: proposals carry a
+ * priority class p in [0,P); classes are admitted in increasing order while
+ * the cumulative weight fits into cap[b]; in the first class that does not
+ * fit, only the proposal of the smallest node id is tried on its own. */
+typedef struct {
+    int P, nt;
+    uint64_t* H;   /* nt * P */
+    int* minv;     /* nt * P */
+} or_admit;
+
+static void admit_init(or_admit* A, int nt, int P) {
+    A->P = P; A->nt = nt;
+    A->H = xcalloc((size_t)nt * (size_t)P, sizeof(uint64_t));
+    A->minv = xmalloc(sizeof(int) * (size_t)nt * (size_t)P);
+    for (size_t i = 0; i < (size_t)nt * (size_t)P; ++i) A->minv[i] = INT_MAX;
+}
+static void admit_free(or_admit* A) { free(A->H); free(A->minv); }
+static void admit_add(or_admit* A, int b, int p, int v, uint32_t w) {
+    size_t i = (size_t)b * (size_t)A->P + (size_t)p;
+    A->H[i] += w;
+    if (v < A->minv[i]) A->minv[i] = v;
+}
+/* returns 1 if proposal (v,b,p,w) is admitted, given cap[b] >= 0 */
+static int admit_test(const or_admit* A, int b, int p, int v, uint32_t w, int64_t cap) {
+    const uint64_t* H = A->H + (size_t)b * (size_t)A->P;
+    uint64_t cum = 0;
+    int t = 0;
+    while (t < A->P && (int64_t)(cum + H[t]) <= cap) { cum += H[t]; ++t; }
+    if (p < t) return 1;
+    if (p == t && A->minv[(size_t)b * (size_t)A->P + (size_t)t] == v && (int64_t)(cum + w) <= cap) return 1;
+    return 0;
+}
+static void admit_reset(or_admit* A, int b) {
+    for (int p = 0; p < A->P; ++p) {
+        A->H[(size_t)b * (size_t)A->P + (size_t)p] = 0;
+        A->minv[(size_t)b * (size_t)A->P + (size_t)p] = INT_MAX;
+    }
+}
+
+void or_lp_refine(const or_graph* g, const or_knobs* kn, int level, uint32_t bound, int* part) {
+    const int n = g->n, k = kn->k;
+    uint32_t* bw = xcalloc((size_t)k, sizeof(uint32_t));
+    or_block_weights(g, part, k, bw);
+    char* active = xmalloc((size_t)(n ? n : 1));
+    char* next_active = xcalloc((size_t)n, 1);
+    int* prop = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    int* cls = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    char* seen = xcalloc((size_t)k, 1);
+    or_acc a;
+    acc_init(&a, k, max_degree(g));
+    or_admit A;
+    admit_init(&A, k, kn->ref_classes);
+    memset(active, 1, (size_t)n);
+    const uint32_t S = (uint32_t)kn->ref_subrounds;
+    for (int r = 0; r < kn->ref_rounds; ++r) {
+        uint64_t ks_sub = or_stream(kn->seed, TAG_RSUB, level, r);
+        uint64_t ks_tie = or_stream(kn->seed, TAG_RTIE, level, r);
+        uint64_t ks_prio = or_stream(kn->seed, TAG_RPRIO, level, r);
+        long long moved = 0;
+        memset(next_active, 0, (size_t)n);
+        for (uint32_t s = 0; s < S; ++s) {
+            for (int v = 0; v < n; ++v) {
+                prop[v] = -1;
+                if (!active[v] || or_hash(ks_sub, (uint32_t)v) % S != s) continue;
+                int b = refine_choice(g, v, part, bw, bound, &a, seen, ks_tie);
+                if (b != part[v]) {
+                    prop[v] = b;
+                    cls[v] = (int)(or_hash(ks_prio, (uint32_t)v) % (uint32_t)kn->ref_classes);
+                    admit_add(&A, b, cls[v], v, (uint32_t)g->vwgt[v]);
+                }
+            }
+            for (int v = 0; v < n; ++v) {
+                int b = prop[v];
+                if (b < 0) continue;
+                int64_t cap = (int64_t)bound - 1 - (int64_t)bw[b];
+                if (!admit_test(&A, b, cls[v], v, (uint32_t)g->vwgt[v], cap)) prop[v] = -2 - b;
+            }
+            for (int v = 0; v < n; ++v) {
+                int b = prop[v];
+                if (b == -1) continue;
+                admit_reset(&A, b >= 0 ? b : -2 - b);
+                if (b < 0) continue;
+                bw[part[v]] -= (uint32_t)g->vwgt[v];
+                bw[b] += (uint32_t)g->vwgt[v];
+                part[v] = b;
+                ++moved;
+                /* label_propagation_refinement.cpp:84-92: neighbours of a moved
+                 * node are visited again in the next round */
+                for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) next_active[g->adjncy[e]] = 1;
+            }
+        }
+        char* t = active; active = next_active; next_active = t;
+        if (moved == 0) break;
+    }
+    acc_free(&a);
+    admit_free(&A);
+    free(bw); free(active); free(next_active); free(prop); free(cls); free(seen);
+}
+
+void or_lp_refine_seq(const or_graph* g, int k, uint32_t bound, int rounds, const int* order,
+                      int* part) {
+    /* label_propagation_refinement.cpp:21-98, queue semantics kept:
+     * round 0 visits every node in `order`; later rounds visit, in push
+     * order, the neighbours of nodes that changed block. */
+    const int n = g->n;
+    uint32_t* bw = xcalloc((size_t)k, sizeof(uint32_t));
+    or_block_weights(g, part, k, bw);
+    int* Q = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    int* NQ = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    char* nq_in = xcalloc((size_t)n, 1);
+    char* seen = xcalloc((size_t)k, 1);
+    or_acc a;
+    acc_init(&a, k, max_degree(g));
+    int qn = n;
+    for (int i = 0; i < n; ++i) Q[i] = order[i];
+    for (int r = 0; r < rounds; ++r) {
+        int nqn = 0;
+        for (int i = 0; i < qn; ++i) {
+            int v = Q[i];
+            int b = refine_choice(g, v, part, bw, bound, &a, seen, 0);
+            int changed = b != part[v];
+            bw[part[v]] -= (uint32_t)g->vwgt[v];
+            bw[b] += (uint32_t)g->vwgt[v];
+            part[v] = b;
+            if (changed)
+                for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) {
+                    int u = g->adjncy[e];
+                    if (!nq_in[u]) { nq_in[u] = 1; NQ[nqn++] = u; }
+                }
+        }
+        int* t = Q; Q = NQ; NQ = t;
+        qn = nqn;
+        for (int i = 0; i < qn; ++i) nq_in[Q[i]] = 0;
+    }
+    acc_free(&a);
+    free(bw); free(Q); free(NQ); free(nq_in); free(seen);
+}
+
+/* --------------------------------------------------------- balance repair */
+
+static int loss_bucket(int64_t loss) {
+    if (loss <= 0) return 0;
+    int b = 1;
+    while (b < 31 && (loss >> b) > 0) ++b; /* b = 1 + floor(log2 loss) */
+    return b;
+}
+
+int or_balance(const or_graph* g, const or_knobs* kn, int level, uint32_t bound, int* part) {
+    const int n = g->n, k = kn->k;
+    uint32_t* bw = xcalloc((size_t)k, sizeof(uint32_t));
+    int* tgt = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    int* cls = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    uint64_t* HS = xcalloc((size_t)k * BAL_CLASSES, sizeof(uint64_t));
+    int* thr = xmalloc(sizeof(int) * (size_t)k);
+    char* seen = xcalloc((size_t)k, 1);
+    or_acc a;
+    acc_init(&a, k, max_degree(g));
+    or_admit A;
+    admit_init(&A, k, kn->ref_classes);
+    int ok = 0;
+    for (int it = 0; it < kn->bal_iters; ++it) {
+        or_block_weights(g, part, k, bw);
+        int over = 0, lightest = 0;
+        for (int b = 0; b < k; ++b) {
+            if (bw[b] > bound) over = 1;
+            if (bw[b] < bw[lightest]) lightest = b;
+        }
+        if (!over) { ok = 1; break; }
+        uint64_t ks_tie = or_stream(kn->seed, TAG_BTIE, level, it);
+        uint64_t ks_cls = or_stream(kn->seed, TAG_BCLS, level, it);
+        uint64_t ks_prio = or_stream(kn->seed, TAG_BPRIO, level, it);
+        /* 1. every node of an overloaded block picks the best target that can
+         *    take it: the most connected feasible neighbouring block, else the
+         *    lightest block */
+        for (int v = 0; v < n; ++v) {
+            tgt[v] = -1;
+            int own = part[v];
+            if (bw[own] <= bound) continue;
+            uint32_t cv = (uint32_t)g->vwgt[v];
+            acc_gather(&a, g, v, part, seen);
+            int t = -1;
+            uint32_t tc = 0;
+            for (int i = 0; i < a.ntouched; ++i) {
+                int b = a.touched[i];
+                if (b == own) continue;
+                if ((uint64_t)bw[b] + cv > bound) continue;
+                uint32_t c = a.acc[b];
+                int better;
+                if (t < 0) better = 1;
+                else if (c != tc) better = c > tc;
+                else {
+                    uint32_t hb = or_hash(ks_tie, (uint32_t)b), ht = or_hash(ks_tie, (uint32_t)t);
+                    better = hb != ht ? hb < ht : b < t;
+                }
+                if (better) { t = b; tc = c; }
+            }
+            if (t < 0 && lightest != own && (uint64_t)bw[lightest] + cv <= bound) { t = lightest; tc = 0; }
+            uint32_t cown = seen[own] ? a.acc[own] : 0;
+            acc_clear(&a, seen);
+            if (t < 0) continue;
+            int64_t loss = (int64_t)cown - (int64_t)tc;
+            tgt[v] = t;
+            cls[v] = loss_bucket(loss) * 8 + (int)(or_hash(ks_cls, (uint32_t)v) % 8u);
+            HS[(size_t)own * BAL_CLASSES + (size_t)cls[v]] += cv;
+        }
+        /* 2. each overloaded block releases its cheapest classes until the
+         *    released weight covers its excess */
+        for (int b = 0; b < k; ++b) {
+            thr[b] = 0;
+            if (bw[b] <= bound) continue;
+            uint64_t excess = bw[b] - bound, cum = 0;
+            int t = 0;
+            while (t < BAL_CLASSES && cum < excess) { cum += HS[(size_t)b * BAL_CLASSES + (size_t)t]; ++t; }
+            thr[b] = t;
+        }
+        /* 3. released nodes are admitted into their targets by priority class */
+        for (int v = 0; v < n; ++v) {
+            if (tgt[v] < 0) continue;
+            if (cls[v] >= thr[part[v]]) { tgt[v] = -1; continue; }
+            cls[v] = (int)(or_hash(ks_prio, (uint32_t)v) % (uint32_t)kn->ref_classes);
+            admit_add(&A, tgt[v], cls[v], v, (uint32_t)g->vwgt[v]);
+        }
+        for (int v = 0; v < n; ++v) {
+            int t = tgt[v];
+            if (t < 0) continue;
+            int64_t cap = (int64_t)bound - (int64_t)bw[t];
+            if (!admit_test(&A, t, cls[v], v, (uint32_t)g->vwgt[v], cap)) tgt[v] = -2 - t;
+        }
+        for (int v = 0; v < n; ++v) {
+            int t = tgt[v];
+            if (t == -1) continue;
+            admit_reset(&A, t >= 0 ? t : -2 - t);
+            if (t < 0) continue;
+            part[v] = t;
+        }
+        memset(HS, 0, sizeof(uint64_t) * (size_t)k * BAL_CLASSES);
+    }
+    if (!ok) {
+        or_block_weights(g, part, k, bw);
+        ok = 1;
+        for (int b = 0; b < k; ++b) if (bw[b] > bound) ok = 0;
+    }
+    acc_free(&a);
+    admit_free(&A);
+    free(bw); free(tgt); free(cls); free(HS); free(thr); free(seen);
+    return ok;
+}
+
+/* ------------------------------------------------- initial partitioning */
+
+/* max-heap of node ids keyed by (gain desc, id asc) with position index */
+typedef struct {
+    int* heap;
+    int* pos;
+    int64_t* key;
+    int size;
+} or_pq;
+
+static void pq_init(or_pq* q, int n, int64_t* key) {
+    q->heap = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    q->pos = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    for (int i = 0; i < n; ++i) q->pos[i] = -1;
+    q->key = key;
+    q->size = 0;
+}
+static void pq_free(or_pq* q) { free(q->heap); free(q->pos); }
+static int pq_less(const or_pq* q, int a, int b) { /* a has lower priority than b */
+    if (q->key[a] != q->key[b]) return q->key[a] < q->key[b];
+    return a > b;
+}
+static void pq_swap(or_pq* q, int i, int j) {
+    int a = q->heap[i], b = q->heap[j];
+    q->heap[i] = b; q->heap[j] = a;
+    q->pos[b] = i; q->pos[a] = j;
+}
+static void pq_up(or_pq* q, int i) {
+    while (i > 0) {
+        int p = (i - 1) / 2;
+        if (!pq_less(q, q->heap[p], q->heap[i])) break;
+        pq_swap(q, i, p);
+        i = p;
+    }
+}
+static void pq_down(or_pq* q, int i) {
+    for (;;) {
+        int l = 2 * i + 1, r = l + 1, m = i;
+        if (l < q->size && pq_less(q, q->heap[m], q->heap[l])) m = l;
+        if (r < q->size && pq_less(q, q->heap[m], q->heap[r])) m = r;
+        if (m == i) break;
+        pq_swap(q, i, m);
+        i = m;
+    }
+}
+static void pq_push(or_pq* q, int v) {
+    q->heap[q->size] = v;
+    q->pos[v] = q->size++;
+    pq_up(q, q->size - 1);
+}
+static int pq_pop(or_pq* q) {
+    int v = q->heap[0];
+    q->pos[v] = -1;
+    --q->size;
+    if (q->size > 0) {
+        q->heap[0] = q->heap[q->size];
+        q->pos[q->heap[0]] = 0;
+        pq_down(q, 0);
+    }
+    return v;
+}
+static void pq_update(or_pq* q, int v) { /* key[v] changed */
+    int i = q->pos[v];
+    pq_up(q, i);
+    pq_down(q, q->pos[v]);
+}
+static void pq_clear(or_pq* q) {
+    for (int i = 0; i < q->size; ++i) q->pos[q->heap[i]] = -1;
+    q->size = 0;
+}
+
+/* last node dequeued by a BFS from s (bipartition.cpp:125-146 grows from a
+ * node found by repeated BFS the same way) */
+static int bfs_last(const or_graph* g, int s, int* queue, char* mark) {
+    int head = 0, tail = 0, last = s;
+    queue[tail++] = s;
+    mark[s] = 1;
+    while (head < tail) {
+        int v = queue[head++];
+        last = v;
+        for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) {
+            int u = g->adjncy[e];
+            if (!mark[u]) { mark[u] = 1; queue[tail++] = u; }
+        }
+    }
+    for (int i = 0; i < tail; ++i) mark[queue[i]] = 0;
+    return last;
+}
+
+static long long cut2(const or_graph* g, const char* side) {
+    long long c = 0;
+    for (int v = 0; v < g->n; ++v)
+        for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e)
+            if (side[v] != side[g->adjncy[e]]) c += g->adjwgt[e];
+    return c / 2;
+}
+
+typedef struct {
+    int n;
+    int *xadj, *adjncy, *adjwgt, *vwgt;
+    int* orig; /* node id in the coarsest graph */
+} or_sub;
+
+/* Greedy graph growing of side 0 from `start` (bipartition.cpp:147-222
+ * restated with a gain queue): the frontier node with the largest
+ * w(v,side0) - w(v,side1) joins next; nodes that would push side 0 above
+ * max0 are skipped; stops once side 0 reaches target0. */
+static void grow(const or_graph* g, int start, uint64_t target0, uint64_t max0, char* side,
+                 int64_t* key, or_pq* q) {
+    const int n = g->n;
+    memset(side, 1, (size_t)n);
+    char* excl = xcalloc((size_t)n, 1);
+    for (int v = 0; v < n; ++v) {
+        int64_t d = 0;
+        for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) d += g->adjwgt[e];
+        key[v] = -d;
+    }
+    uint64_t w0 = 0;
+    int next_free = 0;
+    int cur = start;
+    while (w0 < target0) {
+        int v;
+        if (cur >= 0) { v = cur; cur = -1; }
+        else if (q->size > 0) v = pq_pop(q);
+        else {
+            while (next_free < n && (side[next_free] == 0 || excl[next_free])) ++next_free;
+            if (next_free >= n) break;
+            v = next_free;
+        }
+        if (side[v] == 0 || excl[v]) continue;
+        if (w0 + (uint64_t)g->vwgt[v] > max0) { excl[v] = 1; continue; }
+        side[v] = 0;
+        w0 += (uint64_t)g->vwgt[v];
+        for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) {
+            int u = g->adjncy[e];
+            if (side[u] == 0 || excl[u]) continue;
+            key[u] += 2 * (int64_t)g->adjwgt[e];
+            if (q->pos[u] >= 0) pq_update(q, u);
+            else pq_push(q, u);
+        }
+    }
+    pq_clear(q);
+    free(excl);
+}
+
+static uint64_t overload2(const uint64_t w[2], const uint64_t maxw[2]) {
+    return (w[0] > maxw[0] ? w[0] - maxw[0] : 0) + (w[1] > maxw[1] ? w[1] - maxw[1] : 0);
+}
+
+/* 2-way FM (two_way_fm.cpp restated): per pass, boundary nodes by largest
+ * cut reduction (ties: smaller id), each node moves at most once, a move is
+ * allowed only if the receiving side stays within maxw; afterwards roll back
+ * to the best prefix by (overload, cut).  Returns the cut. */
+static long long fm2(const or_graph* g, char* side, const uint64_t maxw[2], int passes,
+                     int stall_limit, int64_t* key, or_pq* q) {
+    const int n = g->n;
+    uint64_t w[2] = {0, 0};
+    for (int v = 0; v < n; ++v) w[(int)side[v]] += (uint64_t)g->vwgt[v];
+    char* locked = xcalloc((size_t)n, 1);
+    int* moves = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    long long cut = cut2(g, side);
+    for (int pass = 0; pass < passes; ++pass) {
+        for (int v = 0; v < n; ++v) {
+            int64_t in = 0, out = 0;
+            for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) {
+                if (side[g->adjncy[e]] == side[v]) in += g->adjwgt[e];
+                else out += g->adjwgt[e];
+            }
+            key[v] = out - in;
+            if (out > 0) pq_push(q, v);
+        }
+        int nm = 0, best_len = 0, stall = 0;
+        long long cur_cut = cut, best_cut = cut;
+        uint64_t best_ov = overload2(w, maxw);
+        while (q->size > 0 && stall < stall_limit) {
+            int v = pq_pop(q);
+            int from = side[v], to = 1 - from;
+            if (w[to] + (uint64_t)g->vwgt[v] > maxw[to]) continue;
+            side[v] = (char)to;
+            w[from] -= (uint64_t)g->vwgt[v];
+            w[to] += (uint64_t)g->vwgt[v];
+            cur_cut -= key[v];
+            locked[v] = 1;
+            moves[nm++] = v;
+            for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) {
+                int u = g->adjncy[e];
+                if (locked[u]) continue;
+                int64_t d = 2 * (int64_t)g->adjwgt[e];
+                key[u] += side[u] == to ? -d : d;
+                if (q->pos[u] >= 0) pq_update(q, u);
+                else pq_push(q, u);
+            }
+            uint64_t ov = overload2(w, maxw);
+            if (ov < best_ov || (ov == best_ov && cur_cut < best_cut)) {
+                best_ov = ov; best_cut = cur_cut; best_len = nm; stall = 0;
+            } else {
+                ++stall;
+            }
+        }
+        pq_clear(q);
+        for (int i = nm - 1; i >= best_len; --i) {
+            int v = moves[i];
+            int from = side[v], to = 1 - from;
+            side[v] = (char)to;
+            w[from] -= (uint64_t)g->vwgt[v];
+            w[to] += (uint64_t)g->vwgt[v];
+        }
+        for (int i = 0; i < nm; ++i) locked[moves[i]] = 0;
+        cut = best_cut;
+        if (best_len == 0) break;
+    }
+    free(locked);
+    free(moves);
+    return cut;
+}
+
+/* bipartition.cpp:24-75: several growing tries on the coarsest graph of a
+ * bisection, each followed by FM; keep the best by (overload, cut). */
+static void coarsest_bisect(const or_graph* g, uint64_t t0, const uint64_t maxw[2],
+                            const or_knobs* kn, int bis_key, char* best_side) {
+    const int n = g->n;
+    char* side = xmalloc((size_t)(n ? n : 1));
+    int64_t* key = xmalloc(sizeof(int64_t) * (size_t)(n ? n : 1));
+    int* queue = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    char* mark = xcalloc((size_t)n, 1);
+    or_pq q;
+    pq_init(&q, n, key);
+    long long best_cut = LLONG_MAX;
+    uint64_t best_ov = UINT64_MAX;
+    for (int t = 0; t < kn->ip_tries; ++t) {
+        uint64_t ks = or_stream(kn->seed, TAG_IP, bis_key, t);
+        int s0 = 0;
+        uint32_t hbest = UINT32_MAX;
+        for (int v = 0; v < n; ++v) {
+            uint32_t h = or_hash(ks, (uint32_t)v);
+            if (h < hbest) { hbest = h; s0 = v; }
+        }
+        int s1 = bfs_last(g, s0, queue, mark);
+        int start = bfs_last(g, s1, queue, mark);
+        grow(g, start, t0, maxw[0], side, key, &q);
+        long long c = fm2(g, side, maxw, kn->ip_fm_passes, kn->ip_fm_stall, key, &q);
+        uint64_t w[2] = {0, 0};
+        for (int v = 0; v < n; ++v) w[(int)side[v]] += (uint64_t)g->vwgt[v];
+        uint64_t ov = overload2(w, maxw);
+        if (ov < best_ov || (ov == best_ov && c < best_cut)) {
+            best_ov = ov; best_cut = c;
+            memcpy(best_side, side, (size_t)n);
+        }
+    }
+    pq_free(&q);
+    free(side); free(key); free(queue); free(mark);
+}
+
+typedef struct { uint32_t h; int v; } or_hv;
+static int cmp_hv(const void* x, const void* y) {
+    const or_hv* a = (const or_hv*)x;
+    const or_hv* b = (const or_hv*)y;
+    if (a->h != b->h) return a->h < b->h ? -1 : 1;
+    return (a->v > b->v) - (a->v < b->v);
+}
+
+/* Sequential heavy-edge matching on the expansion*^2 rating
+ * (edge_ratings.cpp:316-328, weight bound as random_matching.cpp:85-96):
+ * nodes in hash order; an unmatched node takes its unmatched neighbour of
+ * largest rating (ties: smaller id) with c(u)+c(v) <= maxnode. */
+static void hem(const or_graph* g, uint64_t ks, uint64_t maxnode, int* match) {
+    const int n = g->n;
+    or_hv* ord = xmalloc(sizeof(or_hv) * (size_t)(n ? n : 1));
+    for (int v = 0; v < n; ++v) { ord[v].h = or_hash(ks, (uint32_t)v); ord[v].v = v; match[v] = -1; }
+    qsort(ord, (size_t)n, sizeof(or_hv), cmp_hv);
+    for (int i = 0; i < n; ++i) {
+        int u = ord[i].v;
+        if (match[u] >= 0) continue;
+        uint32_t cu = (uint32_t)g->vwgt[u];
+        int best = -1;
+        double br = 0;
+        for (int e = g->xadj[u]; e < g->xadj[u + 1]; ++e) {
+            int v = g->adjncy[e];
+            if (v == u || match[v] >= 0) continue;
+            uint32_t cv = (uint32_t)g->vwgt[v];
+            if ((uint64_t)cu + cv > maxnode) continue;
+            int w = g->adjwgt[e];
+            double r = 1.0 * w * w / (uint32_t)(cu * cv);
+            if (best < 0 || r > br || (r == br && v < best)) { best = v; br = r; }
+        }
+        if (best < 0) match[u] = u;
+        else { match[u] = best; match[best] = u; }
+    }
+    free(ord);
+}
+
+/* Multilevel bisection (graph_partitioner.cpp:110-145 runs a full k=2
+ * multilevel partitioning): coarsen by matching while the graph has more
+ * than 200 nodes and shrinks by >= 1.1 (multiple_k_stop_rule with
+ * num_vert_stop_factor 100, stop_rules.h:86-112; node weight bound
+ * 1.5*W/200), bisect the coarsest, then FM on every level on the way up. */
+static void ml_bisect(const or_graph* g, uint64_t t0, const uint64_t maxw[2], const or_knobs* kn,
+                      int bis_key, char* side_out) {
+    enum { MAXL = 32 };
+    or_graph H[MAXL + 1];
+    or_sub own[MAXL + 1];
+    int* cmaps[MAXL + 1];
+    H[0] = *g;
+    int L = 0;
+    uint64_t W = 0;
+    for (int v = 0; v < g->n; ++v) W += (uint64_t)g->vwgt[v];
+    uint64_t maxnode = (uint64_t)(1.5 * (double)W / 200.0);
+    while (L < MAXL && H[L].n > 200) {
+        const or_graph* f = &H[L];
+        int* match = xmalloc(sizeof(int) * (size_t)f->n);
+        hem(f, or_stream(kn->seed, TAG_IPM, bis_key, L), maxnode, match);
+        int* label = xmalloc(sizeof(int) * (size_t)f->n);
+        for (int v = 0; v < f->n; ++v) label[v] = match[v] < v ? match[v] : v;
+        free(match);
+        int fm = f->xadj[f->n];
+        or_sub* s = &own[L + 1];
+        s->xadj = xmalloc(sizeof(int) * (size_t)(f->n + 1));
+        s->adjncy = xmalloc(sizeof(int) * (size_t)(fm ? fm : 1));
+        s->adjwgt = xmalloc(sizeof(int) * (size_t)(fm ? fm : 1));
+        s->vwgt = xmalloc(sizeof(int) * (size_t)f->n);
+        s->orig = NULL;
+        cmaps[L] = xmalloc(sizeof(int) * (size_t)f->n);
+        int nc = or_contract(f, label, cmaps[L], s->xadj, s->adjncy, s->adjwgt, s->vwgt);
+        free(label);
+        s->n = nc;
+        if (1.0 * f->n / (double)nc < 1.1) {
+            free(cmaps[L]);
+            free(s->xadj); free(s->adjncy); free(s->adjwgt); free(s->vwgt);
+            break;
+        }
+        H[L + 1].n = nc; H[L + 1].xadj = s->xadj; H[L + 1].adjncy = s->adjncy;
+        H[L + 1].adjwgt = s->adjwgt; H[L + 1].vwgt = s->vwgt;
+        ++L;
+    }
+    char* side = xmalloc((size_t)(H[L].n ? H[L].n : 1));
+    coarsest_bisect(&H[L], t0, maxw, kn, bis_key, side);
+    int64_t* key = xmalloc(sizeof(int64_t) * (size_t)(g->n ? g->n : 1));
+    or_pq q;
+    pq_init(&q, g->n, key);
+    for (int l = L - 1; l >= 0; --l) {
+        char* fs = xmalloc((size_t)(H[l].n ? H[l].n : 1));
+        for (int v = 0; v < H[l].n; ++v) fs[v] = side[cmaps[l][v]];
+        free(side);
+        side = fs;
+        fm2(&H[l], side, maxw, kn->ip_fm_passes, kn->ip_fm_stall, key, &q);
+        free(cmaps[l]);
+        free(own[l + 1].xadj); free(own[l + 1].adjncy); free(own[l + 1].adjwgt); free(own[l + 1].vwgt);
+    }
+    pq_free(&q);
+    free(key);
+    memcpy(side_out, side, (size_t)g->n);
+    free(side);
+}
+
+
+static void sub_free(or_sub* s) {
+    free(s->xadj); free(s->adjncy); free(s->adjwgt); free(s->vwgt); free(s->orig);
+}
+
+/* induced subgraph of the nodes with side[v] == which, ids kept in order */
+static void extract(const or_graph* g, const int* orig, const char* side, int which, or_sub* s) {
+    int* nid = xmalloc(sizeof(int) * (size_t)(g->n ? g->n : 1));
+    int n = 0, m = 0;
+    for (int v = 0; v < g->n; ++v) nid[v] = side[v] == which ? n++ : -1;
+    for (int v = 0; v < g->n; ++v)
+        if (side[v] == which)
+            for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) m += side[g->adjncy[e]] == which;
+    s->n = n;
+    s->xadj = xmalloc(sizeof(int) * (size_t)(n + 1));
+    s->adjncy = xmalloc(sizeof(int) * (size_t)(m ? m : 1));
+    s->adjwgt = xmalloc(sizeof(int) * (size_t)(m ? m : 1));
+    s->vwgt = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    s->orig = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    int pos = 0;
+    for (int v = 0; v < g->n; ++v) {
+        if (side[v] != which) continue;
+        int u = nid[v];
+        s->xadj[u] = pos;
+        s->vwgt[u] = g->vwgt[v];
+        s->orig[u] = orig[v];
+        for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) {
+            int t = g->adjncy[e];
+            if (side[t] != which) continue;
+            s->adjncy[pos] = nid[t];
+            s->adjwgt[pos] = g->adjwgt[e];
+            ++pos;
+        }
+    }
+    s->xadj[n] = pos;
+    free(nid);
+}
+
+static int ceil_log2(int k) {
+    int l = 0;
+    while ((1 << l) < k) ++l;
+    return l;
+}
+
+/* Recursive bisection (graph_partitioner.cpp:110-238 restated): the left
+ * half gets ceil(k/2) blocks; each side may exceed its share of the weight
+ * by eps_b = (1+eps)^(1/ceil(log2 k)) - 1. */
+static void rb(const or_graph* g, const int* orig, int k, int offset, const or_knobs* kn,
+               int rep, int* bis_counter, int* out_part) {
+    if (k == 1 || g->n == 0) {
+        for (int v = 0; v < g->n; ++v) out_part[orig[v]] = offset;
+        return;
+    }
+    const int n = g->n;
+    int bis_id = (*bis_counter)++;
+    int kl = (k + 1) / 2, kr = k - kl;
+    uint64_t W = 0;
+    for (int v = 0; v < n; ++v) W += (uint64_t)g->vwgt[v];
+    uint64_t t0 = W * (uint64_t)kl / (uint64_t)k;
+    uint64_t t1 = W - t0;
+    double eps = kn->imbalance > 0 ? kn->imbalance : 0.0;
+    /* graph_partitioner.cpp:125-133 allows 1-2% per bisection; here the
+     * adaptive (1+eps)^(1/depth)-1, but at least min(eps, 1%) */
+    double eb = pow(1.0 + eps, 1.0 / ceil_log2(k)) - 1.0;
+    double floor_eb = eps < 0.01 ? eps : 0.01;
+    if (eb < floor_eb) eb = floor_eb;
+    uint64_t maxw[2] = {(uint64_t)((1.0 + eb) * (double)t0), (uint64_t)((1.0 + eb) * (double)t1)};
+    char* best_side = xmalloc((size_t)n);
+    ml_bisect(g, t0, maxw, kn, bis_id * 64 + rep, best_side);
+    or_sub L, R;
+    extract(g, orig, best_side, 0, &L);
+    extract(g, orig, best_side, 1, &R);
+    free(best_side);
+    or_graph gl = {L.n, L.xadj, L.adjncy, L.adjwgt, L.vwgt};
+    or_graph gr = {R.n, R.xadj, R.adjncy, R.adjwgt, R.vwgt};
+    rb(&gl, L.orig, kl, offset, kn, rep, bis_counter, out_part);
+    rb(&gr, R.orig, kr, offset + kl, kn, rep, bis_counter, out_part);
+    sub_free(&L);
+    sub_free(&R);
+}
+
+void or_initial_partition(const or_graph* g, const or_knobs* kn, int* part) {
+    /* initial_partitioning.cpp:66-99: several repetitions, keep the best cut */
+    const int n = g->n;
+    int* orig = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    int* cand = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    for (int v = 0; v < n; ++v) orig[v] = v;
+    long long best = LLONG_MAX;
+    for (int rep = 0; rep < kn->ip_reps; ++rep) {
+        int counter = 0;
+        rb(g, orig, kn->k, 0, kn, rep, &counter, cand);
+        long long c = or_edge_cut(g, cand);
+        if (c < best) { best = c; memcpy(part, cand, sizeof(int) * (size_t)n); }
+    }
+    free(orig);
+    free(cand);
+}
+
+/* ------------------------------------------------------------ full call */
+
+typedef struct {
+    or_graph g;
+    int *xadj, *adjncy, *adjwgt, *vwgt; /* owned copies (NULL for level 0) */
+    int* cmap;                          /* fine -> coarse of this level */
+} or_level;
+
+int or_kaffpa(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+              int nparts, double imbalance, int seed, int mode, long long* edgecut, int* part,
+              or_stats* stats) {
+    if (n < 0 || nparts < 1 || !xadj || (n > 0 && !adjncy) || imbalance < 0) return -1;
+    const int m = xadj[n];
+    int* vw = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    int* ew = xmalloc(sizeof(int) * (size_t)(m ? m : 1));
+    for (int v = 0; v < n; ++v) vw[v] = vwgt ? vwgt[v] : 1;
+    for (int e = 0; e < m; ++e) ew[e] = adjcwgt ? adjcwgt[e] : 1;
+    or_knobs kn;
+    or_derive_knobs(n, vw, nparts, imbalance, seed, mode, &kn);
+    or_stats st;
+    memset(&st, 0, sizeof(st));
+
+    or_level lv[64];
+    memset(lv, 0, sizeof(lv));
+    lv[0].g.n = n; lv[0].g.xadj = xadj; lv[0].g.adjncy = adjncy; lv[0].g.adjwgt = ew; lv[0].g.vwgt = vw;
+    int L = 0;
+    /* coarsening.cpp:60-91 level loop with stop_rules.h:64-66 */
+    while (L + 1 < kn.max_levels && lv[L].g.n > 0) {
+        or_graph* f = &lv[L].g;
+        int* label = xmalloc(sizeof(int) * (size_t)f->n);
+        or_lp_cluster(f, &kn, L, label);
+        or_level* c = &lv[L + 1];
+        lv[L].cmap = xmalloc(sizeof(int) * (size_t)f->n);
+        c->xadj = xmalloc(sizeof(int) * (size_t)(f->n + 1));
+        int fm = f->xadj[f->n];
+        c->adjncy = xmalloc(sizeof(int) * (size_t)(fm ? fm : 1));
+        c->adjwgt = xmalloc(sizeof(int) * (size_t)(fm ? fm : 1));
+        c->vwgt = xmalloc(sizeof(int) * (size_t)f->n);
+        int nc = or_contract(f, label, lv[L].cmap, c->xadj, c->adjncy, c->adjwgt, c->vwgt);
+        free(label);
+        c->g.n = nc; c->g.xadj = c->xadj; c->g.adjncy = c->adjncy; c->g.adjwgt = c->adjwgt; c->g.vwgt = c->vwgt;
+        ++L;
+        int cont = (1.0 * f->n / (double)nc >= 1.1) && (uint32_t)nc >= kn.num_stop;
+        if (!cont) break;
+    }
+    /* initial partition of the coarsest graph */
+    int* cpart = xmalloc(sizeof(int) * (size_t)(lv[L].g.n ? lv[L].g.n : 1));
+    or_initial_partition(&lv[L].g, &kn, cpart);
+    st.initial_cut = or_edge_cut(&lv[L].g, cpart);
+    uint32_t* bw = xcalloc((size_t)nparts, sizeof(uint32_t));
+    for (int l = L; l >= 0; --l) {
+        or_graph* g = &lv[l].g;
+        if (l < L) {
+            /* graph_hierarchy.cpp:54-58 projection */
+            int* fp = xmalloc(sizeof(int) * (size_t)(g->n ? g->n : 1));
+            for (int v = 0; v < g->n; ++v) fp[v] = cpart[lv[l].cmap[v]];
+            free(cpart);
+            cpart = fp;
+        }
+        uint32_t bound = l == 0 ? kn.final_bound : kn.upper_bound;
+        or_block_weights(g, cpart, nparts, bw);
+        uint32_t mx = 0;
+        for (int b = 0; b < nparts; ++b) if (bw[b] > mx) mx = bw[b];
+        if (mx > bound) or_balance(g, &kn, l, bound, cpart);
+        or_lp_refine(g, &kn, l, bound, cpart);
+        or_block_weights(g, cpart, nparts, bw);
+        mx = 0;
+        for (int b = 0; b < nparts; ++b) if (bw[b] > mx) mx = bw[b];
+        if (l < 64) {
+            st.level_n[l] = g->n;
+            st.level_m[l] = g->xadj[g->n];
+            st.level_cut[l] = or_edge_cut(g, cpart);
+            st.level_maxbw[l] = mx;
+        }
+        if (l == 0) st.balanced = mx <= bound;
+    }
+    st.levels = L + 1;
+    memcpy(part, cpart, sizeof(int) * (size_t)n);
+    *edgecut = st.level_cut[0];
+    if (stats) *stats = st;
+    free(cpart);
+    free(bw);
+    for (int l = 0; l <= L; ++l) {
+        free(lv[l].cmap);
+        if (l > 0) { free(lv[l].xadj); free(lv[l].adjncy); free(lv[l].adjwgt); free(lv[l].vwgt); }
+    }
+    free(vw);
+    free(ew);
+    return 0;
+}

@@ -1,0 +1,295 @@
+"""ctypes bindings of the checkers -- TEST INFRASTRUCTURE ONLY.
+
+* liboracle.so      : the C restatement of the deterministic schedule.
+* _ref/libkahip_ref.so : the reference KaHIP library compiled from its own
+  sources by oracle/Makefile (present only where the reference sources were
+  available at build time), with ref_harness.cpp's single-routine entry points.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU legs import this.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_OR = None
+_REF = None
+
+c_int_p = ctypes.POINTER(ctypes.c_int)
+
+
+class Knobs(ctypes.Structure):
+    _fields_ = [("k", ctypes.c_int), ("imbalance", ctypes.c_double), ("seed", ctypes.c_int),
+                ("mode", ctypes.c_int), ("total_weight", ctypes.c_uint32),
+                ("upper_bound", ctypes.c_uint32), ("final_bound", ctypes.c_uint32),
+                ("num_stop", ctypes.c_uint32), ("max_vertex_weight", ctypes.c_uint32),
+                ("cluster_bound", ctypes.c_uint32),
+                ("lpc_rounds", ctypes.c_int), ("lpc_subrounds", ctypes.c_int),
+                ("ref_rounds", ctypes.c_int), ("ref_subrounds", ctypes.c_int),
+                ("ref_classes", ctypes.c_int), ("bal_iters", ctypes.c_int),
+                ("ip_reps", ctypes.c_int), ("ip_tries", ctypes.c_int),
+                ("ip_fm_passes", ctypes.c_int), ("ip_fm_stall", ctypes.c_int),
+                ("max_levels", ctypes.c_int)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("levels", ctypes.c_int), ("level_n", ctypes.c_int * 64),
+                ("level_m", ctypes.c_longlong * 64), ("level_cut", ctypes.c_longlong * 64),
+                ("level_maxbw", ctypes.c_uint32 * 64), ("initial_cut", ctypes.c_longlong),
+                ("balanced", ctypes.c_int)]
+
+
+class Graph(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("xadj", c_int_p), ("adjncy", c_int_p),
+                ("adjwgt", c_int_p), ("vwgt", c_int_p)]
+
+
+def _p(a):
+    return a.ctypes.data_as(c_int_p) if a is not None else None
+
+
+def lib():
+    global _OR
+    if _OR is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError("oracle/liboracle.so missing: run `make -C oracle`")
+        L = ctypes.CDLL(path)
+        L.or_edge_cut.restype = ctypes.c_longlong
+        L.or_balance_ratio.restype = ctypes.c_double
+        L.or_lp_cluster_seq.restype = ctypes.c_int
+        L.or_contract.restype = ctypes.c_int
+        L.or_balance.restype = ctypes.c_int
+        L.or_kaffpa.restype = ctypes.c_int
+        L.or_hash.restype = ctypes.c_uint32
+        L.or_hash.argtypes = [ctypes.c_uint64, ctypes.c_uint32]
+        L.or_stream.restype = ctypes.c_uint64
+        L.or_stream.argtypes = [ctypes.c_int] * 4
+        L.or_mix64.restype = ctypes.c_uint64
+        L.or_mix64.argtypes = [ctypes.c_uint64]
+        _OR = L
+    return _OR
+
+
+def ref_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libkahip_ref.so"))
+
+
+def ref():
+    global _REF
+    if _REF is None:
+        path = os.path.join(HERE, "_ref", "libkahip_ref.so")
+        if not os.path.exists(path):
+            raise RuntimeError("oracle/_ref/libkahip_ref.so missing: run `make -C oracle ref`")
+        L = ctypes.CDLL(path)
+        L.ref_edge_cut.restype = ctypes.c_int
+        L.ref_balance.restype = ctypes.c_double
+        L.ref_stop_rule_continue.restype = ctypes.c_int
+        _REF = L
+    return _REF
+
+
+class G:
+    """Keeps numpy arrays alive behind an or_graph struct."""
+
+    def __init__(self, g: dict):
+        self.d = {k: (np.ascontiguousarray(v, np.int32) if isinstance(v, np.ndarray) else v)
+                  for k, v in g.items()}
+        d = self.d
+        self.s = Graph(d["n"], _p(d["xadj"]), _p(d["adjncy"]), _p(d["adjwgt"]), _p(d["vwgt"]))
+
+    @property
+    def ref(self):
+        return ctypes.byref(self.s)
+
+
+# ------------------------------------------------------------------ oracle
+
+def knobs(g: dict, k: int, imbalance=0.03, seed=0, mode=0) -> Knobs:
+    kn = Knobs()
+    lib().or_derive_knobs(g["n"], _p(g["vwgt"]), k, ctypes.c_double(imbalance), seed, mode,
+                          ctypes.byref(kn))
+    return kn
+
+
+def edge_cut(g: dict, part) -> int:
+    return lib().or_edge_cut(G(g).ref, _p(np.ascontiguousarray(part, np.int32)))
+
+
+def block_weights(g: dict, part, k: int) -> np.ndarray:
+    bw = np.zeros(k, np.uint32)
+    lib().or_block_weights(G(g).ref, _p(np.ascontiguousarray(part, np.int32)), k,
+                           bw.ctypes.data_as(ctypes.c_void_p))
+    return bw
+
+
+def rating(g: dict) -> np.ndarray:
+    out = np.empty(g["m"], np.float64)
+    lib().or_rate_expansion_star_2(G(g).ref, out.ctypes.data_as(ctypes.c_void_p))
+    return out
+
+
+def lp_cluster(g: dict, kn: Knobs, level=0) -> np.ndarray:
+    lab = np.empty(g["n"], np.int32)
+    lib().or_lp_cluster(G(g).ref, ctypes.byref(kn), level, _p(lab))
+    return lab
+
+
+def lp_cluster_seq(g: dict, bound: int, rounds: int, order) -> np.ndarray:
+    lab = np.empty(g["n"], np.int32)
+    lib().or_lp_cluster_seq(G(g).ref, ctypes.c_uint32(bound), rounds,
+                            _p(np.ascontiguousarray(order, np.int32)), _p(lab))
+    return lab
+
+
+def contract(g: dict, label) -> tuple[dict, np.ndarray]:
+    n, m = g["n"], g["m"]
+    cmap = np.empty(n, np.int32)
+    cx = np.empty(n + 1, np.int32)
+    ca = np.empty(max(m, 1), np.int32)
+    cw = np.empty(max(m, 1), np.int32)
+    cv = np.empty(max(n, 1), np.int32)
+    nc = lib().or_contract(G(g).ref, _p(np.ascontiguousarray(label, np.int32)), _p(cmap), _p(cx),
+                           _p(ca), _p(cw), _p(cv))
+    mc = int(cx[nc])
+    return dict(n=nc, m=mc, xadj=cx[:nc + 1].copy(), adjncy=ca[:mc].copy(), adjwgt=cw[:mc].copy(),
+                vwgt=cv[:nc].copy()), cmap
+
+
+def lp_refine(g: dict, kn: Knobs, part, bound: int, level=0) -> np.ndarray:
+    p = np.array(part, np.int32)
+    lib().or_lp_refine(G(g).ref, ctypes.byref(kn), level, ctypes.c_uint32(bound), _p(p))
+    return p
+
+
+def lp_refine_seq(g: dict, k: int, bound: int, rounds: int, order, part) -> np.ndarray:
+    p = np.array(part, np.int32)
+    lib().or_lp_refine_seq(G(g).ref, k, ctypes.c_uint32(bound), rounds,
+                           _p(np.ascontiguousarray(order, np.int32)), _p(p))
+    return p
+
+
+def balance(g: dict, kn: Knobs, part, bound: int, level=0) -> tuple[np.ndarray, int]:
+    p = np.array(part, np.int32)
+    ok = lib().or_balance(G(g).ref, ctypes.byref(kn), level, ctypes.c_uint32(bound), _p(p))
+    return p, ok
+
+
+def initial_partition(g: dict, kn: Knobs) -> np.ndarray:
+    p = np.empty(g["n"], np.int32)
+    lib().or_initial_partition(G(g).ref, ctypes.byref(kn), _p(p))
+    return p
+
+
+def kaffpa(g: dict, k: int, imbalance=0.03, seed=0, mode=0, unit_weights=False):
+    """Returns (edgecut, part, stats)."""
+    part = np.empty(g["n"], np.int32)
+    cut = ctypes.c_longlong()
+    st = Stats()
+    rc = lib().or_kaffpa(g["n"], None if unit_weights else _p(g["vwgt"]), _p(g["xadj"]),
+                         None if unit_weights else _p(g["adjwgt"]), _p(g["adjncy"]), k,
+                         ctypes.c_double(imbalance), seed, mode, ctypes.byref(cut), _p(part),
+                         ctypes.byref(st))
+    if rc != 0:
+        raise ValueError(f"or_kaffpa rejected the input ({rc})")
+    return cut.value, part, st
+
+
+# --------------------------------------------------------------- reference
+
+def ref_kaffpa(g: dict, k: int, imbalance=0.03, seed=0, mode=0):
+    """Reference kaffpa() from the library built out of the reference sources."""
+    L = ref()
+    n = ctypes.c_int(g["n"])
+    kk = ctypes.c_int(k)
+    imb = ctypes.c_double(imbalance)
+    cut = ctypes.c_int()
+    part = np.empty(g["n"], np.int32)
+    L.kaffpa(ctypes.byref(n), _p(g["vwgt"]), _p(g["xadj"]), _p(g["adjwgt"]), _p(g["adjncy"]),
+             ctypes.byref(kk), ctypes.byref(imb), ctypes.c_bool(True), seed, mode,
+             ctypes.byref(cut), _p(part))
+    return cut.value, part
+
+
+def ref_balance_config(n: int, vwgt, k: int, imbalance=0.03, mode=0):
+    u, ns, mv = ctypes.c_uint(), ctypes.c_uint(), ctypes.c_uint()
+    ref().ref_balance_config(n, _p(vwgt), k, ctypes.c_double(imbalance), mode, ctypes.byref(u),
+                             ctypes.byref(ns), ctypes.byref(mv))
+    return u.value, ns.value, mv.value
+
+
+def ref_edge_cut(g: dict, part, k: int) -> int:
+    return ref().ref_edge_cut(g["n"], _p(g["xadj"]), _p(g["adjncy"]), _p(g["adjwgt"]),
+                              _p(np.ascontiguousarray(part, np.int32)), k)
+
+
+def ref_balance(g: dict, part, k: int) -> float:
+    return ref().ref_balance(g["n"], _p(g["xadj"]), _p(g["adjncy"]), _p(g["vwgt"]),
+                             _p(np.ascontiguousarray(part, np.int32)), k)
+
+
+def ref_rating(g: dict) -> np.ndarray:
+    out = np.empty(g["m"], np.float64)
+    ref().ref_rate_expansion_star_2(g["n"], _p(g["xadj"]), _p(g["adjncy"]), _p(g["vwgt"]),
+                                    _p(g["adjwgt"]), out.ctypes.data_as(ctypes.c_void_p))
+    return out
+
+
+def _ref_contract(fn, g, arr):
+    n, m = g["n"], g["m"]
+    nc = ctypes.c_int()
+    cx = np.empty(n + 1, np.int32)
+    ca = np.empty(max(m, 1), np.int32)
+    cw = np.empty(max(m, 1), np.int32)
+    cv = np.empty(max(n, 1), np.int32)
+    cmap = np.empty(n, np.int32)
+    fn(n, _p(g["xadj"]), _p(g["adjncy"]), _p(g["vwgt"]), _p(g["adjwgt"]),
+       _p(np.ascontiguousarray(arr, np.int32)), ctypes.byref(nc), _p(cx), _p(ca), _p(cw), _p(cv),
+       _p(cmap))
+    k = nc.value
+    mc = int(cx[k])
+    return dict(n=k, m=mc, xadj=cx[:k + 1].copy(), adjncy=ca[:mc].copy(), adjwgt=cw[:mc].copy(),
+                vwgt=cv[:k].copy()), cmap
+
+
+def ref_contract_clustering(g: dict, cluster):
+    return _ref_contract(ref().ref_contract_clustering, g, cluster)
+
+
+def ref_contract_matching(g: dict, match):
+    return _ref_contract(ref().ref_contract_matching, g, match)
+
+
+def ref_degree_order(g: dict) -> np.ndarray:
+    o = np.empty(g["n"], np.int32)
+    ref().ref_degree_order(g["n"], _p(g["xadj"]), _p(g["adjncy"]), _p(o))
+    return o
+
+
+def ref_lp_cluster(g: dict, bound: int, iterations: int) -> np.ndarray:
+    out = np.empty(g["n"], np.int32)
+    nb = ctypes.c_int()
+    ref().ref_lp_cluster(g["n"], _p(g["xadj"]), _p(g["adjncy"]), _p(g["vwgt"]), _p(g["adjwgt"]),
+                         ctypes.c_uint(bound), iterations, _p(out), ctypes.byref(nb))
+    return out
+
+
+def ref_lp_refine(g: dict, k: int, bound: int, iterations: int, part) -> np.ndarray:
+    p = np.array(part, np.int32)
+    ref().ref_lp_refine(g["n"], _p(g["xadj"]), _p(g["adjncy"]), _p(g["vwgt"]), _p(g["adjwgt"]), k,
+                        ctypes.c_uint(bound), iterations, _p(p))
+    return p
+
+
+def canonical(g: dict) -> dict:
+    """Rows sorted by target (for comparing graphs whose row order differs)."""
+    xadj, adj, w = g["xadj"], g["adjncy"].copy(), g["adjwgt"].copy()
+    for v in range(g["n"]):
+        s, e = xadj[v], xadj[v + 1]
+        o = np.argsort(adj[s:e], kind="stable")
+        adj[s:e] = adj[s:e][o]
+        w[s:e] = w[s:e][o]
+    return dict(g, adjncy=adj, adjwgt=w)
