@@ -1,0 +1,141 @@
+/* kahip_b200.h -- extended C ABI of the B200 KaFFPa library (libkahip_b200.so).
+ *
+ * The drop-in entry point kaffpa() and its siblings are declared in
+ * kaHIP_interface.h with the reference's exact signatures.  This header adds
+ * status-returning variants, a device-pointer variant, and one entry point
+ * per phase of the multilevel scheme so that each phase can be checked
+ * against the CPU oracle.  Plain pointers and sizes only.
+ *
+ * Conventions: graphs are METIS-style int32 CSR (xadj[n+1], adjncy[xadj[n]],
+ * optional adjwgt[xadj[n]] and vwgt[n]; NULL = unit weights), symmetric,
+ * 0-based, no self loops.  Host-pointer entry points copy to the current CUDA
+ * device and back.  Every int-returning call returns 0 on success, a negative
+ * kb200 status on failure (kb200_last_error() describes it), or
+ * KB200_WARN_IMBALANCED when a partition was produced but a block exceeds the
+ * bound.
+ */
+#ifndef KAHIP_B200_H
+#define KAHIP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KB200_OK 0
+#define KB200_ERR_INVALID_INPUT (-1)
+#define KB200_ERR_CUDA (-2)
+#define KB200_ERR_NO_DEVICE (-3)
+#define KB200_ERR_OUT_OF_MEMORY (-4)
+#define KB200_ERR_INTERNAL (-5)
+#define KB200_WARN_IMBALANCED 1
+
+/* Parameters of one call.  kb200_derive_knobs() fills them from
+ * (n, vwgt, k, imbalance, seed, mode) following
+ *   app/balance_configuration.h:19-56   (upper_bound, total_weight),
+ *   lib/partition/coarsening/stop_rules/stop_rules.h:46-66 (num_stop,
+ *                                         max_vertex_weight),
+ *   size_constraint_label_propagation.cpp:57 (cluster_bound),
+ *   app/configuration.h:83-134          (fast / eco presets). */
+typedef struct kb200_knobs {
+    int k;
+    double imbalance;          /* fraction, as kaffpa() takes it */
+    int seed;
+    int mode;                  /* FAST=0 ECO=1 STRONG=2 FASTSOCIAL=3 ECOSOCIAL=4 STRONGSOCIAL=5 */
+    uint32_t total_weight;
+    uint32_t upper_bound;      /* U = (1+eps)*ceil(W/k), truncated */
+    uint32_t final_bound;      /* U, or ceil(W/k) when imbalance == 0 */
+    uint32_t num_stop;
+    uint32_t max_vertex_weight;
+    uint32_t cluster_bound;    /* strict bound on cluster weight during coarsening */
+    int lpc_rounds, lpc_subrounds;                 /* clustering */
+    int ref_rounds, ref_subrounds, ref_classes;    /* refinement */
+    int bal_iters;                                 /* balance repair */
+    int ip_reps, ip_tries, ip_fm_passes, ip_fm_stall; /* initial partitioning */
+    int max_levels;
+} kb200_knobs;
+
+/* Per-call report.  level 0 is the input graph. */
+typedef struct kb200_stats {
+    int levels;
+    int level_n[64];
+    long long level_m[64];
+    long long level_cut[64];       /* cut after refinement (filled when collect_level_cuts) */
+    uint32_t level_maxbw[64];
+    long long initial_cut;         /* cut of the initial partition of the coarsest graph */
+    int balanced;                  /* final max block weight <= final_bound */
+    /* inputs to the report */
+    int collect_level_cuts;        /* in: 1 = compute the cut at every level */
+    int timing;                    /* in: 1 = time kernel families with CUDA events */
+    /* timings (milliseconds) */
+    double ms_total;               /* wall time of the call on the host */
+    double ms_h2d, ms_coarsen, ms_initial, ms_uncoarsen, ms_d2h;
+    /* kernel families (timing == 1): device ms, algorithmic bytes, launches */
+    int nfamilies;
+    char family_name[16][24];
+    double family_ms[16];
+    double family_bytes[16];
+    long long family_launches[16];
+    /* LP sweep work actually performed */
+    long long sweep_vertices, sweep_edges;
+    size_t device_bytes_peak;
+} kb200_stats;
+
+int kb200_derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, int mode,
+                       kb200_knobs* out);
+
+/* Whole multilevel partitioning with host buffers (kaffpa() semantics,
+ * interface/kaHIP_interface.h:30-33) plus status and report. */
+int kb200_kaffpa(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+                 int nparts, double imbalance, int seed, int mode, long long* edgecut, int* part,
+                 kb200_stats* stats);
+
+/* Same with device buffers on the current device; part is a device array.
+ * stream: a cudaStream_t (NULL = a stream owned by the library). */
+int kb200_kaffpa_device(int n, const int* d_vwgt, const int* d_xadj, const int* d_adjcwgt,
+                        const int* d_adjncy, int nparts, double imbalance, int seed, int mode,
+                        long long* edgecut, int* d_part, void* stream, kb200_stats* stats);
+
+/* ---- phases (host buffers), for parity checks against the CPU oracle ---- */
+
+/* LP clustering of one coarsening level: label[n] out. */
+int kb200_lp_cluster(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                     const kb200_knobs* kn, int level, int* label);
+
+/* Contraction of a clustering.  Outputs: nc, mc, cmap[n], cxadj[nc+1],
+ * cadjncy/cadjwgt[mc] (capacity xadj[n]), cvwgt[nc] (capacity n). */
+int kb200_contract(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                   const int* label, int* nc, long long* mc, int* cmap, int* cxadj, int* cadjncy,
+                   int* cadjwgt, int* cvwgt);
+
+/* LP refinement at one level: part[n] in/out. */
+int kb200_lp_refine(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                    const kb200_knobs* kn, int level, uint32_t bound, int* part);
+
+/* Balance repair: part[n] in/out; *balanced = 1 if every block <= bound. */
+int kb200_balance(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                  const kb200_knobs* kn, int level, uint32_t bound, int* part, int* balanced);
+
+/* Edge cut and block weights (bw[k], may be NULL) of a partition. */
+int kb200_edge_cut(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                   const int* part, int k, long long* cut, uint32_t* bw);
+
+/* Projection part_fine[v] = part_coarse[cmap[v]]. */
+int kb200_project(int n, const int* cmap, int nc, const int* part_coarse, int* part_fine);
+
+/* Host initial partitioner (recursive multilevel bisection) of a small graph. */
+int kb200_initial_partition(int n, const int* xadj, const int* adjncy, const int* adjwgt,
+                            const int* vwgt, const kb200_knobs* kn, int* part);
+
+/* Last error message of the calling thread ("" if none). */
+const char* kb200_last_error(void);
+
+/* Number of CUDA devices visible (0 when none). */
+int kb200_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

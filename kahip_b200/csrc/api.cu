@@ -1,0 +1,541 @@
+// api.cu -- the C ABI of libkahip_b200.so.
+//
+// kaffpa() keeps the reference signature (interface/kaHIP_interface.h:30-33)
+// and semantics (interface/kaHIP_interface.cpp:146-166): Metis-style CSR in,
+// edge cut and part[] out, caller owns every array, imbalance is a fraction.
+// Unlike the reference it validates its input on the host; on failure it
+// sets *edgecut = -1 and leaves part[] untouched (the reference has no
+// error channel).  There is no CPU fallback: without a CUDA device the call
+// fails.
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "contract.cuh"
+#include "host/initial_partitioning.h"
+#include "knobs.h"
+#include "partitioner.cuh"
+#include "prims.cuh"
+
+extern "C" {
+#include "../../include/kaHIP_interface.h"
+}
+
+namespace kb {
+namespace {
+
+thread_local std::string g_last_error;
+
+// Contexts are cached per device and reused across calls (streams, pinned
+// buffers and the device arenas survive); one call owns a context at a time.
+std::mutex g_pool_mu;
+std::vector<std::unique_ptr<Ctx>> g_pool[64];
+
+struct Lease {
+    std::unique_ptr<Ctx> ctx;
+    int dev;
+    explicit Lease(int d) : dev(d) {
+        {
+            std::lock_guard<std::mutex> lk(g_pool_mu);
+            if (!g_pool[d].empty()) {
+                ctx = std::move(g_pool[d].back());
+                g_pool[d].pop_back();
+            }
+        }
+        if (!ctx) ctx.reset(new Ctx());
+        ctx->init(d, nullptr);
+    }
+    ~Lease() {
+        if (!ctx) return;
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        g_pool[dev].push_back(std::move(ctx));
+    }
+};
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int current_device(int* dev) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        (void)cudaGetLastError();
+        return fail(KB_ERR_NO_DEVICE, "no CUDA device available (this library has no CPU path)");
+    }
+    e = cudaGetDevice(dev);
+    if (e != cudaSuccess || *dev < 0 || *dev >= 64) return fail(KB_ERR_NO_DEVICE, "cudaGetDevice failed");
+    return KB_OK;
+}
+
+// Host-side validation of a CSR graph (monotone xadj, targets in range,
+// non-negative weights).
+int validate(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt) {
+    if (n < 0) return fail(KB_ERR_INVALID_INPUT, "n < 0");
+    if (!xadj) return fail(KB_ERR_INVALID_INPUT, "xadj is NULL");
+    if (xadj[0] != 0) return fail(KB_ERR_INVALID_INPUT, "xadj[0] != 0");
+    for (int v = 0; v < n; ++v)
+        if (xadj[v + 1] < xadj[v]) return fail(KB_ERR_INVALID_INPUT, "xadj is not monotone");
+    const long long m = xadj[n];
+    if (m > 0 && !adjncy) return fail(KB_ERR_INVALID_INPUT, "adjncy is NULL");
+    for (long long e = 0; e < m; ++e)
+        if (adjncy[e] < 0 || adjncy[e] >= n) return fail(KB_ERR_INVALID_INPUT, "adjncy entry out of range");
+    if (adjwgt)
+        for (long long e = 0; e < m; ++e)
+            if (adjwgt[e] < 0) return fail(KB_ERR_INVALID_INPUT, "negative edge weight");
+    if (vwgt)
+        for (int v = 0; v < n; ++v)
+            if (vwgt[v] < 0) return fail(KB_ERR_INVALID_INPUT, "negative node weight");
+    return KB_OK;
+}
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        return f();
+    } catch (const CudaError& e) {
+        (void)cudaGetLastError();
+        return fail(e.code == cudaErrorMemoryAllocation ? KB_ERR_OUT_OF_MEMORY : KB_ERR_CUDA, e.what());
+    } catch (const std::bad_alloc&) {
+        return fail(KB_ERR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (const std::exception& e) {
+        return fail(KB_ERR_INTERNAL, e.what());
+    }
+}
+
+// Device copies of a host graph (unit weights expanded on the device).
+struct Upload {
+    DevGraph g;
+    int* part = nullptr;
+};
+
+Upload upload(Ctx& ctx, int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt) {
+    Upload u;
+    const long long m = xadj[n];
+    cudaStream_t s = ctx.stream;
+    int* dx = ctx.hier.alloc<int>((size_t)n + 1);
+    int* da = ctx.hier.alloc<int>((size_t)std::max<long long>(m, 1));
+    int* dw = ctx.hier.alloc<int>((size_t)std::max<long long>(m, 1));
+    int* dv = ctx.hier.alloc<int>((size_t)std::max(n, 1));
+    u.part = ctx.hier.alloc<int>((size_t)std::max(n, 1));
+    KB_CUDA(cudaMemcpyAsync(dx, xadj, sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice, s));
+    if (m) KB_CUDA(cudaMemcpyAsync(da, adjncy, sizeof(int) * (size_t)m, cudaMemcpyHostToDevice, s));
+    if (adjwgt) {
+        if (m) KB_CUDA(cudaMemcpyAsync(dw, adjwgt, sizeof(int) * (size_t)m, cudaMemcpyHostToDevice, s));
+    } else {
+        fill_i32(dw, m, 1, s);
+    }
+    if (vwgt) {
+        if (n) KB_CUDA(cudaMemcpyAsync(dv, vwgt, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, s));
+    } else {
+        fill_i32(dv, n, 1, s);
+    }
+    u.g.n = n;
+    u.g.m = m;
+    u.g.xadj = dx;
+    u.g.adjncy = da;
+    u.g.adjwgt = dw;
+    u.g.vwgt = dv;
+    return u;
+}
+
+void fill_stats_families(Ctx& ctx, kb200_stats* st) {
+    if (!st) return;
+    ctx.collect();
+    st->nfamilies = (int)std::min<size_t>(ctx.phases.size(), 16);
+    for (int i = 0; i < st->nfamilies; ++i) {
+        std::strncpy(st->family_name[i], ctx.phases[i].name.c_str(), 23);
+        st->family_name[i][23] = 0;
+        st->family_ms[i] = ctx.phases[i].ms;
+        st->family_bytes[i] = ctx.phases[i].bytes;
+        st->family_launches[i] = ctx.phases[i].launches;
+    }
+    unsigned long long w[2] = {0, 0};
+    KB_CUDA(cudaMemcpy(w, ctx.work, sizeof(w), cudaMemcpyDeviceToHost));
+    st->sweep_vertices = (long long)w[0];
+    st->sweep_edges = (long long)w[1];
+    st->device_bytes_peak = ctx.hier.peak() + ctx.scratch.peak();
+}
+
+void begin_stats(Ctx& ctx, kb200_stats* st) {
+    ctx.timing = st && st->timing;
+    ctx.reset_stats();
+}
+
+using clk = std::chrono::steady_clock;
+double ms_since(clk::time_point t) { return std::chrono::duration<double, std::milli>(clk::now() - t).count(); }
+
+int run_host(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy, int nparts,
+             double imbalance, int seed, int mode, long long* edgecut, int* part, kb200_stats* st) {
+    auto t0 = clk::now();
+    int rc = validate(n, xadj, adjncy, adjcwgt, vwgt);
+    if (rc) return rc;
+    if (nparts < 1) return fail(KB_ERR_INVALID_INPUT, "nparts < 1");
+    if (!(imbalance >= 0)) return fail(KB_ERR_INVALID_INPUT, "imbalance must be >= 0");
+    if (!edgecut || (n > 0 && !part)) return fail(KB_ERR_INVALID_INPUT, "edgecut/part is NULL");
+    int dev;
+    if ((rc = current_device(&dev))) return rc;
+    Knobs kn;
+    derive_knobs(n, vwgt, nparts, imbalance, seed, mode, kn);
+    Lease lease(dev);
+    Ctx& ctx = *lease.ctx;
+    const long long m = xadj[n];
+    for (int attempt = 0;; ++attempt) {
+        try {
+            reserve_for(ctx, n, m, true, attempt == 0 ? 1.0 : 2.0 * attempt);
+            begin_stats(ctx, st);
+            auto th = clk::now();
+            Upload up = upload(ctx, n, xadj, adjncy, adjcwgt, vwgt);
+            KB_CUDA(cudaStreamSynchronize(ctx.stream));
+            double ms_h2d = ms_since(th);
+            long long cut = 0;
+            int r = partition(ctx, up.g, kn, up.part, &cut, st);
+            auto td = clk::now();
+            if (n) KB_CUDA(cudaMemcpyAsync(part, up.part, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, ctx.stream));
+            KB_CUDA(cudaStreamSynchronize(ctx.stream));
+            *edgecut = cut;
+            if (st) {
+                st->ms_h2d = ms_h2d;
+                st->ms_d2h = ms_since(td);
+                fill_stats_families(ctx, st);
+                st->ms_total = ms_since(t0);
+            }
+            return r;
+        } catch (const CudaError& e) {
+            if (e.code == cudaErrorMemoryAllocation && attempt < 2 &&
+                std::string(e.what()).find("arena exhausted") != std::string::npos) {
+                (void)cudaGetLastError();
+                continue;
+            }
+            throw;
+        }
+    }
+}
+
+// Phase helpers: host graph -> device, run f, copy results back.
+struct PhaseRun {
+    Lease lease;
+    Ctx& ctx;
+    Upload up;
+    PhaseRun(int dev, int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt)
+        : lease(dev), ctx(*lease.ctx) {
+        reserve_for(ctx, n, xadj[n], true, 1.0);
+        ctx.timing = false;
+        ctx.reset_stats();
+        up = upload(ctx, n, xadj, adjncy, adjwgt, vwgt);
+        up.g.maxdeg = max_degree(ctx, up.g);
+    }
+};
+
+int check_knobs(const kb200_knobs* kn) {
+    if (!kn) return fail(KB_ERR_INVALID_INPUT, "knobs is NULL");
+    if (kn->k < 1 || kn->lpc_subrounds < 1 || kn->ref_subrounds < 1 || kn->ref_classes < 1)
+        return fail(KB_ERR_INVALID_INPUT, "invalid knobs");
+    return KB_OK;
+}
+
+}  // namespace
+}  // namespace kb
+
+using namespace kb;
+
+#pragma GCC visibility push(default)
+extern "C" {
+
+int kb200_derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, int mode, kb200_knobs* out) {
+    if (!out || k < 1 || n < 0) return fail(KB_ERR_INVALID_INPUT, "invalid arguments");
+    derive_knobs(n, vwgt, k, imbalance, seed, mode, *out);
+    return KB_OK;
+}
+
+int kb200_kaffpa(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy, int nparts,
+                 double imbalance, int seed, int mode, long long* edgecut, int* part, kb200_stats* stats) {
+    g_last_error.clear();
+    return guarded([&] {
+        return run_host(n, vwgt, xadj, adjcwgt, adjncy, nparts, imbalance, seed, mode, edgecut, part, stats);
+    });
+}
+
+int kb200_kaffpa_device(int n, const int* d_vwgt, const int* d_xadj, const int* d_adjcwgt, const int* d_adjncy,
+                        int nparts, double imbalance, int seed, int mode, long long* edgecut, int* d_part,
+                        void* stream, kb200_stats* st) {
+    g_last_error.clear();
+    return guarded([&]() -> int {
+        if (n < 0 || nparts < 1 || !(imbalance >= 0) || !d_xadj || !d_vwgt || !d_adjcwgt || !edgecut)
+            return fail(KB_ERR_INVALID_INPUT, "invalid arguments (device entry point needs explicit weights)");
+        int dev, rc;
+        if ((rc = current_device(&dev))) return rc;
+        Lease lease(dev);
+        Ctx& ctx = *lease.ctx;
+        cudaStream_t user = (cudaStream_t)stream;
+        cudaStream_t saved = ctx.stream;
+        if (user) ctx.stream = user;
+        struct Restore {
+            Ctx& c;
+            cudaStream_t s;
+            ~Restore() { c.stream = s; }
+        } restore{ctx, saved};
+        auto t0 = clk::now();
+        int m32 = 0;
+        KB_CUDA(cudaMemcpyAsync(&m32, d_xadj + n, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+        KB_CUDA(cudaStreamSynchronize(ctx.stream));
+        // node weights are needed on the host for the knobs (total weight)
+        std::vector<int> hv((size_t)n);
+        if (n) KB_CUDA(cudaMemcpyAsync(hv.data(), d_vwgt, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, ctx.stream));
+        KB_CUDA(cudaStreamSynchronize(ctx.stream));
+        Knobs kn;
+        derive_knobs(n, hv.data(), nparts, imbalance, seed, mode, kn);
+        for (int attempt = 0;; ++attempt) {
+            try {
+                reserve_for(ctx, n, m32, false, attempt == 0 ? 1.0 : 2.0 * attempt);
+                begin_stats(ctx, st);
+                DevGraph g;
+                g.n = n;
+                g.m = m32;
+                g.xadj = d_xadj;
+                g.adjncy = d_adjncy;
+                g.adjwgt = d_adjcwgt;
+                g.vwgt = d_vwgt;
+                long long cut = 0;
+                int r = partition(ctx, g, kn, d_part, &cut, st);
+                *edgecut = cut;
+                if (st) {
+                    fill_stats_families(ctx, st);
+                    st->ms_total = ms_since(t0);
+                }
+                return r;
+            } catch (const CudaError& e) {
+                if (e.code == cudaErrorMemoryAllocation && attempt < 2 &&
+                    std::string(e.what()).find("arena exhausted") != std::string::npos) {
+                    (void)cudaGetLastError();
+                    continue;
+                }
+                throw;
+            }
+        }
+    });
+}
+
+int kb200_lp_cluster(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                     const kb200_knobs* kn, int level, int* label) {
+    g_last_error.clear();
+    return guarded([&]() -> int {
+        int rc, dev;
+        if ((rc = validate(n, xadj, adjncy, adjwgt, vwgt)) || (rc = check_knobs(kn))) return rc;
+        if ((rc = current_device(&dev))) return rc;
+        PhaseRun pr(dev, n, xadj, adjncy, adjwgt, vwgt);
+        int* d = pr.ctx.hier.alloc<int>((size_t)std::max(n, 1));
+        lp_cluster(pr.ctx, pr.up.g, *kn, level, d);
+        if (n) KB_CUDA(cudaMemcpyAsync(label, d, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, pr.ctx.stream));
+        KB_CUDA(cudaStreamSynchronize(pr.ctx.stream));
+        return KB_OK;
+    });
+}
+
+int kb200_contract(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt, const int* label,
+                   int* nc, long long* mc, int* cmap, int* cxadj, int* cadjncy, int* cadjwgt, int* cvwgt) {
+    g_last_error.clear();
+    return guarded([&]() -> int {
+        int rc, dev;
+        if ((rc = validate(n, xadj, adjncy, adjwgt, vwgt))) return rc;
+        for (int v = 0; v < n; ++v)
+            if (label[v] < 0 || label[v] >= n) return fail(KB_ERR_INVALID_INPUT, "label out of range");
+        if ((rc = current_device(&dev))) return rc;
+        PhaseRun pr(dev, n, xadj, adjncy, adjwgt, vwgt);
+        cudaStream_t s = pr.ctx.stream;
+        int* dl = pr.ctx.hier.alloc<int>((size_t)std::max(n, 1));
+        int* dm = pr.ctx.hier.alloc<int>((size_t)std::max(n, 1));
+        if (n) KB_CUDA(cudaMemcpyAsync(dl, label, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, s));
+        DevGraph c;
+        int *cx, *ca, *cw, *cv;
+        contract(pr.ctx, pr.up.g, dl, dm, c, &cx, &ca, &cw, &cv);
+        *nc = c.n;
+        *mc = c.m;
+        if (n) KB_CUDA(cudaMemcpyAsync(cmap, dm, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+        KB_CUDA(cudaMemcpyAsync(cxadj, cx, sizeof(int) * ((size_t)c.n + 1), cudaMemcpyDeviceToHost, s));
+        if (c.m) {
+            KB_CUDA(cudaMemcpyAsync(cadjncy, ca, sizeof(int) * (size_t)c.m, cudaMemcpyDeviceToHost, s));
+            KB_CUDA(cudaMemcpyAsync(cadjwgt, cw, sizeof(int) * (size_t)c.m, cudaMemcpyDeviceToHost, s));
+        }
+        if (c.n) KB_CUDA(cudaMemcpyAsync(cvwgt, cv, sizeof(int) * (size_t)c.n, cudaMemcpyDeviceToHost, s));
+        KB_CUDA(cudaStreamSynchronize(s));
+        return KB_OK;
+    });
+}
+
+static int part_phase(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                      const kb200_knobs* kn, int level, uint32_t bound, int* part, int* balanced, bool bal) {
+    g_last_error.clear();
+    return guarded([&]() -> int {
+        int rc, dev;
+        if ((rc = validate(n, xadj, adjncy, adjwgt, vwgt)) || (rc = check_knobs(kn))) return rc;
+        for (int v = 0; v < n; ++v)
+            if (part[v] < 0 || part[v] >= kn->k) return fail(KB_ERR_INVALID_INPUT, "block id out of range");
+        if ((rc = current_device(&dev))) return rc;
+        PhaseRun pr(dev, n, xadj, adjncy, adjwgt, vwgt);
+        cudaStream_t s = pr.ctx.stream;
+        uint32_t* bw = pr.ctx.hier.alloc<uint32_t>((size_t)kn->k);
+        if (n) KB_CUDA(cudaMemcpyAsync(pr.up.part, part, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, s));
+        block_weights_and_cut(pr.ctx, pr.up.g, pr.up.part, kn->k, bw, nullptr);
+        if (bal) {
+            bool ok = balance(pr.ctx, pr.up.g, *kn, level, bound, pr.up.part, bw);
+            if (balanced) *balanced = ok ? 1 : 0;
+        } else {
+            lp_refine(pr.ctx, pr.up.g, *kn, level, bound, pr.up.part, bw);
+        }
+        if (n) KB_CUDA(cudaMemcpyAsync(part, pr.up.part, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+        KB_CUDA(cudaStreamSynchronize(s));
+        return KB_OK;
+    });
+}
+
+int kb200_lp_refine(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                    const kb200_knobs* kn, int level, uint32_t bound, int* part) {
+    return part_phase(n, xadj, adjncy, adjwgt, vwgt, kn, level, bound, part, nullptr, false);
+}
+
+int kb200_balance(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                  const kb200_knobs* kn, int level, uint32_t bound, int* part, int* balanced) {
+    return part_phase(n, xadj, adjncy, adjwgt, vwgt, kn, level, bound, part, balanced, true);
+}
+
+int kb200_edge_cut(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt, const int* part,
+                   int k, long long* cut, uint32_t* bw) {
+    g_last_error.clear();
+    return guarded([&]() -> int {
+        int rc, dev;
+        if ((rc = validate(n, xadj, adjncy, adjwgt, vwgt))) return rc;
+        if (k < 1 || !cut) return fail(KB_ERR_INVALID_INPUT, "invalid arguments");
+        for (int v = 0; v < n; ++v)
+            if (part[v] < 0 || part[v] >= k) return fail(KB_ERR_INVALID_INPUT, "block id out of range");
+        if ((rc = current_device(&dev))) return rc;
+        PhaseRun pr(dev, n, xadj, adjncy, adjwgt, vwgt);
+        cudaStream_t s = pr.ctx.stream;
+        uint32_t* dbw = pr.ctx.hier.alloc<uint32_t>((size_t)k);
+        if (n) KB_CUDA(cudaMemcpyAsync(pr.up.part, part, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, s));
+        unsigned long long* c2 = reinterpret_cast<unsigned long long*>(pr.ctx.dscalars + 32);
+        block_weights_and_cut(pr.ctx, pr.up.g, pr.up.part, k, dbw, c2);
+        unsigned long long h = 0;
+        KB_CUDA(cudaMemcpyAsync(&h, c2, sizeof(h), cudaMemcpyDeviceToHost, s));
+        if (bw) KB_CUDA(cudaMemcpyAsync(bw, dbw, sizeof(uint32_t) * (size_t)k, cudaMemcpyDeviceToHost, s));
+        KB_CUDA(cudaStreamSynchronize(s));
+        *cut = (long long)h / 2;
+        return KB_OK;
+    });
+}
+
+int kb200_project(int n, const int* cmap, int nc, const int* part_coarse, int* part_fine) {
+    g_last_error.clear();
+    return guarded([&]() -> int {
+        int rc, dev;
+        if (n < 0 || nc < 0) return fail(KB_ERR_INVALID_INPUT, "invalid sizes");
+        for (int v = 0; v < n; ++v)
+            if (cmap[v] < 0 || cmap[v] >= nc) return fail(KB_ERR_INVALID_INPUT, "cmap out of range");
+        if ((rc = current_device(&dev))) return rc;
+        Lease lease(dev);
+        Ctx& ctx = *lease.ctx;
+        ctx.hier.reserve(((size_t)n * 8 + (size_t)nc * 4) + (1 << 20));
+        cudaStream_t s = ctx.stream;
+        int* dm = ctx.hier.alloc<int>((size_t)std::max(n, 1));
+        int* dc = ctx.hier.alloc<int>((size_t)std::max(nc, 1));
+        int* df = ctx.hier.alloc<int>((size_t)std::max(n, 1));
+        if (n) KB_CUDA(cudaMemcpyAsync(dm, cmap, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, s));
+        if (nc) KB_CUDA(cudaMemcpyAsync(dc, part_coarse, sizeof(int) * (size_t)nc, cudaMemcpyHostToDevice, s));
+        project(ctx, n, dm, dc, df);
+        if (n) KB_CUDA(cudaMemcpyAsync(part_fine, df, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+        KB_CUDA(cudaStreamSynchronize(s));
+        return KB_OK;
+    });
+}
+
+int kb200_initial_partition(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                            const kb200_knobs* kn, int* part) {
+    g_last_error.clear();
+    return guarded([&]() -> int {
+        int rc;
+        if ((rc = validate(n, xadj, adjncy, adjwgt, vwgt)) || (rc = check_knobs(kn))) return rc;
+        if (!adjwgt || !vwgt) return fail(KB_ERR_INVALID_INPUT, "explicit weights required");
+        initial_partition(n, xadj, adjncy, adjwgt, vwgt, *kn, part);
+        return KB_OK;
+    });
+}
+
+const char* kb200_last_error(void) { return g_last_error.c_str(); }
+
+int kb200_device_count(void) {
+    int c = 0;
+    if (cudaGetDeviceCount(&c) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0;
+    }
+    return c;
+}
+
+// ------------------------------------------------ reference-compatible ABI
+
+void kaffpa(int* n, int* vwgt, int* xadj, int* adjcwgt, int* adjncy, int* nparts, double* imbalance,
+            bool suppress_output, int seed, int mode, int* edgecut, int* part) {
+    (void)suppress_output;  // the reference ignores it on this path too (kaHIP_interface.cpp:108-113)
+    long long cut = -1;
+    int rc = (n && nparts && imbalance)
+                 ? kb200_kaffpa(*n, vwgt, xadj, adjcwgt, adjncy, *nparts, *imbalance, seed, mode, &cut, part, nullptr)
+                 : KB_ERR_INVALID_INPUT;
+    if (edgecut) *edgecut = rc < 0 ? -1 : (int)cut;
+}
+
+void kaffpa_balance(int* n, int* vwgt, int* xadj, int* adjcwgt, int* adjncy, int* nparts, double* imbalance,
+                    bool perfectly_balance, bool suppress_output, int seed, int mode, int* edgecut, int* part) {
+    // perfectly_balance asks for max block <= ceil(W/k)
+    // (kaHIP_interface.cpp:120-133); that is the imbalance-0 bound here.
+    double imb = perfectly_balance ? 0.0 : (imbalance ? *imbalance : -1.0);
+    kaffpa(n, vwgt, xadj, adjcwgt, adjncy, nparts, &imb, suppress_output, seed, mode, edgecut, part);
+}
+
+void kaffpa_balance_NE(int* n, int* vwgt, int* xadj, int* adjcwgt, int* adjncy, int* nparts, double* imbalance,
+                       bool suppress_output, int seed, int mode, int* edgecut, int* part) {
+    (void)n; (void)vwgt; (void)xadj; (void)adjcwgt; (void)adjncy; (void)nparts; (void)imbalance;
+    (void)suppress_output; (void)seed; (void)mode; (void)part;
+    g_last_error = "kaffpa_balance_NE is not provided by the B200 library";
+    if (edgecut) *edgecut = -1;
+}
+
+void process_mapping(int* n, int* vwgt, int* xadj, int* adjcwgt, int* adjncy, int* hierarchy_parameter,
+                     int* distance_parameter, int hierarchy_depth, int mode_partitioning, int mode_mapping,
+                     double* imbalance, bool suppress_output, int seed, int* edgecut, int* qap, int* part) {
+    (void)n; (void)vwgt; (void)xadj; (void)adjcwgt; (void)adjncy; (void)hierarchy_parameter;
+    (void)distance_parameter; (void)hierarchy_depth; (void)mode_partitioning; (void)mode_mapping;
+    (void)imbalance; (void)suppress_output; (void)seed; (void)part;
+    g_last_error = "process_mapping is not provided by the B200 library";
+    if (edgecut) *edgecut = -1;
+    if (qap) *qap = -1;
+}
+
+void node_separator(int* n, int* vwgt, int* xadj, int* adjcwgt, int* adjncy, int* nparts, double* imbalance,
+                    bool suppress_output, int seed, int mode, int* num_separator_vertices, int** separator) {
+    (void)n; (void)vwgt; (void)xadj; (void)adjcwgt; (void)adjncy; (void)nparts; (void)imbalance;
+    (void)suppress_output; (void)seed; (void)mode;
+    g_last_error = "node_separator is not provided by the B200 library";
+    if (num_separator_vertices) *num_separator_vertices = -1;
+    if (separator) *separator = nullptr;
+}
+
+void reduced_nd(int* n, int* xadj, int* adjncy, bool suppress_output, int seed, int mode, int* ordering) {
+    (void)n; (void)xadj; (void)adjncy; (void)suppress_output; (void)seed; (void)mode; (void)ordering;
+    g_last_error = "reduced_nd is not provided by the B200 library";
+}
+
+void edge_partitioning(int* n, int* vwgt, int* xadj, int* adjcwgt, int* adjncy, int* nparts, double* imbalance,
+                       bool suppress_output, int seed, int mode, int* vertexcut, int* part,
+                       int infinity_edge_weight) {
+    (void)n; (void)vwgt; (void)xadj; (void)adjcwgt; (void)adjncy; (void)nparts; (void)imbalance;
+    (void)suppress_output; (void)seed; (void)mode; (void)part; (void)infinity_edge_weight;
+    g_last_error = "edge_partitioning is not provided by the B200 library";
+    if (vertexcut) *vertexcut = -1;
+}
+
+}  // extern "C"
+#pragma GCC visibility pop

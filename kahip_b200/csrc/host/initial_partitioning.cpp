@@ -1,0 +1,473 @@
+// initial_partitioning.cpp -- host initial partitioner for the coarsest graph.
+//
+// Recursive multilevel bisection, as the reference's initial partitioning
+// (initial_partitioning.cpp:39-134 -> graph_partitioner.cpp:110-238 ->
+// bipartition.cpp:24-222) is built, made deterministic:
+//   * k blocks split as ceil(k/2) | floor(k/2), target weights in proportion;
+//     each side may exceed its target by max((1+eps)^(1/ceil log2 k) - 1,
+//     min(eps, 1%));
+//   * a bisection coarsens by sequential heavy-edge matching on the
+//     expansion*^2 rating while the graph has > 200 nodes and shrinks by at
+//     least 1.1 (node weight bound 1.5 W / 200), runs `tries` greedy growings
+//     from a pseudo-peripheral node (BFS twice from a hashed start), each
+//     with 2-way FM, keeps the best by (overload, cut), and refines with FM
+//     on every level on the way up;
+//   * `reps` repetitions of the whole recursion keep the smallest cut.
+// The graph is small (a few thousand nodes), so this stays on the host.
+#include "initial_partitioning.h"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#include "../hash.h"
+
+namespace kb {
+
+namespace {
+
+struct HostGraph {
+    int n = 0;
+    std::vector<int> xadj, adjncy, adjwgt, vwgt;
+    long long weight() const {
+        long long w = 0;
+        for (int x : vwgt) w += x;
+        return w;
+    }
+};
+
+// Indexed binary max-heap over node ids, priority (key desc, id asc).
+class GainHeap {
+public:
+    explicit GainHeap(int n) : pos_(n, -1) { heap_.reserve(n); }
+    bool empty() const { return heap_.empty(); }
+    bool contains(int v) const { return pos_[v] >= 0; }
+    void push(int v, const std::vector<long long>& key) {
+        pos_[v] = (int)heap_.size();
+        heap_.push_back(v);
+        sift_up(pos_[v], key);
+    }
+    int pop(const std::vector<long long>& key) {
+        int top = heap_[0];
+        pos_[top] = -1;
+        int last = heap_.back();
+        heap_.pop_back();
+        if (!heap_.empty()) {
+            heap_[0] = last;
+            pos_[last] = 0;
+            sift_down(0, key);
+        }
+        return top;
+    }
+    void changed(int v, const std::vector<long long>& key) {
+        sift_up(pos_[v], key);
+        sift_down(pos_[v], key);
+    }
+    void clear() {
+        for (int v : heap_) pos_[v] = -1;
+        heap_.clear();
+    }
+
+private:
+    static bool below(int a, int b, const std::vector<long long>& key) {  // a ranks below b
+        return key[a] != key[b] ? key[a] < key[b] : a > b;
+    }
+    void put(int i, int v) { heap_[i] = v; pos_[v] = i; }
+    void sift_up(int i, const std::vector<long long>& key) {
+        int v = heap_[i];
+        while (i > 0) {
+            int p = (i - 1) >> 1;
+            if (!below(heap_[p], v, key)) break;
+            put(i, heap_[p]);
+            i = p;
+        }
+        put(i, v);
+    }
+    void sift_down(int i, const std::vector<long long>& key) {
+        int v = heap_[i];
+        const int sz = (int)heap_.size();
+        for (;;) {
+            int l = 2 * i + 1, r = l + 1, best = i;
+            int bv = v;
+            if (l < sz && below(bv, heap_[l], key)) { best = l; bv = heap_[l]; }
+            if (r < sz && below(bv, heap_[r], key)) { best = r; bv = heap_[r]; }
+            if (best == i) break;
+            put(i, heap_[best]);
+            i = best;
+        }
+        put(i, v);
+    }
+    std::vector<int> heap_;
+    std::vector<int> pos_;
+};
+
+struct Limits {
+    uint64_t maxw[2];
+    uint64_t overload(const uint64_t w[2]) const {
+        uint64_t o = 0;
+        for (int s = 0; s < 2; ++s) o += w[s] > maxw[s] ? w[s] - maxw[s] : 0;
+        return o;
+    }
+};
+
+long long cut_of(const HostGraph& g, const std::vector<char>& side) {
+    long long c = 0;
+    for (int v = 0; v < g.n; ++v)
+        for (int e = g.xadj[v]; e < g.xadj[v + 1]; ++e)
+            if (side[v] != side[g.adjncy[e]]) c += g.adjwgt[e];
+    return c / 2;
+}
+
+// Last node dequeued by a breadth-first search from s.
+int farthest(const HostGraph& g, int s) {
+    std::vector<char> seen(g.n, 0);
+    std::vector<int> q;
+    q.reserve(g.n);
+    q.push_back(s);
+    seen[s] = 1;
+    for (size_t h = 0; h < q.size(); ++h) {
+        int v = q[h];
+        for (int e = g.xadj[v]; e < g.xadj[v + 1]; ++e) {
+            int u = g.adjncy[e];
+            if (!seen[u]) { seen[u] = 1; q.push_back(u); }
+        }
+    }
+    return q.back();
+}
+
+// Greedy growing of side 0 from `start` towards `target0` without
+// exceeding max0.  Gain of a side-1 node = w(to side 0) - w(to side 1).
+void grow_region(const HostGraph& g, int start, uint64_t target0, uint64_t max0,
+                 std::vector<char>& side, std::vector<long long>& key, GainHeap& heap) {
+    side.assign(g.n, 1);
+    std::vector<char> skipped(g.n, 0);
+    for (int v = 0; v < g.n; ++v) {
+        long long d = 0;
+        for (int e = g.xadj[v]; e < g.xadj[v + 1]; ++e) d += g.adjwgt[e];
+        key[v] = -d;
+    }
+    uint64_t w0 = 0;
+    int scan = 0;
+    int pending = start;
+    while (w0 < target0) {
+        int v;
+        if (pending >= 0) {
+            v = pending;
+            pending = -1;
+        } else if (!heap.empty()) {
+            v = heap.pop(key);
+        } else {
+            while (scan < g.n && (side[scan] == 0 || skipped[scan])) ++scan;
+            if (scan == g.n) break;
+            v = scan;
+        }
+        if (side[v] == 0 || skipped[v]) continue;
+        if (w0 + (uint64_t)g.vwgt[v] > max0) { skipped[v] = 1; continue; }
+        side[v] = 0;
+        w0 += (uint64_t)g.vwgt[v];
+        for (int e = g.xadj[v]; e < g.xadj[v + 1]; ++e) {
+            int u = g.adjncy[e];
+            if (side[u] == 0 || skipped[u]) continue;
+            key[u] += 2LL * g.adjwgt[e];
+            if (heap.contains(u)) heap.changed(u, key);
+            else heap.push(u, key);
+        }
+    }
+    heap.clear();
+}
+
+// 2-way FM with rollback to the best prefix by (overload, cut).
+long long fm_refine(const HostGraph& g, std::vector<char>& side, const Limits& lim, int passes,
+                    int stall_limit, std::vector<long long>& key, GainHeap& heap) {
+    uint64_t w[2] = {0, 0};
+    for (int v = 0; v < g.n; ++v) w[(int)side[v]] += (uint64_t)g.vwgt[v];
+    std::vector<char> locked(g.n, 0);
+    std::vector<int> log;
+    log.reserve(g.n);
+    long long cut = cut_of(g, side);
+    for (int pass = 0; pass < passes; ++pass) {
+        for (int v = 0; v < g.n; ++v) {
+            long long inside = 0, outside = 0;
+            for (int e = g.xadj[v]; e < g.xadj[v + 1]; ++e)
+                (side[g.adjncy[e]] == side[v] ? inside : outside) += g.adjwgt[e];
+            key[v] = outside - inside;
+            if (outside > 0) heap.push(v, key);
+        }
+        log.clear();
+        size_t best_len = 0;
+        int stall = 0;
+        long long cur = cut, best_cut = cut;
+        uint64_t best_ov = lim.overload(w);
+        while (!heap.empty() && stall < stall_limit) {
+            int v = heap.pop(key);
+            int from = side[v], to = 1 - from;
+            if (w[to] + (uint64_t)g.vwgt[v] > lim.maxw[to]) continue;
+            side[v] = (char)to;
+            w[from] -= (uint64_t)g.vwgt[v];
+            w[to] += (uint64_t)g.vwgt[v];
+            cur -= key[v];
+            locked[v] = 1;
+            log.push_back(v);
+            for (int e = g.xadj[v]; e < g.xadj[v + 1]; ++e) {
+                int u = g.adjncy[e];
+                if (locked[u]) continue;
+                long long d = 2LL * g.adjwgt[e];
+                key[u] += side[u] == to ? -d : d;
+                if (heap.contains(u)) heap.changed(u, key);
+                else heap.push(u, key);
+            }
+            uint64_t ov = lim.overload(w);
+            if (ov < best_ov || (ov == best_ov && cur < best_cut)) {
+                best_ov = ov;
+                best_cut = cur;
+                best_len = log.size();
+                stall = 0;
+            } else {
+                ++stall;
+            }
+        }
+        heap.clear();
+        while (log.size() > best_len) {
+            int v = log.back();
+            log.pop_back();
+            int from = side[v], to = 1 - from;
+            side[v] = (char)to;
+            w[from] -= (uint64_t)g.vwgt[v];
+            w[to] += (uint64_t)g.vwgt[v];
+        }
+        for (int v : log) locked[v] = 0;
+        // moves that were undone are unlocked too
+        std::fill(locked.begin(), locked.end(), 0);
+        cut = best_cut;
+        if (best_len == 0) break;
+    }
+    return cut;
+}
+
+// Matching-based coarsening step: nodes visited in hash order, each
+// unmatched node takes the unmatched neighbour of best expansion*^2 rating
+// (edge_ratings.cpp:316-328), ties to the smaller id.  Leader = min id.
+std::vector<int> heavy_edge_labels(const HostGraph& g, uint64_t ks, uint64_t maxnode) {
+    std::vector<std::pair<uint32_t, int>> order(g.n);
+    for (int v = 0; v < g.n; ++v) order[v] = {hash32(ks, (uint32_t)v), v};
+    std::sort(order.begin(), order.end());
+    std::vector<int> mate(g.n, -1);
+    for (const auto& hv : order) {
+        int u = hv.second;
+        if (mate[u] >= 0) continue;
+        const uint32_t cu = (uint32_t)g.vwgt[u];
+        int pick = -1;
+        double pr = 0;
+        for (int e = g.xadj[u]; e < g.xadj[u + 1]; ++e) {
+            int v = g.adjncy[e];
+            if (v == u || mate[v] >= 0) continue;
+            const uint32_t cv = (uint32_t)g.vwgt[v];
+            if ((uint64_t)cu + cv > maxnode) continue;
+            const int w = g.adjwgt[e];
+            double r = 1.0 * w * w / (uint32_t)(cu * cv);
+            if (pick < 0 || r > pr || (r == pr && v < pick)) { pick = v; pr = r; }
+        }
+        if (pick < 0) {
+            mate[u] = u;
+        } else {
+            mate[u] = pick;
+            mate[pick] = u;
+        }
+    }
+    std::vector<int> label(g.n);
+    for (int v = 0; v < g.n; ++v) label[v] = std::min(v, mate[v]);
+    return label;
+}
+
+// Contraction on the host (coarse ids by smallest member, rows sorted).
+HostGraph contract_host(const HostGraph& g, const std::vector<int>& label, std::vector<int>& cmap) {
+    std::vector<int> id(g.n, -1);
+    cmap.assign(g.n, 0);
+    int nc = 0;
+    for (int v = 0; v < g.n; ++v) {
+        if (id[label[v]] < 0) id[label[v]] = nc++;
+        cmap[v] = id[label[v]];
+    }
+    HostGraph c;
+    c.n = nc;
+    c.vwgt.assign(nc, 0);
+    for (int v = 0; v < g.n; ++v) c.vwgt[cmap[v]] += g.vwgt[v];
+    std::vector<std::vector<int>> members(nc);
+    for (int v = 0; v < g.n; ++v) members[cmap[v]].push_back(v);
+    std::vector<uint32_t> acc(nc, 0);
+    std::vector<char> hit(nc, 0);
+    std::vector<int> targets;
+    c.xadj.assign(nc + 1, 0);
+    for (int cu = 0; cu < nc; ++cu) {
+        targets.clear();
+        for (int v : members[cu])
+            for (int e = g.xadj[v]; e < g.xadj[v + 1]; ++e) {
+                int t = cmap[g.adjncy[e]];
+                if (t == cu) continue;
+                if (!hit[t]) { hit[t] = 1; targets.push_back(t); }
+                acc[t] += (uint32_t)g.adjwgt[e];
+            }
+        std::sort(targets.begin(), targets.end());
+        for (int t : targets) {
+            c.adjncy.push_back(t);
+            c.adjwgt.push_back((int)acc[t]);
+            acc[t] = 0;
+            hit[t] = 0;
+        }
+        c.xadj[cu + 1] = (int)c.adjncy.size();
+    }
+    return c;
+}
+
+struct Bisector {
+    const Knobs& kn;
+
+    // tries on the coarsest graph of one bisection
+    std::vector<char> coarsest(const HostGraph& g, uint64_t t0, const Limits& lim, int bis_key) const {
+        std::vector<char> best(g.n, 1), side;
+        std::vector<long long> key(g.n, 0);
+        GainHeap heap(g.n);
+        long long best_cut = LLONG_MAX;
+        uint64_t best_ov = UINT64_MAX;
+        for (int t = 0; t < kn.ip_tries; ++t) {
+            const uint64_t ks = stream_key(kn.seed, TAG_IP, bis_key, t);
+            int s0 = 0;
+            uint32_t hmin = UINT32_MAX;
+            for (int v = 0; v < g.n; ++v) {
+                uint32_t h = hash32(ks, (uint32_t)v);
+                if (h < hmin) { hmin = h; s0 = v; }
+            }
+            int start = farthest(g, farthest(g, s0));
+            grow_region(g, start, t0, lim.maxw[0], side, key, heap);
+            long long c = fm_refine(g, side, lim, kn.ip_fm_passes, kn.ip_fm_stall, key, heap);
+            uint64_t w[2] = {0, 0};
+            for (int v = 0; v < g.n; ++v) w[(int)side[v]] += (uint64_t)g.vwgt[v];
+            uint64_t ov = lim.overload(w);
+            if (ov < best_ov || (ov == best_ov && c < best_cut)) {
+                best_ov = ov;
+                best_cut = c;
+                best = side;
+            }
+        }
+        return best;
+    }
+
+    std::vector<char> multilevel(const HostGraph& g, uint64_t t0, const Limits& lim, int bis_key) const {
+        std::vector<HostGraph> levels;
+        std::vector<std::vector<int>> maps;
+        const uint64_t maxnode = (uint64_t)(1.5 * (double)g.weight() / 200.0);
+        const HostGraph* cur = &g;
+        while ((int)levels.size() < 32 && cur->n > 200) {
+            std::vector<int> lab =
+                heavy_edge_labels(*cur, stream_key(kn.seed, TAG_IPM, bis_key, (int)levels.size()), maxnode);
+            std::vector<int> cmap;
+            HostGraph c = contract_host(*cur, lab, cmap);
+            if (1.0 * cur->n / (double)c.n < 1.1) break;
+            maps.push_back(std::move(cmap));
+            levels.push_back(std::move(c));
+            cur = &levels.back();
+        }
+        std::vector<char> side = coarsest(*cur, t0, lim, bis_key);
+        for (int l = (int)levels.size() - 1; l >= 0; --l) {
+            const HostGraph& fine = l == 0 ? g : levels[l - 1];
+            std::vector<char> fs(fine.n);
+            for (int v = 0; v < fine.n; ++v) fs[v] = side[maps[l][v]];
+            side.swap(fs);
+            std::vector<long long> key(fine.n, 0);
+            GainHeap heap(fine.n);
+            fm_refine(fine, side, lim, kn.ip_fm_passes, kn.ip_fm_stall, key, heap);
+        }
+        return side;
+    }
+};
+
+HostGraph induced(const HostGraph& g, const std::vector<int>& orig, const std::vector<char>& side, int which,
+                  std::vector<int>& sub_orig) {
+    std::vector<int> nid(g.n, -1);
+    HostGraph s;
+    sub_orig.clear();
+    for (int v = 0; v < g.n; ++v)
+        if (side[v] == which) {
+            nid[v] = s.n++;
+            sub_orig.push_back(orig[v]);
+        }
+    s.xadj.assign(s.n + 1, 0);
+    s.vwgt.resize(s.n);
+    for (int v = 0; v < g.n; ++v) {
+        if (side[v] != which) continue;
+        int u = nid[v];
+        s.vwgt[u] = g.vwgt[v];
+        for (int e = g.xadj[v]; e < g.xadj[v + 1]; ++e) {
+            int t = g.adjncy[e];
+            if (side[t] != which) continue;
+            s.adjncy.push_back(nid[t]);
+            s.adjwgt.push_back(g.adjwgt[e]);
+        }
+        s.xadj[u + 1] = (int)s.adjncy.size();
+    }
+    return s;
+}
+
+int levels_needed(int k) {
+    int l = 0;
+    while ((1 << l) < k) ++l;
+    return l;
+}
+
+void recurse(const Knobs& kn, const HostGraph& g, const std::vector<int>& orig, int k, int offset, int rep,
+             int& counter, std::vector<int>& out) {
+    if (k == 1 || g.n == 0) {
+        for (int v = 0; v < g.n; ++v) out[orig[v]] = offset;
+        return;
+    }
+    const int bis_id = counter++;
+    const int kl = (k + 1) / 2, kr = k - kl;
+    const uint64_t W = (uint64_t)g.weight();
+    const uint64_t t0 = W * (uint64_t)kl / (uint64_t)k;
+    const uint64_t t1 = W - t0;
+    const double eps = kn.imbalance > 0 ? kn.imbalance : 0.0;
+    double eb = std::pow(1.0 + eps, 1.0 / levels_needed(k)) - 1.0;
+    eb = std::max(eb, std::min(eps, 0.01));
+    Limits lim{{(uint64_t)((1.0 + eb) * (double)t0), (uint64_t)((1.0 + eb) * (double)t1)}};
+    Bisector bis{kn};
+    std::vector<char> side = bis.multilevel(g, t0, lim, bis_id * 64 + rep);
+    std::vector<int> lo, ro;
+    HostGraph L = induced(g, orig, side, 0, lo);
+    HostGraph R = induced(g, orig, side, 1, ro);
+    recurse(kn, L, lo, kl, offset, rep, counter, out);
+    recurse(kn, R, ro, kr, offset + kl, rep, counter, out);
+}
+
+}  // namespace
+
+void initial_partition(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                       const Knobs& kn, int* part) {
+    HostGraph g;
+    g.n = n;
+    g.xadj.assign(xadj, xadj + n + 1);
+    g.adjncy.assign(adjncy, adjncy + xadj[n]);
+    g.adjwgt.assign(adjwgt, adjwgt + xadj[n]);
+    g.vwgt.assign(vwgt, vwgt + n);
+    std::vector<int> orig(n);
+    for (int v = 0; v < n; ++v) orig[v] = v;
+    std::vector<int> cand(n);
+    long long best = LLONG_MAX;
+    for (int rep = 0; rep < kn.ip_reps; ++rep) {
+        int counter = 0;
+        recurse(kn, g, orig, kn.k, 0, rep, counter, cand);
+        long long c = 0;
+        for (int v = 0; v < n; ++v)
+            for (int e = xadj[v]; e < xadj[v + 1]; ++e)
+                if (cand[v] != cand[adjncy[e]]) c += adjwgt[e];
+        c /= 2;
+        if (c < best) {
+            best = c;
+            std::copy(cand.begin(), cand.end(), part);
+        }
+    }
+}
+
+}  // namespace kb

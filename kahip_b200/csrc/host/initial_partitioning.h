@@ -1,0 +1,13 @@
+// initial_partitioning.h -- host initial partitioner of the coarsest graph.
+#pragma once
+
+#include "../knobs.h"
+
+namespace kb {
+
+// Partitions the (small) graph into kn.k blocks; part[n] out.  All arrays
+// are host memory; adjwgt and vwgt must be non-null.
+void initial_partition(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                       const Knobs& kn, int* part);
+
+}  // namespace kb

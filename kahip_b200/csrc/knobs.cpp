@@ -1,0 +1,75 @@
+// knobs.cpp -- parameter derivation for one partitioning call.
+#include "knobs.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace kb {
+
+void derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, int mode, Knobs& kn) {
+    std::memset(&kn, 0, sizeof(kn));
+    kn.k = k;
+    kn.imbalance = imbalance;
+    kn.seed = seed;
+    kn.mode = mode;
+
+    // Total node weight as the reference accumulates it (NodeWeight is a
+    // 32-bit unsigned, app/balance_configuration.h:20-23).
+    uint32_t W = 0;
+    if (vwgt) {
+        for (int v = 0; v < n; ++v) W += (uint32_t)vwgt[v];
+    } else {
+        W = (uint32_t)n;
+    }
+    kn.total_weight = W;
+
+    // kaffpa() turns the fraction into percent (interface/kaHIP_interface.cpp:115);
+    // configurate_balance turns it back and truncates U to NodeWeight
+    // (app/balance_configuration.h:40-47).  With imbalance 0 the reference
+    // switches to "perfectly balanced" mode: U gets +1% slack for the
+    // multilevel phases and the final result must fit ceil(W/k).
+    const double pct = 100 * imbalance;
+    const double eps = pct / 100.0;
+    const double avg = std::ceil(W / (double)k);
+    if (pct == 0) {
+        kn.upper_bound = (uint32_t)((1 + eps + 0.01) * avg);
+        kn.final_bound = (uint32_t)avg;
+    } else {
+        kn.upper_bound = (uint32_t)((1 + eps) * avg);
+        kn.final_bound = kn.upper_bound;
+    }
+
+    // simple_stop_rule (stop_rules.h:46-56): coarsen while the graph keeps
+    // at least max(n / (2*60*k), 60*k) nodes; coarse nodes stay below
+    // 1.5 * W / num_stop.
+    const double x = 60;
+    kn.num_stop = (uint32_t)std::max(n / (2.0 * x * k), 60.0 * k);
+    kn.max_vertex_weight = (uint32_t)(1.5 * W / kn.num_stop);
+
+    // Cluster bound of size-constrained LP clustering, ceil(U / 18)
+    // (size_constraint_label_propagation.cpp:57, cluster_coarsening_factor
+    // app/configuration.h:422), tightened so coarse nodes respect the
+    // max_vertex_weight of the fast/eco presets.  The test is strict (:175).
+    uint32_t cb = (uint32_t)std::ceil(kn.upper_bound / 18.0);
+    cb = std::min<uint32_t>(cb, kn.max_vertex_weight + 1u);
+    kn.cluster_bound = cb;
+
+    // Schedule knobs.  FAST/FASTSOCIAL use the cheap preset; everything else
+    // (ECO, STRONG*, unknown modes -- which the reference maps to eco,
+    // kaHIP_interface.cpp:60-61) the thorough one.
+    const bool fast = mode == 0 || mode == 3;
+    kn.lpc_rounds = fast ? 5 : 10;       // label_iterations = 10 (configuration.h:424)
+    kn.lpc_subrounds = 4;
+    kn.ref_rounds = fast ? 10 : 25;      // label_iterations_refinement = 25 (:425)
+    kn.ref_subrounds = 4;
+    kn.ref_classes = 16;
+    kn.bal_iters = 64;
+    kn.ip_reps = fast ? 1 : 3;
+    kn.ip_tries = 4;                     // bipartition_tries = 4 (fast/eco)
+    kn.ip_fm_passes = fast ? 3 : 6;
+    kn.ip_fm_stall = 100;
+    kn.max_levels = 48;
+}
+
+}  // namespace kb

@@ -1,0 +1,718 @@
+// lp.cu -- label-propagation sweeps on the device: size-constrained LP
+// clustering (coarsening), LP refinement (uncoarsening) and the candidate
+// selection of the exact balance repair.
+//
+// Rules (restated from the reference):
+//   clustering  size_constraint_label_propagation.cpp:134-194
+//   refinement  label_propagation_refinement.cpp:21-98
+// Schedule (this library's, deterministic): synchronous sub-rounds chosen by
+// a counter hash; every decision of a sub-round reads the state at its start;
+// ties broken by hash(tie stream, label) then label id; moves are admitted
+// into capacity-limited targets without sorting (see decide kernels).
+//
+// Work distribution: a warp takes 32 consecutive vertex ids, ballots which of
+// them take part in this sub-round, and hands them to groups of G lanes
+// (G = 8/16/32 by average degree).  A group aggregates one vertex's
+// neighbourhood: degree <= G in registers (match_any + redux), degree <=
+// kTable/2 in a per-group shared-memory hash table, larger degrees are
+// deferred to a block-per-vertex kernel with a global-memory table.
+#include "lp.cuh"
+#include "prims.cuh"
+
+#include <algorithm>
+#include <climits>
+#include <vector>
+
+namespace kb {
+
+namespace {
+
+constexpr uint32_t kEmpty = 0xFFFFFFFFu;
+constexpr int kThreads = 256;
+constexpr int kBalClasses = 256;
+
+enum Mode { CLUSTER = 0, REFINE = 1, BALANCE = 2 };
+
+// Everything a sweep reads or writes; passed by value.
+struct SweepArgs {
+    int n;
+    const int* __restrict__ xadj;
+    const int* __restrict__ adjncy;
+    const int* __restrict__ adjwgt;
+    const int* __restrict__ vwgt;
+    const int* __restrict__ lab;        // cluster id or block id per vertex
+    const uint32_t* __restrict__ lw;    // weight per label (cluster / block)
+    const uint8_t* __restrict__ active; // REFINE: vertex may move this round
+    uint32_t bound;
+    uint32_t S, s;                      // sub-rounds, this sub-round
+    uint64_t ks_sub, ks_tie, ks_prio;
+    int P;                              // admission classes
+    int table;                          // per-group table capacity (power of 2)
+    // outputs
+    int* pv; int* pt; int* pc;          // proposal list
+    unsigned* pcount;
+    uint32_t* inc;                      // CLUSTER: incoming weight per target
+    int* minv;                          // CLUSTER: smallest proposer per target
+    uint32_t* H;                        // REFINE/BALANCE: weight per (target, class)
+    int* minvP;                         // smallest proposer per (target, class)
+    int* heavy; unsigned* hcount;       // deferred high-degree vertices
+    unsigned long long* work;           // [0] vertices, [1] edges
+    int* err;                           // set when an invariant breaks
+    // BALANCE
+    const int* lightest;
+    uint32_t* HS;                       // release weight per (own block, class)
+};
+
+__device__ __forceinline__ uint32_t table_slot(uint32_t key, int cap) {
+    return (key * 0x9E3779B1u) >> (32 - __ffs(cap) + 1);
+}
+
+// Linear probing; the caller guarantees fewer distinct keys than cap/2, so
+// the probe ends within cap steps.  The bound only guards against a broken
+// invariant: the key is then dropped and *err is set.
+__device__ __forceinline__ void table_insert(uint32_t* tk, uint32_t* tv, int cap, uint32_t key,
+                                             uint32_t val, int* err) {
+    uint32_t s = table_slot(key, cap);
+    for (int probe = 0; probe < cap; ++probe) {
+        uint32_t prev = atomicCAS(&tk[s], kEmpty, key);
+        if (prev == kEmpty || prev == key) {
+            atomicAdd(&tv[s], val);
+            return;
+        }
+        s = (s + 1) & (uint32_t)(cap - 1);
+    }
+    atomicOr(err, 1);
+}
+
+// candidate key: larger connection first, then smaller tie hash; id breaks
+// the remaining ties (smaller wins)
+__device__ __forceinline__ uint64_t cand_key(uint32_t conn, uint64_t ks_tie, uint32_t label) {
+    return ((uint64_t)conn << 32) | (uint32_t)~hash32(ks_tie, label);
+}
+
+__device__ __forceinline__ void better(uint64_t& k, uint32_t& id, uint64_t k2, uint32_t id2) {
+    if (k2 > k || (k2 == k && id2 < id)) { k = k2; id = id2; }
+}
+
+template <int G>
+__device__ __forceinline__ void group_argmax(uint64_t& k, uint32_t& id, unsigned gmask) {
+#pragma unroll
+    for (int o = G / 2; o >= 1; o >>= 1) {
+        uint64_t k2 = __shfl_xor_sync(gmask, k, o);
+        uint32_t i2 = __shfl_xor_sync(gmask, id, o);
+        better(k, id, k2, i2);
+    }
+}
+
+// Is label b (connection c) a candidate for vertex of weight cv?
+template <int MODE>
+__device__ __forceinline__ bool cand_ok(const SweepArgs& a, uint32_t b, uint32_t c, uint32_t cv) {
+    if (MODE == BALANCE) return (uint64_t)a.lw[b] + cv <= a.bound;
+    return c > 0 && (uint64_t)a.lw[b] + cv < a.bound;
+}
+
+__device__ __forceinline__ int loss_bucket(long long loss) {
+    if (loss <= 0) return 0;
+    int b = 1;
+    while (b < 31 && (loss >> b) > 0) ++b;
+    return b;
+}
+
+// Final decision for vertex v (executed by one lane).
+template <int MODE>
+__device__ void decide_emit(const SweepArgs& a, int v, uint32_t own, uint32_t cv, uint32_t conn_own,
+                            uint64_t key, uint32_t id) {
+    if (MODE == CLUSTER) {
+        if (id == kEmpty || (uint32_t)(key >> 32) <= conn_own) return;
+        unsigned i = atomicAdd(a.pcount, 1u);
+        a.pv[i] = v;
+        a.pt[i] = (int)id;
+        atomicAdd(&a.inc[id], cv);
+        atomicMin(&a.minv[id], v);
+    } else if (MODE == REFINE) {
+        uint32_t base = a.lw[own] <= a.bound ? conn_own : 0u;
+        if (id == kEmpty || (uint32_t)(key >> 32) <= base) return;
+        int cls = (int)(hash32(a.ks_prio, (uint32_t)v) % (uint32_t)a.P);
+        unsigned i = atomicAdd(a.pcount, 1u);
+        a.pv[i] = v;
+        a.pt[i] = (int)id;
+        a.pc[i] = cls;
+        size_t h = (size_t)id * a.P + cls;
+        atomicAdd(&a.H[h], cv);
+        atomicMin(&a.minvP[h], v);
+    } else {  // BALANCE
+        uint32_t t = id, tc = (uint32_t)(key >> 32);
+        if (t == kEmpty) {
+            int L = *a.lightest;
+            if ((uint32_t)L == own || (uint64_t)a.lw[L] + cv > a.bound) return;
+            t = (uint32_t)L;
+            tc = 0;
+        }
+        long long loss = (long long)conn_own - (long long)tc;
+        int cls = loss_bucket(loss) * 8 + (int)(hash32(a.ks_sub, (uint32_t)v) % 8u);
+        unsigned i = atomicAdd(a.pcount, 1u);
+        a.pv[i] = v;
+        a.pt[i] = (int)t;
+        a.pc[i] = cls;
+        atomicAdd(&a.HS[(size_t)own * kBalClasses + cls], cv);
+    }
+}
+
+template <int MODE>
+__device__ __forceinline__ bool member(const SweepArgs& a, int v) {
+    if (MODE == BALANCE) return a.lw[a.lab[v]] > a.bound;
+    if (MODE == REFINE && !a.active[v]) return false;
+    return hash32(a.ks_sub, (uint32_t)v) % a.S == a.s;
+}
+
+// Group of G lanes aggregates and decides vertex v.
+template <int G, int MODE>
+__device__ void process_vertex(const SweepArgs& a, int v, int gl, unsigned gmask, uint32_t* tk,
+                               uint32_t* tv, unsigned long long& wv, unsigned long long& we) {
+    const int beg = a.xadj[v], end = a.xadj[v + 1], deg = end - beg;
+    const uint32_t own = (uint32_t)a.lab[v];
+    const uint32_t cv = (uint32_t)a.vwgt[v];
+    if (deg > a.table / 2) {
+        if (gl == 0) a.heavy[atomicAdd(a.hcount, 1u)] = v;
+        return;
+    }
+    if (gl == 0) { wv += 1; we += (unsigned long long)deg; }
+    uint32_t conn_own = 0;
+    uint64_t key = 0;
+    uint32_t id = kEmpty;
+    if (deg <= G) {
+        uint32_t l = kEmpty, w = 0;
+        if (gl < deg) {
+            int u = a.adjncy[beg + gl];
+            w = (uint32_t)a.adjwgt[beg + gl];
+            l = (uint32_t)a.lab[u];
+        }
+        unsigned peers = __match_any_sync(gmask, l);
+        uint32_t sum = __reduce_add_sync(peers, w);
+        bool leader = gl < deg && (peers & lanemask_lt()) == 0;
+        unsigned ob = __ballot_sync(gmask, leader && l == own);
+        if (ob) conn_own = __shfl_sync(gmask, sum, __ffs(ob) - 1);
+        if (leader && l != own && cand_ok<MODE>(a, l, sum, cv)) {
+            key = cand_key(sum, a.ks_tie, l);
+            id = l;
+        }
+    } else {
+        const int cap = a.table;
+        for (int c = beg; c < end; c += G) {
+            int e = c + gl;
+            uint32_t l = kEmpty, w = 0;
+            if (e < end) {
+                w = (uint32_t)a.adjwgt[e];
+                l = (uint32_t)a.lab[a.adjncy[e]];
+            }
+            unsigned peers = __match_any_sync(gmask, l);
+            uint32_t sum = __reduce_add_sync(peers, w);
+            if (e < end && (peers & lanemask_lt()) == 0) table_insert(tk, tv, cap, l, sum, a.err);
+        }
+        __syncwarp(gmask);
+        uint32_t co = 0;
+        for (int s = gl; s < cap; s += G) {
+            uint32_t l = tk[s];
+            if (l == kEmpty) continue;
+            uint32_t c = tv[s];
+            tk[s] = kEmpty;
+            tv[s] = 0;
+            if (l == own) co = c;
+            else if (cand_ok<MODE>(a, l, c, cv)) better(key, id, cand_key(c, a.ks_tie, l), l);
+        }
+        conn_own = __reduce_or_sync(gmask, co);
+        __syncwarp(gmask);
+    }
+    group_argmax<G>(key, id, gmask);
+    if (gl == 0) decide_emit<MODE>(a, v, own, cv, conn_own, key, id);
+}
+
+template <int G, int MODE>
+__global__ void __launch_bounds__(kThreads) sweep_kernel(SweepArgs a) {
+    extern __shared__ uint32_t smem[];
+    const int lane = threadIdx.x & 31;
+    const int gid = lane / G, gl = lane % G;
+    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (gid * G));
+    const int groups_per_block = kThreads / G;
+    const int gblock = (threadIdx.x / 32) * (32 / G) + gid;
+    uint32_t* tk = smem + (size_t)gblock * a.table;
+    uint32_t* tv = smem + (size_t)groups_per_block * a.table + (size_t)gblock * a.table;
+    for (int s = gl; s < a.table; s += G) { tk[s] = kEmpty; tv[s] = 0; }
+    __syncwarp();
+    unsigned long long wv = 0, we = 0;
+    const long long nchunks = ((long long)a.n + 31) / 32;
+    const long long warp = ((long long)blockIdx.x * kThreads + threadIdx.x) / 32;
+    const long long nwarps = (long long)gridDim.x * kThreads / 32;
+    for (long long chunk = warp; chunk < nchunks; chunk += nwarps) {
+        int v = (int)(chunk * 32 + lane);
+        bool mem = v < a.n && member<MODE>(a, v);
+        unsigned mask = __ballot_sync(0xffffffffu, mem);
+        while (mask) {
+            int pick = -1;
+#pragma unroll
+            for (int i = 0; i < 32 / G; ++i) {
+                if (mask) {
+                    if (i == gid) pick = __ffs(mask) - 1;
+                    mask &= mask - 1;
+                }
+            }
+            if (pick >= 0) process_vertex<G, MODE>(a, (int)(chunk * 32 + pick), gl, gmask, tk, tv, wv, we);
+        }
+    }
+    // one atomic per warp for the work counters
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        wv += __shfl_xor_sync(0xffffffffu, wv, o);
+        we += __shfl_xor_sync(0xffffffffu, we, o);
+    }
+    if (lane == 0 && (wv | we)) {
+        atomicAdd(&a.work[0], wv);
+        atomicAdd(&a.work[1], we);
+    }
+}
+
+// High-degree vertices: one block per vertex, global-memory table of
+// `gcap` slots per block (gcap >= 2 * maxdeg, power of two).
+template <int MODE>
+__global__ void __launch_bounds__(kThreads) heavy_kernel(SweepArgs a, uint32_t* gtk, uint32_t* gtv,
+                                                         int gcap) {
+    __shared__ uint64_t sk[kThreads / 32];
+    __shared__ uint32_t sid[kThreads / 32];
+    __shared__ uint32_t sco;
+    uint32_t* tk = gtk + (size_t)blockIdx.x * gcap;
+    uint32_t* tv = gtv + (size_t)blockIdx.x * gcap;
+    const unsigned count = *a.hcount;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (unsigned i = blockIdx.x; i < count; i += gridDim.x) {
+        const int v = a.heavy[i];
+        const int beg = a.xadj[v], end = a.xadj[v + 1];
+        const uint32_t own = (uint32_t)a.lab[v];
+        const uint32_t cv = (uint32_t)a.vwgt[v];
+        if (threadIdx.x == 0) {
+            sco = 0;
+            atomicAdd(&a.work[0], 1ull);
+            atomicAdd(&a.work[1], (unsigned long long)(end - beg));
+        }
+        for (int c = beg; c < end; c += kThreads) {
+            int e = c + threadIdx.x;
+            uint32_t l = kEmpty, wt = 0;
+            if (e < end) {
+                wt = (uint32_t)a.adjwgt[e];
+                l = (uint32_t)a.lab[a.adjncy[e]];
+            }
+            unsigned peers = __match_any_sync(0xffffffffu, l);
+            uint32_t sum = __reduce_add_sync(peers, wt);
+            if (e < end && (peers & lanemask_lt()) == 0) table_insert(tk, tv, gcap, l, sum, a.err);
+        }
+        __syncthreads();
+        uint64_t key = 0;
+        uint32_t id = kEmpty;
+        for (int s = threadIdx.x; s < gcap; s += kThreads) {
+            uint32_t l = tk[s];
+            if (l == kEmpty) continue;
+            uint32_t c = tv[s];
+            tk[s] = kEmpty;
+            tv[s] = 0;
+            if (l == own) sco = c;
+            else if (cand_ok<MODE>(a, l, c, cv)) better(key, id, cand_key(c, a.ks_tie, l), l);
+        }
+        group_argmax<32>(key, id, 0xffffffffu);
+        if (lane == 0) { sk[w] = key; sid[w] = id; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int j = 1; j < kThreads / 32; ++j) better(key, id, sk[j], sid[j]);
+            decide_emit<MODE>(a, v, own, cv, sco, key, id);
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- admission
+
+// Clustering: all proposals into b are admitted if they fit together;
+// otherwise only the smallest proposer (which fits by itself).
+__global__ void cluster_decide(const unsigned* pcount, const int* pv, int* pt, const int* vwgt,
+                               const uint32_t* cw, const uint32_t* inc, const int* minv,
+                               uint32_t bound) {
+    const unsigned cnt = *pcount;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        int v = pv[i], b = pt[i];
+        bool ok = ((uint64_t)cw[b] + inc[b] < bound) || minv[b] == v;
+        if (!ok) pt[i] = -1 - b;
+    }
+}
+
+__global__ void cluster_apply(const unsigned* pcount, const int* pv, const int* pt, const int* vwgt,
+                              int* label, uint32_t* cw, uint32_t* inc, int* minv) {
+    const unsigned cnt = *pcount;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        int v = pv[i], t = pt[i];
+        int b = t >= 0 ? t : -1 - t;
+        inc[b] = 0;
+        minv[b] = INT_MAX;
+        if (t < 0) continue;
+        uint32_t cv = (uint32_t)vwgt[v];
+        atomicSub(&cw[label[v]], cv);
+        atomicAdd(&cw[t], cv);
+        label[v] = t;
+    }
+}
+
+// Threshold admission: classes of target b are admitted in increasing order
+// while the cumulative weight stays <= cap(b); in the first class that does
+// not fit, only its smallest proposer is tried alone.
+__device__ __forceinline__ bool admit(const uint32_t* H, const int* minvP, int P, int b, int c, int v,
+                                      uint32_t cv, long long cap) {
+    const uint32_t* h = H + (size_t)b * P;
+    unsigned long long cum = 0;
+    int t = 0;
+    while (t < P && (long long)(cum + h[t]) <= cap) { cum += h[t]; ++t; }
+    if (c < t) return true;
+    return c == t && minvP[(size_t)b * P + t] == v && (long long)(cum + cv) <= cap;
+}
+
+// strict: cap = bound - 1 - w[b] (refinement keeps blocks < bound);
+// otherwise cap = bound - w[b] (balance repair fills up to bound)
+__global__ void class_decide(const unsigned* pcount, const int* pv, int* pt, const int* pc,
+                             const int* vwgt, const uint32_t* bw, const uint32_t* H, const int* minvP,
+                             int P, uint32_t bound, int strict) {
+    const unsigned cnt = *pcount;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        int b = pt[i], c = pc[i];
+        if (b < 0 || c < 0) continue;
+        long long cap = (long long)bound - (strict ? 1 : 0) - (long long)bw[b];
+        if (!admit(H, minvP, P, b, c, pv[i], (uint32_t)vwgt[pv[i]], cap)) pt[i] = -1 - b;
+    }
+}
+
+__global__ void class_apply(const unsigned* pcount, const int* pv, const int* pt, const int* pc,
+                            const int* xadj, const int* adjncy, const int* vwgt, int* part,
+                            uint32_t* bw, uint32_t* H, int* minvP, int P, uint8_t* next_active,
+                            unsigned* moved) {
+    const unsigned cnt = *pcount;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        int v = pv[i], t = pt[i], c = pc[i];
+        if (c < 0) continue;  // dropped before admission (balance)
+        int b = t >= 0 ? t : -1 - t;
+        H[(size_t)b * P + c] = 0;
+        minvP[(size_t)b * P + c] = INT_MAX;
+        if (t < 0) continue;
+        uint32_t cv = (uint32_t)vwgt[v];
+        atomicSub(&bw[part[v]], cv);
+        atomicAdd(&bw[t], cv);
+        part[v] = t;
+        atomicAdd(moved, 1u);
+        if (next_active)
+            for (int e = xadj[v]; e < xadj[v + 1]; ++e) next_active[adjncy[e]] = 1;
+    }
+}
+
+// Balance: per overloaded block, the release threshold class.
+__global__ void balance_threshold(const uint32_t* bw, const uint32_t* HS, int k, uint32_t bound,
+                                  int* thr) {
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= k) return;
+    int t = 0;
+    if (bw[b] > bound) {
+        unsigned long long excess = bw[b] - bound, cum = 0;
+        while (t < kBalClasses && cum < excess) { cum += HS[(size_t)b * kBalClasses + t]; ++t; }
+    }
+    thr[b] = t;
+}
+
+// Balance: released candidates get an admission class; others are dropped.
+__global__ void balance_release(const unsigned* pcount, const int* pv, const int* pt, int* pc,
+                                const int* part, const int* vwgt, const int* thr, uint32_t* H,
+                                int* minvP, int P, uint64_t ks_prio) {
+    const unsigned cnt = *pcount;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        int v = pv[i];
+        if (pc[i] >= thr[part[v]]) { pc[i] = -1; continue; }
+        int c = (int)(hash32(ks_prio, (uint32_t)v) % (uint32_t)P);
+        pc[i] = c;
+        size_t h = (size_t)pt[i] * P + c;
+        atomicAdd(&H[h], (uint32_t)vwgt[v]);
+        atomicMin(&minvP[h], v);
+    }
+}
+
+// lightest block (ties: smaller id) and whether any block exceeds bound
+__global__ void block_scan_kernel(const uint32_t* bw, int k, uint32_t bound, int* lightest,
+                                  int* over) {
+    __shared__ unsigned long long best[32];
+    __shared__ int ov[32];
+    unsigned long long mine = ~0ull;
+    int o = 0;
+    for (int b = threadIdx.x; b < k; b += blockDim.x) {
+        unsigned long long key = ((unsigned long long)bw[b] << 32) | (unsigned)b;
+        if (key < mine) mine = key;
+        if (bw[b] > bound) o = 1;
+    }
+    for (int s = 16; s >= 1; s >>= 1) {
+        unsigned long long x = __shfl_xor_sync(0xffffffffu, mine, s);
+        if (x < mine) mine = x;
+        o |= __shfl_xor_sync(0xffffffffu, o, s);
+    }
+    if ((threadIdx.x & 31) == 0) { best[threadIdx.x >> 5] = mine; ov[threadIdx.x >> 5] = o; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            if (best[w] < mine) mine = best[w];
+            o |= ov[w];
+        }
+        *lightest = (int)(mine & 0xffffffffu);
+        *over = o;
+    }
+}
+
+// ------------------------------------------------------------- host helpers
+
+int pick_group(const DevGraph& g) {
+    double avg = g.n ? (double)g.m / g.n : 0;
+    return avg <= 8 ? 8 : (avg <= 16 ? 16 : 32);
+}
+
+int table_for(int G) { return G == 32 ? 256 : (G == 16 ? 128 : 64); }
+
+int sweep_blocks() { return kNumSMs * 8; }
+
+struct SweepBuffers {
+    int *pv, *pt, *pc;
+    unsigned* counters;  // [0] pcount, [1] hcount, [2] moved
+    int* heavy;
+    uint32_t *gtk, *gtv;
+    int gcap, hblocks;
+    unsigned long long* work;
+    int* err;
+};
+
+SweepBuffers make_buffers(Ctx& ctx, const DevGraph& g) {
+    SweepBuffers b;
+    Arena& A = ctx.scratch;
+    size_t n = (size_t)std::max(g.n, 1);
+    b.pv = A.alloc<int>(n);
+    b.pt = A.alloc<int>(n);
+    b.pc = A.alloc<int>(n);
+    b.heavy = A.alloc<int>(n);
+    b.counters = A.alloc<unsigned>(4);
+    b.work = ctx.work;
+    b.err = ctx.dscalars + 60;
+    int G = pick_group(g);
+    int T = table_for(G);
+    b.gcap = 0;
+    b.hblocks = 0;
+    b.gtk = b.gtv = nullptr;
+    if (g.maxdeg > T / 2) {
+        int cap = 1;
+        while (cap < 2 * g.maxdeg) cap <<= 1;
+        b.gcap = cap;
+        // keep the per-block tables within ~1 GiB
+        long long per = (long long)cap * 8;
+        b.hblocks = (int)std::max<long long>(1, std::min<long long>(2LL * kNumSMs, (1LL << 30) / per));
+        b.gtk = A.alloc<uint32_t>((size_t)cap * b.hblocks);
+        b.gtv = A.alloc<uint32_t>((size_t)cap * b.hblocks);
+        fill_u32(b.gtk, (long long)cap * b.hblocks, kEmpty, ctx.stream);
+        fill_u32(b.gtv, (long long)cap * b.hblocks, 0u, ctx.stream);
+    }
+    return b;
+}
+
+template <int MODE>
+void launch_sweep(Ctx& ctx, const DevGraph& g, SweepArgs a, const SweepBuffers& b) {
+    int G = pick_group(g);
+    a.table = table_for(G);
+    size_t smem = (size_t)2 * (kThreads / G) * a.table * sizeof(uint32_t);
+    int blocks = sweep_blocks();
+    KB_CUDA(cudaMemsetAsync(b.counters, 0, 2 * sizeof(unsigned), ctx.stream));
+    if (G == 8) sweep_kernel<8, MODE><<<blocks, kThreads, smem, ctx.stream>>>(a);
+    else if (G == 16) sweep_kernel<16, MODE><<<blocks, kThreads, smem, ctx.stream>>>(a);
+    else sweep_kernel<32, MODE><<<blocks, kThreads, smem, ctx.stream>>>(a);
+    KB_LAUNCH();
+    if (b.gcap > 0) {
+        heavy_kernel<MODE><<<b.hblocks, kThreads, 0, ctx.stream>>>(a, b.gtk, b.gtv, b.gcap);
+        KB_LAUNCH();
+    }
+}
+
+SweepArgs base_args(const DevGraph& g, const SweepBuffers& b) {
+    SweepArgs a{};
+    a.n = g.n;
+    a.xadj = g.xadj;
+    a.adjncy = g.adjncy;
+    a.adjwgt = g.adjwgt;
+    a.vwgt = g.vwgt;
+    a.pv = b.pv;
+    a.pt = b.pt;
+    a.pc = b.pc;
+    a.pcount = b.counters;
+    a.hcount = b.counters + 1;
+    a.heavy = b.heavy;
+    a.work = b.work;
+    a.err = b.err;
+    return a;
+}
+
+double sweep_bytes(const DevGraph& g, double frac) {
+    // 12 B per directed entry (adjncy, adjwgt, label gather) + 24 B per node
+    return frac * (12.0 * (double)g.m + 24.0 * (double)g.n);
+}
+
+}  // namespace
+
+// --------------------------------------------------------------- clustering
+
+void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* label) {
+    const size_t mk = ctx.scratch.mark();
+    cudaStream_t st = ctx.stream;
+    const size_t n = (size_t)std::max(g.n, 1);
+    uint32_t* cw = ctx.scratch.alloc<uint32_t>(n);
+    uint32_t* inc = ctx.scratch.alloc<uint32_t>(n);
+    int* minv = ctx.scratch.alloc<int>(n);
+    SweepBuffers b = make_buffers(ctx, g);
+    init_labels(ctx, g, label, cw);
+    fill_u32(inc, g.n, 0u, st);
+    fill_i32(minv, g.n, INT_MAX, st);
+    SweepArgs a = base_args(g, b);
+    a.lab = label;
+    a.lw = cw;
+    a.bound = kn.cluster_bound;
+    a.S = (uint32_t)kn.lpc_subrounds;
+    a.inc = inc;
+    a.minv = minv;
+    const int dblocks = kNumSMs * 4;
+    for (int r = 0; r < kn.lpc_rounds; ++r) {
+        a.ks_sub = stream_key(kn.seed, TAG_CSUB, level, r);
+        a.ks_tie = stream_key(kn.seed, TAG_CTIE, level, r);
+        for (uint32_t s = 0; s < a.S; ++s) {
+            a.s = s;
+            {
+                PhaseScope ps(ctx, "lp_cluster_sweep", sweep_bytes(g, 1.0 / a.S));
+                launch_sweep<CLUSTER>(ctx, g, a, b);
+            }
+            PhaseScope ps(ctx, "lp_cluster_admit", 0);
+            cluster_decide<<<dblocks, kThreads, 0, st>>>(b.counters, b.pv, b.pt, g.vwgt, cw, inc, minv,
+                                                         a.bound);
+            KB_LAUNCH();
+            cluster_apply<<<dblocks, kThreads, 0, st>>>(b.counters, b.pv, b.pt, g.vwgt, label, cw, inc,
+                                                        minv);
+            KB_LAUNCH();
+        }
+    }
+    ctx.scratch.release(mk);
+}
+
+// --------------------------------------------------------------- refinement
+
+void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t bound, int* part,
+               uint32_t* bw) {
+    if (g.n == 0) return;
+    const size_t mk = ctx.scratch.mark();
+    cudaStream_t st = ctx.stream;
+    const int k = kn.k, P = kn.ref_classes;
+    uint32_t* H = ctx.scratch.alloc<uint32_t>((size_t)k * P);
+    int* minvP = ctx.scratch.alloc<int>((size_t)k * P);
+    uint8_t* act = ctx.scratch.alloc<uint8_t>((size_t)g.n);
+    uint8_t* nact = ctx.scratch.alloc<uint8_t>((size_t)g.n);
+    SweepBuffers b = make_buffers(ctx, g);
+    fill_u32(H, (long long)k * P, 0u, st);
+    fill_i32(minvP, (long long)k * P, INT_MAX, st);
+    fill_u8(act, g.n, 1, st);
+    SweepArgs a = base_args(g, b);
+    a.lab = part;
+    a.lw = bw;
+    a.bound = bound;
+    a.S = (uint32_t)kn.ref_subrounds;
+    a.P = P;
+    a.H = H;
+    a.minvP = minvP;
+    const int dblocks = kNumSMs * 4;
+    unsigned* moved = b.counters + 2;
+    for (int r = 0; r < kn.ref_rounds; ++r) {
+        a.active = act;
+        a.ks_sub = stream_key(kn.seed, TAG_RSUB, level, r);
+        a.ks_tie = stream_key(kn.seed, TAG_RTIE, level, r);
+        a.ks_prio = stream_key(kn.seed, TAG_RPRIO, level, r);
+        fill_u8(nact, g.n, 0, st);
+        KB_CUDA(cudaMemsetAsync(moved, 0, sizeof(unsigned), st));
+        for (uint32_t s = 0; s < a.S; ++s) {
+            a.s = s;
+            {
+                PhaseScope ps(ctx, "lp_refine_sweep", sweep_bytes(g, 1.0 / a.S));
+                launch_sweep<REFINE>(ctx, g, a, b);
+            }
+            PhaseScope ps(ctx, "lp_refine_admit", 0);
+            class_decide<<<dblocks, kThreads, 0, st>>>(b.counters, b.pv, b.pt, b.pc, g.vwgt, bw, H, minvP,
+                                                       P, bound, 1);
+            KB_LAUNCH();
+            class_apply<<<dblocks, kThreads, 0, st>>>(b.counters, b.pv, b.pt, b.pc, g.xadj, g.adjncy,
+                                                      g.vwgt, part, bw, H, minvP, P, nact, moved);
+            KB_LAUNCH();
+        }
+        std::swap(act, nact);
+        KB_CUDA(cudaMemcpyAsync(ctx.pinned, moved, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        KB_CUDA(cudaStreamSynchronize(st));
+        if (ctx.pinned[0] == 0) break;
+    }
+    ctx.scratch.release(mk);
+}
+
+// ------------------------------------------------------------------ balance
+
+bool balance(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t bound, int* part,
+             uint32_t* bw) {
+    const size_t mk = ctx.scratch.mark();
+    cudaStream_t st = ctx.stream;
+    const int k = kn.k, P = kn.ref_classes;
+    uint32_t* H = ctx.scratch.alloc<uint32_t>((size_t)k * P);
+    int* minvP = ctx.scratch.alloc<int>((size_t)k * P);
+    uint32_t* HS = ctx.scratch.alloc<uint32_t>((size_t)k * kBalClasses);
+    int* thr = ctx.scratch.alloc<int>((size_t)k);
+    int* flags = ctx.scratch.alloc<int>(2);  // [0] lightest, [1] over
+    SweepBuffers b = make_buffers(ctx, g);
+    fill_u32(H, (long long)k * P, 0u, st);
+    fill_i32(minvP, (long long)k * P, INT_MAX, st);
+    SweepArgs a = base_args(g, b);
+    a.lab = part;
+    a.lw = bw;
+    a.bound = bound;
+    a.P = P;
+    a.HS = HS;
+    a.lightest = flags;
+    const int dblocks = kNumSMs * 4;
+    bool ok = false;
+    for (int it = 0; it < kn.bal_iters; ++it) {
+        block_scan_kernel<<<1, 1024, 0, st>>>(bw, k, bound, flags, flags + 1);
+        KB_LAUNCH();
+        KB_CUDA(cudaMemcpyAsync(ctx.pinned, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        KB_CUDA(cudaStreamSynchronize(st));
+        if (ctx.pinned[0] == 0) { ok = true; break; }
+        PhaseScope ps(ctx, "balance", 0);
+        a.ks_tie = stream_key(kn.seed, TAG_BTIE, level, it);
+        a.ks_sub = stream_key(kn.seed, TAG_BCLS, level, it);  // release class stream
+        uint64_t ks_prio = stream_key(kn.seed, TAG_BPRIO, level, it);
+        fill_u32(HS, (long long)k * kBalClasses, 0u, st);
+        launch_sweep<BALANCE>(ctx, g, a, b);
+        balance_threshold<<<div_up(k, 256), 256, 0, st>>>(bw, HS, k, bound, thr);
+        KB_LAUNCH();
+        balance_release<<<dblocks, kThreads, 0, st>>>(b.counters, b.pv, b.pt, b.pc, part, g.vwgt, thr, H,
+                                                      minvP, P, ks_prio);
+        KB_LAUNCH();
+        class_decide<<<dblocks, kThreads, 0, st>>>(b.counters, b.pv, b.pt, b.pc, g.vwgt, bw, H, minvP, P,
+                                                   bound, 0);
+        KB_LAUNCH();
+        class_apply<<<dblocks, kThreads, 0, st>>>(b.counters, b.pv, b.pt, b.pc, g.xadj, g.adjncy, g.vwgt,
+                                                  part, bw, H, minvP, P, nullptr, b.counters + 2);
+        KB_LAUNCH();
+    }
+    if (!ok) {
+        block_scan_kernel<<<1, 1024, 0, st>>>(bw, k, bound, flags, flags + 1);
+        KB_LAUNCH();
+        KB_CUDA(cudaMemcpyAsync(ctx.pinned, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        KB_CUDA(cudaStreamSynchronize(st));
+        ok = ctx.pinned[0] == 0;
+    }
+    ctx.scratch.release(mk);
+    return ok;
+}
+
+}  // namespace kb

@@ -1,0 +1,55 @@
+// lp.cuh -- device graph view and the label-propagation phases
+// (clustering, refinement, balance repair) of the multilevel scheme.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "context.h"
+#include "knobs.h"
+
+namespace kb {
+
+// A graph level resident in device memory (int32 CSR).
+struct DevGraph {
+    int n = 0;
+    long long m = 0;
+    int maxdeg = 0;
+    const int* xadj = nullptr;
+    const int* adjncy = nullptr;
+    const int* adjwgt = nullptr;
+    const int* vwgt = nullptr;
+};
+
+// Work counters of the sweep kernels (vertices and edges actually scanned).
+struct SweepWork {
+    unsigned long long vertices = 0, edges = 0;
+};
+
+// LP clustering of one coarsening level; label[n] (device) out.
+void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* label);
+
+// LP refinement at one level; part[n] in/out, bw[k] in/out (device).
+void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t bound, int* part,
+               uint32_t* bw);
+
+// Exact balance repair; returns true if every block ends <= bound.
+bool balance(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t bound, int* part,
+             uint32_t* bw);
+
+// Block weights (bw[k] zeroed and filled) and, when cut != nullptr, the edge
+// cut (device uint64, sum over directed entries / 2 applied by the caller).
+void block_weights_and_cut(Ctx& ctx, const DevGraph& g, const int* part, int k, uint32_t* bw,
+                           unsigned long long* cut2);
+
+// part_fine[v] = part_coarse[cmap[v]]
+void project(Ctx& ctx, int n, const int* cmap, const int* part_coarse, int* part_fine);
+
+// max degree of g (device reduction + readback)
+int max_degree(Ctx& ctx, const DevGraph& g);
+
+// label[v] = v, cw[v] = vwgt[v]
+void init_labels(Ctx& ctx, const DevGraph& g, int* label, uint32_t* cw);
+
+}  // namespace kb

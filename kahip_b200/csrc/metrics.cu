@@ -1,0 +1,106 @@
+// metrics.cu -- edge cut and block weights (quality_metrics.cpp:23-37),
+// projection (graph_hierarchy.cpp:54-58), max degree, label initialisation.
+#include "lp.cuh"
+#include "prims.cuh"
+
+namespace kb {
+
+namespace {
+
+// One thread per vertex, block-local histogram of block weights when k fits
+// into shared memory, warp-then-block reduction of the cut.
+__global__ void cut_bw_kernel(int n, const int* __restrict__ xadj, const int* __restrict__ adjncy,
+                              const int* __restrict__ adjwgt, const int* __restrict__ vwgt,
+                              const int* __restrict__ part, int k, uint32_t* bw,
+                              unsigned long long* cut2, int use_smem) {
+    extern __shared__ uint32_t hist[];
+    if (use_smem)
+        for (int b = threadIdx.x; b < k; b += blockDim.x) hist[b] = 0;
+    __syncthreads();
+    unsigned long long c = 0;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        int p = part[v];
+        if (use_smem) atomicAdd(&hist[p], (uint32_t)vwgt[v]);
+        else atomicAdd(&bw[p], (uint32_t)vwgt[v]);
+        if (cut2) {
+            for (int e = xadj[v]; e < xadj[v + 1]; ++e)
+                if (part[adjncy[e]] != p) c += (unsigned long long)(long long)adjwgt[e];
+        }
+    }
+    __syncthreads();
+    if (use_smem)
+        for (int b = threadIdx.x; b < k; b += blockDim.x)
+            if (hist[b]) atomicAdd(&bw[b], hist[b]);
+    if (cut2) {
+        for (int o = 16; o >= 1; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if ((threadIdx.x & 31) == 0 && c) atomicAdd(cut2, c);
+    }
+}
+
+__global__ void project_kernel(int n, const int* __restrict__ cmap, const int* __restrict__ pc,
+                               int* __restrict__ pf) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        pf[v] = pc[cmap[v]];
+}
+
+__global__ void maxdeg_kernel(int n, const int* __restrict__ xadj, int* out) {
+    int m = 0;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        m = max(m, xadj[v + 1] - xadj[v]);
+    for (int o = 16; o >= 1; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+__global__ void init_labels_kernel(int n, const int* __restrict__ vwgt, int* label, uint32_t* cw) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        label[v] = v;
+        cw[v] = (uint32_t)vwgt[v];
+    }
+}
+
+int grid_for(long long n, int threads) {
+    return (int)std::max<long long>(1, std::min<long long>(div_up(n, threads), (long long)kNumSMs * 16));
+}
+
+}  // namespace
+
+void block_weights_and_cut(Ctx& ctx, const DevGraph& g, const int* part, int k, uint32_t* bw,
+                           unsigned long long* cut2) {
+    cudaStream_t st = ctx.stream;
+    KB_CUDA(cudaMemsetAsync(bw, 0, sizeof(uint32_t) * (size_t)k, st));
+    if (cut2) KB_CUDA(cudaMemsetAsync(cut2, 0, sizeof(unsigned long long), st));
+    if (g.n == 0) return;
+    int use_smem = k <= 12288;
+    size_t smem = use_smem ? sizeof(uint32_t) * (size_t)k : 0;
+    PhaseScope ps(ctx, cut2 ? "cut_and_weights" : "block_weights",
+                  cut2 ? 12.0 * g.m + 12.0 * g.n : 8.0 * g.n);
+    cut_bw_kernel<<<grid_for(g.n, 256), 256, smem, st>>>(g.n, g.xadj, g.adjncy, g.adjwgt, g.vwgt, part, k,
+                                                         bw, cut2, use_smem);
+    KB_LAUNCH();
+}
+
+void project(Ctx& ctx, int n, const int* cmap, const int* part_coarse, int* part_fine) {
+    if (n == 0) return;
+    PhaseScope ps(ctx, "project", 12.0 * n);
+    project_kernel<<<grid_for(n, 256), 256, 0, ctx.stream>>>(n, cmap, part_coarse, part_fine);
+    KB_LAUNCH();
+}
+
+int max_degree(Ctx& ctx, const DevGraph& g) {
+    if (g.n == 0) return 0;
+    int* d = ctx.dscalars;
+    KB_CUDA(cudaMemsetAsync(d, 0, sizeof(int), ctx.stream));
+    maxdeg_kernel<<<grid_for(g.n, 256), 256, 0, ctx.stream>>>(g.n, g.xadj, d);
+    KB_LAUNCH();
+    KB_CUDA(cudaMemcpyAsync(ctx.pinned, d, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    KB_CUDA(cudaStreamSynchronize(ctx.stream));
+    return (int)ctx.pinned[0];
+}
+
+void init_labels(Ctx& ctx, const DevGraph& g, int* label, uint32_t* cw) {
+    if (g.n == 0) return;
+    init_labels_kernel<<<grid_for(g.n, 256), 256, 0, ctx.stream>>>(g.n, g.vwgt, label, cw);
+    KB_LAUNCH();
+}
+
+}  // namespace kb

@@ -1,0 +1,245 @@
+// partitioner.cu -- the multilevel driver (graph_partitioner.cpp:240-273,
+// coarsening.cpp:30-97, uncoarsening.cpp:43-121 restated for the device):
+// coarsen by LP clustering + contraction until the simple stop rule says
+// stop, partition the coarsest graph on the host, then project, repair
+// balance and refine level by level.  Also holds the Ctx implementation.
+#include "partitioner.cuh"
+
+#include <chrono>
+#include <cstring>
+#include <stdexcept>
+
+#include "contract.cuh"
+#include "host/initial_partitioning.h"
+#include "prims.cuh"
+
+namespace kb {
+
+// ------------------------------------------------------------------- Ctx
+
+Ctx::~Ctx() {
+    if (device >= 0) cudaSetDevice(device);
+    for (auto& p : pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
+    for (auto e : ev_free) cudaEventDestroy(e);
+    if (pinned) cudaFreeHost(pinned);
+    if (dscalars) cudaFree(dscalars);
+    hier.free_all();
+    scratch.free_all();
+    if (own_stream && stream) cudaStreamDestroy(stream);
+}
+
+void Ctx::init(int dev, cudaStream_t s) {
+    device = dev;
+    KB_CUDA(cudaSetDevice(dev));
+    if (!stream) {
+        KB_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        own_stream = true;
+    }
+    if (!pinned) KB_CUDA(cudaMallocHost(&pinned, 64 * sizeof(uint32_t)));
+    if (!dscalars) {
+        KB_CUDA(cudaMalloc(&dscalars, 64 * sizeof(int) + 4 * sizeof(unsigned long long)));
+        work = reinterpret_cast<unsigned long long*>(dscalars + 64);
+    }
+    (void)s;
+}
+
+int Ctx::phase_id(const char* name) {
+    for (size_t i = 0; i < phases.size(); ++i)
+        if (phases[i].name == name) return (int)i;
+    phases.push_back(PhaseTimer{name, 0, 0, 0});
+    return (int)phases.size() - 1;
+}
+
+cudaEvent_t Ctx::ev() {
+    if (!ev_free.empty()) {
+        cudaEvent_t e = ev_free.back();
+        ev_free.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    KB_CUDA(cudaEventCreate(&e));
+    return e;
+}
+
+void Ctx::begin(int phase, cudaEvent_t& a) {
+    (void)phase;
+    a = ev();
+    KB_CUDA(cudaEventRecord(a, stream));
+}
+
+void Ctx::end(int phase, cudaEvent_t a, double bytes) {
+    cudaEvent_t b = ev();
+    KB_CUDA(cudaEventRecord(b, stream));
+    pending.push_back(Pending{phase, a, b, bytes});
+    if (pending.size() > 4096) {
+        KB_CUDA(cudaStreamSynchronize(stream));
+        collect();
+    }
+}
+
+void Ctx::collect() {
+    for (auto& p : pending) {
+        float ms = 0;
+        KB_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+        phases[p.phase].ms += ms;
+        phases[p.phase].bytes += p.bytes;
+        phases[p.phase].launches += 1;
+        ev_free.push_back(p.a);
+        ev_free.push_back(p.b);
+    }
+    pending.clear();
+}
+
+void Ctx::reset_stats() {
+    phases.clear();
+    if (work) KB_CUDA(cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), stream));
+    if (dscalars) KB_CUDA(cudaMemsetAsync(dscalars + 60, 0, sizeof(int), stream));
+}
+
+// ------------------------------------------------------------ the driver
+
+namespace {
+
+using clk = std::chrono::steady_clock;
+double ms_since(clk::time_point t) {
+    return std::chrono::duration<double, std::milli>(clk::now() - t).count();
+}
+
+struct Level {
+    DevGraph g;
+    int* cmap = nullptr;  // fine -> coarse (null at the coarsest level)
+    int* part = nullptr;
+};
+
+uint32_t read_max_bw(Ctx& ctx, const uint32_t* bw, int k, std::vector<uint32_t>& host) {
+    host.resize((size_t)k);
+    KB_CUDA(cudaMemcpyAsync(host.data(), bw, sizeof(uint32_t) * (size_t)k, cudaMemcpyDeviceToHost, ctx.stream));
+    KB_CUDA(cudaStreamSynchronize(ctx.stream));
+    uint32_t mx = 0;
+    for (uint32_t x : host) mx = std::max(mx, x);
+    return mx;
+}
+
+long long read_cut(Ctx& ctx, const DevGraph& g, const int* part, int k, uint32_t* bw) {
+    unsigned long long* c = reinterpret_cast<unsigned long long*>(ctx.dscalars + 32);
+    block_weights_and_cut(ctx, g, part, k, bw, c);
+    unsigned long long h = 0;
+    KB_CUDA(cudaMemcpyAsync(&h, c, sizeof(h), cudaMemcpyDeviceToHost, ctx.stream));
+    KB_CUDA(cudaStreamSynchronize(ctx.stream));
+    return (long long)h / 2;
+}
+
+}  // namespace
+
+void reserve_for(Ctx& ctx, int n, long long m, bool copy_input, double factor) {
+    double hier = (copy_input ? 4.0 * (n + 1) + 8.0 * m + 4.0 * n : 0.0) + 12.0 * m + 40.0 * n + (64 << 20);
+    double scr = 40.0 * m + 48.0 * n + (1.2 * (1 << 30)) + (64 << 20);
+    ctx.hier.reserve((size_t)(hier * factor));
+    ctx.scratch.reserve((size_t)(scr * factor));
+}
+
+int partition(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_part, long long* edgecut,
+              kb200_stats* st) {
+    const int k = kn.k;
+    const bool collect = st && st->collect_level_cuts;
+    cudaStream_t s = ctx.stream;
+    std::vector<Level> lv;
+    lv.push_back(Level{g0, nullptr, d_part});
+    lv[0].g.maxdeg = max_degree(ctx, lv[0].g);
+
+    // ---------------------------------------------------------- coarsening
+    auto t0 = clk::now();
+    {
+        int L = 0;
+        while (L + 1 < kn.max_levels && lv[L].g.n > 0) {
+            const DevGraph& f = lv[L].g;
+            lv[L].cmap = ctx.hier.alloc<int>((size_t)f.n);
+            const size_t mk = ctx.scratch.mark();
+            int* label = ctx.scratch.alloc<int>((size_t)f.n);
+            lp_cluster(ctx, f, kn, L, label);
+            Level c;
+            int *cx, *ca, *cw, *cv;
+            contract(ctx, f, label, lv[L].cmap, c.g, &cx, &ca, &cw, &cv);
+            ctx.scratch.release(mk);
+            c.g.maxdeg = max_degree(ctx, c.g);
+            const int nf = f.n, nc = c.g.n;
+            lv.push_back(c);
+            ++L;
+            bool cont = (1.0 * nf / (double)nc >= 1.1) && (uint32_t)nc >= kn.num_stop;
+            if (!cont) break;
+        }
+    }
+    KB_CUDA(cudaStreamSynchronize(s));
+    double ms_coarsen = ms_since(t0);
+    const int L = (int)lv.size() - 1;
+
+    // ------------------------------------------------ initial partitioning
+    auto t1 = clk::now();
+    for (int l = 1; l <= L; ++l) lv[l].part = ctx.hier.alloc<int>((size_t)std::max(lv[l].g.n, 1));
+    long long initial_cut = 0;
+    {
+        const DevGraph& c = lv[L].g;
+        std::vector<int> hx((size_t)c.n + 1), ha((size_t)c.m), hw((size_t)c.m), hv((size_t)c.n), hp((size_t)c.n);
+        KB_CUDA(cudaMemcpyAsync(hx.data(), c.xadj, sizeof(int) * hx.size(), cudaMemcpyDeviceToHost, s));
+        if (c.m) {
+            KB_CUDA(cudaMemcpyAsync(ha.data(), c.adjncy, sizeof(int) * ha.size(), cudaMemcpyDeviceToHost, s));
+            KB_CUDA(cudaMemcpyAsync(hw.data(), c.adjwgt, sizeof(int) * hw.size(), cudaMemcpyDeviceToHost, s));
+        }
+        if (c.n) KB_CUDA(cudaMemcpyAsync(hv.data(), c.vwgt, sizeof(int) * hv.size(), cudaMemcpyDeviceToHost, s));
+        KB_CUDA(cudaStreamSynchronize(s));
+        initial_partition(c.n, hx.data(), ha.data(), hw.data(), hv.data(), kn, hp.data());
+        for (int v = 0; v < c.n; ++v)
+            for (int e = hx[v]; e < hx[v + 1]; ++e)
+                if (hp[v] != hp[ha[e]]) initial_cut += hw[e];
+        initial_cut /= 2;
+        if (c.n) KB_CUDA(cudaMemcpyAsync(lv[L].part, hp.data(), sizeof(int) * hp.size(), cudaMemcpyHostToDevice, s));
+        KB_CUDA(cudaStreamSynchronize(s));
+    }
+    double ms_initial = ms_since(t1);
+
+    // -------------------------------------------------------- uncoarsening
+    auto t2 = clk::now();
+    uint32_t* bw = ctx.hier.alloc<uint32_t>((size_t)k);
+    std::vector<uint32_t> hbw;
+    bool balanced = true;
+    long long final_cut = 0;
+    for (int l = L; l >= 0; --l) {
+        const DevGraph& g = lv[l].g;
+        if (l < L) project(ctx, g.n, lv[l].cmap, lv[l + 1].part, lv[l].part);
+        const uint32_t bound = l == 0 ? kn.final_bound : kn.upper_bound;
+        block_weights_and_cut(ctx, g, lv[l].part, k, bw, nullptr);
+        bool ok = balance(ctx, g, kn, l, bound, lv[l].part, bw);
+        lp_refine(ctx, g, kn, l, bound, lv[l].part, bw);
+        if (l == 0) balanced = ok;
+        if (collect || l == 0) {
+            long long c = read_cut(ctx, g, lv[l].part, k, bw);
+            uint32_t mx = read_max_bw(ctx, bw, k, hbw);
+            if (l == 0) { final_cut = c; balanced = mx <= bound; }
+            if (st && l < 64) { st->level_cut[l] = c; st->level_maxbw[l] = mx; }
+        }
+    }
+    KB_CUDA(cudaStreamSynchronize(s));
+    double ms_uncoarsen = ms_since(t2);
+
+    {
+        int err = 0;
+        KB_CUDA(cudaMemcpy(&err, ctx.dscalars + 60, sizeof(int), cudaMemcpyDeviceToHost));
+        if (err) throw std::runtime_error("device hash table overflow (internal invariant broken)");
+    }
+    *edgecut = final_cut;
+    if (st) {
+        st->levels = L + 1;
+        for (int l = 0; l <= L && l < 64; ++l) {
+            st->level_n[l] = lv[l].g.n;
+            st->level_m[l] = lv[l].g.m;
+        }
+        st->initial_cut = initial_cut;
+        st->balanced = balanced ? 1 : 0;
+        st->ms_coarsen = ms_coarsen;
+        st->ms_initial = ms_initial;
+        st->ms_uncoarsen = ms_uncoarsen;
+    }
+    return balanced ? KB_OK : KB_WARN_IMBALANCED;
+}
+
+}  // namespace kb

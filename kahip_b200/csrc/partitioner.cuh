@@ -1,0 +1,19 @@
+// partitioner.cuh -- the multilevel driver (partitioner.cu).
+#pragma once
+
+#include "lp.cuh"
+
+namespace kb {
+
+// Reserves both arenas for a graph of n nodes and m directed entries
+// (copy_input: the level-0 graph is copied into the hierarchy arena).
+void reserve_for(Ctx& ctx, int n, long long m, bool copy_input, double factor);
+
+// Partitions the device graph g0 (level 0) into kn.k blocks; d_part[n] out.
+// Returns KB_OK or KB_WARN_IMBALANCED.  Throws CudaError on CUDA failures
+// (including an exhausted arena, which the caller answers with a larger
+// reservation).
+int partition(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_part, long long* edgecut,
+              kb200_stats* st);
+
+}  // namespace kb

@@ -1,0 +1,219 @@
+"""ctypes bindings of libkahip_b200.so (the C ABI in include/kahip_b200.h and
+include/kaHIP_interface.h).
+
+The library is loaded from the package directory (built in-tree by
+``kahip_b200/csrc/Makefile``).  Loading needs no GPU; every compute entry
+point fails with KB200_ERR_NO_DEVICE when no CUDA device is visible -- there
+is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libkahip_b200.so")
+
+OK, ERR_INVALID_INPUT, ERR_CUDA, ERR_NO_DEVICE, ERR_OUT_OF_MEMORY, ERR_INTERNAL = 0, -1, -2, -3, -4, -5
+WARN_IMBALANCED = 1
+
+FAST, ECO, STRONG, FASTSOCIAL, ECOSOCIAL, STRONGSOCIAL = range(6)
+
+c_int_p = ctypes.POINTER(ctypes.c_int)
+c_u32_p = ctypes.POINTER(ctypes.c_uint32)
+c_ll_p = ctypes.POINTER(ctypes.c_longlong)
+
+
+class Knobs(ctypes.Structure):
+    """kb200_knobs"""
+    _fields_ = [("k", ctypes.c_int), ("imbalance", ctypes.c_double), ("seed", ctypes.c_int),
+                ("mode", ctypes.c_int), ("total_weight", ctypes.c_uint32),
+                ("upper_bound", ctypes.c_uint32), ("final_bound", ctypes.c_uint32),
+                ("num_stop", ctypes.c_uint32), ("max_vertex_weight", ctypes.c_uint32),
+                ("cluster_bound", ctypes.c_uint32),
+                ("lpc_rounds", ctypes.c_int), ("lpc_subrounds", ctypes.c_int),
+                ("ref_rounds", ctypes.c_int), ("ref_subrounds", ctypes.c_int),
+                ("ref_classes", ctypes.c_int), ("bal_iters", ctypes.c_int),
+                ("ip_reps", ctypes.c_int), ("ip_tries", ctypes.c_int),
+                ("ip_fm_passes", ctypes.c_int), ("ip_fm_stall", ctypes.c_int),
+                ("max_levels", ctypes.c_int)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class Stats(ctypes.Structure):
+    """kb200_stats"""
+    _fields_ = [("levels", ctypes.c_int), ("level_n", ctypes.c_int * 64),
+                ("level_m", ctypes.c_longlong * 64), ("level_cut", ctypes.c_longlong * 64),
+                ("level_maxbw", ctypes.c_uint32 * 64), ("initial_cut", ctypes.c_longlong),
+                ("balanced", ctypes.c_int), ("collect_level_cuts", ctypes.c_int),
+                ("timing", ctypes.c_int), ("ms_total", ctypes.c_double), ("ms_h2d", ctypes.c_double),
+                ("ms_coarsen", ctypes.c_double), ("ms_initial", ctypes.c_double),
+                ("ms_uncoarsen", ctypes.c_double), ("ms_d2h", ctypes.c_double),
+                ("nfamilies", ctypes.c_int), ("family_name", (ctypes.c_char * 24) * 16),
+                ("family_ms", ctypes.c_double * 16), ("family_bytes", ctypes.c_double * 16),
+                ("family_launches", ctypes.c_longlong * 16), ("sweep_vertices", ctypes.c_longlong),
+                ("sweep_edges", ctypes.c_longlong), ("device_bytes_peak", ctypes.c_size_t)]
+
+    def families(self) -> dict:
+        return {self.family_name[i].value.decode(): dict(ms=self.family_ms[i], bytes=self.family_bytes[i],
+                                                         launches=self.family_launches[i])
+                for i in range(self.nfamilies)}
+
+    def levels_list(self):
+        return [dict(n=self.level_n[i], m=self.level_m[i], cut=self.level_cut[i],
+                     maxbw=self.level_maxbw[i]) for i in range(self.levels)]
+
+
+EXPORTS = [
+    # extended ABI (include/kahip_b200.h)
+    "kb200_derive_knobs", "kb200_kaffpa", "kb200_kaffpa_device", "kb200_lp_cluster", "kb200_contract",
+    "kb200_lp_refine", "kb200_balance", "kb200_edge_cut", "kb200_project", "kb200_initial_partition",
+    "kb200_last_error", "kb200_device_count",
+    # reference-compatible ABI (include/kaHIP_interface.h)
+    "kaffpa", "kaffpa_balance", "kaffpa_balance_NE", "process_mapping", "node_separator", "reduced_nd",
+    "edge_partitioning",
+]
+
+_LIB = None
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C kahip_b200/csrc`")
+        L = ctypes.CDLL(LIB_PATH)
+        i, vp, d, u32 = ctypes.c_int, ctypes.c_void_p, ctypes.c_double, ctypes.c_uint32
+        L.kb200_derive_knobs.argtypes = [i, vp, i, d, i, i, ctypes.POINTER(Knobs)]
+        L.kb200_kaffpa.argtypes = [i, vp, vp, vp, vp, i, d, i, i, c_ll_p, vp, ctypes.POINTER(Stats)]
+        L.kb200_kaffpa_device.argtypes = [i, vp, vp, vp, vp, i, d, i, i, c_ll_p, vp, vp, ctypes.POINTER(Stats)]
+        L.kb200_lp_cluster.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, vp]
+        L.kb200_contract.argtypes = [i, vp, vp, vp, vp, vp, c_int_p, c_ll_p, vp, vp, vp, vp, vp]
+        L.kb200_lp_refine.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, u32, vp]
+        L.kb200_balance.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, u32, vp, c_int_p]
+        L.kb200_edge_cut.argtypes = [i, vp, vp, vp, vp, vp, i, c_ll_p, vp]
+        L.kb200_project.argtypes = [i, vp, i, vp, vp]
+        L.kb200_initial_partition.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), vp]
+        L.kb200_last_error.restype = ctypes.c_char_p
+        L.kb200_last_error.argtypes = []
+        L.kb200_device_count.argtypes = []
+        L.kaffpa.argtypes = [c_int_p, vp, vp, vp, vp, c_int_p, ctypes.POINTER(d), ctypes.c_bool, i, i,
+                             c_int_p, vp]
+        L.kaffpa.restype = None
+        _LIB = L
+    return _LIB
+
+
+class KaHIPError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"kb200 status {code}: {msg}")
+        self.code = code
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()  # torch tensor
+
+
+def _i32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _check(rc: int):
+    if rc < 0:
+        raise KaHIPError(rc, lib().kb200_last_error().decode())
+    return rc
+
+
+def derive_knobs(n: int, vwgt, k: int, imbalance=0.03, seed=0, mode=FAST) -> Knobs:
+    kn = Knobs()
+    vw = _i32(vwgt)
+    _check(lib().kb200_derive_knobs(n, _ptr(vw), k, imbalance, seed, mode, ctypes.byref(kn)))
+    return kn
+
+
+def kaffpa_ex(xadj, adjncy, nparts, imbalance=0.03, seed=0, mode=FAST, vwgt=None, adjwgt=None,
+              stats: Stats | None = None):
+    """Returns (status, edgecut, part)."""
+    xadj, adjncy, vwgt, adjwgt = _i32(xadj), _i32(adjncy), _i32(vwgt), _i32(adjwgt)
+    n = len(xadj) - 1
+    part = np.zeros(max(n, 0), np.int32)
+    cut = ctypes.c_longlong(-1)
+    rc = lib().kb200_kaffpa(n, _ptr(vwgt), _ptr(xadj), _ptr(adjwgt), _ptr(adjncy), nparts, imbalance, seed,
+                            mode, ctypes.byref(cut), _ptr(part), ctypes.byref(stats) if stats else None)
+    _check(rc)
+    return rc, cut.value, part
+
+
+def lp_cluster(g: dict, kn: Knobs, level=0) -> np.ndarray:
+    lab = np.empty(g["n"], np.int32)
+    _check(lib().kb200_lp_cluster(g["n"], _ptr(g["xadj"]), _ptr(g["adjncy"]), _ptr(g["adjwgt"]),
+                                  _ptr(g["vwgt"]), ctypes.byref(kn), level, _ptr(lab)))
+    return lab
+
+
+def contract(g: dict, label):
+    n, m = g["n"], g["m"]
+    nc, mc = ctypes.c_int(), ctypes.c_longlong()
+    cmap = np.empty(n, np.int32)
+    cx = np.empty(n + 1, np.int32)
+    ca = np.empty(max(m, 1), np.int32)
+    cw = np.empty(max(m, 1), np.int32)
+    cv = np.empty(max(n, 1), np.int32)
+    lab = _i32(label)
+    _check(lib().kb200_contract(n, _ptr(g["xadj"]), _ptr(g["adjncy"]), _ptr(g["adjwgt"]), _ptr(g["vwgt"]),
+                                _ptr(lab), ctypes.byref(nc), ctypes.byref(mc), _ptr(cmap), _ptr(cx), _ptr(ca),
+                                _ptr(cw), _ptr(cv)))
+    k, mk = nc.value, mc.value
+    return dict(n=k, m=mk, xadj=cx[:k + 1].copy(), adjncy=ca[:mk].copy(), adjwgt=cw[:mk].copy(),
+                vwgt=cv[:k].copy()), cmap
+
+
+def lp_refine(g: dict, kn: Knobs, part, bound: int, level=0) -> np.ndarray:
+    p = np.array(part, np.int32)
+    _check(lib().kb200_lp_refine(g["n"], _ptr(g["xadj"]), _ptr(g["adjncy"]), _ptr(g["adjwgt"]),
+                                 _ptr(g["vwgt"]), ctypes.byref(kn), level, bound, _ptr(p)))
+    return p
+
+
+def balance(g: dict, kn: Knobs, part, bound: int, level=0):
+    p = np.array(part, np.int32)
+    ok = ctypes.c_int(0)
+    _check(lib().kb200_balance(g["n"], _ptr(g["xadj"]), _ptr(g["adjncy"]), _ptr(g["adjwgt"]), _ptr(g["vwgt"]),
+                               ctypes.byref(kn), level, bound, _ptr(p), ctypes.byref(ok)))
+    return p, ok.value
+
+
+def edge_cut(g: dict, part, k: int):
+    """Returns (cut, block_weights)."""
+    cut = ctypes.c_longlong()
+    bw = np.zeros(k, np.uint32)
+    p = _i32(part)
+    _check(lib().kb200_edge_cut(g["n"], _ptr(g["xadj"]), _ptr(g["adjncy"]), _ptr(g["adjwgt"]), _ptr(g["vwgt"]),
+                                _ptr(p), k, ctypes.byref(cut), _ptr(bw)))
+    return cut.value, bw
+
+
+def project(cmap, nc: int, part_coarse) -> np.ndarray:
+    cm, pc = _i32(cmap), _i32(part_coarse)
+    out = np.empty(len(cm), np.int32)
+    _check(lib().kb200_project(len(cm), _ptr(cm), nc, _ptr(pc), _ptr(out)))
+    return out
+
+
+def initial_partition(g: dict, kn: Knobs) -> np.ndarray:
+    p = np.empty(g["n"], np.int32)
+    _check(lib().kb200_initial_partition(g["n"], _ptr(g["xadj"]), _ptr(g["adjncy"]), _ptr(g["adjwgt"]),
+                                         _ptr(g["vwgt"]), ctypes.byref(kn), _ptr(p)))
+    return p
+
+
+def device_count() -> int:
+    return lib().kb200_device_count()
