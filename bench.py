@@ -1,0 +1,405 @@
+#!/usr/bin/env python3
+"""Benchmark: ms per kaffpa-fast partition of a 2D random geometric graph,
+n = 2^24 (r = 0.55*sqrt(ln n / n), ~265M directed CSR entries, int32, unit
+weights), k = 64, imbalance 3%, seed 0, on one B200 -- plus the LP sweep's
+achieved HBM bandwidth against the measured peak and the edge cut.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Arms
+  ours       value   = device-resident ms per partition (graph already in HBM,
+                       kb200_kaffpa_device), CUDA events on the library's stream
+             e2e     = the same through the host C ABI (kb200_kaffpa, pinned
+                       host CSR in, part[] out), H2D + D2H inside the timer
+  reference  the reference kaffpa() (KaHIP built from its sources into
+             oracle/_ref) on the host cores, one process per core, on a
+             bounded sample of the workload (RGG2D n=2^22, same generator),
+             scaled to the full workload by directed-edge count.
+
+With N > 1 (torchrun), every rank partitions its own replica (weak scaling,
+no collective on the data path); value = max-over-ranks time / (K*N).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ms per kaffpa-fast partition & GE/s LP sweep (% HBM peak); cut vs plain at eps=3%"
+FULL_LOGN = 24
+SAMPLE_LOGN = 22
+K_BLOCKS = 64
+IMBALANCE = 0.03
+MODE_FAST = 0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--logn", type=int, default=FULL_LOGN, help="log2 of the RGG size (default 24)")
+    p.add_argument("--k", type=int, default=K_BLOCKS)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    FIELDS = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.uuid = uuid
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 10:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        rows = [r for r in self.rows if self.uuid is None or r[1] == self.uuid] or self.rows
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(r[2]) for r in rows if num(r[2]) is not None]
+        mx = [num(r[3]) for r in rows if num(r[3]) is not None]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, val in zip(names, r[6:10]):
+                if val.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# ------------------------------------------------------------ reference arm
+
+def _ref_worker_init():
+    os.environ["KBGEN_THREADS"] = "1"
+
+
+_SAMPLE = {}
+
+
+def _ref_task(args):
+    logn, k, seed = args
+    from kahip_b200 import graphs
+    from oracle import oracle
+    g = _SAMPLE.get(logn)
+    if g is None:
+        g = graphs.rgg2d(1 << logn, seed=0)
+        _SAMPLE[logn] = g
+    t = time.perf_counter()
+    cut, _ = oracle.ref_kaffpa(dict(g, vwgt=None, adjwgt=None), k, IMBALANCE, seed, MODE_FAST)
+    return (time.perf_counter() - t) * 1e3, cut, g["m"]
+
+
+def reference_sample_ms(logn: int, k: int, procs: int, seeds):
+    """Runs the reference kaffpa on the sample graph in `procs` processes;
+    returns (wall ms, per-run ms list, cuts, m_sample)."""
+    ctx = mp.get_context("spawn")
+    t = time.perf_counter()
+    with ctx.Pool(procs, initializer=_ref_worker_init) as pool:
+        res = pool.map(_ref_task, [(logn, k, s) for s in seeds])
+    wall = (time.perf_counter() - t) * 1e3
+    return wall, [r[0] for r in res], [r[1] for r in res], res[0][2]
+
+
+def host_procs_for_reference():
+    n = os.cpu_count() or 1
+    try:
+        with open("/proc/meminfo") as f:
+            avail = next(int(l.split()[1]) for l in f if l.startswith("MemAvailable")) * 1024
+        n = min(n, max(1, int(avail // (3 << 30))))  # ~3 GB per reference process on the 2^22 sample
+    except (OSError, StopIteration):
+        pass
+    return max(1, n)
+
+
+def full_m(logn: int) -> int:
+    from kahip_b200 import graphs
+    # the directed entry count of the full workload (generated once; cheap relative to the run)
+    return graphs.rgg2d(1 << logn, seed=0)["m"]
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return
+    from oracle import oracle
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libkahip_ref.so was not built "
+                          "(reference sources absent when __graft_entry__.build() ran)"}))
+        return
+    procs = host_procs_for_reference()
+    m_full = full_m(args.logn)
+    step_ms = []
+    cuts = []
+    m_sample = None
+    for step in range(args.warmup + args.steps):
+        seeds = [step * procs + i for i in range(procs)]
+        wall, per, c, m_sample = reference_sample_ms(SAMPLE_LOGN, args.k, procs, seeds)
+        if step >= args.warmup:
+            step_ms.append(wall / procs)
+            cuts += c
+    scale = m_full / m_sample
+    value = statistics.mean(step_ms) * scale
+    sample = (f"reference kaffpa fast (KaHIP built from its sources) on RGG2D n=2^{SAMPLE_LOGN} "
+              f"(m_directed={m_sample}), {procs} concurrent processes (one per core) per step; "
+              f"ms per partition = step wall / {procs}, scaled x{scale:.3f} by directed edges to n=2^{args.logn}")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "ms", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded RGG2D generator)",
+        "config": workload_config(args, m_full),
+        "cpu_baseline": {"value": value, "unit": "ms", "cores": procs, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_cut_sample_mean": statistics.mean(cuts) if cuts else None,
+    }
+    print(json.dumps(line))
+
+
+def workload_config(args, m):
+    return {"workload": f"kaffpa fast on RGG2D n=2^{args.logn} (r=0.55*sqrt(ln n/n)), k={args.k}, eps=3%",
+            "n": 1 << args.logn, "m_directed": m, "k": args.k, "imbalance": IMBALANCE, "preset": "fast",
+            "seed": 0, "graph_seed": 0, "l2": "inputs (~2.2 GB CSR) exceed the 126 MB L2; no flush",
+            "parallelism": "replicas" if args.gpus > 1 else "single GPU"}
+
+
+# ------------------------------------------------------------------- ours
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from kahip_b200 import graphs, native
+
+    if world > 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+
+    g = graphs.rgg2d(1 << args.logn, seed=0)
+    n, m = g["n"], g["m"]
+    d_xadj = torch.from_numpy(g["xadj"]).to(dev)
+    d_adj = torch.from_numpy(g["adjncy"]).to(dev)
+    d_w = torch.ones(m, dtype=torch.int32, device=dev)
+    d_vw = torch.ones(n, dtype=torch.int32, device=dev)
+    d_part = torch.empty(n, dtype=torch.int32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+
+    def call(st=None):
+        return native.kaffpa_device(n, d_xadj, d_adj, d_w, d_vw, d_part, args.k, IMBALANCE, 0, MODE_FAST,
+                                    stream=stream, stats=st)
+
+    for _ in range(max(3, args.warmup)):
+        call()
+    torch.cuda.synchronize()
+
+    # ---- timed region: K device-resident partitions, instrumented ----
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid)
+    sampler.start()
+    time.sleep(0.3)
+    fam = {}
+    cuts = []
+    sweep_v = sweep_e = 0
+    ms_phase = {"coarsen": 0.0, "initial": 0.0, "uncoarsen": 0.0}
+    levels = None
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = native.kernel_launches()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        st = native.Stats()
+        st.timing = 1
+        rc, cut = call(st)
+        cuts.append(cut)
+        for name, f in st.families().items():
+            a = fam.setdefault(name, {"ms": 0.0, "bytes": 0.0, "launches": 0})
+            a["ms"] += f["ms"]
+            a["bytes"] += f["bytes"]
+            a["launches"] += f["launches"]
+        sweep_v += st.sweep_vertices
+        sweep_e += st.sweep_edges
+        ms_phase["coarsen"] += st.ms_coarsen
+        ms_phase["initial"] += st.ms_initial
+        ms_phase["uncoarsen"] += st.ms_uncoarsen
+        levels = [(st.level_n[i], st.level_m[i]) for i in range(st.levels)]
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = native.kernel_launches() - launches0
+    sampler.stop()
+    elapsed = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    ms_per_step = elapsed / args.steps
+    value = elapsed / (args.steps * world)
+
+    # quality of the (deterministic) partition of the last timed call
+    part = d_part.cpu().numpy()
+    bw = np.bincount(part, minlength=args.k)
+    kn = native.derive_knobs(n, None, args.k, IMBALANCE, 0, MODE_FAST)
+
+    # ---- end to end through the host C ABI (pinned host buffers) ----
+    h_xadj = torch.from_numpy(g["xadj"]).pin_memory()
+    h_adj = torch.from_numpy(g["adjncy"]).pin_memory()
+    h_part = torch.empty(n, dtype=torch.int32).pin_memory()
+    L = native.lib()
+    import ctypes
+    e2e_cut = ctypes.c_longlong()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_steps = max(1, min(args.steps, 5))
+    for _ in range(e2e_steps):
+        rc = L.kb200_kaffpa(n, None, h_xadj.data_ptr(), None, h_adj.data_ptr(), args.k, IMBALANCE, 0, MODE_FAST,
+                            ctypes.byref(e2e_cut), h_part.data_ptr(), None)
+        if rc < 0:
+            raise RuntimeError(L.kb200_last_error().decode())
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item()) / world
+    e2e_same = bool(np.array_equal(h_part.numpy(), part)) and e2e_cut.value == cuts[-1]
+
+    # ---- roofline: the LP clustering sweep (every vertex swept once per round) ----
+    peak, peak_kind = measured_peaks()
+    sweep = fam.get("lp_cluster_sweep", {"ms": 0, "bytes": 0, "launches": 0})
+    achieved = sweep["bytes"] / (sweep["ms"] * 1e-3) / 1e9 if sweep["ms"] else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "lp_cluster_sweep_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            traffic = json.load(f).get("dram_bytes_per_launch_scaled")
+    total_fam_ms = sum(f["ms"] for f in fam.values()) or 1.0
+    roofline = {
+        "kernel": "lp_cluster_sweep (sweep_kernel<G, CLUSTER>)", "bound": "hbm",
+        "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": (achieved / peak) if achieved else None, "peak_source": f"hbm_gbs of {peak_kind}",
+        "traffic": traffic,
+        "bytes_per_launch": sweep["bytes"] / max(1, sweep["launches"]),
+        "ms_per_launch": sweep["ms"] / max(1, sweep["launches"]),
+        "share_of_timed_kernels": sweep["ms"] / total_fam_ms,
+        "ge_per_s": (sweep["bytes"] / 12.0 / (sweep["ms"] * 1e-3) / 1e9) if sweep["ms"] else None,
+    }
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded RGG2D generator)",
+        "config": workload_config(args, m),
+        "roofline": roofline,
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 4 * (n + 1 + m),
+                "d2h_bytes_per_step": 4 * n, "api": "kb200_kaffpa (host C ABI, NULL weights, pinned buffers)",
+                "same_partition_as_device_path": e2e_same},
+        "gpu_launches": launches,
+        "clocks": sampler.summary(),
+        "quality": {"cut": cuts[-1], "max_block": int(bw.max()), "bound": int(kn.final_bound),
+                    "balanced": bool(bw.max() <= kn.final_bound), "deterministic_over_steps": len(set(cuts)) == 1},
+        "phases_ms_per_step": {k: v / args.steps for k, v in ms_phase.items()},
+        "kernel_families_ms_per_step": {k: v["ms"] / args.steps for k, v in sorted(fam.items(), key=lambda x: -x[1]["ms"])},
+        "levels": levels,
+        "sweep_work_per_step": {"vertices": sweep_v / args.steps, "edges": sweep_e / args.steps},
+    }
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle
+        if oracle.ref_available():
+            wall, per, c, m_sample = reference_sample_ms(SAMPLE_LOGN, args.k, 1, [0])
+            scale = m / m_sample
+            line["cpu_baseline"] = {
+                "value": per[0] * scale, "unit": "ms", "cores": 1, "kind": "reference",
+                "sample": (f"one reference kaffpa fast run (KaHIP built from its sources, single-threaded) on "
+                           f"RGG2D n=2^{SAMPLE_LOGN} (m_directed={m_sample}, {per[0]:.0f} ms, cut {c[0]}), "
+                           f"scaled x{scale:.3f} by directed edges to n=2^{args.logn}")}
+        else:
+            line["cpu_baseline"] = {"value": None, "unit": "ms", "cores": 0, "kind": "reference",
+                                    "sample": "unavailable: oracle/_ref not built"}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -132,6 +132,9 @@ int kb200_initial_partition(int n, const int* xadj, const int* adjncy, const int
 /* Last error message of the calling thread ("" if none). */
 const char* kb200_last_error(void);
 
+/* Number of kernels this library has launched so far (process-wide). */
+long long kb200_kernel_launches(void);
+
 /* Number of CUDA devices visible (0 when none). */
 int kb200_device_count(void);
 

@@ -25,6 +25,9 @@ extern "C" {
 }
 
 namespace kb {
+
+std::atomic<long long> g_kernel_launches{0};
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -72,9 +75,13 @@ int current_device(int* dev) {
     return KB_OK;
 }
 
-// Host-side validation of a CSR graph (monotone xadj, targets in range,
-// non-negative weights).
+// Host-side validation of the O(n) part of a CSR graph (xadj starts at 0
+// and is monotone).  Targets in range and non-negative weights are checked
+// on the device right after the upload (check_uploaded), before any kernel
+// reads through adjncy.
 int validate(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt) {
+    (void)adjwgt;
+    (void)vwgt;
     if (n < 0) return fail(KB_ERR_INVALID_INPUT, "n < 0");
     if (!xadj) return fail(KB_ERR_INVALID_INPUT, "xadj is NULL");
     if (xadj[0] != 0) return fail(KB_ERR_INVALID_INPUT, "xadj[0] != 0");
@@ -82,21 +89,28 @@ int validate(int n, const int* xadj, const int* adjncy, const int* adjwgt, const
         if (xadj[v + 1] < xadj[v]) return fail(KB_ERR_INVALID_INPUT, "xadj is not monotone");
     const long long m = xadj[n];
     if (m > 0 && !adjncy) return fail(KB_ERR_INVALID_INPUT, "adjncy is NULL");
-    for (long long e = 0; e < m; ++e)
-        if (adjncy[e] < 0 || adjncy[e] >= n) return fail(KB_ERR_INVALID_INPUT, "adjncy entry out of range");
-    if (adjwgt)
-        for (long long e = 0; e < m; ++e)
-            if (adjwgt[e] < 0) return fail(KB_ERR_INVALID_INPUT, "negative edge weight");
-    if (vwgt)
-        for (int v = 0; v < n; ++v)
-            if (vwgt[v] < 0) return fail(KB_ERR_INVALID_INPUT, "negative node weight");
     return KB_OK;
+}
+
+// Device-side checks of an uploaded graph; throws InvalidInput.
+struct InvalidInput : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+void check_uploaded(Ctx& ctx, const DevGraph& g, uint32_t* total_weight = nullptr) {
+    int flags = check_graph(ctx, g, total_weight);
+    if (flags & 1) throw InvalidInput("adjncy entry out of range");
+    if (flags & 2) throw InvalidInput("negative edge weight");
+    if (flags & 4) throw InvalidInput("negative node weight");
+    if (flags & 8) throw InvalidInput("xadj does not start at 0 or is not monotone");
 }
 
 template <class F>
 int guarded(F&& f) {
     try {
         return f();
+    } catch (const InvalidInput& e) {
+        return fail(KB_ERR_INVALID_INPUT, e.what());
     } catch (const CudaError& e) {
         (void)cudaGetLastError();
         return fail(e.code == cudaErrorMemoryAllocation ? KB_ERR_OUT_OF_MEMORY : KB_ERR_CUDA, e.what());
@@ -190,7 +204,7 @@ int run_host(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const 
             begin_stats(ctx, st);
             auto th = clk::now();
             Upload up = upload(ctx, n, xadj, adjncy, adjcwgt, vwgt);
-            KB_CUDA(cudaStreamSynchronize(ctx.stream));
+            check_uploaded(ctx, up.g);
             double ms_h2d = ms_since(th);
             long long cut = 0;
             int r = partition(ctx, up.g, kn, up.part, &cut, st);
@@ -227,6 +241,7 @@ struct PhaseRun {
         ctx.timing = false;
         ctx.reset_stats();
         up = upload(ctx, n, xadj, adjncy, adjwgt, vwgt);
+        check_uploaded(ctx, up.g);
         up.g.maxdeg = max_degree(ctx, up.g);
     }
 };
@@ -283,23 +298,22 @@ int kb200_kaffpa_device(int n, const int* d_vwgt, const int* d_xadj, const int* 
         int m32 = 0;
         KB_CUDA(cudaMemcpyAsync(&m32, d_xadj + n, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
         KB_CUDA(cudaStreamSynchronize(ctx.stream));
-        // node weights are needed on the host for the knobs (total weight)
-        std::vector<int> hv((size_t)n);
-        if (n) KB_CUDA(cudaMemcpyAsync(hv.data(), d_vwgt, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, ctx.stream));
-        KB_CUDA(cudaStreamSynchronize(ctx.stream));
+        if (m32 < 0) return fail(KB_ERR_INVALID_INPUT, "xadj[n] < 0");
+        DevGraph g;
+        g.n = n;
+        g.m = m32;
+        g.xadj = d_xadj;
+        g.adjncy = d_adjncy;
+        g.adjwgt = d_adjcwgt;
+        g.vwgt = d_vwgt;
+        uint32_t W = 0;
+        check_uploaded(ctx, g, &W);
         Knobs kn;
-        derive_knobs(n, hv.data(), nparts, imbalance, seed, mode, kn);
+        derive_knobs_total(n, W, nparts, imbalance, seed, mode, kn);
         for (int attempt = 0;; ++attempt) {
             try {
                 reserve_for(ctx, n, m32, false, attempt == 0 ? 1.0 : 2.0 * attempt);
                 begin_stats(ctx, st);
-                DevGraph g;
-                g.n = n;
-                g.m = m32;
-                g.xadj = d_xadj;
-                g.adjncy = d_adjncy;
-                g.adjwgt = d_adjcwgt;
-                g.vwgt = d_vwgt;
                 long long cut = 0;
                 int r = partition(ctx, g, kn, d_part, &cut, st);
                 *edgecut = cut;
@@ -465,6 +479,8 @@ int kb200_initial_partition(int n, const int* xadj, const int* adjncy, const int
 }
 
 const char* kb200_last_error(void) { return g_last_error.c_str(); }
+
+long long kb200_kernel_launches(void) { return g_kernel_launches.load(); }
 
 int kb200_device_count(void) {
     int c = 0;

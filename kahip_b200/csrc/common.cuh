@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -38,8 +39,15 @@ inline void check(cudaError_t e, const char* file, int line) {
         throw CudaError(e, buf);
     }
 }
+// Number of kernels this library has launched (all threads, all devices).
+extern std::atomic<long long> g_kernel_launches;
+
 #define KB_CUDA(x) ::kb::check((x), __FILE__, __LINE__)
-#define KB_LAUNCH() ::kb::check(cudaGetLastError(), __FILE__, __LINE__)
+#define KB_LAUNCH()                                                          \
+    do {                                                                     \
+        ::kb::g_kernel_launches.fetch_add(1, std::memory_order_relaxed);     \
+        ::kb::check(cudaGetLastError(), __FILE__, __LINE__);                 \
+    } while (0)
 
 constexpr int kWarp = 32;
 constexpr int kNumSMs = 148;

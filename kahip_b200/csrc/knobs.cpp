@@ -8,12 +8,6 @@
 namespace kb {
 
 void derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, int mode, Knobs& kn) {
-    std::memset(&kn, 0, sizeof(kn));
-    kn.k = k;
-    kn.imbalance = imbalance;
-    kn.seed = seed;
-    kn.mode = mode;
-
     // Total node weight as the reference accumulates it (NodeWeight is a
     // 32-bit unsigned, app/balance_configuration.h:20-23).
     uint32_t W = 0;
@@ -22,6 +16,15 @@ void derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, int
     } else {
         W = (uint32_t)n;
     }
+    derive_knobs_total(n, W, k, imbalance, seed, mode, kn);
+}
+
+void derive_knobs_total(int n, uint32_t W, int k, double imbalance, int seed, int mode, Knobs& kn) {
+    std::memset(&kn, 0, sizeof(kn));
+    kn.k = k;
+    kn.imbalance = imbalance;
+    kn.seed = seed;
+    kn.mode = mode;
     kn.total_weight = W;
 
     // kaffpa() turns the fraction into percent (interface/kaHIP_interface.cpp:115);

@@ -16,4 +16,7 @@ using Knobs = kb200_knobs;
 // Fills kn; see knobs.cpp for the reference lines each value follows.
 void derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, int mode, Knobs& kn);
 
+// Same, from the node weight sum W (accumulated as a 32-bit unsigned).
+void derive_knobs_total(int n, uint32_t W, int k, double imbalance, int seed, int mode, Knobs& kn);
+
 }  // namespace kb

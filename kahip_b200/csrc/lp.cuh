@@ -49,6 +49,12 @@ void project(Ctx& ctx, int n, const int* cmap, const int* part_coarse, int* part
 // max degree of g (device reduction + readback)
 int max_degree(Ctx& ctx, const DevGraph& g);
 
+// Device-side input checks: bit 1 = target out of range, 2 = negative edge
+// weight, 4 = negative node weight, 8 = xadj not starting at 0 / not
+// monotone.  Also returns the node weight sum (32-bit, as the reference's
+// NodeWeight accumulates it).  Synchronises the stream.
+int check_graph(Ctx& ctx, const DevGraph& g, uint32_t* total_weight = nullptr);
+
 // label[v] = v, cw[v] = vwgt[v]
 void init_labels(Ctx& ctx, const DevGraph& g, int* label, uint32_t* cw);
 

@@ -58,6 +58,31 @@ __global__ void init_labels_kernel(int n, const int* __restrict__ vwgt, int* lab
     }
 }
 
+__global__ void check_graph_kernel(int n, long long m, const int* __restrict__ xadj,
+                                   const int* __restrict__ adjncy, const int* __restrict__ adjwgt,
+                                   const int* __restrict__ vwgt, int* flags, unsigned* wsum) {
+    int f = 0;
+    unsigned w = 0;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < m;
+         e += (long long)gridDim.x * blockDim.x) {
+        int t = adjncy[e];
+        if (t < 0 || t >= n) f |= 1;
+        if (adjwgt[e] < 0) f |= 2;
+    }
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        if (vwgt[v] < 0) f |= 4;
+        if (xadj[v + 1] < xadj[v]) f |= 8;
+        w += (unsigned)vwgt[v];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && xadj[0] != 0) f |= 8;
+    f = __reduce_or_sync(0xffffffffu, f);
+    w = __reduce_add_sync(0xffffffffu, w);
+    if ((threadIdx.x & 31) == 0) {
+        if (f) atomicOr(flags, f);
+        if (w) atomicAdd(wsum, w);
+    }
+}
+
 int grid_for(long long n, int threads) {
     return (int)std::max<long long>(1, std::min<long long>(div_up(n, threads), (long long)kNumSMs * 16));
 }
@@ -95,6 +120,20 @@ int max_degree(Ctx& ctx, const DevGraph& g) {
     KB_CUDA(cudaMemcpyAsync(ctx.pinned, d, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
     KB_CUDA(cudaStreamSynchronize(ctx.stream));
     return (int)ctx.pinned[0];
+}
+
+int check_graph(Ctx& ctx, const DevGraph& g, uint32_t* total_weight) {
+    int* d = ctx.dscalars + 2;  // [2] flags, [3] node weight sum
+    KB_CUDA(cudaMemsetAsync(d, 0, 2 * sizeof(int), ctx.stream));
+    if (g.m > 0 || g.n > 0) {
+        check_graph_kernel<<<grid_for(std::max<long long>(g.m, g.n), 256), 256, 0, ctx.stream>>>(
+            g.n, g.m, g.xadj, g.adjncy, g.adjwgt, g.vwgt, d, reinterpret_cast<unsigned*>(d + 1));
+        KB_LAUNCH();
+    }
+    KB_CUDA(cudaMemcpyAsync(ctx.pinned + 2, d, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    KB_CUDA(cudaStreamSynchronize(ctx.stream));
+    if (total_weight) *total_weight = ctx.pinned[3];
+    return (int)ctx.pinned[2];
 }
 
 void init_labels(Ctx& ctx, const DevGraph& g, int* label, uint32_t* cw) {

@@ -72,7 +72,7 @@ EXPORTS = [
     # extended ABI (include/kahip_b200.h)
     "kb200_derive_knobs", "kb200_kaffpa", "kb200_kaffpa_device", "kb200_lp_cluster", "kb200_contract",
     "kb200_lp_refine", "kb200_balance", "kb200_edge_cut", "kb200_project", "kb200_initial_partition",
-    "kb200_last_error", "kb200_device_count",
+    "kb200_last_error", "kb200_kernel_launches", "kb200_device_count",
     # reference-compatible ABI (include/kaHIP_interface.h)
     "kaffpa", "kaffpa_balance", "kaffpa_balance_NE", "process_mapping", "node_separator", "reduced_nd",
     "edge_partitioning",
@@ -101,6 +101,8 @@ def lib():
         L.kb200_last_error.restype = ctypes.c_char_p
         L.kb200_last_error.argtypes = []
         L.kb200_device_count.argtypes = []
+        L.kb200_kernel_launches.argtypes = []
+        L.kb200_kernel_launches.restype = ctypes.c_longlong
         L.kaffpa.argtypes = [c_int_p, vp, vp, vp, vp, c_int_p, ctypes.POINTER(d), ctypes.c_bool, i, i,
                              c_int_p, vp]
         L.kaffpa.restype = None
@@ -217,3 +219,20 @@ def initial_partition(g: dict, kn: Knobs) -> np.ndarray:
 
 def device_count() -> int:
     return lib().kb200_device_count()
+
+
+def kernel_launches() -> int:
+    return lib().kb200_kernel_launches()
+
+
+def kaffpa_device(n, xadj, adjncy, adjwgt, vwgt, part, nparts, imbalance=0.03, seed=0, mode=FAST,
+                  stream=None, stats: Stats | None = None):
+    """Device-resident call: every array is a CUDA tensor (int32) of the current
+    device; stream is a torch.cuda.Stream (or None).  Returns (status, edgecut)."""
+    cut = ctypes.c_longlong(-1)
+    rc = lib().kb200_kaffpa_device(n, _ptr(vwgt), _ptr(xadj), _ptr(adjwgt), _ptr(adjncy), nparts, imbalance,
+                                   seed, mode, ctypes.byref(cut), _ptr(part),
+                                   None if stream is None else stream.cuda_stream,
+                                   ctypes.byref(stats) if stats else None)
+    _check(rc)
+    return rc, cut.value

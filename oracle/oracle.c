@@ -99,6 +99,13 @@ void or_derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, 
     o->max_levels = 48;
 }
 
+/* stop_rules.h:64-66: continue coarsening after a level that went from nf to
+ * nc nodes? */
+int or_stop_continue(const or_knobs* kn, int nf, int nc) {
+    double rate = 1.0 * nf / (double)nc;
+    return rate >= 1.1 && (uint32_t)nc >= kn->num_stop;
+}
+
 /* ----------------------------------------------------------------- metrics */
 
 long long or_edge_cut(const or_graph* g, const int* part) {
@@ -1136,8 +1143,7 @@ int or_kaffpa(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const
         free(label);
         c->g.n = nc; c->g.xadj = c->xadj; c->g.adjncy = c->adjncy; c->g.adjwgt = c->adjwgt; c->g.vwgt = c->vwgt;
         ++L;
-        int cont = (1.0 * f->n / (double)nc >= 1.1) && (uint32_t)nc >= kn.num_stop;
-        if (!cont) break;
+        if (!or_stop_continue(&kn, f->n, nc)) break;
     }
     /* initial partition of the coarsest graph */
     int* cpart = xmalloc(sizeof(int) * (size_t)(lv[L].g.n ? lv[L].g.n : 1));

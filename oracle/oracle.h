@@ -64,6 +64,9 @@ uint32_t or_hash(uint64_t stream, uint32_t x);
 void or_derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, int mode,
                      or_knobs* out);
 
+/* stop_rules.h:64-66 */
+int or_stop_continue(const or_knobs* kn, int nf, int nc);
+
 /* quality_metrics.cpp:23-37 and :265-288 */
 long long or_edge_cut(const or_graph* g, const int* part);
 void or_block_weights(const or_graph* g, const int* part, int k, uint32_t* bw);

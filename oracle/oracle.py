@@ -115,6 +115,14 @@ def knobs(g: dict, k: int, imbalance=0.03, seed=0, mode=0) -> Knobs:
     return kn
 
 
+def stop_continue(kn: Knobs, nf: int, nc: int) -> bool:
+    return bool(lib().or_stop_continue(ctypes.byref(kn), nf, nc))
+
+
+def balance_ratio(g: dict, part, k: int) -> float:
+    return lib().or_balance_ratio(G(g).ref, _p(np.ascontiguousarray(part, np.int32)), k)
+
+
 def edge_cut(g: dict, part) -> int:
     return lib().or_edge_cut(G(g).ref, _p(np.ascontiguousarray(part, np.int32)))
 
@@ -219,6 +227,11 @@ def ref_balance_config(n: int, vwgt, k: int, imbalance=0.03, mode=0):
     ref().ref_balance_config(n, _p(vwgt), k, ctypes.c_double(imbalance), mode, ctypes.byref(u),
                              ctypes.byref(ns), ctypes.byref(mv))
     return u.value, ns.value, mv.value
+
+
+def ref_stop_continue(nf: int, nc: int, n0: int, k: int, work_load: int) -> bool:
+    return bool(ref().ref_stop_rule_continue(ctypes.c_uint(nf), ctypes.c_uint(nc), n0, k,
+                                             ctypes.c_uint(work_load)))
 
 
 def ref_edge_cut(g: dict, part, k: int) -> int:
