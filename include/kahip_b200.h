@@ -129,6 +129,23 @@ int kb200_project(int n, const int* cmap, int nc, const int* part_coarse, int* p
 int kb200_initial_partition(int n, const int* xadj, const int* adjncy, const int* adjwgt,
                             const int* vwgt, const kb200_knobs* kn, int* part);
 
+/* Edge cut and block weights of a device-resident partition, computed
+ * without allocating anything.  No counterpart in the reference (which has no
+ * device code); it exists for callers that must not call cudaMalloc while
+ * they run (fixed device-memory budgets, allocator-free sections, device
+ * memory owned by another runtime).  All arrays are device pointers on the
+ * current device (adjwgt / vwgt may be NULL = unit weights); *d_cut and
+ * d_bw[k] are written asynchronously on `stream` (a cudaStream_t, NULL = the
+ * default stream); *d_cut = -1 if a block id or target is out of range.
+ * Limits: k <= 65536 (larger k returns KB200_ERR_INVALID_INPUT).  Its working
+ * memory is one 256 KiB __device__ array held by every GPU that loads the
+ * library until exit and shared by all calls: calls that overlap on the GPU
+ * race and give wrong results.  The first call on a device looks up that
+ * array's address, so make it before any stream capture begins. */
+int kb200_edge_cut_noalloc(int n, const int* d_xadj, const int* d_adjncy, const int* d_adjwgt,
+                           const int* d_vwgt, const int* d_part, int k, long long* d_cut, uint32_t* d_bw,
+                           void* stream);
+
 /* Last error message of the calling thread ("" if none). */
 const char* kb200_last_error(void);
 

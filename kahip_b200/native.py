@@ -72,7 +72,7 @@ EXPORTS = [
     # extended ABI (include/kahip_b200.h)
     "kb200_derive_knobs", "kb200_kaffpa", "kb200_kaffpa_device", "kb200_lp_cluster", "kb200_contract",
     "kb200_lp_refine", "kb200_balance", "kb200_edge_cut", "kb200_project", "kb200_initial_partition",
-    "kb200_last_error", "kb200_kernel_launches", "kb200_device_count",
+    "kb200_last_error", "kb200_kernel_launches", "kb200_device_count", "kb200_edge_cut_noalloc",
     # reference-compatible ABI (include/kaHIP_interface.h)
     "kaffpa", "kaffpa_balance", "kaffpa_balance_NE", "process_mapping", "node_separator", "reduced_nd",
     "edge_partitioning",
