@@ -21,6 +21,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "../hash.h"
@@ -417,13 +418,16 @@ int levels_needed(int k) {
     return l;
 }
 
+// Recursion over the bisection tree.  A bisection's hash streams depend only
+// on its position in the tree (root 1, children 2i and 2i+1) and the
+// repetition, so the two halves are independent; large halves run on their
+// own host thread, with identical results to a sequential recursion.
 void recurse(const Knobs& kn, const HostGraph& g, const std::vector<int>& orig, int k, int offset, int rep,
-             int& counter, std::vector<int>& out) {
+             uint32_t node, std::vector<int>& out, int spawn_depth) {
     if (k == 1 || g.n == 0) {
         for (int v = 0; v < g.n; ++v) out[orig[v]] = offset;
         return;
     }
-    const int bis_id = counter++;
     const int kl = (k + 1) / 2, kr = k - kl;
     const uint64_t W = (uint64_t)g.weight();
     const uint64_t t0 = W * (uint64_t)kl / (uint64_t)k;
@@ -433,12 +437,28 @@ void recurse(const Knobs& kn, const HostGraph& g, const std::vector<int>& orig, 
     eb = std::max(eb, std::min(eps, 0.01));
     Limits lim{{(uint64_t)((1.0 + eb) * (double)t0), (uint64_t)((1.0 + eb) * (double)t1)}};
     Bisector bis{kn};
-    std::vector<char> side = bis.multilevel(g, t0, lim, bis_id * 64 + rep);
+    std::vector<char> side = bis.multilevel(g, t0, lim, (int)(node * 64u + (uint32_t)rep));
     std::vector<int> lo, ro;
     HostGraph L = induced(g, orig, side, 0, lo);
     HostGraph R = induced(g, orig, side, 1, ro);
-    recurse(kn, L, lo, kl, offset, rep, counter, out);
-    recurse(kn, R, ro, kr, offset + kl, rep, counter, out);
+    side.clear();
+    side.shrink_to_fit();
+    // out[] entries written by the two halves are disjoint
+    if (spawn_depth > 0 && kl > 1 && kr > 1 && L.n > 512 && R.n > 512) {
+        std::thread left([&] { recurse(kn, L, lo, kl, offset, rep, 2u * node, out, spawn_depth - 1); });
+        recurse(kn, R, ro, kr, offset + kl, rep, 2u * node + 1u, out, spawn_depth - 1);
+        left.join();
+    } else {
+        recurse(kn, L, lo, kl, offset, rep, 2u * node, out, 0);
+        recurse(kn, R, ro, kr, offset + kl, rep, 2u * node + 1u, out, 0);
+    }
+}
+
+int spawn_depth_for_host() {
+    unsigned t = std::thread::hardware_concurrency();
+    int d = 0;
+    while (d < 5 && (2u << d) <= t) ++d;
+    return d;
 }
 
 }  // namespace
@@ -455,9 +475,9 @@ void initial_partition(int n, const int* xadj, const int* adjncy, const int* adj
     for (int v = 0; v < n; ++v) orig[v] = v;
     std::vector<int> cand(n);
     long long best = LLONG_MAX;
+    const int depth = spawn_depth_for_host();
     for (int rep = 0; rep < kn.ip_reps; ++rep) {
-        int counter = 0;
-        recurse(kn, g, orig, kn.k, 0, rep, counter, cand);
+        recurse(kn, g, orig, kn.k, 0, rep, 1u, cand, depth);
         long long c = 0;
         for (int v = 0; v < n; ++v)
             for (int e = xadj[v]; e < xadj[v + 1]; ++e)

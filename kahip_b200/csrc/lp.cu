@@ -49,8 +49,7 @@ struct SweepArgs {
     int P;                              // admission classes
     int table;                          // per-group table capacity (power of 2)
     // outputs
-    int* pv; int* pt; int* pc;          // proposal list
-    unsigned* pcount;
+    int* pt; int* pc;                   // per vertex: proposed target / class (-1: none)
     uint32_t* inc;                      // CLUSTER: incoming weight per target
     int* minv;                          // CLUSTER: smallest proposer per target
     uint32_t* H;                        // REFINE/BALANCE: weight per (target, class)
@@ -123,20 +122,16 @@ template <int MODE>
 __device__ void decide_emit(const SweepArgs& a, int v, uint32_t own, uint32_t cv, uint32_t conn_own,
                             uint64_t key, uint32_t id) {
     if (MODE == CLUSTER) {
-        if (id == kEmpty || (uint32_t)(key >> 32) <= conn_own) return;
-        unsigned i = atomicAdd(a.pcount, 1u);
-        a.pv[i] = v;
-        a.pt[i] = (int)id;
+        if (id == kEmpty || (uint32_t)(key >> 32) <= conn_own) { a.pt[v] = -1; return; }
+        a.pt[v] = (int)id;
         atomicAdd(&a.inc[id], cv);
         atomicMin(&a.minv[id], v);
     } else if (MODE == REFINE) {
         uint32_t base = a.lw[own] <= a.bound ? conn_own : 0u;
-        if (id == kEmpty || (uint32_t)(key >> 32) <= base) return;
+        if (id == kEmpty || (uint32_t)(key >> 32) <= base) { a.pt[v] = -1; return; }
         int cls = (int)(hash32(a.ks_prio, (uint32_t)v) % (uint32_t)a.P);
-        unsigned i = atomicAdd(a.pcount, 1u);
-        a.pv[i] = v;
-        a.pt[i] = (int)id;
-        a.pc[i] = cls;
+        a.pt[v] = (int)id;
+        a.pc[v] = cls;
         size_t h = (size_t)id * a.P + cls;
         atomicAdd(&a.H[h], cv);
         atomicMin(&a.minvP[h], v);
@@ -144,16 +139,14 @@ __device__ void decide_emit(const SweepArgs& a, int v, uint32_t own, uint32_t cv
         uint32_t t = id, tc = (uint32_t)(key >> 32);
         if (t == kEmpty) {
             int L = *a.lightest;
-            if ((uint32_t)L == own || (uint64_t)a.lw[L] + cv > a.bound) return;
+            if ((uint32_t)L == own || (uint64_t)a.lw[L] + cv > a.bound) { a.pt[v] = -1; return; }
             t = (uint32_t)L;
             tc = 0;
         }
         long long loss = (long long)conn_own - (long long)tc;
         int cls = loss_bucket(loss) * 8 + (int)(hash32(a.ks_sub, (uint32_t)v) % 8u);
-        unsigned i = atomicAdd(a.pcount, 1u);
-        a.pv[i] = v;
-        a.pt[i] = (int)t;
-        a.pc[i] = cls;
+        a.pt[v] = (int)t;
+        a.pc[v] = cls;
         atomicAdd(&a.HS[(size_t)own * kBalClasses + cls], cv);
     }
 }
@@ -246,6 +239,7 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(SweepArgs a) {
     for (long long chunk = warp; chunk < nchunks; chunk += nwarps) {
         int v = (int)(chunk * 32 + lane);
         bool mem = v < a.n && member<MODE>(a, v);
+        if (v < a.n && !mem) a.pt[v] = -1;
         unsigned mask = __ballot_sync(0xffffffffu, mem);
         while (mask) {
             int pick = -1;
@@ -329,25 +323,27 @@ __global__ void __launch_bounds__(kThreads) heavy_kernel(SweepArgs a, uint32_t* 
 
 // ---------------------------------------------------------------- admission
 
+// Proposal encoding per vertex: pt[v] = target (>= 0), -1 = no proposal,
+// -2 - target = rejected (its accumulators still need resetting).
+
 // Clustering: all proposals into b are admitted if they fit together;
 // otherwise only the smallest proposer (which fits by itself).
-__global__ void cluster_decide(const unsigned* pcount, const int* pv, int* pt, const int* vwgt,
-                               const uint32_t* cw, const uint32_t* inc, const int* minv,
+__global__ void cluster_decide(int n, int* pt, const uint32_t* cw, const uint32_t* inc, const int* minv,
                                uint32_t bound) {
-    const unsigned cnt = *pcount;
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
-        int v = pv[i], b = pt[i];
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        int b = pt[v];
+        if (b < 0) continue;
         bool ok = ((uint64_t)cw[b] + inc[b] < bound) || minv[b] == v;
-        if (!ok) pt[i] = -1 - b;
+        if (!ok) pt[v] = -2 - b;
     }
 }
 
-__global__ void cluster_apply(const unsigned* pcount, const int* pv, const int* pt, const int* vwgt,
-                              int* label, uint32_t* cw, uint32_t* inc, int* minv) {
-    const unsigned cnt = *pcount;
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
-        int v = pv[i], t = pt[i];
-        int b = t >= 0 ? t : -1 - t;
+__global__ void cluster_apply(int n, const int* pt, const int* vwgt, int* label, uint32_t* cw, uint32_t* inc,
+                              int* minv) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        int t = pt[v];
+        if (t == -1) continue;
+        int b = t >= 0 ? t : -2 - t;
         inc[b] = 0;
         minv[b] = INT_MAX;
         if (t < 0) continue;
@@ -373,27 +369,28 @@ __device__ __forceinline__ bool admit(const uint32_t* H, const int* minvP, int P
 
 // strict: cap = bound - 1 - w[b] (refinement keeps blocks < bound);
 // otherwise cap = bound - w[b] (balance repair fills up to bound)
-__global__ void class_decide(const unsigned* pcount, const int* pv, int* pt, const int* pc,
-                             const int* vwgt, const uint32_t* bw, const uint32_t* H, const int* minvP,
-                             int P, uint32_t bound, int strict) {
-    const unsigned cnt = *pcount;
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
-        int b = pt[i], c = pc[i];
-        if (b < 0 || c < 0) continue;
+__global__ void class_decide(int n, int* pt, const int* pc, const int* vwgt, const uint32_t* bw,
+                             const uint32_t* H, const int* minvP, int P, uint32_t bound, int strict) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        int b = pt[v];
+        if (b < 0) continue;
+        int c = pc[v];
+        if (c < 0) continue;
         long long cap = (long long)bound - (strict ? 1 : 0) - (long long)bw[b];
-        if (!admit(H, minvP, P, b, c, pv[i], (uint32_t)vwgt[pv[i]], cap)) pt[i] = -1 - b;
+        if (!admit(H, minvP, P, b, c, v, (uint32_t)vwgt[v], cap)) pt[v] = -2 - b;
     }
 }
 
-__global__ void class_apply(const unsigned* pcount, const int* pv, const int* pt, const int* pc,
-                            const int* xadj, const int* adjncy, const int* vwgt, int* part,
-                            uint32_t* bw, uint32_t* H, int* minvP, int P, uint8_t* next_active,
-                            unsigned* moved) {
-    const unsigned cnt = *pcount;
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
-        int v = pv[i], t = pt[i], c = pc[i];
+__global__ void class_apply(int n, const int* pt, const int* pc, const int* xadj, const int* adjncy,
+                            const int* vwgt, int* part, uint32_t* bw, uint32_t* H, int* minvP, int P,
+                            uint8_t* next_active, unsigned* moved) {
+    unsigned mv = 0;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        int t = pt[v];
+        if (t == -1) continue;
+        int c = pc[v];
         if (c < 0) continue;  // dropped before admission (balance)
-        int b = t >= 0 ? t : -1 - t;
+        int b = t >= 0 ? t : -2 - t;
         H[(size_t)b * P + c] = 0;
         minvP[(size_t)b * P + c] = INT_MAX;
         if (t < 0) continue;
@@ -401,10 +398,12 @@ __global__ void class_apply(const unsigned* pcount, const int* pv, const int* pt
         atomicSub(&bw[part[v]], cv);
         atomicAdd(&bw[t], cv);
         part[v] = t;
-        atomicAdd(moved, 1u);
+        ++mv;
         if (next_active)
             for (int e = xadj[v]; e < xadj[v + 1]; ++e) next_active[adjncy[e]] = 1;
     }
+    mv = __reduce_add_sync(0xffffffffu, mv);
+    if ((threadIdx.x & 31) == 0 && mv) atomicAdd(moved, mv);
 }
 
 // Balance: per overloaded block, the release threshold class.
@@ -421,16 +420,15 @@ __global__ void balance_threshold(const uint32_t* bw, const uint32_t* HS, int k,
 }
 
 // Balance: released candidates get an admission class; others are dropped.
-__global__ void balance_release(const unsigned* pcount, const int* pv, const int* pt, int* pc,
-                                const int* part, const int* vwgt, const int* thr, uint32_t* H,
-                                int* minvP, int P, uint64_t ks_prio) {
-    const unsigned cnt = *pcount;
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
-        int v = pv[i];
-        if (pc[i] >= thr[part[v]]) { pc[i] = -1; continue; }
+__global__ void balance_release(int n, const int* pt, int* pc, const int* part, const int* vwgt, const int* thr,
+                                uint32_t* H, int* minvP, int P, uint64_t ks_prio) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        int t = pt[v];
+        if (t < 0) continue;
+        if (pc[v] >= thr[part[v]]) { pc[v] = -1; continue; }
         int c = (int)(hash32(ks_prio, (uint32_t)v) % (uint32_t)P);
-        pc[i] = c;
-        size_t h = (size_t)pt[i] * P + c;
+        pc[v] = c;
+        size_t h = (size_t)t * P + c;
         atomicAdd(&H[h], (uint32_t)vwgt[v]);
         atomicMin(&minvP[h], v);
     }
@@ -477,8 +475,8 @@ int table_for(int G) { return G == 32 ? 256 : (G == 16 ? 128 : 64); }
 int sweep_blocks() { return kNumSMs * 8; }
 
 struct SweepBuffers {
-    int *pv, *pt, *pc;
-    unsigned* counters;  // [0] pcount, [1] hcount, [2] moved
+    int *pt, *pc;
+    unsigned* counters;  // [0] unused, [1] hcount, [2] moved
     int* heavy;
     uint32_t *gtk, *gtv;
     int gcap, hblocks;
@@ -490,7 +488,6 @@ SweepBuffers make_buffers(Ctx& ctx, const DevGraph& g) {
     SweepBuffers b;
     Arena& A = ctx.scratch;
     size_t n = (size_t)std::max(g.n, 1);
-    b.pv = A.alloc<int>(n);
     b.pt = A.alloc<int>(n);
     b.pc = A.alloc<int>(n);
     b.heavy = A.alloc<int>(n);
@@ -506,9 +503,10 @@ SweepBuffers make_buffers(Ctx& ctx, const DevGraph& g) {
         int cap = 1;
         while (cap < 2 * g.maxdeg) cap <<= 1;
         b.gcap = cap;
-        // keep the per-block tables within ~1 GiB
+        // per-block tables within min(1 GiB, 8 B per directed entry of the level)
         long long per = (long long)cap * 8;
-        b.hblocks = (int)std::max<long long>(1, std::min<long long>(2LL * kNumSMs, (1LL << 30) / per));
+        long long budget = std::min<long long>(1LL << 30, 8LL * g.m);
+        b.hblocks = (int)std::max<long long>(1, std::min<long long>(2LL * kNumSMs, budget / per));
         b.gtk = A.alloc<uint32_t>((size_t)cap * b.hblocks);
         b.gtv = A.alloc<uint32_t>((size_t)cap * b.hblocks);
         fill_u32(b.gtk, (long long)cap * b.hblocks, kEmpty, ctx.stream);
@@ -541,10 +539,8 @@ SweepArgs base_args(const DevGraph& g, const SweepBuffers& b) {
     a.adjncy = g.adjncy;
     a.adjwgt = g.adjwgt;
     a.vwgt = g.vwgt;
-    a.pv = b.pv;
     a.pt = b.pt;
     a.pc = b.pc;
-    a.pcount = b.counters;
     a.hcount = b.counters + 1;
     a.heavy = b.heavy;
     a.work = b.work;
@@ -579,7 +575,7 @@ void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* la
     a.S = (uint32_t)kn.lpc_subrounds;
     a.inc = inc;
     a.minv = minv;
-    const int dblocks = kNumSMs * 4;
+    const int dblocks = (int)std::max<long long>(1, std::min<long long>(div_up(g.n, kThreads), kNumSMs * 8LL));
     for (int r = 0; r < kn.lpc_rounds; ++r) {
         a.ks_sub = stream_key(kn.seed, TAG_CSUB, level, r);
         a.ks_tie = stream_key(kn.seed, TAG_CTIE, level, r);
@@ -590,11 +586,9 @@ void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* la
                 launch_sweep<CLUSTER>(ctx, g, a, b);
             }
             PhaseScope ps(ctx, "lp_cluster_admit", 0);
-            cluster_decide<<<dblocks, kThreads, 0, st>>>(b.counters, b.pv, b.pt, g.vwgt, cw, inc, minv,
-                                                         a.bound);
+            cluster_decide<<<dblocks, kThreads, 0, st>>>(g.n, b.pt, cw, inc, minv, a.bound);
             KB_LAUNCH();
-            cluster_apply<<<dblocks, kThreads, 0, st>>>(b.counters, b.pv, b.pt, g.vwgt, label, cw, inc,
-                                                        minv);
+            cluster_apply<<<dblocks, kThreads, 0, st>>>(g.n, b.pt, g.vwgt, label, cw, inc, minv);
             KB_LAUNCH();
         }
     }
@@ -625,7 +619,7 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
     a.P = P;
     a.H = H;
     a.minvP = minvP;
-    const int dblocks = kNumSMs * 4;
+    const int dblocks = (int)std::max<long long>(1, std::min<long long>(div_up(g.n, kThreads), kNumSMs * 8LL));
     unsigned* moved = b.counters + 2;
     for (int r = 0; r < kn.ref_rounds; ++r) {
         a.active = act;
@@ -641,11 +635,10 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
                 launch_sweep<REFINE>(ctx, g, a, b);
             }
             PhaseScope ps(ctx, "lp_refine_admit", 0);
-            class_decide<<<dblocks, kThreads, 0, st>>>(b.counters, b.pv, b.pt, b.pc, g.vwgt, bw, H, minvP,
-                                                       P, bound, 1);
+            class_decide<<<dblocks, kThreads, 0, st>>>(g.n, b.pt, b.pc, g.vwgt, bw, H, minvP, P, bound, 1);
             KB_LAUNCH();
-            class_apply<<<dblocks, kThreads, 0, st>>>(b.counters, b.pv, b.pt, b.pc, g.xadj, g.adjncy,
-                                                      g.vwgt, part, bw, H, minvP, P, nact, moved);
+            class_apply<<<dblocks, kThreads, 0, st>>>(g.n, b.pt, b.pc, g.xadj, g.adjncy, g.vwgt, part, bw, H,
+                                                      minvP, P, nact, moved);
             KB_LAUNCH();
         }
         std::swap(act, nact);
@@ -678,7 +671,7 @@ bool balance(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t b
     a.P = P;
     a.HS = HS;
     a.lightest = flags;
-    const int dblocks = kNumSMs * 4;
+    const int dblocks = (int)std::max<long long>(1, std::min<long long>(div_up(g.n, kThreads), kNumSMs * 8LL));
     bool ok = false;
     for (int it = 0; it < kn.bal_iters; ++it) {
         block_scan_kernel<<<1, 1024, 0, st>>>(bw, k, bound, flags, flags + 1);
@@ -694,14 +687,12 @@ bool balance(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t b
         launch_sweep<BALANCE>(ctx, g, a, b);
         balance_threshold<<<div_up(k, 256), 256, 0, st>>>(bw, HS, k, bound, thr);
         KB_LAUNCH();
-        balance_release<<<dblocks, kThreads, 0, st>>>(b.counters, b.pv, b.pt, b.pc, part, g.vwgt, thr, H,
-                                                      minvP, P, ks_prio);
+        balance_release<<<dblocks, kThreads, 0, st>>>(g.n, b.pt, b.pc, part, g.vwgt, thr, H, minvP, P, ks_prio);
         KB_LAUNCH();
-        class_decide<<<dblocks, kThreads, 0, st>>>(b.counters, b.pv, b.pt, b.pc, g.vwgt, bw, H, minvP, P,
-                                                   bound, 0);
+        class_decide<<<dblocks, kThreads, 0, st>>>(g.n, b.pt, b.pc, g.vwgt, bw, H, minvP, P, bound, 0);
         KB_LAUNCH();
-        class_apply<<<dblocks, kThreads, 0, st>>>(b.counters, b.pv, b.pt, b.pc, g.xadj, g.adjncy, g.vwgt,
-                                                  part, bw, H, minvP, P, nullptr, b.counters + 2);
+        class_apply<<<dblocks, kThreads, 0, st>>>(g.n, b.pt, b.pc, g.xadj, g.adjncy, g.vwgt, part, bw, H, minvP,
+                                                  P, nullptr, b.counters + 2);
         KB_LAUNCH();
     }
     if (!ok) {

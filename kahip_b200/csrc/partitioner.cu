@@ -133,7 +133,9 @@ long long read_cut(Ctx& ctx, const DevGraph& g, const int* part, int k, uint32_t
 
 void reserve_for(Ctx& ctx, int n, long long m, bool copy_input, double factor) {
     double hier = (copy_input ? 4.0 * (n + 1) + 8.0 * m + 4.0 * n : 0.0) + 12.0 * m + 40.0 * n + (64 << 20);
-    double scr = 40.0 * m + 48.0 * n + (1.2 * (1 << 30)) + (64 << 20);
+    // heavy-vertex hash tables are capped at min(1 GiB, 8 B per directed entry)
+    double heavy = std::min(1.0 * (1 << 30), 8.0 * m) + (1 << 20);
+    double scr = 40.0 * m + 48.0 * n + heavy + (64 << 20);
     ctx.hier.reserve((size_t)(hier * factor));
     ctx.scratch.reserve((size_t)(scr * factor));
 }

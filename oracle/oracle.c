@@ -1051,13 +1051,15 @@ static int ceil_log2(int k) {
  * half gets ceil(k/2) blocks; each side may exceed its share of the weight
  * by eps_b = (1+eps)^(1/ceil(log2 k)) - 1. */
 static void rb(const or_graph* g, const int* orig, int k, int offset, const or_knobs* kn,
-               int rep, int* bis_counter, int* out_part) {
+               int rep, uint32_t node, int* out_part) {
     if (k == 1 || g->n == 0) {
         for (int v = 0; v < g->n; ++v) out_part[orig[v]] = offset;
         return;
     }
     const int n = g->n;
-    int bis_id = (*bis_counter)++;
+    /* bisections are numbered by their position in the recursion tree (root
+     * 1, children 2i and 2i+1), so both halves can be computed independently */
+    int bis_key = (int)(node * 64u + (uint32_t)rep);
     int kl = (k + 1) / 2, kr = k - kl;
     uint64_t W = 0;
     for (int v = 0; v < n; ++v) W += (uint64_t)g->vwgt[v];
@@ -1071,15 +1073,15 @@ static void rb(const or_graph* g, const int* orig, int k, int offset, const or_k
     if (eb < floor_eb) eb = floor_eb;
     uint64_t maxw[2] = {(uint64_t)((1.0 + eb) * (double)t0), (uint64_t)((1.0 + eb) * (double)t1)};
     char* best_side = xmalloc((size_t)n);
-    ml_bisect(g, t0, maxw, kn, bis_id * 64 + rep, best_side);
+    ml_bisect(g, t0, maxw, kn, bis_key, best_side);
     or_sub L, R;
     extract(g, orig, best_side, 0, &L);
     extract(g, orig, best_side, 1, &R);
     free(best_side);
     or_graph gl = {L.n, L.xadj, L.adjncy, L.adjwgt, L.vwgt};
     or_graph gr = {R.n, R.xadj, R.adjncy, R.adjwgt, R.vwgt};
-    rb(&gl, L.orig, kl, offset, kn, rep, bis_counter, out_part);
-    rb(&gr, R.orig, kr, offset + kl, kn, rep, bis_counter, out_part);
+    rb(&gl, L.orig, kl, offset, kn, rep, 2u * node, out_part);
+    rb(&gr, R.orig, kr, offset + kl, kn, rep, 2u * node + 1u, out_part);
     sub_free(&L);
     sub_free(&R);
 }
@@ -1092,8 +1094,7 @@ void or_initial_partition(const or_graph* g, const or_knobs* kn, int* part) {
     for (int v = 0; v < n; ++v) orig[v] = v;
     long long best = LLONG_MAX;
     for (int rep = 0; rep < kn->ip_reps; ++rep) {
-        int counter = 0;
-        rb(g, orig, kn->k, 0, kn, rep, &counter, cand);
+        rb(g, orig, kn->k, 0, kn, rep, 1u, cand);
         long long c = or_edge_cut(g, cand);
         if (c < best) { best = c; memcpy(part, cand, sizeof(int) * (size_t)n); }
     }
