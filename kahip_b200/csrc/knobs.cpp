@@ -68,8 +68,10 @@ void derive_knobs_total(int n, uint32_t W, int k, double imbalance, int seed, in
     kn.ref_subrounds = 4;
     kn.ref_classes = 16;
     kn.bal_iters = 64;
-    kn.ip_reps = fast ? 1 : 3;
-    kn.ip_tries = 4;                     // bipartition_tries = 4 (fast/eco)
+    kn.ip_reps = fast ? 1 : 2;
+    kn.ip_tries = fast ? 8 : 16;         // bipartition_tries = 4 (fast/eco) at every level of
+                                         // the reference's multilevel bisection; more growing
+                                         // tries on one level here
     kn.ip_fm_passes = fast ? 3 : 6;
     kn.ip_fm_stall = 100;
     kn.max_levels = 48;

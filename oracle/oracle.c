@@ -92,8 +92,8 @@ void or_derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, 
     o->ref_subrounds = 4;
     o->ref_classes = 16;
     o->bal_iters = 64;
-    o->ip_reps = fast ? 1 : 3;
-    o->ip_tries = 4;
+    o->ip_reps = fast ? 1 : 2;
+    o->ip_tries = fast ? 8 : 16;
     o->ip_fm_passes = fast ? 3 : 6;
     o->ip_fm_stall = 100;
     o->max_levels = 48;

@@ -1,0 +1,94 @@
+"""The CPU oracle against committed reference outputs (tests/golden/
+reference_outputs.npz, produced by tests/golden/make_golden.py from the
+reference KaHIP library built from its sources).  Needs no reference sources
+and no GPU."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import csr_from_edges
+
+from oracle import oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_outputs.npz")
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(GOLDEN)
+
+
+@pytest.fixture(scope="module")
+def gset():
+    import sys
+    sys.path.insert(0, os.path.dirname(GOLDEN))
+    from make_golden import fingerprint, graph_set
+    gs = graph_set()
+    return gs, fingerprint
+
+
+def test_generators_reproduce_fixture_inputs(gold, gset):
+    gs, fp = gset
+    for name, g in gs.items():
+        assert np.array_equal(fp(g), gold[f"{name}/fingerprint"]), f"generator drift for {name}"
+
+
+def test_balance_configuration(gold):
+    for (n, k, imb, mode), out in zip(gold["balance_cases"], gold["balance_out"]):
+        n, k, mode = int(n), int(k), int(mode)
+        kn = O.knobs(dict(n=n, vwgt=np.ones(n, np.int32)), k, float(imb), 0, mode)
+        assert (kn.upper_bound, kn.num_stop, kn.max_vertex_weight) == tuple(int(x) for x in out)
+
+
+def test_rating_cut_balance_contraction(gold, gset):
+    gs, _ = gset
+    for name, g in gs.items():
+        assert np.array_equal(O.rating(g).view(np.uint64), gold[f"{name}/rating"].view(np.uint64))
+        for p, k, c, b in zip(gold[f"{name}/cut_parts"], (2, 5, 64), gold[f"{name}/cut"], gold[f"{name}/balance"]):
+            cut2 = 2 * O.edge_cut(g, p)
+            ref_int = int((((cut2 + (1 << 31)) % (1 << 32)) - (1 << 31)) / 2)  # reference sums in 32-bit int
+            assert ref_int == c
+            assert O.balance_ratio(g, p, k) == b
+        c, cmap = O.contract(g, gold[f"{name}/contract_label"])
+        assert np.array_equal(cmap, gold[f"{name}/contract_cmap"])
+        for key in ("xadj", "adjncy", "adjwgt", "vwgt"):
+            assert np.array_equal(c[key], gold[f"{name}/contract_{key}"]), key
+
+
+def test_sequential_lp_rules(gold, gset):
+    gs, _ = gset
+    name = "tiefree_rgg2d_1500"
+    g = gs[name]
+    order = gold[f"{name}/order"]
+    for bound, rounds in [(40, 1), (200, 10)]:
+        assert np.array_equal(O.lp_cluster_seq(g, bound, rounds, order), gold[f"{name}/lpc_{bound}_{rounds}"])
+    out = O.lp_refine_seq(g, 8, int(gold[f"{name}/lpr_bound"][0]), 25, order, gold[f"{name}/lpr_part0"])
+    assert np.array_equal(out, gold[f"{name}/lpr_out"])
+
+
+def test_interface_example_cut(gold):
+    assert int(gold["interface_test/eco_k2_cut"][0]) == 2
+    g = csr_from_edges(5, [(0, 1), (0, 4), (1, 2), (1, 4), (2, 3), (3, 4)])
+    cut, part, _ = O.kaffpa(g, 2, 0.03, 0, 1)
+    assert cut == O.edge_cut(g, part) and cut >= 2
+
+
+def test_oracle_quality_vs_reference(gold, gset, graphs):
+    """Quality bar, not parity.  On a 2^18-node RGG the deterministic schedule
+    must cut no more than reference kaffpa fast.  On a 2000-node graph (a
+    single coarsening level, LP instead of FM refinement) it is allowed to
+    trail by up to 60%."""
+    big = graphs.rgg2d(1 << 18, seed=0)
+    _, fp = gset
+    assert np.array_equal(fp(big), gold["rgg2d_18/fingerprint"])
+    for k in (8, 64):
+        cut, part, st = O.kaffpa(big, k, 0.03, 0, 0)
+        assert st.balanced
+        assert cut <= int(gold[f"rgg2d_18/kaffpa_cut_fast_k{k}"][0])
+    gs, _ = gset
+    g = gs["rgg2d_2000"]
+    for mode, key in ((0, "kaffpa_cut_fast_k8"), (1, "kaffpa_cut_eco_k8")):
+        cut, part, st = O.kaffpa(g, 8, 0.03, 0, mode)
+        assert st.balanced
+        assert cut <= 1.6 * int(gold[f"rgg2d_2000/{key}"][0])
