@@ -47,7 +47,6 @@ struct SweepArgs {
     uint32_t S, s;                      // sub-rounds, this sub-round
     uint64_t ks_sub, ks_tie, ks_prio;
     int P;                              // admission classes
-    int table;                          // per-group table capacity (power of 2)
     // outputs
     int* pt; int* pc;                   // per vertex: proposed target / class (-1: none)
     uint32_t* inc;                      // CLUSTER: incoming weight per target
@@ -158,99 +157,185 @@ __device__ __forceinline__ bool member(const SweepArgs& a, int v) {
     return hash32(a.ks_sub, (uint32_t)v) % a.S == a.s;
 }
 
-// Group of G lanes aggregates and decides vertex v.
-template <int G, int MODE>
-__device__ void process_vertex(const SweepArgs& a, int v, int gl, unsigned gmask, uint32_t* tk,
-                               uint32_t* tv, unsigned long long& wv, unsigned long long& we) {
-    const int beg = a.xadj[v], end = a.xadj[v + 1], deg = end - beg;
-    const uint32_t own = (uint32_t)a.lab[v];
-    const uint32_t cv = (uint32_t)a.vwgt[v];
-    if (deg > a.table / 2) {
-        if (gl == 0) a.heavy[atomicAdd(a.hcount, 1u)] = v;
-        return;
-    }
-    if (gl == 0) { wv += 1; we += (unsigned long long)deg; }
-    uint32_t conn_own = 0;
-    uint64_t key = 0;
-    uint32_t id = kEmpty;
-    if (deg <= G) {
-        uint32_t l = kEmpty, w = 0;
-        if (gl < deg) {
-            int u = a.adjncy[beg + gl];
-            w = (uint32_t)a.adjwgt[beg + gl];
-            l = (uint32_t)a.lab[u];
-        }
-        unsigned peers = __match_any_sync(gmask, l);
-        uint32_t sum = __reduce_add_sync(peers, w);
-        bool leader = gl < deg && (peers & lanemask_lt()) == 0;
-        unsigned ob = __ballot_sync(gmask, leader && l == own);
-        if (ob) conn_own = __shfl_sync(gmask, sum, __ffs(ob) - 1);
-        if (leader && l != own && cand_ok<MODE>(a, l, sum, cv)) {
-            key = cand_key(sum, a.ks_tie, l);
-            id = l;
-        }
-    } else {
-        const int cap = a.table;
-        for (int c = beg; c < end; c += G) {
-            int e = c + gl;
-            uint32_t l = kEmpty, w = 0;
-            if (e < end) {
-                w = (uint32_t)a.adjwgt[e];
-                l = (uint32_t)a.lab[a.adjncy[e]];
-            }
-            unsigned peers = __match_any_sync(gmask, l);
-            uint32_t sum = __reduce_add_sync(peers, w);
-            if (e < end && (peers & lanemask_lt()) == 0) table_insert(tk, tv, cap, l, sum, a.err);
-        }
-        __syncwarp(gmask);
-        uint32_t co = 0;
-        for (int s = gl; s < cap; s += G) {
-            uint32_t l = tk[s];
-            if (l == kEmpty) continue;
-            uint32_t c = tv[s];
-            tk[s] = kEmpty;
-            tv[s] = 0;
-            if (l == own) co = c;
-            else if (cand_ok<MODE>(a, l, c, cv)) better(key, id, cand_key(c, a.ks_tie, l), l);
-        }
-        conn_own = __reduce_or_sync(gmask, co);
-        __syncwarp(gmask);
-    }
-    group_argmax<G>(key, id, gmask);
-    if (gl == 0) decide_emit<MODE>(a, v, own, cv, conn_own, key, id);
+// ------------------------------------------------ chunk-cooperative sweep
+//
+// A warp owns 32 consecutive vertex ids.  Members of the sub-round with
+// degree <= kWin are laid out back to back (warp prefix sum of degrees) and
+// processed in windows of at most kWin edges: every lane takes one edge slot
+// per 32-edge batch, all adjacency loads of a window are issued before the
+// label gathers, (member, label) pairs are merged with a 64-bit match_any and
+// summed into a per-warp shared hash table; each member's best candidate is
+// then found with shared-memory atomicMax / atomicMin.  Members of degree
+// > kWin go to the block-per-vertex kernel.
+
+constexpr int kWin = 128;                 // edges per window (<= 4 batches)
+constexpr int kBatches = kWin / 32;
+constexpr int kTab = 2 * kWin;            // table slots per warp (load <= 1/2)
+constexpr unsigned long long kEmpty64 = ~0ull;
+constexpr int kWarpsPerBlock = kThreads / 32;
+
+struct WarpTable {
+    unsigned long long key[kTab];  // (member lane << 32) | label
+    uint32_t val[kTab];
+    uint16_t used[kWin];           // slots filled in the current window
+    unsigned long long bkey[32];   // per member: best candidate key
+    uint32_t bid[32];              // per member: best candidate label
+    uint32_t cown[32];             // per member: connection to its own label
+    uint32_t own[32];
+    uint32_t cv[32];
+    uint32_t nused;
+};
+
+__device__ __forceinline__ uint32_t slot64(unsigned long long k) {
+    return (uint32_t)((k * 0x9E3779B97F4A7C15ull) >> (64 - 8)) & (kTab - 1);  // kTab == 256
 }
 
-template <int G, int MODE>
+template <int MODE>
 __global__ void __launch_bounds__(kThreads) sweep_kernel(SweepArgs a) {
-    extern __shared__ uint32_t smem[];
+    static_assert(kTab == 256, "slot64 assumes 256 slots");
+    __shared__ WarpTable tabs[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
-    const int gid = lane / G, gl = lane % G;
-    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (gid * G));
-    const int groups_per_block = kThreads / G;
-    const int gblock = (threadIdx.x / 32) * (32 / G) + gid;
-    uint32_t* tk = smem + (size_t)gblock * a.table;
-    uint32_t* tv = smem + (size_t)groups_per_block * a.table + (size_t)gblock * a.table;
-    for (int s = gl; s < a.table; s += G) { tk[s] = kEmpty; tv[s] = 0; }
+    WarpTable& T = tabs[threadIdx.x >> 5];
+    for (int i = lane; i < kTab; i += 32) { T.key[i] = kEmpty64; T.val[i] = 0; }
+    if (lane == 0) T.nused = 0;
     __syncwarp();
     unsigned long long wv = 0, we = 0;
     const long long nchunks = ((long long)a.n + 31) / 32;
     const long long warp = ((long long)blockIdx.x * kThreads + threadIdx.x) / 32;
     const long long nwarps = (long long)gridDim.x * kThreads / 32;
     for (long long chunk = warp; chunk < nchunks; chunk += nwarps) {
-        int v = (int)(chunk * 32 + lane);
-        bool mem = v < a.n && member<MODE>(a, v);
-        if (v < a.n && !mem) a.pt[v] = -1;
-        unsigned mask = __ballot_sync(0xffffffffu, mem);
-        while (mask) {
-            int pick = -1;
+        const int v = (int)(chunk * 32 + lane);
+        const bool valid_v = v < a.n;
+        const bool mem = valid_v && member<MODE>(a, v);
+        int beg = 0, deg = 0;
+        bool heavy = false;
+        if (mem) {
+            beg = a.xadj[v];
+            deg = a.xadj[v + 1] - beg;
+            if (deg > kWin) {  // high degree: block-per-vertex kernel decides it
+                a.heavy[atomicAdd(a.hcount, 1u)] = v;
+                deg = 0;
+                heavy = true;
+            } else {
+                wv += 1;
+                we += (unsigned long long)deg;
+            }
+            T.own[lane] = (uint32_t)a.lab[v];
+            T.cv[lane] = (uint32_t)a.vwgt[v];
+        } else if (valid_v) {
+            a.pt[v] = -1;
+        }
+        const bool light = mem && !heavy;
+        // inclusive prefix sum of degrees over the chunk
+        int incl = deg;
 #pragma unroll
-            for (int i = 0; i < 32 / G; ++i) {
-                if (mask) {
-                    if (i == gid) pick = __ffs(mask) - 1;
-                    mask &= mask - 1;
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int off = incl - deg;
+        const unsigned lightmask = __ballot_sync(0xffffffffu, light);
+        if (!lightmask) continue;
+        int wstart = __ffs(lightmask) - 1;
+        while (wstart < 32) {
+            // window: lanes [wstart, wend) whose edges fit into kWin slots
+            const int base = __shfl_sync(0xffffffffu, off, wstart);
+            const bool inwin = lane >= wstart && incl - base <= kWin;
+            const unsigned wmask = __ballot_sync(0xffffffffu, inwin);
+            const int wend = 32 - __clz(wmask);
+            const int E = __shfl_sync(0xffffffffu, incl, wend - 1) - base;
+            const bool wmember = light && lane >= wstart && lane < wend;
+            if (wmember) {
+                T.bkey[lane] = 0;
+                T.bid[lane] = kEmpty;
+                T.cown[lane] = 0;
+            }
+            // gather the window's edges: all adjacency loads, then all labels
+            int own_lane[kBatches];
+            int tgt[kBatches];
+            uint32_t wgt[kBatches];
+#pragma unroll
+            for (int b = 0; b < kBatches; ++b) {
+                const int q = b * 32 + lane;
+                // largest window lane o with off[o] - base <= q (binary lifting)
+                int o = wstart;
+#pragma unroll
+                for (int step = 16; step >= 1; step >>= 1) {
+                    const int c = o + step;
+                    const int oc = __shfl_sync(0xffffffffu, off, c < 32 ? c : 31) - base;
+                    if (c < wend && oc <= q) o = c;
+                }
+                const int ob = __shfl_sync(0xffffffffu, beg, o);
+                const int oo = __shfl_sync(0xffffffffu, off, o) - base;
+                own_lane[b] = o;
+                tgt[b] = -1;
+                wgt[b] = 0;
+                if (q < E) {
+                    const int e = ob + (q - oo);
+                    tgt[b] = a.adjncy[e];
+                    wgt[b] = (uint32_t)a.adjwgt[e];
                 }
             }
-            if (pick >= 0) process_vertex<G, MODE>(a, (int)(chunk * 32 + pick), gl, gmask, tk, tv, wv, we);
+#pragma unroll
+            for (int b = 0; b < kBatches; ++b)
+                if (tgt[b] >= 0) tgt[b] = a.lab[tgt[b]];
+#pragma unroll
+            for (int b = 0; b < kBatches; ++b) {
+                if (b * 32 >= E) break;
+                const bool ok = tgt[b] >= 0;
+                const unsigned long long key =
+                    ok ? (((unsigned long long)own_lane[b] << 32) | (uint32_t)tgt[b]) : kEmpty64;
+                const unsigned peers = __match_any_sync(0xffffffffu, key);
+                const uint32_t sum = __reduce_add_sync(peers, wgt[b]);
+                if (ok && (peers & lanemask_lt()) == 0) {
+                    uint32_t sl = slot64(key);
+                    for (int probe = 0; probe < kTab; ++probe) {
+                        const unsigned long long prev = atomicCAS(&T.key[sl], kEmpty64, key);
+                        if (prev == kEmpty64) {
+                            T.used[atomicAdd(&T.nused, 1u)] = (uint16_t)sl;
+                            atomicAdd(&T.val[sl], sum);
+                            break;
+                        }
+                        if (prev == key) {
+                            atomicAdd(&T.val[sl], sum);
+                            break;
+                        }
+                        sl = (sl + 1) & (kTab - 1);
+                        if (probe == kTab - 1) atomicOr(a.err, 1);
+                    }
+                }
+                __syncwarp();
+            }
+            // per member: connection to its own label and the best candidate
+            const uint32_t nused = T.nused;
+            for (uint32_t i = lane; i < nused; i += 32) {
+                const uint32_t sl = T.used[i];
+                const unsigned long long k = T.key[sl];
+                const int o = (int)(k >> 32);
+                const uint32_t l = (uint32_t)k;
+                const uint32_t c = T.val[sl];
+                if (l == T.own[o]) T.cown[o] = c;
+                else if (cand_ok<MODE>(a, l, c, T.cv[o])) atomicMax(&T.bkey[o], cand_key(c, a.ks_tie, l));
+            }
+            __syncwarp();
+            for (uint32_t i = lane; i < nused; i += 32) {
+                const uint32_t sl = T.used[i];
+                const unsigned long long k = T.key[sl];
+                const int o = (int)(k >> 32);
+                const uint32_t l = (uint32_t)k;
+                const uint32_t c = T.val[sl];
+                if (l != T.own[o] && cand_ok<MODE>(a, l, c, T.cv[o]) && cand_key(c, a.ks_tie, l) == T.bkey[o])
+                    atomicMin(&T.bid[o], l);
+                T.key[sl] = kEmpty64;
+                T.val[sl] = 0;
+            }
+            __syncwarp();
+            if (lane == 0) T.nused = 0;
+            if (wmember) decide_emit<MODE>(a, v, T.own[lane], T.cv[lane], T.cown[lane], T.bkey[lane], T.bid[lane]);
+            __syncwarp();
+            // next window starts at the first light lane at or after wend
+            const unsigned rest = lightmask & (wend < 32 ? (~0u << wend) : 0u);
+            wstart = rest ? __ffs(rest) - 1 : 32;
         }
     }
     // one atomic per warp for the work counters
@@ -465,14 +550,7 @@ __global__ void block_scan_kernel(const uint32_t* bw, int k, uint32_t bound, int
 
 // ------------------------------------------------------------- host helpers
 
-int pick_group(const DevGraph& g) {
-    double avg = g.n ? (double)g.m / g.n : 0;
-    return avg <= 8 ? 8 : (avg <= 16 ? 16 : 32);
-}
-
-int table_for(int G) { return G == 32 ? 256 : (G == 16 ? 128 : 64); }
-
-int sweep_blocks() { return kNumSMs * 8; }
+int sweep_blocks() { return kNumSMs * 5; }  // 48 registers, 32 KB shared: 5 blocks per SM
 
 struct SweepBuffers {
     int *pt, *pc;
@@ -494,12 +572,10 @@ SweepBuffers make_buffers(Ctx& ctx, const DevGraph& g) {
     b.counters = A.alloc<unsigned>(4);
     b.work = ctx.work;
     b.err = ctx.dscalars + 60;
-    int G = pick_group(g);
-    int T = table_for(G);
     b.gcap = 0;
     b.hblocks = 0;
     b.gtk = b.gtv = nullptr;
-    if (g.maxdeg > T / 2) {
+    if (g.maxdeg > kWin) {
         int cap = 1;
         while (cap < 2 * g.maxdeg) cap <<= 1;
         b.gcap = cap;
@@ -517,14 +593,10 @@ SweepBuffers make_buffers(Ctx& ctx, const DevGraph& g) {
 
 template <int MODE>
 void launch_sweep(Ctx& ctx, const DevGraph& g, SweepArgs a, const SweepBuffers& b) {
-    int G = pick_group(g);
-    a.table = table_for(G);
-    size_t smem = (size_t)2 * (kThreads / G) * a.table * sizeof(uint32_t);
-    int blocks = sweep_blocks();
+    const long long chunks = ((long long)g.n + 31) / 32;
+    int blocks = (int)std::max<long long>(1, std::min<long long>(div_up(chunks, kWarpsPerBlock), sweep_blocks()));
     KB_CUDA(cudaMemsetAsync(b.counters, 0, 2 * sizeof(unsigned), ctx.stream));
-    if (G == 8) sweep_kernel<8, MODE><<<blocks, kThreads, smem, ctx.stream>>>(a);
-    else if (G == 16) sweep_kernel<16, MODE><<<blocks, kThreads, smem, ctx.stream>>>(a);
-    else sweep_kernel<32, MODE><<<blocks, kThreads, smem, ctx.stream>>>(a);
+    sweep_kernel<MODE><<<blocks, kThreads, 0, ctx.stream>>>(a);
     KB_LAUNCH();
     if (b.gcap > 0) {
         heavy_kernel<MODE><<<b.hblocks, kThreads, 0, ctx.stream>>>(a, b.gtk, b.gtv, b.gcap);
