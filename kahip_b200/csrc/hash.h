@@ -42,8 +42,21 @@ KB_HD uint64_t stream_key(int seed, int tag, int level, int round) {
     return mix64(s ^ (uint64_t)(uint32_t)round);
 }
 
+// Per-item hash: a murmur3-style 32-bit finaliser (MurmurHash3 fmix32,
+// Appleby) keyed by both halves of the stream key.
 KB_HD uint32_t hash32(uint64_t ks, uint32_t x) {
-    return (uint32_t)(mix64(ks ^ (uint64_t)x) >> 32);
+    uint32_t h = (x * 0x9E3779B1u) ^ (uint32_t)ks;
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    h *= (uint32_t)(ks >> 32) | 1u;
+    h ^= h >> 16;
+    return h;
+}
+
+// Maps a uniform 32-bit hash onto [0, n) (multiply-shift range reduction).
+KB_HD uint32_t hash_range(uint32_t h, uint32_t n) {
+    return (uint32_t)(((uint64_t)h * n) >> 32);
 }
 
 }  // namespace kb

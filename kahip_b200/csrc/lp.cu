@@ -54,6 +54,7 @@ struct SweepArgs {
     uint32_t* H;                        // REFINE/BALANCE: weight per (target, class)
     int* minvP;                         // smallest proposer per (target, class)
     int* heavy; unsigned* hcount;       // deferred high-degree vertices
+    int* flist; unsigned* fcount;       // vertices with more distinct labels than register slots
     unsigned long long* work;           // [0] vertices, [1] edges
     int* err;                           // set when an invariant breaks
     // BALANCE
@@ -128,7 +129,7 @@ __device__ void decide_emit(const SweepArgs& a, int v, uint32_t own, uint32_t cv
     } else if (MODE == REFINE) {
         uint32_t base = a.lw[own] <= a.bound ? conn_own : 0u;
         if (id == kEmpty || (uint32_t)(key >> 32) <= base) { a.pt[v] = -1; return; }
-        int cls = (int)(hash32(a.ks_prio, (uint32_t)v) % (uint32_t)a.P);
+        int cls = (int)hash_range(hash32(a.ks_prio, (uint32_t)v), (uint32_t)a.P);
         a.pt[v] = (int)id;
         a.pc[v] = cls;
         size_t h = (size_t)id * a.P + cls;
@@ -143,7 +144,7 @@ __device__ void decide_emit(const SweepArgs& a, int v, uint32_t own, uint32_t cv
             tc = 0;
         }
         long long loss = (long long)conn_own - (long long)tc;
-        int cls = loss_bucket(loss) * 8 + (int)(hash32(a.ks_sub, (uint32_t)v) % 8u);
+        int cls = loss_bucket(loss) * 8 + (int)hash_range(hash32(a.ks_sub, (uint32_t)v), 8u);
         a.pt[v] = (int)t;
         a.pc[v] = cls;
         atomicAdd(&a.HS[(size_t)own * kBalClasses + cls], cv);
@@ -154,7 +155,7 @@ template <int MODE>
 __device__ __forceinline__ bool member(const SweepArgs& a, int v) {
     if (MODE == BALANCE) return a.lw[a.lab[v]] > a.bound;
     if (MODE == REFINE && !a.active[v]) return false;
-    return hash32(a.ks_sub, (uint32_t)v) % a.S == a.s;
+    return hash_range(hash32(a.ks_sub, (uint32_t)v), a.S) == a.s;
 }
 
 // ------------------------------------------------ chunk-cooperative sweep
@@ -190,8 +191,10 @@ __device__ __forceinline__ uint32_t slot64(unsigned long long k) {
     return (uint32_t)((k * 0x9E3779B97F4A7C15ull) >> (64 - 8)) & (kTab - 1);  // kTab == 256
 }
 
+// Processes the vertices of a list (the lane kernel's overflow list): every
+// listed vertex is a member of the current sub-round.
 template <int MODE>
-__global__ void __launch_bounds__(kThreads) sweep_kernel(SweepArgs a) {
+__global__ void __launch_bounds__(kThreads) chunk_kernel(SweepArgs a) {
     static_assert(kTab == 256, "slot64 assumes 256 slots");
     __shared__ WarpTable tabs[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
@@ -200,13 +203,14 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(SweepArgs a) {
     if (lane == 0) T.nused = 0;
     __syncwarp();
     unsigned long long wv = 0, we = 0;
-    const long long nchunks = ((long long)a.n + 31) / 32;
+    const unsigned count = *a.fcount;
+    const long long nchunks = ((long long)count + 31) / 32;
     const long long warp = ((long long)blockIdx.x * kThreads + threadIdx.x) / 32;
     const long long nwarps = (long long)gridDim.x * kThreads / 32;
     for (long long chunk = warp; chunk < nchunks; chunk += nwarps) {
-        const int v = (int)(chunk * 32 + lane);
-        const bool valid_v = v < a.n;
-        const bool mem = valid_v && member<MODE>(a, v);
+        const long long li = chunk * 32 + lane;
+        const bool mem = li < (long long)count;
+        const int v = mem ? a.flist[li] : 0;
         int beg = 0, deg = 0;
         bool heavy = false;
         if (mem) {
@@ -222,8 +226,6 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(SweepArgs a) {
             }
             T.own[lane] = (uint32_t)a.lab[v];
             T.cv[lane] = (uint32_t)a.vwgt[v];
-        } else if (valid_v) {
-            a.pt[v] = -1;
         }
         const bool light = mem && !heavy;
         // inclusive prefix sum of degrees over the chunk
@@ -339,6 +341,148 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(SweepArgs a) {
         }
     }
     // one atomic per warp for the work counters
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        wv += __shfl_xor_sync(0xffffffffu, wv, o);
+        we += __shfl_xor_sync(0xffffffffu, we, o);
+    }
+    if (lane == 0 && (wv | we)) {
+        atomicAdd(&a.work[0], wv);
+        atomicAdd(&a.work[1], we);
+    }
+}
+
+// ------------------------------------------------------ lane-per-vertex sweep
+//
+// The main sweep: a warp takes 128 consecutive vertex ids, compacts the
+// members of the sub-round onto its lanes, and every lane aggregates its own
+// vertex's neighbourhood in kSlots register slots (connection per label; the
+// own label is kept apart), four edges at a time with all loads issued
+// before use.  A vertex whose neighbours carry more distinct labels than
+// slots goes to the overflow list (chunk_kernel); one of degree > kWin goes
+// to the high-degree list (heavy_kernel).
+
+constexpr int kSlots = 8;
+constexpr int kSpan = 4;  // chunks of 32 ids per warp task
+
+// r-th set bit (0-based) of mask
+__device__ __forceinline__ int nth_set_bit(unsigned mask, int r) {
+    int lo = 0, hi = 31;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        const unsigned below = mid == 31 ? mask : (mask & ((2u << mid) - 1u));
+        if (__popc(below) > r) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+
+// 0: decided, 1: too many distinct labels, 2: degree above kWin
+template <int MODE>
+__device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, unsigned long long& we) {
+    const int beg = a.xadj[v], end = a.xadj[v + 1];
+    if (end - beg > kWin) return 2;
+    const uint32_t own = (uint32_t)a.lab[v];
+    const uint32_t cv = (uint32_t)a.vwgt[v];
+    uint32_t sl[kSlots], sc[kSlots];
+#pragma unroll
+    for (int i = 0; i < kSlots; ++i) { sl[i] = kEmpty; sc[i] = 0; }
+    uint32_t cown = 0;
+    bool overflow = false;
+    for (int e = beg; e < end && !overflow; e += 4) {
+        int u[4];
+        uint32_t w[4], l[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            u[t] = -1;
+            w[t] = 0;
+            if (e + t < end) {
+                u[t] = a.adjncy[e + t];
+                w[t] = (uint32_t)a.adjwgt[e + t];
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) l[t] = u[t] >= 0 ? (uint32_t)a.lab[u[t]] : kEmpty;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            if (u[t] < 0) continue;
+            if (l[t] == own) { cown += w[t]; continue; }
+            bool hit = false;
+#pragma unroll
+            for (int i = 0; i < kSlots; ++i)
+                if (sl[i] == l[t]) { sc[i] += w[t]; hit = true; }
+            if (!hit) {
+#pragma unroll
+                for (int i = 0; i < kSlots; ++i)
+                    if (!hit && sl[i] == kEmpty) { sl[i] = l[t]; sc[i] = w[t]; hit = true; }
+                overflow |= !hit;
+            }
+        }
+    }
+    if (overflow) return 1;
+    wv += 1;
+    we += (unsigned long long)(end - beg);
+    uint64_t key = 0;
+    uint32_t id = kEmpty;
+#pragma unroll
+    for (int i = 0; i < kSlots; ++i)
+        if (sl[i] != kEmpty && cand_ok<MODE>(a, sl[i], sc[i], cv)) better(key, id, cand_key(sc[i], a.ks_tie, sl[i]), sl[i]);
+    decide_emit<MODE>(a, v, own, cv, cown, key, id);
+    return 0;
+}
+
+__device__ __forceinline__ void append_aggregated(bool pred, int v, int* list, unsigned* count) {
+    const unsigned m = __ballot_sync(0xffffffffu, pred);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(count, (unsigned)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (pred) list[base + __popc(m & lanemask_lt())] = v;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kThreads) lane_kernel(SweepArgs a) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long wv = 0, we = 0;
+    const long long span = 32LL * kSpan;
+    const long long ntasks = ((long long)a.n + span - 1) / span;
+    const long long warp = ((long long)blockIdx.x * kThreads + threadIdx.x) / 32;
+    const long long nwarps = (long long)gridDim.x * kThreads / 32;
+    for (long long task = warp; task < ntasks; task += nwarps) {
+        const long long base = task * span;
+        unsigned m[kSpan];
+        int total = 0;
+#pragma unroll
+        for (int c = 0; c < kSpan; ++c) {
+            const long long vv = base + c * 32 + lane;
+            const bool valid = vv < a.n;
+            const bool mem = valid && member<MODE>(a, (int)vv);
+            if (valid && !mem) a.pt[vv] = -1;
+            m[c] = __ballot_sync(0xffffffffu, mem);
+            total += __popc(m[c]);
+        }
+        for (int p = 0; p < total; p += 32) {
+            const int r = p + lane;
+            int v = -1;
+            if (r < total) {
+                int rr = r, c = 0;
+#pragma unroll
+                for (int cc = 0; cc < kSpan - 1; ++cc)
+                    if (c == cc && rr >= __popc(m[cc])) { rr -= __popc(m[cc]); c = cc + 1; }
+                unsigned mc = m[0];
+#pragma unroll
+                for (int cc = 1; cc < kSpan; ++cc)
+                    if (c == cc) mc = m[cc];
+                v = (int)(base + c * 32 + nth_set_bit(mc, rr));
+            }
+            int status = 0;
+            if (v >= 0) status = lane_vertex<MODE>(a, v, wv, we);
+            append_aggregated(status == 1, v, a.flist, a.fcount);
+            append_aggregated(status == 2, v, a.heavy, a.hcount);
+        }
+    }
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) {
         wv += __shfl_xor_sync(0xffffffffu, wv, o);
@@ -511,7 +655,7 @@ __global__ void balance_release(int n, const int* pt, int* pc, const int* part, 
         int t = pt[v];
         if (t < 0) continue;
         if (pc[v] >= thr[part[v]]) { pc[v] = -1; continue; }
-        int c = (int)(hash32(ks_prio, (uint32_t)v) % (uint32_t)P);
+        int c = (int)hash_range(hash32(ks_prio, (uint32_t)v), (uint32_t)P);
         pc[v] = c;
         size_t h = (size_t)t * P + c;
         atomicAdd(&H[h], (uint32_t)vwgt[v]);
@@ -554,8 +698,9 @@ int sweep_blocks() { return kNumSMs * 5; }  // 48 registers, 32 KB shared: 5 blo
 
 struct SweepBuffers {
     int *pt, *pc;
-    unsigned* counters;  // [0] unused, [1] hcount, [2] moved
+    unsigned* counters;  // [0] fcount, [1] hcount, [2] moved
     int* heavy;
+    int* flist;
     uint32_t *gtk, *gtv;
     int gcap, hblocks;
     unsigned long long* work;
@@ -569,6 +714,7 @@ SweepBuffers make_buffers(Ctx& ctx, const DevGraph& g) {
     b.pt = A.alloc<int>(n);
     b.pc = A.alloc<int>(n);
     b.heavy = A.alloc<int>(n);
+    b.flist = A.alloc<int>(n);
     b.counters = A.alloc<unsigned>(4);
     b.work = ctx.work;
     b.err = ctx.dscalars + 60;
@@ -593,10 +739,13 @@ SweepBuffers make_buffers(Ctx& ctx, const DevGraph& g) {
 
 template <int MODE>
 void launch_sweep(Ctx& ctx, const DevGraph& g, SweepArgs a, const SweepBuffers& b) {
-    const long long chunks = ((long long)g.n + 31) / 32;
-    int blocks = (int)std::max<long long>(1, std::min<long long>(div_up(chunks, kWarpsPerBlock), sweep_blocks()));
+    const long long tasks = ((long long)g.n + 32 * kSpan - 1) / (32 * kSpan);
+    const int lblocks = (int)std::max<long long>(1, std::min<long long>(div_up(tasks, kWarpsPerBlock), kNumSMs * 8LL));
     KB_CUDA(cudaMemsetAsync(b.counters, 0, 2 * sizeof(unsigned), ctx.stream));
-    sweep_kernel<MODE><<<blocks, kThreads, 0, ctx.stream>>>(a);
+    lane_kernel<MODE><<<lblocks, kThreads, 0, ctx.stream>>>(a);
+    KB_LAUNCH();
+    const int cblocks = (int)std::max<long long>(1, std::min<long long>(div_up(g.n, 32 * kWarpsPerBlock), sweep_blocks()));
+    chunk_kernel<MODE><<<cblocks, kThreads, 0, ctx.stream>>>(a);
     KB_LAUNCH();
     if (b.gcap > 0) {
         heavy_kernel<MODE><<<b.hblocks, kThreads, 0, ctx.stream>>>(a, b.gtk, b.gtv, b.gcap);
@@ -615,6 +764,8 @@ SweepArgs base_args(const DevGraph& g, const SweepBuffers& b) {
     a.pc = b.pc;
     a.hcount = b.counters + 1;
     a.heavy = b.heavy;
+    a.fcount = b.counters;
+    a.flist = b.flist;
     a.work = b.work;
     a.err = b.err;
     return a;

