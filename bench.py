@@ -273,7 +273,7 @@ def main():
     time.sleep(0.3)
     fam = {}
     cuts = []
-    sweep_v = sweep_e = 0
+    sweep_v = sweep_e = sweep_o = 0
     ms_phase = {"coarsen": 0.0, "initial": 0.0, "uncoarsen": 0.0}
     levels = None
     if world > 1:
@@ -295,6 +295,7 @@ def main():
             a["launches"] += f["launches"]
         sweep_v += st.sweep_vertices
         sweep_e += st.sweep_edges
+        sweep_o += st.sweep_overflow_vertices
         ms_phase["coarsen"] += st.ms_coarsen
         ms_phase["initial"] += st.ms_initial
         ms_phase["uncoarsen"] += st.ms_uncoarsen
@@ -379,7 +380,8 @@ def main():
         "phases_ms_per_step": {k: v / args.steps for k, v in ms_phase.items()},
         "kernel_families_ms_per_step": {k: v["ms"] / args.steps for k, v in sorted(fam.items(), key=lambda x: -x[1]["ms"])},
         "levels": levels,
-        "sweep_work_per_step": {"vertices": sweep_v / args.steps, "edges": sweep_e / args.steps},
+        "sweep_work_per_step": {"vertices": sweep_v / args.steps, "edges": sweep_e / args.steps,
+                                "overflow_vertices": sweep_o / args.steps},
     }
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

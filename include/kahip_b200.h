@@ -80,6 +80,7 @@ typedef struct kb200_stats {
     long long family_launches[16];
     /* LP sweep work actually performed */
     long long sweep_vertices, sweep_edges;
+    long long sweep_overflow_vertices;   /* of which needed the shared-table path */
     size_t device_bytes_peak;
 } kb200_stats;
 

@@ -168,10 +168,11 @@ void fill_stats_families(Ctx& ctx, kb200_stats* st) {
         st->family_bytes[i] = ctx.phases[i].bytes;
         st->family_launches[i] = ctx.phases[i].launches;
     }
-    unsigned long long w[2] = {0, 0};
+    unsigned long long w[3] = {0, 0, 0};
     KB_CUDA(cudaMemcpy(w, ctx.work, sizeof(w), cudaMemcpyDeviceToHost));
     st->sweep_vertices = (long long)w[0];
     st->sweep_edges = (long long)w[1];
+    st->sweep_overflow_vertices = (long long)w[2];
     st->device_bytes_peak = ctx.hier.peak() + ctx.scratch.peak();
 }
 

@@ -55,6 +55,8 @@ struct SweepArgs {
     int* minvP;                         // smallest proposer per (target, class)
     int* heavy; unsigned* hcount;       // deferred high-degree vertices
     int* flist; unsigned* fcount;       // vertices with more distinct labels than register slots
+    int singletons;                     // every label is its own vertex id and rows have
+                                        // strictly increasing targets (clustering round 0)
     unsigned long long* work;           // [0] vertices, [1] edges
     int* err;                           // set when an invariant breaks
     // BALANCE
@@ -349,6 +351,7 @@ __global__ void __launch_bounds__(kThreads) chunk_kernel(SweepArgs a) {
     if (lane == 0 && (wv | we)) {
         atomicAdd(&a.work[0], wv);
         atomicAdd(&a.work[1], we);
+        atomicAdd(&a.work[2], wv);  // vertices that needed the overflow path
     }
 }
 
@@ -388,6 +391,36 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
 #pragma unroll
     for (int i = 0; i < kSlots; ++i) { sl[i] = kEmpty; sc[i] = 0; }
     uint32_t cown = 0;
+    if (MODE == CLUSTER && a.singletons) {
+        // label[u] == u and no target repeats: the connection to cluster u is
+        // exactly w(v,u), so the best candidate is a running maximum
+        uint64_t key = 0;
+        uint32_t id = kEmpty;
+        for (int e = beg; e < end; e += 4) {
+            int u[4];
+            uint32_t w[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                u[t] = -1;
+                w[t] = 0;
+                if (e + t < end) {
+                    u[t] = a.adjncy[e + t];
+                    w[t] = (uint32_t)a.adjwgt[e + t];
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                if (u[t] < 0) continue;
+                const uint32_t l = (uint32_t)u[t];
+                if (l == own) { cown += w[t]; continue; }
+                if (cand_ok<MODE>(a, l, w[t], cv)) better(key, id, cand_key(w[t], a.ks_tie, l), l);
+            }
+        }
+        wv += 1;
+        we += (unsigned long long)(end - beg);
+        decide_emit<MODE>(a, v, own, cv, cown, key, id);
+        return 0;
+    }
     bool overflow = false;
     for (int e = beg; e < end && !overflow; e += 4) {
         int u[4];
@@ -443,46 +476,47 @@ __device__ __forceinline__ void append_aggregated(bool pred, int v, int* list, u
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kThreads) lane_kernel(SweepArgs a) {
+__global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
+    // per-warp queue of members still to be processed, so that every pass
+    // over the lanes is full
+    __shared__ int queue[kWarpsPerBlock][32 * kSpan + 32];
     const int lane = threadIdx.x & 31;
+    int* q = queue[threadIdx.x >> 5];
+    int qn = 0;  // warp-uniform
     unsigned long long wv = 0, we = 0;
     const long long span = 32LL * kSpan;
     const long long ntasks = ((long long)a.n + span - 1) / span;
     const long long warp = ((long long)blockIdx.x * kThreads + threadIdx.x) / 32;
     const long long nwarps = (long long)gridDim.x * kThreads / 32;
+    auto pass = [&](int v) {
+        int status = 0;
+        if (v >= 0) status = lane_vertex<MODE>(a, v, wv, we);
+        append_aggregated(status == 1, v, a.flist, a.fcount);
+        append_aggregated(status == 2, v, a.heavy, a.hcount);
+    };
     for (long long task = warp; task < ntasks; task += nwarps) {
         const long long base = task * span;
-        unsigned m[kSpan];
-        int total = 0;
 #pragma unroll
         for (int c = 0; c < kSpan; ++c) {
             const long long vv = base + c * 32 + lane;
             const bool valid = vv < a.n;
             const bool mem = valid && member<MODE>(a, (int)vv);
             if (valid && !mem) a.pt[vv] = -1;
-            m[c] = __ballot_sync(0xffffffffu, mem);
-            total += __popc(m[c]);
+            const unsigned m = __ballot_sync(0xffffffffu, mem);
+            if (mem) q[qn + __popc(m & lanemask_lt())] = (int)vv;
+            qn += __popc(m);
         }
-        for (int p = 0; p < total; p += 32) {
-            const int r = p + lane;
-            int v = -1;
-            if (r < total) {
-                int rr = r, c = 0;
-#pragma unroll
-                for (int cc = 0; cc < kSpan - 1; ++cc)
-                    if (c == cc && rr >= __popc(m[cc])) { rr -= __popc(m[cc]); c = cc + 1; }
-                unsigned mc = m[0];
-#pragma unroll
-                for (int cc = 1; cc < kSpan; ++cc)
-                    if (c == cc) mc = m[cc];
-                v = (int)(base + c * 32 + nth_set_bit(mc, rr));
-            }
-            int status = 0;
-            if (v >= 0) status = lane_vertex<MODE>(a, v, wv, we);
-            append_aggregated(status == 1, v, a.flist, a.fcount);
-            append_aggregated(status == 2, v, a.heavy, a.hcount);
+        __syncwarp();
+        while (qn >= 32) {
+            const int v = q[lane];
+            __syncwarp();
+            for (int i = lane; i + 32 < qn; i += 32) q[i] = q[i + 32];
+            __syncwarp();
+            qn -= 32;
+            pass(v);
         }
     }
+    if (qn > 0) pass(lane < qn ? q[lane] : -1);
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) {
         wv += __shfl_xor_sync(0xffffffffu, wv, o);
@@ -737,17 +771,31 @@ SweepBuffers make_buffers(Ctx& ctx, const DevGraph& g) {
     return b;
 }
 
+const char* family(int mode, int part) {
+    static const char* names[3][3] = {{"lp_cluster_sweep", "lp_cluster_overflow", "lp_cluster_heavy"},
+                                      {"lp_refine_sweep", "lp_refine_overflow", "lp_refine_heavy"},
+                                      {"balance_sweep", "balance_overflow", "balance_heavy"}};
+    return names[mode][part];
+}
+
 template <int MODE>
-void launch_sweep(Ctx& ctx, const DevGraph& g, SweepArgs a, const SweepBuffers& b) {
+void launch_sweep(Ctx& ctx, const DevGraph& g, SweepArgs a, const SweepBuffers& b, double bytes) {
     const long long tasks = ((long long)g.n + 32 * kSpan - 1) / (32 * kSpan);
-    const int lblocks = (int)std::max<long long>(1, std::min<long long>(div_up(tasks, kWarpsPerBlock), kNumSMs * 8LL));
+    const int lblocks = (int)std::max<long long>(1, std::min<long long>(div_up(tasks, kWarpsPerBlock), kNumSMs * 4LL));
     KB_CUDA(cudaMemsetAsync(b.counters, 0, 2 * sizeof(unsigned), ctx.stream));
-    lane_kernel<MODE><<<lblocks, kThreads, 0, ctx.stream>>>(a);
-    KB_LAUNCH();
-    const int cblocks = (int)std::max<long long>(1, std::min<long long>(div_up(g.n, 32 * kWarpsPerBlock), sweep_blocks()));
-    chunk_kernel<MODE><<<cblocks, kThreads, 0, ctx.stream>>>(a);
-    KB_LAUNCH();
+    {
+        PhaseScope ps(ctx, family(MODE, 0), bytes);
+        lane_kernel<MODE><<<lblocks, kThreads, 0, ctx.stream>>>(a);
+        KB_LAUNCH();
+    }
+    {
+        PhaseScope ps(ctx, family(MODE, 1), 0);
+        const int cblocks = (int)std::max<long long>(1, std::min<long long>(div_up(g.n, 32 * kWarpsPerBlock), sweep_blocks()));
+        chunk_kernel<MODE><<<cblocks, kThreads, 0, ctx.stream>>>(a);
+        KB_LAUNCH();
+    }
     if (b.gcap > 0) {
+        PhaseScope ps(ctx, family(MODE, 2), 0);
         heavy_kernel<MODE><<<b.hblocks, kThreads, 0, ctx.stream>>>(a, b.gtk, b.gtv, b.gcap);
         KB_LAUNCH();
     }
@@ -799,15 +847,16 @@ void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* la
     a.inc = inc;
     a.minv = minv;
     const int dblocks = (int)std::max<long long>(1, std::min<long long>(div_up(g.n, kThreads), kNumSMs * 8LL));
+    const bool sorted_rows = rows_strictly_increasing(ctx, g);
     for (int r = 0; r < kn.lpc_rounds; ++r) {
         a.ks_sub = stream_key(kn.seed, TAG_CSUB, level, r);
         a.ks_tie = stream_key(kn.seed, TAG_CTIE, level, r);
         for (uint32_t s = 0; s < a.S; ++s) {
             a.s = s;
-            {
-                PhaseScope ps(ctx, "lp_cluster_sweep", sweep_bytes(g, 1.0 / a.S));
-                launch_sweep<CLUSTER>(ctx, g, a, b);
-            }
+            // before the first sub-round every vertex is its own cluster; with
+            // no repeated targets per row nothing needs aggregating
+            a.singletons = (r == 0 && s == 0 && sorted_rows) ? 1 : 0;
+            launch_sweep<CLUSTER>(ctx, g, a, b, sweep_bytes(g, 1.0 / a.S));
             PhaseScope ps(ctx, "lp_cluster_admit", 0);
             cluster_decide<<<dblocks, kThreads, 0, st>>>(g.n, b.pt, cw, inc, minv, a.bound);
             KB_LAUNCH();
@@ -853,10 +902,7 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
         KB_CUDA(cudaMemsetAsync(moved, 0, sizeof(unsigned), st));
         for (uint32_t s = 0; s < a.S; ++s) {
             a.s = s;
-            {
-                PhaseScope ps(ctx, "lp_refine_sweep", sweep_bytes(g, 1.0 / a.S));
-                launch_sweep<REFINE>(ctx, g, a, b);
-            }
+            launch_sweep<REFINE>(ctx, g, a, b, sweep_bytes(g, 1.0 / a.S));
             PhaseScope ps(ctx, "lp_refine_admit", 0);
             class_decide<<<dblocks, kThreads, 0, st>>>(g.n, b.pt, b.pc, g.vwgt, bw, H, minvP, P, bound, 1);
             KB_LAUNCH();
@@ -907,7 +953,7 @@ bool balance(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t b
         a.ks_sub = stream_key(kn.seed, TAG_BCLS, level, it);  // release class stream
         uint64_t ks_prio = stream_key(kn.seed, TAG_BPRIO, level, it);
         fill_u32(HS, (long long)k * kBalClasses, 0u, st);
-        launch_sweep<BALANCE>(ctx, g, a, b);
+        launch_sweep<BALANCE>(ctx, g, a, b, 0);
         balance_threshold<<<div_up(k, 256), 256, 0, st>>>(bw, HS, k, bound, thr);
         KB_LAUNCH();
         balance_release<<<dblocks, kThreads, 0, st>>>(g.n, b.pt, b.pc, part, g.vwgt, thr, H, minvP, P, ks_prio);

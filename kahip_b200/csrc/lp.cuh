@@ -55,6 +55,10 @@ int max_degree(Ctx& ctx, const DevGraph& g);
 // NodeWeight accumulates it).  Synchronises the stream.
 int check_graph(Ctx& ctx, const DevGraph& g, uint32_t* total_weight = nullptr);
 
+// true if every row lists its targets in strictly increasing order
+// (synchronises the stream)
+bool rows_strictly_increasing(Ctx& ctx, const DevGraph& g);
+
 // label[v] = v, cw[v] = vwgt[v]
 void init_labels(Ctx& ctx, const DevGraph& g, int* label, uint32_t* cw);
 

@@ -83,6 +83,16 @@ __global__ void check_graph_kernel(int n, long long m, const int* __restrict__ x
     }
 }
 
+__global__ void rows_sorted_kernel(int n, const int* __restrict__ xadj, const int* __restrict__ adjncy,
+                                   int* bad) {
+    int f = 0;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        for (int e = xadj[v] + 1; e < xadj[v + 1]; ++e)
+            if (adjncy[e] <= adjncy[e - 1]) f = 1;
+    f = __reduce_or_sync(0xffffffffu, f);
+    if ((threadIdx.x & 31) == 0 && f) atomicOr(bad, 1);
+}
+
 int grid_for(long long n, int threads) {
     return (int)std::max<long long>(1, std::min<long long>(div_up(n, threads), (long long)kNumSMs * 16));
 }
@@ -134,6 +144,17 @@ int check_graph(Ctx& ctx, const DevGraph& g, uint32_t* total_weight) {
     KB_CUDA(cudaStreamSynchronize(ctx.stream));
     if (total_weight) *total_weight = ctx.pinned[3];
     return (int)ctx.pinned[2];
+}
+
+bool rows_strictly_increasing(Ctx& ctx, const DevGraph& g) {
+    if (g.n == 0) return true;
+    int* d = ctx.dscalars + 4;
+    KB_CUDA(cudaMemsetAsync(d, 0, sizeof(int), ctx.stream));
+    rows_sorted_kernel<<<grid_for(g.n, 256), 256, 0, ctx.stream>>>(g.n, g.xadj, g.adjncy, d);
+    KB_LAUNCH();
+    KB_CUDA(cudaMemcpyAsync(ctx.pinned + 4, d, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    KB_CUDA(cudaStreamSynchronize(ctx.stream));
+    return ctx.pinned[4] == 0;
 }
 
 void init_labels(Ctx& ctx, const DevGraph& g, int* label, uint32_t* cw) {

@@ -92,7 +92,7 @@ void Ctx::collect() {
 
 void Ctx::reset_stats() {
     phases.clear();
-    if (work) KB_CUDA(cudaMemsetAsync(work, 0, 2 * sizeof(unsigned long long), stream));
+    if (work) KB_CUDA(cudaMemsetAsync(work, 0, 4 * sizeof(unsigned long long), stream));
     if (dscalars) KB_CUDA(cudaMemsetAsync(dscalars + 60, 0, sizeof(int), stream));
 }
 

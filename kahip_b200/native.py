@@ -56,7 +56,8 @@ class Stats(ctypes.Structure):
                 ("nfamilies", ctypes.c_int), ("family_name", (ctypes.c_char * 24) * 16),
                 ("family_ms", ctypes.c_double * 16), ("family_bytes", ctypes.c_double * 16),
                 ("family_launches", ctypes.c_longlong * 16), ("sweep_vertices", ctypes.c_longlong),
-                ("sweep_edges", ctypes.c_longlong), ("device_bytes_peak", ctypes.c_size_t)]
+                ("sweep_edges", ctypes.c_longlong), ("sweep_overflow_vertices", ctypes.c_longlong),
+                ("device_bytes_peak", ctypes.c_size_t)]
 
     def families(self) -> dict:
         return {self.family_name[i].value.decode(): dict(ms=self.family_ms[i], bytes=self.family_bytes[i],
