@@ -11,10 +11,10 @@
 // Pipeline (all on the device):
 //   1. leader[c] = min member (atomicMin); prefix sum over leader flags
 //      gives coarse ids; cmap gather; coarse node weights (atomicAdd).
-//   2. every fine node pre-aggregates its neighbours by coarse target
-//      (match_any within G-lane chunks) and writes (cu<<tb|cv, w) entries
-//      into its warp chunk's slice of an m-sized buffer.
-//   3. compaction of the chunk slices (prefix sum of chunk counts).
+//   2. every fine node merges its neighbours by coarse target in register
+//      slots and writes (cu<<tb|cv, w) entries into its own CSR range of an
+//      m-sized buffer.
+//   3. compaction (prefix sum of the per-vertex entry counts).
 //   4. stable LSD radix sort on the 2*tb key bits.
 //   5. reduce-by-key -> coarse adjncy/adjwgt, row counts -> prefix sum -> xadj.
 #include "contract.cuh"
@@ -54,75 +54,92 @@ __global__ void make_cmap(int n, const int* __restrict__ label, const int* __res
     }
 }
 
-template <int G>
+// One thread per fine vertex: merges its neighbours by coarse target in
+// kEmitSlots register slots (edges inside its own coarse node are dropped)
+// and writes the (cu<<tb | cv, w) entries into its own CSR range, flushing
+// the slots whenever a new target finds them full -- repeated targets that
+// this leaves are merged by the sort + reduce that follows.
+constexpr int kEmitSlots = 8;
+
 __global__ void __launch_bounds__(kThreads) emit_kernel(int n, const int* __restrict__ xadj,
                                                         const int* __restrict__ adjncy,
                                                         const int* __restrict__ adjwgt,
                                                         const int* __restrict__ cmap, uint64_t* ekey,
-                                                        uint32_t* eval, uint32_t* ccount, int tb) {
-    __shared__ uint32_t wcount[kThreads / 32];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int gid = lane / G, gl = lane % G;
-    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (gid * G));
-    const long long nchunks = ((long long)n + 31) / 32;
-    const long long warp = ((long long)blockIdx.x * kThreads + threadIdx.x) / 32;
-    const long long nwarps = (long long)gridDim.x * kThreads / 32;
-    for (long long chunk = warp; chunk < nchunks; chunk += nwarps) {
-        if (lane == 0) wcount[wib] = 0;
-        __syncwarp();
-        const long long rstart = xadj[chunk * 32];
-        int v0 = (int)(chunk * 32 + lane);
-        unsigned mask = __ballot_sync(0xffffffffu, v0 < n);
-        while (mask) {
-            int pick = -1;
+                                                        uint32_t* eval, uint32_t* vcount, int tb) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const int beg = xadj[v], end = xadj[v + 1];
+        const uint32_t own = (uint32_t)cmap[v];
+        const uint64_t hi = (uint64_t)own << tb;
+        uint32_t st[kEmitSlots], sw[kEmitSlots];
+        int used = 0;
+        int pos = beg;
+        for (int e = beg; e < end; e += 4) {
+            int u[4];
+            uint32_t w[4], t[4];
 #pragma unroll
-            for (int i = 0; i < 32 / G; ++i) {
-                if (mask) {
-                    if (i == gid) pick = __ffs(mask) - 1;
-                    mask &= mask - 1;
+            for (int j = 0; j < 4; ++j) {
+                u[j] = -1;
+                w[j] = 0;
+                if (e + j < end) {
+                    u[j] = adjncy[e + j];
+                    w[j] = (uint32_t)adjwgt[e + j];
                 }
             }
-            if (pick >= 0) {
-                const int v = (int)(chunk * 32 + pick);
-                const uint32_t own = (uint32_t)cmap[v];
-                const int beg = xadj[v], end = xadj[v + 1];
-                for (int c = beg; c < end; c += G) {
-                    int e = c + gl;
-                    uint32_t t = kEmpty, w = 0;
-                    if (e < end) {
-                        t = (uint32_t)cmap[adjncy[e]];
-                        w = (uint32_t)adjwgt[e];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) t[j] = u[j] >= 0 ? (uint32_t)cmap[u[j]] : kEmpty;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (u[j] < 0 || t[j] == own) continue;
+                bool hit = false;
+#pragma unroll
+                for (int i = 0; i < kEmitSlots; ++i)
+                    if (i < used && st[i] == t[j]) { sw[i] += w[j]; hit = true; }
+                if (hit) continue;
+                if (used == kEmitSlots) {
+#pragma unroll
+                    for (int i = 0; i < kEmitSlots; ++i) {
+                        ekey[pos] = hi | st[i];
+                        eval[pos] = sw[i];
+                        ++pos;
                     }
-                    unsigned peers = __match_any_sync(gmask, t);
-                    uint32_t sum = __reduce_add_sync(peers, w);
-                    if (e < end && (peers & lanemask_lt()) == 0 && t != own) {
-                        uint32_t p = atomicAdd(&wcount[wib], 1u);
-                        ekey[rstart + p] = ((uint64_t)own << tb) | t;
-                        eval[rstart + p] = sum;
-                    }
+                    used = 0;
                 }
+#pragma unroll
+                for (int i = 0; i < kEmitSlots; ++i)
+                    if (i == used) { st[i] = t[j]; sw[i] = w[j]; }
+                ++used;
             }
         }
-        __syncwarp();
-        if (lane == 0) ccount[chunk] = wcount[wib];
-        __syncwarp();
+#pragma unroll
+        for (int i = 0; i < kEmitSlots; ++i)
+            if (i < used) {
+                ekey[pos] = hi | st[i];
+                eval[pos] = sw[i];
+                ++pos;
+            }
+        vcount[v] = (uint32_t)(pos - beg);
     }
 }
 
-__global__ void compact_chunks(long long nchunks, const int* __restrict__ xadj,
-                               const uint32_t* __restrict__ ccount, const uint32_t* __restrict__ coff,
-                               const uint64_t* __restrict__ ekey, const uint32_t* __restrict__ eval,
-                               uint64_t* K, uint32_t* V) {
+// entries of vertex v move from its CSR range to voff[v] in the sort input;
+// a warp copies 32 consecutive vertices, lanes striding over each one's entries
+__global__ void compact_vertices(int n, const int* __restrict__ xadj, const uint32_t* __restrict__ vcount,
+                                 const uint32_t* __restrict__ voff, const uint64_t* __restrict__ ekey,
+                                 const uint32_t* __restrict__ eval, uint64_t* K, uint32_t* V) {
     const int lane = threadIdx.x & 31;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
     const long long nwarps = (long long)gridDim.x * blockDim.x / 32;
-    for (long long c = warp; c < nchunks; c += nwarps) {
-        uint32_t cnt = ccount[c];
-        long long src = xadj[c * 32];
-        long long dst = coff[c];
-        for (uint32_t i = lane; i < cnt; i += 32) {
-            K[dst + i] = ekey[src + i];
-            V[dst + i] = eval[src + i];
+    for (long long c = warp; c * 32 < n; c += nwarps) {
+        const int v0 = (int)(c * 32);
+        const int vend = min(n, v0 + 32);
+        for (int v = v0; v < vend; ++v) {
+            const uint32_t cnt = vcount[v];
+            const long long src = xadj[v];
+            const long long dst = voff[v];
+            for (uint32_t i = lane; i < cnt; i += 32) {
+                K[dst + i] = ekey[src + i];
+                V[dst + i] = eval[src + i];
+            }
         }
     }
 }
@@ -150,10 +167,6 @@ __global__ void reduce_runs(long long E, const uint64_t* __restrict__ K, const u
     }
 }
 
-int pick_group(int n, long long m) {
-    double avg = n ? (double)m / n : 0;
-    return avg <= 8 ? 8 : (avg <= 16 ? 16 : 32);
-}
 
 }  // namespace
 
@@ -195,22 +208,18 @@ void contract(Ctx& ctx, const DevGraph& g, const int* label, int* cmap, DevGraph
     KB_LAUNCH();
     int tb = 1;
     while ((1LL << tb) < (long long)nc) ++tb;
-    // 2. emission into chunk slices
+    // 2. emission into each vertex's CSR range
     const long long m = g.m;
-    const long long nchunks = ((long long)n + 31) / 32;
     uint64_t* ekey = ctx.scratch.alloc<uint64_t>((size_t)std::max<long long>(m, 1));
     uint32_t* eval = ctx.scratch.alloc<uint32_t>((size_t)std::max<long long>(m, 1));
-    uint32_t* ccount = ctx.scratch.alloc<uint32_t>((size_t)nchunks + 1);
-    uint32_t* coff = ctx.scratch.alloc<uint32_t>((size_t)nchunks + 1);
+    uint32_t* vcount = ctx.scratch.alloc<uint32_t>((size_t)n + 1);
+    uint32_t* voff = ctx.scratch.alloc<uint32_t>((size_t)n + 1);
     {
         PhaseScope ps(ctx, "contract_emit", 12.0 * m + 8.0 * n);
-        int G = pick_group(n, m);
-        int blocks = kNumSMs * 8;
-        if (G == 8) emit_kernel<8><<<blocks, kThreads, 0, st>>>(n, g.xadj, g.adjncy, g.adjwgt, cmap, ekey, eval, ccount, tb);
-        else if (G == 16) emit_kernel<16><<<blocks, kThreads, 0, st>>>(n, g.xadj, g.adjncy, g.adjwgt, cmap, ekey, eval, ccount, tb);
-        else emit_kernel<32><<<blocks, kThreads, 0, st>>>(n, g.xadj, g.adjncy, g.adjwgt, cmap, ekey, eval, ccount, tb);
+        emit_kernel<<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, g.adjncy, g.adjwgt, cmap, ekey, eval,
+                                                                vcount, tb);
         KB_LAUNCH();
-        exclusive_scan_u32(ccount, coff, nchunks, tot, st, ctx.scratch);
+        exclusive_scan_u32(vcount, voff, n, tot, st, ctx.scratch);
     }
     KB_CUDA(cudaMemcpyAsync(ctx.pinned, tot, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     KB_CUDA(cudaStreamSynchronize(st));
@@ -222,7 +231,7 @@ void contract(Ctx& ctx, const DevGraph& g, const int* label, int* cmap, DevGraph
     uint32_t* V1 = ctx.scratch.alloc<uint32_t>((size_t)std::max<long long>(E, 1));
     {
         PhaseScope ps(ctx, "contract_compact", 24.0 * E);
-        compact_chunks<<<kNumSMs * 8, kThreads, 0, st>>>(nchunks, g.xadj, ccount, coff, ekey, eval, K0, V0);
+        compact_vertices<<<kNumSMs * 8, kThreads, 0, st>>>(n, g.xadj, vcount, voff, ekey, eval, K0, V0);
         KB_LAUNCH();
     }
     // 4. sort by (cu, cv)

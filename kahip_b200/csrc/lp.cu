@@ -54,7 +54,9 @@ struct SweepArgs {
     uint32_t* H;                        // REFINE/BALANCE: weight per (target, class)
     int* minvP;                         // smallest proposer per (target, class)
     int* heavy; unsigned* hcount;       // deferred high-degree vertices
-    int* flist; unsigned* fcount;       // vertices with more distinct labels than register slots
+    int* flist; unsigned* fcount;       // vertices with more distinct labels than kSlots
+    int* flist2; unsigned* fcount2;     // ... and than kSlotsWide
+    int* plist; unsigned* pcount;       // vertices that proposed a move this sub-round
     int singletons;                     // every label is its own vertex id and rows have
                                         // strictly increasing targets (clustering round 0)
     unsigned long long* work;           // [0] vertices, [1] edges
@@ -120,17 +122,18 @@ __device__ __forceinline__ int loss_bucket(long long loss) {
 }
 
 // Final decision for vertex v (executed by one lane).
+// Returns true when v proposes a move (pt[v] = target; the caller lists v).
 template <int MODE>
-__device__ void decide_emit(const SweepArgs& a, int v, uint32_t own, uint32_t cv, uint32_t conn_own,
+__device__ bool decide_emit(const SweepArgs& a, int v, uint32_t own, uint32_t cv, uint32_t conn_own,
                             uint64_t key, uint32_t id) {
     if (MODE == CLUSTER) {
-        if (id == kEmpty || (uint32_t)(key >> 32) <= conn_own) { a.pt[v] = -1; return; }
+        if (id == kEmpty || (uint32_t)(key >> 32) <= conn_own) return false;
         a.pt[v] = (int)id;
         atomicAdd(&a.inc[id], cv);
         atomicMin(&a.minv[id], v);
     } else if (MODE == REFINE) {
         uint32_t base = a.lw[own] <= a.bound ? conn_own : 0u;
-        if (id == kEmpty || (uint32_t)(key >> 32) <= base) { a.pt[v] = -1; return; }
+        if (id == kEmpty || (uint32_t)(key >> 32) <= base) return false;
         int cls = (int)hash_range(hash32(a.ks_prio, (uint32_t)v), (uint32_t)a.P);
         a.pt[v] = (int)id;
         a.pc[v] = cls;
@@ -141,7 +144,7 @@ __device__ void decide_emit(const SweepArgs& a, int v, uint32_t own, uint32_t cv
         uint32_t t = id, tc = (uint32_t)(key >> 32);
         if (t == kEmpty) {
             int L = *a.lightest;
-            if ((uint32_t)L == own || (uint64_t)a.lw[L] + cv > a.bound) { a.pt[v] = -1; return; }
+            if ((uint32_t)L == own || (uint64_t)a.lw[L] + cv > a.bound) return false;
             t = (uint32_t)L;
             tc = 0;
         }
@@ -151,6 +154,18 @@ __device__ void decide_emit(const SweepArgs& a, int v, uint32_t own, uint32_t cv
         a.pc[v] = cls;
         atomicAdd(&a.HS[(size_t)own * kBalClasses + cls], cv);
     }
+    return true;
+}
+
+__device__ __forceinline__ void append_aggregated(bool pred, int v, int* list, unsigned* count) {
+    const unsigned m = __ballot_sync(0xffffffffu, pred);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(count, (unsigned)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (pred) list[base + __popc(m & lanemask_lt())] = v;
 }
 
 template <int MODE>
@@ -205,14 +220,14 @@ __global__ void __launch_bounds__(kThreads) chunk_kernel(SweepArgs a) {
     if (lane == 0) T.nused = 0;
     __syncwarp();
     unsigned long long wv = 0, we = 0;
-    const unsigned count = *a.fcount;
+    const unsigned count = *a.fcount2;
     const long long nchunks = ((long long)count + 31) / 32;
     const long long warp = ((long long)blockIdx.x * kThreads + threadIdx.x) / 32;
     const long long nwarps = (long long)gridDim.x * kThreads / 32;
     for (long long chunk = warp; chunk < nchunks; chunk += nwarps) {
         const long long li = chunk * 32 + lane;
         const bool mem = li < (long long)count;
-        const int v = mem ? a.flist[li] : 0;
+        const int v = mem ? a.flist2[li] : 0;
         int beg = 0, deg = 0;
         bool heavy = false;
         if (mem) {
@@ -335,7 +350,9 @@ __global__ void __launch_bounds__(kThreads) chunk_kernel(SweepArgs a) {
             }
             __syncwarp();
             if (lane == 0) T.nused = 0;
-            if (wmember) decide_emit<MODE>(a, v, T.own[lane], T.cv[lane], T.cown[lane], T.bkey[lane], T.bid[lane]);
+            bool prop = false;
+            if (wmember) prop = decide_emit<MODE>(a, v, T.own[lane], T.cv[lane], T.cown[lane], T.bkey[lane], T.bid[lane]);
+            append_aggregated(prop, v, a.plist, a.pcount);
             __syncwarp();
             // next window starts at the first light lane at or after wend
             const unsigned rest = lightmask & (wend < 32 ? (~0u << wend) : 0u);
@@ -366,6 +383,7 @@ __global__ void __launch_bounds__(kThreads) chunk_kernel(SweepArgs a) {
 // to the high-degree list (heavy_kernel).
 
 constexpr int kSlots = 8;
+constexpr int kSlotsWide = 16;
 constexpr int kSpan = 4;  // chunks of 32 ids per warp task
 
 // r-th set bit (0-based) of mask
@@ -380,16 +398,17 @@ __device__ __forceinline__ int nth_set_bit(unsigned mask, int r) {
     return lo;
 }
 
-// 0: decided, 1: too many distinct labels, 2: degree above kWin
-template <int MODE>
+// 0: decided (stays), 3: decided (proposes a move), 1: too many distinct
+// labels for NS slots, 2: degree above kWin
+template <int MODE, int NS>
 __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, unsigned long long& we) {
     const int beg = a.xadj[v], end = a.xadj[v + 1];
     if (end - beg > kWin) return 2;
     const uint32_t own = (uint32_t)a.lab[v];
     const uint32_t cv = (uint32_t)a.vwgt[v];
-    uint32_t sl[kSlots], sc[kSlots];
+    uint32_t sl[NS], sc[NS];
 #pragma unroll
-    for (int i = 0; i < kSlots; ++i) { sl[i] = kEmpty; sc[i] = 0; }
+    for (int i = 0; i < NS; ++i) { sl[i] = kEmpty; sc[i] = 0; }
     uint32_t cown = 0;
     if (MODE == CLUSTER && a.singletons) {
         // label[u] == u and no target repeats: the connection to cluster u is
@@ -418,8 +437,7 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
         }
         wv += 1;
         we += (unsigned long long)(end - beg);
-        decide_emit<MODE>(a, v, own, cv, cown, key, id);
-        return 0;
+        return decide_emit<MODE>(a, v, own, cv, cown, key, id) ? 3 : 0;
     }
     bool overflow = false;
     for (int e = beg; e < end && !overflow; e += 4) {
@@ -442,11 +460,11 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
             if (l[t] == own) { cown += w[t]; continue; }
             bool hit = false;
 #pragma unroll
-            for (int i = 0; i < kSlots; ++i)
+            for (int i = 0; i < NS; ++i)
                 if (sl[i] == l[t]) { sc[i] += w[t]; hit = true; }
             if (!hit) {
 #pragma unroll
-                for (int i = 0; i < kSlots; ++i)
+                for (int i = 0; i < NS; ++i)
                     if (!hit && sl[i] == kEmpty) { sl[i] = l[t]; sc[i] = w[t]; hit = true; }
                 overflow |= !hit;
             }
@@ -458,22 +476,11 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
     uint64_t key = 0;
     uint32_t id = kEmpty;
 #pragma unroll
-    for (int i = 0; i < kSlots; ++i)
+    for (int i = 0; i < NS; ++i)
         if (sl[i] != kEmpty && cand_ok<MODE>(a, sl[i], sc[i], cv)) better(key, id, cand_key(sc[i], a.ks_tie, sl[i]), sl[i]);
-    decide_emit<MODE>(a, v, own, cv, cown, key, id);
-    return 0;
+    return decide_emit<MODE>(a, v, own, cv, cown, key, id) ? 3 : 0;
 }
 
-__device__ __forceinline__ void append_aggregated(bool pred, int v, int* list, unsigned* count) {
-    const unsigned m = __ballot_sync(0xffffffffu, pred);
-    if (!m) return;
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(m) - 1;
-    unsigned base = 0;
-    if (lane == leader) base = atomicAdd(count, (unsigned)__popc(m));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (pred) list[base + __popc(m & lanemask_lt())] = v;
-}
 
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
@@ -490,9 +497,10 @@ __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
     const long long nwarps = (long long)gridDim.x * kThreads / 32;
     auto pass = [&](int v) {
         int status = 0;
-        if (v >= 0) status = lane_vertex<MODE>(a, v, wv, we);
+        if (v >= 0) status = lane_vertex<MODE, kSlots>(a, v, wv, we);
         append_aggregated(status == 1, v, a.flist, a.fcount);
         append_aggregated(status == 2, v, a.heavy, a.hcount);
+        append_aggregated(status == 3, v, a.plist, a.pcount);
     };
     for (long long task = warp; task < ntasks; task += nwarps) {
         const long long base = task * span;
@@ -501,7 +509,6 @@ __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
             const long long vv = base + c * 32 + lane;
             const bool valid = vv < a.n;
             const bool mem = valid && member<MODE>(a, (int)vv);
-            if (valid && !mem) a.pt[vv] = -1;
             const unsigned m = __ballot_sync(0xffffffffu, mem);
             if (mem) q[qn + __popc(m & lanemask_lt())] = (int)vv;
             qn += __popc(m);
@@ -525,6 +532,33 @@ __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
     if (lane == 0 && (wv | we)) {
         atomicAdd(&a.work[0], wv);
         atomicAdd(&a.work[1], we);
+    }
+}
+
+// Second tier: the overflow list of the lane kernel with kSlotsWide slots.
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, 3) wide_kernel(SweepArgs a) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long wv = 0, we = 0;
+    const unsigned count = *a.fcount;
+    const long long warp = ((long long)blockIdx.x * kThreads + threadIdx.x) / 32;
+    const long long nwarps = (long long)gridDim.x * kThreads / 32;
+    for (long long base = warp * 32; base < count; base += nwarps * 32) {
+        const int v = base + lane < count ? a.flist[base + lane] : -1;
+        int status = 0;
+        if (v >= 0) status = lane_vertex<MODE, kSlotsWide>(a, v, wv, we);
+        append_aggregated(status == 1, v, a.flist2, a.fcount2);
+        append_aggregated(status == 3, v, a.plist, a.pcount);
+    }
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        wv += __shfl_xor_sync(0xffffffffu, wv, o);
+        we += __shfl_xor_sync(0xffffffffu, we, o);
+    }
+    if (lane == 0 && (wv | we)) {
+        atomicAdd(&a.work[0], wv);
+        atomicAdd(&a.work[1], we);
+        atomicAdd(&a.work[2], wv);
     }
 }
 
@@ -578,7 +612,7 @@ __global__ void __launch_bounds__(kThreads) heavy_kernel(SweepArgs a, uint32_t* 
         __syncthreads();
         if (threadIdx.x == 0) {
             for (int j = 1; j < kThreads / 32; ++j) better(key, id, sk[j], sid[j]);
-            decide_emit<MODE>(a, v, own, cv, sco, key, id);
+            if (decide_emit<MODE>(a, v, own, cv, sco, key, id)) a.plist[atomicAdd(a.pcount, 1u)] = v;
         }
         __syncthreads();
     }
@@ -591,9 +625,11 @@ __global__ void __launch_bounds__(kThreads) heavy_kernel(SweepArgs a, uint32_t* 
 
 // Clustering: all proposals into b are admitted if they fit together;
 // otherwise only the smallest proposer (which fits by itself).
-__global__ void cluster_decide(int n, int* pt, const uint32_t* cw, const uint32_t* inc, const int* minv,
-                               uint32_t bound) {
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+__global__ void cluster_decide(const int* plist, const unsigned* pcount, int* pt, const uint32_t* cw,
+                               const uint32_t* inc, const int* minv, uint32_t bound) {
+    const unsigned cnt = *pcount;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const int v = plist[i];
         int b = pt[v];
         if (b < 0) continue;
         bool ok = ((uint64_t)cw[b] + inc[b] < bound) || minv[b] == v;
@@ -601,9 +637,11 @@ __global__ void cluster_decide(int n, int* pt, const uint32_t* cw, const uint32_
     }
 }
 
-__global__ void cluster_apply(int n, const int* pt, const int* vwgt, int* label, uint32_t* cw, uint32_t* inc,
-                              int* minv) {
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+__global__ void cluster_apply(const int* plist, const unsigned* pcount, const int* pt, const int* vwgt, int* label,
+                              uint32_t* cw, uint32_t* inc, int* minv) {
+    const unsigned cnt = *pcount;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const int v = plist[i];
         int t = pt[v];
         if (t == -1) continue;
         int b = t >= 0 ? t : -2 - t;
@@ -632,9 +670,12 @@ __device__ __forceinline__ bool admit(const uint32_t* H, const int* minvP, int P
 
 // strict: cap = bound - 1 - w[b] (refinement keeps blocks < bound);
 // otherwise cap = bound - w[b] (balance repair fills up to bound)
-__global__ void class_decide(int n, int* pt, const int* pc, const int* vwgt, const uint32_t* bw,
-                             const uint32_t* H, const int* minvP, int P, uint32_t bound, int strict) {
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+__global__ void class_decide(const int* plist, const unsigned* pcount, int* pt, const int* pc, const int* vwgt,
+                             const uint32_t* bw, const uint32_t* H, const int* minvP, int P, uint32_t bound,
+                             int strict) {
+    const unsigned cnt = *pcount;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const int v = plist[i];
         int b = pt[v];
         if (b < 0) continue;
         int c = pc[v];
@@ -644,11 +685,13 @@ __global__ void class_decide(int n, int* pt, const int* pc, const int* vwgt, con
     }
 }
 
-__global__ void class_apply(int n, const int* pt, const int* pc, const int* xadj, const int* adjncy,
-                            const int* vwgt, int* part, uint32_t* bw, uint32_t* H, int* minvP, int P,
-                            uint8_t* next_active, unsigned* moved) {
+__global__ void class_apply(const int* plist, const unsigned* pcount, const int* pt, const int* pc,
+                            const int* xadj, const int* adjncy, const int* vwgt, int* part, uint32_t* bw,
+                            uint32_t* H, int* minvP, int P, uint8_t* next_active, unsigned* moved) {
     unsigned mv = 0;
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const unsigned cnt = *pcount;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const int v = plist[i];
         int t = pt[v];
         if (t == -1) continue;
         int c = pc[v];
@@ -683,9 +726,12 @@ __global__ void balance_threshold(const uint32_t* bw, const uint32_t* HS, int k,
 }
 
 // Balance: released candidates get an admission class; others are dropped.
-__global__ void balance_release(int n, const int* pt, int* pc, const int* part, const int* vwgt, const int* thr,
-                                uint32_t* H, int* minvP, int P, uint64_t ks_prio) {
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+__global__ void balance_release(const int* plist, const unsigned* pcount, const int* pt, int* pc, const int* part,
+                                const int* vwgt, const int* thr, uint32_t* H, int* minvP, int P,
+                                uint64_t ks_prio) {
+    const unsigned cnt = *pcount;
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        const int v = plist[i];
         int t = pt[v];
         if (t < 0) continue;
         if (pc[v] >= thr[part[v]]) { pc[v] = -1; continue; }
@@ -732,9 +778,11 @@ int sweep_blocks() { return kNumSMs * 5; }  // 48 registers, 32 KB shared: 5 blo
 
 struct SweepBuffers {
     int *pt, *pc;
-    unsigned* counters;  // [0] fcount, [1] hcount, [2] moved
+    unsigned* counters;  // [0] fcount, [1] hcount, [2] pcount, [3] fcount2, [4] moved
     int* heavy;
     int* flist;
+    int* flist2;
+    int* plist;
     uint32_t *gtk, *gtv;
     int gcap, hblocks;
     unsigned long long* work;
@@ -749,7 +797,9 @@ SweepBuffers make_buffers(Ctx& ctx, const DevGraph& g) {
     b.pc = A.alloc<int>(n);
     b.heavy = A.alloc<int>(n);
     b.flist = A.alloc<int>(n);
-    b.counters = A.alloc<unsigned>(4);
+    b.flist2 = A.alloc<int>(n);
+    b.plist = A.alloc<int>(n);
+    b.counters = A.alloc<unsigned>(8);
     b.work = ctx.work;
     b.err = ctx.dscalars + 60;
     b.gcap = 0;
@@ -782,7 +832,7 @@ template <int MODE>
 void launch_sweep(Ctx& ctx, const DevGraph& g, SweepArgs a, const SweepBuffers& b, double bytes) {
     const long long tasks = ((long long)g.n + 32 * kSpan - 1) / (32 * kSpan);
     const int lblocks = (int)std::max<long long>(1, std::min<long long>(div_up(tasks, kWarpsPerBlock), kNumSMs * 4LL));
-    KB_CUDA(cudaMemsetAsync(b.counters, 0, 2 * sizeof(unsigned), ctx.stream));
+    KB_CUDA(cudaMemsetAsync(b.counters, 0, 4 * sizeof(unsigned), ctx.stream));
     {
         PhaseScope ps(ctx, family(MODE, 0), bytes);
         lane_kernel<MODE><<<lblocks, kThreads, 0, ctx.stream>>>(a);
@@ -790,6 +840,9 @@ void launch_sweep(Ctx& ctx, const DevGraph& g, SweepArgs a, const SweepBuffers& 
     }
     {
         PhaseScope ps(ctx, family(MODE, 1), 0);
+        const int wblocks = (int)std::max<long long>(1, std::min<long long>(div_up(g.n, 32 * kWarpsPerBlock), kNumSMs * 3LL));
+        wide_kernel<MODE><<<wblocks, kThreads, 0, ctx.stream>>>(a);
+        KB_LAUNCH();
         const int cblocks = (int)std::max<long long>(1, std::min<long long>(div_up(g.n, 32 * kWarpsPerBlock), sweep_blocks()));
         chunk_kernel<MODE><<<cblocks, kThreads, 0, ctx.stream>>>(a);
         KB_LAUNCH();
@@ -814,6 +867,10 @@ SweepArgs base_args(const DevGraph& g, const SweepBuffers& b) {
     a.heavy = b.heavy;
     a.fcount = b.counters;
     a.flist = b.flist;
+    a.pcount = b.counters + 2;
+    a.plist = b.plist;
+    a.fcount2 = b.counters + 3;
+    a.flist2 = b.flist2;
     a.work = b.work;
     a.err = b.err;
     return a;
@@ -858,9 +915,9 @@ void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* la
             a.singletons = (r == 0 && s == 0 && sorted_rows) ? 1 : 0;
             launch_sweep<CLUSTER>(ctx, g, a, b, sweep_bytes(g, 1.0 / a.S));
             PhaseScope ps(ctx, "lp_cluster_admit", 0);
-            cluster_decide<<<dblocks, kThreads, 0, st>>>(g.n, b.pt, cw, inc, minv, a.bound);
+            cluster_decide<<<dblocks, kThreads, 0, st>>>(b.plist, a.pcount, b.pt, cw, inc, minv, a.bound);
             KB_LAUNCH();
-            cluster_apply<<<dblocks, kThreads, 0, st>>>(g.n, b.pt, g.vwgt, label, cw, inc, minv);
+            cluster_apply<<<dblocks, kThreads, 0, st>>>(b.plist, a.pcount, b.pt, g.vwgt, label, cw, inc, minv);
             KB_LAUNCH();
         }
     }
@@ -892,7 +949,7 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
     a.H = H;
     a.minvP = minvP;
     const int dblocks = (int)std::max<long long>(1, std::min<long long>(div_up(g.n, kThreads), kNumSMs * 8LL));
-    unsigned* moved = b.counters + 2;
+    unsigned* moved = b.counters + 4;
     for (int r = 0; r < kn.ref_rounds; ++r) {
         a.active = act;
         a.ks_sub = stream_key(kn.seed, TAG_RSUB, level, r);
@@ -904,10 +961,11 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
             a.s = s;
             launch_sweep<REFINE>(ctx, g, a, b, sweep_bytes(g, 1.0 / a.S));
             PhaseScope ps(ctx, "lp_refine_admit", 0);
-            class_decide<<<dblocks, kThreads, 0, st>>>(g.n, b.pt, b.pc, g.vwgt, bw, H, minvP, P, bound, 1);
+            class_decide<<<dblocks, kThreads, 0, st>>>(b.plist, a.pcount, b.pt, b.pc, g.vwgt, bw, H, minvP, P, bound,
+                                                       1);
             KB_LAUNCH();
-            class_apply<<<dblocks, kThreads, 0, st>>>(g.n, b.pt, b.pc, g.xadj, g.adjncy, g.vwgt, part, bw, H,
-                                                      minvP, P, nact, moved);
+            class_apply<<<dblocks, kThreads, 0, st>>>(b.plist, a.pcount, b.pt, b.pc, g.xadj, g.adjncy, g.vwgt, part,
+                                                      bw, H, minvP, P, nact, moved);
             KB_LAUNCH();
         }
         std::swap(act, nact);
@@ -956,12 +1014,13 @@ bool balance(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t b
         launch_sweep<BALANCE>(ctx, g, a, b, 0);
         balance_threshold<<<div_up(k, 256), 256, 0, st>>>(bw, HS, k, bound, thr);
         KB_LAUNCH();
-        balance_release<<<dblocks, kThreads, 0, st>>>(g.n, b.pt, b.pc, part, g.vwgt, thr, H, minvP, P, ks_prio);
+        balance_release<<<dblocks, kThreads, 0, st>>>(b.plist, a.pcount, b.pt, b.pc, part, g.vwgt, thr, H, minvP, P,
+                                                      ks_prio);
         KB_LAUNCH();
-        class_decide<<<dblocks, kThreads, 0, st>>>(g.n, b.pt, b.pc, g.vwgt, bw, H, minvP, P, bound, 0);
+        class_decide<<<dblocks, kThreads, 0, st>>>(b.plist, a.pcount, b.pt, b.pc, g.vwgt, bw, H, minvP, P, bound, 0);
         KB_LAUNCH();
-        class_apply<<<dblocks, kThreads, 0, st>>>(g.n, b.pt, b.pc, g.xadj, g.adjncy, g.vwgt, part, bw, H, minvP,
-                                                  P, nullptr, b.counters + 2);
+        class_apply<<<dblocks, kThreads, 0, st>>>(b.plist, a.pcount, b.pt, b.pc, g.xadj, g.adjncy, g.vwgt, part, bw,
+                                                  H, minvP, P, nullptr, b.counters + 4);
         KB_LAUNCH();
     }
     if (!ok) {
