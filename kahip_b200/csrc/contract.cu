@@ -121,25 +121,18 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(int n, const int* __rest
     }
 }
 
-// entries of vertex v move from its CSR range to voff[v] in the sort input;
-// a warp copies 32 consecutive vertices, lanes striding over each one's entries
+// entries of vertex v move from its CSR range to voff[v] in the sort input
+// (one thread per vertex; a vertex has at most a few entries)
 __global__ void compact_vertices(int n, const int* __restrict__ xadj, const uint32_t* __restrict__ vcount,
                                  const uint32_t* __restrict__ voff, const uint64_t* __restrict__ ekey,
                                  const uint32_t* __restrict__ eval, uint64_t* K, uint32_t* V) {
-    const int lane = threadIdx.x & 31;
-    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
-    const long long nwarps = (long long)gridDim.x * blockDim.x / 32;
-    for (long long c = warp; c * 32 < n; c += nwarps) {
-        const int v0 = (int)(c * 32);
-        const int vend = min(n, v0 + 32);
-        for (int v = v0; v < vend; ++v) {
-            const uint32_t cnt = vcount[v];
-            const long long src = xadj[v];
-            const long long dst = voff[v];
-            for (uint32_t i = lane; i < cnt; i += 32) {
-                K[dst + i] = ekey[src + i];
-                V[dst + i] = eval[src + i];
-            }
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const uint32_t cnt = vcount[v];
+        const long long src = xadj[v];
+        const long long dst = voff[v];
+        for (uint32_t i = 0; i < cnt; ++i) {
+            K[dst + i] = ekey[src + i];
+            V[dst + i] = eval[src + i];
         }
     }
 }
@@ -231,7 +224,7 @@ void contract(Ctx& ctx, const DevGraph& g, const int* label, int* cmap, DevGraph
     uint32_t* V1 = ctx.scratch.alloc<uint32_t>((size_t)std::max<long long>(E, 1));
     {
         PhaseScope ps(ctx, "contract_compact", 24.0 * E);
-        compact_vertices<<<kNumSMs * 8, kThreads, 0, st>>>(n, g.xadj, vcount, voff, ekey, eval, K0, V0);
+        compact_vertices<<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, vcount, voff, ekey, eval, K0, V0);
         KB_LAUNCH();
     }
     // 4. sort by (cu, cv)

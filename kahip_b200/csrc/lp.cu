@@ -33,6 +33,17 @@ constexpr int kBalClasses = 256;
 
 enum Mode { CLUSTER = 0, REFINE = 1, BALANCE = 2 };
 
+// A list filled by many warps without contention: warp w appends to stripe
+// w % kStripes through that stripe's counter.  Every stripe has a capacity
+// `cap` computed on the host from the number of warps of the producing
+// kernels and the work each warp can be given.
+constexpr int kStripes = 128;
+struct SList {
+    int* data;        // kStripes * cap entries
+    unsigned* counts; // kStripes counters
+    long long cap;
+};
+
 // Everything a sweep reads or writes; passed by value.
 struct SweepArgs {
     int n;
@@ -54,9 +65,9 @@ struct SweepArgs {
     uint32_t* H;                        // REFINE/BALANCE: weight per (target, class)
     int* minvP;                         // smallest proposer per (target, class)
     int* heavy; unsigned* hcount;       // deferred high-degree vertices
-    int* flist; unsigned* fcount;       // vertices with more distinct labels than kSlots
-    int* flist2; unsigned* fcount2;     // ... and than kSlotsWide
-    int* plist; unsigned* pcount;       // vertices that proposed a move this sub-round
+    SList flist;                        // vertices with more distinct labels than kSlots
+    SList plist;                        // vertices that proposed a move this sub-round
+    int* hplist; unsigned* hpcount;     // proposals of high-degree vertices
     int singletons;                     // every label is its own vertex id and rows have
                                         // strictly increasing targets (clustering round 0)
     unsigned long long* work;           // [0] vertices, [1] edges
@@ -157,6 +168,11 @@ __device__ bool decide_emit(const SweepArgs& a, int v, uint32_t own, uint32_t cv
     return true;
 }
 
+__device__ __forceinline__ int warp_global_id() {
+    return (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+}
+
+// warp-aggregated append to a plain list (one atomic per warp call)
 __device__ __forceinline__ void append_aggregated(bool pred, int v, int* list, unsigned* count) {
     const unsigned m = __ballot_sync(0xffffffffu, pred);
     if (!m) return;
@@ -166,6 +182,12 @@ __device__ __forceinline__ void append_aggregated(bool pred, int v, int* list, u
     if (lane == leader) base = atomicAdd(count, (unsigned)__popc(m));
     base = __shfl_sync(0xffffffffu, base, leader);
     if (pred) list[base + __popc(m & lanemask_lt())] = v;
+}
+
+// warp-aggregated append to this warp's stripe of a striped list
+__device__ __forceinline__ void append_striped(bool pred, int v, const SList& L) {
+    const int stripe = warp_global_id() % kStripes;
+    append_aggregated(pred, v, L.data + (long long)stripe * L.cap, L.counts + stripe);
 }
 
 template <int MODE>
@@ -220,14 +242,27 @@ __global__ void __launch_bounds__(kThreads) chunk_kernel(SweepArgs a) {
     if (lane == 0) T.nused = 0;
     __syncwarp();
     unsigned long long wv = 0, we = 0;
-    const unsigned count = *a.fcount2;
-    const long long nchunks = ((long long)count + 31) / 32;
+    // chunks of 32 entries over the stripes of the overflow list
+    __shared__ unsigned sprefix[kStripes + 1];
+    if (threadIdx.x == 0) {
+        unsigned run = 0;
+        for (int i = 0; i < kStripes; ++i) {
+            sprefix[i] = run;
+            run += (a.flist.counts[i] + 31u) / 32u;
+        }
+        sprefix[kStripes] = run;
+    }
+    __syncthreads();
+    const long long nchunks = sprefix[kStripes];
     const long long warp = ((long long)blockIdx.x * kThreads + threadIdx.x) / 32;
     const long long nwarps = (long long)gridDim.x * kThreads / 32;
     for (long long chunk = warp; chunk < nchunks; chunk += nwarps) {
-        const long long li = chunk * 32 + lane;
-        const bool mem = li < (long long)count;
-        const int v = mem ? a.flist2[li] : 0;
+        int stripe = 0;
+        for (int step = 64; step >= 1; step >>= 1)
+            if (stripe + step < kStripes && sprefix[stripe + step] <= chunk) stripe += step;
+        const long long li = (chunk - sprefix[stripe]) * 32 + lane;
+        const bool mem = li < (long long)a.flist.counts[stripe];
+        const int v = mem ? a.flist.data[(long long)stripe * a.flist.cap + li] : 0;
         int beg = 0, deg = 0;
         bool heavy = false;
         if (mem) {
@@ -352,7 +387,7 @@ __global__ void __launch_bounds__(kThreads) chunk_kernel(SweepArgs a) {
             if (lane == 0) T.nused = 0;
             bool prop = false;
             if (wmember) prop = decide_emit<MODE>(a, v, T.own[lane], T.cv[lane], T.cown[lane], T.bkey[lane], T.bid[lane]);
-            append_aggregated(prop, v, a.plist, a.pcount);
+            append_striped(prop, v, a.plist);
             __syncwarp();
             // next window starts at the first light lane at or after wend
             const unsigned rest = lightmask & (wend < 32 ? (~0u << wend) : 0u);
@@ -383,7 +418,6 @@ __global__ void __launch_bounds__(kThreads) chunk_kernel(SweepArgs a) {
 // to the high-degree list (heavy_kernel).
 
 constexpr int kSlots = 8;
-constexpr int kSlotsWide = 16;
 constexpr int kSpan = 4;  // chunks of 32 ids per warp task
 
 // r-th set bit (0-based) of mask
@@ -498,9 +532,9 @@ __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
     auto pass = [&](int v) {
         int status = 0;
         if (v >= 0) status = lane_vertex<MODE, kSlots>(a, v, wv, we);
-        append_aggregated(status == 1, v, a.flist, a.fcount);
+        append_striped(status == 1, v, a.flist);
         append_aggregated(status == 2, v, a.heavy, a.hcount);
-        append_aggregated(status == 3, v, a.plist, a.pcount);
+        append_striped(status == 3, v, a.plist);
     };
     for (long long task = warp; task < ntasks; task += nwarps) {
         const long long base = task * span;
@@ -532,33 +566,6 @@ __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
     if (lane == 0 && (wv | we)) {
         atomicAdd(&a.work[0], wv);
         atomicAdd(&a.work[1], we);
-    }
-}
-
-// Second tier: the overflow list of the lane kernel with kSlotsWide slots.
-template <int MODE>
-__global__ void __launch_bounds__(kThreads, 3) wide_kernel(SweepArgs a) {
-    const int lane = threadIdx.x & 31;
-    unsigned long long wv = 0, we = 0;
-    const unsigned count = *a.fcount;
-    const long long warp = ((long long)blockIdx.x * kThreads + threadIdx.x) / 32;
-    const long long nwarps = (long long)gridDim.x * kThreads / 32;
-    for (long long base = warp * 32; base < count; base += nwarps * 32) {
-        const int v = base + lane < count ? a.flist[base + lane] : -1;
-        int status = 0;
-        if (v >= 0) status = lane_vertex<MODE, kSlotsWide>(a, v, wv, we);
-        append_aggregated(status == 1, v, a.flist2, a.fcount2);
-        append_aggregated(status == 3, v, a.plist, a.pcount);
-    }
-#pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) {
-        wv += __shfl_xor_sync(0xffffffffu, wv, o);
-        we += __shfl_xor_sync(0xffffffffu, we, o);
-    }
-    if (lane == 0 && (wv | we)) {
-        atomicAdd(&a.work[0], wv);
-        atomicAdd(&a.work[1], we);
-        atomicAdd(&a.work[2], wv);
     }
 }
 
@@ -612,7 +619,7 @@ __global__ void __launch_bounds__(kThreads) heavy_kernel(SweepArgs a, uint32_t* 
         __syncthreads();
         if (threadIdx.x == 0) {
             for (int j = 1; j < kThreads / 32; ++j) better(key, id, sk[j], sid[j]);
-            if (decide_emit<MODE>(a, v, own, cv, sco, key, id)) a.plist[atomicAdd(a.pcount, 1u)] = v;
+            if (decide_emit<MODE>(a, v, own, cv, sco, key, id)) a.hplist[atomicAdd(a.hpcount, 1u)] = v;
         }
         __syncthreads();
     }
@@ -620,16 +627,27 @@ __global__ void __launch_bounds__(kThreads) heavy_kernel(SweepArgs a, uint32_t* 
 
 // ---------------------------------------------------------------- admission
 
+// Iterates the proposals of a sub-round: the stripes of the lane/chunk list
+// plus the high-degree list (treated as stripe kStripes).  Blocks take
+// stripes round-robin; the threads of the blocks sharing a stripe stride over
+// its entries.  The body's `continue` moves on to the next proposal.
+// The grid must be a multiple of kStripes + 1 blocks (admit_blocks()).
+#define FOR_EACH_PROPOSAL(pl, hpl, hpc, v)                                                              \
+    for (unsigned s_ = blockIdx.x % (kStripes + 1), G_ = gridDim.x / (kStripes + 1),                   \
+                  i_ = (blockIdx.x / (kStripes + 1)) * blockDim.x + threadIdx.x,                       \
+                  n_ = s_ < kStripes ? (pl).counts[s_] : *(hpc);                                       \
+         i_ < n_; i_ += G_ * blockDim.x)                                                               \
+        for (int v = s_ < kStripes ? (pl).data[(long long)s_ * (pl).cap + i_] : (hpl)[i_], once_ = 1;     \
+             once_; once_ = 0)
+
 // Proposal encoding per vertex: pt[v] = target (>= 0), -1 = no proposal,
 // -2 - target = rejected (its accumulators still need resetting).
 
 // Clustering: all proposals into b are admitted if they fit together;
 // otherwise only the smallest proposer (which fits by itself).
-__global__ void cluster_decide(const int* plist, const unsigned* pcount, int* pt, const uint32_t* cw,
+__global__ void cluster_decide(SList pl, const int* hpl, const unsigned* hpc, int* pt, const uint32_t* cw,
                                const uint32_t* inc, const int* minv, uint32_t bound) {
-    const unsigned cnt = *pcount;
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
-        const int v = plist[i];
+    FOR_EACH_PROPOSAL(pl, hpl, hpc, v) {
         int b = pt[v];
         if (b < 0) continue;
         bool ok = ((uint64_t)cw[b] + inc[b] < bound) || minv[b] == v;
@@ -637,11 +655,9 @@ __global__ void cluster_decide(const int* plist, const unsigned* pcount, int* pt
     }
 }
 
-__global__ void cluster_apply(const int* plist, const unsigned* pcount, const int* pt, const int* vwgt, int* label,
-                              uint32_t* cw, uint32_t* inc, int* minv) {
-    const unsigned cnt = *pcount;
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
-        const int v = plist[i];
+__global__ void cluster_apply(SList pl, const int* hpl, const unsigned* hpc, const int* pt, const int* vwgt,
+                              int* label, uint32_t* cw, uint32_t* inc, int* minv) {
+    FOR_EACH_PROPOSAL(pl, hpl, hpc, v) {
         int t = pt[v];
         if (t == -1) continue;
         int b = t >= 0 ? t : -2 - t;
@@ -670,12 +686,10 @@ __device__ __forceinline__ bool admit(const uint32_t* H, const int* minvP, int P
 
 // strict: cap = bound - 1 - w[b] (refinement keeps blocks < bound);
 // otherwise cap = bound - w[b] (balance repair fills up to bound)
-__global__ void class_decide(const int* plist, const unsigned* pcount, int* pt, const int* pc, const int* vwgt,
-                             const uint32_t* bw, const uint32_t* H, const int* minvP, int P, uint32_t bound,
-                             int strict) {
-    const unsigned cnt = *pcount;
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
-        const int v = plist[i];
+__global__ void class_decide(SList pl, const int* hpl, const unsigned* hpc, int* pt, const int* pc,
+                             const int* vwgt, const uint32_t* bw, const uint32_t* H, const int* minvP, int P,
+                             uint32_t bound, int strict) {
+    FOR_EACH_PROPOSAL(pl, hpl, hpc, v) {
         int b = pt[v];
         if (b < 0) continue;
         int c = pc[v];
@@ -685,13 +699,11 @@ __global__ void class_decide(const int* plist, const unsigned* pcount, int* pt, 
     }
 }
 
-__global__ void class_apply(const int* plist, const unsigned* pcount, const int* pt, const int* pc,
+__global__ void class_apply(SList pl, const int* hpl, const unsigned* hpc, const int* pt, const int* pc,
                             const int* xadj, const int* adjncy, const int* vwgt, int* part, uint32_t* bw,
                             uint32_t* H, int* minvP, int P, uint8_t* next_active, unsigned* moved) {
     unsigned mv = 0;
-    const unsigned cnt = *pcount;
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
-        const int v = plist[i];
+    FOR_EACH_PROPOSAL(pl, hpl, hpc, v) {
         int t = pt[v];
         if (t == -1) continue;
         int c = pc[v];
@@ -726,12 +738,10 @@ __global__ void balance_threshold(const uint32_t* bw, const uint32_t* HS, int k,
 }
 
 // Balance: released candidates get an admission class; others are dropped.
-__global__ void balance_release(const int* plist, const unsigned* pcount, const int* pt, int* pc, const int* part,
-                                const int* vwgt, const int* thr, uint32_t* H, int* minvP, int P,
+__global__ void balance_release(SList pl, const int* hpl, const unsigned* hpc, const int* pt, int* pc,
+                                const int* part, const int* vwgt, const int* thr, uint32_t* H, int* minvP, int P,
                                 uint64_t ks_prio) {
-    const unsigned cnt = *pcount;
-    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
-        const int v = plist[i];
+    FOR_EACH_PROPOSAL(pl, hpl, hpc, v) {
         int t = pt[v];
         if (t < 0) continue;
         if (pc[v] >= thr[part[v]]) { pc[v] = -1; continue; }
@@ -778,28 +788,42 @@ int sweep_blocks() { return kNumSMs * 5; }  // 48 registers, 32 KB shared: 5 blo
 
 struct SweepBuffers {
     int *pt, *pc;
-    unsigned* counters;  // [0] fcount, [1] hcount, [2] pcount, [3] fcount2, [4] moved
+    unsigned* counters;  // [0, kStripes) overflow, [kStripes, 2 kStripes) proposals,
+                         // [2 kStripes] heavy, [+1] heavy proposals, [+2] moved
     int* heavy;
-    int* flist;
-    int* flist2;
-    int* plist;
+    int* hplist;
+    SList flist, plist;
+    int lblocks, cblocks;
     uint32_t *gtk, *gtv;
     int gcap, hblocks;
     unsigned long long* work;
     int* err;
 };
 
+constexpr int kCntHeavy = 2 * kStripes, kCntHeavyProp = 2 * kStripes + 1, kCntMoved = 2 * kStripes + 2;
+
+int admit_blocks() { return (kStripes + 1) * 4; }
+
 SweepBuffers make_buffers(Ctx& ctx, const DevGraph& g) {
     SweepBuffers b;
     Arena& A = ctx.scratch;
-    size_t n = (size_t)std::max(g.n, 1);
-    b.pt = A.alloc<int>(n);
-    b.pc = A.alloc<int>(n);
-    b.heavy = A.alloc<int>(n);
-    b.flist = A.alloc<int>(n);
-    b.flist2 = A.alloc<int>(n);
-    b.plist = A.alloc<int>(n);
-    b.counters = A.alloc<unsigned>(8);
+    const long long n = std::max(g.n, 1);
+    b.pt = A.alloc<int>((size_t)n);
+    b.pc = A.alloc<int>((size_t)n);
+    b.heavy = A.alloc<int>((size_t)n);
+    b.hplist = A.alloc<int>((size_t)n);
+    b.counters = A.alloc<unsigned>(2 * kStripes + 8);
+    // stripe capacities from the producers' warp counts and per-warp work
+    const long long tasks = (n + 32 * kSpan - 1) / (32 * kSpan);
+    b.lblocks = (int)std::max<long long>(1, std::min<long long>(div_up(tasks, kWarpsPerBlock), kNumSMs * 4LL));
+    const long long wl = (long long)b.lblocks * kWarpsPerBlock;
+    const long long cap_l = ((wl + kStripes - 1) / kStripes) * ((tasks + wl - 1) / wl) * 32 * kSpan;
+    b.cblocks = (int)std::max<long long>(1, std::min<long long>(div_up(n, 32 * kWarpsPerBlock), sweep_blocks()));
+    const long long wc = (long long)b.cblocks * kWarpsPerBlock;
+    const long long chunks_max = (n + 31) / 32 + kStripes;
+    const long long cap_c = ((wc + kStripes - 1) / kStripes) * ((chunks_max + wc - 1) / wc) * 32;
+    b.flist = SList{A.alloc<int>((size_t)(kStripes * cap_l)), b.counters, cap_l};
+    b.plist = SList{A.alloc<int>((size_t)(kStripes * (cap_l + cap_c))), b.counters + kStripes, cap_l + cap_c};
     b.work = ctx.work;
     b.err = ctx.dscalars + 60;
     b.gcap = 0;
@@ -830,21 +854,15 @@ const char* family(int mode, int part) {
 
 template <int MODE>
 void launch_sweep(Ctx& ctx, const DevGraph& g, SweepArgs a, const SweepBuffers& b, double bytes) {
-    const long long tasks = ((long long)g.n + 32 * kSpan - 1) / (32 * kSpan);
-    const int lblocks = (int)std::max<long long>(1, std::min<long long>(div_up(tasks, kWarpsPerBlock), kNumSMs * 4LL));
-    KB_CUDA(cudaMemsetAsync(b.counters, 0, 4 * sizeof(unsigned), ctx.stream));
+    KB_CUDA(cudaMemsetAsync(b.counters, 0, sizeof(unsigned) * kCntMoved, ctx.stream));
     {
         PhaseScope ps(ctx, family(MODE, 0), bytes);
-        lane_kernel<MODE><<<lblocks, kThreads, 0, ctx.stream>>>(a);
+        lane_kernel<MODE><<<b.lblocks, kThreads, 0, ctx.stream>>>(a);
         KB_LAUNCH();
     }
     {
         PhaseScope ps(ctx, family(MODE, 1), 0);
-        const int wblocks = (int)std::max<long long>(1, std::min<long long>(div_up(g.n, 32 * kWarpsPerBlock), kNumSMs * 3LL));
-        wide_kernel<MODE><<<wblocks, kThreads, 0, ctx.stream>>>(a);
-        KB_LAUNCH();
-        const int cblocks = (int)std::max<long long>(1, std::min<long long>(div_up(g.n, 32 * kWarpsPerBlock), sweep_blocks()));
-        chunk_kernel<MODE><<<cblocks, kThreads, 0, ctx.stream>>>(a);
+        chunk_kernel<MODE><<<b.cblocks, kThreads, 0, ctx.stream>>>(a);
         KB_LAUNCH();
     }
     if (b.gcap > 0) {
@@ -863,14 +881,12 @@ SweepArgs base_args(const DevGraph& g, const SweepBuffers& b) {
     a.vwgt = g.vwgt;
     a.pt = b.pt;
     a.pc = b.pc;
-    a.hcount = b.counters + 1;
+    a.hcount = b.counters + kCntHeavy;
     a.heavy = b.heavy;
-    a.fcount = b.counters;
     a.flist = b.flist;
-    a.pcount = b.counters + 2;
     a.plist = b.plist;
-    a.fcount2 = b.counters + 3;
-    a.flist2 = b.flist2;
+    a.hplist = b.hplist;
+    a.hpcount = b.counters + kCntHeavyProp;
     a.work = b.work;
     a.err = b.err;
     return a;
@@ -903,7 +919,6 @@ void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* la
     a.S = (uint32_t)kn.lpc_subrounds;
     a.inc = inc;
     a.minv = minv;
-    const int dblocks = (int)std::max<long long>(1, std::min<long long>(div_up(g.n, kThreads), kNumSMs * 8LL));
     const bool sorted_rows = rows_strictly_increasing(ctx, g);
     for (int r = 0; r < kn.lpc_rounds; ++r) {
         a.ks_sub = stream_key(kn.seed, TAG_CSUB, level, r);
@@ -915,9 +930,11 @@ void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* la
             a.singletons = (r == 0 && s == 0 && sorted_rows) ? 1 : 0;
             launch_sweep<CLUSTER>(ctx, g, a, b, sweep_bytes(g, 1.0 / a.S));
             PhaseScope ps(ctx, "lp_cluster_admit", 0);
-            cluster_decide<<<dblocks, kThreads, 0, st>>>(b.plist, a.pcount, b.pt, cw, inc, minv, a.bound);
+            cluster_decide<<<admit_blocks(), kThreads, 0, st>>>(b.plist, b.hplist, a.hpcount, b.pt, cw, inc, minv,
+                                                                a.bound);
             KB_LAUNCH();
-            cluster_apply<<<dblocks, kThreads, 0, st>>>(b.plist, a.pcount, b.pt, g.vwgt, label, cw, inc, minv);
+            cluster_apply<<<admit_blocks(), kThreads, 0, st>>>(b.plist, b.hplist, a.hpcount, b.pt, g.vwgt, label, cw,
+                                                               inc, minv);
             KB_LAUNCH();
         }
     }
@@ -948,8 +965,7 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
     a.P = P;
     a.H = H;
     a.minvP = minvP;
-    const int dblocks = (int)std::max<long long>(1, std::min<long long>(div_up(g.n, kThreads), kNumSMs * 8LL));
-    unsigned* moved = b.counters + 4;
+    unsigned* moved = b.counters + kCntMoved;
     for (int r = 0; r < kn.ref_rounds; ++r) {
         a.active = act;
         a.ks_sub = stream_key(kn.seed, TAG_RSUB, level, r);
@@ -961,11 +977,11 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
             a.s = s;
             launch_sweep<REFINE>(ctx, g, a, b, sweep_bytes(g, 1.0 / a.S));
             PhaseScope ps(ctx, "lp_refine_admit", 0);
-            class_decide<<<dblocks, kThreads, 0, st>>>(b.plist, a.pcount, b.pt, b.pc, g.vwgt, bw, H, minvP, P, bound,
-                                                       1);
+            class_decide<<<admit_blocks(), kThreads, 0, st>>>(b.plist, b.hplist, a.hpcount, b.pt, b.pc, g.vwgt, bw,
+                                                              H, minvP, P, bound, 1);
             KB_LAUNCH();
-            class_apply<<<dblocks, kThreads, 0, st>>>(b.plist, a.pcount, b.pt, b.pc, g.xadj, g.adjncy, g.vwgt, part,
-                                                      bw, H, minvP, P, nact, moved);
+            class_apply<<<admit_blocks(), kThreads, 0, st>>>(b.plist, b.hplist, a.hpcount, b.pt, b.pc, g.xadj,
+                                                             g.adjncy, g.vwgt, part, bw, H, minvP, P, nact, moved);
             KB_LAUNCH();
         }
         std::swap(act, nact);
@@ -998,7 +1014,6 @@ bool balance(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t b
     a.P = P;
     a.HS = HS;
     a.lightest = flags;
-    const int dblocks = (int)std::max<long long>(1, std::min<long long>(div_up(g.n, kThreads), kNumSMs * 8LL));
     bool ok = false;
     for (int it = 0; it < kn.bal_iters; ++it) {
         block_scan_kernel<<<1, 1024, 0, st>>>(bw, k, bound, flags, flags + 1);
@@ -1014,13 +1029,14 @@ bool balance(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t b
         launch_sweep<BALANCE>(ctx, g, a, b, 0);
         balance_threshold<<<div_up(k, 256), 256, 0, st>>>(bw, HS, k, bound, thr);
         KB_LAUNCH();
-        balance_release<<<dblocks, kThreads, 0, st>>>(b.plist, a.pcount, b.pt, b.pc, part, g.vwgt, thr, H, minvP, P,
-                                                      ks_prio);
+        balance_release<<<admit_blocks(), kThreads, 0, st>>>(b.plist, b.hplist, a.hpcount, b.pt, b.pc, part, g.vwgt,
+                                                             thr, H, minvP, P, ks_prio);
         KB_LAUNCH();
-        class_decide<<<dblocks, kThreads, 0, st>>>(b.plist, a.pcount, b.pt, b.pc, g.vwgt, bw, H, minvP, P, bound, 0);
+        class_decide<<<admit_blocks(), kThreads, 0, st>>>(b.plist, b.hplist, a.hpcount, b.pt, b.pc, g.vwgt, bw, H,
+                                                          minvP, P, bound, 0);
         KB_LAUNCH();
-        class_apply<<<dblocks, kThreads, 0, st>>>(b.plist, a.pcount, b.pt, b.pc, g.xadj, g.adjncy, g.vwgt, part, bw,
-                                                  H, minvP, P, nullptr, b.counters + 4);
+        class_apply<<<admit_blocks(), kThreads, 0, st>>>(b.plist, b.hplist, a.hpcount, b.pt, b.pc, g.xadj, g.adjncy,
+                                                         g.vwgt, part, bw, H, minvP, P, nullptr, b.counters + kCntMoved);
         KB_LAUNCH();
     }
     if (!ok) {
