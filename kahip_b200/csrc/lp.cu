@@ -65,7 +65,6 @@ struct SweepArgs {
     uint32_t* H;                        // REFINE/BALANCE: weight per (target, class)
     int* minvP;                         // smallest proposer per (target, class)
     int* heavy; unsigned* hcount;       // deferred high-degree vertices
-    SList flist;                        // vertices with more distinct labels than kSlots
     SList plist;                        // vertices that proposed a move this sub-round
     int* hplist; unsigned* hpcount;     // proposals of high-degree vertices
     int singletons;                     // every label is its own vertex id and rows have
@@ -197,16 +196,7 @@ __device__ __forceinline__ bool member(const SweepArgs& a, int v) {
     return hash_range(hash32(a.ks_sub, (uint32_t)v), a.S) == a.s;
 }
 
-// ------------------------------------------------ chunk-cooperative sweep
-//
-// A warp owns 32 consecutive vertex ids.  Members of the sub-round with
-// degree <= kWin are laid out back to back (warp prefix sum of degrees) and
-// processed in windows of at most kWin edges: every lane takes one edge slot
-// per 32-edge batch, all adjacency loads of a window are issued before the
-// label gathers, (member, label) pairs are merged with a 64-bit match_any and
-// summed into a per-warp shared hash table; each member's best candidate is
-// then found with shared-memory atomicMax / atomicMin.  Members of degree
-// > kWin go to the block-per-vertex kernel.
+// ------------------------------------------------ chunk-cooperative path
 
 constexpr int kWin = 128;                 // edges per window (<= 4 batches)
 constexpr int kBatches = kWin / 32;
@@ -230,180 +220,148 @@ __device__ __forceinline__ uint32_t slot64(unsigned long long k) {
     return (uint32_t)((k * 0x9E3779B97F4A7C15ull) >> (64 - 8)) & (kTab - 1);  // kTab == 256
 }
 
-// Processes the vertices of a list (the lane kernel's overflow list): every
-// listed vertex is a member of the current sub-round.
+// Decides up to 32 vertices (lane i: vertex v when mem) with the per-warp
+// shared table: the members' edges are laid back to back (warp prefix sum of
+// degrees) and processed in windows of at most kWin edges; every lane takes
+// one edge slot per 32-edge batch, all adjacency loads of a window are issued
+// before the label gathers, (member, label) pairs are merged with a 64-bit
+// match_any and summed into the table, and each member's best candidate is
+// found with shared-memory atomicMax / atomicMin.  Used for the vertices
+// whose neighbours carry more distinct labels than the lane path's slots.
 template <int MODE>
-__global__ void __launch_bounds__(kThreads) chunk_kernel(SweepArgs a) {
-    static_assert(kTab == 256, "slot64 assumes 256 slots");
-    __shared__ WarpTable tabs[kWarpsPerBlock];
+__device__ void chunk_process(const SweepArgs& a, WarpTable& T, bool mem, int v, unsigned long long& wv,
+                              unsigned long long& we, unsigned long long& wo) {
     const int lane = threadIdx.x & 31;
-    WarpTable& T = tabs[threadIdx.x >> 5];
-    for (int i = lane; i < kTab; i += 32) { T.key[i] = kEmpty64; T.val[i] = 0; }
-    if (lane == 0) T.nused = 0;
-    __syncwarp();
-    unsigned long long wv = 0, we = 0;
-    // chunks of 32 entries over the stripes of the overflow list
-    __shared__ unsigned sprefix[kStripes + 1];
-    if (threadIdx.x == 0) {
-        unsigned run = 0;
-        for (int i = 0; i < kStripes; ++i) {
-            sprefix[i] = run;
-            run += (a.flist.counts[i] + 31u) / 32u;
+    int beg = 0, deg = 0;
+    bool heavy = false;
+    if (mem) {
+        beg = a.xadj[v];
+        deg = a.xadj[v + 1] - beg;
+        if (deg > kWin) {  // high degree: block-per-vertex kernel decides it
+            a.heavy[atomicAdd(a.hcount, 1u)] = v;
+            deg = 0;
+            heavy = true;
+        } else {
+            wv += 1;
+            we += (unsigned long long)deg;
+            wo += 1;
         }
-        sprefix[kStripes] = run;
+        T.own[lane] = (uint32_t)a.lab[v];
+        T.cv[lane] = (uint32_t)a.vwgt[v];
     }
-    __syncthreads();
-    const long long nchunks = sprefix[kStripes];
-    const long long warp = ((long long)blockIdx.x * kThreads + threadIdx.x) / 32;
-    const long long nwarps = (long long)gridDim.x * kThreads / 32;
-    for (long long chunk = warp; chunk < nchunks; chunk += nwarps) {
-        int stripe = 0;
-        for (int step = 64; step >= 1; step >>= 1)
-            if (stripe + step < kStripes && sprefix[stripe + step] <= chunk) stripe += step;
-        const long long li = (chunk - sprefix[stripe]) * 32 + lane;
-        const bool mem = li < (long long)a.flist.counts[stripe];
-        const int v = mem ? a.flist.data[(long long)stripe * a.flist.cap + li] : 0;
-        int beg = 0, deg = 0;
-        bool heavy = false;
-        if (mem) {
-            beg = a.xadj[v];
-            deg = a.xadj[v + 1] - beg;
-            if (deg > kWin) {  // high degree: block-per-vertex kernel decides it
-                a.heavy[atomicAdd(a.hcount, 1u)] = v;
-                deg = 0;
-                heavy = true;
-            } else {
-                wv += 1;
-                we += (unsigned long long)deg;
-            }
-            T.own[lane] = (uint32_t)a.lab[v];
-            T.cv[lane] = (uint32_t)a.vwgt[v];
+    const bool light = mem && !heavy;
+    // inclusive prefix sum of degrees over the chunk
+    int incl = deg;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const int off = incl - deg;
+    const unsigned lightmask = __ballot_sync(0xffffffffu, light);
+    if (!lightmask) return;
+    int wstart = __ffs(lightmask) - 1;
+    while (wstart < 32) {
+        // window: lanes [wstart, wend) whose edges fit into kWin slots
+        const int base = __shfl_sync(0xffffffffu, off, wstart);
+        const bool inwin = lane >= wstart && incl - base <= kWin;
+        const unsigned wmask = __ballot_sync(0xffffffffu, inwin);
+        const int wend = 32 - __clz(wmask);
+        const int E = __shfl_sync(0xffffffffu, incl, wend - 1) - base;
+        const bool wmember = light && lane >= wstart && lane < wend;
+        if (wmember) {
+            T.bkey[lane] = 0;
+            T.bid[lane] = kEmpty;
+            T.cown[lane] = 0;
         }
-        const bool light = mem && !heavy;
-        // inclusive prefix sum of degrees over the chunk
-        int incl = deg;
+        // gather the window's edges: all adjacency loads, then all labels
+        int own_lane[kBatches];
+        int tgt[kBatches];
+        uint32_t wgt[kBatches];
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
+        for (int b = 0; b < kBatches; ++b) {
+            const int q = b * 32 + lane;
+            // largest window lane o with off[o] - base <= q (binary lifting)
+            int o = wstart;
+#pragma unroll
+            for (int step = 16; step >= 1; step >>= 1) {
+                const int c = o + step;
+                const int oc = __shfl_sync(0xffffffffu, off, c < 32 ? c : 31) - base;
+                if (c < wend && oc <= q) o = c;
+            }
+            const int ob = __shfl_sync(0xffffffffu, beg, o);
+            const int oo = __shfl_sync(0xffffffffu, off, o) - base;
+            own_lane[b] = o;
+            tgt[b] = -1;
+            wgt[b] = 0;
+            if (q < E) {
+                const int e = ob + (q - oo);
+                tgt[b] = a.adjncy[e];
+                wgt[b] = (uint32_t)a.adjwgt[e];
+            }
         }
-        const int off = incl - deg;
-        const unsigned lightmask = __ballot_sync(0xffffffffu, light);
-        if (!lightmask) continue;
-        int wstart = __ffs(lightmask) - 1;
-        while (wstart < 32) {
-            // window: lanes [wstart, wend) whose edges fit into kWin slots
-            const int base = __shfl_sync(0xffffffffu, off, wstart);
-            const bool inwin = lane >= wstart && incl - base <= kWin;
-            const unsigned wmask = __ballot_sync(0xffffffffu, inwin);
-            const int wend = 32 - __clz(wmask);
-            const int E = __shfl_sync(0xffffffffu, incl, wend - 1) - base;
-            const bool wmember = light && lane >= wstart && lane < wend;
-            if (wmember) {
-                T.bkey[lane] = 0;
-                T.bid[lane] = kEmpty;
-                T.cown[lane] = 0;
-            }
-            // gather the window's edges: all adjacency loads, then all labels
-            int own_lane[kBatches];
-            int tgt[kBatches];
-            uint32_t wgt[kBatches];
 #pragma unroll
-            for (int b = 0; b < kBatches; ++b) {
-                const int q = b * 32 + lane;
-                // largest window lane o with off[o] - base <= q (binary lifting)
-                int o = wstart;
+        for (int b = 0; b < kBatches; ++b)
+            if (tgt[b] >= 0) tgt[b] = a.lab[tgt[b]];
 #pragma unroll
-                for (int step = 16; step >= 1; step >>= 1) {
-                    const int c = o + step;
-                    const int oc = __shfl_sync(0xffffffffu, off, c < 32 ? c : 31) - base;
-                    if (c < wend && oc <= q) o = c;
-                }
-                const int ob = __shfl_sync(0xffffffffu, beg, o);
-                const int oo = __shfl_sync(0xffffffffu, off, o) - base;
-                own_lane[b] = o;
-                tgt[b] = -1;
-                wgt[b] = 0;
-                if (q < E) {
-                    const int e = ob + (q - oo);
-                    tgt[b] = a.adjncy[e];
-                    wgt[b] = (uint32_t)a.adjwgt[e];
-                }
-            }
-#pragma unroll
-            for (int b = 0; b < kBatches; ++b)
-                if (tgt[b] >= 0) tgt[b] = a.lab[tgt[b]];
-#pragma unroll
-            for (int b = 0; b < kBatches; ++b) {
-                if (b * 32 >= E) break;
-                const bool ok = tgt[b] >= 0;
-                const unsigned long long key =
-                    ok ? (((unsigned long long)own_lane[b] << 32) | (uint32_t)tgt[b]) : kEmpty64;
-                const unsigned peers = __match_any_sync(0xffffffffu, key);
-                const uint32_t sum = __reduce_add_sync(peers, wgt[b]);
-                if (ok && (peers & lanemask_lt()) == 0) {
-                    uint32_t sl = slot64(key);
-                    for (int probe = 0; probe < kTab; ++probe) {
-                        const unsigned long long prev = atomicCAS(&T.key[sl], kEmpty64, key);
-                        if (prev == kEmpty64) {
-                            T.used[atomicAdd(&T.nused, 1u)] = (uint16_t)sl;
-                            atomicAdd(&T.val[sl], sum);
-                            break;
-                        }
-                        if (prev == key) {
-                            atomicAdd(&T.val[sl], sum);
-                            break;
-                        }
-                        sl = (sl + 1) & (kTab - 1);
-                        if (probe == kTab - 1) atomicOr(a.err, 1);
+        for (int b = 0; b < kBatches; ++b) {
+            if (b * 32 >= E) break;
+            const bool ok = tgt[b] >= 0;
+            const unsigned long long key =
+                ok ? (((unsigned long long)own_lane[b] << 32) | (uint32_t)tgt[b]) : kEmpty64;
+            const unsigned peers = __match_any_sync(0xffffffffu, key);
+            const uint32_t sum = __reduce_add_sync(peers, wgt[b]);
+            if (ok && (peers & lanemask_lt()) == 0) {
+                uint32_t sl = slot64(key);
+                for (int probe = 0; probe < kTab; ++probe) {
+                    const unsigned long long prev = atomicCAS(&T.key[sl], kEmpty64, key);
+                    if (prev == kEmpty64) {
+                        T.used[atomicAdd(&T.nused, 1u)] = (uint16_t)sl;
+                        atomicAdd(&T.val[sl], sum);
+                        break;
                     }
+                    if (prev == key) {
+                        atomicAdd(&T.val[sl], sum);
+                        break;
+                    }
+                    sl = (sl + 1) & (kTab - 1);
+                    if (probe == kTab - 1) atomicOr(a.err, 1);
                 }
-                __syncwarp();
-            }
-            // per member: connection to its own label and the best candidate
-            const uint32_t nused = T.nused;
-            for (uint32_t i = lane; i < nused; i += 32) {
-                const uint32_t sl = T.used[i];
-                const unsigned long long k = T.key[sl];
-                const int o = (int)(k >> 32);
-                const uint32_t l = (uint32_t)k;
-                const uint32_t c = T.val[sl];
-                if (l == T.own[o]) T.cown[o] = c;
-                else if (cand_ok<MODE>(a, l, c, T.cv[o])) atomicMax(&T.bkey[o], cand_key(c, a.ks_tie, l));
             }
             __syncwarp();
-            for (uint32_t i = lane; i < nused; i += 32) {
-                const uint32_t sl = T.used[i];
-                const unsigned long long k = T.key[sl];
-                const int o = (int)(k >> 32);
-                const uint32_t l = (uint32_t)k;
-                const uint32_t c = T.val[sl];
-                if (l != T.own[o] && cand_ok<MODE>(a, l, c, T.cv[o]) && cand_key(c, a.ks_tie, l) == T.bkey[o])
-                    atomicMin(&T.bid[o], l);
-                T.key[sl] = kEmpty64;
-                T.val[sl] = 0;
-            }
-            __syncwarp();
-            if (lane == 0) T.nused = 0;
-            bool prop = false;
-            if (wmember) prop = decide_emit<MODE>(a, v, T.own[lane], T.cv[lane], T.cown[lane], T.bkey[lane], T.bid[lane]);
-            append_striped(prop, v, a.plist);
-            __syncwarp();
-            // next window starts at the first light lane at or after wend
-            const unsigned rest = lightmask & (wend < 32 ? (~0u << wend) : 0u);
-            wstart = rest ? __ffs(rest) - 1 : 32;
         }
-    }
-    // one atomic per warp for the work counters
-#pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) {
-        wv += __shfl_xor_sync(0xffffffffu, wv, o);
-        we += __shfl_xor_sync(0xffffffffu, we, o);
-    }
-    if (lane == 0 && (wv | we)) {
-        atomicAdd(&a.work[0], wv);
-        atomicAdd(&a.work[1], we);
-        atomicAdd(&a.work[2], wv);  // vertices that needed the overflow path
+        // per member: connection to its own label and the best candidate
+        const uint32_t nused = T.nused;
+        for (uint32_t i = lane; i < nused; i += 32) {
+            const uint32_t sl = T.used[i];
+            const unsigned long long k = T.key[sl];
+            const int o = (int)(k >> 32);
+            const uint32_t l = (uint32_t)k;
+            const uint32_t c = T.val[sl];
+            if (l == T.own[o]) T.cown[o] = c;
+            else if (cand_ok<MODE>(a, l, c, T.cv[o])) atomicMax(&T.bkey[o], cand_key(c, a.ks_tie, l));
+        }
+        __syncwarp();
+        for (uint32_t i = lane; i < nused; i += 32) {
+            const uint32_t sl = T.used[i];
+            const unsigned long long k = T.key[sl];
+            const int o = (int)(k >> 32);
+            const uint32_t l = (uint32_t)k;
+            const uint32_t c = T.val[sl];
+            if (l != T.own[o] && cand_ok<MODE>(a, l, c, T.cv[o]) && cand_key(c, a.ks_tie, l) == T.bkey[o])
+                atomicMin(&T.bid[o], l);
+            T.key[sl] = kEmpty64;
+            T.val[sl] = 0;
+        }
+        __syncwarp();
+        if (lane == 0) T.nused = 0;
+        bool prop = false;
+        if (wmember) prop = decide_emit<MODE>(a, v, T.own[lane], T.cv[lane], T.cown[lane], T.bkey[lane], T.bid[lane]);
+        append_striped(prop, v, a.plist);
+        __syncwarp();
+        // next window starts at the first light lane at or after wend
+        const unsigned rest = lightmask & (wend < 32 ? (~0u << wend) : 0u);
+        wstart = rest ? __ffs(rest) - 1 : 32;
     }
 }
 
@@ -414,8 +372,8 @@ __global__ void __launch_bounds__(kThreads) chunk_kernel(SweepArgs a) {
 // vertex's neighbourhood in kSlots register slots (connection per label; the
 // own label is kept apart), four edges at a time with all loads issued
 // before use.  A vertex whose neighbours carry more distinct labels than
-// slots goes to the overflow list (chunk_kernel); one of degree > kWin goes
-// to the high-degree list (heavy_kernel).
+// slots is queued per warp and decided by chunk_process in the same kernel;
+// one of degree > kWin goes to the high-degree list (heavy_kernel).
 
 constexpr int kSlots = 8;
 constexpr int kSpan = 4;  // chunks of 32 ids per warp task
@@ -518,23 +476,44 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
 
 template <int MODE>
 __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
+    static_assert(kTab == 256, "slot64 assumes 256 slots");
     // per-warp queue of members still to be processed, so that every pass
-    // over the lanes is full
+    // over the lanes is full, and of vertices that overflowed the slots
     __shared__ int queue[kWarpsPerBlock][32 * kSpan + 32];
+    __shared__ int oqueue[kWarpsPerBlock][64];
+    __shared__ WarpTable tabs[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
     int* q = queue[threadIdx.x >> 5];
-    int qn = 0;  // warp-uniform
-    unsigned long long wv = 0, we = 0;
+    int* oq = oqueue[threadIdx.x >> 5];
+    WarpTable& T = tabs[threadIdx.x >> 5];
+    for (int i = lane; i < kTab; i += 32) { T.key[i] = kEmpty64; T.val[i] = 0; }
+    if (lane == 0) T.nused = 0;
+    __syncwarp();
+    int qn = 0, oqn = 0;  // warp-uniform
+    unsigned long long wv = 0, we = 0, wo = 0;
     const long long span = 32LL * kSpan;
     const long long ntasks = ((long long)a.n + span - 1) / span;
     const long long warp = ((long long)blockIdx.x * kThreads + threadIdx.x) / 32;
     const long long nwarps = (long long)gridDim.x * kThreads / 32;
+    auto overflow_pass = [&]() {
+        const bool mem = lane < oqn && lane < 32;
+        const int v = mem ? oq[lane] : 0;
+        __syncwarp();
+        for (int i = lane; i + 32 < oqn; i += 32) oq[i] = oq[i + 32];
+        __syncwarp();
+        oqn = oqn > 32 ? oqn - 32 : 0;
+        chunk_process<MODE>(a, T, mem, v, wv, we, wo);
+    };
     auto pass = [&](int v) {
         int status = 0;
         if (v >= 0) status = lane_vertex<MODE, kSlots>(a, v, wv, we);
-        append_striped(status == 1, v, a.flist);
+        const unsigned om = __ballot_sync(0xffffffffu, status == 1);
+        if (status == 1) oq[oqn + __popc(om & lanemask_lt())] = v;
+        oqn += __popc(om);
+        __syncwarp();
         append_aggregated(status == 2, v, a.heavy, a.hcount);
         append_striped(status == 3, v, a.plist);
+        if (oqn >= 32) overflow_pass();
     };
     for (long long task = warp; task < ntasks; task += nwarps) {
         const long long base = task * span;
@@ -558,14 +537,17 @@ __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
         }
     }
     if (qn > 0) pass(lane < qn ? q[lane] : -1);
+    while (oqn > 0) overflow_pass();
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) {
         wv += __shfl_xor_sync(0xffffffffu, wv, o);
         we += __shfl_xor_sync(0xffffffffu, we, o);
+        wo += __shfl_xor_sync(0xffffffffu, wo, o);
     }
     if (lane == 0 && (wv | we)) {
         atomicAdd(&a.work[0], wv);
         atomicAdd(&a.work[1], we);
+        if (wo) atomicAdd(&a.work[2], wo);
     }
 }
 
@@ -788,12 +770,12 @@ int sweep_blocks() { return kNumSMs * 5; }  // 48 registers, 32 KB shared: 5 blo
 
 struct SweepBuffers {
     int *pt, *pc;
-    unsigned* counters;  // [0, kStripes) overflow, [kStripes, 2 kStripes) proposals,
+    unsigned* counters;  // [0, kStripes) unused, [kStripes, 2 kStripes) proposals,
                          // [2 kStripes] heavy, [+1] heavy proposals, [+2] moved
     int* heavy;
     int* hplist;
-    SList flist, plist;
-    int lblocks, cblocks;
+    SList plist;
+    int lblocks;
     uint32_t *gtk, *gtv;
     int gcap, hblocks;
     unsigned long long* work;
@@ -818,12 +800,7 @@ SweepBuffers make_buffers(Ctx& ctx, const DevGraph& g) {
     b.lblocks = (int)std::max<long long>(1, std::min<long long>(div_up(tasks, kWarpsPerBlock), kNumSMs * 4LL));
     const long long wl = (long long)b.lblocks * kWarpsPerBlock;
     const long long cap_l = ((wl + kStripes - 1) / kStripes) * ((tasks + wl - 1) / wl) * 32 * kSpan;
-    b.cblocks = (int)std::max<long long>(1, std::min<long long>(div_up(n, 32 * kWarpsPerBlock), sweep_blocks()));
-    const long long wc = (long long)b.cblocks * kWarpsPerBlock;
-    const long long chunks_max = (n + 31) / 32 + kStripes;
-    const long long cap_c = ((wc + kStripes - 1) / kStripes) * ((chunks_max + wc - 1) / wc) * 32;
-    b.flist = SList{A.alloc<int>((size_t)(kStripes * cap_l)), b.counters, cap_l};
-    b.plist = SList{A.alloc<int>((size_t)(kStripes * (cap_l + cap_c))), b.counters + kStripes, cap_l + cap_c};
+    b.plist = SList{A.alloc<int>((size_t)(kStripes * cap_l)), b.counters + kStripes, cap_l};
     b.work = ctx.work;
     b.err = ctx.dscalars + 60;
     b.gcap = 0;
@@ -860,11 +837,6 @@ void launch_sweep(Ctx& ctx, const DevGraph& g, SweepArgs a, const SweepBuffers& 
         lane_kernel<MODE><<<b.lblocks, kThreads, 0, ctx.stream>>>(a);
         KB_LAUNCH();
     }
-    {
-        PhaseScope ps(ctx, family(MODE, 1), 0);
-        chunk_kernel<MODE><<<b.cblocks, kThreads, 0, ctx.stream>>>(a);
-        KB_LAUNCH();
-    }
     if (b.gcap > 0) {
         PhaseScope ps(ctx, family(MODE, 2), 0);
         heavy_kernel<MODE><<<b.hblocks, kThreads, 0, ctx.stream>>>(a, b.gtk, b.gtv, b.gcap);
@@ -883,7 +855,6 @@ SweepArgs base_args(const DevGraph& g, const SweepBuffers& b) {
     a.pc = b.pc;
     a.hcount = b.counters + kCntHeavy;
     a.heavy = b.heavy;
-    a.flist = b.flist;
     a.plist = b.plist;
     a.hplist = b.hplist;
     a.hpcount = b.counters + kCntHeavyProp;
