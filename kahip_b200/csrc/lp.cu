@@ -894,11 +894,14 @@ void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* la
     for (int r = 0; r < kn.lpc_rounds; ++r) {
         a.ks_sub = stream_key(kn.seed, TAG_CSUB, level, r);
         a.ks_tie = stream_key(kn.seed, TAG_CTIE, level, r);
+        // round 0 is one fully synchronous sub-round (every cluster is still a
+        // single node), later rounds use lpc_subrounds sub-rounds
+        a.S = r == 0 ? 1u : (uint32_t)kn.lpc_subrounds;
         for (uint32_t s = 0; s < a.S; ++s) {
             a.s = s;
-            // before the first sub-round every vertex is its own cluster; with
-            // no repeated targets per row nothing needs aggregating
-            a.singletons = (r == 0 && s == 0 && sorted_rows) ? 1 : 0;
+            // in round 0 every vertex is its own cluster; with no repeated
+            // targets per row nothing needs aggregating
+            a.singletons = (r == 0 && sorted_rows) ? 1 : 0;
             launch_sweep<CLUSTER>(ctx, g, a, b, sweep_bytes(g, 1.0 / a.S));
             PhaseScope ps(ctx, "lp_cluster_admit", 0);
             cluster_decide<<<admit_blocks(), kThreads, 0, st>>>(b.plist, b.hplist, a.hpcount, b.pt, cw, inc, minv,

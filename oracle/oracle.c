@@ -244,10 +244,12 @@ void or_lp_cluster(const or_graph* g, const or_knobs* kn, int level, int* label)
     or_acc a;
     acc_init(&a, n, max_degree(g));
     for (int v = 0; v < n; ++v) { label[v] = v; cw[v] = (uint32_t)g->vwgt[v]; minv[v] = INT_MAX; }
-    const uint32_t S = (uint32_t)kn->lpc_subrounds;
     for (int r = 0; r < kn->lpc_rounds; ++r) {
         uint64_t ks_sub = or_stream(kn->seed, TAG_CSUB, level, r);
         uint64_t ks_tie = or_stream(kn->seed, TAG_CTIE, level, r);
+        /* round 0 runs as one fully synchronous sub-round (every cluster is
+         * still a single node), later rounds in lpc_subrounds sub-rounds */
+        const uint32_t S = r == 0 ? 1u : (uint32_t)kn->lpc_subrounds;
         for (uint32_t s = 0; s < S; ++s) {
             /* 1. every active node decides against the state at sub-round start */
             for (int v = 0; v < n; ++v) {
