@@ -392,15 +392,12 @@ __device__ __forceinline__ int nth_set_bit(unsigned mask, int r) {
 
 // 0: decided (stays), 3: decided (proposes a move), 1: too many distinct
 // labels for NS slots, 2: degree above kWin
-template <int MODE, int NS>
+template <int MODE, int NS, bool UNIT>
 __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, unsigned long long& we) {
     const int beg = a.xadj[v], end = a.xadj[v + 1];
     if (end - beg > kWin) return 2;
     const uint32_t own = (uint32_t)a.lab[v];
     const uint32_t cv = (uint32_t)a.vwgt[v];
-    uint32_t sl[NS], sc[NS];
-#pragma unroll
-    for (int i = 0; i < NS; ++i) { sl[i] = kEmpty; sc[i] = 0; }
     uint32_t cown = 0;
     if (MODE == CLUSTER && a.singletons) {
         // label[u] == u and no target repeats: the connection to cluster u is
@@ -416,7 +413,7 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
                 w[t] = 0;
                 if (e + t < end) {
                     u[t] = a.adjncy[e + t];
-                    w[t] = (uint32_t)a.adjwgt[e + t];
+                    w[t] = UNIT ? 1u : (uint32_t)a.adjwgt[e + t];
                 }
             }
 #pragma unroll
@@ -431,6 +428,11 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
         we += (unsigned long long)(end - beg);
         return decide_emit<MODE>(a, v, own, cv, cown, key, id) ? 3 : 0;
     }
+    // NS register slots (label, connection); a new label enters at slot 0 and
+    // shifts the others up, so slot NS-1 filled means the slots are full
+    uint32_t sl[NS], sc[NS];
+#pragma unroll
+    for (int i = 0; i < NS; ++i) { sl[i] = kEmpty; sc[i] = 0; }
     bool overflow = false;
     for (int e = beg; e < end && !overflow; e += 4) {
         int u[4];
@@ -441,7 +443,7 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
             w[t] = 0;
             if (e + t < end) {
                 u[t] = a.adjncy[e + t];
-                w[t] = (uint32_t)a.adjwgt[e + t];
+                w[t] = UNIT ? 1u : (uint32_t)a.adjwgt[e + t];
             }
         }
 #pragma unroll
@@ -449,16 +451,21 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
             if (u[t] < 0) continue;
-            if (l[t] == own) { cown += w[t]; continue; }
+            const uint32_t lt = l[t], wt = w[t];
+            if (lt == own) { cown += wt; continue; }
             bool hit = false;
 #pragma unroll
-            for (int i = 0; i < NS; ++i)
-                if (sl[i] == l[t]) { sc[i] += w[t]; hit = true; }
+            for (int i = 0; i < NS; ++i) {
+                const bool m = sl[i] == lt;
+                sc[i] += m ? wt : 0u;
+                hit |= m;
+            }
             if (!hit) {
+                overflow |= sl[NS - 1] != kEmpty;
 #pragma unroll
-                for (int i = 0; i < NS; ++i)
-                    if (!hit && sl[i] == kEmpty) { sl[i] = l[t]; sc[i] = w[t]; hit = true; }
-                overflow |= !hit;
+                for (int i = NS - 1; i > 0; --i) { sl[i] = sl[i - 1]; sc[i] = sc[i - 1]; }
+                sl[0] = lt;
+                sc[0] = wt;
             }
         }
     }
@@ -474,7 +481,7 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
 }
 
 
-template <int MODE>
+template <int MODE, bool UNIT>
 __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
     static_assert(kTab == 256, "slot64 assumes 256 slots");
     // per-warp queue of members still to be processed, so that every pass
@@ -506,7 +513,7 @@ __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
     };
     auto pass = [&](int v) {
         int status = 0;
-        if (v >= 0) status = lane_vertex<MODE, kSlots>(a, v, wv, we);
+        if (v >= 0) status = lane_vertex<MODE, kSlots, UNIT>(a, v, wv, we);
         const unsigned om = __ballot_sync(0xffffffffu, status == 1);
         if (status == 1) oq[oqn + __popc(om & lanemask_lt())] = v;
         oqn += __popc(om);
@@ -834,7 +841,8 @@ void launch_sweep(Ctx& ctx, const DevGraph& g, SweepArgs a, const SweepBuffers& 
     KB_CUDA(cudaMemsetAsync(b.counters, 0, sizeof(unsigned) * kCntMoved, ctx.stream));
     {
         PhaseScope ps(ctx, family(MODE, 0), bytes);
-        lane_kernel<MODE><<<b.lblocks, kThreads, 0, ctx.stream>>>(a);
+        if (g.unit_weights) lane_kernel<MODE, true><<<b.lblocks, kThreads, 0, ctx.stream>>>(a);
+        else lane_kernel<MODE, false><<<b.lblocks, kThreads, 0, ctx.stream>>>(a);
         KB_LAUNCH();
     }
     if (b.gcap > 0) {

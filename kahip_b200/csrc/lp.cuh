@@ -16,6 +16,7 @@ struct DevGraph {
     int n = 0;
     long long m = 0;
     int maxdeg = 0;
+    bool unit_weights = false;  // every edge weight is 1 (lets sweeps skip adjwgt)
     const int* xadj = nullptr;
     const int* adjncy = nullptr;
     const int* adjwgt = nullptr;
@@ -51,7 +52,7 @@ int max_degree(Ctx& ctx, const DevGraph& g);
 
 // Device-side input checks: bit 1 = target out of range, 2 = negative edge
 // weight, 4 = negative node weight, 8 = xadj not starting at 0 / not
-// monotone.  Also returns the node weight sum (32-bit, as the reference's
+// monotone, 16 = some edge weight differs from 1 (not an error).  Also returns the node weight sum (32-bit, as the reference's
 // NodeWeight accumulates it).  Synchronises the stream.
 int check_graph(Ctx& ctx, const DevGraph& g, uint32_t* total_weight = nullptr);
 

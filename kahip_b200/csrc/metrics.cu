@@ -67,7 +67,9 @@ __global__ void check_graph_kernel(int n, long long m, const int* __restrict__ x
          e += (long long)gridDim.x * blockDim.x) {
         int t = adjncy[e];
         if (t < 0 || t >= n) f |= 1;
-        if (adjwgt[e] < 0) f |= 2;
+        const int w = adjwgt[e];
+        if (w < 0) f |= 2;
+        if (w != 1) f |= 16;
     }
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
         if (vwgt[v] < 0) f |= 4;
