@@ -124,9 +124,10 @@ long long cut_of(const HostGraph& g, const std::vector<char>& side) {
 
 // Last node dequeued by a breadth-first search from s.
 int farthest(const HostGraph& g, int s) {
-    std::vector<char> seen(g.n, 0);
-    std::vector<int> q;
-    q.reserve(g.n);
+    thread_local std::vector<char> seen;
+    thread_local std::vector<int> q;
+    seen.assign(g.n, 0);
+    q.clear();
     q.push_back(s);
     seen[s] = 1;
     for (size_t h = 0; h < q.size(); ++h) {
@@ -144,7 +145,8 @@ int farthest(const HostGraph& g, int s) {
 void grow_region(const HostGraph& g, int start, uint64_t target0, uint64_t max0,
                  std::vector<char>& side, std::vector<long long>& key, GainHeap& heap) {
     side.assign(g.n, 1);
-    std::vector<char> skipped(g.n, 0);
+    thread_local std::vector<char> skipped;
+    skipped.assign(g.n, 0);
     for (int v = 0; v < g.n; ++v) {
         long long d = 0;
         for (int e = g.xadj[v]; e < g.xadj[v + 1]; ++e) d += g.adjwgt[e];
@@ -185,9 +187,10 @@ long long fm_refine(const HostGraph& g, std::vector<char>& side, const Limits& l
                     int stall_limit, std::vector<long long>& key, GainHeap& heap) {
     uint64_t w[2] = {0, 0};
     for (int v = 0; v < g.n; ++v) w[(int)side[v]] += (uint64_t)g.vwgt[v];
-    std::vector<char> locked(g.n, 0);
-    std::vector<int> log;
-    log.reserve(g.n);
+    thread_local std::vector<char> locked;
+    thread_local std::vector<int> log;
+    locked.assign(g.n, 0);
+    log.clear();
     long long cut = cut_of(g, side);
     for (int pass = 0; pass < passes; ++pass) {
         for (int v = 0; v < g.n; ++v) {
@@ -296,21 +299,31 @@ HostGraph contract_host(const HostGraph& g, const std::vector<int>& label, std::
     c.n = nc;
     c.vwgt.assign(nc, 0);
     for (int v = 0; v < g.n; ++v) c.vwgt[cmap[v]] += g.vwgt[v];
-    std::vector<std::vector<int>> members(nc);
-    for (int v = 0; v < g.n; ++v) members[cmap[v]].push_back(v);
+    // members of every coarse node by counting sort
+    std::vector<int> start(nc + 1, 0), mem(g.n);
+    for (int v = 0; v < g.n; ++v) start[cmap[v] + 1]++;
+    for (int i = 0; i < nc; ++i) start[i + 1] += start[i];
+    {
+        std::vector<int> fill(start.begin(), start.end() - 1);
+        for (int v = 0; v < g.n; ++v) mem[fill[cmap[v]]++] = v;
+    }
     std::vector<uint32_t> acc(nc, 0);
     std::vector<char> hit(nc, 0);
     std::vector<int> targets;
     c.xadj.assign(nc + 1, 0);
+    c.adjncy.reserve(g.xadj[g.n]);
+    c.adjwgt.reserve(g.xadj[g.n]);
     for (int cu = 0; cu < nc; ++cu) {
         targets.clear();
-        for (int v : members[cu])
+        for (int i = start[cu]; i < start[cu + 1]; ++i) {
+            const int v = mem[i];
             for (int e = g.xadj[v]; e < g.xadj[v + 1]; ++e) {
                 int t = cmap[g.adjncy[e]];
                 if (t == cu) continue;
                 if (!hit[t]) { hit[t] = 1; targets.push_back(t); }
                 acc[t] += (uint32_t)g.adjwgt[e];
             }
+        }
         std::sort(targets.begin(), targets.end());
         for (int t : targets) {
             c.adjncy.push_back(t);
@@ -444,7 +457,7 @@ void recurse(const Knobs& kn, const HostGraph& g, const std::vector<int>& orig, 
     side.clear();
     side.shrink_to_fit();
     // out[] entries written by the two halves are disjoint
-    if (spawn_depth > 0 && kl > 1 && kr > 1 && L.n > 512 && R.n > 512) {
+    if (spawn_depth > 0 && kl > 1 && kr > 1 && L.n > 64 && R.n > 64) {
         std::thread left([&] { recurse(kn, L, lo, kl, offset, rep, 2u * node, out, spawn_depth - 1); });
         recurse(kn, R, ro, kr, offset + kl, rep, 2u * node + 1u, out, spawn_depth - 1);
         left.join();
@@ -457,7 +470,7 @@ void recurse(const Knobs& kn, const HostGraph& g, const std::vector<int>& orig, 
 int spawn_depth_for_host() {
     unsigned t = std::thread::hardware_concurrency();
     int d = 0;
-    while (d < 5 && (2u << d) <= t) ++d;
+    while (d < 6 && (2u << d) <= t) ++d;
     return d;
 }
 

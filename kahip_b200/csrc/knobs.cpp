@@ -69,7 +69,7 @@ void derive_knobs_total(int n, uint32_t W, int k, double imbalance, int seed, in
     kn.ref_classes = 16;
     kn.bal_iters = 64;
     kn.ip_reps = fast ? 1 : 2;
-    kn.ip_tries = fast ? 8 : 16;         // bipartition_tries = 4 (fast/eco) at every level of
+    kn.ip_tries = fast ? 4 : 16;         // bipartition_tries = 4 (fast/eco) at every level of
                                          // the reference's multilevel bisection; more growing
                                          // tries on one level here
     kn.ip_fm_passes = fast ? 3 : 6;

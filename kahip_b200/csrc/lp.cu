@@ -872,8 +872,10 @@ SweepArgs base_args(const DevGraph& g, const SweepBuffers& b) {
 }
 
 double sweep_bytes(const DevGraph& g, double frac) {
-    // 12 B per directed entry (adjncy, adjwgt, label gather) + 24 B per node
-    return frac * (12.0 * (double)g.m + 24.0 * (double)g.n);
+    // per directed entry: adjncy + label gather (+ adjwgt unless all weights
+    // are 1, then the sweep does not read it); per node: xadj, own label,
+    // node weight, target weight, label write, weight update
+    return frac * ((g.unit_weights ? 8.0 : 12.0) * (double)g.m + 24.0 * (double)g.n);
 }
 
 }  // namespace

@@ -106,7 +106,7 @@ void or_derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, 
     o->ref_classes = 16;
     o->bal_iters = 64;
     o->ip_reps = fast ? 1 : 2;
-    o->ip_tries = fast ? 8 : 16;
+    o->ip_tries = fast ? 4 : 16;
     o->ip_fm_passes = fast ? 3 : 6;
     o->ip_fm_stall = 100;
     o->max_levels = 48;
