@@ -354,7 +354,7 @@ def main():
             traffic = json.load(f).get("dram_bytes_per_launch_scaled")
     total_fam_ms = sum(f["ms"] for f in fam.values()) or 1.0
     roofline = {
-        "kernel": "lp_cluster_sweep (sweep_kernel<G, CLUSTER>)", "bound": "hbm",
+        "kernel": "lp_cluster_sweep (lane_kernel<CLUSTER> + chunk_process + heavy_kernel)", "bound": "hbm",
         "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": (achieved / peak) if achieved else None, "peak_source": f"hbm_gbs of {peak_kind}",
         "traffic": traffic,
