@@ -55,6 +55,8 @@ typedef struct kb200_knobs {
     int bal_iters;                                 /* balance repair */
     int ip_reps, ip_tries, ip_fm_passes, ip_fm_stall; /* initial partitioning */
     int max_levels;
+    int coarsening;            /* 0 = LP clustering (default), 1 = heavy-edge matching */
+    int match_rounds;          /* cap on locally-dominant matching rounds per level */
 } kb200_knobs;
 
 /* Per-call report.  level 0 is the input graph. */
@@ -99,7 +101,24 @@ int kb200_kaffpa_device(int n, const int* d_vwgt, const int* d_xadj, const int* 
                         const int* d_adjncy, int nparts, double imbalance, int seed, int mode,
                         long long* edgecut, int* d_part, void* stream, kb200_stats* stats);
 
+/* Whole partitioning with explicit knobs (kb200_derive_knobs() output,
+ * possibly edited: coarsening, round counts ...); kn->k blocks. */
+int kb200_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+                       const kb200_knobs* kn, long long* edgecut, int* part, kb200_stats* stats);
+
+/* Same with device buffers (explicit weights), like kb200_kaffpa_device. */
+int kb200_kaffpa_device_knobs(int n, const int* d_vwgt, const int* d_xadj, const int* d_adjcwgt,
+                              const int* d_adjncy, const kb200_knobs* kn, long long* edgecut, int* d_part,
+                              void* stream, kb200_stats* stats);
+
 /* ---- phases (host buffers), for parity checks against the CPU oracle ---- */
+
+/* Heavy-edge matching of one coarsening level (replaces random_matching.cpp:
+ * 20-116 / gpa_matching.cpp:25-129): label[n] out = min(v, mate(v)) or v.
+ * rating: NULL = expansion*^2 (edge_ratings.cpp:316-328); else one 32-bit
+ * rating per directed entry (must be symmetric), larger = match first. */
+int kb200_hem_match(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                    const kb200_knobs* kn, int level, const uint32_t* rating, int* label);
 
 /* LP clustering of one coarsening level: label[n] out. */
 int kb200_lp_cluster(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,

@@ -17,6 +17,7 @@
 #include "contract.cuh"
 #include "host/initial_partitioning.h"
 #include "knobs.h"
+#include "match.cuh"
 #include "partitioner.cuh"
 #include "prims.cuh"
 
@@ -185,18 +186,22 @@ void begin_stats(Ctx& ctx, kb200_stats* st) {
 using clk = std::chrono::steady_clock;
 double ms_since(clk::time_point t) { return std::chrono::duration<double, std::milli>(clk::now() - t).count(); }
 
-int run_host(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy, int nparts,
-             double imbalance, int seed, int mode, long long* edgecut, int* part, kb200_stats* st) {
+int check_knobs(const kb200_knobs* kn) {
+    if (!kn) return fail(KB_ERR_INVALID_INPUT, "knobs is NULL");
+    if (kn->k < 1 || kn->lpc_subrounds < 1 || kn->ref_subrounds < 1 || kn->ref_classes < 1 ||
+        kn->coarsening < 0 || kn->coarsening > 1 || kn->max_levels < 1 || kn->max_levels > 64)
+        return fail(KB_ERR_INVALID_INPUT, "invalid knobs");
+    return KB_OK;
+}
+
+int run_host(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy, const Knobs& kn,
+             long long* edgecut, int* part, kb200_stats* st) {
     auto t0 = clk::now();
     int rc = validate(n, xadj, adjncy, adjcwgt, vwgt);
-    if (rc) return rc;
-    if (nparts < 1) return fail(KB_ERR_INVALID_INPUT, "nparts < 1");
-    if (!(imbalance >= 0)) return fail(KB_ERR_INVALID_INPUT, "imbalance must be >= 0");
+    if (rc || (rc = check_knobs(&kn))) return rc;
     if (!edgecut || (n > 0 && !part)) return fail(KB_ERR_INVALID_INPUT, "edgecut/part is NULL");
     int dev;
     if ((rc = current_device(&dev))) return rc;
-    Knobs kn;
-    derive_knobs(n, vwgt, nparts, imbalance, seed, mode, kn);
     Lease lease(dev);
     Ctx& ctx = *lease.ctx;
     const long long m = xadj[n];
@@ -248,13 +253,6 @@ struct PhaseRun {
     }
 };
 
-int check_knobs(const kb200_knobs* kn) {
-    if (!kn) return fail(KB_ERR_INVALID_INPUT, "knobs is NULL");
-    if (kn->k < 1 || kn->lpc_subrounds < 1 || kn->ref_subrounds < 1 || kn->ref_classes < 1)
-        return fail(KB_ERR_INVALID_INPUT, "invalid knobs");
-    return KB_OK;
-}
-
 }  // namespace
 }  // namespace kb
 
@@ -272,16 +270,37 @@ int kb200_derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed
 int kb200_kaffpa(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy, int nparts,
                  double imbalance, int seed, int mode, long long* edgecut, int* part, kb200_stats* stats) {
     g_last_error.clear();
-    return guarded([&] {
-        return run_host(n, vwgt, xadj, adjcwgt, adjncy, nparts, imbalance, seed, mode, edgecut, part, stats);
+    return guarded([&]() -> int {
+        if (n < 0 || !xadj) return fail(KB_ERR_INVALID_INPUT, "invalid graph");
+        if (nparts < 1) return fail(KB_ERR_INVALID_INPUT, "nparts < 1");
+        if (!(imbalance >= 0)) return fail(KB_ERR_INVALID_INPUT, "imbalance must be >= 0");
+        Knobs kn;
+        derive_knobs(n, vwgt, nparts, imbalance, seed, mode, kn);
+        return run_host(n, vwgt, xadj, adjcwgt, adjncy, kn, edgecut, part, stats);
     });
 }
 
-int kb200_kaffpa_device(int n, const int* d_vwgt, const int* d_xadj, const int* d_adjcwgt, const int* d_adjncy,
-                        int nparts, double imbalance, int seed, int mode, long long* edgecut, int* d_part,
-                        void* stream, kb200_stats* st) {
+int kb200_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+                       const kb200_knobs* kn, long long* edgecut, int* part, kb200_stats* stats) {
     g_last_error.clear();
     return guarded([&]() -> int {
+        int rc;
+        if ((rc = check_knobs(kn))) return rc;
+        return run_host(n, vwgt, xadj, adjcwgt, adjncy, *kn, edgecut, part, stats);
+    });
+}
+
+static int run_device(int n, const int* d_vwgt, const int* d_xadj, const int* d_adjcwgt, const int* d_adjncy,
+                      const kb200_knobs* kn_in, int nparts, double imbalance, int seed, int mode, long long* edgecut,
+                      int* d_part, void* stream, kb200_stats* st) {
+    g_last_error.clear();
+    return guarded([&]() -> int {
+        if (kn_in) {
+            int rc = check_knobs(kn_in);
+            if (rc) return rc;
+            nparts = kn_in->k;
+            imbalance = kn_in->imbalance;
+        }
         if (n < 0 || nparts < 1 || !(imbalance >= 0) || !d_xadj || !d_vwgt || !d_adjcwgt || !edgecut)
             return fail(KB_ERR_INVALID_INPUT, "invalid arguments (device entry point needs explicit weights)");
         int dev, rc;
@@ -311,7 +330,8 @@ int kb200_kaffpa_device(int n, const int* d_vwgt, const int* d_xadj, const int* 
         uint32_t W = 0;
         check_uploaded(ctx, g, &W);
         Knobs kn;
-        derive_knobs_total(n, W, nparts, imbalance, seed, mode, kn);
+        if (kn_in) kn = *kn_in;
+        else derive_knobs_total(n, W, nparts, imbalance, seed, mode, kn);
         for (int attempt = 0;; ++attempt) {
             try {
                 reserve_for(ctx, n, m32, false, attempt == 0 ? 1.0 : 2.0 * attempt);
@@ -333,6 +353,47 @@ int kb200_kaffpa_device(int n, const int* d_vwgt, const int* d_xadj, const int* 
                 throw;
             }
         }
+    });
+}
+
+int kb200_kaffpa_device(int n, const int* d_vwgt, const int* d_xadj, const int* d_adjcwgt, const int* d_adjncy,
+                        int nparts, double imbalance, int seed, int mode, long long* edgecut, int* d_part,
+                        void* stream, kb200_stats* st) {
+    return run_device(n, d_vwgt, d_xadj, d_adjcwgt, d_adjncy, nullptr, nparts, imbalance, seed, mode, edgecut, d_part,
+                      stream, st);
+}
+
+int kb200_kaffpa_device_knobs(int n, const int* d_vwgt, const int* d_xadj, const int* d_adjcwgt,
+                              const int* d_adjncy, const kb200_knobs* kn, long long* edgecut, int* d_part,
+                              void* stream, kb200_stats* st) {
+    if (!kn) {
+        g_last_error = "knobs is NULL";
+        return KB_ERR_INVALID_INPUT;
+    }
+    return run_device(n, d_vwgt, d_xadj, d_adjcwgt, d_adjncy, kn, kn->k, kn->imbalance, kn->seed, kn->mode, edgecut,
+                      d_part, stream, st);
+}
+
+int kb200_hem_match(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                    const kb200_knobs* kn, int level, const uint32_t* rating, int* label) {
+    g_last_error.clear();
+    return guarded([&]() -> int {
+        int rc, dev;
+        if ((rc = validate(n, xadj, adjncy, adjwgt, vwgt)) || (rc = check_knobs(kn))) return rc;
+        if ((rc = current_device(&dev))) return rc;
+        PhaseRun pr(dev, n, xadj, adjncy, adjwgt, vwgt);
+        cudaStream_t s = pr.ctx.stream;
+        int* d = pr.ctx.hier.alloc<int>((size_t)std::max(n, 1));
+        uint32_t* dr = nullptr;
+        const long long m = xadj[n];
+        if (rating) {
+            dr = pr.ctx.hier.alloc<uint32_t>((size_t)std::max<long long>(m, 1));
+            if (m) KB_CUDA(cudaMemcpyAsync(dr, rating, sizeof(uint32_t) * (size_t)m, cudaMemcpyHostToDevice, s));
+        }
+        hem_match(pr.ctx, pr.up.g, *kn, level, dr, d);
+        if (n) KB_CUDA(cudaMemcpyAsync(label, d, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+        KB_CUDA(cudaStreamSynchronize(s));
+        return KB_OK;
     });
 }
 

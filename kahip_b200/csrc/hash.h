@@ -24,6 +24,7 @@ enum HashTag : int {
     TAG_BPRIO = 8,  // balance: admission priority class
     TAG_IP = 9,     // initial partitioning: start nodes
     TAG_IPM = 10,   // initial partitioning: matching order
+    TAG_MATCH = 11, // heavy-edge matching: pair hash
 };
 
 // splitmix64 output function (Steele, Lea & Flood, OOPSLA 2014).

@@ -75,6 +75,8 @@ void derive_knobs_total(int n, uint32_t W, int k, double imbalance, int seed, in
     kn.ip_fm_passes = fast ? 3 : 6;
     kn.ip_fm_stall = 100;
     kn.max_levels = 48;
+    kn.coarsening = 0;                   // LP clustering; 1 selects heavy-edge matching
+    kn.match_rounds = 16;                // matching converges in < 10 rounds on meshes
 }
 
 }  // namespace kb

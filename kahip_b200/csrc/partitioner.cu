@@ -11,6 +11,7 @@
 
 #include "contract.cuh"
 #include "host/initial_partitioning.h"
+#include "match.cuh"
 #include "prims.cuh"
 
 namespace kb {
@@ -158,7 +159,8 @@ int partition(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_part, long l
             lv[L].cmap = ctx.hier.alloc<int>((size_t)f.n);
             const size_t mk = ctx.scratch.mark();
             int* label = ctx.scratch.alloc<int>((size_t)f.n);
-            lp_cluster(ctx, f, kn, L, label);
+            if (kn.coarsening == 1) hem_match(ctx, f, kn, L, nullptr, label);
+            else lp_cluster(ctx, f, kn, L, label);
             Level c;
             int *cx, *ca, *cw, *cv;
             contract(ctx, f, label, lv[L].cmap, c.g, &cx, &ca, &cw, &cv);

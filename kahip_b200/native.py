@@ -38,7 +38,8 @@ class Knobs(ctypes.Structure):
                 ("ref_classes", ctypes.c_int), ("bal_iters", ctypes.c_int),
                 ("ip_reps", ctypes.c_int), ("ip_tries", ctypes.c_int),
                 ("ip_fm_passes", ctypes.c_int), ("ip_fm_stall", ctypes.c_int),
-                ("max_levels", ctypes.c_int)]
+                ("max_levels", ctypes.c_int), ("coarsening", ctypes.c_int),
+                ("match_rounds", ctypes.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -71,7 +72,8 @@ class Stats(ctypes.Structure):
 
 EXPORTS = [
     # extended ABI (include/kahip_b200.h)
-    "kb200_derive_knobs", "kb200_kaffpa", "kb200_kaffpa_device", "kb200_lp_cluster", "kb200_contract",
+    "kb200_derive_knobs", "kb200_kaffpa", "kb200_kaffpa_device", "kb200_kaffpa_knobs",
+    "kb200_kaffpa_device_knobs", "kb200_hem_match", "kb200_lp_cluster", "kb200_contract",
     "kb200_lp_refine", "kb200_balance", "kb200_edge_cut", "kb200_project", "kb200_initial_partition",
     "kb200_last_error", "kb200_kernel_launches", "kb200_device_count", "kb200_edge_cut_noalloc",
     # reference-compatible ABI (include/kaHIP_interface.h)
@@ -92,6 +94,11 @@ def lib():
         L.kb200_derive_knobs.argtypes = [i, vp, i, d, i, i, ctypes.POINTER(Knobs)]
         L.kb200_kaffpa.argtypes = [i, vp, vp, vp, vp, i, d, i, i, c_ll_p, vp, ctypes.POINTER(Stats)]
         L.kb200_kaffpa_device.argtypes = [i, vp, vp, vp, vp, i, d, i, i, c_ll_p, vp, vp, ctypes.POINTER(Stats)]
+        L.kb200_kaffpa_knobs.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), c_ll_p, vp,
+                                         ctypes.POINTER(Stats)]
+        L.kb200_kaffpa_device_knobs.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), c_ll_p, vp, vp,
+                                                ctypes.POINTER(Stats)]
+        L.kb200_hem_match.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, vp, vp]
         L.kb200_lp_cluster.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, vp]
         L.kb200_contract.argtypes = [i, vp, vp, vp, vp, vp, c_int_p, c_ll_p, vp, vp, vp, vp, vp]
         L.kb200_lp_refine.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, u32, vp]
@@ -153,6 +160,28 @@ def kaffpa_ex(xadj, adjncy, nparts, imbalance=0.03, seed=0, mode=FAST, vwgt=None
                             mode, ctypes.byref(cut), _ptr(part), ctypes.byref(stats) if stats else None)
     _check(rc)
     return rc, cut.value, part
+
+
+def kaffpa_knobs(xadj, adjncy, kn: Knobs, vwgt=None, adjwgt=None, stats: Stats | None = None):
+    """Whole partitioning with explicit knobs.  Returns (status, edgecut, part)."""
+    xadj, adjncy, vwgt, adjwgt = _i32(xadj), _i32(adjncy), _i32(vwgt), _i32(adjwgt)
+    n = len(xadj) - 1
+    part = np.zeros(max(n, 0), np.int32)
+    cut = ctypes.c_longlong(-1)
+    rc = lib().kb200_kaffpa_knobs(n, _ptr(vwgt), _ptr(xadj), _ptr(adjwgt), _ptr(adjncy), ctypes.byref(kn),
+                                  ctypes.byref(cut), _ptr(part), ctypes.byref(stats) if stats else None)
+    _check(rc)
+    return rc, cut.value, part
+
+
+def hem_match(g: dict, kn: Knobs, level=0, rating=None) -> np.ndarray:
+    """Heavy-edge matching labels of one level; rating: optional uint32 per directed entry."""
+    lab = np.empty(g["n"], np.int32)
+    rq = None if rating is None else np.ascontiguousarray(rating, np.uint32)
+    _check(lib().kb200_hem_match(g["n"], _ptr(g["xadj"]), _ptr(g["adjncy"]), _ptr(g["adjwgt"]),
+                                 _ptr(g["vwgt"]), ctypes.byref(kn), level,
+                                 None if rq is None else rq.ctypes.data_as(ctypes.c_void_p), _ptr(lab)))
+    return lab
 
 
 def lp_cluster(g: dict, kn: Knobs, level=0) -> np.ndarray:
@@ -235,5 +264,16 @@ def kaffpa_device(n, xadj, adjncy, adjwgt, vwgt, part, nparts, imbalance=0.03, s
                                    seed, mode, ctypes.byref(cut), _ptr(part),
                                    None if stream is None else stream.cuda_stream,
                                    ctypes.byref(stats) if stats else None)
+    _check(rc)
+    return rc, cut.value
+
+
+def kaffpa_device_knobs(n, xadj, adjncy, adjwgt, vwgt, part, kn: Knobs, stream=None, stats: Stats | None = None):
+    """kaffpa_device with explicit knobs (kn.k blocks).  Returns (status, edgecut)."""
+    cut = ctypes.c_longlong(-1)
+    rc = lib().kb200_kaffpa_device_knobs(n, _ptr(vwgt), _ptr(xadj), _ptr(adjwgt), _ptr(adjncy), ctypes.byref(kn),
+                                         ctypes.byref(cut), _ptr(part),
+                                         None if stream is None else stream.cuda_stream,
+                                         ctypes.byref(stats) if stats else None)
     _check(rc)
     return rc, cut.value

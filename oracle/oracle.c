@@ -13,7 +13,7 @@
 
 enum {
     TAG_CSUB = 1, TAG_CTIE = 2, TAG_RSUB = 3, TAG_RTIE = 4, TAG_RPRIO = 5,
-    TAG_BTIE = 6, TAG_BCLS = 7, TAG_BPRIO = 8, TAG_IP = 9, TAG_IPM = 10
+    TAG_BTIE = 6, TAG_BCLS = 7, TAG_BPRIO = 8, TAG_IP = 9, TAG_IPM = 10, TAG_MATCH = 11
 };
 
 #define BAL_CLASSES 256
@@ -110,6 +110,8 @@ void or_derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, 
     o->ip_fm_passes = fast ? 3 : 6;
     o->ip_fm_stall = 100;
     o->max_levels = 48;
+    o->coarsening = 0;
+    o->match_rounds = 16;
 }
 
 /* stop_rules.h:64-66: continue coarsening after a level that went from nf to
@@ -157,6 +159,68 @@ void or_rate_expansion_star_2(const or_graph* g, double* rating) {
             rating[e] = 1.0 * w * w / (uint32_t)(cu * cv);
         }
     }
+}
+
+/* ------------------------------------------------------ heavy-edge matching */
+
+/* Primary key of an entry: the rating's IEEE bits (order-preserving for
+ * non-negative doubles; NaN from 0/0 counts as 0) or the supplied 32-bit
+ * rating. */
+static uint64_t match_primary(const or_graph* g, const uint32_t* rq, int e, uint32_t cv, uint32_t cu) {
+    if (rq) return rq[e];
+    int w = g->adjwgt[e];
+    double r = 1.0 * w * w / (uint32_t)(cu * cv);
+    if (r != r) r = 0.0;
+    uint64_t b;
+    memcpy(&b, &r, sizeof b);
+    return b;
+}
+
+/* Secondary key: hash of the unordered pair, then the complement of the
+ * endpoint sum (unique among the entries of one row). */
+static uint64_t match_secondary(uint64_t ks, uint32_t a, uint32_t b) {
+    uint32_t lo = a < b ? a : b, hi = a < b ? b : a;
+    uint32_t h = or_hash(ks, or_hash(ks, lo) ^ hi);
+    return ((uint64_t)h << 32) | (uint32_t)~(lo + hi);
+}
+
+void or_hem_match(const or_graph* g, const or_knobs* kn, int level, const uint32_t* rq, int* label) {
+    const int n = g->n;
+    const uint64_t ks = or_stream(kn->seed, TAG_MATCH, level, 0);
+    /* state: >= 0 unmatched (its weight), -1 matched, -2 no eligible neighbour left */
+    long long* state = xmalloc(sizeof(long long) * (size_t)(n ? n : 1));
+    int* best = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    int* mate = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    for (int v = 0; v < n; ++v) { state[v] = (uint32_t)g->vwgt[v]; mate[v] = -1; }
+    for (int r = 0; r < kn->match_rounds; ++r) {
+        for (int v = 0; v < n; ++v) {
+            best[v] = -1;
+            if (state[v] < 0) continue;
+            const uint32_t cv = (uint32_t)state[v];
+            uint64_t b1 = 0, b2 = 0;
+            for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) {
+                int u = g->adjncy[e];
+                if (u == v || state[u] < 0) continue;
+                if ((uint64_t)cv + (uint64_t)state[u] > kn->max_vertex_weight) continue;
+                uint64_t k1 = match_primary(g, rq, e, cv, (uint32_t)state[u]);
+                uint64_t k2 = match_secondary(ks, (uint32_t)v, (uint32_t)u);
+                if (best[v] < 0 || k1 > b1 || (k1 == b1 && k2 > b2)) { best[v] = u; b1 = k1; b2 = k2; }
+            }
+        }
+        int matched = 0;
+        for (int v = 0; v < n; ++v) {
+            if (state[v] < 0) continue;
+            if (best[v] >= 0 && best[best[v]] == v) { mate[v] = best[v]; ++matched; }
+        }
+        for (int v = 0; v < n; ++v) {
+            if (state[v] < 0) continue;
+            if (mate[v] >= 0) state[v] = -1;
+            else if (best[v] < 0) state[v] = -2;
+        }
+        if (!matched) break;
+    }
+    for (int v = 0; v < n; ++v) label[v] = mate[v] >= 0 && mate[v] < v ? mate[v] : v;
+    free(state); free(best); free(mate);
 }
 
 /* --------------------------------------------------- neighbourhood scratch */
@@ -1129,13 +1193,21 @@ int or_kaffpa(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const
               int nparts, double imbalance, int seed, int mode, long long* edgecut, int* part,
               or_stats* stats) {
     if (n < 0 || nparts < 1 || !xadj || (n > 0 && !adjncy) || imbalance < 0) return -1;
+    or_knobs kn;
+    or_derive_knobs(n, vwgt, nparts, imbalance, seed, mode, &kn);
+    return or_kaffpa_knobs(n, vwgt, xadj, adjcwgt, adjncy, &kn, edgecut, part, stats);
+}
+
+int or_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+                    const or_knobs* knobs, long long* edgecut, int* part, or_stats* stats) {
+    if (n < 0 || !knobs || knobs->k < 1 || !xadj || (n > 0 && !adjncy)) return -1;
+    const int nparts = knobs->k;
     const int m = xadj[n];
     int* vw = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
     int* ew = xmalloc(sizeof(int) * (size_t)(m ? m : 1));
     for (int v = 0; v < n; ++v) vw[v] = vwgt ? vwgt[v] : 1;
     for (int e = 0; e < m; ++e) ew[e] = adjcwgt ? adjcwgt[e] : 1;
-    or_knobs kn;
-    or_derive_knobs(n, vw, nparts, imbalance, seed, mode, &kn);
+    or_knobs kn = *knobs;
     or_stats st;
     memset(&st, 0, sizeof(st));
 
@@ -1147,7 +1219,8 @@ int or_kaffpa(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const
     while (L + 1 < kn.max_levels && lv[L].g.n > 0) {
         or_graph* f = &lv[L].g;
         int* label = xmalloc(sizeof(int) * (size_t)f->n);
-        or_lp_cluster(f, &kn, L, label);
+        if (kn.coarsening == 1) or_hem_match(f, &kn, L, NULL, label);
+        else or_lp_cluster(f, &kn, L, label);
         or_level* c = &lv[L + 1];
         lv[L].cmap = xmalloc(sizeof(int) * (size_t)f->n);
         c->xadj = xmalloc(sizeof(int) * (size_t)(f->n + 1));

@@ -44,6 +44,8 @@ typedef struct {
     int bal_iters;
     int ip_reps, ip_tries, ip_fm_passes, ip_fm_stall;
     int max_levels;
+    int coarsening;         /* 0 = LP clustering, 1 = heavy-edge matching */
+    int match_rounds;       /* cap on locally-dominant matching rounds */
 } or_knobs;
 
 typedef struct {
@@ -75,6 +77,14 @@ double or_balance_ratio(const or_graph* g, const int* part, int k);
 /* edge_ratings.cpp:316-328 */
 void or_rate_expansion_star_2(const or_graph* g, double* rating);
 
+/* Heavy-edge matching of one coarsening level: synchronous locally-dominant
+ * rounds on a strict edge order (rating, edge hash, endpoints).  rating_q:
+ * NULL = expansion*^2 (edge_ratings.cpp:316-328) computed per entry, else one
+ * 32-bit rating per directed entry (symmetric).  Pairs obey
+ * c(u)+c(v) <= max_vertex_weight (random_matching.cpp:85-112).
+ * label[v] = min(v, mate(v)), or v when unmatched. */
+void or_hem_match(const or_graph* g, const or_knobs* kn, int level, const uint32_t* rating_q, int* label);
+
 /* LP clustering, synchronous schedule (one coarsening level). label[n] out. */
 void or_lp_cluster(const or_graph* g, const or_knobs* kn, int level, int* label);
 /* LP clustering, sequential schedule in a given node order (pin mode):
@@ -103,6 +113,9 @@ void or_initial_partition(const or_graph* g, const or_knobs* kn, int* part);
 int or_kaffpa(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
               int nparts, double imbalance, int seed, int mode, long long* edgecut, int* part,
               or_stats* stats);
+/* Same with explicit knobs (kn->k blocks). */
+int or_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+                    const or_knobs* kn, long long* edgecut, int* part, or_stats* stats);
 
 #ifdef __cplusplus
 }

@@ -32,7 +32,8 @@ class Knobs(ctypes.Structure):
                 ("ref_classes", ctypes.c_int), ("bal_iters", ctypes.c_int),
                 ("ip_reps", ctypes.c_int), ("ip_tries", ctypes.c_int),
                 ("ip_fm_passes", ctypes.c_int), ("ip_fm_stall", ctypes.c_int),
-                ("max_levels", ctypes.c_int)]
+                ("max_levels", ctypes.c_int), ("coarsening", ctypes.c_int),
+                ("match_rounds", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -64,6 +65,7 @@ def lib():
         L.or_contract.restype = ctypes.c_int
         L.or_balance.restype = ctypes.c_int
         L.or_kaffpa.restype = ctypes.c_int
+        L.or_kaffpa_knobs.restype = ctypes.c_int
         L.or_hash.restype = ctypes.c_uint32
         L.or_hash.argtypes = [ctypes.c_uint64, ctypes.c_uint32]
         L.or_stream.restype = ctypes.c_uint64
@@ -127,6 +129,14 @@ def edge_cut(g: dict, part) -> int:
     return lib().or_edge_cut(G(g).ref, _p(np.ascontiguousarray(part, np.int32)))
 
 
+def stream(seed: int, tag: int, level: int, rnd: int) -> int:
+    return int(lib().or_stream(seed, tag, level, rnd))
+
+
+def hash32(ks: int, x: int) -> int:
+    return int(lib().or_hash(ctypes.c_uint64(ks), ctypes.c_uint32(x & 0xFFFFFFFF)))
+
+
 def block_weights(g: dict, part, k: int) -> np.ndarray:
     bw = np.zeros(k, np.uint32)
     lib().or_block_weights(G(g).ref, _p(np.ascontiguousarray(part, np.int32)), k,
@@ -143,6 +153,15 @@ def rating(g: dict) -> np.ndarray:
 def lp_cluster(g: dict, kn: Knobs, level=0) -> np.ndarray:
     lab = np.empty(g["n"], np.int32)
     lib().or_lp_cluster(G(g).ref, ctypes.byref(kn), level, _p(lab))
+    return lab
+
+
+def hem_match(g: dict, kn: Knobs, level=0, rating_q=None) -> np.ndarray:
+    """Heavy-edge matching labels of one level (min(v, mate) or v)."""
+    lab = np.empty(g["n"], np.int32)
+    rq = None if rating_q is None else np.ascontiguousarray(rating_q, np.uint32)
+    lib().or_hem_match(G(g).ref, ctypes.byref(kn), level,
+                       None if rq is None else rq.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), _p(lab))
     return lab
 
 
@@ -203,6 +222,19 @@ def kaffpa(g: dict, k: int, imbalance=0.03, seed=0, mode=0, unit_weights=False):
                          ctypes.byref(st))
     if rc != 0:
         raise ValueError(f"or_kaffpa rejected the input ({rc})")
+    return cut.value, part, st
+
+
+def kaffpa_knobs(g: dict, kn: Knobs, unit_weights=False):
+    """Whole schedule with explicit knobs.  Returns (edgecut, part, stats)."""
+    part = np.empty(g["n"], np.int32)
+    cut = ctypes.c_longlong()
+    st = Stats()
+    rc = lib().or_kaffpa_knobs(g["n"], None if unit_weights else _p(g["vwgt"]), _p(g["xadj"]),
+                               None if unit_weights else _p(g["adjwgt"]), _p(g["adjncy"]), ctypes.byref(kn),
+                               ctypes.byref(cut), _p(part), ctypes.byref(st))
+    if rc != 0:
+        raise ValueError(f"or_kaffpa_knobs rejected the input ({rc})")
     return cut.value, part, st
 
 

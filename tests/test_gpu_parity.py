@@ -205,3 +205,65 @@ def test_invalid_input_rejected(N):
         N.kaffpa_ex(np.array([0, 1, 2]), np.array([1, 5]), 2)       # target out of range
     with pytest.raises(KaHIPError):
         N.kaffpa_ex(np.array([0, 1, 2]), np.array([1, 0]), 0)       # k < 1
+
+
+def _sym_rating(g, seed):
+    """A symmetric uint32 rating per directed entry (stands in for a learned one)."""
+    rng = np.random.default_rng(seed)
+    n, xadj, adj = g["n"], g["xadj"], g["adjncy"]
+    src = np.repeat(np.arange(n), np.diff(xadj))
+    key = np.minimum(src, adj).astype(np.int64) * n + np.maximum(src, adj)
+    uniq, inv = np.unique(key, return_inverse=True)
+    r = rng.integers(0, 1 << 12, size=len(uniq)).astype(np.uint32)  # many equal ratings
+    return r[inv]
+
+
+@pytest.mark.parametrize("name", CASE_NAMES)
+@pytest.mark.parametrize("k,seed", [(8, 0), (64, 5)])
+def test_hem_match_parity(N, O, cases, name, k, seed):
+    g = cases[name]
+    kn_o = O.knobs(g, k, 0.03, seed, 0)
+    kn_p = N.derive_knobs(g["n"], g["vwgt"], k, 0.03, seed, 0)
+    for level in (0, 3):
+        a = O.hem_match(g, kn_o, level)
+        b = N.hem_match(g, kn_p, level)
+        assert np.array_equal(a, b), f"matching differs at {np.flatnonzero(a != b)[:10]}"
+    rq = _sym_rating(g, seed)
+    a = O.hem_match(g, kn_o, 1, rq)
+    b = N.hem_match(g, kn_p, 1, rq)
+    assert np.array_equal(a, b)
+    # a capped number of rounds is part of the schedule too
+    kn_o.match_rounds = kn_p.match_rounds = 2
+    assert np.array_equal(O.hem_match(g, kn_o, 0), N.hem_match(g, kn_p, 0))
+
+
+@pytest.mark.parametrize("name", CASE_NAMES)
+@pytest.mark.parametrize("k,mode,seed", [(8, 0, 0), (64, 1, 2)])
+def test_kaffpa_matching_coarsening_parity(N, O, cases, name, k, mode, seed):
+    g = cases[name]
+    kn_o = O.knobs(g, k, 0.03, seed, mode)
+    kn_p = N.derive_knobs(g["n"], g["vwgt"], k, 0.03, seed, mode)
+    kn_o.coarsening = kn_p.coarsening = 1
+    cut_o, part_o, st_o = O.kaffpa_knobs(g, kn_o)
+    st = N.Stats()
+    st.collect_level_cuts = 1
+    rc, cut_p, part_p = N.kaffpa_knobs(g["xadj"], g["adjncy"], kn_p, vwgt=g["vwgt"], adjwgt=g["adjwgt"], stats=st)
+    assert st.levels == st_o.levels
+    for l in range(st.levels):
+        assert (st.level_n[l], st.level_m[l], st.level_cut[l], st.level_maxbw[l]) == \
+               (st_o.level_n[l], st_o.level_m[l], st_o.level_cut[l], st_o.level_maxbw[l]), l
+    assert cut_p == cut_o
+    assert np.array_equal(part_p, part_o)
+    assert O.block_weights(g, part_p, k).max() <= kn_o.final_bound
+
+
+def test_matching_hub_rows(N, O):
+    """Rows longer than a warp's lane budget take the warp-cooperative path."""
+    n = 3000
+    edges = [(0, v) for v in range(1, n)] + [(v, v + 1) for v in range(1, n - 1)] + \
+            [(7, v) for v in range(100, 900)]
+    g = csr_from_edges(n, edges, weights=[1 + (i * 7919) % 13 for i in range(len(edges))])
+    for k in (2, 16):
+        kn_o = O.knobs(g, k, 0.03, 1, 0)
+        kn_p = N.derive_knobs(g["n"], g["vwgt"], k, 0.03, 1, 0)
+        assert np.array_equal(O.hem_match(g, kn_o, 0), N.hem_match(g, kn_p, 0))
