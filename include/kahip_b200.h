@@ -111,6 +111,45 @@ int kb200_kaffpa_device_knobs(int n, const int* d_vwgt, const int* d_xadj, const
                               const int* d_adjncy, const kb200_knobs* kn, long long* edgecut, int* d_part,
                               void* stream, kb200_stats* stats);
 
+/* ---- batches: many independent calls on one device ----
+ * Each worker thread leases its own context and stream; items are taken
+ * largest first.  Every item's result equals a single call with the same
+ * arguments.  workers <= 0 picks min(count, max(4, min(32, host threads))). */
+typedef struct kb200_batch_item {
+    int n;                     /* in: host CSR graph (NULL weights = unit) */
+    const int* xadj;
+    const int* adjncy;
+    const int* adjwgt;
+    const int* vwgt;
+    int nparts;                /* in: kaffpa() parameters of this item */
+    double imbalance;
+    int seed;
+    int mode;
+    int* part;                 /* out: caller-allocated n ints */
+    long long edgecut;         /* out: -1 when the item failed */
+    int status;                /* out: kb200 status of this item */
+} kb200_batch_item;
+
+typedef struct kb200_batch_report {
+    int workers;               /* concurrent workers used */
+    int failed;                /* items with a negative status */
+    double ms_total;           /* wall time of the batch on the host */
+} kb200_batch_report;
+
+/* Independent graphs, host buffers (KaFFPaE-style populations of several
+ * graphs, parameter sweeps).  Returns 0 when every item succeeded, else the
+ * first failing item's status. */
+int kb200_kaffpa_batch(kb200_batch_item* items, int count, int workers, kb200_batch_report* report);
+
+/* One device-resident graph, `count` seeds (a KaFFPaE-style population;
+ * lib/parallel_mh/parallel_mh_async.cpp:49-54 gives each member its own
+ * seed).  d_parts: count * n device ints, member i at d_parts + i*n;
+ * cuts[count] host out. */
+int kb200_kaffpa_population(int n, const int* d_vwgt, const int* d_xadj, const int* d_adjcwgt,
+                            const int* d_adjncy, int nparts, double imbalance, int mode, const int* seeds,
+                            int count, long long* cuts, int* d_parts, int workers,
+                            kb200_batch_report* report);
+
 /* ---- phases (host buffers), for parity checks against the CPU oracle ---- */
 
 /* Heavy-edge matching of one coarsening level (replaces random_matching.cpp:

@@ -7,11 +7,14 @@
 // sets *edgecut = -1 and leaves part[] untouched (the reference has no
 // error channel).  There is no CPU fallback: without a CUDA device the call
 // fails.
+#include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstring>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "contract.cuh"
@@ -194,6 +197,9 @@ int check_knobs(const kb200_knobs* kn) {
     return KB_OK;
 }
 
+int run_host_in(Ctx& ctx, int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+                const Knobs& kn, long long* edgecut, int* part, kb200_stats* st, clk::time_point t0);
+
 int run_host(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy, const Knobs& kn,
              long long* edgecut, int* part, kb200_stats* st) {
     auto t0 = clk::now();
@@ -203,7 +209,12 @@ int run_host(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const 
     int dev;
     if ((rc = current_device(&dev))) return rc;
     Lease lease(dev);
-    Ctx& ctx = *lease.ctx;
+    return run_host_in(*lease.ctx, n, vwgt, xadj, adjcwgt, adjncy, kn, edgecut, part, st, t0);
+}
+
+// The body of a host-buffer call on a leased context (input already validated).
+int run_host_in(Ctx& ctx, int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+                const Knobs& kn, long long* edgecut, int* part, kb200_stats* st, clk::time_point t0) {
     const long long m = xadj[n];
     for (int attempt = 0;; ++attempt) {
         try {
@@ -537,6 +548,163 @@ int kb200_initial_partition(int n, const int* xadj, const int* adjncy, const int
         if ((rc = validate(n, xadj, adjncy, adjwgt, vwgt)) || (rc = check_knobs(kn))) return rc;
         if (!adjwgt || !vwgt) return fail(KB_ERR_INVALID_INPUT, "explicit weights required");
         initial_partition(n, xadj, adjncy, adjwgt, vwgt, *kn, part);
+        return KB_OK;
+    });
+}
+
+// ------------------------------------------------------------- batches
+//
+// Many independent partitioning calls on the current device.  Each worker
+// thread leases its own context (arenas, stream) and takes items from a
+// shared counter, largest first; host initial partitioning runs on the
+// worker's thread (no nested threads), so the host cores are shared among
+// graphs instead.  Every item's result is the one a single call with the same
+// arguments returns.
+
+static int batch_workers(int requested, int count) {
+    if (requested > 0) return std::min(requested, std::max(count, 1));
+    unsigned hc = std::thread::hardware_concurrency();
+    int w = (int)std::max(4u, std::min(32u, hc ? hc : 8u));
+    return std::min(w, std::max(count, 1));
+}
+
+int kb200_kaffpa_batch(kb200_batch_item* items, int count, int workers, kb200_batch_report* report) {
+    g_last_error.clear();
+    return guarded([&]() -> int {
+        if (count < 0 || (count > 0 && !items)) return fail(KB_ERR_INVALID_INPUT, "invalid batch");
+        int dev, rc;
+        if ((rc = current_device(&dev))) return rc;
+        auto t0 = clk::now();
+        std::vector<int> order((size_t)count);
+        for (int i = 0; i < count; ++i) order[(size_t)i] = i;
+        auto size_of = [&](int i) {
+            const kb200_batch_item& it = items[i];
+            return (it.n >= 0 && it.xadj) ? (long long)it.xadj[it.n] + it.n : 0LL;
+        };
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return size_of(a) > size_of(b); });
+        const int W = batch_workers(workers, count);
+        std::atomic<int> next{0};
+        auto work = [&]() {
+            cudaSetDevice(dev);
+            set_ip_thread_limit(W > 1 ? 0 : -1);
+            std::unique_ptr<Lease> lease;
+            for (int j; (j = next.fetch_add(1)) < count;) {
+                kb200_batch_item& it = items[order[(size_t)j]];
+                it.edgecut = -1;
+                it.status = guarded([&]() -> int {
+                    int r = validate(it.n, it.xadj, it.adjncy, it.adjwgt, it.vwgt);
+                    if (r) return r;
+                    if (it.nparts < 1 || !(it.imbalance >= 0) || (it.n > 0 && !it.part))
+                        return fail(KB_ERR_INVALID_INPUT, "invalid batch item");
+                    Knobs kn;
+                    derive_knobs(it.n, it.vwgt, it.nparts, it.imbalance, it.seed, it.mode, kn);
+                    if (!lease) lease.reset(new Lease(dev));
+                    return run_host_in(*lease->ctx, it.n, it.vwgt, it.xadj, it.adjwgt, it.adjncy, kn, &it.edgecut,
+                                       it.part, nullptr, clk::now());
+                });
+            }
+            set_ip_thread_limit(-1);
+        };
+        std::vector<std::thread> pool;
+        for (int w = 1; w < W; ++w) pool.emplace_back(work);
+        work();
+        for (auto& t : pool) t.join();
+        int failed = 0, first = KB_OK;
+        for (int i = 0; i < count; ++i)
+            if (items[i].status < 0) {
+                if (!failed) first = items[i].status;
+                ++failed;
+            }
+        if (report) {
+            report->workers = W;
+            report->failed = failed;
+            report->ms_total = ms_since(t0);
+        }
+        if (failed) return fail(first, "some batch items failed (see their status)");
+        return KB_OK;
+    });
+}
+
+int kb200_kaffpa_population(int n, const int* d_vwgt, const int* d_xadj, const int* d_adjcwgt, const int* d_adjncy,
+                            int nparts, double imbalance, int mode, const int* seeds, int count, long long* cuts,
+                            int* d_parts, int workers, kb200_batch_report* report) {
+    g_last_error.clear();
+    return guarded([&]() -> int {
+        if (n < 0 || nparts < 1 || !(imbalance >= 0) || !d_xadj || !d_vwgt || !d_adjcwgt || count < 0 ||
+            (count > 0 && (!seeds || !cuts || !d_parts)))
+            return fail(KB_ERR_INVALID_INPUT, "invalid arguments");
+        int dev, rc;
+        if ((rc = current_device(&dev))) return rc;
+        auto t0 = clk::now();
+        DevGraph g;
+        uint32_t W = 0;
+        {
+            Lease lease(dev);
+            Ctx& ctx = *lease.ctx;
+            int m32 = 0;
+            KB_CUDA(cudaMemcpyAsync(&m32, d_xadj + n, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+            KB_CUDA(cudaStreamSynchronize(ctx.stream));
+            if (m32 < 0) return fail(KB_ERR_INVALID_INPUT, "xadj[n] < 0");
+            g.n = n;
+            g.m = m32;
+            g.xadj = d_xadj;
+            g.adjncy = d_adjncy;
+            g.adjwgt = d_adjcwgt;
+            g.vwgt = d_vwgt;
+            check_uploaded(ctx, g, &W);
+        }
+        const int Wk = batch_workers(workers, count);
+        std::atomic<int> next{0};
+        std::vector<int> status((size_t)count, KB_OK);
+        auto work = [&]() {
+            cudaSetDevice(dev);
+            set_ip_thread_limit(Wk > 1 ? 0 : -1);
+            std::unique_ptr<Lease> lease;
+            for (int i; (i = next.fetch_add(1)) < count;) {
+                cuts[i] = -1;
+                status[(size_t)i] = guarded([&]() -> int {
+                    if (!lease) lease.reset(new Lease(dev));
+                    Ctx& ctx = *lease->ctx;
+                    Knobs kn;
+                    derive_knobs_total(n, W, nparts, imbalance, seeds[i], mode, kn);
+                    for (int attempt = 0;; ++attempt) {
+                        try {
+                            reserve_for(ctx, n, g.m, false, attempt == 0 ? 1.0 : 2.0 * attempt);
+                            begin_stats(ctx, nullptr);
+                            long long cut = 0;
+                            int r = partition(ctx, g, kn, d_parts + (size_t)i * (size_t)n, &cut, nullptr);
+                            KB_CUDA(cudaStreamSynchronize(ctx.stream));
+                            cuts[i] = cut;
+                            return r;
+                        } catch (const CudaError& e) {
+                            if (e.code == cudaErrorMemoryAllocation && attempt < 2 &&
+                                std::string(e.what()).find("arena exhausted") != std::string::npos) {
+                                (void)cudaGetLastError();
+                                continue;
+                            }
+                            throw;
+                        }
+                    }
+                });
+            }
+            set_ip_thread_limit(-1);
+        };
+        std::vector<std::thread> pool;
+        for (int w = 1; w < Wk; ++w) pool.emplace_back(work);
+        work();
+        for (auto& t : pool) t.join();
+        int failed = 0, first = KB_OK;
+        for (int i = 0; i < count; ++i)
+            if (status[(size_t)i] < 0) {
+                if (!failed) first = status[(size_t)i];
+                ++failed;
+            }
+        if (report) {
+            report->workers = Wk;
+            report->failed = failed;
+            report->ms_total = ms_since(t0);
+        }
+        if (failed) return fail(first, "some population members failed");
         return KB_OK;
     });
 }

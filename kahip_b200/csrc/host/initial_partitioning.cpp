@@ -467,7 +467,10 @@ void recurse(const Knobs& kn, const HostGraph& g, const std::vector<int>& orig, 
     }
 }
 
+thread_local int t_spawn_limit = -1;
+
 int spawn_depth_for_host() {
+    if (t_spawn_limit >= 0) return t_spawn_limit;
     unsigned t = std::thread::hardware_concurrency();
     int d = 0;
     while (d < 6 && (2u << d) <= t) ++d;
@@ -475,6 +478,8 @@ int spawn_depth_for_host() {
 }
 
 }  // namespace
+
+void set_ip_thread_limit(int depth) { t_spawn_limit = depth; }
 
 void initial_partition(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
                        const Knobs& kn, int* part) {
