@@ -52,6 +52,11 @@ def parse():
     p.add_argument("--logn", type=int, default=FULL_LOGN, help="log2 of the RGG size (default 24)")
     p.add_argument("--k", type=int, default=K_BLOCKS)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", choices=["rgg", "batch", "population"], default="rgg",
+                   help="rgg: the headline single-graph workload (default); batch: many independent graphs "
+                        "of uneven size; population: many seeds of one device-resident RGG2D n=2^20")
+    p.add_argument("--batch-count", type=int, default=512, help="graphs in the batch workload")
+    p.add_argument("--population", type=int, default=64, help="seeds in the population workload")
     return p.parse_args()
 
 
@@ -244,6 +249,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
+    if args.workload != "rgg":
+        run_many(args, world, rank, dev)
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     g = graphs.rgg2d(1 << args.logn, seed=0)
     n, m = g["n"], g["m"]
@@ -417,6 +427,133 @@ def main():
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
+
+
+# ------------------------------------------------- batch / population forms
+
+def _ref_batch_task(args):
+    idx, count, seed = args
+    from kahip_b200 import graphs
+    from oracle import oracle
+    g, k = graphs.batch_mix(count, seed=seed)[idx]
+    t = time.perf_counter()
+    oracle.ref_kaffpa(dict(g, vwgt=None), k, IMBALANCE, idx, MODE_FAST)
+    return (time.perf_counter() - t) * 1e3
+
+
+def run_many(args, world, rank, dev):
+    """Many independent partitions per step: `batch` (graphs of uneven size,
+    n log-uniform in [1e3, 2e5], RGG2D / grid / R-MAT mix, k in {2..64}) or
+    `population` (seeds of one device-resident RGG2D n=2^20, k=64).  value =
+    partitions/s of the whole job; the serial GPU loop (one worker, same
+    inputs) is timed beside it."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from kahip_b200 import graphs, native
+
+    ranks_seed = 1000 * rank
+    if args.workload == "batch":
+        mix = graphs.batch_mix(args.batch_count, seed=ranks_seed)
+        gs = [g for g, _ in mix]
+        ks = [k for _, k in mix]
+        seeds = list(range(len(gs)))
+        nodes = sum(g["n"] for g in gs)
+        entries = sum(g["m"] for g in gs)
+        h2d = sum(4 * (g["n"] + 1 + 2 * g["m"] + g["n"]) for g in gs)
+        d2h = sum(4 * g["n"] for g in gs)
+
+        def step(workers):
+            cuts, parts, status, rep = native.kaffpa_batch(gs, ks, IMBALANCE, seeds, MODE_FAST, workers=workers)
+            assert rep.failed == 0
+            return rep.ms_total, rep.workers, cuts
+
+        count = len(gs)
+        workload = (f"batch of {count} independent graphs, n log-uniform in [1e3, 2e5] (total {nodes} nodes, "
+                    f"{entries} directed entries), RGG2D/grid/R-MAT mix, k in {{2..64}}, kaffpa fast, eps=3%")
+    else:
+        g = graphs.rgg2d(1 << 20, seed=0)
+        n = g["n"]
+        t = {key: torch.from_numpy(np.ascontiguousarray(g[key], np.int32)).to(dev)
+             for key in ("xadj", "adjncy", "adjwgt", "vwgt")}
+        count = args.population
+        seeds = [ranks_seed + i for i in range(count)]
+        parts = torch.empty(count * n, dtype=torch.int32, device=dev)
+        nodes, entries, h2d, d2h = count * n, count * g["m"], 0, 0
+
+        def step(workers):
+            torch.cuda.synchronize()
+            cuts, rep = native.kaffpa_population(n, t["xadj"], t["adjncy"], t["adjwgt"], t["vwgt"], parts, 64,
+                                                 seeds, IMBALANCE, MODE_FAST, workers=workers)
+            torch.cuda.synchronize()
+            assert rep.failed == 0
+            return rep.ms_total, rep.workers, cuts
+
+        workload = (f"population of {count} seeds of one device-resident RGG2D n=2^20 "
+                    f"({g['m']} directed entries), k=64, kaffpa fast, eps=3%")
+
+    for _ in range(max(1, args.warmup)):
+        step(0)
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid)
+    sampler.start()
+    if world > 1:
+        dist.barrier()
+    ms = []
+    workers = 0
+    launches0 = native.kernel_launches()
+    for _ in range(args.steps):
+        t_ms, workers, cuts = step(0)
+        ms.append(t_ms)
+    launches = native.kernel_launches() - launches0
+    if world > 1:
+        dist.barrier()
+    sampler.stop()
+    elapsed = sum(ms)
+    if world > 1:
+        tt = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed = float(tt.item())
+    value = count * args.steps * world / (elapsed * 1e-3)
+    serial_ms, _, cuts1 = step(1)
+    same = bool(np.array_equal(np.asarray(cuts1), np.asarray(cuts)))
+    cpu = None
+    if rank == 0 and args.workload == "batch" and not args.no_cpu_baseline:
+        from oracle import oracle
+        if oracle.ref_available():
+            procs = host_procs_for_reference()
+            sample = min(count, 4 * procs)
+            ctx = mp.get_context("spawn")
+            t0 = time.perf_counter()
+            with ctx.Pool(procs, initializer=_ref_worker_init) as pool:
+                pool.map(_ref_batch_task, [(i, args.batch_count, ranks_seed) for i in range(sample)])
+            wall = time.perf_counter() - t0
+            cpu = {"value": sample / wall, "unit": "partitions/s", "cores": procs, "kind": "reference",
+                   "sample": f"reference kaffpa fast on the first {sample} graphs of the batch, {procs} processes"}
+    if rank != 0:
+        return
+    line = {
+        "metric": f"partitions/s ({args.workload} form)", "value": value, "unit": "partitions/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": elapsed / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32", "data": "synthetic (seeded generators)",
+        "config": {"workload": workload, "workers": workers, "graphs_per_step": count,
+                   "l2": "each step streams more than the 126 MB L2; no flush"},
+        "serial_gpu_loop": {"value": count / (serial_ms * 1e-3), "unit": "partitions/s", "workers": 1,
+                            "same_cuts_as_batched": same},
+        "e2e": {"value": value, "unit": "partitions/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "api": "kb200_kaffpa_batch" if args.workload == "batch" else "kb200_kaffpa_population"},
+        "gpu_launches": launches,
+        "clocks": sampler.summary(),
+        "mean_cut": float(np.mean(cuts)),
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line))
 
 
 if __name__ == "__main__":

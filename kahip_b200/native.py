@@ -70,10 +70,24 @@ class Stats(ctypes.Structure):
                      maxbw=self.level_maxbw[i]) for i in range(self.levels)]
 
 
+class BatchItem(ctypes.Structure):
+    """kb200_batch_item"""
+    _fields_ = [("n", ctypes.c_int), ("xadj", ctypes.c_void_p), ("adjncy", ctypes.c_void_p),
+                ("adjwgt", ctypes.c_void_p), ("vwgt", ctypes.c_void_p), ("nparts", ctypes.c_int),
+                ("imbalance", ctypes.c_double), ("seed", ctypes.c_int), ("mode", ctypes.c_int),
+                ("part", ctypes.c_void_p), ("edgecut", ctypes.c_longlong), ("status", ctypes.c_int)]
+
+
+class BatchReport(ctypes.Structure):
+    """kb200_batch_report"""
+    _fields_ = [("workers", ctypes.c_int), ("failed", ctypes.c_int), ("ms_total", ctypes.c_double)]
+
+
 EXPORTS = [
     # extended ABI (include/kahip_b200.h)
     "kb200_derive_knobs", "kb200_kaffpa", "kb200_kaffpa_device", "kb200_kaffpa_knobs",
-    "kb200_kaffpa_device_knobs", "kb200_hem_match", "kb200_lp_cluster", "kb200_contract",
+    "kb200_kaffpa_device_knobs", "kb200_kaffpa_batch", "kb200_kaffpa_population", "kb200_hem_match",
+    "kb200_lp_cluster", "kb200_contract",
     "kb200_lp_refine", "kb200_balance", "kb200_edge_cut", "kb200_project", "kb200_initial_partition",
     "kb200_last_error", "kb200_kernel_launches", "kb200_device_count", "kb200_edge_cut_noalloc",
     # reference-compatible ABI (include/kaHIP_interface.h)
@@ -99,6 +113,9 @@ def lib():
         L.kb200_kaffpa_device_knobs.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), c_ll_p, vp, vp,
                                                 ctypes.POINTER(Stats)]
         L.kb200_hem_match.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, vp, vp]
+        L.kb200_kaffpa_batch.argtypes = [ctypes.POINTER(BatchItem), i, i, ctypes.POINTER(BatchReport)]
+        L.kb200_kaffpa_population.argtypes = [i, vp, vp, vp, vp, i, d, i, vp, i, vp, vp, i,
+                                              ctypes.POINTER(BatchReport)]
         L.kb200_lp_cluster.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, vp]
         L.kb200_contract.argtypes = [i, vp, vp, vp, vp, vp, c_int_p, c_ll_p, vp, vp, vp, vp, vp]
         L.kb200_lp_refine.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, u32, vp]
@@ -277,3 +294,45 @@ def kaffpa_device_knobs(n, xadj, adjncy, adjwgt, vwgt, part, kn: Knobs, stream=N
                                          ctypes.byref(stats) if stats else None)
     _check(rc)
     return rc, cut.value
+
+
+def kaffpa_batch(graphs: list, nparts, imbalance=0.03, seeds=0, modes=FAST, workers=0):
+    """Partitions many host graphs (dicts with xadj/adjncy and optional
+    adjwgt/vwgt) in one batch.  nparts/imbalance/seeds/modes: scalars or one
+    per graph.  Returns (cuts, parts, statuses, report)."""
+    cnt = len(graphs)
+
+    def per(x):
+        return list(x) if isinstance(x, (list, tuple, np.ndarray)) else [x] * cnt
+
+    ks, imbs, sds, mds = per(nparts), per(imbalance), per(seeds), per(modes)
+    keep = []
+    items = (BatchItem * max(cnt, 1))()
+    parts = []
+    for i, g in enumerate(graphs):
+        arrs = [_i32(g.get(key)) for key in ("xadj", "adjncy", "adjwgt", "vwgt")]
+        keep.append(arrs)
+        n = len(arrs[0]) - 1
+        p = np.zeros(max(n, 0), np.int32)
+        parts.append(p)
+        items[i] = BatchItem(n, _ptr(arrs[0]), _ptr(arrs[1]), _ptr(arrs[2]), _ptr(arrs[3]), int(ks[i]),
+                             float(imbs[i]), int(sds[i]), int(mds[i]), _ptr(p), -1, 0)
+    rep = BatchReport()
+    rc = lib().kb200_kaffpa_batch(items, cnt, workers, ctypes.byref(rep))
+    cuts = np.array([items[i].edgecut for i in range(cnt)], np.int64)
+    status = np.array([items[i].status for i in range(cnt)], np.int32)
+    if rc < 0 and rep.failed == 0:
+        _check(rc)
+    return cuts, parts, status, rep
+
+
+def kaffpa_population(n, xadj, adjncy, adjwgt, vwgt, parts, nparts, seeds, imbalance=0.03, mode=FAST, workers=0):
+    """One device-resident graph (CUDA int32 tensors), len(seeds) members;
+    parts: CUDA int32 tensor of len(seeds) * n.  Returns (cuts, report)."""
+    sd = np.ascontiguousarray(seeds, np.int32)
+    cuts = np.full(len(sd), -1, np.int64)
+    rep = BatchReport()
+    _check(lib().kb200_kaffpa_population(n, _ptr(vwgt), _ptr(xadj), _ptr(adjwgt), _ptr(adjncy), nparts, imbalance,
+                                         mode, _ptr(sd), len(sd), _ptr(cuts), _ptr(parts), workers,
+                                         ctypes.byref(rep)))
+    return cuts, rep
