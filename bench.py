@@ -37,7 +37,23 @@ sys.path.insert(0, ROOT)
 
 METRIC = "ms per kaffpa-fast partition & GE/s LP sweep (% HBM peak); cut vs plain at eps=3%"
 FULL_LOGN = 24
-SAMPLE_LOGN = 22
+
+# single-graph workloads: generator, description, log2 size of the bounded
+# reference sample
+GRAPH_KINDS = {
+    "rgg2d": ("RGG2D", "r=0.55*sqrt(ln n/n), unit weights", 22),
+    "rgg3d": ("RGG3D", "r=0.55*cbrt(ln n/n), unit weights", 20),
+    "rmat": ("R-MAT", "16n samples, a,b,c,d=.57,.19,.19,.05, duplicate multiplicity as edge weight", 14),
+}
+
+
+def make_graph(kind: str, logn: int):
+    from kahip_b200 import graphs
+    if kind == "rgg2d":
+        return graphs.rgg2d(1 << logn, seed=0)
+    if kind == "rgg3d":
+        return graphs.rgg3d(1 << logn, seed=0)
+    return graphs.rmat(logn, seed=0)
 K_BLOCKS = 64
 IMBALANCE = 0.03
 MODE_FAST = 0
@@ -55,6 +71,8 @@ def parse():
     p.add_argument("--workload", choices=["rgg", "batch", "population"], default="rgg",
                    help="rgg: the headline single-graph workload (default); batch: many independent graphs "
                         "of uneven size; population: many seeds of one device-resident RGG2D n=2^20")
+    p.add_argument("--graph", choices=sorted(GRAPH_KINDS), default="rgg2d",
+                   help="single-graph workload kind (default rgg2d, the headline)")
     p.add_argument("--batch-count", type=int, default=512, help="graphs in the batch workload")
     p.add_argument("--population", type=int, default=64, help="seeds in the population workload")
     return p.parse_args()
@@ -143,25 +161,25 @@ _SAMPLE = {}
 
 
 def _ref_task(args):
-    logn, k, seed = args
-    from kahip_b200 import graphs
+    kind, logn, k, seed = args
     from oracle import oracle
-    g = _SAMPLE.get(logn)
+    g = _SAMPLE.get((kind, logn))
     if g is None:
-        g = graphs.rgg2d(1 << logn, seed=0)
-        _SAMPLE[logn] = g
+        g = make_graph(kind, logn)
+        _SAMPLE[(kind, logn)] = g
     t = time.perf_counter()
-    cut, _ = oracle.ref_kaffpa(dict(g, vwgt=None, adjwgt=None), k, IMBALANCE, seed, MODE_FAST)
+    unit = kind != "rmat"
+    cut, _ = oracle.ref_kaffpa(dict(g, vwgt=None, adjwgt=None) if unit else g, k, IMBALANCE, seed, MODE_FAST)
     return (time.perf_counter() - t) * 1e3, cut, g["m"]
 
 
-def reference_sample_ms(logn: int, k: int, procs: int, seeds):
+def reference_sample_ms(logn: int, k: int, procs: int, seeds, kind: str = "rgg2d"):
     """Runs the reference kaffpa on the sample graph in `procs` processes;
     returns (wall ms, per-run ms list, cuts, m_sample)."""
     ctx = mp.get_context("spawn")
     t = time.perf_counter()
     with ctx.Pool(procs, initializer=_ref_worker_init) as pool:
-        res = pool.map(_ref_task, [(logn, k, s) for s in seeds])
+        res = pool.map(_ref_task, [(kind, logn, k, s) for s in seeds])
     wall = (time.perf_counter() - t) * 1e3
     return wall, [r[0] for r in res], [r[1] for r in res], res[0][2]
 
@@ -177,10 +195,9 @@ def host_procs_for_reference():
     return max(1, n)
 
 
-def full_m(logn: int) -> int:
-    from kahip_b200 import graphs
+def full_m(kind: str, logn: int) -> int:
     # the directed entry count of the full workload (generated once; cheap relative to the run)
-    return graphs.rgg2d(1 << logn, seed=0)["m"]
+    return make_graph(kind, logn)["m"]
 
 
 def run_reference_arm(args, rank):
@@ -192,25 +209,28 @@ def run_reference_arm(args, rank):
                           "(reference sources absent when __graft_entry__.build() ran)"}))
         return
     procs = host_procs_for_reference()
-    m_full = full_m(args.logn)
+    m_full = full_m(args.graph, args.logn)
+    sample_logn = GRAPH_KINDS[args.graph][2]
     step_ms = []
     cuts = []
     m_sample = None
     for step in range(args.warmup + args.steps):
         seeds = [step * procs + i for i in range(procs)]
-        wall, per, c, m_sample = reference_sample_ms(SAMPLE_LOGN, args.k, procs, seeds)
+        wall, per, c, m_sample = reference_sample_ms(sample_logn, args.k, procs, seeds, args.graph)
         if step >= args.warmup:
             step_ms.append(wall / procs)
             cuts += c
     scale = m_full / m_sample
     value = statistics.mean(step_ms) * scale
-    sample = (f"reference kaffpa fast (KaHIP built from its sources) on RGG2D n=2^{SAMPLE_LOGN} "
+    sample = (f"reference kaffpa fast (KaHIP built from its sources) on {GRAPH_KINDS[args.graph][0]} "
+              f"n=2^{sample_logn} "
               f"(m_directed={m_sample}), {procs} concurrent processes (one per core) per step; "
               f"ms per partition = step wall / {procs}, scaled x{scale:.3f} by directed edges to n=2^{args.logn}")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "ms", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded RGG2D generator)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": f"synthetic (seeded {GRAPH_KINDS[args.graph][0]} generator)",
         "config": workload_config(args, m_full),
         "cpu_baseline": {"value": value, "unit": "ms", "cores": procs, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -220,7 +240,8 @@ def run_reference_arm(args, rank):
 
 
 def workload_config(args, m):
-    return {"workload": f"kaffpa fast on RGG2D n=2^{args.logn} (r=0.55*sqrt(ln n/n)), k={args.k}, eps=3%",
+    name, desc, _ = GRAPH_KINDS[args.graph]
+    return {"workload": f"kaffpa fast on {name} n=2^{args.logn} ({desc}), k={args.k}, eps=3%",
             "n": 1 << args.logn, "m_directed": m, "k": args.k, "imbalance": IMBALANCE, "preset": "fast",
             "seed": 0, "graph_seed": 0, "l2": "inputs (~2.2 GB CSR) exceed the 126 MB L2; no flush",
             "parallelism": "replicas" if args.gpus > 1 else "single GPU"}
@@ -255,12 +276,13 @@ def main():
             dist.destroy_process_group()
         return
 
-    g = graphs.rgg2d(1 << args.logn, seed=0)
+    g = make_graph(args.graph, args.logn)
+    unit = args.graph != "rmat"
     n, m = g["n"], g["m"]
     d_xadj = torch.from_numpy(g["xadj"]).to(dev)
     d_adj = torch.from_numpy(g["adjncy"]).to(dev)
-    d_w = torch.ones(m, dtype=torch.int32, device=dev)
-    d_vw = torch.ones(n, dtype=torch.int32, device=dev)
+    d_w = torch.from_numpy(g["adjwgt"]).to(dev)
+    d_vw = torch.from_numpy(g["vwgt"]).to(dev)
     d_part = torch.empty(n, dtype=torch.int32, device=dev)
     stream = torch.cuda.Stream(device=dev)
 
@@ -332,13 +354,15 @@ def main():
     # ---- end to end through the host C ABI (pinned host buffers) ----
     h_xadj = torch.from_numpy(g["xadj"]).pin_memory()
     h_adj = torch.from_numpy(g["adjncy"]).pin_memory()
+    h_w = None if unit else torch.from_numpy(g["adjwgt"]).pin_memory()
     h_part = torch.empty(n, dtype=torch.int32).pin_memory()
     L = native.lib()
     import ctypes
     e2e_cut = ctypes.c_longlong()
 
     def e2e_call():
-        rc = L.kb200_kaffpa(n, None, h_xadj.data_ptr(), None, h_adj.data_ptr(), args.k, IMBALANCE, 0, MODE_FAST,
+        rc = L.kb200_kaffpa(n, None, h_xadj.data_ptr(), None if h_w is None else h_w.data_ptr(), h_adj.data_ptr(),
+                            args.k, IMBALANCE, 0, MODE_FAST,
                             ctypes.byref(e2e_cut), h_part.data_ptr(), None)
         if rc < 0:
             raise RuntimeError(L.kb200_last_error().decode())
@@ -393,11 +417,12 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": ms_per_step, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded RGG2D generator)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": f"synthetic (seeded {GRAPH_KINDS[args.graph][0]} generator)",
         "config": workload_config(args, m),
         "roofline": roofline,
-        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 4 * (n + 1 + m),
-                "d2h_bytes_per_step": 4 * n, "api": "kb200_kaffpa (host C ABI, NULL weights, pinned buffers)",
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": 4 * (n + 1 + m) + (0 if unit else 4 * m),
+                "d2h_bytes_per_step": 4 * n, "api": "kb200_kaffpa (host C ABI, pinned buffers, NULL = unit weights)",
                 "same_partition_as_device_path": e2e_same},
         "gpu_launches": launches,
         "clocks": sampler.summary(),
@@ -413,12 +438,14 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle
         if oracle.ref_available():
-            wall, per, c, m_sample = reference_sample_ms(SAMPLE_LOGN, args.k, 1, [0])
+            sample_logn = GRAPH_KINDS[args.graph][2]
+            wall, per, c, m_sample = reference_sample_ms(sample_logn, args.k, 1, [0], args.graph)
             scale = m / m_sample
             line["cpu_baseline"] = {
                 "value": per[0] * scale, "unit": "ms", "cores": 1, "kind": "reference",
                 "sample": (f"one reference kaffpa fast run (KaHIP built from its sources, single-threaded) on "
-                           f"RGG2D n=2^{SAMPLE_LOGN} (m_directed={m_sample}, {per[0]:.0f} ms, cut {c[0]}), "
+                           f"{GRAPH_KINDS[args.graph][0]} n=2^{sample_logn} (m_directed={m_sample}, "
+                           f"{per[0]:.0f} ms, cut {c[0]}), "
                            f"scaled x{scale:.3f} by directed edges to n=2^{args.logn}")}
         else:
             line["cpu_baseline"] = {"value": None, "unit": "ms", "cores": 0, "kind": "reference",
@@ -435,7 +462,8 @@ def _ref_batch_task(args):
     idx, count, seed = args
     from kahip_b200 import graphs
     from oracle import oracle
-    g, k = graphs.batch_mix(count, seed=seed)[idx]
+    spec = graphs.batch_specs(count, seed=seed)[idx]
+    g, k = graphs.batch_graph(spec), spec[2]
     t = time.perf_counter()
     oracle.ref_kaffpa(dict(g, vwgt=None), k, IMBALANCE, idx, MODE_FAST)
     return (time.perf_counter() - t) * 1e3

@@ -96,27 +96,38 @@ def from_csr(xadj, adjncy, adjwgt=None, vwgt=None) -> dict:
                 vwgt=np.ones(n, np.int32) if vwgt is None else np.ascontiguousarray(vwgt, np.int32))
 
 
-def batch_mix(count: int, seed: int = 0, nmin: float = 1e3, nmax: float = 2e5,
-              ks=(2, 4, 8, 16, 32, 64)) -> list:
-    """A seeded mix of independent graphs for the batched form: n log-uniform
-    in [nmin, nmax], kind uniform over 2D RGG (r = 0.55 sqrt(ln n / n)), 2D
-    grid with the 5-point stencil (nx*ny ~ n) and R-MAT (2^round(log2 n)
-    nodes, 4 samples per node -> average degree ~8, a,b,c = .57,.19,.19);
-    k uniform over `ks`.  Returns [(graph, k), ...]."""
+def batch_specs(count: int, seed: int = 0, nmin: float = 1e3, nmax: float = 2e5,
+                ks=(2, 4, 8, 16, 32, 64)) -> list:
+    """Seeded specs (kind, n, k, graph_seed) of the batched form's graphs: n
+    log-uniform in [nmin, nmax], kind uniform over 2D RGG / 2D grid / R-MAT,
+    k uniform over `ks`."""
     rng = np.random.default_rng(seed)
     out = []
-    for i in range(count):
+    for _ in range(count):
         n = int(np.exp(rng.uniform(np.log(nmin), np.log(nmax))))
         kind = int(rng.integers(0, 3))
         k = int(ks[int(rng.integers(0, len(ks)))])
         gs = int(rng.integers(0, 1 << 30))
-        if kind == 0:
-            g = rgg2d(n, seed=gs)
-        elif kind == 1:
-            nx = max(1, int(round(np.sqrt(n))))
-            g = grid2d(nx, max(1, n // nx))
-        else:
-            scale = max(1, int(round(np.log2(n))))
-            g = rmat(scale, samples=4 << scale, seed=gs)
-        out.append((g, k))
+        out.append((kind, n, k, gs))
     return out
+
+
+def batch_graph(spec) -> dict:
+    """The graph of one batch spec: RGG2D (r = 0.55 sqrt(ln n / n)), grid with
+    the 5-point stencil (nx*ny ~ n) or R-MAT (2^round(log2 n) nodes, 4 samples
+    per node -> average degree ~8, a,b,c = .57,.19,.19)."""
+    kind, n, _, gs = spec
+    if kind == 0:
+        return rgg2d(n, seed=gs)
+    if kind == 1:
+        nx = max(1, int(round(np.sqrt(n))))
+        return grid2d(nx, max(1, n // nx))
+    scale = max(1, int(round(np.log2(n))))
+    return rmat(scale, samples=4 << scale, seed=gs)
+
+
+def batch_mix(count: int, seed: int = 0, nmin: float = 1e3, nmax: float = 2e5,
+              ks=(2, 4, 8, 16, 32, 64)) -> list:
+    """A seeded mix of independent graphs for the batched form (see
+    batch_specs / batch_graph).  Returns [(graph, k), ...]."""
+    return [(batch_graph(sp), sp[2]) for sp in batch_specs(count, seed, nmin, nmax, ks)]
