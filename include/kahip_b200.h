@@ -55,9 +55,17 @@ typedef struct kb200_knobs {
     int bal_iters;                                 /* balance repair */
     int ip_reps, ip_tries, ip_fm_passes, ip_fm_stall; /* initial partitioning */
     int max_levels;
-    int coarsening;            /* 0 = LP clustering (default), 1 = heavy-edge matching */
+    int coarsening;            /* 0 = LP clustering (default), 1 = heavy-edge matching on
+                                  expansion*^2, 2 = heavy-edge matching on the learned rating */
     int match_rounds;          /* cap on locally-dominant matching rounds per level */
+    const float* rating_model; /* coarsening 2: host array of KB200_RATING_PARAMS floats
+                                  (NULL = fall back to expansion*^2) */
+    double rating_fallback;    /* coarsening 2: > 0 also runs the expansion*^2 matching and
+                                  keeps it when learned cut > rating_fallback * its cut */
 } kb200_knobs;
+
+/* Parameter count of the learned edge rating (kahip_b200/csrc/learned.cuh). */
+#define KB200_RATING_PARAMS 27137
 
 /* Per-call report.  level 0 is the input graph. */
 typedef struct kb200_stats {
@@ -84,6 +92,8 @@ typedef struct kb200_stats {
     long long sweep_vertices, sweep_edges;
     long long sweep_overflow_vertices;   /* of which needed the shared-table path */
     size_t device_bytes_peak;
+    int rating_fallback_used;  /* coarsening 2 with rating_fallback: 1 = the expansion*^2
+                                  partition was returned */
 } kb200_stats;
 
 int kb200_derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, int mode,
@@ -149,6 +159,36 @@ int kb200_kaffpa_population(int n, const int* d_vwgt, const int* d_xadj, const i
                             const int* d_adjncy, int nparts, double imbalance, int mode, const int* seeds,
                             int count, long long* cuts, int* d_parts, int workers,
                             kb200_batch_report* report);
+
+/* ---- learned edge rating (no counterpart in the reference) ----
+ * A 3-layer message-passing network (hidden 64, BF16 weights and
+ * activations, FP32 accumulation) predicting per directed entry the
+ * probability p that a partition cuts the edge; the matching rating is
+ * floor((1 - p) * 2^24).  params: KB200_RATING_PARAMS host floats. */
+
+/* prob[m] / rating[m] out (either may be NULL); use_tc = 1 runs the layer
+ * GEMMs on the tensor cores (tcgen05), 0 on the CUDA cores. */
+int kb200_rating_infer(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                       const float* params, int use_tc, float* prob, uint32_t* rating);
+
+/* One training graph: host CSR (explicit weights) and one 0/1 label per
+ * directed entry (1 = cut). */
+typedef struct kb200_train_graph {
+    int n;
+    const int* xadj;
+    const int* adjncy;
+    const int* adjwgt;
+    const int* vwgt;
+    const uint8_t* label;
+} kb200_train_graph;
+
+/* Adam on the weighted BCE of the labels, one graph per step (round robin):
+ * params in/out (host), loss[steps] out (host, may be NULL). */
+int kb200_rating_train(const kb200_train_graph* graphs, int count, int steps, float lr, float* params,
+                       float* loss);
+
+/* Loss and gradient of one graph at params (host out: grad[KB200_RATING_PARAMS], *loss). */
+int kb200_rating_grad(const kb200_train_graph* graph, const float* params, float* grad, float* loss);
 
 /* ---- phases (host buffers), for parity checks against the CPU oracle ---- */
 

@@ -20,6 +20,7 @@
 #include "contract.cuh"
 #include "host/initial_partitioning.h"
 #include "knobs.h"
+#include "learned.cuh"
 #include "match.cuh"
 #include "partitioner.cuh"
 #include "prims.cuh"
@@ -192,7 +193,7 @@ double ms_since(clk::time_point t) { return std::chrono::duration<double, std::m
 int check_knobs(const kb200_knobs* kn) {
     if (!kn) return fail(KB_ERR_INVALID_INPUT, "knobs is NULL");
     if (kn->k < 1 || kn->lpc_subrounds < 1 || kn->ref_subrounds < 1 || kn->ref_classes < 1 ||
-        kn->coarsening < 0 || kn->coarsening > 1 || kn->max_levels < 1 || kn->max_levels > 64)
+        kn->coarsening < 0 || kn->coarsening > 2 || kn->max_levels < 1 || kn->max_levels > 64)
         return fail(KB_ERR_INVALID_INPUT, "invalid knobs");
     return KB_OK;
 }
@@ -404,6 +405,116 @@ int kb200_hem_match(int n, const int* xadj, const int* adjncy, const int* adjwgt
         hem_match(pr.ctx, pr.up.g, *kn, level, dr, d);
         if (n) KB_CUDA(cudaMemcpyAsync(label, d, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
         KB_CUDA(cudaStreamSynchronize(s));
+        return KB_OK;
+    });
+}
+
+int kb200_rating_infer(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                       const float* params, int use_tc, float* prob, uint32_t* rating) {
+    g_last_error.clear();
+    return guarded([&]() -> int {
+        int rc, dev;
+        if ((rc = validate(n, xadj, adjncy, adjwgt, vwgt))) return rc;
+        if (!params) return fail(KB_ERR_INVALID_INPUT, "params is NULL");
+        if ((rc = current_device(&dev))) return rc;
+        PhaseRun pr(dev, n, xadj, adjncy, adjwgt, vwgt);
+        cudaStream_t s = pr.ctx.stream;
+        const long long m = xadj[n];
+        const size_t mm = (size_t)std::max<long long>(m, 1);
+        float* dp = pr.ctx.hier.alloc<float>(rm::kParams);
+        float* dprob = prob ? pr.ctx.hier.alloc<float>(mm) : nullptr;
+        uint32_t* drat = rating ? pr.ctx.hier.alloc<uint32_t>(mm) : nullptr;
+        KB_CUDA(cudaMemcpyAsync(dp, params, sizeof(float) * rm::kParams, cudaMemcpyHostToDevice, s));
+        rating_infer(pr.ctx, pr.up.g, dp, dprob, drat, use_tc != 0);
+        int err = 0;
+        KB_CUDA(cudaMemcpyAsync(&err, pr.ctx.dscalars + 60, sizeof(int), cudaMemcpyDeviceToHost, s));
+        if (m && prob) KB_CUDA(cudaMemcpyAsync(prob, dprob, sizeof(float) * (size_t)m, cudaMemcpyDeviceToHost, s));
+        if (m && rating)
+            KB_CUDA(cudaMemcpyAsync(rating, drat, sizeof(uint32_t) * (size_t)m, cudaMemcpyDeviceToHost, s));
+        KB_CUDA(cudaStreamSynchronize(s));
+        if (err) return fail(KB_ERR_INTERNAL, "tensor-core layer kernel gave up waiting for its MMAs");
+        return KB_OK;
+    });
+}
+
+// Device copies of training graphs (explicit weights) and their labels.
+struct TrainUpload {
+    std::vector<TrainGraph> tg;
+};
+
+static int upload_train(Ctx& ctx, const kb200_train_graph* graphs, int count, TrainUpload& out) {
+    cudaStream_t s = ctx.stream;
+    for (int i = 0; i < count; ++i) {
+        const kb200_train_graph& t = graphs[i];
+        int rc = validate(t.n, t.xadj, t.adjncy, t.adjwgt, t.vwgt);
+        if (rc) return rc;
+        if (!t.adjwgt || !t.vwgt || (t.xadj[t.n] > 0 && !t.label))
+            return fail(KB_ERR_INVALID_INPUT, "training graphs need explicit weights and labels");
+        Upload u = upload(ctx, t.n, t.xadj, t.adjncy, t.adjwgt, t.vwgt);
+        check_uploaded(ctx, u.g);
+        u.g.maxdeg = max_degree(ctx, u.g);
+        const long long m = t.xadj[t.n];
+        uint8_t* dl = ctx.hier.alloc<uint8_t>((size_t)std::max<long long>(m, 1));
+        if (m) KB_CUDA(cudaMemcpyAsync(dl, t.label, (size_t)m, cudaMemcpyHostToDevice, s));
+        out.tg.push_back(TrainGraph{u.g, dl});
+    }
+    return KB_OK;
+}
+
+static void reserve_train(Ctx& ctx, const kb200_train_graph* graphs, int count) {
+    double hier = (double)rm::kParams * 4 + (1 << 20), scr = (1 << 24);
+    long long nmax = 1;
+    for (int i = 0; i < count; ++i) {
+        const long long n = graphs[i].n, m = graphs[i].xadj[graphs[i].n];
+        hier += 4.0 * (n + 1) + 13.0 * m + 8.0 * n + 2048;
+        nmax = std::max(nmax, n);
+    }
+    scr += (double)nmax * 4 * (2 + 1 + 4 * 64 + 3 * 64 + 32 + 32 + 5 * 64) + 4.0 * rm::kParams * 4 + (1 << 20);
+    ctx.hier.reserve((size_t)hier);
+    ctx.scratch.reserve((size_t)scr);
+}
+
+int kb200_rating_train(const kb200_train_graph* graphs, int count, int steps, float lr, float* params, float* loss) {
+    g_last_error.clear();
+    return guarded([&]() -> int {
+        int rc, dev;
+        if (count < 1 || !graphs || steps < 0 || !params) return fail(KB_ERR_INVALID_INPUT, "invalid arguments");
+        if ((rc = current_device(&dev))) return rc;
+        Lease lease(dev);
+        Ctx& ctx = *lease.ctx;
+        reserve_train(ctx, graphs, count);
+        ctx.timing = false;
+        ctx.reset_stats();
+        TrainUpload tu;
+        if ((rc = upload_train(ctx, graphs, count, tu))) return rc;
+        float* dp = ctx.hier.alloc<float>(rm::kParams);
+        KB_CUDA(cudaMemcpyAsync(dp, params, sizeof(float) * rm::kParams, cudaMemcpyHostToDevice, ctx.stream));
+        rating_train(ctx, tu.tg.data(), count, steps, lr, dp, loss);
+        KB_CUDA(cudaMemcpyAsync(params, dp, sizeof(float) * rm::kParams, cudaMemcpyDeviceToHost, ctx.stream));
+        KB_CUDA(cudaStreamSynchronize(ctx.stream));
+        return KB_OK;
+    });
+}
+
+int kb200_rating_grad(const kb200_train_graph* graph, const float* params, float* grad, float* loss) {
+    g_last_error.clear();
+    return guarded([&]() -> int {
+        int rc, dev;
+        if (!graph || !params || !grad || !loss) return fail(KB_ERR_INVALID_INPUT, "invalid arguments");
+        if ((rc = current_device(&dev))) return rc;
+        Lease lease(dev);
+        Ctx& ctx = *lease.ctx;
+        reserve_train(ctx, graph, 1);
+        ctx.timing = false;
+        ctx.reset_stats();
+        TrainUpload tu;
+        if ((rc = upload_train(ctx, graph, 1, tu))) return rc;
+        float* dp = ctx.hier.alloc<float>(rm::kParams);
+        float* dg = ctx.hier.alloc<float>(rm::kParams);
+        KB_CUDA(cudaMemcpyAsync(dp, params, sizeof(float) * rm::kParams, cudaMemcpyHostToDevice, ctx.stream));
+        rating_grad(ctx, tu.tg[0], dp, dg, loss);
+        KB_CUDA(cudaMemcpyAsync(grad, dg, sizeof(float) * rm::kParams, cudaMemcpyDeviceToHost, ctx.stream));
+        KB_CUDA(cudaStreamSynchronize(ctx.stream));
         return KB_OK;
     });
 }

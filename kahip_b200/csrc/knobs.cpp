@@ -77,6 +77,8 @@ void derive_knobs_total(int n, uint32_t W, int k, double imbalance, int seed, in
     kn.max_levels = 48;
     kn.coarsening = 0;                   // LP clustering; 1 selects heavy-edge matching
     kn.match_rounds = 16;                // matching converges in < 10 rounds on meshes
+    kn.rating_model = nullptr;
+    kn.rating_fallback = 0.0;
 }
 
 }  // namespace kb

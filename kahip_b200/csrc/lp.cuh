@@ -60,6 +60,14 @@ int check_graph(Ctx& ctx, const DevGraph& g, uint32_t* total_weight = nullptr);
 // (synchronises the stream)
 bool rows_strictly_increasing(Ctx& ctx, const DevGraph& g);
 
+// Bundles the isolated vertices (degree 0) of a level, which no clustering
+// or matching can merge: in increasing id order, consecutive groups of
+// G = (bound - 1) / (largest isolated node weight) vertices (all of them when
+// that weight is 0) share the label of their first member, so every bundle
+// weighs less than `bound`.  Nothing changes when G < 2 or fewer than two
+// vertices are isolated.  label[] of non-isolated vertices is left as is.
+void bundle_isolated(Ctx& ctx, const DevGraph& g, uint32_t bound, int* label);
+
 // label[v] = v, cw[v] = vwgt[v]
 void init_labels(Ctx& ctx, const DevGraph& g, int* label, uint32_t* cw);
 

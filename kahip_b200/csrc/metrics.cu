@@ -51,6 +51,31 @@ __global__ void maxdeg_kernel(int n, const int* __restrict__ xadj, int* out) {
     if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
+// isolated vertices: flag[v] = 1, and the largest isolated node weight
+__global__ void iso_flags(int n, const int* __restrict__ xadj, const int* __restrict__ vwgt, uint32_t* flag,
+                          unsigned* wmax) {
+    unsigned w = 0;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const bool iso = xadj[v + 1] == xadj[v];
+        flag[v] = iso ? 1u : 0u;
+        if (iso) w = max(w, (unsigned)vwgt[v]);
+    }
+    for (int o = 16; o >= 1; o >>= 1) w = max(w, __shfl_xor_sync(0xffffffffu, w, o));
+    if ((threadIdx.x & 31) == 0 && w) atomicMax(wmax, w);
+}
+
+// ids[rank] = v for isolated v (rank = exclusive prefix count)
+__global__ void iso_ids(int n, const int* __restrict__ xadj, const uint32_t* __restrict__ rank, int* ids) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        if (xadj[v + 1] == xadj[v]) ids[rank[v]] = v;
+}
+
+__global__ void iso_label(int n, const int* __restrict__ xadj, const uint32_t* __restrict__ rank,
+                          const int* __restrict__ ids, uint32_t group, int* label) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        if (xadj[v + 1] == xadj[v]) label[v] = ids[(rank[v] / group) * group];
+}
+
 __global__ void init_labels_kernel(int n, const int* __restrict__ vwgt, int* label, uint32_t* cw) {
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
         label[v] = v;
@@ -157,6 +182,34 @@ bool rows_strictly_increasing(Ctx& ctx, const DevGraph& g) {
     KB_CUDA(cudaMemcpyAsync(ctx.pinned + 4, d, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
     KB_CUDA(cudaStreamSynchronize(ctx.stream));
     return ctx.pinned[4] == 0;
+}
+
+void bundle_isolated(Ctx& ctx, const DevGraph& g, uint32_t bound, int* label) {
+    if (g.n < 2 || bound < 2) return;
+    cudaStream_t s = ctx.stream;
+    const size_t mk = ctx.scratch.mark();
+    uint32_t* rank = ctx.scratch.alloc<uint32_t>((size_t)g.n);
+    int* ids = ctx.scratch.alloc<int>((size_t)g.n);
+    uint32_t* d = reinterpret_cast<uint32_t*>(ctx.dscalars + 6);  // [6] count, [7] max weight
+    {
+        PhaseScope ps(ctx, "isolated_bundles", 12.0 * g.n);
+        KB_CUDA(cudaMemsetAsync(d, 0, 2 * sizeof(uint32_t), s));
+        iso_flags<<<grid_for(g.n, 256), 256, 0, s>>>(g.n, g.xadj, g.vwgt, rank, d + 1);
+        KB_LAUNCH();
+        exclusive_scan_u32(rank, rank, g.n, d, s, ctx.scratch);
+    }
+    KB_CUDA(cudaMemcpyAsync(ctx.pinned + 6, d, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    KB_CUDA(cudaStreamSynchronize(s));
+    const uint32_t count = ctx.pinned[6], wmax = ctx.pinned[7];
+    const uint32_t group = wmax == 0 ? count : (bound - 1) / wmax;
+    if (count >= 2 && group >= 2) {
+        PhaseScope ps(ctx, "isolated_bundles", 12.0 * g.n);
+        iso_ids<<<grid_for(g.n, 256), 256, 0, s>>>(g.n, g.xadj, rank, ids);
+        KB_LAUNCH();
+        iso_label<<<grid_for(g.n, 256), 256, 0, s>>>(g.n, g.xadj, rank, ids, group, label);
+        KB_LAUNCH();
+    }
+    ctx.scratch.release(mk);
 }
 
 void init_labels(Ctx& ctx, const DevGraph& g, int* label, uint32_t* cw) {

@@ -11,6 +11,7 @@
 
 #include "contract.cuh"
 #include "host/initial_partitioning.h"
+#include "learned.cuh"
 #include "match.cuh"
 #include "prims.cuh"
 
@@ -141,14 +142,20 @@ void reserve_for(Ctx& ctx, int n, long long m, bool copy_input, double factor) {
     ctx.scratch.reserve((size_t)(scr * factor));
 }
 
-int partition(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_part, long long* edgecut,
-              kb200_stats* st) {
+static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_part, long long* edgecut,
+                          kb200_stats* st) {
     const int k = kn.k;
     const bool collect = st && st->collect_level_cuts;
     cudaStream_t s = ctx.stream;
     std::vector<Level> lv;
     lv.push_back(Level{g0, nullptr, d_part});
     lv[0].g.maxdeg = max_degree(ctx, lv[0].g);
+    // learned rating: the model's parameters, once per call
+    float* d_model = nullptr;
+    if (kn.coarsening == 2 && kn.rating_model) {
+        d_model = ctx.hier.alloc<float>(rm::kParams);
+        KB_CUDA(cudaMemcpyAsync(d_model, kn.rating_model, sizeof(float) * rm::kParams, cudaMemcpyHostToDevice, s));
+    }
 
     // ---------------------------------------------------------- coarsening
     auto t0 = clk::now();
@@ -159,8 +166,16 @@ int partition(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_part, long l
             lv[L].cmap = ctx.hier.alloc<int>((size_t)f.n);
             const size_t mk = ctx.scratch.mark();
             int* label = ctx.scratch.alloc<int>((size_t)f.n);
-            if (kn.coarsening == 1) hem_match(ctx, f, kn, L, nullptr, label);
-            else lp_cluster(ctx, f, kn, L, label);
+            if (kn.coarsening == 2 && d_model) {
+                uint32_t* rating = ctx.scratch.alloc<uint32_t>((size_t)std::max<long long>(f.m, 1));
+                rating_infer(ctx, f, d_model, nullptr, rating, true);
+                hem_match(ctx, f, kn, L, rating, label);
+            } else if (kn.coarsening >= 1) {
+                hem_match(ctx, f, kn, L, nullptr, label);
+            } else {
+                lp_cluster(ctx, f, kn, L, label);
+            }
+            bundle_isolated(ctx, f, kn.coarsening == 0 ? kn.cluster_bound : kn.max_vertex_weight + 1u, label);
             Level c;
             int *cx, *ca, *cw, *cv;
             contract(ctx, f, label, lv[L].cmap, c.g, &cx, &ca, &cw, &cv);
@@ -244,6 +259,35 @@ int partition(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_part, long l
         st->ms_uncoarsen = ms_uncoarsen;
     }
     return balanced ? KB_OK : KB_WARN_IMBALANCED;
+}
+
+int partition(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_part, long long* edgecut,
+              kb200_stats* st) {
+    if (st) st->rating_fallback_used = 0;
+    if (!(kn.coarsening == 2 && kn.rating_model && kn.rating_fallback > 0))
+        return partition_once(ctx, g0, kn, d_part, edgecut, st);
+    // learned rating with a guard: the expansion*^2 matching runs too, and
+    // its partition is kept when the learned one cuts more than
+    // rating_fallback times as much
+    int* plain = ctx.hier.alloc<int>((size_t)std::max(g0.n, 1));
+    const size_t mk = ctx.hier.mark();
+    Knobs kp = kn;
+    kp.coarsening = 1;
+    long long cut_plain = 0;
+    const int rp = partition_once(ctx, g0, kp, plain, &cut_plain, nullptr);
+    ctx.hier.release(mk);
+    long long cut_learned = 0;
+    const int rl = partition_once(ctx, g0, kn, d_part, &cut_learned, st);
+    if ((double)cut_learned > kn.rating_fallback * (double)cut_plain) {
+        if (g0.n)
+            KB_CUDA(cudaMemcpyAsync(d_part, plain, sizeof(int) * (size_t)g0.n, cudaMemcpyDeviceToDevice, ctx.stream));
+        KB_CUDA(cudaStreamSynchronize(ctx.stream));
+        *edgecut = cut_plain;
+        if (st) st->rating_fallback_used = 1;
+        return rp;
+    }
+    *edgecut = cut_learned;
+    return rl;
 }
 
 }  // namespace kb

@@ -39,7 +39,8 @@ class Knobs(ctypes.Structure):
                 ("ip_reps", ctypes.c_int), ("ip_tries", ctypes.c_int),
                 ("ip_fm_passes", ctypes.c_int), ("ip_fm_stall", ctypes.c_int),
                 ("max_levels", ctypes.c_int), ("coarsening", ctypes.c_int),
-                ("match_rounds", ctypes.c_int)]
+                ("match_rounds", ctypes.c_int), ("rating_model", ctypes.c_void_p),
+                ("rating_fallback", ctypes.c_double)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -58,7 +59,7 @@ class Stats(ctypes.Structure):
                 ("family_ms", ctypes.c_double * 16), ("family_bytes", ctypes.c_double * 16),
                 ("family_launches", ctypes.c_longlong * 16), ("sweep_vertices", ctypes.c_longlong),
                 ("sweep_edges", ctypes.c_longlong), ("sweep_overflow_vertices", ctypes.c_longlong),
-                ("device_bytes_peak", ctypes.c_size_t)]
+                ("device_bytes_peak", ctypes.c_size_t), ("rating_fallback_used", ctypes.c_int)]
 
     def families(self) -> dict:
         return {self.family_name[i].value.decode(): dict(ms=self.family_ms[i], bytes=self.family_bytes[i],
@@ -68,6 +69,15 @@ class Stats(ctypes.Structure):
     def levels_list(self):
         return [dict(n=self.level_n[i], m=self.level_m[i], cut=self.level_cut[i],
                      maxbw=self.level_maxbw[i]) for i in range(self.levels)]
+
+
+RATING_PARAMS = 27137
+
+
+class TrainGraph(ctypes.Structure):
+    """kb200_train_graph"""
+    _fields_ = [("n", ctypes.c_int), ("xadj", ctypes.c_void_p), ("adjncy", ctypes.c_void_p),
+                ("adjwgt", ctypes.c_void_p), ("vwgt", ctypes.c_void_p), ("label", ctypes.c_void_p)]
 
 
 class BatchItem(ctypes.Structure):
@@ -87,6 +97,7 @@ EXPORTS = [
     # extended ABI (include/kahip_b200.h)
     "kb200_derive_knobs", "kb200_kaffpa", "kb200_kaffpa_device", "kb200_kaffpa_knobs",
     "kb200_kaffpa_device_knobs", "kb200_kaffpa_batch", "kb200_kaffpa_population", "kb200_hem_match",
+    "kb200_rating_infer", "kb200_rating_train", "kb200_rating_grad",
     "kb200_lp_cluster", "kb200_contract",
     "kb200_lp_refine", "kb200_balance", "kb200_edge_cut", "kb200_project", "kb200_initial_partition",
     "kb200_last_error", "kb200_kernel_launches", "kb200_device_count", "kb200_edge_cut_noalloc",
@@ -113,6 +124,9 @@ def lib():
         L.kb200_kaffpa_device_knobs.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), c_ll_p, vp, vp,
                                                 ctypes.POINTER(Stats)]
         L.kb200_hem_match.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, vp, vp]
+        L.kb200_rating_infer.argtypes = [i, vp, vp, vp, vp, vp, i, vp, vp]
+        L.kb200_rating_train.argtypes = [ctypes.POINTER(TrainGraph), i, i, ctypes.c_float, vp, vp]
+        L.kb200_rating_grad.argtypes = [ctypes.POINTER(TrainGraph), vp, vp, vp]
         L.kb200_kaffpa_batch.argtypes = [ctypes.POINTER(BatchItem), i, i, ctypes.POINTER(BatchReport)]
         L.kb200_kaffpa_population.argtypes = [i, vp, vp, vp, vp, i, d, i, vp, i, vp, vp, i,
                                               ctypes.POINTER(BatchReport)]
@@ -336,3 +350,47 @@ def kaffpa_population(n, xadj, adjncy, adjwgt, vwgt, parts, nparts, seeds, imbal
                                          mode, _ptr(sd), len(sd), _ptr(cuts), _ptr(parts), workers,
                                          ctypes.byref(rep)))
     return cuts, rep
+
+
+# ------------------------------------------------------ learned edge rating
+
+def rating_infer(g: dict, params, use_tc=True):
+    """(prob[m] float32, rating[m] uint32) of every directed entry of g."""
+    P = np.ascontiguousarray(params, np.float32)
+    assert P.size == RATING_PARAMS
+    m = int(g["xadj"][-1])
+    prob = np.empty(max(m, 1), np.float32)
+    rat = np.empty(max(m, 1), np.uint32)
+    _check(lib().kb200_rating_infer(g["n"], _ptr(g["xadj"]), _ptr(g["adjncy"]), _ptr(g["adjwgt"]), _ptr(g["vwgt"]),
+                                    _ptr(P), 1 if use_tc else 0, _ptr(prob), _ptr(rat)))
+    return prob[:m], rat[:m]
+
+
+def _train_structs(graphs_labels):
+    keep = []
+    arr = (TrainGraph * len(graphs_labels))()
+    for i, (g, lab) in enumerate(graphs_labels):
+        a = [_i32(g[k]) for k in ("xadj", "adjncy", "adjwgt", "vwgt")]
+        lb = np.ascontiguousarray(lab, np.uint8)
+        keep.append((a, lb))
+        arr[i] = TrainGraph(g["n"], _ptr(a[0]), _ptr(a[1]), _ptr(a[2]), _ptr(a[3]), _ptr(lb))
+    return arr, keep
+
+
+def rating_train(graphs_labels, params, steps: int, lr=3e-3):
+    """Trains in place on [(graph, label[m]), ...]; returns (params, loss[steps])."""
+    P = np.array(params, np.float32, copy=True)
+    arr, keep = _train_structs(graphs_labels)
+    loss = np.zeros(max(steps, 1), np.float32)
+    _check(lib().kb200_rating_train(arr, len(graphs_labels), steps, ctypes.c_float(lr), _ptr(P), _ptr(loss)))
+    return P, loss[:steps]
+
+
+def rating_grad(g: dict, label, params):
+    """(grad[RATING_PARAMS], loss) of one graph."""
+    P = np.ascontiguousarray(params, np.float32)
+    arr, keep = _train_structs([(g, label)])
+    G = np.zeros(RATING_PARAMS, np.float32)
+    loss = np.zeros(1, np.float32)
+    _check(lib().kb200_rating_grad(arr, _ptr(P), _ptr(G), _ptr(loss)))
+    return G, float(loss[0])

@@ -223,6 +223,30 @@ void or_hem_match(const or_graph* g, const or_knobs* kn, int level, const uint32
     free(state); free(best); free(mate);
 }
 
+/* ------------------------------------------------------ isolated vertices */
+
+/* No rule of the reference merges a vertex without neighbours; these bundles
+ * keep coarsening going on graphs with many of them (R-MAT). */
+void or_bundle_isolated(const or_graph* g, uint32_t bound, int* label) {
+    if (g->n < 2 || bound < 2) return;
+    uint32_t count = 0, wmax = 0;
+    for (int v = 0; v < g->n; ++v)
+        if (g->xadj[v + 1] == g->xadj[v]) {
+            ++count;
+            if ((uint32_t)g->vwgt[v] > wmax) wmax = (uint32_t)g->vwgt[v];
+        }
+    uint32_t group = wmax == 0 ? count : (bound - 1) / wmax;
+    if (count < 2 || group < 2) return;
+    uint32_t rank = 0;
+    int first = -1;
+    for (int v = 0; v < g->n; ++v) {
+        if (g->xadj[v + 1] != g->xadj[v]) continue;
+        if (rank % group == 0) first = v;
+        label[v] = first;
+        ++rank;
+    }
+}
+
 /* --------------------------------------------------- neighbourhood scratch */
 
 typedef struct {
@@ -1201,6 +1225,7 @@ int or_kaffpa(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const
 int or_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
                     const or_knobs* knobs, long long* edgecut, int* part, or_stats* stats) {
     if (n < 0 || !knobs || knobs->k < 1 || !xadj || (n > 0 && !adjncy)) return -1;
+    if (knobs->coarsening < 0 || knobs->coarsening > 1) return -1;
     const int nparts = knobs->k;
     const int m = xadj[n];
     int* vw = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
@@ -1221,6 +1246,7 @@ int or_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt,
         int* label = xmalloc(sizeof(int) * (size_t)f->n);
         if (kn.coarsening == 1) or_hem_match(f, &kn, L, NULL, label);
         else or_lp_cluster(f, &kn, L, label);
+        or_bundle_isolated(f, kn.coarsening == 0 ? kn.cluster_bound : kn.max_vertex_weight + 1u, label);
         or_level* c = &lv[L + 1];
         lv[L].cmap = xmalloc(sizeof(int) * (size_t)f->n);
         c->xadj = xmalloc(sizeof(int) * (size_t)(f->n + 1));

@@ -44,8 +44,11 @@ typedef struct {
     int bal_iters;
     int ip_reps, ip_tries, ip_fm_passes, ip_fm_stall;
     int max_levels;
-    int coarsening;         /* 0 = LP clustering, 1 = heavy-edge matching */
+    int coarsening;         /* 0 = LP clustering, 1 = heavy-edge matching (2, the learned
+                               rating, is not restated here) */
     int match_rounds;       /* cap on locally-dominant matching rounds */
+    const float* rating_model; /* unused by the oracle (same layout as the product's knobs) */
+    double rating_fallback;    /* unused by the oracle */
 } or_knobs;
 
 typedef struct {
@@ -84,6 +87,12 @@ void or_rate_expansion_star_2(const or_graph* g, double* rating);
  * c(u)+c(v) <= max_vertex_weight (random_matching.cpp:85-112).
  * label[v] = min(v, mate(v)), or v when unmatched. */
 void or_hem_match(const or_graph* g, const or_knobs* kn, int level, const uint32_t* rating_q, int* label);
+
+/* Isolated vertices (degree 0) in increasing id order, in consecutive groups
+ * of G = (bound-1) / (largest isolated node weight) (all of them when that
+ * weight is 0), take the label of the group's first member; nothing happens
+ * when G < 2 or fewer than two vertices are isolated.  label[] in/out. */
+void or_bundle_isolated(const or_graph* g, uint32_t bound, int* label);
 
 /* LP clustering, synchronous schedule (one coarsening level). label[n] out. */
 void or_lp_cluster(const or_graph* g, const or_knobs* kn, int level, int* label);

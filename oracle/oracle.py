@@ -33,7 +33,8 @@ class Knobs(ctypes.Structure):
                 ("ip_reps", ctypes.c_int), ("ip_tries", ctypes.c_int),
                 ("ip_fm_passes", ctypes.c_int), ("ip_fm_stall", ctypes.c_int),
                 ("max_levels", ctypes.c_int), ("coarsening", ctypes.c_int),
-                ("match_rounds", ctypes.c_int)]
+                ("match_rounds", ctypes.c_int), ("rating_model", ctypes.c_void_p),
+                ("rating_fallback", ctypes.c_double)]
 
 
 class Stats(ctypes.Structure):
