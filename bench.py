@@ -68,7 +68,7 @@ def parse():
     p.add_argument("--logn", type=int, default=FULL_LOGN, help="log2 of the RGG size (default 24)")
     p.add_argument("--k", type=int, default=K_BLOCKS)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["rgg", "batch", "population"], default="rgg",
+    p.add_argument("--workload", choices=["rgg", "batch", "population", "learned"], default="rgg",
                    help="rgg: the headline single-graph workload (default); batch: many independent graphs "
                         "of uneven size; population: many seeds of one device-resident RGG2D n=2^20")
     p.add_argument("--graph", choices=sorted(GRAPH_KINDS), default="rgg2d",
@@ -270,6 +270,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
+    if args.workload == "learned":
+        run_learned(args, rank, dev)
+        if world > 1:
+            dist.destroy_process_group()
+        return
     if args.workload != "rgg":
         run_many(args, world, rank, dev)
         if world > 1:
@@ -454,6 +459,74 @@ def main():
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
+
+
+# ------------------------------------------------------ learned edge rating
+
+def run_learned(args, rank, dev):
+    """Held-out evaluation of the learned edge rating: RGG2D n=2^23 and R-MAT
+    n=2^22 (16n samples), k=64, eps=3%, kaffpa fast knobs with three
+    coarsenings -- LP clustering (the default), heavy-edge matching on
+    expansion*^2 (the plain rating) and on the learned rating -- device
+    resident, CUDA events on the library's stream.  value = ms per partition
+    of the learned form on the RGG2D graph."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from kahip_b200 import graphs, native
+    from kahip_b200.learned import load_model
+
+    model = load_model()
+    if model is None:
+        if rank == 0:
+            print(json.dumps({"metric": "learned edge rating", "unavailable": "kahip_b200/data/rating_mpnn.f32 absent"}))
+        return
+    P, meta = model
+    results = {}
+    stream = torch.cuda.Stream(device=dev)
+    for name, g in (("rgg2d_2^23", graphs.rgg2d(1 << 23, seed=77)), ("rmat_2^22", graphs.rmat(22, seed=78))):
+        n = g["n"]
+        t = {key: torch.from_numpy(np.ascontiguousarray(g[key], np.int32)).to(dev)
+             for key in ("xadj", "adjncy", "adjwgt", "vwgt")}
+        part = torch.empty(n, dtype=torch.int32, device=dev)
+        res = {"n": n, "m_directed": g["m"]}
+        for label, coarsening in (("lp", 0), ("plain_rating", 1), ("learned_rating", 2)):
+            kn = native.derive_knobs(n, g["vwgt"], 64, IMBALANCE, 0, MODE_FAST)
+            kn.coarsening = coarsening
+            kn.rating_model = P.ctypes.data_as(ctypes.c_void_p) if coarsening == 2 else None
+            for _ in range(max(1, args.warmup)):
+                native.kaffpa_device_knobs(n, t["xadj"], t["adjncy"], t["adjwgt"], t["vwgt"], part, kn, stream=stream)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                _, cut = native.kaffpa_device_knobs(n, t["xadj"], t["adjncy"], t["adjwgt"], t["vwgt"], part, kn,
+                                                    stream=stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            bw = np.bincount(part.cpu().numpy(), minlength=64)
+            res[label] = {"ms": e0.elapsed_time(e1) / args.steps, "cut": int(cut),
+                          "balanced": bool(bw.max() <= kn.final_bound)}
+        res["learned_over_plain_cut"] = res["learned_rating"]["cut"] / max(1, res["plain_rating"]["cut"])
+        res["learned_over_plain_ms"] = res["learned_rating"]["ms"] / max(1e-9, res["plain_rating"]["ms"])
+        results[name] = res
+        del t, part
+        torch.cuda.empty_cache()
+    if rank != 0:
+        return
+    line = {
+        "metric": "ms per kaffpa-fast partition with the learned-rating matching; cut vs the plain rating",
+        "value": results["rgg2d_2^23"]["learned_rating"]["ms"], "unit": "ms", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": False, "dtype": "bf16 (network) / int32 (partitioning)",
+        "data": "synthetic (seeded generators), held out from training",
+        "config": {"workload": "learned edge rating: RGG2D n=2^23 and R-MAT n=2^22, k=64, eps=3%",
+                   "model": {k: meta[k] for k in ("training_graphs", "steps", "validated") if k in meta}},
+        "results": results,
+    }
+    print(json.dumps(line))
 
 
 # ------------------------------------------------- batch / population forms
