@@ -575,6 +575,11 @@ __global__ void __launch_bounds__(kThreads) heavy_kernel(SweepArgs a, uint32_t* 
         const int beg = a.xadj[v], end = a.xadj[v + 1];
         const uint32_t own = (uint32_t)a.lab[v];
         const uint32_t cv = (uint32_t)a.vwgt[v];
+        // this vertex uses the first cap entries of the block's table (a
+        // power of two >= 2 * degree, at most gcap), so inserting, scanning
+        // and clearing cost O(degree), not O(max degree)
+        int cap = 256;
+        while (cap < 2 * (end - beg) && cap < gcap) cap <<= 1;
         if (threadIdx.x == 0) {
             sco = 0;
             atomicAdd(&a.work[0], 1ull);
@@ -589,12 +594,12 @@ __global__ void __launch_bounds__(kThreads) heavy_kernel(SweepArgs a, uint32_t* 
             }
             unsigned peers = __match_any_sync(0xffffffffu, l);
             uint32_t sum = __reduce_add_sync(peers, wt);
-            if (e < end && (peers & lanemask_lt()) == 0) table_insert(tk, tv, gcap, l, sum, a.err);
+            if (e < end && (peers & lanemask_lt()) == 0) table_insert(tk, tv, cap, l, sum, a.err);
         }
         __syncthreads();
         uint64_t key = 0;
         uint32_t id = kEmpty;
-        for (int s = threadIdx.x; s < gcap; s += kThreads) {
+        for (int s = threadIdx.x; s < cap; s += kThreads) {
             uint32_t l = tk[s];
             if (l == kEmpty) continue;
             uint32_t c = tv[s];
