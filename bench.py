@@ -262,7 +262,7 @@ def main():
     import torch
     import torch.distributed as dist
 
-    from kahip_b200 import graphs, native
+    from kahip_b200 import graphs, native, replicas
 
     if world > 1:
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
@@ -343,11 +343,7 @@ def main():
         dist.barrier()
     launches = native.kernel_launches() - launches0
     sampler.stop()
-    elapsed = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = replicas.max_over_ranks(ev0.elapsed_time(ev1), dev)
     ms_per_step = elapsed / args.steps
     value = elapsed / (args.steps * world)
 
@@ -383,11 +379,7 @@ def main():
     e2e_steps = max(1, min(args.steps, 5))
     for _ in range(e2e_steps):
         e2e_call()
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item()) / world
+    e2e_ms = replicas.max_over_ranks((time.perf_counter() - t0) * 1e3 / e2e_steps, dev) / world
     e2e_same = bool(np.array_equal(h_part.numpy(), part)) and e2e_cut.value == cuts[-1]
 
     # ---- roofline: the LP clustering sweep (every vertex swept once per round) ----
@@ -552,7 +544,7 @@ def run_many(args, world, rank, dev):
     import torch
     import torch.distributed as dist
 
-    from kahip_b200 import graphs, native
+    from kahip_b200 import graphs, native, replicas
 
     ranks_seed = 1000 * rank
     if args.workload == "batch":
@@ -579,7 +571,7 @@ def run_many(args, world, rank, dev):
         t = {key: torch.from_numpy(np.ascontiguousarray(g[key], np.int32)).to(dev)
              for key in ("xadj", "adjncy", "adjwgt", "vwgt")}
         count = args.population
-        seeds = [ranks_seed + i for i in range(count)]
+        seeds = [replicas.member_seed(i, rank, world) for i in range(count)]
         parts = torch.empty(count * n, dtype=torch.int32, device=dev)
         nodes, entries, h2d, d2h = count * n, count * g["m"], 0, 0
 
@@ -615,11 +607,7 @@ def run_many(args, world, rank, dev):
     if world > 1:
         dist.barrier()
     sampler.stop()
-    elapsed = sum(ms)
-    if world > 1:
-        tt = torch.tensor([elapsed], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        elapsed = float(tt.item())
+    elapsed = replicas.max_over_ranks(sum(ms), dev)
     value = count * args.steps * world / (elapsed * 1e-3)
     serial_ms, _, cuts1 = step(1)
     same = bool(np.array_equal(np.asarray(cuts1), np.asarray(cuts)))

@@ -261,7 +261,7 @@ struct PhaseRun {
         ctx.reset_stats();
         up = upload(ctx, n, xadj, adjncy, adjwgt, vwgt);
         check_uploaded(ctx, up.g);
-        up.g.maxdeg = max_degree(ctx, up.g);
+        degree_stats(ctx, up.g);
     }
 };
 
@@ -452,7 +452,7 @@ static int upload_train(Ctx& ctx, const kb200_train_graph* graphs, int count, Tr
             return fail(KB_ERR_INVALID_INPUT, "training graphs need explicit weights and labels");
         Upload u = upload(ctx, t.n, t.xadj, t.adjncy, t.adjwgt, t.vwgt);
         check_uploaded(ctx, u.g);
-        u.g.maxdeg = max_degree(ctx, u.g);
+        degree_stats(ctx, u.g);
         const long long m = t.xadj[t.n];
         uint8_t* dl = ctx.hier.alloc<uint8_t>((size_t)std::max<long long>(m, 1));
         if (m) KB_CUDA(cudaMemcpyAsync(dl, t.label, (size_t)m, cudaMemcpyHostToDevice, s));

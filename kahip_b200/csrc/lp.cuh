@@ -16,6 +16,7 @@ struct DevGraph {
     int n = 0;
     long long m = 0;
     int maxdeg = 0;
+    unsigned iso_count = 0, iso_wmax = 0;  // isolated vertices and their largest weight (max_degree fills them)
     bool unit_weights = false;  // every edge weight is 1 (lets sweeps skip adjwgt)
     const int* xadj = nullptr;
     const int* adjncy = nullptr;
@@ -50,6 +51,9 @@ void project(Ctx& ctx, int n, const int* cmap, const int* part_coarse, int* part
 // max degree of g (device reduction + readback)
 int max_degree(Ctx& ctx, const DevGraph& g);
 
+// Same, and fills g.maxdeg, g.iso_count and g.iso_wmax in one readback.
+void degree_stats(Ctx& ctx, DevGraph& g);
+
 // Device-side input checks: bit 1 = target out of range, 2 = negative edge
 // weight, 4 = negative node weight, 8 = xadj not starting at 0 / not
 // monotone, 16 = some edge weight differs from 1 (not an error).  Also returns the node weight sum (32-bit, as the reference's
@@ -66,6 +70,7 @@ bool rows_strictly_increasing(Ctx& ctx, const DevGraph& g);
 // that weight is 0) share the label of their first member, so every bundle
 // weighs less than `bound`.  Nothing changes when G < 2 or fewer than two
 // vertices are isolated.  label[] of non-isolated vertices is left as is.
+// Uses g.iso_count / g.iso_wmax (degree_stats) and does not synchronise.
 void bundle_isolated(Ctx& ctx, const DevGraph& g, uint32_t bound, int* label);
 
 // label[v] = v, cw[v] = vwgt[v]

@@ -43,25 +43,34 @@ __global__ void project_kernel(int n, const int* __restrict__ cmap, const int* _
         pf[v] = pc[cmap[v]];
 }
 
-__global__ void maxdeg_kernel(int n, const int* __restrict__ xadj, int* out) {
+// out[0] = max degree, out[1] = isolated vertices, out[2] = their largest weight
+__global__ void maxdeg_kernel(int n, const int* __restrict__ xadj, const int* __restrict__ vwgt, int* out) {
     int m = 0;
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
-        m = max(m, xadj[v + 1] - xadj[v]);
-    for (int o = 16; o >= 1; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+    unsigned iso = 0, w = 0;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const int d = xadj[v + 1] - xadj[v];
+        m = max(m, d);
+        if (d == 0) {
+            ++iso;
+            w = max(w, (unsigned)vwgt[v]);
+        }
+    }
+    for (int o = 16; o >= 1; o >>= 1) {
+        m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+        iso += __shfl_xor_sync(0xffffffffu, iso, o);
+        w = max(w, __shfl_xor_sync(0xffffffffu, w, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(out, m);
+        if (iso) atomicAdd(reinterpret_cast<unsigned*>(out + 1), iso);
+        if (w) atomicMax(reinterpret_cast<unsigned*>(out + 2), w);
+    }
 }
 
-// isolated vertices: flag[v] = 1, and the largest isolated node weight
-__global__ void iso_flags(int n, const int* __restrict__ xadj, const int* __restrict__ vwgt, uint32_t* flag,
-                          unsigned* wmax) {
-    unsigned w = 0;
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-        const bool iso = xadj[v + 1] == xadj[v];
-        flag[v] = iso ? 1u : 0u;
-        if (iso) w = max(w, (unsigned)vwgt[v]);
-    }
-    for (int o = 16; o >= 1; o >>= 1) w = max(w, __shfl_xor_sync(0xffffffffu, w, o));
-    if ((threadIdx.x & 31) == 0 && w) atomicMax(wmax, w);
+// flag[v] = 1 for isolated vertices
+__global__ void iso_flags(int n, const int* __restrict__ xadj, uint32_t* flag) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        flag[v] = xadj[v + 1] == xadj[v] ? 1u : 0u;
 }
 
 // ids[rank] = v for isolated v (rank = exclusive prefix count)
@@ -148,15 +157,25 @@ void project(Ctx& ctx, int n, const int* cmap, const int* part_coarse, int* part
     KB_LAUNCH();
 }
 
-int max_degree(Ctx& ctx, const DevGraph& g) {
-    if (g.n == 0) return 0;
-    int* d = ctx.dscalars;
-    KB_CUDA(cudaMemsetAsync(d, 0, sizeof(int), ctx.stream));
-    maxdeg_kernel<<<grid_for(g.n, 256), 256, 0, ctx.stream>>>(g.n, g.xadj, d);
+void degree_stats(Ctx& ctx, DevGraph& g) {
+    g.maxdeg = 0;
+    g.iso_count = g.iso_wmax = 0;
+    if (g.n == 0) return;
+    int* d = ctx.dscalars + 8;  // [8] max degree, [9] isolated count, [10] their max weight
+    KB_CUDA(cudaMemsetAsync(d, 0, 3 * sizeof(int), ctx.stream));
+    maxdeg_kernel<<<grid_for(g.n, 256), 256, 0, ctx.stream>>>(g.n, g.xadj, g.vwgt, d);
     KB_LAUNCH();
-    KB_CUDA(cudaMemcpyAsync(ctx.pinned, d, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    KB_CUDA(cudaMemcpyAsync(ctx.pinned + 8, d, 3 * sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
     KB_CUDA(cudaStreamSynchronize(ctx.stream));
-    return (int)ctx.pinned[0];
+    g.maxdeg = (int)ctx.pinned[8];
+    g.iso_count = ctx.pinned[9];
+    g.iso_wmax = ctx.pinned[10];
+}
+
+int max_degree(Ctx& ctx, const DevGraph& g) {
+    DevGraph h = g;
+    degree_stats(ctx, h);
+    return h.maxdeg;
 }
 
 int check_graph(Ctx& ctx, const DevGraph& g, uint32_t* total_weight) {
@@ -185,30 +204,22 @@ bool rows_strictly_increasing(Ctx& ctx, const DevGraph& g) {
 }
 
 void bundle_isolated(Ctx& ctx, const DevGraph& g, uint32_t bound, int* label) {
-    if (g.n < 2 || bound < 2) return;
+    const uint32_t count = g.iso_count, wmax = g.iso_wmax;
+    if (g.n < 2 || bound < 2 || count < 2) return;
+    const uint32_t group = wmax == 0 ? count : (bound - 1) / wmax;
+    if (group < 2) return;
     cudaStream_t s = ctx.stream;
     const size_t mk = ctx.scratch.mark();
     uint32_t* rank = ctx.scratch.alloc<uint32_t>((size_t)g.n);
     int* ids = ctx.scratch.alloc<int>((size_t)g.n);
-    uint32_t* d = reinterpret_cast<uint32_t*>(ctx.dscalars + 6);  // [6] count, [7] max weight
-    {
-        PhaseScope ps(ctx, "isolated_bundles", 12.0 * g.n);
-        KB_CUDA(cudaMemsetAsync(d, 0, 2 * sizeof(uint32_t), s));
-        iso_flags<<<grid_for(g.n, 256), 256, 0, s>>>(g.n, g.xadj, g.vwgt, rank, d + 1);
-        KB_LAUNCH();
-        exclusive_scan_u32(rank, rank, g.n, d, s, ctx.scratch);
-    }
-    KB_CUDA(cudaMemcpyAsync(ctx.pinned + 6, d, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    KB_CUDA(cudaStreamSynchronize(s));
-    const uint32_t count = ctx.pinned[6], wmax = ctx.pinned[7];
-    const uint32_t group = wmax == 0 ? count : (bound - 1) / wmax;
-    if (count >= 2 && group >= 2) {
-        PhaseScope ps(ctx, "isolated_bundles", 12.0 * g.n);
-        iso_ids<<<grid_for(g.n, 256), 256, 0, s>>>(g.n, g.xadj, rank, ids);
-        KB_LAUNCH();
-        iso_label<<<grid_for(g.n, 256), 256, 0, s>>>(g.n, g.xadj, rank, ids, group, label);
-        KB_LAUNCH();
-    }
+    PhaseScope ps(ctx, "isolated_bundles", 16.0 * g.n);
+    iso_flags<<<grid_for(g.n, 256), 256, 0, s>>>(g.n, g.xadj, rank);
+    KB_LAUNCH();
+    exclusive_scan_u32(rank, rank, g.n, nullptr, s, ctx.scratch);
+    iso_ids<<<grid_for(g.n, 256), 256, 0, s>>>(g.n, g.xadj, rank, ids);
+    KB_LAUNCH();
+    iso_label<<<grid_for(g.n, 256), 256, 0, s>>>(g.n, g.xadj, rank, ids, group, label);
+    KB_LAUNCH();
     ctx.scratch.release(mk);
 }
 

@@ -149,7 +149,7 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
     cudaStream_t s = ctx.stream;
     std::vector<Level> lv;
     lv.push_back(Level{g0, nullptr, d_part});
-    lv[0].g.maxdeg = max_degree(ctx, lv[0].g);
+    degree_stats(ctx, lv[0].g);
     // learned rating: the model's parameters, once per call
     float* d_model = nullptr;
     if (kn.coarsening == 2 && kn.rating_model) {
@@ -180,7 +180,7 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
             int *cx, *ca, *cw, *cv;
             contract(ctx, f, label, lv[L].cmap, c.g, &cx, &ca, &cw, &cv);
             ctx.scratch.release(mk);
-            c.g.maxdeg = max_degree(ctx, c.g);
+            degree_stats(ctx, c.g);
             const int nf = f.n, nc = c.g.n;
             lv.push_back(c);
             ++L;
