@@ -73,6 +73,9 @@ bool rows_strictly_increasing(Ctx& ctx, const DevGraph& g);
 // Uses g.iso_count / g.iso_wmax (degree_stats) and does not synchronise.
 void bundle_isolated(Ctx& ctx, const DevGraph& g, uint32_t bound, int* label);
 
+// Number of v with label[v] == v (synchronises the stream).
+long long count_leaders(Ctx& ctx, int n, const int* label);
+
 // label[v] = v, cw[v] = vwgt[v]
 void init_labels(Ctx& ctx, const DevGraph& g, int* label, uint32_t* cw);
 

@@ -85,6 +85,13 @@ __global__ void iso_label(int n, const int* __restrict__ xadj, const uint32_t* _
         if (xadj[v + 1] == xadj[v]) label[v] = ids[(rank[v] / group) * group];
 }
 
+__global__ void leaders_kernel(int n, const int* __restrict__ label, unsigned* out) {
+    unsigned c = 0;
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) c += label[v] == v;
+    for (int o = 16; o >= 1; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
 __global__ void init_labels_kernel(int n, const int* __restrict__ vwgt, int* label, uint32_t* cw) {
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
         label[v] = v;
@@ -221,6 +228,17 @@ void bundle_isolated(Ctx& ctx, const DevGraph& g, uint32_t bound, int* label) {
     iso_label<<<grid_for(g.n, 256), 256, 0, s>>>(g.n, g.xadj, rank, ids, group, label);
     KB_LAUNCH();
     ctx.scratch.release(mk);
+}
+
+long long count_leaders(Ctx& ctx, int n, const int* label) {
+    if (n == 0) return 0;
+    unsigned* d = reinterpret_cast<unsigned*>(ctx.dscalars + 12);
+    KB_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned), ctx.stream));
+    leaders_kernel<<<grid_for(n, 256), 256, 0, ctx.stream>>>(n, label, d);
+    KB_LAUNCH();
+    KB_CUDA(cudaMemcpyAsync(ctx.pinned + 12, d, sizeof(unsigned), cudaMemcpyDeviceToHost, ctx.stream));
+    KB_CUDA(cudaStreamSynchronize(ctx.stream));
+    return (long long)ctx.pinned[12];
 }
 
 void init_labels(Ctx& ctx, const DevGraph& g, int* label, uint32_t* cw) {

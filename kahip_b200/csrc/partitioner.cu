@@ -166,16 +166,25 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
             lv[L].cmap = ctx.hier.alloc<int>((size_t)f.n);
             const size_t mk = ctx.scratch.mark();
             int* label = ctx.scratch.alloc<int>((size_t)f.n);
-            if (kn.coarsening == 2 && d_model) {
-                uint32_t* rating = ctx.scratch.alloc<uint32_t>((size_t)std::max<long long>(f.m, 1));
-                rating_infer(ctx, f, d_model, nullptr, rating, true);
-                hem_match(ctx, f, kn, L, rating, label);
-            } else if (kn.coarsening >= 1) {
-                hem_match(ctx, f, kn, L, nullptr, label);
-            } else {
-                lp_cluster(ctx, f, kn, L, label);
+            bool lp = kn.coarsening == 0;
+            if (!lp) {
+                if (kn.coarsening == 2 && d_model) {
+                    uint32_t* rating = ctx.scratch.alloc<uint32_t>((size_t)std::max<long long>(f.m, 1));
+                    rating_infer(ctx, f, d_model, nullptr, rating, true);
+                    hem_match(ctx, f, kn, L, rating, label);
+                } else {
+                    hem_match(ctx, f, kn, L, nullptr, label);
+                }
+                bundle_isolated(ctx, f, kn.max_vertex_weight + 1u, label);
+                // a matching that removes less than a quarter of the nodes
+                // (stars, skewed degrees) gives way to LP clustering
+                const long long nc = count_leaders(ctx, f.n, label);
+                lp = 4 * nc > 3 * (long long)f.n;
             }
-            bundle_isolated(ctx, f, kn.coarsening == 0 ? kn.cluster_bound : kn.max_vertex_weight + 1u, label);
+            if (lp) {
+                lp_cluster(ctx, f, kn, L, label);
+                bundle_isolated(ctx, f, kn.cluster_bound, label);
+            }
             Level c;
             int *cx, *ca, *cw, *cv;
             contract(ctx, f, label, lv[L].cmap, c.g, &cx, &ca, &cw, &cv);

@@ -1244,9 +1244,21 @@ int or_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt,
     while (L + 1 < kn.max_levels && lv[L].g.n > 0) {
         or_graph* f = &lv[L].g;
         int* label = xmalloc(sizeof(int) * (size_t)f->n);
-        if (kn.coarsening == 1) or_hem_match(f, &kn, L, NULL, label);
-        else or_lp_cluster(f, &kn, L, label);
-        or_bundle_isolated(f, kn.coarsening == 0 ? kn.cluster_bound : kn.max_vertex_weight + 1u, label);
+        if (kn.coarsening == 1) {
+            or_hem_match(f, &kn, L, NULL, label);
+            or_bundle_isolated(f, kn.max_vertex_weight + 1u, label);
+            /* a matching that removes less than a quarter of the nodes (stars,
+             * skewed degrees) gives way to LP clustering for this level */
+            long long nc = 0;
+            for (int v = 0; v < f->n; ++v) nc += label[v] == v;
+            if (4 * nc > 3 * (long long)f->n) {
+                or_lp_cluster(f, &kn, L, label);
+                or_bundle_isolated(f, kn.cluster_bound, label);
+            }
+        } else {
+            or_lp_cluster(f, &kn, L, label);
+            or_bundle_isolated(f, kn.cluster_bound, label);
+        }
         or_level* c = &lv[L + 1];
         lv[L].cmap = xmalloc(sizeof(int) * (size_t)f->n);
         c->xadj = xmalloc(sizeof(int) * (size_t)(f->n + 1));

@@ -106,3 +106,21 @@ def test_matching_coarsening_quality(graphs):
     cut_m, part, st_m = O.kaffpa_knobs(g, kn)
     assert st_m.balanced and st_m.levels > st.levels
     assert cut_m <= 1.25 * cut_lp
+
+
+def test_matching_gives_way_to_lp_on_stars(graphs):
+    """A star cannot be matched down (one pair per hub); such a level is
+    clustered by LP instead, so coarsening keeps going."""
+    from conftest import csr_from_edges
+    hubs, leaves = 40, 400
+    edges = [(h, hubs + h * leaves + i) for h in range(hubs) for i in range(leaves)]
+    edges += [(h, (h + 1) % hubs) for h in range(hubs)]
+    g = csr_from_edges(hubs * (leaves + 1), edges)
+    kn = O.knobs(g, 4, 0.03, 0, 0)
+    kn.coarsening = 1
+    kn.match_rounds = 1000
+    lab = O.hem_match(g, kn, 0)
+    assert len(np.unique(lab)) > 0.75 * g["n"]  # the matching alone barely shrinks it
+    cut, part, st = O.kaffpa_knobs(g, kn)
+    assert st.levels >= 2 and st.level_n[1] < 0.75 * g["n"]
+    assert st.balanced
