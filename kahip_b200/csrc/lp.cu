@@ -434,20 +434,38 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
 #pragma unroll
     for (int i = 0; i < NS; ++i) { sl[i] = kEmpty; sc[i] = 0; }
     bool overflow = false;
+    // software pipeline: the row entries of the next group of four are
+    // loaded while the labels of the current group are gathered
+    int un[4];
+    uint32_t wn[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        un[t] = -1;
+        wn[t] = 0;
+        if (beg + t < end) {
+            un[t] = a.adjncy[beg + t];
+            wn[t] = UNIT ? 1u : (uint32_t)a.adjwgt[beg + t];
+        }
+    }
     for (int e = beg; e < end && !overflow; e += 4) {
         int u[4];
         uint32_t w[4], l[4];
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
-            u[t] = -1;
-            w[t] = 0;
-            if (e + t < end) {
-                u[t] = a.adjncy[e + t];
-                w[t] = UNIT ? 1u : (uint32_t)a.adjwgt[e + t];
-            }
+            u[t] = un[t];
+            w[t] = wn[t];
         }
 #pragma unroll
         for (int t = 0; t < 4; ++t) l[t] = u[t] >= 0 ? (uint32_t)a.lab[u[t]] : kEmpty;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            un[t] = -1;
+            wn[t] = 0;
+            if (e + 4 + t < end) {
+                un[t] = a.adjncy[e + 4 + t];
+                wn[t] = UNIT ? 1u : (uint32_t)a.adjwgt[e + 4 + t];
+            }
+        }
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
             if (u[t] < 0) continue;
