@@ -84,10 +84,10 @@ typedef struct kb200_stats {
     double ms_h2d, ms_coarsen, ms_initial, ms_uncoarsen, ms_d2h;
     /* kernel families (timing == 1): device ms, algorithmic bytes, launches */
     int nfamilies;
-    char family_name[16][24];
-    double family_ms[16];
-    double family_bytes[16];
-    long long family_launches[16];
+    char family_name[32][24];
+    double family_ms[32];
+    double family_bytes[32];
+    long long family_launches[32];
     /* LP sweep work actually performed */
     long long sweep_vertices, sweep_edges;
     long long sweep_overflow_vertices;   /* of which needed the shared-table path */

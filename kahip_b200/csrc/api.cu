@@ -166,7 +166,7 @@ Upload upload(Ctx& ctx, int n, const int* xadj, const int* adjncy, const int* ad
 void fill_stats_families(Ctx& ctx, kb200_stats* st) {
     if (!st) return;
     ctx.collect();
-    st->nfamilies = (int)std::min<size_t>(ctx.phases.size(), 16);
+    st->nfamilies = (int)std::min<size_t>(ctx.phases.size(), 32);
     for (int i = 0; i < st->nfamilies; ++i) {
         std::strncpy(st->family_name[i], ctx.phases[i].name.c_str(), 23);
         st->family_name[i][23] = 0;

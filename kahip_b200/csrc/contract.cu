@@ -13,10 +13,14 @@
 //      gives coarse ids; cmap gather; coarse node weights (atomicAdd).
 //   2. every fine node merges its neighbours by coarse target in register
 //      slots and writes (cu<<tb|cv, w) entries into its own CSR range of an
-//      m-sized buffer.
-//   3. compaction (prefix sum of the per-vertex entry counts).
-//   4. stable LSD radix sort on the 2*tb key bits.
-//   5. reduce-by-key -> coarse adjncy/adjwgt, row counts -> prefix sum -> xadj.
+//      m-sized buffer (long rows: the whole warp).
+//   3. the entries move into per-coarse-row buckets (row sizes by atomics,
+//      prefix sum, one atomic reservation per fine node).
+//   4. a warp per coarse row sorts its bucket in shared memory (bitonic),
+//      sums the weights of equal targets and keeps the distinct entries;
+//      rows longer than kSegMax go through a stable LSD radix sort on the
+//      2*tb key bits and a reduce-by-key instead.
+//   5. distinct counts -> prefix sum -> xadj; rows copied into place.
 #include "contract.cuh"
 #include "prims.cuh"
 
@@ -60,14 +64,82 @@ __global__ void make_cmap(int n, const int* __restrict__ label, const int* __res
 // the slots whenever a new target finds them full -- repeated targets that
 // this leaves are merged by the sort + reduce that follows.
 constexpr int kEmitSlots = 8;
+constexpr int kEmitLaneDeg = 256;  // longer rows are emitted by the whole warp
+
+// Merges the entries [e0, e1) with stride `step` of vertex v's row into
+// kEmitSlots register slots and writes them at positions taken from *pos
+// (a register counter when one lane owns the row, a shared counter when a
+// warp shares it -- atomic then).  Returns nothing; *pos advances.
+template <bool SHARED_POS>
+__device__ __forceinline__ void emit_range(int e0, int e1, int step, uint32_t own, uint64_t hi,
+                                           const int* __restrict__ adjncy, const int* __restrict__ adjwgt,
+                                           const int* __restrict__ cmap, uint64_t* ekey, uint32_t* eval,
+                                           int* pos) {
+    uint32_t st[kEmitSlots], sw[kEmitSlots];
+    int used = 0;
+    auto flush = [&](int cnt) {
+        int p = SHARED_POS ? atomicAdd(pos, cnt) : *pos;
+        if (!SHARED_POS) *pos += cnt;
+#pragma unroll
+        for (int i = 0; i < kEmitSlots; ++i)
+            if (i < cnt) {
+                ekey[p] = hi | st[i];
+                eval[p] = sw[i];
+                ++p;
+            }
+    };
+    for (int e = e0; e < e1; e += step) {
+        const uint32_t t = (uint32_t)cmap[adjncy[e]];
+        const uint32_t w = (uint32_t)adjwgt[e];
+        if (t == own) continue;
+        bool hit = false;
+#pragma unroll
+        for (int i = 0; i < kEmitSlots; ++i)
+            if (i < used && st[i] == t) { sw[i] += w; hit = true; }
+        if (hit) continue;
+        if (used == kEmitSlots) {
+            flush(kEmitSlots);
+            used = 0;
+        }
+#pragma unroll
+        for (int i = 0; i < kEmitSlots; ++i)
+            if (i == used) { st[i] = t; sw[i] = w; }
+        ++used;
+    }
+    if (used) flush(used);
+}
 
 __global__ void __launch_bounds__(kThreads) emit_kernel(int n, const int* __restrict__ xadj,
                                                         const int* __restrict__ adjncy,
                                                         const int* __restrict__ adjwgt,
                                                         const int* __restrict__ cmap, uint64_t* ekey,
                                                         uint32_t* eval, uint32_t* vcount, int tb) {
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-        const int beg = xadj[v], end = xadj[v + 1];
+    __shared__ int wpos[kThreads / 32];
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    // the loop runs warp-uniformly (every lane takes the same number of
+    // iterations) so that long rows can be shared by the warp
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
+        const int v = (int)(base + threadIdx.x);
+        const bool valid = v < n;
+        const int beg = valid ? xadj[v] : 0, end = valid ? xadj[v + 1] : 0;
+        const bool wide = valid && end - beg > kEmitLaneDeg;
+        unsigned wm = __ballot_sync(0xffffffffu, wide);
+        while (wm) {
+            const int src = __ffs(wm) - 1;
+            wm &= wm - 1;
+            const int hv = __shfl_sync(0xffffffffu, v, src);
+            const int hb = __shfl_sync(0xffffffffu, beg, src);
+            const int he = __shfl_sync(0xffffffffu, end, src);
+            const uint32_t hown = (uint32_t)cmap[hv];
+            if (lane == 0) wpos[wp] = hb;
+            __syncwarp();
+            emit_range<true>(hb + lane, he, 32, hown, (uint64_t)hown << tb, adjncy, adjwgt, cmap, ekey, eval,
+                             &wpos[wp]);
+            __syncwarp();
+            if (lane == src) vcount[hv] = (uint32_t)(wpos[wp] - hb);
+            __syncwarp();
+        }
+        if (!valid || wide) continue;
         const uint32_t own = (uint32_t)cmap[v];
         const uint64_t hi = (uint64_t)own << tb;
         uint32_t st[kEmitSlots], sw[kEmitSlots];
@@ -122,12 +194,28 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(int n, const int* __rest
 }
 
 // entries of vertex v move from its CSR range to voff[v] in the sort input
-// (one thread per vertex; a vertex has at most a few entries)
+// (one thread per vertex; vertices with many entries are copied by the warp)
 __global__ void compact_vertices(int n, const int* __restrict__ xadj, const uint32_t* __restrict__ vcount,
                                  const uint32_t* __restrict__ voff, const uint64_t* __restrict__ ekey,
                                  const uint32_t* __restrict__ eval, uint64_t* K, uint32_t* V) {
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-        const uint32_t cnt = vcount[v];
+    const int lane = threadIdx.x & 31;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
+        const int v = (int)(base + threadIdx.x);
+        const uint32_t cnt = v < n ? vcount[v] : 0u;
+        const bool wide = cnt > 64;
+        unsigned wm = __ballot_sync(0xffffffffu, wide);
+        while (wm) {
+            const int s = __ffs(wm) - 1;
+            wm &= wm - 1;
+            const int hv = __shfl_sync(0xffffffffu, v, s);
+            const uint32_t hc = __shfl_sync(0xffffffffu, cnt, s);
+            const long long src = xadj[hv], dst = voff[hv];
+            for (uint32_t i = lane; i < hc; i += 32) {
+                K[dst + i] = ekey[src + i];
+                V[dst + i] = eval[src + i];
+            }
+        }
+        if (v >= n || wide) continue;
         const long long src = xadj[v];
         const long long dst = voff[v];
         for (uint32_t i = 0; i < cnt; ++i) {
@@ -160,6 +248,168 @@ __global__ void reduce_runs(long long E, const uint64_t* __restrict__ K, const u
     }
 }
 
+// ---- segmented merge: entries bucketed by coarse source row, each row
+// sorted and merged on its own
+
+// rowsz[cmap[v]] += vcount[v]
+__global__ void row_sizes(int n, const int* __restrict__ cmap, const uint32_t* __restrict__ vcount,
+                          uint32_t* rowsz) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const uint32_t c = vcount[v];
+        if (c) atomicAdd(&rowsz[cmap[v]], c);
+    }
+}
+
+// Moves vertex v's entries to its coarse row's bucket as (cv << 32 | w);
+// vertices with many entries are copied by the warp.  The order inside a
+// bucket depends on the atomics; the per-row sort below removes it.
+__global__ void scatter_rows(int n, const int* __restrict__ xadj, const int* __restrict__ cmap,
+                             const uint32_t* __restrict__ vcount, const uint32_t* __restrict__ rowoff,
+                             uint32_t* rowfill, const uint64_t* __restrict__ ekey,
+                             const uint32_t* __restrict__ eval, uint64_t mask, uint64_t* bucket) {
+    const int lane = threadIdx.x & 31;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
+        const int v = (int)(base + threadIdx.x);
+        const uint32_t cnt = v < n ? vcount[v] : 0u;
+        long long dst = 0;
+        if (cnt) {
+            const int c = cmap[v];
+            dst = (long long)rowoff[c] + atomicAdd(&rowfill[c], cnt);
+        }
+        const bool wide = cnt > 64;
+        unsigned wm = __ballot_sync(0xffffffffu, wide);
+        while (wm) {
+            const int s = __ffs(wm) - 1;
+            wm &= wm - 1;
+            const int hv = __shfl_sync(0xffffffffu, v, s);
+            const uint32_t hc = __shfl_sync(0xffffffffu, cnt, s);
+            const long long hd = __shfl_sync(0xffffffffu, dst, s);
+            const long long src = xadj[hv];
+            for (uint32_t i = lane; i < hc; i += 32)
+                bucket[hd + i] = ((ekey[src + i] & mask) << 32) | eval[src + i];
+        }
+        if (wide || cnt == 0) continue;
+        const long long src = xadj[v];
+        for (uint32_t i = 0; i < cnt; ++i) bucket[dst + i] = ((ekey[src + i] & mask) << 32) | eval[src + i];
+    }
+}
+
+constexpr int kSegMax = 1024;       // rows up to this many entries merge in shared memory
+constexpr int kMergeWarps = 4;
+
+// Warp per coarse row: sorts the row's bucket (bitonic, in shared memory),
+// sums the weights of equal targets and writes the distinct entries back to
+// the start of the bucket; ucnt[row] = their number.  Longer rows are left
+// for the global path (bigsz[row] = their size).
+__global__ void __launch_bounds__(kMergeWarps * 32) merge_rows(int nc, const uint32_t* __restrict__ rowoff,
+                                                                uint64_t* bucket, uint32_t* ucnt,
+                                                                uint32_t* bigsz) {
+    __shared__ uint64_t buf[kMergeWarps][kSegMax];
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    uint64_t* b = buf[wp];
+    for (long long r = (long long)blockIdx.x * kMergeWarps + wp; r < nc; r += (long long)gridDim.x * kMergeWarps) {
+        const long long beg = rowoff[r];
+        const int s = (int)(rowoff[r + 1] - beg);
+        if (s > kSegMax) {
+            if (lane == 0) { bigsz[r] = (uint32_t)s; ucnt[r] = 0; }
+            continue;
+        }
+        if (lane == 0) bigsz[r] = 0;
+        int P = 1;
+        while (P < s) P <<= 1;
+        for (int i = lane; i < P; i += 32) b[i] = i < s ? bucket[beg + i] : ~0ull;
+        __syncwarp();
+        for (int k = 2; k <= P; k <<= 1)
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                for (int i = lane; i < P; i += 32) {
+                    const int l = i ^ j;
+                    if (l > i) {
+                        const uint64_t x = b[i], y = b[l];
+                        const bool up = (i & k) == 0;
+                        if ((x > y) == up) { b[i] = y; b[l] = x; }
+                    }
+                }
+                __syncwarp();
+            }
+        // distinct targets, weights summed over each run
+        uint32_t written = 0;
+        for (int i0 = 0; i0 < s; i0 += 32) {
+            const int i = i0 + lane;
+            bool head = false;
+            uint64_t outv = 0;
+            if (i < s) {
+                const uint32_t t = (uint32_t)(b[i] >> 32);
+                head = i == 0 || (uint32_t)(b[i - 1] >> 32) != t;
+                if (head) {
+                    uint32_t sum = (uint32_t)b[i];
+                    for (int j = i + 1; j < s && (uint32_t)(b[j] >> 32) == t; ++j) sum += (uint32_t)b[j];
+                    outv = ((uint64_t)t << 32) | sum;
+                }
+            }
+            const unsigned hm = __ballot_sync(0xffffffffu, head);
+            if (head) bucket[beg + written + __popc(hm & ((1u << lane) - 1u))] = outv;
+            written += __popc(hm);
+        }
+        if (lane == 0) ucnt[r] = written;
+        __syncwarp();
+    }
+}
+
+// Entries of the long rows, gathered for the global sort: key cu << tb | cv.
+__global__ void gather_big(int nc, const uint32_t* __restrict__ rowoff, const uint32_t* __restrict__ bigsz,
+                           const uint32_t* __restrict__ bigoff, const uint64_t* __restrict__ bucket, int tb,
+                           uint64_t* K, uint32_t* V) {
+    for (int r = blockIdx.x; r < nc; r += gridDim.x) {
+        const uint32_t s = bigsz[r];
+        if (!s) continue;
+        const long long src = rowoff[r], dst = bigoff[r];
+        for (uint32_t i = threadIdx.x; i < s; i += blockDim.x) {
+            const uint64_t x = bucket[src + i];
+            K[dst + i] = ((uint64_t)r << tb) | (x >> 32);
+            V[dst + i] = (uint32_t)x;
+        }
+    }
+}
+
+// The distinct keys of the sorted long-row entries go back to the start of
+// their row's bucket, in order: position = global distinct index minus the
+// row's first distinct index (ufirst, an atomicMin).
+__global__ void first_unique(long long E, const uint64_t* __restrict__ K, const uint32_t* __restrict__ uidx, int tb,
+                             uint32_t* ufirst) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += (long long)gridDim.x * blockDim.x)
+        if (i == 0 || (K[i - 1] >> tb) != (K[i] >> tb)) ufirst[K[i] >> tb] = uidx[i];
+}
+
+__global__ void reduce_big(long long E, const uint64_t* __restrict__ K, const uint32_t* __restrict__ V,
+                           const uint32_t* __restrict__ uidx, const uint32_t* __restrict__ ufirst,
+                           const uint32_t* __restrict__ rowoff, int tb, uint64_t* bucket, uint32_t* ucnt) {
+    const uint64_t mask = (1ull << tb) - 1ull;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < E; i += (long long)gridDim.x * blockDim.x) {
+        const uint64_t k = K[i];
+        if (i > 0 && K[i - 1] == k) continue;
+        uint32_t s = V[i];
+        for (long long j = i + 1; j < E && K[j] == k; ++j) s += V[j];
+        const uint32_t r = (uint32_t)(k >> tb);
+        bucket[(long long)rowoff[r] + (uidx[i] - ufirst[r])] = ((k & mask) << 32) | s;
+        atomicAdd(&ucnt[r], 1u);
+    }
+}
+
+// Warp per row: the distinct entries move from the bucket to the coarse CSR.
+__global__ void copy_rows(int nc, const uint32_t* __restrict__ rowoff, const uint32_t* __restrict__ ucnt,
+                          const int* __restrict__ cxadj, const uint64_t* __restrict__ bucket, int* cadj, int* cw) {
+    const int lane = threadIdx.x & 31;
+    for (long long r = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32; r < nc;
+         r += (long long)gridDim.x * blockDim.x / 32) {
+        const long long src = rowoff[r], dst = cxadj[r];
+        const uint32_t u = ucnt[r];
+        for (uint32_t i = lane; i < u; i += 32) {
+            const uint64_t x = bucket[src + i];
+            cadj[dst + i] = (int)(x >> 32);
+            cw[dst + i] = (int)(uint32_t)x;
+        }
+    }
+}
 
 }  // namespace
 
@@ -206,59 +456,83 @@ void contract(Ctx& ctx, const DevGraph& g, const int* label, int* cmap, DevGraph
     uint64_t* ekey = ctx.scratch.alloc<uint64_t>((size_t)std::max<long long>(m, 1));
     uint32_t* eval = ctx.scratch.alloc<uint32_t>((size_t)std::max<long long>(m, 1));
     uint32_t* vcount = ctx.scratch.alloc<uint32_t>((size_t)n + 1);
-    uint32_t* voff = ctx.scratch.alloc<uint32_t>((size_t)n + 1);
     {
         PhaseScope ps(ctx, "contract_emit", 12.0 * m + 8.0 * n);
         emit_kernel<<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, g.adjncy, g.adjwgt, cmap, ekey, eval,
                                                                 vcount, tb);
         KB_LAUNCH();
-        exclusive_scan_u32(vcount, voff, n, tot, st, ctx.scratch);
     }
-    KB_CUDA(cudaMemcpyAsync(ctx.pinned, tot, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    KB_CUDA(cudaStreamSynchronize(st));
-    const long long E = ctx.pinned[0];
-    // 3. compaction
-    uint64_t* K0 = ctx.scratch.alloc<uint64_t>((size_t)std::max<long long>(E, 1));
-    uint32_t* V0 = ctx.scratch.alloc<uint32_t>((size_t)std::max<long long>(E, 1));
-    uint64_t* K1 = ctx.scratch.alloc<uint64_t>((size_t)std::max<long long>(E, 1));
-    uint32_t* V1 = ctx.scratch.alloc<uint32_t>((size_t)std::max<long long>(E, 1));
+    // 3. bucket the entries by coarse source row (at most m of them)
+    uint32_t* rowsz = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
+    uint32_t* rowoff = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
+    uint32_t* ucnt = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
+    uint32_t* bigsz = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
+    uint32_t* bigoff = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
+    uint64_t* bucket = ctx.scratch.alloc<uint64_t>((size_t)std::max<long long>(m, 1));
+    uint32_t* big = reinterpret_cast<uint32_t*>(ctx.dscalars + 16);  // [16] long-row entries
     {
-        PhaseScope ps(ctx, "contract_compact", 24.0 * E);
-        compact_vertices<<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, vcount, voff, ekey, eval, K0, V0);
+        PhaseScope ps(ctx, "contract_bucket", 8.0 * n + 20.0 * m);
+        KB_CUDA(cudaMemsetAsync(rowsz, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
+        row_sizes<<<grid_for(n, 256), 256, 0, st>>>(n, cmap, vcount, rowsz);
+        KB_LAUNCH();
+        exclusive_scan_u32(rowsz, rowoff, (long long)nc + 1, nullptr, st, ctx.scratch);
+        KB_CUDA(cudaMemsetAsync(rowsz, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
+        scatter_rows<<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, cmap, vcount, rowoff, rowsz, ekey, eval,
+                                                                 (1ull << tb) - 1ull, bucket);
         KB_LAUNCH();
     }
-    // 4. sort by (cu, cv)
-    int which;
+    // 4. merge each row: shared-memory sort for rows up to kSegMax entries
     {
-        int bits = 2 * tb;
-        PhaseScope ps(ctx, "contract_sort", 32.0 * E * ((bits + 7) / 8));
-        which = radix_sort_pairs(K0, V0, K1, V1, E, bits, st, ctx.scratch);
-    }
-    uint64_t* K = which ? K1 : K0;
-    uint32_t* V = which ? V1 : V0;
-    // 5. reduce runs
-    uint32_t* uidx = ctx.scratch.alloc<uint32_t>((size_t)std::max<long long>(E, 1));
-    uint32_t* rowcnt = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
-    {
-        PhaseScope ps(ctx, "contract_reduce", 28.0 * E);
-        head_flags<<<grid_for(E, 256), 256, 0, st>>>(E, K, uidx);
+        PhaseScope ps(ctx, "contract_merge", 16.0 * m);
+        const int gb = (int)std::max<long long>(1, std::min<long long>(div_up(nc, kMergeWarps), (long long)kNumSMs * 16));
+        // ucnt / bigsz have nc + 1 entries (the scans read the last one)
+        KB_CUDA(cudaMemsetAsync(ucnt, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
+        KB_CUDA(cudaMemsetAsync(bigsz, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
+        merge_rows<<<gb, kMergeWarps * 32, 0, st>>>(nc, rowoff, bucket, ucnt, bigsz);
         KB_LAUNCH();
-        exclusive_scan_u32(uidx, uidx, E, tot, st, ctx.scratch);
+        exclusive_scan_u32(bigsz, bigoff, (long long)nc + 1, big, st, ctx.scratch);
     }
-    KB_CUDA(cudaMemcpyAsync(ctx.pinned, tot, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    KB_CUDA(cudaMemcpyAsync(ctx.pinned, big, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     KB_CUDA(cudaStreamSynchronize(st));
-    const long long mc = E > 0 ? (long long)ctx.pinned[0] : 0;
+    const long long EB = ctx.pinned[0];
+    if (EB > 0) {
+        // longer rows: global LSD radix sort of their entries, then reduce
+        const size_t mk2 = ctx.scratch.mark();
+        uint64_t* K0 = ctx.scratch.alloc<uint64_t>((size_t)EB);
+        uint32_t* V0 = ctx.scratch.alloc<uint32_t>((size_t)EB);
+        uint64_t* K1 = ctx.scratch.alloc<uint64_t>((size_t)EB);
+        uint32_t* V1 = ctx.scratch.alloc<uint32_t>((size_t)EB);
+        uint32_t* uidx = ctx.scratch.alloc<uint32_t>((size_t)EB);
+        uint32_t* ufirst = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
+        PhaseScope ps(ctx, "contract_sort", 32.0 * EB * ((2 * tb + 7) / 8));
+        gather_big<<<grid_for(nc, 256), 256, 0, st>>>(nc, rowoff, bigsz, bigoff, bucket, tb, K0, V0);
+        KB_LAUNCH();
+        const int which = radix_sort_pairs(K0, V0, K1, V1, EB, 2 * tb, st, ctx.scratch);
+        uint64_t* K = which ? K1 : K0;
+        uint32_t* V = which ? V1 : V0;
+        head_flags<<<grid_for(EB, 256), 256, 0, st>>>(EB, K, uidx);
+        KB_LAUNCH();
+        exclusive_scan_u32(uidx, uidx, EB, nullptr, st, ctx.scratch);
+        first_unique<<<grid_for(EB, 256), 256, 0, st>>>(EB, K, uidx, tb, ufirst);
+        KB_LAUNCH();
+        reduce_big<<<grid_for(EB, 256), 256, 0, st>>>(EB, K, V, uidx, ufirst, rowoff, tb, bucket, ucnt);
+        KB_LAUNCH();
+        ctx.scratch.release(mk2);
+    }
+    // 5. row lengths -> coarse xadj, then the rows themselves
+    {
+        PhaseScope ps(ctx, "contract_rows", 4.0 * nc);
+        exclusive_scan_u32(ucnt, reinterpret_cast<uint32_t*>(cxadj), (long long)nc + 1, big, st, ctx.scratch);
+    }
+    KB_CUDA(cudaMemcpyAsync(ctx.pinned, big, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    KB_CUDA(cudaStreamSynchronize(st));
+    const long long mc = (long long)ctx.pinned[0];
     int* cadj = ctx.hier.alloc<int>((size_t)std::max<long long>(mc, 1));
     int* cwgt = ctx.hier.alloc<int>((size_t)std::max<long long>(mc, 1));
-    KB_CUDA(cudaMemsetAsync(rowcnt, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
     {
-        PhaseScope ps(ctx, "contract_reduce", 12.0 * E);
-        if (E > 0) {
-            reduce_runs<<<grid_for(E, 256), 256, 0, st>>>(E, K, V, uidx, tb, cadj, cwgt, rowcnt);
-            KB_LAUNCH();
-        }
-        exclusive_scan_u32(rowcnt, reinterpret_cast<uint32_t*>(cxadj), (long long)nc + 1, nullptr, st,
-                           ctx.scratch);
+        PhaseScope ps(ctx, "contract_rows", 16.0 * mc + 12.0 * nc);
+        copy_rows<<<grid_for(32LL * nc, 256), 256, 0, st>>>(nc, rowoff, ucnt, cxadj, bucket, cadj, cwgt);
+        KB_LAUNCH();
     }
     out = DevGraph{};
     out.n = nc;

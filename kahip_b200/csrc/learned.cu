@@ -124,6 +124,20 @@ __global__ void __launch_bounds__(kT) dense_fwd(int n, const float* P, int woff,
     }
 }
 
+// Eight consecutive z values (q-th group of a row) with one or two 16-byte loads.
+__device__ __forceinline__ void load_z8(const float* z, long long u, int q, float* out) {
+    const float4* p = reinterpret_cast<const float4*>(z + u * rm::Z) + 2 * q;
+    const float4 a = p[0], b = p[1];
+    out[0] = a.x; out[1] = a.y; out[2] = a.z; out[3] = a.w;
+    out[4] = b.x; out[5] = b.y; out[6] = b.z; out[7] = b.w;
+}
+__device__ __forceinline__ void load_z8(const __nv_bfloat16* z, long long u, int q, float* out) {
+    const uint4 b = reinterpret_cast<const uint4*>(z + u * rm::Z)[q];
+    const __nv_bfloat162* h2 = reinterpret_cast<const __nv_bfloat162*>(&b);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { out[2 * k] = __low2float(h2[k]); out[2 * k + 1] = __high2float(h2[k]); }
+}
+
 // Per-entry score; lane per entry, warp per row.  prob/rating outputs.
 template <class T>
 __global__ void __launch_bounds__(kT) head_fwd(int n, const int* xadj, const int* adjncy, const int* adjwgt,
@@ -147,13 +161,19 @@ __global__ void __launch_bounds__(kT) head_fwd(int n, const int* xadj, const int
             float f0, f1;
             edge_feat(adjwgt[e], (uint32_t)vwgt[u], cv, f0, f1);
             float s = bo;
-#pragma unroll 8
-            for (int j = 0; j < rm::Z; ++j) {
-                // IEEE addition commutes exactly: both directions of the edge
-                // get the same sum
-                const float a = ld(z + (long long)u * rm::Z + j) + zv[wp][j];
-                const float t = a + (wf[2 * j] * f0 + wf[2 * j + 1] * f1);
-                s += wo[j] * fmaxf(t, 0.f);
+#pragma unroll 1
+            for (int q = 0; q < rm::Z / 8; ++q) {
+                float zu[8];
+                load_z8(z, u, q, zu);
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const int j = 8 * q + k;
+                    // IEEE addition commutes exactly: both directions of the
+                    // edge get the same sum
+                    const float a = zu[k] + zv[wp][j];
+                    const float t = a + (wf[2 * j] * f0 + wf[2 * j + 1] * f1);
+                    s += wo[j] * fmaxf(t, 0.f);
+                }
             }
             const float p = 1.0f / (1.0f + expf(-s));
             if (prob) prob[e] = p;

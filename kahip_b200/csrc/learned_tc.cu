@@ -114,33 +114,70 @@ __global__ void __launch_bounds__(kTcThreads) fused_layer_tc(int n, const int* x
     bool ok = true;
     const long long tiles = ((long long)n + kTile - 1) / kTile;
     for (long long t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-        // 1. gather the A tile: warp w fills rows 32w .. 32w+31
-        for (int r = warp * 32; r < warp * 32 + 32; ++r) {
-            const long long v = t * kTile + r;
-            float x0 = 0.f, x1 = 0.f, a0 = 0.f, a1 = 0.f;
-            if (v < n) {
-                const __nv_bfloat162 hv = reinterpret_cast<const __nv_bfloat162*>(h + v * rm::H)[lane];
-                x0 = __low2float(hv);
-                x1 = __high2float(hv);
-                if (AGG) {
-                    const int beg = xadj[v], end = xadj[v + 1];
-                    for (int e = beg; e < end; ++e) {
-                        const int u = adjncy[e];
-                        const float w = (float)adjwgt[e];
-                        const __nv_bfloat162 hu = reinterpret_cast<const __nv_bfloat162*>(h + (long long)u * rm::H)[lane];
-                        a0 += w * __low2float(hu);
-                        a1 += w * __high2float(hu);
+        // 1. gather the A tile: warp w fills rows 32w .. 32w+31, four rows at
+        // a time (one per group of 8 lanes); lane j of a group owns features
+        // 8j .. 8j+7 (16 bytes of a row) and keeps four neighbour rows in
+        // flight
+        {
+            const int grp = lane >> 3, j = lane & 7;
+            for (int r = warp * 32 + grp; r < warp * 32 + 32; r += 4) {
+                const long long v = t * kTile + r;
+                float x[8], acc[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) { x[q] = 0.f; acc[q] = 0.f; }
+                if (v < n) {
+                    const uint4 hv = reinterpret_cast<const uint4*>(h + v * rm::H)[j];
+                    const __nv_bfloat162* hp = reinterpret_cast<const __nv_bfloat162*>(&hv);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) { x[2 * q] = __low2float(hp[q]); x[2 * q + 1] = __high2float(hp[q]); }
+                    if (AGG) {
+                        const int beg = xadj[v], end = xadj[v + 1];
+                        int e = beg;
+                        for (; e + 4 <= end; e += 4) {
+                            int u[4];
+                            float w[4];
+                            uint4 hu[4];
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) { u[k] = adjncy[e + k]; w[k] = (float)adjwgt[e + k]; }
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) hu[k] = reinterpret_cast<const uint4*>(h + (long long)u[k] * rm::H)[j];
+#pragma unroll
+                            for (int k = 0; k < 4; ++k) {
+                                const __nv_bfloat162* p2 = reinterpret_cast<const __nv_bfloat162*>(&hu[k]);
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) {
+                                    acc[2 * q] += w[k] * __low2float(p2[q]);
+                                    acc[2 * q + 1] += w[k] * __high2float(p2[q]);
+                                }
+                            }
+                        }
+                        for (; e < end; ++e) {
+                            const float w = (float)adjwgt[e];
+                            const uint4 hu = reinterpret_cast<const uint4*>(h + (long long)adjncy[e] * rm::H)[j];
+                            const __nv_bfloat162* p2 = reinterpret_cast<const __nv_bfloat162*>(&hu);
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) {
+                                acc[2 * q] += w * __low2float(p2[q]);
+                                acc[2 * q + 1] += w * __high2float(p2[q]);
+                            }
+                        }
+                        const float d = wdeg[v];
+                        const float inv = d > 0.f ? 1.0f / d : 0.f;
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) acc[q] *= inv;
                     }
-                    const float d = wdeg[v];
-                    const float inv = d > 0.f ? 1.0f / d : 0.f;
-                    a0 *= inv;
-                    a1 *= inv;
                 }
+                uint4 ox, oa;
+                __nv_bfloat162* px = reinterpret_cast<__nv_bfloat162*>(&ox);
+                __nv_bfloat162* pa = reinterpret_cast<__nv_bfloat162*>(&oa);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    px[q] = __floats2bfloat162_rn(x[2 * q], x[2 * q + 1]);
+                    pa[q] = __floats2bfloat162_rn(acc[2 * q], acc[2 * q + 1]);
+                }
+                *reinterpret_cast<uint4*>(sa + core_off(r, 8 * j, kTile)) = ox;
+                if (AGG) *reinterpret_cast<uint4*>(sa + core_off(r, 64 + 8 * j, kTile)) = oa;
             }
-            *reinterpret_cast<__nv_bfloat162*>(sa + core_off(r, 2 * lane, kTile)) = __floats2bfloat162_rn(x0, x1);
-            if (AGG)
-                *reinterpret_cast<__nv_bfloat162*>(sa + core_off(r, 64 + 2 * lane, kTile)) =
-                    __floats2bfloat162_rn(a0, a1);
         }
         // generic-proxy smem writes -> visible to the tensor core (async proxy)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

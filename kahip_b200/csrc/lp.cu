@@ -576,16 +576,27 @@ __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
     }
 }
 
-// High-degree vertices: one block per vertex, global-memory table of
-// `gcap` slots per block (gcap >= 2 * maxdeg, power of two).
+// High-degree vertices: one block per vertex.  Its connections aggregate in
+// a hash table in shared memory (rows up to kSmemTab / 2 entries) or, for
+// longer rows, in the block's global-memory table of `gcap` slots
+// (gcap >= 2 * maxdeg, power of two; gtk may be null when every row fits
+// the shared table).
+constexpr int kSmemTab = 4096;
+
 template <int MODE>
 __global__ void __launch_bounds__(kThreads) heavy_kernel(SweepArgs a, uint32_t* gtk, uint32_t* gtv,
                                                          int gcap) {
     __shared__ uint64_t sk[kThreads / 32];
     __shared__ uint32_t sid[kThreads / 32];
     __shared__ uint32_t sco;
-    uint32_t* tk = gtk + (size_t)blockIdx.x * gcap;
-    uint32_t* tv = gtv + (size_t)blockIdx.x * gcap;
+    __shared__ uint32_t stk[kSmemTab], stv[kSmemTab];
+    for (int s = threadIdx.x; s < kSmemTab; s += kThreads) {
+        stk[s] = kEmpty;
+        stv[s] = 0;
+    }
+    __syncthreads();
+    uint32_t* gk = gtk ? gtk + (size_t)blockIdx.x * gcap : nullptr;
+    uint32_t* gv = gtv ? gtv + (size_t)blockIdx.x * gcap : nullptr;
     const unsigned count = *a.hcount;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (unsigned i = blockIdx.x; i < count; i += gridDim.x) {
@@ -598,6 +609,8 @@ __global__ void __launch_bounds__(kThreads) heavy_kernel(SweepArgs a, uint32_t* 
         // and clearing cost O(degree), not O(max degree)
         int cap = 256;
         while (cap < 2 * (end - beg) && cap < gcap) cap <<= 1;
+        uint32_t* tk = cap <= kSmemTab ? stk : gk;
+        uint32_t* tv = cap <= kSmemTab ? stv : gv;
         if (threadIdx.x == 0) {
             sco = 0;
             atomicAdd(&a.work[0], 1ull);
@@ -840,14 +853,19 @@ SweepBuffers make_buffers(Ctx& ctx, const DevGraph& g) {
         int cap = 1;
         while (cap < 2 * g.maxdeg) cap <<= 1;
         b.gcap = cap;
-        // per-block tables within min(1 GiB, 8 B per directed entry of the level)
-        long long per = (long long)cap * 8;
-        long long budget = std::min<long long>(1LL << 30, 8LL * g.m);
-        b.hblocks = (int)std::max<long long>(1, std::min<long long>(2LL * kNumSMs, budget / per));
-        b.gtk = A.alloc<uint32_t>((size_t)cap * b.hblocks);
-        b.gtv = A.alloc<uint32_t>((size_t)cap * b.hblocks);
-        fill_u32(b.gtk, (long long)cap * b.hblocks, kEmpty, ctx.stream);
-        fill_u32(b.gtv, (long long)cap * b.hblocks, 0u, ctx.stream);
+        if (cap <= kSmemTab) {
+            // every row fits the blocks' shared-memory tables
+            b.hblocks = 8 * kNumSMs;
+        } else {
+            // per-block global tables within min(1 GiB, 8 B per directed entry of the level)
+            long long per = (long long)cap * 8;
+            long long budget = std::min<long long>(1LL << 30, 8LL * g.m);
+            b.hblocks = (int)std::max<long long>(1, std::min<long long>(8LL * kNumSMs, budget / per));
+            b.gtk = A.alloc<uint32_t>((size_t)cap * b.hblocks);
+            b.gtv = A.alloc<uint32_t>((size_t)cap * b.hblocks);
+            fill_u32(b.gtk, (long long)cap * b.hblocks, kEmpty, ctx.stream);
+            fill_u32(b.gtv, (long long)cap * b.hblocks, 0u, ctx.stream);
+        }
     }
     return b;
 }

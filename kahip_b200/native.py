@@ -55,9 +55,9 @@ class Stats(ctypes.Structure):
                 ("timing", ctypes.c_int), ("ms_total", ctypes.c_double), ("ms_h2d", ctypes.c_double),
                 ("ms_coarsen", ctypes.c_double), ("ms_initial", ctypes.c_double),
                 ("ms_uncoarsen", ctypes.c_double), ("ms_d2h", ctypes.c_double),
-                ("nfamilies", ctypes.c_int), ("family_name", (ctypes.c_char * 24) * 16),
-                ("family_ms", ctypes.c_double * 16), ("family_bytes", ctypes.c_double * 16),
-                ("family_launches", ctypes.c_longlong * 16), ("sweep_vertices", ctypes.c_longlong),
+                ("nfamilies", ctypes.c_int), ("family_name", (ctypes.c_char * 24) * 32),
+                ("family_ms", ctypes.c_double * 32), ("family_bytes", ctypes.c_double * 32),
+                ("family_launches", ctypes.c_longlong * 32), ("sweep_vertices", ctypes.c_longlong),
                 ("sweep_edges", ctypes.c_longlong), ("sweep_overflow_vertices", ctypes.c_longlong),
                 ("device_bytes_peak", ctypes.c_size_t), ("rating_fallback_used", ctypes.c_int)]
 
