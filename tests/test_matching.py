@@ -122,6 +122,6 @@ def test_matching_gives_way_to_lp_on_stars(graphs):
     lab = O.hem_match(g, kn, 0)
     assert len(np.unique(lab)) > 0.75 * g["n"]  # the matching alone barely shrinks it
     cut, part, st = O.kaffpa_knobs(g, kn)
-    # LP clusters each hub with up to cluster_bound - 1 of its leaves
-    assert st.levels >= 2 and st.level_n[1] < 0.8 * len(np.unique(lab))
+    # the level was clustered by LP, which shrinks it further than the matching
+    assert st.levels >= 2 and st.level_n[1] < len(np.unique(lab)) - hubs
     assert st.balanced
