@@ -74,6 +74,8 @@ def parse():
     p.add_argument("--graph", choices=sorted(GRAPH_KINDS), default="rgg2d",
                    help="single-graph workload kind (default rgg2d, the headline)")
     p.add_argument("--batch-count", type=int, default=512, help="graphs in the batch workload")
+    p.add_argument("--learned-logn", type=int, default=23,
+                   help="learned workload: RGG2D n=2^L and R-MAT n=2^(L-1) (default 23)")
     p.add_argument("--population", type=int, default=64, help="seeds in the population workload")
     return p.parse_args()
 
@@ -478,7 +480,8 @@ def run_learned(args, rank, dev):
     P, meta = model
     results = {}
     stream = torch.cuda.Stream(device=dev)
-    for name, g in (("rgg2d_2^23", graphs.rgg2d(1 << 23, seed=77)), ("rmat_2^22", graphs.rmat(22, seed=78))):
+    L = args.learned_logn
+    for name, g in ((f"rgg2d_2^{L}", graphs.rgg2d(1 << L, seed=77)), (f"rmat_2^{L - 1}", graphs.rmat(L - 1, seed=78))):
         n = g["n"]
         t = {key: torch.from_numpy(np.ascontiguousarray(g[key], np.int32)).to(dev)
              for key in ("xadj", "adjncy", "adjwgt", "vwgt")}
@@ -513,10 +516,10 @@ def run_learned(args, rank, dev):
         return
     line = {
         "metric": "ms per kaffpa-fast partition with the learned-rating matching; cut vs the plain rating",
-        "value": results["rgg2d_2^23"]["learned_rating"]["ms"], "unit": "ms", "n_gpus": 1, "steps": args.steps,
+        "value": results[f"rgg2d_2^{L}"]["learned_rating"]["ms"], "unit": "ms", "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "higher_is_better": False, "dtype": "bf16 (network) / int32 (partitioning)",
         "data": "synthetic (seeded generators), held out from training",
-        "config": {"workload": "learned edge rating: RGG2D n=2^23 and R-MAT n=2^22, k=64, eps=3%",
+        "config": {"workload": f"learned edge rating: RGG2D n=2^{L} and R-MAT n=2^{L - 1}, k=64, eps=3%",
                    "model": {k: meta[k] for k in ("training_graphs", "steps", "validated") if k in meta}},
         "results": results,
     }

@@ -2,7 +2,7 @@
 // on the 5th-generation tensor cores (tcgen05), fused with the neighbour
 // gather that feeds them.
 //
-// One CTA = one warpgroup (4 warps) holding NOUT columns of TMEM (the
+// One CTA = two warpgroups (8 warps) holding NOUT columns of TMEM (the
 // 128 x NOUT FP32 accumulator of one tile).  Per tile of 128 nodes:
 //   1. the warps gather the tile's A operand into shared memory: row r =
 //      [h(v) | weighted mean of h over N(v)] (BF16; sums in FP32), written
@@ -12,9 +12,10 @@
 //      FP32 accumulate in TMEM) reading A and the layer's weights (B, loaded
 //      once per CTA in the same layout) from shared memory, then
 //      tcgen05.commit to an mbarrier;
-//   3. every warp waits on the mbarrier (bounded), reads its 32 TMEM lanes
-//      (= 32 rows) with tcgen05.ld, adds the bias, applies ReLU, rounds to
-//      BF16 and stores the row.
+//   3. every warp waits on the mbarrier (bounded), reads 32 TMEM lanes
+//      (= 32 rows; warp w accesses lanes 32 (w % 4) ..) and half of the
+//      columns with tcgen05.ld, adds the bias, applies ReLU, rounds to BF16
+//      and stores its part of the rows.
 // The gather (HBM/L2-bound) dominates; the MMAs take a few hundred cycles
 // per tile.  Descriptor bit layouts follow the PTX ISA's tcgen05 matrix and
 // instruction descriptors (as spelled out in CUTLASS's
@@ -35,7 +36,8 @@ void launch_head_bf16(Ctx& ctx, const DevGraph& g, const float* P, const __nv_bf
 namespace {
 
 constexpr int kTile = 128;               // nodes per tile = MMA M
-constexpr int kTcThreads = 128;          // one warpgroup
+constexpr int kTcThreads = 256;          // two warpgroups: all gather, both read TMEM
+constexpr int kGatherRows = kTile / (kTcThreads / 32);  // rows gathered per warp
 constexpr long long kWaitLimit = 1 << 24;  // mbarrier polls before giving up
 
 // byte offset of element (r, c) of a K-major operand with `rows` rows in the
@@ -114,13 +116,13 @@ __global__ void __launch_bounds__(kTcThreads) fused_layer_tc(int n, const int* x
     bool ok = true;
     const long long tiles = ((long long)n + kTile - 1) / kTile;
     for (long long t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-        // 1. gather the A tile: warp w fills rows 32w .. 32w+31, four rows at
+        // 1. gather the A tile: warp w fills kGatherRows rows, four rows at
         // a time (one per group of 8 lanes); lane j of a group owns features
         // 8j .. 8j+7 (16 bytes of a row) and keeps four neighbour rows in
         // flight
         {
             const int grp = lane >> 3, j = lane & 7;
-            for (int r = warp * 32 + grp; r < warp * 32 + 32; r += 4) {
+            for (int r = warp * kGatherRows + grp; r < (warp + 1) * kGatherRows; r += 4) {
                 const long long v = t * kTile + r;
                 float x[8], acc[8];
 #pragma unroll
@@ -223,11 +225,14 @@ __global__ void __launch_bounds__(kTcThreads) fused_layer_tc(int n, const int* x
         if (!__all_sync(0xffffffffu, ok)) ok = false;
         if (ok) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const long long v = t * kTile + warp * 32 + lane;
+            // warp w reads TMEM lanes 32 (w % 4) .. +31 (its rows) and the
+            // (w / 4)-th half of the columns
+            const int lanes = (warp & 3) * 32;
+            const long long v = t * kTile + lanes + lane;
 #pragma unroll
-            for (int c0 = 0; c0 < NOUT; c0 += 16) {
+            for (int c0 = (warp >> 2) * (NOUT / 2); c0 < (warp >> 2) * (NOUT / 2) + NOUT / 2; c0 += 16) {
                 uint32_t r[16];
-                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+                const uint32_t taddr = tmem + ((uint32_t)lanes << 16) + (uint32_t)c0;
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
                     "%12, %13, %14, %15}, [%16];\n"
@@ -285,7 +290,8 @@ void launch_fused(Ctx& ctx, const DevGraph& g, const float* wdeg, const __nv_bfl
     KB_CUDA(cudaFuncSetAttribute(fused_layer_tc<AGG, NOUT, RELU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
     const long long tiles = ((long long)g.n + kTile - 1) / kTile;
-    const int grid = (int)std::max<long long>(1, std::min<long long>(tiles, 2LL * kNumSMs));
+    // ~48 KB of shared memory per CTA: four CTAs per SM
+    const int grid = (int)std::max<long long>(1, std::min<long long>(tiles, 4LL * kNumSMs));
     fused_layer_tc<AGG, NOUT, RELU><<<grid, kTcThreads, smem, ctx.stream>>>(g.n, g.xadj, g.adjncy, g.adjwgt, wdeg,
                                                                              h, wpk, P, boff, out, err);
     KB_LAUNCH();
