@@ -584,8 +584,11 @@ __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
 constexpr int kSmemTab = 4096;
 
 template <int MODE>
+// `which`: 0 = every listed vertex, 1 = only those whose table fits in
+// shared memory, 2 = only the others (the two kinds can run as separate
+// launches with different grids; the decisions do not depend on the order).
 __global__ void __launch_bounds__(kThreads) heavy_kernel(SweepArgs a, uint32_t* gtk, uint32_t* gtv,
-                                                         int gcap) {
+                                                         int gcap, int which) {
     __shared__ uint64_t sk[kThreads / 32];
     __shared__ uint32_t sid[kThreads / 32];
     __shared__ uint32_t sco;
@@ -609,6 +612,7 @@ __global__ void __launch_bounds__(kThreads) heavy_kernel(SweepArgs a, uint32_t* 
         // and clearing cost O(degree), not O(max degree)
         int cap = 256;
         while (cap < 2 * (end - beg) && cap < gcap) cap <<= 1;
+        if ((which == 1 && cap > kSmemTab) || (which == 2 && cap <= kSmemTab)) continue;
         uint32_t* tk = cap <= kSmemTab ? stk : gk;
         uint32_t* tv = cap <= kSmemTab ? stv : gv;
         if (threadIdx.x == 0) {
@@ -888,8 +892,17 @@ void launch_sweep(Ctx& ctx, const DevGraph& g, SweepArgs a, const SweepBuffers& 
     }
     if (b.gcap > 0) {
         PhaseScope ps(ctx, family(MODE, 2), 0);
-        heavy_kernel<MODE><<<b.hblocks, kThreads, 0, ctx.stream>>>(a, b.gtk, b.gtv, b.gcap);
-        KB_LAUNCH();
+        if (b.gcap <= kSmemTab) {
+            heavy_kernel<MODE><<<b.hblocks, kThreads, 0, ctx.stream>>>(a, nullptr, nullptr, b.gcap, 0);
+            KB_LAUNCH();
+        } else {
+            // rows that fit the shared tables on many blocks, the longest
+            // rows on the blocks that own a global table
+            heavy_kernel<MODE><<<8 * kNumSMs, kThreads, 0, ctx.stream>>>(a, nullptr, nullptr, b.gcap, 1);
+            KB_LAUNCH();
+            heavy_kernel<MODE><<<b.hblocks, kThreads, 0, ctx.stream>>>(a, b.gtk, b.gtv, b.gcap, 2);
+            KB_LAUNCH();
+        }
     }
 }
 
