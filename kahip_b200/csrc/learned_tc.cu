@@ -75,12 +75,64 @@ __global__ void pack_weights(const float* P, int woff, __nv_bfloat16* out) {
     }
 }
 
+// Rows longer than kLongRow (hubs of skewed graphs) would stall a whole
+// tile on one group of eight lanes; their weighted neighbour sums are formed
+// first, one block per row, in a fixed order (deterministic).
+constexpr int kLongRow = 1024;
+constexpr int kLongThreads = 1024;
+
+__device__ __forceinline__ int end_of(const int* xadj, long long v) { return xadj[v + 1]; }
+
+// hrank[v] = index of v among the long rows (or -1); list[] = the long rows.
+__global__ void long_rows(int n, const int* xadj, int* hrank, int* list, unsigned* count) {
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
+        if (xadj[v + 1] - xadj[v] > kLongRow) {
+            const unsigned i = atomicAdd(count, 1u);
+            list[i] = (int)v;
+            hrank[v] = (int)i;
+        } else {
+            hrank[v] = -1;
+        }
+    }
+}
+
+// hagg[rank][f] = sum_u w_vu h[u][f] over a long row; warp w of the block
+// sums the entries e = beg + w + 32 k (lane l owns features 2l, 2l+1), then
+// the 32 warp sums are added in warp order.
+__global__ void __launch_bounds__(kLongThreads) long_row_sums(const int* xadj, const int* adjncy, const int* adjwgt,
+                                                              const __nv_bfloat16* h, const int* list,
+                                                              const unsigned* count, float* hagg) {
+    __shared__ float part[kLongThreads / 32][rm::H];
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    const unsigned cnt = *count;
+    for (unsigned i = blockIdx.x; i < cnt; i += gridDim.x) {
+        const int v = list[i];
+        const int beg = xadj[v], end = xadj[v + 1];
+        float a0 = 0.f, a1 = 0.f;
+        for (int e = beg + wp; e < end; e += kLongThreads / 32) {
+            const __nv_bfloat162 hu = reinterpret_cast<const __nv_bfloat162*>(h + (long long)adjncy[e] * rm::H)[lane];
+            const float w = (float)adjwgt[e];
+            a0 += w * __low2float(hu);
+            a1 += w * __high2float(hu);
+        }
+        part[wp][2 * lane] = a0;
+        part[wp][2 * lane + 1] = a1;
+        __syncthreads();
+        if (threadIdx.x < rm::H) {
+            float s = 0.f;
+            for (int k = 0; k < kLongThreads / 32; ++k) s += part[k][threadIdx.x];
+            hagg[(size_t)i * rm::H + threadIdx.x] = s;
+        }
+        __syncthreads();
+    }
+}
+
 template <bool AGG, int NOUT, bool RELU>
 __global__ void __launch_bounds__(kTcThreads) fused_layer_tc(int n, const int* xadj, const int* adjncy,
                                                              const int* adjwgt, const float* wdeg,
                                                              const __nv_bfloat16* h, const __nv_bfloat16* wpk,
                                                              const float* P, int boff, __nv_bfloat16* out,
-                                                             int* err) {
+                                                             const int* hrank, const float* hagg, int* err) {
     constexpr int K = AGG ? 128 : 64;
     constexpr uint32_t A_BYTES = kTile * K * 2, B_BYTES = NOUT * K * 2;
     constexpr uint32_t LBO_A = kTile * 16, LBO_B = NOUT * 16, SBO = 128;
@@ -132,7 +184,14 @@ __global__ void __launch_bounds__(kTcThreads) fused_layer_tc(int n, const int* x
                     const __nv_bfloat162* hp = reinterpret_cast<const __nv_bfloat162*>(&hv);
 #pragma unroll
                     for (int q = 0; q < 4; ++q) { x[2 * q] = __low2float(hp[q]); x[2 * q + 1] = __high2float(hp[q]); }
-                    if (AGG) {
+                    if (AGG && end_of(xadj, v) - xadj[v] > kLongRow) {
+                        // long row: its weighted sum was formed by long_row_sums
+                        const float* src = hagg + (size_t)hrank[v] * rm::H + 8 * j;
+                        const float d = wdeg[v];
+                        const float inv = d > 0.f ? 1.0f / d : 0.f;
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) acc[q] = src[q] * inv;
+                    } else if (AGG) {
                         const int beg = xadj[v], end = xadj[v + 1];
                         int e = beg;
                         for (; e + 4 <= end; e += 4) {
@@ -284,7 +343,8 @@ __global__ void __launch_bounds__(kTcThreads) fused_layer_tc(int n, const int* x
 
 template <bool AGG, int NOUT, bool RELU>
 void launch_fused(Ctx& ctx, const DevGraph& g, const float* wdeg, const __nv_bfloat16* h,
-                  const __nv_bfloat16* wpk, const float* P, int boff, __nv_bfloat16* out, int* err) {
+                  const __nv_bfloat16* wpk, const float* P, int boff, __nv_bfloat16* out, const int* hrank,
+                  const float* hagg, int* err) {
     constexpr int K = AGG ? 128 : 64;
     const size_t smem = (size_t)kTile * K * 2 + (size_t)NOUT * K * 2 + 64 + NOUT * sizeof(float);
     KB_CUDA(cudaFuncSetAttribute(fused_layer_tc<AGG, NOUT, RELU>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -293,7 +353,8 @@ void launch_fused(Ctx& ctx, const DevGraph& g, const float* wdeg, const __nv_bfl
     // ~48 KB of shared memory per CTA: four CTAs per SM
     const int grid = (int)std::max<long long>(1, std::min<long long>(tiles, 4LL * kNumSMs));
     fused_layer_tc<AGG, NOUT, RELU><<<grid, kTcThreads, smem, ctx.stream>>>(g.n, g.xadj, g.adjncy, g.adjwgt, wdeg,
-                                                                             h, wpk, P, boff, out, err);
+                                                                             h, wpk, P, boff, out, hrank, hagg,
+                                                                             err);
     KB_LAUNCH();
 }
 
@@ -311,8 +372,21 @@ void rating_infer_tc(Ctx& ctx, const DevGraph& g, const float* P, float* prob, u
     for (auto& p : wl) p = ctx.scratch.alloc<__nv_bfloat16>((size_t)rm::H * 2 * rm::H);
     __nv_bfloat16* wz = ctx.scratch.alloc<__nv_bfloat16>((size_t)rm::Z * rm::H);
     int* err = ctx.dscalars + 60;
+    // long rows (more than kLongRow entries): at most m / (kLongRow + 1) of them
+    const long long lmax = g.m / (kLongRow + 1) + 1;
+    const bool has_long = g.maxdeg > kLongRow;
+    int* hrank = ctx.scratch.alloc<int>(nn);
+    int* hlist = ctx.scratch.alloc<int>((size_t)lmax);
+    float* hagg = ctx.scratch.alloc<float>((size_t)lmax * rm::H);
+    unsigned* hcount = reinterpret_cast<unsigned*>(ctx.dscalars + 20);
     {
         PhaseScope ps(ctx, "rating_layers", 0);
+        if (has_long) {
+            KB_CUDA(cudaMemsetAsync(hcount, 0, sizeof(unsigned), s));
+            long_rows<<<(int)std::min<long long>(div_up(g.n, 256), 16LL * kNumSMs), 256, 0, s>>>(g.n, g.xadj, hrank,
+                                                                                             hlist, hcount);
+            KB_LAUNCH();
+        }
         for (int l = 1; l <= 3; ++l) {
             pack_weights<128, 64><<<32, 256, 0, s>>>(P, rm::layer_w(l), wl[l - 1]);
             KB_LAUNCH();
@@ -323,10 +397,15 @@ void rating_infer_tc(Ctx& ctx, const DevGraph& g, const float* P, float* prob, u
         __nv_bfloat16* cur = ha;
         __nv_bfloat16* nxt = hb;
         for (int l = 1; l <= 3; ++l) {
-            launch_fused<true, 64, true>(ctx, g, wdeg, cur, wl[l - 1], P, rm::layer_b(l), nxt, err);
+            if (has_long) {
+                long_row_sums<<<(int)std::min<long long>(lmax, 2LL * kNumSMs), kLongThreads, 0, s>>>(
+                    g.xadj, g.adjncy, g.adjwgt, cur, hlist, hcount, hagg);
+                KB_LAUNCH();
+            }
+            launch_fused<true, 64, true>(ctx, g, wdeg, cur, wl[l - 1], P, rm::layer_b(l), nxt, hrank, hagg, err);
             std::swap(cur, nxt);
         }
-        launch_fused<false, 32, false>(ctx, g, wdeg, cur, wz, P, rm::BZ, z, err);
+        launch_fused<false, 32, false>(ctx, g, wdeg, cur, wz, P, rm::BZ, z, hrank, hagg, err);
     }
     PhaseScope ps(ctx, "rating_head", 0);
     launch_head_bf16(ctx, g, P, z, prob, rating);

@@ -116,7 +116,14 @@ def graphs_for_tests(graphs):
     g2["adjwgt"] = (g2["adjwgt"] % 7 + 1).astype(np.int32)
     g2["vwgt"] = np.random.default_rng(3).integers(1, 9, g2["n"]).astype(np.int32)
     g3 = graphs.grid2d(40, 37)
-    return [g1, g2, g3]
+    # two hubs of 1500 and 2500 entries (rows longer than the tensor-core
+    # kernel's gather limit go through the per-row pre-sum) on a ring
+    from conftest import csr_from_edges
+    n4 = 4100
+    edges = [(v, (v + 1) % n4) for v in range(2, n4)] + [(0, v) for v in range(2, 1502)] + \
+            [(1, v) for v in range(1600, 4100)]
+    g4 = csr_from_edges(n4, edges, weights=[1 + (i * 7) % 5 for i in range(len(edges))])
+    return [g1, g2, g3, g4]
 
 
 def test_forward_matches_torch_and_tensor_cores(N, graphs):
