@@ -317,20 +317,44 @@ __global__ void __launch_bounds__(kMergeWarps * 32) merge_rows(int nc, const uin
         if (lane == 0) bigsz[r] = 0;
         int P = 1;
         while (P < s) P <<= 1;
-        for (int i = lane; i < P; i += 32) b[i] = i < s ? bucket[beg + i] : ~0ull;
-        __syncwarp();
-        for (int k = 2; k <= P; k <<= 1)
-            for (int j = k >> 1; j > 0; j >>= 1) {
-                for (int i = lane; i < P; i += 32) {
-                    const int l = i ^ j;
-                    if (l > i) {
-                        const uint64_t x = b[i], y = b[l];
-                        const bool up = (i & k) == 0;
-                        if ((x > y) == up) { b[i] = y; b[l] = x; }
+        if (P <= 64) {
+            // bitonic sort in registers: element i = lane + 32 r, r = 0, 1
+            uint64_t x0 = lane < s ? bucket[beg + lane] : ~0ull;
+            uint64_t x1 = lane + 32 < s ? bucket[beg + lane + 32] : ~0ull;
+            for (int k = 2; k <= 64; k <<= 1)
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    if (j == 32) {
+                        // partner in the same lane: elements lane and lane + 32
+                        const bool up = (lane & k) == 0;
+                        if ((x0 > x1) == up) { const uint64_t t = x0; x0 = x1; x1 = t; }
+                    } else {
+                        const uint64_t y0 = __shfl_xor_sync(0xffffffffu, x0, j);
+                        const uint64_t y1 = __shfl_xor_sync(0xffffffffu, x1, j);
+                        const bool lower = (lane & j) == 0;
+                        const bool up0 = (lane & k) == 0, up1 = ((lane + 32) & k) == 0;
+                        x0 = (lower == up0) ? (x0 < y0 ? x0 : y0) : (x0 > y0 ? x0 : y0);
+                        x1 = (lower == up1) ? (x1 < y1 ? x1 : y1) : (x1 > y1 ? x1 : y1);
                     }
                 }
-                __syncwarp();
-            }
+            b[lane] = x0;
+            b[lane + 32] = x1;
+            __syncwarp();
+        } else {
+            for (int i = lane; i < P; i += 32) b[i] = i < s ? bucket[beg + i] : ~0ull;
+            __syncwarp();
+            for (int k = 2; k <= P; k <<= 1)
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    for (int i = lane; i < P; i += 32) {
+                        const int l = i ^ j;
+                        if (l > i) {
+                            const uint64_t x = b[i], y = b[l];
+                            const bool up = (i & k) == 0;
+                            if ((x > y) == up) { b[i] = y; b[l] = x; }
+                        }
+                    }
+                    __syncwarp();
+                }
+        }
         // distinct targets, weights summed over each run
         uint32_t written = 0;
         for (int i0 = 0; i0 < s; i0 += 32) {

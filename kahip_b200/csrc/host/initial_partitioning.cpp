@@ -255,9 +255,19 @@ long long fm_refine(const HostGraph& g, std::vector<char>& side, const Limits& l
 // unmatched node takes the unmatched neighbour of best expansion*^2 rating
 // (edge_ratings.cpp:316-328), ties to the smaller id.  Leader = min id.
 std::vector<int> heavy_edge_labels(const HostGraph& g, uint64_t ks, uint64_t maxnode) {
+    // (hash, id) order by a stable LSD radix sort on the hash (ids start
+    // ascending): the same order as sorting the pairs
+    thread_local std::vector<std::pair<uint32_t, int>> tmp;
     std::vector<std::pair<uint32_t, int>> order(g.n);
+    tmp.resize(g.n);
     for (int v = 0; v < g.n; ++v) order[v] = {hash32(ks, (uint32_t)v), v};
-    std::sort(order.begin(), order.end());
+    for (int sh = 0; sh < 32; sh += 8) {
+        int cnt[257] = {0};
+        for (int i = 0; i < g.n; ++i) ++cnt[((order[i].first >> sh) & 255u) + 1];
+        for (int b = 0; b < 256; ++b) cnt[b + 1] += cnt[b];
+        for (int i = 0; i < g.n; ++i) tmp[cnt[(order[i].first >> sh) & 255u]++] = order[i];
+        order.swap(tmp);
+    }
     std::vector<int> mate(g.n, -1);
     for (const auto& hv : order) {
         int u = hv.second;
@@ -324,7 +334,16 @@ HostGraph contract_host(const HostGraph& g, const std::vector<int>& label, std::
                 acc[t] += (uint32_t)g.adjwgt[e];
             }
         }
-        std::sort(targets.begin(), targets.end());
+        if (targets.size() <= 24) {
+            for (size_t i = 1; i < targets.size(); ++i) {
+                const int x = targets[i];
+                size_t j = i;
+                for (; j > 0 && targets[j - 1] > x; --j) targets[j] = targets[j - 1];
+                targets[j] = x;
+            }
+        } else {
+            std::sort(targets.begin(), targets.end());
+        }
         for (int t : targets) {
             c.adjncy.push_back(t);
             c.adjwgt.push_back((int)acc[t]);
