@@ -105,6 +105,7 @@ struct InvalidInput : std::runtime_error {
 void check_uploaded(Ctx& ctx, DevGraph& g, uint32_t* total_weight = nullptr) {
     int flags = check_graph(ctx, g, total_weight);
     g.unit_weights = (flags & 16) == 0;
+    g.rows_sorted = (flags & 32) ? 0 : 1;
     if (flags & 1) throw InvalidInput("adjncy entry out of range");
     if (flags & 2) throw InvalidInput("negative edge weight");
     if (flags & 4) throw InvalidInput("negative node weight");

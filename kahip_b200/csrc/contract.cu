@@ -561,6 +561,7 @@ void contract(Ctx& ctx, const DevGraph& g, const int* label, int* cmap, DevGraph
     out = DevGraph{};
     out.n = nc;
     out.m = mc;
+    out.rows_sorted = 1;  // rows come out sorted by target, without repeats
     out.xadj = cxadj;
     out.adjncy = cadj;
     out.adjwgt = cwgt;

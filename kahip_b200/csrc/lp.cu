@@ -954,7 +954,7 @@ void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* la
     a.S = (uint32_t)kn.lpc_subrounds;
     a.inc = inc;
     a.minv = minv;
-    const bool sorted_rows = rows_strictly_increasing(ctx, g);
+    const bool sorted_rows = g.rows_sorted >= 0 ? g.rows_sorted == 1 : rows_strictly_increasing(ctx, g);
     for (int r = 0; r < kn.lpc_rounds; ++r) {
         a.ks_sub = stream_key(kn.seed, TAG_CSUB, level, r);
         a.ks_tie = stream_key(kn.seed, TAG_CTIE, level, r);

@@ -18,6 +18,7 @@ struct DevGraph {
     int maxdeg = 0;
     unsigned iso_count = 0, iso_wmax = 0;  // isolated vertices and their largest weight (max_degree fills them)
     bool unit_weights = false;  // every edge weight is 1 (lets sweeps skip adjwgt)
+    int rows_sorted = -1;       // 1 / 0: rows do / do not list targets strictly increasing; -1 unknown
     const int* xadj = nullptr;
     const int* adjncy = nullptr;
     const int* adjwgt = nullptr;
@@ -56,7 +57,8 @@ void degree_stats(Ctx& ctx, DevGraph& g);
 
 // Device-side input checks: bit 1 = target out of range, 2 = negative edge
 // weight, 4 = negative node weight, 8 = xadj not starting at 0 / not
-// monotone, 16 = some edge weight differs from 1 (not an error).  Also returns the node weight sum (32-bit, as the reference's
+// monotone, 16 = some edge weight differs from 1 (not an error), 32 = some
+// row does not list its targets in strictly increasing order (not an error).  Also returns the node weight sum (32-bit, as the reference's
 // NodeWeight accumulates it).  Synchronises the stream.
 int check_graph(Ctx& ctx, const DevGraph& g, uint32_t* total_weight = nullptr);
 

@@ -114,8 +114,14 @@ __global__ void check_graph_kernel(int n, long long m, const int* __restrict__ x
     }
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
         if (vwgt[v] < 0) f |= 4;
-        if (xadj[v + 1] < xadj[v]) f |= 8;
+        const int b = xadj[v], e1 = xadj[v + 1];
+        if (e1 < b) f |= 8;
         w += (unsigned)vwgt[v];
+        // rows listing their targets in strictly increasing order (not an
+        // error; lets the first clustering round skip aggregation)
+        if (!(f & 32) && b >= 0 && e1 <= m)
+            for (int e = b + 1; e < e1; ++e)
+                if (adjncy[e] <= adjncy[e - 1]) { f |= 32; break; }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && xadj[0] != 0) f |= 8;
     f = __reduce_or_sync(0xffffffffu, f);
