@@ -498,15 +498,18 @@ def run_learned(args, rank, dev):
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
+            st = native.Stats()
             e0.record(stream)
             for _ in range(args.steps):
                 _, cut = native.kaffpa_device_knobs(n, t["xadj"], t["adjncy"], t["adjwgt"], t["vwgt"], part, kn,
-                                                    stream=stream)
+                                                    stream=stream, stats=st)
             e1.record(stream)
             torch.cuda.synchronize()
             bw = np.bincount(part.cpu().numpy(), minlength=64)
             res[label] = {"ms": e0.elapsed_time(e1) / args.steps, "cut": int(cut),
-                          "balanced": bool(bw.max() <= kn.final_bound)}
+                          "balanced": bool(bw.max() <= kn.final_bound), "levels": st.levels,
+                          "ms_coarsen": st.ms_coarsen, "ms_initial": st.ms_initial,
+                          "ms_uncoarsen": st.ms_uncoarsen}
         res["learned_over_plain_cut"] = res["learned_rating"]["cut"] / max(1, res["plain_rating"]["cut"])
         res["learned_over_plain_ms"] = res["learned_rating"]["ms"] / max(1e-9, res["plain_rating"]["ms"])
         results[name] = res

@@ -176,10 +176,10 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
                     hem_match(ctx, f, kn, L, nullptr, label);
                 }
                 bundle_isolated(ctx, f, kn.max_vertex_weight + 1u, label);
-                // a matching that removes less than a quarter of the nodes
+                // a matching that removes less than 40 % of the nodes
                 // (stars, skewed degrees) gives way to LP clustering
                 const long long nc = count_leaders(ctx, f.n, label);
-                lp = 4 * nc > 3 * (long long)f.n;
+                lp = 5 * nc > 3 * (long long)f.n;
             }
             if (lp) {
                 lp_cluster(ctx, f, kn, L, label);

@@ -1247,11 +1247,11 @@ int or_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt,
         if (kn.coarsening == 1) {
             or_hem_match(f, &kn, L, NULL, label);
             or_bundle_isolated(f, kn.max_vertex_weight + 1u, label);
-            /* a matching that removes less than a quarter of the nodes (stars,
+            /* a matching that removes less than 40 % of the nodes (stars,
              * skewed degrees) gives way to LP clustering for this level */
             long long nc = 0;
             for (int v = 0; v < f->n; ++v) nc += label[v] == v;
-            if (4 * nc > 3 * (long long)f->n) {
+            if (5 * nc > 3 * (long long)f->n) {
                 or_lp_cluster(f, &kn, L, label);
                 or_bundle_isolated(f, kn.cluster_bound, label);
             }
