@@ -245,6 +245,21 @@ int kb200_edge_cut_noalloc(int n, const int* d_xadj, const int* d_adjncy, const 
                            const int* d_vwgt, const int* d_part, int k, long long* d_cut, uint32_t* d_bw,
                            void* stream);
 
+/* ---- graph and partition files (host; no counterpart needed on the device) ----
+ * kb200_read_metis: METIS text format as the reference reads it
+ * (lib/io/graph_io.cpp:82-191: header "n m [fmt]", fmt 1/10/11 = edge /
+ * node / both weights, 1-based targets, '%' comments); parsed in parallel.
+ * kb200_read_bgf: ParHIP binary graph, version 3 (parallel_graph_io.cpp:
+ * 474-594).  Both return 0 and library-allocated arrays (unit weights
+ * filled in; release each with kb200_free), or -1 (kb200_io_error() says
+ * why; self-loops and miscounted nodes/edges are errors).
+ * kb200_write_partition: one block id per line (graph_io::writePartition). */
+int kb200_read_metis(const char* path, int* n, long long* m, int** xadj, int** adjncy, int** adjwgt, int** vwgt);
+int kb200_read_bgf(const char* path, int* n, long long* m, int** xadj, int** adjncy, int** adjwgt, int** vwgt);
+int kb200_write_partition(const char* path, int n, const int* part);
+void kb200_free(void* p);
+const char* kb200_io_error(void);
+
 /* Last error message of the calling thread ("" if none). */
 const char* kb200_last_error(void);
 

@@ -98,6 +98,7 @@ EXPORTS = [
     "kb200_derive_knobs", "kb200_kaffpa", "kb200_kaffpa_device", "kb200_kaffpa_knobs",
     "kb200_kaffpa_device_knobs", "kb200_kaffpa_batch", "kb200_kaffpa_population", "kb200_hem_match",
     "kb200_rating_infer", "kb200_rating_train", "kb200_rating_grad",
+    "kb200_read_metis", "kb200_read_bgf", "kb200_write_partition", "kb200_free", "kb200_io_error",
     "kb200_lp_cluster", "kb200_contract",
     "kb200_lp_refine", "kb200_balance", "kb200_edge_cut", "kb200_project", "kb200_initial_partition",
     "kb200_last_error", "kb200_kernel_launches", "kb200_device_count", "kb200_edge_cut_noalloc",
@@ -127,6 +128,14 @@ def lib():
         L.kb200_rating_infer.argtypes = [i, vp, vp, vp, vp, vp, i, vp, vp]
         L.kb200_rating_train.argtypes = [ctypes.POINTER(TrainGraph), i, i, ctypes.c_float, vp, vp]
         L.kb200_rating_grad.argtypes = [ctypes.POINTER(TrainGraph), vp, vp, vp]
+        pp = ctypes.POINTER(ctypes.c_void_p)
+        L.kb200_read_metis.argtypes = [ctypes.c_char_p, c_int_p, c_ll_p, pp, pp, pp, pp]
+        L.kb200_read_bgf.argtypes = [ctypes.c_char_p, c_int_p, c_ll_p, pp, pp, pp, pp]
+        L.kb200_write_partition.argtypes = [ctypes.c_char_p, i, vp]
+        L.kb200_free.argtypes = [vp]
+        L.kb200_free.restype = None
+        L.kb200_io_error.restype = ctypes.c_char_p
+        L.kb200_io_error.argtypes = []
         L.kb200_kaffpa_batch.argtypes = [ctypes.POINTER(BatchItem), i, i, ctypes.POINTER(BatchReport)]
         L.kb200_kaffpa_population.argtypes = [i, vp, vp, vp, vp, i, d, i, vp, i, vp, vp, i,
                                               ctypes.POINTER(BatchReport)]
@@ -394,3 +403,40 @@ def rating_grad(g: dict, label, params):
     loss = np.zeros(1, np.float32)
     _check(lib().kb200_rating_grad(arr, _ptr(P), _ptr(G), _ptr(loss)))
     return G, float(loss[0])
+
+
+# ------------------------------------------------------------------ files
+
+def _read(fn, path: str) -> dict:
+    n, m = ctypes.c_int(), ctypes.c_longlong()
+    ptrs = [ctypes.c_void_p() for _ in range(4)]
+    rc = fn(os.fsencode(path), ctypes.byref(n), ctypes.byref(m), *[ctypes.byref(p) for p in ptrs])
+    if rc < 0:
+        raise KaHIPError(rc, lib().kb200_io_error().decode())
+    try:
+        def arr(p, cnt):
+            return np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_int)), shape=(max(cnt, 1),))[:cnt].copy()
+        N, M = n.value, m.value
+        return dict(n=N, m=M, xadj=arr(ptrs[0], N + 1), adjncy=arr(ptrs[1], M), adjwgt=arr(ptrs[2], M),
+                    vwgt=arr(ptrs[3], N))
+    finally:
+        for p in ptrs:
+            lib().kb200_free(p)
+
+
+def read_metis(path: str) -> dict:
+    """A METIS text graph file (unit weights filled in)."""
+    return _read(lib().kb200_read_metis, path)
+
+
+def read_bgf(path: str) -> dict:
+    """A ParHIP binary graph file (version 3)."""
+    return _read(lib().kb200_read_bgf, path)
+
+
+def write_partition(path: str, part) -> None:
+    """One block id per line."""
+    p = _i32(part)
+    rc = lib().kb200_write_partition(os.fsencode(path), len(p), _ptr(p))
+    if rc < 0:
+        raise KaHIPError(rc, lib().kb200_io_error().decode())

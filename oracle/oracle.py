@@ -241,6 +241,25 @@ def kaffpa_knobs(g: dict, kn: Knobs, unit_weights=False):
 
 # --------------------------------------------------------------- reference
 
+def ref_read_metis(path: str) -> dict:
+    """graph_io::readGraphWeighted of the reference, as a CSR dict (run in a
+    separate process: oracle/_ref/ref_read_metis)."""
+    import subprocess
+    import tempfile
+    exe = os.path.join(HERE, "_ref", "ref_read_metis")
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "csr.bin")
+        subprocess.run([exe, path, out], check=True)
+        raw = open(out, "rb").read()
+    n = int(np.frombuffer(raw[:4], np.int32)[0])
+    m = int(np.frombuffer(raw[4:12], np.int64)[0])
+    a = np.frombuffer(raw[12:], np.int32)
+    x, a = a[:n + 1], a[n + 1:]
+    adj, a = a[:m], a[m:]
+    w, v = a[:m], a[m:m + n]
+    return dict(n=n, m=m, xadj=x.copy(), adjncy=adj.copy(), adjwgt=w.copy(), vwgt=v.copy())
+
+
 def ref_kaffpa(g: dict, k: int, imbalance=0.03, seed=0, mode=0):
     """Reference kaffpa() from the library built out of the reference sources."""
     L = ref()

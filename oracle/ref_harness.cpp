@@ -25,6 +25,7 @@
 #include "partition/coarsening/stop_rules/stop_rules.h"
 #include "partition/uncoarsening/refinement/label_propagation_refinement/label_propagation_refinement.h"
 #include "partition/uncoarsening/refinement/quotient_graph_refinement/complete_boundary.h"
+#include "io/graph_io.h"
 #include "tools/quality_metrics.h"
 #include "tools/random_functions.h"
 #include "configuration.h"
@@ -270,6 +271,28 @@ void ref_lp_refine(int n, const int* xadj, const int* adjncy, const int* vwgt,
     label_propagation_refinement lpr;
     lpr.perform_refinement(pc, G, boundary);
     for (int v = 0; v < n; ++v) part[v] = (int)G.getPartitionIndex(v);
+}
+
+// graph_io::readGraphWeighted (lib/io/graph_io.cpp:82-191).  First call with
+// null arrays returns n and the entry count; the second call fills them.
+int ref_read_metis(const char* path, int* n, long long* m, int* xadj, int* adjncy, int* adjwgt, int* vwgt) {
+    graph_access G;
+    if (graph_io::readGraphWeighted(G, path) != 0) return -1;
+    *n = (int)G.number_of_nodes();
+    *m = (long long)G.number_of_edges();
+    if (!xadj) return 0;
+    int e = 0;
+    for (int v = 0; v < *n; ++v) {
+        xadj[v] = e;
+        vwgt[v] = (int)G.getNodeWeight(v);
+        for (EdgeID x = G.get_first_edge(v); x < G.get_first_invalid_edge(v); ++x) {
+            adjncy[e] = (int)G.getEdgeTarget(x);
+            adjwgt[e] = (int)G.getEdgeWeight(x);
+            ++e;
+        }
+    }
+    xadj[*n] = e;
+    return 0;
 }
 
 }  // extern "C"
