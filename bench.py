@@ -487,12 +487,16 @@ def run_learned(args, rank, dev):
              for key in ("xadj", "adjncy", "adjwgt", "vwgt")}
         part = torch.empty(n, dtype=torch.int32, device=dev)
         res = {"n": n, "m_directed": g["m"]}
-        for label, coarsening, guard in (("lp", 0, 0.0), ("plain_rating", 1, 0.0), ("learned_rating", 2, 0.0),
-                                         ("learned_rating_guarded", 2, 1.0)):
+        for label, coarsening, guard, levels in (("lp", 0, 0.0, 0), ("plain_rating", 1, 0.0, 0),
+                                                 ("learned_rating", 2, 0.0, 0),
+                                                 ("learned_rating_level0", 2, 0.0, 1),
+                                                 ("learned_rating_levels01", 2, 0.0, 2),
+                                                 ("learned_rating_guarded", 2, 1.0, 0)):
             kn = native.derive_knobs(n, g["vwgt"], 64, IMBALANCE, 0, MODE_FAST)
             kn.coarsening = coarsening
             kn.rating_model = P.ctypes.data_as(ctypes.c_void_p) if coarsening == 2 else None
             kn.rating_fallback = guard
+            kn.rating_levels = levels
             for _ in range(max(1, args.warmup)):
                 native.kaffpa_device_knobs(n, t["xadj"], t["adjncy"], t["adjwgt"], t["vwgt"], part, kn, stream=stream)
             torch.cuda.synchronize()

@@ -62,6 +62,8 @@ typedef struct kb200_knobs {
                                   (NULL = fall back to expansion*^2) */
     double rating_fallback;    /* coarsening 2: > 0 also runs the expansion*^2 matching and
                                   keeps it when learned cut > rating_fallback * its cut */
+    int rating_levels;         /* coarsening 2: levels 0 .. rating_levels-1 use the learned
+                                  rating, deeper ones expansion*^2 (<= 0: every level) */
 } kb200_knobs;
 
 /* Parameter count of the learned edge rating (kahip_b200/csrc/learned.cuh). */

@@ -79,6 +79,7 @@ void derive_knobs_total(int n, uint32_t W, int k, double imbalance, int seed, in
     kn.match_rounds = 16;                // matching converges in < 10 rounds on meshes
     kn.rating_model = nullptr;
     kn.rating_fallback = 0.0;
+    kn.rating_levels = 0;
 }
 
 }  // namespace kb

@@ -168,7 +168,7 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
             int* label = ctx.scratch.alloc<int>((size_t)f.n);
             bool lp = kn.coarsening == 0;
             if (!lp) {
-                if (kn.coarsening == 2 && d_model) {
+                if (kn.coarsening == 2 && d_model && (kn.rating_levels <= 0 || L < kn.rating_levels)) {
                     uint32_t* rating = ctx.scratch.alloc<uint32_t>((size_t)std::max<long long>(f.m, 1));
                     rating_infer(ctx, f, d_model, nullptr, rating, true);
                     hem_match(ctx, f, kn, L, rating, label);

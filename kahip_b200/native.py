@@ -40,7 +40,7 @@ class Knobs(ctypes.Structure):
                 ("ip_fm_passes", ctypes.c_int), ("ip_fm_stall", ctypes.c_int),
                 ("max_levels", ctypes.c_int), ("coarsening", ctypes.c_int),
                 ("match_rounds", ctypes.c_int), ("rating_model", ctypes.c_void_p),
-                ("rating_fallback", ctypes.c_double)]
+                ("rating_fallback", ctypes.c_double), ("rating_levels", ctypes.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -49,6 +49,7 @@ typedef struct {
     int match_rounds;       /* cap on locally-dominant matching rounds */
     const float* rating_model; /* unused by the oracle (same layout as the product's knobs) */
     double rating_fallback;    /* unused by the oracle */
+    int rating_levels;         /* unused by the oracle */
 } or_knobs;
 
 typedef struct {
