@@ -109,37 +109,21 @@ __device__ __forceinline__ void emit_range(int e0, int e1, int step, uint32_t ow
     if (used) flush(used);
 }
 
+// Long rows (> kEmitLaneDeg entries) are left to emit_wide; their
+// write cursor wpos[v] starts at the row's first entry.
 __global__ void __launch_bounds__(kThreads) emit_kernel(int n, const int* __restrict__ xadj,
                                                         const int* __restrict__ adjncy,
                                                         const int* __restrict__ adjwgt,
                                                         const int* __restrict__ cmap, uint64_t* ekey,
-                                                        uint32_t* eval, uint32_t* vcount, int tb) {
-    __shared__ int wpos[kThreads / 32];
-    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
-    // the loop runs warp-uniformly (every lane takes the same number of
-    // iterations) so that long rows can be shared by the warp
+                                                        uint32_t* eval, uint32_t* vcount, int* wpos, int tb) {
     for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
         const int v = (int)(base + threadIdx.x);
-        const bool valid = v < n;
-        const int beg = valid ? xadj[v] : 0, end = valid ? xadj[v + 1] : 0;
-        const bool wide = valid && end - beg > kEmitLaneDeg;
-        unsigned wm = __ballot_sync(0xffffffffu, wide);
-        while (wm) {
-            const int src = __ffs(wm) - 1;
-            wm &= wm - 1;
-            const int hv = __shfl_sync(0xffffffffu, v, src);
-            const int hb = __shfl_sync(0xffffffffu, beg, src);
-            const int he = __shfl_sync(0xffffffffu, end, src);
-            const uint32_t hown = (uint32_t)cmap[hv];
-            if (lane == 0) wpos[wp] = hb;
-            __syncwarp();
-            emit_range<true>(hb + lane, he, 32, hown, (uint64_t)hown << tb, adjncy, adjwgt, cmap, ekey, eval,
-                             &wpos[wp]);
-            __syncwarp();
-            if (lane == src) vcount[hv] = (uint32_t)(wpos[wp] - hb);
-            __syncwarp();
+        if (v >= n) continue;
+        const int beg = xadj[v], end = xadj[v + 1];
+        if (end - beg > kEmitLaneDeg) {
+            wpos[v] = beg;
+            continue;
         }
-        if (!valid || wide) continue;
         const uint32_t own = (uint32_t)cmap[v];
         const uint64_t hi = (uint64_t)own << tb;
         uint32_t st[kEmitSlots], sw[kEmitSlots];
@@ -191,6 +175,44 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(int n, const int* __rest
             }
         vcount[v] = (uint32_t)(pos - beg);
     }
+}
+
+// Long rows, spread over warps: the entry space is cut into chunks of
+// kEmitChunk entries; the warp of a chunk emits the part of every long row
+// that falls into it (light rows are emit_kernel's), taking write positions
+// from the row's cursor by atomics.  Chunks of one row are not merged with
+// each other here; the per-row merge later is.
+constexpr int kEmitChunk = 2048;
+
+__global__ void __launch_bounds__(kThreads) emit_wide(int n, long long m, const int* __restrict__ xadj,
+                                                      const int* __restrict__ adjncy, const int* __restrict__ adjwgt,
+                                                      const int* __restrict__ cmap, uint64_t* ekey, uint32_t* eval,
+                                                      int* wpos, int tb) {
+    const int lane = threadIdx.x & 31;
+    const long long chunks = (m + kEmitChunk - 1) / kEmitChunk;
+    for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32; c < chunks;
+         c += (long long)gridDim.x * blockDim.x / 32) {
+        const long long lo = c * kEmitChunk, hi = std::min<long long>(lo + kEmitChunk, m);
+        // v = the row holding entry lo: largest v with xadj[v] <= lo
+        int a = 0, b = n;
+        while (b - a > 1) {
+            const int mid = (a + b) >> 1;
+            if (xadj[mid] <= lo) a = mid;
+            else b = mid;
+        }
+        for (int v = a; v < n && xadj[v] < hi; ++v) {
+            const int beg = xadj[v], end = xadj[v + 1];
+            if (end - beg <= kEmitLaneDeg) continue;
+            const int s = (int)std::max<long long>(lo, beg), e = (int)std::min<long long>(hi, end);
+            const uint32_t own = (uint32_t)cmap[v];
+            emit_range<true>(s + lane, e, 32, own, (uint64_t)own << tb, adjncy, adjwgt, cmap, ekey, eval, wpos + v);
+        }
+    }
+}
+
+__global__ void wide_counts(int n, const int* __restrict__ xadj, const int* __restrict__ wpos, uint32_t* vcount) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
+        if (xadj[v + 1] - xadj[v] > kEmitLaneDeg) vcount[v] = (uint32_t)(wpos[v] - xadj[v]);
 }
 
 // entries of vertex v move from its CSR range to voff[v] in the sort input
@@ -480,11 +502,20 @@ void contract(Ctx& ctx, const DevGraph& g, const int* label, int* cmap, DevGraph
     uint64_t* ekey = ctx.scratch.alloc<uint64_t>((size_t)std::max<long long>(m, 1));
     uint32_t* eval = ctx.scratch.alloc<uint32_t>((size_t)std::max<long long>(m, 1));
     uint32_t* vcount = ctx.scratch.alloc<uint32_t>((size_t)n + 1);
+    int* wpos = ctx.scratch.alloc<int>((size_t)n + 1);
     {
         PhaseScope ps(ctx, "contract_emit", 12.0 * m + 8.0 * n);
         emit_kernel<<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, g.adjncy, g.adjwgt, cmap, ekey, eval,
-                                                                vcount, tb);
+                                                                vcount, wpos, tb);
         KB_LAUNCH();
+        if (g.maxdeg > kEmitLaneDeg) {
+            const long long chunks = (m + kEmitChunk - 1) / kEmitChunk;
+            emit_wide<<<grid_for(32LL * chunks, kThreads), kThreads, 0, st>>>(n, m, g.xadj, g.adjncy, g.adjwgt, cmap,
+                                                                           ekey, eval, wpos, tb);
+            KB_LAUNCH();
+            wide_counts<<<grid_for(n, 256), 256, 0, st>>>(n, g.xadj, wpos, vcount);
+            KB_LAUNCH();
+        }
     }
     // 3. bucket the entries by coarse source row (at most m of them)
     uint32_t* rowsz = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
