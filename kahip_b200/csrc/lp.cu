@@ -583,17 +583,17 @@ __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
 // the shared table).
 constexpr int kSmemTab = 4096;
 
-template <int MODE>
+// BT threads per block (more for the longest rows).
 // `which`: 0 = every listed vertex, 1 = only those whose table fits in
 // shared memory, 2 = only the others (the two kinds can run as separate
 // launches with different grids; the decisions do not depend on the order).
-__global__ void __launch_bounds__(kThreads) heavy_kernel(SweepArgs a, uint32_t* gtk, uint32_t* gtv,
-                                                         int gcap, int which) {
-    __shared__ uint64_t sk[kThreads / 32];
-    __shared__ uint32_t sid[kThreads / 32];
+template <int MODE, int BT>
+__global__ void __launch_bounds__(BT) heavy_kernel(SweepArgs a, uint32_t* gtk, uint32_t* gtv, int gcap, int which) {
+    __shared__ uint64_t sk[BT / 32];
+    __shared__ uint32_t sid[BT / 32];
     __shared__ uint32_t sco;
     __shared__ uint32_t stk[kSmemTab], stv[kSmemTab];
-    for (int s = threadIdx.x; s < kSmemTab; s += kThreads) {
+    for (int s = threadIdx.x; s < kSmemTab; s += BT) {
         stk[s] = kEmpty;
         stv[s] = 0;
     }
@@ -620,7 +620,7 @@ __global__ void __launch_bounds__(kThreads) heavy_kernel(SweepArgs a, uint32_t* 
             atomicAdd(&a.work[0], 1ull);
             atomicAdd(&a.work[1], (unsigned long long)(end - beg));
         }
-        for (int c = beg; c < end; c += kThreads) {
+        for (int c = beg; c < end; c += BT) {
             int e = c + threadIdx.x;
             uint32_t l = kEmpty, wt = 0;
             if (e < end) {
@@ -634,7 +634,7 @@ __global__ void __launch_bounds__(kThreads) heavy_kernel(SweepArgs a, uint32_t* 
         __syncthreads();
         uint64_t key = 0;
         uint32_t id = kEmpty;
-        for (int s = threadIdx.x; s < cap; s += kThreads) {
+        for (int s = threadIdx.x; s < cap; s += BT) {
             uint32_t l = tk[s];
             if (l == kEmpty) continue;
             uint32_t c = tv[s];
@@ -647,7 +647,7 @@ __global__ void __launch_bounds__(kThreads) heavy_kernel(SweepArgs a, uint32_t* 
         if (lane == 0) { sk[w] = key; sid[w] = id; }
         __syncthreads();
         if (threadIdx.x == 0) {
-            for (int j = 1; j < kThreads / 32; ++j) better(key, id, sk[j], sid[j]);
+            for (int j = 1; j < BT / 32; ++j) better(key, id, sk[j], sid[j]);
             if (decide_emit<MODE>(a, v, own, cv, sco, key, id)) a.hplist[atomicAdd(a.hpcount, 1u)] = v;
         }
         __syncthreads();
@@ -893,14 +893,14 @@ void launch_sweep(Ctx& ctx, const DevGraph& g, SweepArgs a, const SweepBuffers& 
     if (b.gcap > 0) {
         PhaseScope ps(ctx, family(MODE, 2), 0);
         if (b.gcap <= kSmemTab) {
-            heavy_kernel<MODE><<<b.hblocks, kThreads, 0, ctx.stream>>>(a, nullptr, nullptr, b.gcap, 0);
+            heavy_kernel<MODE, kThreads><<<b.hblocks, kThreads, 0, ctx.stream>>>(a, nullptr, nullptr, b.gcap, 0);
             KB_LAUNCH();
         } else {
             // rows that fit the shared tables on many blocks, the longest
             // rows on the blocks that own a global table
-            heavy_kernel<MODE><<<8 * kNumSMs, kThreads, 0, ctx.stream>>>(a, nullptr, nullptr, b.gcap, 1);
+            heavy_kernel<MODE, kThreads><<<8 * kNumSMs, kThreads, 0, ctx.stream>>>(a, nullptr, nullptr, b.gcap, 1);
             KB_LAUNCH();
-            heavy_kernel<MODE><<<b.hblocks, kThreads, 0, ctx.stream>>>(a, b.gtk, b.gtv, b.gcap, 2);
+            heavy_kernel<MODE, 1024><<<b.hblocks, 1024, 0, ctx.stream>>>(a, b.gtk, b.gtv, b.gcap, 2);
             KB_LAUNCH();
         }
     }
