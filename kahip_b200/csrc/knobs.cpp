@@ -65,7 +65,7 @@ void derive_knobs_total(int n, uint32_t W, int k, double imbalance, int seed, in
     kn.lpc_rounds = fast ? 5 : 10;       // label_iterations = 10 (configuration.h:424)
     kn.lpc_subrounds = 2;                // later rounds: two sub-rounds (round 0 is one)
     kn.ref_rounds = fast ? 10 : 25;      // label_iterations_refinement = 25 (:425)
-    kn.ref_subrounds = 4;
+    kn.ref_subrounds = 2;
     kn.ref_classes = 16;
     kn.bal_iters = 64;
     kn.ip_reps = fast ? 1 : 2;

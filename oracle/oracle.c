@@ -102,7 +102,7 @@ void or_derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, 
     o->lpc_rounds = fast ? 5 : 10;
     o->lpc_subrounds = 2;
     o->ref_rounds = fast ? 10 : 25;
-    o->ref_subrounds = 4;
+    o->ref_subrounds = 2;
     o->ref_classes = 16;
     o->bal_iters = 64;
     o->ip_reps = fast ? 1 : 2;
