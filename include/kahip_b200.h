@@ -64,6 +64,10 @@ typedef struct kb200_knobs {
                                   keeps it when learned cut > rating_fallback * its cut */
     int rating_levels;         /* coarsening 2: levels 0 .. rating_levels-1 use the learned
                                   rating, deeper ones expansion*^2 (<= 0: every level) */
+    int refinement;            /* 0 = LP refinement (default), 1 = Jet refinement */
+    int jet_iters, jet_patience;  /* Jet: iteration cap, iterations without a better cut */
+    int jet_c0, jet_c;         /* Jet: negative-gain tolerance in quarters of the own
+                                  connection, finest level / coarser levels */
 } kb200_knobs;
 
 /* Parameter count of the learned edge rating (kahip_b200/csrc/learned.cuh). */
@@ -214,6 +218,11 @@ int kb200_contract(int n, const int* xadj, const int* adjncy, const int* adjwgt,
 /* LP refinement at one level: part[n] in/out. */
 int kb200_lp_refine(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
                     const kb200_knobs* kn, int level, uint32_t bound, int* part);
+
+/* Jet refinement at one level (stands in for the reference's k-way FM,
+ * kway_graph_refinement_core.cpp:47-171): part[n] in/out. */
+int kb200_jet_refine(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                     const kb200_knobs* kn, int level, uint32_t bound, int* part);
 
 /* Balance repair: part[n] in/out; *balanced = 1 if every block <= bound. */
 int kb200_balance(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,

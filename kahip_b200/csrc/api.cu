@@ -19,6 +19,7 @@
 
 #include "contract.cuh"
 #include "host/initial_partitioning.h"
+#include "jet.cuh"
 #include "knobs.h"
 #include "learned.cuh"
 #include "match.cuh"
@@ -194,7 +195,8 @@ double ms_since(clk::time_point t) { return std::chrono::duration<double, std::m
 int check_knobs(const kb200_knobs* kn) {
     if (!kn) return fail(KB_ERR_INVALID_INPUT, "knobs is NULL");
     if (kn->k < 1 || kn->lpc_subrounds < 1 || kn->ref_subrounds < 1 || kn->ref_classes < 1 ||
-        kn->coarsening < 0 || kn->coarsening > 2 || kn->max_levels < 1 || kn->max_levels > 64)
+        kn->coarsening < 0 || kn->coarsening > 2 || kn->max_levels < 1 || kn->max_levels > 64 ||
+        kn->refinement < 0 || kn->refinement > 1 || kn->jet_iters < 0 || kn->jet_patience < 1)
         return fail(KB_ERR_INVALID_INPUT, "invalid knobs");
     return KB_OK;
 }
@@ -568,7 +570,7 @@ int kb200_contract(int n, const int* xadj, const int* adjncy, const int* adjwgt,
 }
 
 static int part_phase(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
-                      const kb200_knobs* kn, int level, uint32_t bound, int* part, int* balanced, bool bal) {
+                      const kb200_knobs* kn, int level, uint32_t bound, int* part, int* balanced, int what) {
     g_last_error.clear();
     return guarded([&]() -> int {
         int rc, dev;
@@ -581,9 +583,11 @@ static int part_phase(int n, const int* xadj, const int* adjncy, const int* adjw
         uint32_t* bw = pr.ctx.hier.alloc<uint32_t>((size_t)kn->k);
         if (n) KB_CUDA(cudaMemcpyAsync(pr.up.part, part, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, s));
         block_weights_and_cut(pr.ctx, pr.up.g, pr.up.part, kn->k, bw, nullptr);
-        if (bal) {
+        if (what == 1) {
             bool ok = balance(pr.ctx, pr.up.g, *kn, level, bound, pr.up.part, bw);
             if (balanced) *balanced = ok ? 1 : 0;
+        } else if (what == 2) {
+            jet_refine(pr.ctx, pr.up.g, *kn, level, bound, pr.up.part, bw);
         } else {
             lp_refine(pr.ctx, pr.up.g, *kn, level, bound, pr.up.part, bw);
         }
@@ -595,12 +599,17 @@ static int part_phase(int n, const int* xadj, const int* adjncy, const int* adjw
 
 int kb200_lp_refine(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
                     const kb200_knobs* kn, int level, uint32_t bound, int* part) {
-    return part_phase(n, xadj, adjncy, adjwgt, vwgt, kn, level, bound, part, nullptr, false);
+    return part_phase(n, xadj, adjncy, adjwgt, vwgt, kn, level, bound, part, nullptr, 0);
+}
+
+int kb200_jet_refine(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                     const kb200_knobs* kn, int level, uint32_t bound, int* part) {
+    return part_phase(n, xadj, adjncy, adjwgt, vwgt, kn, level, bound, part, nullptr, 2);
 }
 
 int kb200_balance(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
                   const kb200_knobs* kn, int level, uint32_t bound, int* part, int* balanced) {
-    return part_phase(n, xadj, adjncy, adjwgt, vwgt, kn, level, bound, part, balanced, true);
+    return part_phase(n, xadj, adjncy, adjwgt, vwgt, kn, level, bound, part, balanced, 1);
 }
 
 int kb200_edge_cut(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt, const int* part,

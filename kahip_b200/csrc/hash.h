@@ -25,6 +25,7 @@ enum HashTag : int {
     TAG_IP = 9,     // initial partitioning: start nodes
     TAG_IPM = 10,   // initial partitioning: matching order
     TAG_MATCH = 11, // heavy-edge matching: pair hash
+    TAG_JTIE = 12,  // Jet refinement: destination tie-break
 };
 
 // splitmix64 output function (Steele, Lea & Flood, OOPSLA 2014).

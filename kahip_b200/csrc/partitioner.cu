@@ -11,6 +11,7 @@
 
 #include "contract.cuh"
 #include "host/initial_partitioning.h"
+#include "jet.cuh"
 #include "learned.cuh"
 #include "match.cuh"
 #include "prims.cuh"
@@ -237,7 +238,8 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
         const uint32_t bound = l == 0 ? kn.final_bound : kn.upper_bound;
         block_weights_and_cut(ctx, g, lv[l].part, k, bw, nullptr);
         bool ok = balance(ctx, g, kn, l, bound, lv[l].part, bw);
-        lp_refine(ctx, g, kn, l, bound, lv[l].part, bw);
+        if (kn.refinement == 1) jet_refine(ctx, g, kn, l, bound, lv[l].part, bw);
+        else lp_refine(ctx, g, kn, l, bound, lv[l].part, bw);
         if (l == 0) balanced = ok;
         if (collect || l == 0) {
             long long c = read_cut(ctx, g, lv[l].part, k, bw);

@@ -40,7 +40,9 @@ class Knobs(ctypes.Structure):
                 ("ip_fm_passes", ctypes.c_int), ("ip_fm_stall", ctypes.c_int),
                 ("max_levels", ctypes.c_int), ("coarsening", ctypes.c_int),
                 ("match_rounds", ctypes.c_int), ("rating_model", ctypes.c_void_p),
-                ("rating_fallback", ctypes.c_double), ("rating_levels", ctypes.c_int)]
+                ("rating_fallback", ctypes.c_double), ("rating_levels", ctypes.c_int),
+                ("refinement", ctypes.c_int), ("jet_iters", ctypes.c_int), ("jet_patience", ctypes.c_int),
+                ("jet_c0", ctypes.c_int), ("jet_c", ctypes.c_int)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -99,7 +101,7 @@ EXPORTS = [
     "kb200_kaffpa_device_knobs", "kb200_kaffpa_batch", "kb200_kaffpa_population", "kb200_hem_match",
     "kb200_rating_infer", "kb200_rating_train", "kb200_rating_grad",
     "kb200_read_metis", "kb200_read_bgf", "kb200_write_partition", "kb200_free", "kb200_io_error",
-    "kb200_lp_cluster", "kb200_contract",
+    "kb200_lp_cluster", "kb200_contract", "kb200_jet_refine",
     "kb200_lp_refine", "kb200_balance", "kb200_edge_cut", "kb200_project", "kb200_initial_partition",
     "kb200_last_error", "kb200_kernel_launches", "kb200_device_count", "kb200_edge_cut_noalloc",
     # reference-compatible ABI (include/kaHIP_interface.h)
@@ -142,6 +144,7 @@ def lib():
         L.kb200_lp_cluster.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, vp]
         L.kb200_contract.argtypes = [i, vp, vp, vp, vp, vp, c_int_p, c_ll_p, vp, vp, vp, vp, vp]
         L.kb200_lp_refine.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, u32, vp]
+        L.kb200_jet_refine.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, u32, vp]
         L.kb200_balance.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, u32, vp, c_int_p]
         L.kb200_edge_cut.argtypes = [i, vp, vp, vp, vp, vp, i, c_ll_p, vp]
         L.kb200_project.argtypes = [i, vp, i, vp, vp]
@@ -246,6 +249,13 @@ def contract(g: dict, label):
     k, mk = nc.value, mc.value
     return dict(n=k, m=mk, xadj=cx[:k + 1].copy(), adjncy=ca[:mk].copy(), adjwgt=cw[:mk].copy(),
                 vwgt=cv[:k].copy()), cmap
+
+
+def jet_refine(g: dict, kn: Knobs, part, bound: int, level=0) -> np.ndarray:
+    p = np.array(part, np.int32)
+    _check(lib().kb200_jet_refine(g["n"], _ptr(g["xadj"]), _ptr(g["adjncy"]), _ptr(g["adjwgt"]),
+                                  _ptr(g["vwgt"]), ctypes.byref(kn), level, bound, _ptr(p)))
+    return p
 
 
 def lp_refine(g: dict, kn: Knobs, part, bound: int, level=0) -> np.ndarray:

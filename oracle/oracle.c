@@ -13,7 +13,7 @@
 
 enum {
     TAG_CSUB = 1, TAG_CTIE = 2, TAG_RSUB = 3, TAG_RTIE = 4, TAG_RPRIO = 5,
-    TAG_BTIE = 6, TAG_BCLS = 7, TAG_BPRIO = 8, TAG_IP = 9, TAG_IPM = 10, TAG_MATCH = 11
+    TAG_BTIE = 6, TAG_BCLS = 7, TAG_BPRIO = 8, TAG_IP = 9, TAG_IPM = 10, TAG_MATCH = 11, TAG_JTIE = 12
 };
 
 #define BAL_CLASSES 256
@@ -112,6 +112,11 @@ void or_derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, 
     o->max_levels = 48;
     o->coarsening = 0;
     o->match_rounds = 16;
+    o->refinement = 0;
+    o->jet_iters = 32;
+    o->jet_patience = 12;
+    o->jet_c0 = 1;
+    o->jet_c = 3;
 }
 
 /* stop_rules.h:64-66: continue coarsening after a level that went from nf to
@@ -752,6 +757,114 @@ int or_balance(const or_graph* g, const or_knobs* kn, int level, uint32_t bound,
     return ok;
 }
 
+/* ------------------------------------------------------------ Jet refinement */
+
+static uint64_t overload_of(const uint32_t* bw, int k, uint32_t bound) {
+    uint64_t o = 0;
+    for (int b = 0; b < k; ++b) if (bw[b] > bound) o += bw[b] - bound;
+    return o;
+}
+
+/* Jet refinement (Gilbert, Madduri, Boman, Rajamanickam, "Jet: Multilevel
+ * Graph Partitioning on GPUs", 2023) in synchronous iterations; it stands in
+ * for the reference's k-way FM (kway_graph_refinement_core.cpp:47-171):
+ *   1. every vertex not moved in the previous iteration picks its most
+ *      connected other block d (ties as in refinement, stream TAG_JTIE); it
+ *      is a candidate when 4 (conn(d) - conn(own)) >= -c4 conn(own)
+ *      (c4 = jet_c0 on level 0, jet_c above): negative gains are allowed;
+ *   2. afterburner: a candidate's gain is recomputed with every neighbour of
+ *      higher priority (larger gain, then smaller id) already in its
+ *      destination; it moves if that gain is >= 0;
+ *   3. moves are applied, blocks above the bound are repaired (or_balance);
+ *   4. the best partition by (overload, cut) is kept; the loop ends after
+ *      jet_patience iterations without a better one, an iteration without
+ *      moves, or jet_iters iterations. */
+void or_jet_refine(const or_graph* g, const or_knobs* kn, int level, uint32_t bound, int* part) {
+    const int n = g->n, k = kn->k;
+    if (n == 0) return;
+    uint32_t* bw = xcalloc((size_t)k, sizeof(uint32_t));
+    int* best = xmalloc(sizeof(int) * (size_t)n);
+    int* dest = xmalloc(sizeof(int) * (size_t)n);
+    long long* gain = xmalloc(sizeof(long long) * (size_t)n);
+    int* moved_at = xmalloc(sizeof(int) * (size_t)n);
+    char* keep = xmalloc((size_t)n);
+    char* seen = xcalloc((size_t)k, 1);
+    or_acc a;
+    acc_init(&a, k, max_degree(g));
+    for (int v = 0; v < n; ++v) moved_at[v] = -2;
+    memcpy(best, part, sizeof(int) * (size_t)n);
+    or_block_weights(g, part, k, bw);
+    uint64_t best_ov = overload_of(bw, k, bound);
+    long long best_cut = or_edge_cut(g, part);
+    const int c4 = level == 0 ? kn->jet_c0 : kn->jet_c;
+    int since = 0;
+    for (int it = 0; it < kn->jet_iters; ++it) {
+        const uint64_t ks_tie = or_stream(kn->seed, TAG_JTIE, level, it);
+        for (int v = 0; v < n; ++v) {
+            dest[v] = -1;
+            if (moved_at[v] == it - 1) continue;
+            acc_gather(&a, g, v, part, seen);
+            const int own = part[v];
+            const long long co = seen[own] ? (long long)a.acc[own] : 0;
+            int d = -1;
+            uint32_t dc = 0;
+            for (int i = 0; i < a.ntouched; ++i) {
+                int b = a.touched[i];
+                if (b == own) continue;
+                uint32_t c = a.acc[b];
+                if (c == 0) continue;
+                if (d < 0 || beats(c, b, dc, d, -1, ks_tie)) { d = b; dc = c; }
+            }
+            acc_clear(&a, seen);
+            if (d < 0) continue;
+            const long long gv = (long long)dc - co;
+            if (4 * gv >= -(long long)c4 * co) { dest[v] = d; gain[v] = gv; }
+        }
+        long long moved = 0;
+        for (int v = 0; v < n; ++v) {
+            keep[v] = 0;
+            if (dest[v] < 0) continue;
+            long long adj = 0;
+            for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) {
+                int u = g->adjncy[e];
+                int bu = part[u];
+                if (dest[u] >= 0 && (gain[u] > gain[v] || (gain[u] == gain[v] && u < v))) bu = dest[u];
+                if (bu == dest[v]) adj += g->adjwgt[e];
+                else if (bu == part[v]) adj -= g->adjwgt[e];
+            }
+            keep[v] = adj >= 0;
+        }
+        for (int v = 0; v < n; ++v) {
+            if (!keep[v]) continue;
+            bw[part[v]] -= (uint32_t)g->vwgt[v];
+            bw[dest[v]] += (uint32_t)g->vwgt[v];
+            part[v] = dest[v];
+            moved_at[v] = it;
+            ++moved;
+        }
+        uint32_t mx = 0;
+        for (int b = 0; b < k; ++b) if (bw[b] > mx) mx = bw[b];
+        if (mx > bound) {
+            or_balance(g, kn, level, bound, part);
+            or_block_weights(g, part, k, bw);
+        }
+        const uint64_t ov = overload_of(bw, k, bound);
+        const long long cut = or_edge_cut(g, part);
+        if (ov < best_ov || (ov == best_ov && cut < best_cut)) {
+            best_ov = ov;
+            best_cut = cut;
+            memcpy(best, part, sizeof(int) * (size_t)n);
+            since = 0;
+        } else {
+            ++since;
+        }
+        if (moved == 0 || since >= kn->jet_patience) break;
+    }
+    memcpy(part, best, sizeof(int) * (size_t)n);
+    acc_free(&a);
+    free(bw); free(best); free(dest); free(gain); free(moved_at); free(keep); free(seen);
+}
+
 /* ------------------------------------------------- initial partitioning */
 
 /* max-heap of node ids keyed by (gain desc, id asc) with position index */
@@ -1225,7 +1338,7 @@ int or_kaffpa(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const
 int or_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
                     const or_knobs* knobs, long long* edgecut, int* part, or_stats* stats) {
     if (n < 0 || !knobs || knobs->k < 1 || !xadj || (n > 0 && !adjncy)) return -1;
-    if (knobs->coarsening < 0 || knobs->coarsening > 1) return -1;
+    if (knobs->coarsening < 0 || knobs->coarsening > 1 || knobs->refinement < 0 || knobs->refinement > 1) return -1;
     const int nparts = knobs->k;
     const int m = xadj[n];
     int* vw = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
@@ -1291,7 +1404,8 @@ int or_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt,
         uint32_t mx = 0;
         for (int b = 0; b < nparts; ++b) if (bw[b] > mx) mx = bw[b];
         if (mx > bound) or_balance(g, &kn, l, bound, cpart);
-        or_lp_refine(g, &kn, l, bound, cpart);
+        if (kn.refinement == 1) or_jet_refine(g, &kn, l, bound, cpart);
+        else or_lp_refine(g, &kn, l, bound, cpart);
         or_block_weights(g, cpart, nparts, bw);
         mx = 0;
         for (int b = 0; b < nparts; ++b) if (bw[b] > mx) mx = bw[b];

@@ -50,6 +50,8 @@ typedef struct {
     const float* rating_model; /* unused by the oracle (same layout as the product's knobs) */
     double rating_fallback;    /* unused by the oracle */
     int rating_levels;         /* unused by the oracle */
+    int refinement;            /* 0 = LP refinement, 1 = Jet refinement */
+    int jet_iters, jet_patience, jet_c0, jet_c;
 } or_knobs;
 
 typedef struct {
@@ -94,6 +96,10 @@ void or_hem_match(const or_graph* g, const or_knobs* kn, int level, const uint32
  * weight is 0), take the label of the group's first member; nothing happens
  * when G < 2 or fewer than two vertices are isolated.  label[] in/out. */
 void or_bundle_isolated(const or_graph* g, uint32_t bound, int* label);
+
+/* Jet refinement of one level (Gilbert et al. 2023, synchronous form; see
+ * oracle.c): part[n] in/out, blocks kept at or below `bound`. */
+void or_jet_refine(const or_graph* g, const or_knobs* kn, int level, uint32_t bound, int* part);
 
 /* LP clustering, synchronous schedule (one coarsening level). label[n] out. */
 void or_lp_cluster(const or_graph* g, const or_knobs* kn, int level, int* label);

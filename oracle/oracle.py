@@ -34,7 +34,9 @@ class Knobs(ctypes.Structure):
                 ("ip_fm_passes", ctypes.c_int), ("ip_fm_stall", ctypes.c_int),
                 ("max_levels", ctypes.c_int), ("coarsening", ctypes.c_int),
                 ("match_rounds", ctypes.c_int), ("rating_model", ctypes.c_void_p),
-                ("rating_fallback", ctypes.c_double), ("rating_levels", ctypes.c_int)]
+                ("rating_fallback", ctypes.c_double), ("rating_levels", ctypes.c_int),
+                ("refinement", ctypes.c_int), ("jet_iters", ctypes.c_int), ("jet_patience", ctypes.c_int),
+                ("jet_c0", ctypes.c_int), ("jet_c", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -185,6 +187,12 @@ def contract(g: dict, label) -> tuple[dict, np.ndarray]:
     mc = int(cx[nc])
     return dict(n=nc, m=mc, xadj=cx[:nc + 1].copy(), adjncy=ca[:mc].copy(), adjwgt=cw[:mc].copy(),
                 vwgt=cv[:nc].copy()), cmap
+
+
+def jet_refine(g: dict, kn: Knobs, part, bound: int, level=0) -> np.ndarray:
+    p = np.array(part, np.int32)
+    lib().or_jet_refine(G(g).ref, ctypes.byref(kn), level, ctypes.c_uint32(bound), _p(p))
+    return p
 
 
 def lp_refine(g: dict, kn: Knobs, part, bound: int, level=0) -> np.ndarray:

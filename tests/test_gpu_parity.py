@@ -267,3 +267,50 @@ def test_matching_hub_rows(N, O):
         kn_o = O.knobs(g, k, 0.03, 1, 0)
         kn_p = N.derive_knobs(g["n"], g["vwgt"], k, 0.03, 1, 0)
         assert np.array_equal(O.hem_match(g, kn_o, 0), N.hem_match(g, kn_p, 0))
+
+
+@pytest.mark.parametrize("name", CASE_NAMES)
+@pytest.mark.parametrize("k,level", [(8, 0), (33, 2)])
+def test_jet_refine_parity(N, O, cases, name, k, level):
+    g = cases[name]
+    kn_o = O.knobs(g, k, 0.03, 3, 1)
+    kn_p = N.derive_knobs(g["n"], g["vwgt"], k, 0.03, 3, 1)
+    rng = np.random.default_rng(k)
+    part = (np.arange(g["n"]) * k // g["n"]).astype(np.int32)
+    flip = rng.random(g["n"]) < 0.05
+    part[flip] = rng.integers(0, k, flip.sum())
+    a = O.jet_refine(g, kn_o, part, kn_o.upper_bound, level)
+    b = N.jet_refine(g, kn_p, part, kn_p.upper_bound, level)
+    assert np.array_equal(a, b), f"Jet differs at {np.flatnonzero(a != b)[:10]}"
+
+
+@pytest.mark.parametrize("name", CASE_NAMES)
+@pytest.mark.parametrize("k,mode,seed", [(8, 0, 0), (64, 1, 2)])
+def test_kaffpa_jet_parity(N, O, cases, name, k, mode, seed):
+    g = cases[name]
+    kn_o = O.knobs(g, k, 0.03, seed, mode)
+    kn_p = N.derive_knobs(g["n"], g["vwgt"], k, 0.03, seed, mode)
+    kn_o.refinement = kn_p.refinement = 1
+    cut_o, part_o, st_o = O.kaffpa_knobs(g, kn_o)
+    st = N.Stats()
+    st.collect_level_cuts = 1
+    rc, cut_p, part_p = N.kaffpa_knobs(g["xadj"], g["adjncy"], kn_p, vwgt=g["vwgt"], adjwgt=g["adjwgt"], stats=st)
+    assert st.levels == st_o.levels
+    for l in range(st.levels):
+        assert (st.level_cut[l], st.level_maxbw[l]) == (st_o.level_cut[l], st_o.level_maxbw[l]), l
+    assert cut_p == cut_o and np.array_equal(part_p, part_o)
+    assert O.block_weights(g, part_p, k).max() <= kn_o.final_bound
+
+
+def test_jet_hub_rows(N, O):
+    """Rows past the lane path's limits (many distinct blocks, long rows)."""
+    n = 5000
+    edges = [(0, v) for v in range(1, n)] + [(v, v + 1) for v in range(1, n - 1)] + \
+            [(1, v) for v in range(2000, 2600)]
+    g = csr_from_edges(n, edges, weights=[1 + (i * 13) % 7 for i in range(len(edges))])
+    for k in (16, 100):
+        kn_o = O.knobs(g, k, 0.05, 1, 1)
+        kn_p = N.derive_knobs(g["n"], g["vwgt"], k, 0.05, 1, 1)
+        part = (np.arange(n) * k // n).astype(np.int32)
+        assert np.array_equal(O.jet_refine(g, kn_o, part, kn_o.upper_bound, 1),
+                              N.jet_refine(g, kn_p, part, kn_p.upper_bound, 1))
