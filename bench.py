@@ -57,6 +57,7 @@ def make_graph(kind: str, logn: int):
 K_BLOCKS = 64
 IMBALANCE = 0.03
 MODE_FAST = 0
+MODES = {"fast": 0, "eco": 1}
 
 
 def parse():
@@ -71,6 +72,9 @@ def parse():
     p.add_argument("--workload", choices=["rgg", "batch", "population", "learned"], default="rgg",
                    help="rgg: the headline single-graph workload (default); batch: many independent graphs "
                         "of uneven size; population: many seeds of one device-resident RGG2D n=2^20")
+    p.add_argument("--mode", choices=["fast", "eco"], default="fast",
+                   help="kaffpa preset of the single-graph workload (fast, the headline: LP refinement; "
+                        "eco: Jet refinement)")
     p.add_argument("--graph", choices=sorted(GRAPH_KINDS), default="rgg2d",
                    help="single-graph workload kind (default rgg2d, the headline)")
     p.add_argument("--batch-count", type=int, default=512, help="graphs in the batch workload")
@@ -163,7 +167,7 @@ _SAMPLE = {}
 
 
 def _ref_task(args):
-    kind, logn, k, seed = args
+    kind, logn, k, seed, mode = args
     from oracle import oracle
     g = _SAMPLE.get((kind, logn))
     if g is None:
@@ -171,17 +175,17 @@ def _ref_task(args):
         _SAMPLE[(kind, logn)] = g
     t = time.perf_counter()
     unit = kind != "rmat"
-    cut, _ = oracle.ref_kaffpa(dict(g, vwgt=None, adjwgt=None) if unit else g, k, IMBALANCE, seed, MODE_FAST)
+    cut, _ = oracle.ref_kaffpa(dict(g, vwgt=None, adjwgt=None) if unit else g, k, IMBALANCE, seed, mode)
     return (time.perf_counter() - t) * 1e3, cut, g["m"]
 
 
-def reference_sample_ms(logn: int, k: int, procs: int, seeds, kind: str = "rgg2d"):
+def reference_sample_ms(logn: int, k: int, procs: int, seeds, kind: str = "rgg2d", mode: int = MODE_FAST):
     """Runs the reference kaffpa on the sample graph in `procs` processes;
     returns (wall ms, per-run ms list, cuts, m_sample)."""
     ctx = mp.get_context("spawn")
     t = time.perf_counter()
     with ctx.Pool(procs, initializer=_ref_worker_init) as pool:
-        res = pool.map(_ref_task, [(kind, logn, k, s) for s in seeds])
+        res = pool.map(_ref_task, [(kind, logn, k, s, mode) for s in seeds])
     wall = (time.perf_counter() - t) * 1e3
     return wall, [r[0] for r in res], [r[1] for r in res], res[0][2]
 
@@ -218,13 +222,13 @@ def run_reference_arm(args, rank):
     m_sample = None
     for step in range(args.warmup + args.steps):
         seeds = [step * procs + i for i in range(procs)]
-        wall, per, c, m_sample = reference_sample_ms(sample_logn, args.k, procs, seeds, args.graph)
+        wall, per, c, m_sample = reference_sample_ms(sample_logn, args.k, procs, seeds, args.graph, MODES[args.mode])
         if step >= args.warmup:
             step_ms.append(wall / procs)
             cuts += c
     scale = m_full / m_sample
     value = statistics.mean(step_ms) * scale
-    sample = (f"reference kaffpa fast (KaHIP built from its sources) on {GRAPH_KINDS[args.graph][0]} "
+    sample = (f"reference kaffpa {args.mode} (KaHIP built from its sources) on {GRAPH_KINDS[args.graph][0]} "
               f"n=2^{sample_logn} "
               f"(m_directed={m_sample}), {procs} concurrent processes (one per core) per step; "
               f"ms per partition = step wall / {procs}, scaled x{scale:.3f} by directed edges to n=2^{args.logn}")
@@ -243,8 +247,8 @@ def run_reference_arm(args, rank):
 
 def workload_config(args, m):
     name, desc, _ = GRAPH_KINDS[args.graph]
-    return {"workload": f"kaffpa fast on {name} n=2^{args.logn} ({desc}), k={args.k}, eps=3%",
-            "n": 1 << args.logn, "m_directed": m, "k": args.k, "imbalance": IMBALANCE, "preset": "fast",
+    return {"workload": f"kaffpa {args.mode} on {name} n=2^{args.logn} ({desc}), k={args.k}, eps=3%",
+            "n": 1 << args.logn, "m_directed": m, "k": args.k, "imbalance": IMBALANCE, "preset": args.mode,
             "seed": 0, "graph_seed": 0, "l2": "inputs (~2.2 GB CSR) exceed the 126 MB L2; no flush",
             "parallelism": "replicas" if args.gpus > 1 else "single GPU"}
 
@@ -294,7 +298,7 @@ def main():
     stream = torch.cuda.Stream(device=dev)
 
     def call(st=None):
-        return native.kaffpa_device(n, d_xadj, d_adj, d_w, d_vw, d_part, args.k, IMBALANCE, 0, MODE_FAST,
+        return native.kaffpa_device(n, d_xadj, d_adj, d_w, d_vw, d_part, args.k, IMBALANCE, 0, MODES[args.mode],
                                     stream=stream, stats=st)
 
     for _ in range(max(3, args.warmup)):
@@ -352,7 +356,7 @@ def main():
     # quality of the (deterministic) partition of the last timed call
     part = d_part.cpu().numpy()
     bw = np.bincount(part, minlength=args.k)
-    kn = native.derive_knobs(n, None, args.k, IMBALANCE, 0, MODE_FAST)
+    kn = native.derive_knobs(n, None, args.k, IMBALANCE, 0, MODES[args.mode])
 
     # ---- end to end through the host C ABI (pinned host buffers) ----
     h_xadj = torch.from_numpy(g["xadj"]).pin_memory()
@@ -365,7 +369,7 @@ def main():
 
     def e2e_call():
         rc = L.kb200_kaffpa(n, None, h_xadj.data_ptr(), None if h_w is None else h_w.data_ptr(), h_adj.data_ptr(),
-                            args.k, IMBALANCE, 0, MODE_FAST,
+                            args.k, IMBALANCE, 0, MODES[args.mode],
                             ctypes.byref(e2e_cut), h_part.data_ptr(), None)
         if rc < 0:
             raise RuntimeError(L.kb200_last_error().decode())
@@ -438,11 +442,11 @@ def main():
         from oracle import oracle
         if oracle.ref_available():
             sample_logn = GRAPH_KINDS[args.graph][2]
-            wall, per, c, m_sample = reference_sample_ms(sample_logn, args.k, 1, [0], args.graph)
+            wall, per, c, m_sample = reference_sample_ms(sample_logn, args.k, 1, [0], args.graph, MODES[args.mode])
             scale = m / m_sample
             line["cpu_baseline"] = {
                 "value": per[0] * scale, "unit": "ms", "cores": 1, "kind": "reference",
-                "sample": (f"one reference kaffpa fast run (KaHIP built from its sources, single-threaded) on "
+                "sample": (f"one reference kaffpa {args.mode} run (KaHIP built from its sources, single-threaded) on "
                            f"{GRAPH_KINDS[args.graph][0]} n=2^{sample_logn} (m_directed={m_sample}, "
                            f"{per[0]:.0f} ms, cut {c[0]}), "
                            f"scaled x{scale:.3f} by directed edges to n=2^{args.logn}")}
