@@ -14,8 +14,12 @@
 //                neighbours (larger gain, then smaller id) already moved;
 //                kept when >= 0;
 //   jet_apply    moves, block weights (integer atomics: order-free).
-// Then the host repairs the balance if needed (balance()), reads the cut and
-// block weights, and keeps the best partition by (overload, cut).
+// Then the host repairs the balance if needed (balance()).  The partition
+// an iteration leaves is judged at the start of the next one: jet_choose
+// scans every row anyway, so it also sums the cut of the partition it reads
+// (locked rows included), and the block weights are kept current by
+// jet_apply and balance(); the best partition by (overload, cut) is kept.
+// Only an iteration cap that ends the loop needs a separate cut pass.
 #include "jet.cuh"
 
 #include <vector>
@@ -31,6 +35,7 @@ constexpr int kThreads = 256;
 constexpr int kSlots = 8;
 constexpr int kLaneRow = 256;
 constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr int kLocked = 0x40000000;  // wide-list flag: the row only adds to the cut (n < 2^30)
 
 struct JetArgs {
     int n, k;
@@ -44,9 +49,16 @@ struct JetArgs {
     uint64_t ks_tie;
     int* dest;
     long long* gain;
-    int* wide;           // vertices left to jet_choose_wide
+    int* wide;           // vertices left to jet_choose_wide (| kLocked for locked rows)
     unsigned* nwide;
+    unsigned long long* cut2;  // twice the cut of part, summed by the choose kernels
 };
+
+__device__ __forceinline__ void add_cut(const JetArgs& A, unsigned long long c) {
+#pragma unroll
+    for (int off = 16; off; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(A.cut2, c);
+}
 
 // (conn desc, hash asc, id asc)
 __device__ __forceinline__ bool beats(uint32_t cb, uint32_t b, uint32_t ca, uint32_t a, uint64_t ks) {
@@ -66,25 +78,33 @@ __device__ __forceinline__ void candidate(const JetArgs& A, int v, int own, long
 }
 
 __global__ void __launch_bounds__(kThreads) jet_choose(JetArgs A) {
+    unsigned long long cut = 0;
     for (long long v0 = (long long)blockIdx.x * kThreads + threadIdx.x; v0 < A.n; v0 += (long long)gridDim.x * kThreads) {
         const int v = (int)v0;
         A.dest[v] = -1;
-        if (A.moved_at[v] == A.it - 1) continue;
+        const bool locked = A.moved_at[v] == A.it - 1;
         const int beg = A.xadj[v], end = A.xadj[v + 1];
         if (end - beg > kLaneRow) {
-            A.wide[atomicAdd(A.nwide, 1u)] = v;
+            A.wide[atomicAdd(A.nwide, 1u)] = locked ? (v | kLocked) : v;
             continue;
         }
         const int own = A.part[v];
+        if (locked) {
+            for (int e = beg; e < end; ++e)
+                if (A.part[A.adjncy[e]] != own) cut += (uint32_t)A.adjwgt[e];
+            continue;
+        }
         uint32_t sl[kSlots], sc[kSlots];
 #pragma unroll
         for (int i = 0; i < kSlots; ++i) { sl[i] = kNone; sc[i] = 0; }
         long long co = 0;
+        unsigned long long other = 0;
         bool overflow = false;
         for (int e = beg; e < end && !overflow; ++e) {
             const uint32_t b = (uint32_t)A.part[A.adjncy[e]];
             const uint32_t w = (uint32_t)A.adjwgt[e];
             if ((int)b == own) { co += w; continue; }
+            other += w;
             bool hit = false;
 #pragma unroll
             for (int i = 0; i < kSlots; ++i) {
@@ -101,9 +121,11 @@ __global__ void __launch_bounds__(kThreads) jet_choose(JetArgs A) {
             }
         }
         if (overflow) {
+            // the row is scanned again, and its cut summed, by jet_choose_wide
             A.wide[atomicAdd(A.nwide, 1u)] = v;
             continue;
         }
+        cut += other;
         uint32_t d = kNone, dc = 0;
 #pragma unroll
         for (int i = 0; i < kSlots; ++i)
@@ -113,6 +135,7 @@ __global__ void __launch_bounds__(kThreads) jet_choose(JetArgs A) {
             }
         candidate(A, v, own, co, d, dc);
     }
+    add_cut(A, cut);
 }
 
 // Block per listed vertex; cnt = this block's k counters (zero between
@@ -123,12 +146,24 @@ __global__ void __launch_bounds__(kThreads) jet_choose_wide(JetArgs A, uint32_t*
     uint32_t* cnt = counters + (size_t)blockIdx.x * A.k;
     const unsigned count = *A.nwide;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned long long cut = 0;
     for (unsigned i = blockIdx.x; i < count; i += gridDim.x) {
-        const int v = A.wide[i];
+        const int raw = A.wide[i];
+        const int v = raw & ~kLocked;
         const int beg = A.xadj[v], end = A.xadj[v + 1];
         const int own = A.part[v];
-        for (int e = beg + threadIdx.x; e < end; e += kThreads)
-            atomicAdd(&cnt[A.part[A.adjncy[e]]], (uint32_t)A.adjwgt[e]);
+        if (raw & kLocked) {
+            // block-uniform branch: a locked row only adds to the cut
+            for (int e = beg + threadIdx.x; e < end; e += kThreads)
+                if (A.part[A.adjncy[e]] != own) cut += (uint32_t)A.adjwgt[e];
+            continue;
+        }
+        for (int e = beg + threadIdx.x; e < end; e += kThreads) {
+            const int b = A.part[A.adjncy[e]];
+            const uint32_t x = (uint32_t)A.adjwgt[e];
+            atomicAdd(&cnt[b], x);
+            if (b != own) cut += x;
+        }
         __syncthreads();
         const long long co = cnt[own];
         __syncthreads();
@@ -163,6 +198,7 @@ __global__ void __launch_bounds__(kThreads) jet_choose_wide(JetArgs A, uint32_t*
         }
         __syncthreads();
     }
+    add_cut(A, cut);
 }
 
 __device__ __forceinline__ long long afterburn_sum(const JetArgs& A, int v, int beg, int end, int step, int first) {
@@ -236,11 +272,12 @@ int grid_for(long long items) {
 }  // namespace
 
 void jet_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t bound, int* part, uint32_t* bw) {
-    if (g.n == 0) return;
+    if (g.n == 0 || kn.jet_iters <= 0) return;
     cudaStream_t s = ctx.stream;
     const size_t mk = ctx.scratch.mark();
     const int n = g.n, k = kn.k;
     int* best = ctx.scratch.alloc<int>((size_t)n);
+    uint32_t* best_bw = ctx.scratch.alloc<uint32_t>((size_t)k);
     int* dest = ctx.scratch.alloc<int>((size_t)n);
     long long* gain = ctx.scratch.alloc<long long>((size_t)n);
     int* moved_at = ctx.scratch.alloc<int>((size_t)n);
@@ -253,21 +290,6 @@ void jet_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_
     KB_CUDA(cudaMemsetAsync(counters, 0, sizeof(uint32_t) * (size_t)wblocks * k, s));
     fill_i32_kernel<<<grid_for(n), kThreads, 0, s>>>(n, -2, moved_at);
     KB_LAUNCH();
-    KB_CUDA(cudaMemcpyAsync(best, part, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
-    std::vector<uint32_t> hbw((size_t)k);
-    auto measure = [&](uint64_t& ov, long long& cut) {
-        block_weights_and_cut(ctx, g, part, k, bw, cut2);
-        unsigned long long c2 = 0;
-        KB_CUDA(cudaMemcpyAsync(&c2, cut2, sizeof(c2), cudaMemcpyDeviceToHost, s));
-        KB_CUDA(cudaMemcpyAsync(hbw.data(), bw, sizeof(uint32_t) * (size_t)k, cudaMemcpyDeviceToHost, s));
-        KB_CUDA(cudaStreamSynchronize(s));
-        ov = 0;
-        for (uint32_t x : hbw) if (x > bound) ov += x - bound;
-        cut = (long long)(c2 / 2);
-    };
-    uint64_t best_ov;
-    long long best_cut;
-    measure(best_ov, best_cut);
     JetArgs A{};
     A.n = n;
     A.k = k;
@@ -281,49 +303,71 @@ void jet_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_
     A.gain = gain;
     A.wide = wide;
     A.nwide = ctr;
+    A.cut2 = cut2;
+    // bw holds the block weights of part on entry (the callers keep it
+    // current) and stays current: jet_apply and balance() update it
+    std::vector<uint32_t> hbw((size_t)k);
+    uint64_t best_ov = 0;
+    long long best_cut = 0;
+    bool part_is_best = false;  // best[] is stale while the current partition is the best one
+    unsigned moved = 0;
     int since = 0;
-    for (int it = 0; it < kn.jet_iters; ++it) {
-        A.it = it;
-        A.ks_tie = stream_key(kn.seed, TAG_JTIE, level, it);
-        {
+    for (int it = 0;; ++it) {
+        // cut of the partition left by the previous iteration (the input at it = 0)
+        KB_CUDA(cudaMemsetAsync(cut2, 0, sizeof(unsigned long long), s));
+        if (it < kn.jet_iters) {
+            A.it = it;
+            A.ks_tie = stream_key(kn.seed, TAG_JTIE, level, it);
             PhaseScope ps(ctx, "jet_choose", 12.0 * (double)g.m + 16.0 * n);
-            KB_CUDA(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned), s));
+            KB_CUDA(cudaMemsetAsync(ctr, 0, sizeof(unsigned), s));
             jet_choose<<<grid_for(n), kThreads, 0, s>>>(A);
             KB_LAUNCH();
             jet_choose_wide<<<wblocks, kThreads, 0, s>>>(A, counters);
             KB_LAUNCH();
+        } else {
+            block_weights_and_cut(ctx, g, part, k, bw, cut2);
+        }
+        unsigned long long c2 = 0;
+        KB_CUDA(cudaMemcpyAsync(&c2, cut2, sizeof(c2), cudaMemcpyDeviceToHost, s));
+        KB_CUDA(cudaMemcpyAsync(hbw.data(), bw, sizeof(uint32_t) * (size_t)k, cudaMemcpyDeviceToHost, s));
+        KB_CUDA(cudaStreamSynchronize(s));
+        uint64_t ov = 0;
+        for (uint32_t x : hbw) if (x > bound) ov += x - bound;
+        const long long cut = (long long)(c2 / 2);
+        if (it == 0 || ov < best_ov || (ov == best_ov && cut < best_cut)) {
+            best_ov = ov;
+            best_cut = cut;
+            part_is_best = true;
+            since = 0;
+        } else {
+            ++since;
+        }
+        if (it > 0 && (moved == 0 || since >= kn.jet_patience)) break;
+        if (it == kn.jet_iters) break;
+        if (part_is_best) {
+            KB_CUDA(cudaMemcpyAsync(best, part, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+            KB_CUDA(cudaMemcpyAsync(best_bw, bw, sizeof(uint32_t) * (size_t)k, cudaMemcpyDeviceToDevice, s));
+            part_is_best = false;
         }
         {
             PhaseScope ps(ctx, "jet_afterburn", 0);
             jet_afterburn<<<grid_for(n), kThreads, 0, s>>>(A, keep);
             KB_LAUNCH();
+            KB_CUDA(cudaMemsetAsync(ctr + 1, 0, sizeof(unsigned), s));
             jet_apply<<<grid_for(n), kThreads, 0, s>>>(n, it, keep, dest, g.vwgt, part, moved_at, bw, ctr + 1);
             KB_LAUNCH();
         }
-        unsigned moved = 0;
         KB_CUDA(cudaMemcpyAsync(&moved, ctr + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-        // block weights after the moves decide whether the balance needs repair
-        block_weights_and_cut(ctx, g, part, k, bw, nullptr);
         KB_CUDA(cudaMemcpyAsync(hbw.data(), bw, sizeof(uint32_t) * (size_t)k, cudaMemcpyDeviceToHost, s));
         KB_CUDA(cudaStreamSynchronize(s));
         uint32_t mx = 0;
         for (uint32_t x : hbw) mx = std::max(mx, x);
         if (mx > bound) balance(ctx, g, kn, level, bound, part, bw);
-        uint64_t ov;
-        long long cut;
-        measure(ov, cut);
-        if (ov < best_ov || (ov == best_ov && cut < best_cut)) {
-            best_ov = ov;
-            best_cut = cut;
-            KB_CUDA(cudaMemcpyAsync(best, part, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
-            since = 0;
-        } else {
-            ++since;
-        }
-        if (moved == 0 || since >= kn.jet_patience) break;
     }
-    KB_CUDA(cudaMemcpyAsync(part, best, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
-    block_weights_and_cut(ctx, g, part, k, bw, nullptr);
+    if (!part_is_best) {
+        KB_CUDA(cudaMemcpyAsync(part, best, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
+        KB_CUDA(cudaMemcpyAsync(bw, best_bw, sizeof(uint32_t) * (size_t)k, cudaMemcpyDeviceToDevice, s));
+    }
     ctx.scratch.release(mk);
 }
 
