@@ -14,13 +14,23 @@
 //     on every level on the way up;
 //   * `reps` repetitions of the whole recursion keep the smallest cut.
 // The graph is small (a few thousand nodes), so this stays on the host.
+// Repetitions, the two halves of a bisection and the tries of a bisection
+// are independent (their hash streams are keyed by position, not by order
+// of execution) and run as tasks of one process-wide thread pool; results
+// are reduced in index order, so they do not depend on the thread count.
 #include "initial_partitioning.h"
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cmath>
+#include <condition_variable>
 #include <cstdint>
 #include <cstring>
+#include <deque>
+#include <functional>
+#include <memory>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -29,6 +39,107 @@
 namespace kb {
 
 namespace {
+
+// Fork-join pool: run(count, f) calls f(0..count-1) on the caller and on
+// idle workers and returns when all calls are done; a waiting caller runs
+// queued work meanwhile, so nested run() calls cannot deadlock.
+class TaskPool {
+public:
+    static TaskPool& get() {
+        static TaskPool* pool = new TaskPool();  // never destroyed: workers may outlive static teardown
+        return *pool;
+    }
+
+    void run(int count, const std::function<void(int)>& f) {
+        if (count <= 0) return;
+        if (count == 1 || workers_ == 0) {
+            for (int i = 0; i < count; ++i) f(i);
+            return;
+        }
+        auto job = std::make_shared<Job>();
+        job->f = &f;
+        job->count = count;
+        int posted = 0;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            for (int i = 1; i < count && i <= workers_; ++i, ++posted) queue_.push_back(job);
+            queued_.store((int)queue_.size(), std::memory_order_release);
+        }
+        for (int i = 0; i < posted; ++i) cv_.notify_one();
+        work_on(*job);
+        while (job->done.load(std::memory_order_acquire) < count) {
+            if (!run_one()) std::this_thread::yield();
+        }
+    }
+
+private:
+    struct Job {
+        const std::function<void(int)>* f = nullptr;
+        int count = 0;
+        std::atomic<int> next{0}, done{0};
+    };
+
+    TaskPool() {
+        unsigned hw = std::thread::hardware_concurrency();
+        workers_ = (int)std::min(15u, hw > 1 ? hw - 1 : 0u);
+        for (int i = 0; i < workers_; ++i) std::thread([this] { loop(); }).detach();
+    }
+
+    static void work_on(Job& j) {
+        for (int i; (i = j.next.fetch_add(1, std::memory_order_relaxed)) < j.count;) {
+            (*j.f)(i);
+            j.done.fetch_add(1, std::memory_order_release);
+        }
+    }
+
+    bool run_one() {
+        if (queued_.load(std::memory_order_acquire) == 0) return false;
+        std::shared_ptr<Job> j;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            if (queue_.empty()) return false;
+            j = std::move(queue_.front());
+            queue_.pop_front();
+            queued_.store((int)queue_.size(), std::memory_order_release);
+        }
+        work_on(*j);
+        return true;
+    }
+
+    void loop() {
+        for (;;) {
+            // a short spin before sleeping: fork-join waves come in quick succession
+            for (int spin = 0; spin < 20000; ++spin) {
+                if (run_one()) spin = 0;
+                else std::this_thread::yield();
+            }
+            std::shared_ptr<Job> j;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [this] { return !queue_.empty(); });
+                j = std::move(queue_.front());
+                queue_.pop_front();
+                queued_.store((int)queue_.size(), std::memory_order_release);
+            }
+            work_on(*j);
+        }
+    }
+
+    int workers_ = 0;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<std::shared_ptr<Job>> queue_;
+    std::atomic<int> queued_{0};
+};
+
+// f(0..count-1), on the pool when par is set
+void for_each_index(int count, bool par, const std::function<void(int)>& f) {
+    if (par) {
+        TaskPool::get().run(count, f);
+    } else {
+        for (int i = 0; i < count; ++i) f(i);
+    }
+}
 
 struct HostGraph {
     int n = 0;
@@ -359,13 +470,14 @@ struct Bisector {
     const Knobs& kn;
 
     // tries on the coarsest graph of one bisection
-    std::vector<char> coarsest(const HostGraph& g, uint64_t t0, const Limits& lim, int bis_key) const {
-        std::vector<char> best(g.n, 1), side;
-        std::vector<long long> key(g.n, 0);
-        GainHeap heap(g.n);
-        long long best_cut = LLONG_MAX;
-        uint64_t best_ov = UINT64_MAX;
-        for (int t = 0; t < kn.ip_tries; ++t) {
+    std::vector<char> coarsest(const HostGraph& g, uint64_t t0, const Limits& lim, int bis_key, bool par) const {
+        struct Try {
+            std::vector<char> side;
+            uint64_t ov = 0;
+            long long cut = 0;
+        };
+        std::vector<Try> tries((size_t)std::max(kn.ip_tries, 0));
+        for_each_index(kn.ip_tries, par && g.n > 32, [&](int t) {
             const uint64_t ks = stream_key(kn.seed, TAG_IP, bis_key, t);
             int s0 = 0;
             uint32_t hmin = UINT32_MAX;
@@ -373,22 +485,25 @@ struct Bisector {
                 uint32_t h = hash32(ks, (uint32_t)v);
                 if (h < hmin) { hmin = h; s0 = v; }
             }
+            std::vector<long long> key(g.n, 0);
+            GainHeap heap(g.n);
+            Try& r = tries[t];
             int start = farthest(g, farthest(g, s0));
-            grow_region(g, start, t0, lim.maxw[0], side, key, heap);
-            long long c = fm_refine(g, side, lim, kn.ip_fm_passes, kn.ip_fm_stall, key, heap);
+            grow_region(g, start, t0, lim.maxw[0], r.side, key, heap);
+            r.cut = fm_refine(g, r.side, lim, kn.ip_fm_passes, kn.ip_fm_stall, key, heap);
             uint64_t w[2] = {0, 0};
-            for (int v = 0; v < g.n; ++v) w[(int)side[v]] += (uint64_t)g.vwgt[v];
-            uint64_t ov = lim.overload(w);
-            if (ov < best_ov || (ov == best_ov && c < best_cut)) {
-                best_ov = ov;
-                best_cut = c;
-                best = side;
-            }
-        }
-        return best;
+            for (int v = 0; v < g.n; ++v) w[(int)r.side[v]] += (uint64_t)g.vwgt[v];
+            r.ov = lim.overload(w);
+        });
+        // the first try of the smallest (overload, cut)
+        int b = -1;
+        for (int t = 0; t < kn.ip_tries; ++t)
+            if (b < 0 || tries[t].ov < tries[b].ov || (tries[t].ov == tries[b].ov && tries[t].cut < tries[b].cut))
+                b = t;
+        return b < 0 ? std::vector<char>(g.n, 1) : std::move(tries[b].side);
     }
 
-    std::vector<char> multilevel(const HostGraph& g, uint64_t t0, const Limits& lim, int bis_key) const {
+    std::vector<char> multilevel(const HostGraph& g, uint64_t t0, const Limits& lim, int bis_key, bool par) const {
         std::vector<HostGraph> levels;
         std::vector<std::vector<int>> maps;
         const uint64_t maxnode = (uint64_t)(1.5 * (double)g.weight() / 200.0);
@@ -403,7 +518,7 @@ struct Bisector {
             levels.push_back(std::move(c));
             cur = &levels.back();
         }
-        std::vector<char> side = coarsest(*cur, t0, lim, bis_key);
+        std::vector<char> side = coarsest(*cur, t0, lim, bis_key, par);
         for (int l = (int)levels.size() - 1; l >= 0; --l) {
             const HostGraph& fine = l == 0 ? g : levels[l - 1];
             std::vector<char> fs(fine.n);
@@ -452,10 +567,10 @@ int levels_needed(int k) {
 
 // Recursion over the bisection tree.  A bisection's hash streams depend only
 // on its position in the tree (root 1, children 2i and 2i+1) and the
-// repetition, so the two halves are independent; large halves run on their
-// own host thread, with identical results to a sequential recursion.
+// repetition, so the two halves are independent and run as pool tasks when
+// par is set, with results identical to a sequential recursion.
 void recurse(const Knobs& kn, const HostGraph& g, const std::vector<int>& orig, int k, int offset, int rep,
-             uint32_t node, std::vector<int>& out, int spawn_depth) {
+             uint32_t node, std::vector<int>& out, bool par) {
     if (k == 1 || g.n == 0) {
         for (int v = 0; v < g.n; ++v) out[orig[v]] = offset;
         return;
@@ -469,32 +584,21 @@ void recurse(const Knobs& kn, const HostGraph& g, const std::vector<int>& orig, 
     eb = std::max(eb, std::min(eps, 0.01));
     Limits lim{{(uint64_t)((1.0 + eb) * (double)t0), (uint64_t)((1.0 + eb) * (double)t1)}};
     Bisector bis{kn};
-    std::vector<char> side = bis.multilevel(g, t0, lim, (int)(node * 64u + (uint32_t)rep));
+    std::vector<char> side = bis.multilevel(g, t0, lim, (int)(node * 64u + (uint32_t)rep), par);
     std::vector<int> lo, ro;
     HostGraph L = induced(g, orig, side, 0, lo);
     HostGraph R = induced(g, orig, side, 1, ro);
     side.clear();
     side.shrink_to_fit();
     // out[] entries written by the two halves are disjoint
-    if (spawn_depth > 0 && kl > 1 && kr > 1 && L.n > 64 && R.n > 64) {
-        std::thread left([&] { recurse(kn, L, lo, kl, offset, rep, 2u * node, out, spawn_depth - 1); });
-        recurse(kn, R, ro, kr, offset + kl, rep, 2u * node + 1u, out, spawn_depth - 1);
-        left.join();
-    } else {
-        recurse(kn, L, lo, kl, offset, rep, 2u * node, out, 0);
-        recurse(kn, R, ro, kr, offset + kl, rep, 2u * node + 1u, out, 0);
-    }
+    const bool fork = par && kl > 1 && kr > 1 && L.n > 64 && R.n > 64;
+    for_each_index(2, fork, [&](int h) {
+        if (h == 0) recurse(kn, L, lo, kl, offset, rep, 2u * node, out, par);
+        else recurse(kn, R, ro, kr, offset + kl, rep, 2u * node + 1u, out, par);
+    });
 }
 
 thread_local int t_spawn_limit = -1;
-
-int spawn_depth_for_host() {
-    if (t_spawn_limit >= 0) return t_spawn_limit;
-    unsigned t = std::thread::hardware_concurrency();
-    int d = 0;
-    while (d < 6 && (2u << d) <= t) ++d;
-    return d;
-}
 
 }  // namespace
 
@@ -510,21 +614,25 @@ void initial_partition(int n, const int* xadj, const int* adjncy, const int* adj
     g.vwgt.assign(vwgt, vwgt + n);
     std::vector<int> orig(n);
     for (int v = 0; v < n; ++v) orig[v] = v;
-    std::vector<int> cand(n);
-    long long best = LLONG_MAX;
-    const int depth = spawn_depth_for_host();
-    for (int rep = 0; rep < kn.ip_reps; ++rep) {
-        recurse(kn, g, orig, kn.k, 0, rep, 1u, cand, depth);
-        long long c = 0;
+    const bool par = t_spawn_limit != 0 && std::thread::hardware_concurrency() > 1;
+    const int reps = std::max(kn.ip_reps, 0);
+    std::vector<std::vector<int>> cand((size_t)reps);
+    std::vector<long long> cut((size_t)reps, 0);
+    for_each_index(reps, par, [&](int rep) {
+        cand[rep].assign(n, 0);
+        recurse(kn, g, orig, kn.k, 0, rep, 1u, cand[rep], par);
+        const std::vector<int>& c = cand[rep];
+        long long x = 0;
         for (int v = 0; v < n; ++v)
             for (int e = xadj[v]; e < xadj[v + 1]; ++e)
-                if (cand[v] != cand[adjncy[e]]) c += adjwgt[e];
-        c /= 2;
-        if (c < best) {
-            best = c;
-            std::copy(cand.begin(), cand.end(), part);
-        }
-    }
+                if (c[v] != c[adjncy[e]]) x += adjwgt[e];
+        cut[rep] = x / 2;
+    });
+    // the first repetition of the smallest cut
+    int b = -1;
+    for (int rep = 0; rep < reps; ++rep)
+        if (b < 0 || cut[rep] < cut[b]) b = rep;
+    if (b >= 0) std::copy(cand[b].begin(), cand[b].end(), part);
 }
 
 }  // namespace kb

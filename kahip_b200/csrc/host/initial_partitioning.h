@@ -10,9 +10,9 @@ namespace kb {
 void initial_partition(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
                        const Knobs& kn, int* part);
 
-// Caps, for calls made by the calling thread, the depth of the bisection
-// tree down to which the two halves run on separate host threads (0 = no
-// extra threads; -1 = derived from the host's core count).  Results do not
+// For calls made by the calling thread: 0 runs the partitioner on that
+// thread alone; any other value (default -1) lets repetitions, bisection
+// halves and tries run on the process-wide host thread pool.  Results do not
 // depend on it.
 void set_ip_thread_limit(int depth);
 
