@@ -122,6 +122,32 @@ int kb200_kaffpa_device(int n, const int* d_vwgt, const int* d_xadj, const int* 
 int kb200_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
                        const kb200_knobs* kn, long long* edgecut, int* part, kb200_stats* stats);
 
+/* KaFFPaE combine operator (replaces population::combine,
+ * lib/parallel_mh/population.cpp:189-250, which has no C entry point in the
+ * reference): part_a and part_b are two partitions of the graph into kn->k
+ * blocks.  The better one by (overload against the final bound, cut; part_a
+ * on ties) becomes the initial partition of a multilevel run whose
+ * coarsening never joins nodes that either parent separates; part[] out is
+ * never worse than that parent. */
+int kb200_kaffpa_combine(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+                         const kb200_knobs* kn, const int* part_a, const int* part_b, long long* edgecut, int* part,
+                         kb200_stats* stats);
+
+/* KaFFPaE-style evolutionary partitioning on one device (replaces the
+ * kaffpaE program's loop, lib/parallel_mh/parallel_mh_async.cpp:49-…, with
+ * population.cpp:120-173 insertion and :358-369 tournament selection; the
+ * reference has no C entry point for it).  `population` members come from
+ * the plain partitioner with seeds kn->seed + i; each of `generations`
+ * rounds combines `per_generation` tournament-selected pairs (deterministic
+ * hash draws; every selection of a round reads the population at the
+ * round's start) with kb200_kaffpa_combine's operator and inserts the
+ * offspring in order.  part[]/edgecut: the best member by (overload, cut);
+ * history[generations + 1] (optional): the best cut after the initial
+ * population and after every round. */
+int kb200_kaffpae(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+                  const kb200_knobs* kn, int population, int generations, int per_generation, long long* edgecut,
+                  int* part, long long* history);
+
 /* Same with device buffers (explicit weights), like kb200_kaffpa_device. */
 int kb200_kaffpa_device_knobs(int n, const int* d_vwgt, const int* d_xadj, const int* d_adjcwgt,
                               const int* d_adjncy, const kb200_knobs* kn, long long* edgecut, int* d_part,

@@ -23,6 +23,7 @@
 #include "knobs.h"
 #include "learned.cuh"
 #include "match.cuh"
+#include "evolve.cuh"
 #include "partitioner.cuh"
 #include "prims.cuh"
 
@@ -202,7 +203,8 @@ int check_knobs(const kb200_knobs* kn) {
 }
 
 int run_host_in(Ctx& ctx, int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
-                const Knobs& kn, long long* edgecut, int* part, kb200_stats* st, clk::time_point t0);
+                const Knobs& kn, long long* edgecut, int* part, kb200_stats* st, clk::time_point t0,
+                const int* parent_a = nullptr, const int* parent_b = nullptr);
 
 int run_host(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy, const Knobs& kn,
              long long* edgecut, int* part, kb200_stats* st) {
@@ -216,20 +218,34 @@ int run_host(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const 
     return run_host_in(*lease.ctx, n, vwgt, xadj, adjcwgt, adjncy, kn, edgecut, part, st, t0);
 }
 
-// The body of a host-buffer call on a leased context (input already validated).
+// The body of a host-buffer call on a leased context (input already
+// validated).  With parent_a / parent_b (host, n each) it is a combine.
 int run_host_in(Ctx& ctx, int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
-                const Knobs& kn, long long* edgecut, int* part, kb200_stats* st, clk::time_point t0) {
+                const Knobs& kn, long long* edgecut, int* part, kb200_stats* st, clk::time_point t0,
+                const int* parent_a, const int* parent_b) {
     const long long m = xadj[n];
+    const bool comb = parent_a != nullptr;
     for (int attempt = 0;; ++attempt) {
         try {
-            reserve_for(ctx, n, m, true, attempt == 0 ? 1.0 : 2.0 * attempt);
+            // a combine also holds both parents per level and one filtered level graph
+            reserve_for(ctx, n, m, true, (attempt == 0 ? 1.0 : 2.0 * attempt) * (comb ? 1.5 : 1.0));
             begin_stats(ctx, st);
             auto th = clk::now();
             Upload up = upload(ctx, n, xadj, adjncy, adjcwgt, vwgt);
             check_uploaded(ctx, up.g);
+            int* dpar = nullptr;
+            if (comb) {
+                dpar = ctx.hier.alloc<int>(2 * (size_t)std::max(n, 1));
+                if (n) {
+                    KB_CUDA(cudaMemcpyAsync(dpar, parent_a, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, ctx.stream));
+                    KB_CUDA(cudaMemcpyAsync(dpar + n, parent_b, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice,
+                                            ctx.stream));
+                }
+            }
             double ms_h2d = ms_since(th);
             long long cut = 0;
-            int r = partition(ctx, up.g, kn, up.part, &cut, st);
+            int r = comb ? combine(ctx, up.g, kn, dpar, dpar + n, up.part, &cut, st)
+                         : partition(ctx, up.g, kn, up.part, &cut, st);
             auto td = clk::now();
             if (n) KB_CUDA(cudaMemcpyAsync(part, up.part, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, ctx.stream));
             KB_CUDA(cudaStreamSynchronize(ctx.stream));
@@ -292,6 +308,68 @@ int kb200_kaffpa(int n, const int* vwgt, const int* xadj, const int* adjcwgt, co
         Knobs kn;
         derive_knobs(n, vwgt, nparts, imbalance, seed, mode, kn);
         return run_host(n, vwgt, xadj, adjcwgt, adjncy, kn, edgecut, part, stats);
+    });
+}
+
+int kb200_kaffpa_combine(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+                         const kb200_knobs* kn, const int* part_a, const int* part_b, long long* edgecut, int* part,
+                         kb200_stats* stats) {
+    g_last_error.clear();
+    return guarded([&]() -> int {
+        auto t0 = clk::now();
+        int rc = validate(n, xadj, adjncy, adjcwgt, vwgt);
+        if (rc || (rc = check_knobs(kn))) return rc;
+        if (kn->coarsening < 0 || kn->coarsening > 2) return fail(KB_ERR_INVALID_INPUT, "unknown coarsening");
+        if (!edgecut || (n > 0 && (!part || !part_a || !part_b)))
+            return fail(KB_ERR_INVALID_INPUT, "edgecut/part/parents is NULL");
+        for (int v = 0; v < n; ++v)
+            if (part_a[v] < 0 || part_a[v] >= kn->k || part_b[v] < 0 || part_b[v] >= kn->k)
+                return fail(KB_ERR_INVALID_INPUT, "parent block id out of range");
+        int dev;
+        if ((rc = current_device(&dev))) return rc;
+        Lease lease(dev);
+        return run_host_in(*lease.ctx, n, vwgt, xadj, adjcwgt, adjncy, *kn, edgecut, part, stats, t0, part_a,
+                           part_b);
+    });
+}
+
+int kb200_kaffpae(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+                  const kb200_knobs* kn, int population, int generations, int per_generation, long long* edgecut,
+                  int* part, long long* history) {
+    g_last_error.clear();
+    return guarded([&]() -> int {
+        int rc = validate(n, xadj, adjncy, adjcwgt, vwgt);
+        if (rc || (rc = check_knobs(kn))) return rc;
+        if (population < 1 || generations < 0 || per_generation < 1)
+            return fail(KB_ERR_INVALID_INPUT, "population >= 1, generations >= 0, per_generation >= 1 required");
+        if (!edgecut || (n > 0 && !part)) return fail(KB_ERR_INVALID_INPUT, "edgecut/part is NULL");
+        int dev;
+        if ((rc = current_device(&dev))) return rc;
+        Lease lease(dev);
+        Ctx& ctx = *lease.ctx;
+        const long long m = xadj[n];
+        for (int attempt = 0;; ++attempt) {
+            try {
+                reserve_for(ctx, n, m, true, (attempt == 0 ? 1.0 : 2.0 * attempt) * 1.5);
+                ctx.timing = false;
+                ctx.reset_stats();
+                Upload up = upload(ctx, n, xadj, adjncy, adjcwgt, vwgt);
+                check_uploaded(ctx, up.g);
+                long long cut = 0;
+                int r = kaffpae(ctx, up.g, *kn, population, generations, per_generation, up.part, &cut, history);
+                if (n) KB_CUDA(cudaMemcpyAsync(part, up.part, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, ctx.stream));
+                KB_CUDA(cudaStreamSynchronize(ctx.stream));
+                *edgecut = cut;
+                return r;
+            } catch (const CudaError& e) {
+                if (e.code == cudaErrorMemoryAllocation && attempt < 2 &&
+                    std::string(e.what()).find("arena exhausted") != std::string::npos) {
+                    (void)cudaGetLastError();
+                    continue;
+                }
+                throw;
+            }
+        }
     });
 }
 

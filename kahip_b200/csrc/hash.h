@@ -26,6 +26,7 @@ enum HashTag : int {
     TAG_IPM = 10,   // initial partitioning: matching order
     TAG_MATCH = 11, // heavy-edge matching: pair hash
     TAG_JTIE = 12,  // Jet refinement: destination tie-break
+    TAG_EVO = 13,   // evolutionary partitioning: tournament draws
 };
 
 // splitmix64 output function (Steele, Lea & Flood, OOPSLA 2014).

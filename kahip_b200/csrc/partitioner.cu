@@ -9,6 +9,7 @@
 #include <cstring>
 #include <stdexcept>
 
+#include "combine.cuh"
 #include "contract.cuh"
 #include "host/initial_partitioning.h"
 #include "jet.cuh"
@@ -143,12 +144,17 @@ void reserve_for(Ctx& ctx, int n, long long m, bool copy_input, double factor) {
     ctx.scratch.reserve((size_t)(scr * factor));
 }
 
+// p1/p2 (device, n each, optional): the parents of a combine, p1 the better
+// one; the coarsening then runs on the edges inside both parents' blocks and
+// the coarsest graph takes p1 instead of an initial partitioning.
 static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_part, long long* edgecut,
-                          kb200_stats* st) {
+                          kb200_stats* st, const int* p1 = nullptr, const int* p2 = nullptr) {
     const int k = kn.k;
     const bool collect = st && st->collect_level_cuts;
+    const bool combine = p1 != nullptr;
     cudaStream_t s = ctx.stream;
     std::vector<Level> lv;
+    std::vector<const int*> P1{p1}, P2{p2};
     lv.push_back(Level{g0, nullptr, d_part});
     degree_stats(ctx, lv[0].g);
     // learned rating: the model's parameters, once per call
@@ -167,30 +173,42 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
             lv[L].cmap = ctx.hier.alloc<int>((size_t)f.n);
             const size_t mk = ctx.scratch.mark();
             int* label = ctx.scratch.alloc<int>((size_t)f.n);
+            // a combine clusters on the edges inside both parents' blocks and
+            // bundles no isolated nodes (they may lie in different blocks)
+            DevGraph filtered;
+            if (combine) filter_by_parents(ctx, f, P1[L], P2[L], filtered);
+            const DevGraph& cg = combine ? filtered : f;
             bool lp = kn.coarsening == 0;
             if (!lp) {
                 if (kn.coarsening == 2 && d_model && (kn.rating_levels <= 0 || L < kn.rating_levels)) {
-                    uint32_t* rating = ctx.scratch.alloc<uint32_t>((size_t)std::max<long long>(f.m, 1));
-                    rating_infer(ctx, f, d_model, nullptr, rating, true);
-                    hem_match(ctx, f, kn, L, rating, label);
+                    uint32_t* rating = ctx.scratch.alloc<uint32_t>((size_t)std::max<long long>(cg.m, 1));
+                    rating_infer(ctx, cg, d_model, nullptr, rating, true);
+                    hem_match(ctx, cg, kn, L, rating, label);
                 } else {
-                    hem_match(ctx, f, kn, L, nullptr, label);
+                    hem_match(ctx, cg, kn, L, nullptr, label);
                 }
-                bundle_isolated(ctx, f, kn.max_vertex_weight + 1u, label);
+                if (!combine) bundle_isolated(ctx, cg, kn.max_vertex_weight + 1u, label);
                 // a matching that removes less than 40 % of the nodes
                 // (stars, skewed degrees) gives way to LP clustering
                 const long long nc = count_leaders(ctx, f.n, label);
                 lp = 5 * nc > 3 * (long long)f.n;
             }
             if (lp) {
-                lp_cluster(ctx, f, kn, L, label);
-                bundle_isolated(ctx, f, kn.cluster_bound, label);
+                lp_cluster(ctx, cg, kn, L, label);
+                if (!combine) bundle_isolated(ctx, cg, kn.cluster_bound, label);
             }
             Level c;
             int *cx, *ca, *cw, *cv;
             contract(ctx, f, label, lv[L].cmap, c.g, &cx, &ca, &cw, &cv);
             ctx.scratch.release(mk);
             degree_stats(ctx, c.g);
+            if (combine) {
+                int* q1 = ctx.hier.alloc<int>((size_t)std::max(c.g.n, 1));
+                int* q2 = ctx.hier.alloc<int>((size_t)std::max(c.g.n, 1));
+                parents_to_coarse(ctx, f.n, lv[L].cmap, P1[L], P2[L], q1, q2);
+                P1.push_back(q1);
+                P2.push_back(q2);
+            }
             const int nf = f.n, nc = c.g.n;
             lv.push_back(c);
             ++L;
@@ -206,7 +224,16 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
     auto t1 = clk::now();
     for (int l = 1; l <= L; ++l) lv[l].part = ctx.hier.alloc<int>((size_t)std::max(lv[l].g.n, 1));
     long long initial_cut = 0;
-    {
+    if (combine) {
+        // the better parent, carried down the hierarchy
+        const DevGraph& c = lv[L].g;
+        if (c.n)
+            KB_CUDA(cudaMemcpyAsync(lv[L].part, P1[L], sizeof(int) * (size_t)c.n, cudaMemcpyDeviceToDevice, s));
+        const size_t mk = ctx.scratch.mark();
+        uint32_t* tbw = ctx.scratch.alloc<uint32_t>((size_t)k);
+        initial_cut = read_cut(ctx, c, lv[L].part, k, tbw);
+        ctx.scratch.release(mk);
+    } else {
         const DevGraph& c = lv[L].g;
         std::vector<int> hx((size_t)c.n + 1), ha((size_t)c.m), hw((size_t)c.m), hv((size_t)c.n), hp((size_t)c.n);
         KB_CUDA(cudaMemcpyAsync(hx.data(), c.xadj, sizeof(int) * hx.size(), cudaMemcpyDeviceToHost, s));
@@ -270,6 +297,46 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
         st->ms_uncoarsen = ms_uncoarsen;
     }
     return balanced ? KB_OK : KB_WARN_IMBALANCED;
+}
+
+void partition_quality(Ctx& ctx, const DevGraph& g, const int* part, int k, uint32_t bound, uint64_t* ov,
+                       long long* cut) {
+    const size_t mk = ctx.scratch.mark();
+    uint32_t* bw = ctx.scratch.alloc<uint32_t>((size_t)k);
+    *cut = read_cut(ctx, g, part, k, bw);
+    std::vector<uint32_t> h((size_t)k);
+    KB_CUDA(cudaMemcpyAsync(h.data(), bw, sizeof(uint32_t) * (size_t)k, cudaMemcpyDeviceToHost, ctx.stream));
+    KB_CUDA(cudaStreamSynchronize(ctx.stream));
+    ctx.scratch.release(mk);
+    *ov = 0;
+    for (uint32_t x : h) if (x > bound) *ov += x - bound;
+}
+
+int combine(Ctx& ctx, const DevGraph& g0, const Knobs& kn, const int* pa, const int* pb, int* d_part,
+            long long* edgecut, kb200_stats* st) {
+    if (st) st->rating_fallback_used = 0;
+    uint64_t ova, ovb;
+    long long ca, cb;
+    partition_quality(ctx, g0, pa, kn.k, kn.final_bound, &ova, &ca);
+    partition_quality(ctx, g0, pb, kn.k, kn.final_bound, &ovb, &cb);
+    const bool b_first = ovb < ova || (ovb == ova && cb < ca);
+    const int* p1 = b_first ? pb : pa;
+    const int* p2 = b_first ? pa : pb;
+    const uint64_t ov1 = b_first ? ovb : ova;
+    const long long c1 = b_first ? cb : ca;
+    int r = partition_once(ctx, g0, kn, d_part, edgecut, st, p1, p2);
+    uint64_t ovr;
+    long long cr;
+    partition_quality(ctx, g0, d_part, kn.k, kn.final_bound, &ovr, &cr);
+    if (ov1 < ovr || (ov1 == ovr && c1 < cr)) {
+        // never worse than the better parent
+        if (g0.n) KB_CUDA(cudaMemcpyAsync(d_part, p1, sizeof(int) * (size_t)g0.n, cudaMemcpyDeviceToDevice, ctx.stream));
+        KB_CUDA(cudaStreamSynchronize(ctx.stream));
+        *edgecut = c1;
+        r = ov1 == 0 ? KB_OK : KB_WARN_IMBALANCED;
+        if (st) st->balanced = ov1 == 0 ? 1 : 0;
+    }
+    return r;
 }
 
 int partition(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_part, long long* edgecut,

@@ -16,4 +16,15 @@ void reserve_for(Ctx& ctx, int n, long long m, bool copy_input, double factor);
 int partition(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_part, long long* edgecut,
               kb200_stats* st);
 
+// (overload against bound, cut) of the device partition part of g.
+void partition_quality(Ctx& ctx, const DevGraph& g, const int* part, int k, uint32_t bound, uint64_t* ov,
+                       long long* cut);
+
+// KaFFPaE combine of the device partitions pa and pb of g0 (population.cpp:
+// 189-250): the better parent by (overload, cut) (pa on ties) is the initial
+// partition of a coarsening that keeps both parents' blocks apart; the
+// result (d_part) is never worse than that parent.  Same returns as partition.
+int combine(Ctx& ctx, const DevGraph& g0, const Knobs& kn, const int* pa, const int* pb, int* d_part,
+            long long* edgecut, kb200_stats* st);
+
 }  // namespace kb

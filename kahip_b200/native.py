@@ -97,7 +97,8 @@ class BatchReport(ctypes.Structure):
 
 EXPORTS = [
     # extended ABI (include/kahip_b200.h)
-    "kb200_derive_knobs", "kb200_kaffpa", "kb200_kaffpa_device", "kb200_kaffpa_knobs",
+    "kb200_derive_knobs", "kb200_kaffpa", "kb200_kaffpa_device", "kb200_kaffpa_knobs", "kb200_kaffpa_combine",
+    "kb200_kaffpae",
     "kb200_kaffpa_device_knobs", "kb200_kaffpa_batch", "kb200_kaffpa_population", "kb200_hem_match",
     "kb200_rating_infer", "kb200_rating_train", "kb200_rating_grad",
     "kb200_read_metis", "kb200_read_bgf", "kb200_write_partition", "kb200_free", "kb200_io_error",
@@ -126,6 +127,9 @@ def lib():
                                          ctypes.POINTER(Stats)]
         L.kb200_kaffpa_device_knobs.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), c_ll_p, vp, vp,
                                                 ctypes.POINTER(Stats)]
+        L.kb200_kaffpa_combine.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), vp, vp, c_ll_p, vp,
+                                           ctypes.POINTER(Stats)]
+        L.kb200_kaffpae.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, i, i, c_ll_p, vp, vp]
         L.kb200_hem_match.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, vp, vp]
         L.kb200_rating_infer.argtypes = [i, vp, vp, vp, vp, vp, i, vp, vp]
         L.kb200_rating_train.argtypes = [ctypes.POINTER(TrainGraph), i, i, ctypes.c_float, vp, vp]
@@ -215,6 +219,40 @@ def kaffpa_knobs(xadj, adjncy, kn: Knobs, vwgt=None, adjwgt=None, stats: Stats |
                                   ctypes.byref(cut), _ptr(part), ctypes.byref(stats) if stats else None)
     _check(rc)
     return rc, cut.value, part
+
+
+def kaffpa_combine(g: dict, kn: Knobs, part_a, part_b, stats: Stats | None = None, unit_weights=False):
+    """KaFFPaE combine of two partitions of g (kb200_kaffpa_combine).
+    Returns (status, edgecut, part)."""
+    n = g["n"]
+    xadj, adjncy = _i32(g["xadj"]), _i32(g["adjncy"])
+    vwgt = None if unit_weights else _i32(g["vwgt"])
+    adjwgt = None if unit_weights else _i32(g["adjwgt"])
+    pa = np.ascontiguousarray(part_a, dtype=np.int32)
+    pb = np.ascontiguousarray(part_b, dtype=np.int32)
+    part = np.zeros(max(n, 0), np.int32)
+    cut = ctypes.c_longlong(-1)
+    rc = lib().kb200_kaffpa_combine(n, _ptr(vwgt), _ptr(xadj), _ptr(adjwgt), _ptr(adjncy), ctypes.byref(kn),
+                                    _ptr(pa), _ptr(pb), ctypes.byref(cut), _ptr(part),
+                                    ctypes.byref(stats) if stats else None)
+    _check(rc)
+    return rc, cut.value, part
+
+
+def kaffpae(g: dict, kn: Knobs, population: int, generations: int, per_generation: int, unit_weights=False):
+    """KaFFPaE-style evolution on the device (kb200_kaffpae).
+    Returns (status, edgecut, part, history)."""
+    n = g["n"]
+    xadj, adjncy = _i32(g["xadj"]), _i32(g["adjncy"])
+    vwgt = None if unit_weights else _i32(g["vwgt"])
+    adjwgt = None if unit_weights else _i32(g["adjwgt"])
+    part = np.zeros(max(n, 0), np.int32)
+    hist = np.zeros(max(generations, 0) + 1, np.int64)
+    cut = ctypes.c_longlong(-1)
+    rc = lib().kb200_kaffpae(n, _ptr(vwgt), _ptr(xadj), _ptr(adjwgt), _ptr(adjncy), ctypes.byref(kn), population,
+                             generations, per_generation, ctypes.byref(cut), _ptr(part), hist.ctypes.data)
+    _check(rc)
+    return rc, cut.value, part, hist
 
 
 def hem_match(g: dict, kn: Knobs, level=0, rating=None) -> np.ndarray:

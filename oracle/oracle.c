@@ -13,7 +13,8 @@
 
 enum {
     TAG_CSUB = 1, TAG_CTIE = 2, TAG_RSUB = 3, TAG_RTIE = 4, TAG_RPRIO = 5,
-    TAG_BTIE = 6, TAG_BCLS = 7, TAG_BPRIO = 8, TAG_IP = 9, TAG_IPM = 10, TAG_MATCH = 11, TAG_JTIE = 12
+    TAG_BTIE = 6, TAG_BCLS = 7, TAG_BPRIO = 8, TAG_IP = 9, TAG_IPM = 10, TAG_MATCH = 11, TAG_JTIE = 12,
+    TAG_EVO = 13
 };
 
 #define BAL_CLASSES 256
@@ -1335,11 +1336,55 @@ int or_kaffpa(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const
     return or_kaffpa_knobs(n, vwgt, xadj, adjcwgt, adjncy, &kn, edgecut, part, stats);
 }
 
-int or_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
-                    const or_knobs* knobs, long long* edgecut, int* part, or_stats* stats) {
+/* The edges of f whose ends lie in the same block of both parents; the
+ * clusterings of a combine run only on these (size_constraint_label_
+ * propagation.cpp:175-178: graph_allready_partitioned / combine). */
+static void parents_filter(const or_graph* f, const int* p1, const int* p2, or_graph* out, int** fx, int** fa,
+                           int** fw) {
+    const int n = f->n, m = f->xadj[n];
+    *fx = xmalloc(sizeof(int) * (size_t)(n + 1));
+    *fa = xmalloc(sizeof(int) * (size_t)(m ? m : 1));
+    *fw = xmalloc(sizeof(int) * (size_t)(m ? m : 1));
+    int c = 0;
+    (*fx)[0] = 0;
+    for (int v = 0; v < n; ++v) {
+        for (int e = f->xadj[v]; e < f->xadj[v + 1]; ++e) {
+            const int u = f->adjncy[e];
+            if (p1[u] != p1[v] || p2[u] != p2[v]) continue;
+            (*fa)[c] = u;
+            (*fw)[c] = f->adjwgt[e];
+            ++c;
+        }
+        (*fx)[v + 1] = c;
+    }
+    out->n = n; out->xadj = *fx; out->adjncy = *fa; out->adjwgt = *fw; out->vwgt = f->vwgt;
+}
+
+/* (overload against bound, cut) of a partition of g */
+static void part_quality(const or_graph* g, const int* part, int k, uint32_t bound, uint64_t* ov, long long* cut) {
+    uint32_t* bw = xcalloc((size_t)k, sizeof(uint32_t));
+    or_block_weights(g, part, k, bw);
+    *ov = overload_of(bw, k, bound);
+    *cut = or_edge_cut(g, part);
+    free(bw);
+}
+
+/* The multilevel driver.  With parents (p1 the better partition, p2 the
+ * other) it is the KaFFPaE combine: coarsening never joins nodes that lie in
+ * different blocks of either parent, the coarsest graph takes p1 instead of
+ * an initial partitioning, and a result worse than p1 by (overload, cut) is
+ * replaced by p1 (population.cpp:189-250). */
+static int kaffpa_core(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+                       const or_knobs* knobs, const int* p1_in, const int* p2_in, long long* edgecut, int* part,
+                       or_stats* stats) {
     if (n < 0 || !knobs || knobs->k < 1 || !xadj || (n > 0 && !adjncy)) return -1;
     if (knobs->coarsening < 0 || knobs->coarsening > 1 || knobs->refinement < 0 || knobs->refinement > 1) return -1;
     const int nparts = knobs->k;
+    const int combine = p1_in != NULL;
+    int* P1[64];
+    int* P2[64];
+    memset(P1, 0, sizeof(P1));
+    memset(P2, 0, sizeof(P2));
     const int m = xadj[n];
     int* vw = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
     int* ew = xmalloc(sizeof(int) * (size_t)(m ? m : 1));
@@ -1357,21 +1402,36 @@ int or_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt,
     while (L + 1 < kn.max_levels && lv[L].g.n > 0) {
         or_graph* f = &lv[L].g;
         int* label = xmalloc(sizeof(int) * (size_t)f->n);
+        /* a combine clusters on the edges inside both parents' blocks and
+         * never bundles isolated nodes (they may lie in different blocks) */
+        or_graph flt;
+        int *fx = NULL, *fa = NULL, *fw = NULL;
+        if (combine) {
+            if (L == 0) {
+                P1[0] = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+                P2[0] = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+                memcpy(P1[0], p1_in, sizeof(int) * (size_t)n);
+                memcpy(P2[0], p2_in, sizeof(int) * (size_t)n);
+            }
+            parents_filter(f, P1[L], P2[L], &flt, &fx, &fa, &fw);
+        }
+        const or_graph* cg = combine ? &flt : f;
         if (kn.coarsening == 1) {
-            or_hem_match(f, &kn, L, NULL, label);
-            or_bundle_isolated(f, kn.max_vertex_weight + 1u, label);
+            or_hem_match(cg, &kn, L, NULL, label);
+            if (!combine) or_bundle_isolated(cg, kn.max_vertex_weight + 1u, label);
             /* a matching that removes less than 40 % of the nodes (stars,
              * skewed degrees) gives way to LP clustering for this level */
             long long nc = 0;
             for (int v = 0; v < f->n; ++v) nc += label[v] == v;
             if (5 * nc > 3 * (long long)f->n) {
-                or_lp_cluster(f, &kn, L, label);
-                or_bundle_isolated(f, kn.cluster_bound, label);
+                or_lp_cluster(cg, &kn, L, label);
+                if (!combine) or_bundle_isolated(cg, kn.cluster_bound, label);
             }
         } else {
-            or_lp_cluster(f, &kn, L, label);
-            or_bundle_isolated(f, kn.cluster_bound, label);
+            or_lp_cluster(cg, &kn, L, label);
+            if (!combine) or_bundle_isolated(cg, kn.cluster_bound, label);
         }
+        free(fx); free(fa); free(fw);
         or_level* c = &lv[L + 1];
         lv[L].cmap = xmalloc(sizeof(int) * (size_t)f->n);
         c->xadj = xmalloc(sizeof(int) * (size_t)(f->n + 1));
@@ -1382,12 +1442,29 @@ int or_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt,
         int nc = or_contract(f, label, lv[L].cmap, c->xadj, c->adjncy, c->adjwgt, c->vwgt);
         free(label);
         c->g.n = nc; c->g.xadj = c->xadj; c->g.adjncy = c->adjncy; c->g.adjwgt = c->adjwgt; c->g.vwgt = c->vwgt;
+        if (combine) {
+            /* every coarse node lies inside one block of each parent */
+            P1[L + 1] = xmalloc(sizeof(int) * (size_t)(nc ? nc : 1));
+            P2[L + 1] = xmalloc(sizeof(int) * (size_t)(nc ? nc : 1));
+            for (int v = 0; v < f->n; ++v) {
+                P1[L + 1][lv[L].cmap[v]] = P1[L][v];
+                P2[L + 1][lv[L].cmap[v]] = P2[L][v];
+            }
+        }
         ++L;
         if (!or_stop_continue(&kn, f->n, nc)) break;
     }
     /* initial partition of the coarsest graph */
     int* cpart = xmalloc(sizeof(int) * (size_t)(lv[L].g.n ? lv[L].g.n : 1));
-    or_initial_partition(&lv[L].g, &kn, cpart);
+    if (combine) {
+        if (L == 0 && !P1[0]) { /* no level was built (n == 0 or max_levels 1) */
+            P1[0] = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+            memcpy(P1[0], p1_in, sizeof(int) * (size_t)n);
+        }
+        memcpy(cpart, P1[L], sizeof(int) * (size_t)lv[L].g.n);
+    } else {
+        or_initial_partition(&lv[L].g, &kn, cpart);
+    }
     st.initial_cut = or_edge_cut(&lv[L].g, cpart);
     uint32_t* bw = xcalloc((size_t)nparts, sizeof(uint32_t));
     for (int l = L; l >= 0; --l) {
@@ -1420,6 +1497,18 @@ int or_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt,
     st.levels = L + 1;
     memcpy(part, cpart, sizeof(int) * (size_t)n);
     *edgecut = st.level_cut[0];
+    if (combine) {
+        uint64_t ov_r, ov_p;
+        long long cut_r, cut_p;
+        part_quality(&lv[0].g, part, nparts, kn.final_bound, &ov_r, &cut_r);
+        part_quality(&lv[0].g, p1_in, nparts, kn.final_bound, &ov_p, &cut_p);
+        if (ov_p < ov_r || (ov_p == ov_r && cut_p < cut_r)) {
+            memcpy(part, p1_in, sizeof(int) * (size_t)n);
+            *edgecut = cut_p;
+            st.balanced = ov_p == 0;
+        }
+    }
+    for (int l = 0; l < 64; ++l) { free(P1[l]); free(P2[l]); }
     if (stats) *stats = st;
     free(cpart);
     free(bw);
@@ -1430,4 +1519,150 @@ int or_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt,
     free(vw);
     free(ew);
     return 0;
+}
+
+int or_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+                    const or_knobs* knobs, long long* edgecut, int* part, or_stats* stats) {
+    return kaffpa_core(n, vwgt, xadj, adjcwgt, adjncy, knobs, NULL, NULL, edgecut, part, stats);
+}
+
+int or_kaffpa_combine(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+                      const or_knobs* knobs, const int* part_a, const int* part_b, long long* edgecut, int* part,
+                      or_stats* stats) {
+    if (n < 0 || !knobs || knobs->k < 1 || !xadj || (n > 0 && (!adjncy || !part_a || !part_b))) return -1;
+    for (int v = 0; v < n; ++v)
+        if (part_a[v] < 0 || part_a[v] >= knobs->k || part_b[v] < 0 || part_b[v] >= knobs->k) return -1;
+    /* the better parent by (overload, cut); part_a on ties */
+    const int m = xadj[n];
+    int* vw = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    int* ew = xmalloc(sizeof(int) * (size_t)(m ? m : 1));
+    for (int v = 0; v < n; ++v) vw[v] = vwgt ? vwgt[v] : 1;
+    for (int e = 0; e < m; ++e) ew[e] = adjcwgt ? adjcwgt[e] : 1;
+    or_graph g = {n, xadj, adjncy, ew, vw};
+    uint64_t ova, ovb;
+    long long ca, cb;
+    part_quality(&g, part_a, knobs->k, knobs->final_bound, &ova, &ca);
+    part_quality(&g, part_b, knobs->k, knobs->final_bound, &ovb, &cb);
+    free(vw);
+    free(ew);
+    const int b_first = ovb < ova || (ovb == ova && cb < ca);
+    return kaffpa_core(n, vwgt, xadj, adjcwgt, adjncy, knobs, b_first ? part_b : part_a, b_first ? part_a : part_b,
+                       edgecut, part, stats);
+}
+
+static int kaffpa_core_combine(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+                               const or_knobs* knobs, const int* part_a, const int* part_b, long long* edgecut,
+                               int* part) {
+    return or_kaffpa_combine(n, vwgt, xadj, adjcwgt, adjncy, knobs, part_a, part_b, edgecut, part, NULL);
+}
+
+/* ------------------------------------------------ evolutionary partitioning */
+
+typedef struct {
+    uint64_t ov;
+    long long cut;
+} or_obj;
+
+static int obj_less(or_obj a, or_obj b) { return a.ov < b.ov || (a.ov == b.ov && a.cut < b.cut); }
+
+/* directed entries whose cut status differs between two partitions (twice
+ * the size of the symmetric difference of their cut-edge sets) */
+static long long cut_difference(const or_graph* g, const int* a, const int* b) {
+    long long d = 0;
+    for (int v = 0; v < g->n; ++v)
+        for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) {
+            const int u = g->adjncy[e];
+            d += (a[v] != a[u]) != (b[v] != b[u]);
+        }
+    return d;
+}
+
+/* the better of two members by (objective, index) */
+static int fitter(const or_obj* obj, int a, int b) {
+    if (obj_less(obj[a], obj[b])) return a;
+    if (obj_less(obj[b], obj[a])) return b;
+    return a < b ? a : b;
+}
+
+static void or_evo_select(const or_obj* obj, int P, uint64_t ks, int* first, int* second) {
+    const int x0 = (int)or_range(or_hash(ks, 0), (uint32_t)P), x1 = (int)or_range(or_hash(ks, 1), (uint32_t)P);
+    const int x2 = (int)or_range(or_hash(ks, 2), (uint32_t)P), x3 = (int)or_range(or_hash(ks, 3), (uint32_t)P);
+    const int f = fitter(obj, x0, x1);
+    int s2 = fitter(obj, x2, x3);
+    if (s2 == f) s2 = s2 == x2 ? x3 : x2;
+    if (s2 == f) s2 = (f + 1) % P;
+    *first = f;
+    *second = s2;
+}
+
+int or_kaffpae(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+               const or_knobs* knobs, int population, int generations, int per_generation, long long* edgecut,
+               int* part, long long* history) {
+    if (n < 0 || !knobs || knobs->k < 1 || population < 1 || generations < 0 || per_generation < 1) return -1;
+    const int P = population, W = per_generation, k = knobs->k;
+    const int m = xadj[n];
+    int* vw = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    int* ew = xmalloc(sizeof(int) * (size_t)(m ? m : 1));
+    for (int v = 0; v < n; ++v) vw[v] = vwgt ? vwgt[v] : 1;
+    for (int e = 0; e < m; ++e) ew[e] = adjcwgt ? adjcwgt[e] : 1;
+    or_graph g = {n, xadj, adjncy, ew, vw};
+    const size_t nn = (size_t)(n ? n : 1);
+    int* pop = xmalloc(sizeof(int) * nn * (size_t)P);
+    int* off = xmalloc(sizeof(int) * nn * (size_t)W);
+    or_obj* obj = xmalloc(sizeof(or_obj) * (size_t)P);
+    or_obj* oobj = xmalloc(sizeof(or_obj) * (size_t)W);
+    int rc = 0;
+    /* population: member i is the plain partitioner with seed + i */
+    for (int i = 0; i < P && !rc; ++i) {
+        or_knobs kn = *knobs;
+        kn.seed = knobs->seed + i;
+        long long c;
+        rc = kaffpa_core(n, vwgt, xadj, adjcwgt, adjncy, &kn, NULL, NULL, &c, pop + (size_t)i * nn, NULL);
+        part_quality(&g, pop + (size_t)i * nn, k, knobs->final_bound, &obj[i].ov, &obj[i].cut);
+    }
+    int best = 0;
+    for (int i = 1; i < P; ++i) best = fitter(obj, best, i);
+    if (history) history[0] = obj[best].cut;
+    for (int t = 0; t < generations && !rc; ++t) {
+        if (P >= 2) {
+            /* every offspring of a generation reads the population at its start */
+            for (int j = 0; j < W && !rc; ++j) {
+                int a, b;
+                or_evo_select(obj, P, or_stream(knobs->seed, TAG_EVO, t, j), &a, &b);
+                or_knobs kn = *knobs;
+                kn.seed = knobs->seed + P + t * W + j;
+                long long c;
+                rc = kaffpa_core_combine(n, vwgt, xadj, adjcwgt, adjncy, &kn, pop + (size_t)a * nn,
+                                         pop + (size_t)b * nn, &c, off + (size_t)j * nn);
+                part_quality(&g, off + (size_t)j * nn, k, knobs->final_bound, &oobj[j].ov, &oobj[j].cut);
+            }
+            /* population.cpp:120-173: an offspring worse than the worst member
+             * is dropped; otherwise it replaces the member most similar to it
+             * (fewest differing cut edges) among those not better than it */
+            for (int j = 0; j < W && !rc; ++j) {
+                int worst = 0;
+                for (int i = 1; i < P; ++i)
+                    if (obj_less(obj[worst], obj[i])) worst = i;
+                if (obj_less(obj[worst], oobj[j])) continue;
+                int pick = -1;
+                long long pd = 0;
+                for (int i = 0; i < P; ++i) {
+                    if (obj_less(obj[i], oobj[j])) continue;
+                    const long long d = cut_difference(&g, pop + (size_t)i * nn, off + (size_t)j * nn);
+                    if (pick < 0 || d < pd) { pick = i; pd = d; }
+                }
+                memcpy(pop + (size_t)pick * nn, off + (size_t)j * nn, sizeof(int) * (size_t)n);
+                obj[pick] = oobj[j];
+            }
+        }
+        best = 0;
+        for (int i = 1; i < P; ++i) best = fitter(obj, best, i);
+        if (history) history[t + 1] = obj[best].cut;
+    }
+    if (!rc) {
+        memcpy(part, pop + (size_t)best * nn, sizeof(int) * (size_t)n);
+        *edgecut = obj[best].cut;
+    }
+    free(pop); free(off); free(obj); free(oobj); free(vw); free(ew);
+    return rc;
 }

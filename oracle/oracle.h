@@ -133,6 +133,25 @@ int or_kaffpa(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const
 int or_kaffpa_knobs(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
                     const or_knobs* kn, long long* edgecut, int* part, or_stats* stats);
 
+/* KaFFPaE combine of two partitions of the same graph (population.cpp:189-250):
+ * coarsening keeps every node pair that some parent separates apart, the
+ * coarsest graph takes the better parent (by overload, then cut; part_a on
+ * ties), and the result is never worse than that parent. */
+int or_kaffpa_combine(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+                      const or_knobs* kn, const int* part_a, const int* part_b, long long* edgecut, int* part,
+                      or_stats* stats);
+
+/* KaFFPaE-style evolution on one process (parallel_mh_async.cpp:49-…,
+ * population.cpp:120-173,358-369): `population` members from the plain
+ * partitioner (seed + i), then `generations` rounds of `per_generation`
+ * combines of tournament-selected pairs (all reading the population at the
+ * round's start), each offspring inserted in order by the reference's rule.
+ * part/edgecut: the best member; history[generations + 1] (optional): the
+ * best cut after the initial population and after every round. */
+int or_kaffpae(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
+               const or_knobs* kn, int population, int generations, int per_generation, long long* edgecut,
+               int* part, long long* history);
+
 #ifdef __cplusplus
 }
 #endif

@@ -69,6 +69,8 @@ def lib():
         L.or_balance.restype = ctypes.c_int
         L.or_kaffpa.restype = ctypes.c_int
         L.or_kaffpa_knobs.restype = ctypes.c_int
+        L.or_kaffpa_combine.restype = ctypes.c_int
+        L.or_kaffpae.restype = ctypes.c_int
         L.or_hash.restype = ctypes.c_uint32
         L.or_hash.argtypes = [ctypes.c_uint64, ctypes.c_uint32]
         L.or_stream.restype = ctypes.c_uint64
@@ -244,6 +246,36 @@ def kaffpa_knobs(g: dict, kn: Knobs, unit_weights=False):
                                ctypes.byref(cut), _p(part), ctypes.byref(st))
     if rc != 0:
         raise ValueError(f"or_kaffpa_knobs rejected the input ({rc})")
+    return cut.value, part, st
+
+
+def kaffpae(g: dict, kn: Knobs, population: int, generations: int, per_generation: int, unit_weights=False):
+    """KaFFPaE-style evolution (oracle.c or_kaffpae).  Returns (edgecut, part, history)."""
+    part = np.empty(g["n"], np.int32)
+    hist = np.zeros(generations + 1, np.int64)
+    cut = ctypes.c_longlong()
+    rc = lib().or_kaffpae(g["n"], None if unit_weights else _p(g["vwgt"]), _p(g["xadj"]),
+                          None if unit_weights else _p(g["adjwgt"]), _p(g["adjncy"]), ctypes.byref(kn),
+                          population, generations, per_generation, ctypes.byref(cut), _p(part),
+                          hist.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)))
+    if rc != 0:
+        raise ValueError(f"or_kaffpae rejected the input ({rc})")
+    return cut.value, part, hist
+
+
+def kaffpa_combine(g: dict, kn: Knobs, part_a, part_b, unit_weights=False):
+    """KaFFPaE combine of two partitions (oracle.c or_kaffpa_combine).
+    Returns (edgecut, part, stats)."""
+    part = np.empty(g["n"], np.int32)
+    pa = np.ascontiguousarray(part_a, dtype=np.int32)
+    pb = np.ascontiguousarray(part_b, dtype=np.int32)
+    cut = ctypes.c_longlong()
+    st = Stats()
+    rc = lib().or_kaffpa_combine(g["n"], None if unit_weights else _p(g["vwgt"]), _p(g["xadj"]),
+                                 None if unit_weights else _p(g["adjwgt"]), _p(g["adjncy"]), ctypes.byref(kn),
+                                 _p(pa), _p(pb), ctypes.byref(cut), _p(part), ctypes.byref(st))
+    if rc != 0:
+        raise ValueError(f"or_kaffpa_combine rejected the input ({rc})")
     return cut.value, part, st
 
 

@@ -32,6 +32,16 @@ def test_library_loads_and_exports_every_declared_symbol():
     assert set(native.EXPORTS) == declared
 
 
+def test_every_bound_entry_point_declares_its_argument_types():
+    # without argtypes ctypes passes Python ints (array addresses) as 32-bit
+    # C ints; kb200_edge_cut_noalloc is bound by its own test
+    from kahip_b200 import native
+    L = native.lib()
+    missing = [e for e in native.EXPORTS
+               if e.startswith("kb200_") and e != "kb200_edge_cut_noalloc" and getattr(L, e).argtypes is None]
+    assert not missing, missing
+
+
 def test_no_device_no_fallback():
     from kahip_b200 import native
     if native.device_count() > 0:

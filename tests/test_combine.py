@@ -1,0 +1,93 @@
+"""KaFFPaE combine in the oracle (CPU): the coarsest graph keeps every cut
+edge of the better parent (its initial cut equals that parent's cut), the
+child is never worse than the better parent by (overload, cut), the better
+parent is chosen whatever the argument order, and the result is
+deterministic."""
+import numpy as np
+import pytest
+
+from conftest import tie_free
+
+from oracle import oracle as O
+
+
+def parents(g, k, mode, coarsening):
+    out = []
+    for seed in (11, 12):
+        kn = O.knobs(g, k, 0.03, seed, mode)
+        kn.coarsening = coarsening
+        out.append(O.kaffpa_knobs(g, kn)[1])
+    return out
+
+
+def quality(g, part, k, bound):
+    bw = O.block_weights(g, part, k)
+    return int(np.maximum(bw.astype(np.int64) - bound, 0).sum()), O.edge_cut(g, part)
+
+
+@pytest.mark.parametrize("which", ["rgg2d", "rgg3d", "rmat", "tiefree"])
+@pytest.mark.parametrize("mode,coarsening", [(0, 0), (0, 1), (1, 1)])
+def test_child_keeps_parent_cut_edges_and_never_worsens(graphs, which, mode, coarsening):
+    g = {"rgg2d": lambda: graphs.rgg2d(1 << 13, seed=1), "rgg3d": lambda: graphs.rgg3d(1 << 12, seed=2),
+         "rmat": lambda: graphs.rmat(11, seed=3), "tiefree": lambda: tie_free(graphs.rgg2d(5000, seed=4))}[which]()
+    k = 8
+    pa, pb = parents(g, k, mode, coarsening)
+    kn = O.knobs(g, k, 0.03, 3, mode)
+    kn.coarsening = coarsening
+    qa, qb = quality(g, pa, k, kn.final_bound), quality(g, pb, k, kn.final_bound)
+    better = pa if qa <= qb else pb
+    cut, part, st = O.kaffpa_combine(g, kn, pa, pb)
+    assert st.initial_cut == O.edge_cut(g, better)
+    q = quality(g, part, k, kn.final_bound)
+    assert q <= min(qa, qb) and cut == q[1]
+    if qa != qb:
+        cut2, part2, _ = O.kaffpa_combine(g, kn, pb, pa)
+        assert cut2 == cut and np.array_equal(part2, part)
+    assert np.array_equal(O.kaffpa_combine(g, kn, pa, pb)[1], part)
+
+
+def test_identical_parents_and_empty_graph(graphs):
+    g = graphs.rgg2d(3000, seed=9)
+    kn = O.knobs(g, 4, 0.03, 0, 0)
+    p = O.kaffpa_knobs(g, kn)[1]
+    cut, part, st = O.kaffpa_combine(g, kn, p, p)
+    assert st.initial_cut == O.edge_cut(g, p) and cut <= O.edge_cut(g, p)
+    e = {"n": 0, "m": 0, "xadj": np.zeros(1, np.int32), "adjncy": np.zeros(0, np.int32),
+         "adjwgt": np.zeros(0, np.int32), "vwgt": np.zeros(0, np.int32)}
+    cut, part, _ = O.kaffpa_combine(e, O.knobs(e, 4, 0.03, 0, 0), np.zeros(0, np.int32), np.zeros(0, np.int32))
+    assert cut == 0 and len(part) == 0
+
+
+def test_rejects_out_of_range_parent(graphs):
+    g = graphs.rgg2d(500, seed=1)
+    kn = O.knobs(g, 4, 0.03, 0, 0)
+    p = np.zeros(g["n"], np.int32)
+    q = p.copy()
+    q[7] = 4
+    with pytest.raises(ValueError):
+        O.kaffpa_combine(g, kn, p, q)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_evolution_never_loses_its_best(graphs, mode):
+    g = graphs.rgg2d(1 << 12, seed=2)
+    kn = O.knobs(g, 8, 0.03, 4, mode)
+    cut, part, hist = O.kaffpae(g, kn, 4, 3, 2)
+    assert all(hist[i + 1] <= hist[i] for i in range(len(hist) - 1))
+    assert cut == hist[-1] == O.edge_cut(g, part)
+    # the initial population is the plain partitioner with seeds seed + i
+    firsts = []
+    for i in range(4):
+        k2 = O.knobs(g, 8, 0.03, 4 + i, mode)
+        firsts.append(O.kaffpa_knobs(g, k2)[0])
+    assert hist[0] == min(firsts)
+    again = O.kaffpae(g, kn, 4, 3, 2)
+    assert again[0] == cut and np.array_equal(again[1], part)
+
+
+def test_evolution_single_member_is_the_plain_partitioner(graphs):
+    g = graphs.rgg2d(2000, seed=3)
+    kn = O.knobs(g, 4, 0.03, 9, 0)
+    cut, part, hist = O.kaffpae(g, kn, 1, 2, 1)
+    c0, p0, _ = O.kaffpa_knobs(g, kn)
+    assert cut == c0 and np.array_equal(part, p0) and list(hist) == [c0] * 3
