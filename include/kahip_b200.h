@@ -143,10 +143,11 @@ int kb200_kaffpa_combine(int n, const int* vwgt, const int* xadj, const int* adj
  * round's start) with kb200_kaffpa_combine's operator and inserts the
  * offspring in order.  part[]/edgecut: the best member by (overload, cut);
  * history[generations + 1] (optional): the best cut after the initial
- * population and after every round. */
+ * population and after every round.  workers: concurrent partitionings on
+ * the device (0 = min(per_generation, 4)); results do not depend on it. */
 int kb200_kaffpae(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
-                  const kb200_knobs* kn, int population, int generations, int per_generation, long long* edgecut,
-                  int* part, long long* history);
+                  const kb200_knobs* kn, int population, int generations, int per_generation, int workers,
+                  long long* edgecut, int* part, long long* history);
 
 /* Same with device buffers (explicit weights), like kb200_kaffpa_device. */
 int kb200_kaffpa_device_knobs(int n, const int* d_vwgt, const int* d_xadj, const int* d_adjcwgt,

@@ -334,8 +334,8 @@ int kb200_kaffpa_combine(int n, const int* vwgt, const int* xadj, const int* adj
 }
 
 int kb200_kaffpae(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
-                  const kb200_knobs* kn, int population, int generations, int per_generation, long long* edgecut,
-                  int* part, long long* history) {
+                  const kb200_knobs* kn, int population, int generations, int per_generation, int workers,
+                  long long* edgecut, int* part, long long* history) {
     g_last_error.clear();
     return guarded([&]() -> int {
         int rc = validate(n, xadj, adjncy, adjcwgt, vwgt);
@@ -343,20 +343,31 @@ int kb200_kaffpae(int n, const int* vwgt, const int* xadj, const int* adjcwgt, c
         if (population < 1 || generations < 0 || per_generation < 1)
             return fail(KB_ERR_INVALID_INPUT, "population >= 1, generations >= 0, per_generation >= 1 required");
         if (!edgecut || (n > 0 && !part)) return fail(KB_ERR_INVALID_INPUT, "edgecut/part is NULL");
+        if (workers < 0) return fail(KB_ERR_INVALID_INPUT, "workers must be >= 0");
         int dev;
         if ((rc = current_device(&dev))) return rc;
         Lease lease(dev);
         Ctx& ctx = *lease.ctx;
+        // worker contexts: 0 = as many as a round has offspring, at most 4
+        const int Wk = workers > 0 ? workers : std::max(1, std::min(4, std::max(per_generation, 1)));
+        std::vector<std::unique_ptr<Lease>> leases;
+        std::vector<Ctx*> wctx;
+        for (int w = 0; w < Wk; ++w) {
+            leases.emplace_back(new Lease(dev));
+            wctx.push_back(leases.back()->ctx.get());
+        }
         const long long m = xadj[n];
         for (int attempt = 0;; ++attempt) {
             try {
-                reserve_for(ctx, n, m, true, (attempt == 0 ? 1.0 : 2.0 * attempt) * 1.5);
+                // the main context holds the graph; the workers reserve their own arenas
+                reserve_for(ctx, n, m, true, attempt == 0 ? 1.0 : 2.0 * attempt);
                 ctx.timing = false;
                 ctx.reset_stats();
                 Upload up = upload(ctx, n, xadj, adjncy, adjcwgt, vwgt);
                 check_uploaded(ctx, up.g);
                 long long cut = 0;
-                int r = kaffpae(ctx, up.g, *kn, population, generations, per_generation, up.part, &cut, history);
+                int r = kaffpae(ctx, wctx, up.g, *kn, population, generations, per_generation, up.part, &cut,
+                                history);
                 if (n) KB_CUDA(cudaMemcpyAsync(part, up.part, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, ctx.stream));
                 KB_CUDA(cudaStreamSynchronize(ctx.stream));
                 *edgecut = cut;

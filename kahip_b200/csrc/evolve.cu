@@ -13,6 +13,11 @@
 // difference is one pass over the edges.
 #include "evolve.cuh"
 
+#include <atomic>
+#include <exception>
+#include <mutex>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "common.cuh"
@@ -82,30 +87,75 @@ struct DevBuf {
     DevBuf& operator=(const DevBuf&) = delete;
 };
 
+// f(c, i) for i in [0, count) on the worker contexts, one host thread per
+// context; each task gets freshly reserved arenas (grown when exhausted).
+// The first exception is rethrown after every thread has joined.
+template <class F>
+void run_tasks(const std::vector<Ctx*>& workers, const DevGraph& g0, int count, F f) {
+    const int T = std::max(1, std::min((int)workers.size(), count));
+    std::atomic<int> next{0};
+    std::exception_ptr err;
+    std::mutex mu;
+    auto body = [&](int t) {
+        Ctx& c = *workers[(size_t)t];
+        cudaSetDevice(c.device);
+        for (int i; (i = next.fetch_add(1)) < count;) {
+            try {
+                for (int attempt = 0;; ++attempt) {
+                    try {
+                        reserve_for(c, g0.n, g0.m, false, (attempt == 0 ? 1.0 : 2.0 * attempt) * 1.5);
+                        c.timing = false;
+                        c.reset_stats();
+                        f(c, i);
+                        break;
+                    } catch (const CudaError& e) {
+                        if (e.code == cudaErrorMemoryAllocation && attempt < 2 &&
+                            std::string(e.what()).find("arena exhausted") != std::string::npos) {
+                            (void)cudaGetLastError();
+                            continue;
+                        }
+                        throw;
+                    }
+                }
+            } catch (...) {
+                std::lock_guard<std::mutex> lk(mu);
+                if (!err) err = std::current_exception();
+                next.store(count);
+            }
+        }
+    };
+    std::vector<std::thread> threads;
+    for (int t = 1; t < T; ++t) threads.emplace_back(body, t);
+    body(0);
+    for (auto& th : threads) th.join();
+    if (err) std::rethrow_exception(err);
+}
+
 }  // namespace
 
-int kaffpae(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int population, int generations, int per_generation,
-            int* d_best, long long* edgecut, long long* history) {
+int kaffpae(Ctx& ctx, const std::vector<Ctx*>& workers, const DevGraph& g0, const Knobs& kn, int population,
+            int generations, int per_generation, int* d_best, long long* edgecut, long long* history) {
     const int P = population, W = per_generation, n = g0.n;
     const size_t nn = (size_t)std::max(n, 1);
     DevBuf pop(nn * (size_t)P), off(nn * (size_t)W);
     std::vector<Obj> obj((size_t)P), oobj((size_t)W);
-    for (int i = 0; i < P; ++i) {
+    // members: the plain partitioner with seeds seed + i
+    run_tasks(workers, g0, P, [&](Ctx& c, int i) {
         Knobs k = kn;
         k.seed = kn.seed + i;
-        const size_t mk = ctx.hier.mark();
-        long long c = 0;
-        partition(ctx, g0, k, pop.p + (size_t)i * nn, &c, nullptr);
-        ctx.hier.release(mk);
-        partition_quality(ctx, g0, pop.p + (size_t)i * nn, kn.k, kn.final_bound, &obj[i].ov, &obj[i].cut);
-    }
+        long long cut = 0;
+        partition(c, g0, k, pop.p + (size_t)i * nn, &cut, nullptr);
+        partition_quality(c, g0, pop.p + (size_t)i * nn, kn.k, kn.final_bound, &obj[(size_t)i].ov,
+                          &obj[(size_t)i].cut);
+    });
     int best = 0;
     for (int i = 1; i < P; ++i) best = fitter(obj, best, i);
     if (history) history[0] = obj[best].cut;
+    std::vector<int> pa((size_t)W), pb((size_t)W);
     for (int t = 0; t < generations; ++t) {
         if (P >= 2) {
+            // selections read the population at the round's start
             for (int j = 0; j < W; ++j) {
-                // tournaments of two hash-drawn members each
                 const uint64_t ks = stream_key(kn.seed, TAG_EVO, t, j);
                 const int x0 = (int)hash_range(hash32(ks, 0u), (uint32_t)P);
                 const int x1 = (int)hash_range(hash32(ks, 1u), (uint32_t)P);
@@ -115,15 +165,19 @@ int kaffpae(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int population, int g
                 int b = fitter(obj, x2, x3);
                 if (b == a) b = b == x2 ? x3 : x2;
                 if (b == a) b = (a + 1) % P;
+                pa[(size_t)j] = a;
+                pb[(size_t)j] = b;
+            }
+            run_tasks(workers, g0, W, [&](Ctx& c, int j) {
                 Knobs k = kn;
                 k.seed = kn.seed + P + t * W + j;
-                const size_t mk = ctx.hier.mark();
-                long long c = 0;
-                combine(ctx, g0, k, pop.p + (size_t)a * nn, pop.p + (size_t)b * nn, off.p + (size_t)j * nn, &c,
-                        nullptr);
-                ctx.hier.release(mk);
-                partition_quality(ctx, g0, off.p + (size_t)j * nn, kn.k, kn.final_bound, &oobj[j].ov, &oobj[j].cut);
-            }
+                long long cut = 0;
+                combine(c, g0, k, pop.p + (size_t)pa[(size_t)j] * nn, pop.p + (size_t)pb[(size_t)j] * nn,
+                        off.p + (size_t)j * nn, &cut, nullptr);
+                partition_quality(c, g0, off.p + (size_t)j * nn, kn.k, kn.final_bound, &oobj[(size_t)j].ov,
+                                  &oobj[(size_t)j].cut);
+            });
+            // insertion in offspring order
             for (int j = 0; j < W; ++j) {
                 int worst = 0;
                 for (int i = 1; i < P; ++i)
@@ -141,6 +195,7 @@ int kaffpae(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int population, int g
                                             cudaMemcpyDeviceToDevice, ctx.stream));
                 obj[pick] = oobj[j];
             }
+            KB_CUDA(cudaStreamSynchronize(ctx.stream));
         }
         best = 0;
         for (int i = 1; i < P; ++i) best = fitter(obj, best, i);

@@ -129,7 +129,7 @@ def lib():
                                                 ctypes.POINTER(Stats)]
         L.kb200_kaffpa_combine.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), vp, vp, c_ll_p, vp,
                                            ctypes.POINTER(Stats)]
-        L.kb200_kaffpae.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, i, i, c_ll_p, vp, vp]
+        L.kb200_kaffpae.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, i, i, i, c_ll_p, vp, vp]
         L.kb200_hem_match.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), i, vp, vp]
         L.kb200_rating_infer.argtypes = [i, vp, vp, vp, vp, vp, i, vp, vp]
         L.kb200_rating_train.argtypes = [ctypes.POINTER(TrainGraph), i, i, ctypes.c_float, vp, vp]
@@ -239,7 +239,8 @@ def kaffpa_combine(g: dict, kn: Knobs, part_a, part_b, stats: Stats | None = Non
     return rc, cut.value, part
 
 
-def kaffpae(g: dict, kn: Knobs, population: int, generations: int, per_generation: int, unit_weights=False):
+def kaffpae(g: dict, kn: Knobs, population: int, generations: int, per_generation: int, workers=0,
+            unit_weights=False):
     """KaFFPaE-style evolution on the device (kb200_kaffpae).
     Returns (status, edgecut, part, history)."""
     n = g["n"]
@@ -250,7 +251,7 @@ def kaffpae(g: dict, kn: Knobs, population: int, generations: int, per_generatio
     hist = np.zeros(max(generations, 0) + 1, np.int64)
     cut = ctypes.c_longlong(-1)
     rc = lib().kb200_kaffpae(n, _ptr(vwgt), _ptr(xadj), _ptr(adjwgt), _ptr(adjncy), ctypes.byref(kn), population,
-                             generations, per_generation, ctypes.byref(cut), _ptr(part), hist.ctypes.data)
+                             generations, per_generation, workers, ctypes.byref(cut), _ptr(part), hist.ctypes.data)
     _check(rc)
     return rc, cut.value, part, hist
 

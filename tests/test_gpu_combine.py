@@ -70,3 +70,11 @@ def test_evolution_matches_oracle(N, O, graphs, which, mode, k):
     _, cut_d, part_d, hist_d = N.kaffpae(g, kn_d, 4, 3, 2)
     assert cut_d == cut_o and np.array_equal(part_d, part_o)
     assert np.array_equal(hist_d, hist_o)
+
+
+def test_evolution_does_not_depend_on_workers(N, graphs):
+    g = graphs.rgg2d(1 << 13, seed=8)
+    kn = N.derive_knobs(g["n"], g["vwgt"], 8, 0.03, 3, 0)
+    runs = [N.kaffpae(g, kn, 5, 2, 3, workers=w) for w in (1, 2, 3)]
+    for r in runs[1:]:
+        assert r[1] == runs[0][1] and np.array_equal(r[2], runs[0][2]) and np.array_equal(r[3], runs[0][3])
