@@ -86,16 +86,30 @@ int current_device(int* dev) {
 // and is monotone).  Targets in range and non-negative weights are checked
 // on the device right after the upload (check_uploaded), before any kernel
 // reads through adjncy.
+// Host checks that size the upload: O(1).  Monotonicity of xadj, targets in
+// range and weight signs are checked on the device right after the upload
+// (check_uploaded), before any kernel reads through xadj; a host-side scan of
+// xadj would cost ~10 ms per 2^24 nodes on every call.
 int validate(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt) {
     (void)adjwgt;
     (void)vwgt;
     if (n < 0) return fail(KB_ERR_INVALID_INPUT, "n < 0");
     if (!xadj) return fail(KB_ERR_INVALID_INPUT, "xadj is NULL");
     if (xadj[0] != 0) return fail(KB_ERR_INVALID_INPUT, "xadj[0] != 0");
+    const long long m = xadj[n];
+    if (m < 0) return fail(KB_ERR_INVALID_INPUT, "xadj[n] < 0");
+    if (m > 0 && !adjncy) return fail(KB_ERR_INVALID_INPUT, "adjncy is NULL");
+    return KB_OK;
+}
+
+// Full host check for entry points that read the graph on the host.
+int validate_host_graph(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt) {
+    int rc = validate(n, xadj, adjncy, adjwgt, vwgt);
+    if (rc) return rc;
     for (int v = 0; v < n; ++v)
         if (xadj[v + 1] < xadj[v]) return fail(KB_ERR_INVALID_INPUT, "xadj is not monotone");
-    const long long m = xadj[n];
-    if (m > 0 && !adjncy) return fail(KB_ERR_INVALID_INPUT, "adjncy is NULL");
+    for (long long e = 0; e < xadj[n]; ++e)
+        if (adjncy[e] < 0 || adjncy[e] >= n) return fail(KB_ERR_INVALID_INPUT, "adjncy entry out of range");
     return KB_OK;
 }
 
@@ -204,10 +218,13 @@ int check_knobs(const kb200_knobs* kn) {
 
 int run_host_in(Ctx& ctx, int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
                 const Knobs& kn, long long* edgecut, int* part, kb200_stats* st, clk::time_point t0,
-                const int* parent_a = nullptr, const int* parent_b = nullptr);
+                const int* parent_a = nullptr, const int* parent_b = nullptr, bool derive_on_device = false);
 
+// derive_on_device: kn carries k, imbalance, seed and mode only; the other
+// knobs come from the node-weight sum the device check computes (saves a
+// host pass over vwgt).
 int run_host(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy, const Knobs& kn,
-             long long* edgecut, int* part, kb200_stats* st) {
+             long long* edgecut, int* part, kb200_stats* st, bool derive_on_device = false) {
     auto t0 = clk::now();
     int rc = validate(n, xadj, adjncy, adjcwgt, vwgt);
     if (rc || (rc = check_knobs(&kn))) return rc;
@@ -215,14 +232,16 @@ int run_host(int n, const int* vwgt, const int* xadj, const int* adjcwgt, const 
     int dev;
     if ((rc = current_device(&dev))) return rc;
     Lease lease(dev);
-    return run_host_in(*lease.ctx, n, vwgt, xadj, adjcwgt, adjncy, kn, edgecut, part, st, t0);
+    return run_host_in(*lease.ctx, n, vwgt, xadj, adjcwgt, adjncy, kn, edgecut, part, st, t0, nullptr, nullptr,
+                       derive_on_device);
 }
 
 // The body of a host-buffer call on a leased context (input already
 // validated).  With parent_a / parent_b (host, n each) it is a combine.
 int run_host_in(Ctx& ctx, int n, const int* vwgt, const int* xadj, const int* adjcwgt, const int* adjncy,
-                const Knobs& kn, long long* edgecut, int* part, kb200_stats* st, clk::time_point t0,
-                const int* parent_a, const int* parent_b) {
+                const Knobs& kn_in, long long* edgecut, int* part, kb200_stats* st, clk::time_point t0,
+                const int* parent_a, const int* parent_b, bool derive_on_device) {
+    Knobs kn = kn_in;
     const long long m = xadj[n];
     const bool comb = parent_a != nullptr;
     for (int attempt = 0;; ++attempt) {
@@ -232,7 +251,9 @@ int run_host_in(Ctx& ctx, int n, const int* vwgt, const int* xadj, const int* ad
             begin_stats(ctx, st);
             auto th = clk::now();
             Upload up = upload(ctx, n, xadj, adjncy, adjcwgt, vwgt);
-            check_uploaded(ctx, up.g);
+            uint32_t W = 0;
+            check_uploaded(ctx, up.g, &W);
+            if (derive_on_device) derive_knobs_total(n, W, kn_in.k, kn_in.imbalance, kn_in.seed, kn_in.mode, kn);
             int* dpar = nullptr;
             if (comb) {
                 dpar = ctx.hier.alloc<int>(2 * (size_t)std::max(n, 1));
@@ -306,8 +327,9 @@ int kb200_kaffpa(int n, const int* vwgt, const int* xadj, const int* adjcwgt, co
         if (nparts < 1) return fail(KB_ERR_INVALID_INPUT, "nparts < 1");
         if (!(imbalance >= 0)) return fail(KB_ERR_INVALID_INPUT, "imbalance must be >= 0");
         Knobs kn;
-        derive_knobs(n, vwgt, nparts, imbalance, seed, mode, kn);
-        return run_host(n, vwgt, xadj, adjcwgt, adjncy, kn, edgecut, part, stats);
+        // unit weights: W = n now; explicit weights: W from the device check
+        derive_knobs(n, nullptr, nparts, imbalance, seed, mode, kn);
+        return run_host(n, vwgt, xadj, adjcwgt, adjncy, kn, edgecut, part, stats, vwgt != nullptr);
     });
 }
 
@@ -755,7 +777,7 @@ int kb200_initial_partition(int n, const int* xadj, const int* adjncy, const int
     g_last_error.clear();
     return guarded([&]() -> int {
         int rc;
-        if ((rc = validate(n, xadj, adjncy, adjwgt, vwgt)) || (rc = check_knobs(kn))) return rc;
+        if ((rc = validate_host_graph(n, xadj, adjncy, adjwgt, vwgt)) || (rc = check_knobs(kn))) return rc;
         if (!adjwgt || !vwgt) return fail(KB_ERR_INVALID_INPUT, "explicit weights required");
         initial_partition(n, xadj, adjncy, adjwgt, vwgt, *kn, part);
         return KB_OK;

@@ -60,9 +60,11 @@ def test_no_device_no_fallback():
 
 
 def test_host_validation_before_device():
+    # what sizes the upload is checked on the host (monotonicity, targets and
+    # weights are checked on the device right after the upload)
     from kahip_b200 import native
     with pytest.raises(native.KaHIPError) as e:
-        native.kaffpa_ex(np.array([0, 2, 1]), np.array([1, 0]), 2)
+        native.kaffpa_ex(np.array([0, 2, -1]), np.array([1, 0]), 2)
     assert e.value.code == native.ERR_INVALID_INPUT
     with pytest.raises(native.KaHIPError) as e:
         native.kaffpa_ex(np.array([1, 2, 3]), np.array([1, 0]), 2)
