@@ -110,7 +110,10 @@ __device__ __forceinline__ void emit_range(int e0, int e1, int step, uint32_t ow
 }
 
 // Long rows (> kEmitLaneDeg entries) are left to emit_wide; their
-// write cursor wpos[v] starts at the row's first entry.
+// write cursor wpos[v] starts at the row's first entry.  UNIT: every edge
+// weight is 1 (adjwgt is not read).  The row entries of the next group of
+// four are loaded while the coarse ids of the current group are gathered.
+template <bool UNIT>
 __global__ void __launch_bounds__(kThreads) emit_kernel(int n, const int* __restrict__ xadj,
                                                         const int* __restrict__ adjncy,
                                                         const int* __restrict__ adjwgt,
@@ -129,20 +132,36 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(int n, const int* __rest
         uint32_t st[kEmitSlots], sw[kEmitSlots];
         int used = 0;
         int pos = beg;
+        int un[4];
+        uint32_t wn[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            un[j] = -1;
+            wn[j] = 0;
+            if (beg + j < end) {
+                un[j] = adjncy[beg + j];
+                wn[j] = UNIT ? 1u : (uint32_t)adjwgt[beg + j];
+            }
+        }
         for (int e = beg; e < end; e += 4) {
             int u[4];
             uint32_t w[4], t[4];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                u[j] = -1;
-                w[j] = 0;
-                if (e + j < end) {
-                    u[j] = adjncy[e + j];
-                    w[j] = (uint32_t)adjwgt[e + j];
-                }
+                u[j] = un[j];
+                w[j] = wn[j];
             }
 #pragma unroll
             for (int j = 0; j < 4; ++j) t[j] = u[j] >= 0 ? (uint32_t)cmap[u[j]] : kEmpty;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                un[j] = -1;
+                wn[j] = 0;
+                if (e + 4 + j < end) {
+                    un[j] = adjncy[e + 4 + j];
+                    wn[j] = UNIT ? 1u : (uint32_t)adjwgt[e + 4 + j];
+                }
+            }
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 if (u[j] < 0 || t[j] == own) continue;
@@ -504,9 +523,13 @@ void contract(Ctx& ctx, const DevGraph& g, const int* label, int* cmap, DevGraph
     uint32_t* vcount = ctx.scratch.alloc<uint32_t>((size_t)n + 1);
     int* wpos = ctx.scratch.alloc<int>((size_t)n + 1);
     {
-        PhaseScope ps(ctx, "contract_emit", 12.0 * m + 8.0 * n);
-        emit_kernel<<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, g.adjncy, g.adjwgt, cmap, ekey, eval,
-                                                                vcount, wpos, tb);
+        PhaseScope ps(ctx, "contract_emit", (g.unit_weights ? 8.0 : 12.0) * m + 8.0 * n);
+        if (g.unit_weights)
+            emit_kernel<true><<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, g.adjncy, g.adjwgt, cmap, ekey,
+                                                                          eval, vcount, wpos, tb);
+        else
+            emit_kernel<false><<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, g.adjncy, g.adjwgt, cmap, ekey,
+                                                                           eval, vcount, wpos, tb);
         KB_LAUNCH();
         if (g.maxdeg > kEmitLaneDeg) {
             const long long chunks = (m + kEmitChunk - 1) / kEmitChunk;
