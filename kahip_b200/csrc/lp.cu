@@ -69,6 +69,8 @@ struct SweepArgs {
     int* hplist; unsigned* hpcount;     // proposals of high-degree vertices
     int singletons;                     // every label is its own vertex id and rows have
                                         // strictly increasing targets (clustering round 0)
+    const uint32_t* tie;                // singletons: hash32(ks_tie, u) per vertex
+    int all_fit;                        // singletons: every neighbour cluster fits (2 max c(v) < bound)
     unsigned long long* work;           // [0] vertices, [1] edges
     int* err;                           // set when an invariant breaks
     // BALANCE
@@ -401,7 +403,9 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
     uint32_t cown = 0;
     if (MODE == CLUSTER && a.singletons) {
         // label[u] == u and no target repeats: the connection to cluster u is
-        // exactly w(v,u), so the best candidate is a running maximum
+        // exactly w(v,u), so the best candidate is a running maximum; the
+        // tie hashes come precomputed per vertex, and the size test is
+        // skipped when every pair of node weights fits under the bound
         uint64_t key = 0;
         uint32_t id = kEmpty;
         for (int e = beg; e < end; e += 4) {
@@ -416,12 +420,16 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
                     w[t] = UNIT ? 1u : (uint32_t)a.adjwgt[e + t];
                 }
             }
+            uint32_t h[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) h[t] = u[t] >= 0 ? a.tie[u[t]] : 0u;
 #pragma unroll
             for (int t = 0; t < 4; ++t) {
                 if (u[t] < 0) continue;
                 const uint32_t l = (uint32_t)u[t];
                 if (l == own) { cown += w[t]; continue; }
-                if (cand_ok<MODE>(a, l, w[t], cv)) better(key, id, cand_key(w[t], a.ks_tie, l), l);
+                if (a.all_fit ? w[t] > 0 : cand_ok<MODE>(a, l, w[t], cv))
+                    better(key, id, ((uint64_t)w[t] << 32) | (uint32_t)~h[t], l);
             }
         }
         wv += 1;
@@ -950,6 +958,11 @@ double sweep_bytes(const DevGraph& g, double frac) {
 
 // --------------------------------------------------------------- clustering
 
+__global__ void tie_hash_kernel(int n, uint64_t ks, uint32_t* tie) {
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x)
+        tie[v] = hash32(ks, (uint32_t)v);
+}
+
 void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* label) {
     const size_t mk = ctx.scratch.mark();
     cudaStream_t st = ctx.stream;
@@ -975,11 +988,21 @@ void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* la
         // round 0 is one fully synchronous sub-round (every cluster is still a
         // single node), later rounds use lpc_subrounds sub-rounds
         a.S = r == 0 ? 1u : (uint32_t)kn.lpc_subrounds;
+        // in round 0 every vertex is its own cluster; with no repeated
+        // targets per row nothing needs aggregating
+        a.singletons = (r == 0 && sorted_rows) ? 1 : 0;
+        a.tie = nullptr;
+        a.all_fit = 0;
+        if (a.singletons && g.n > 0) {
+            uint32_t* tie = ctx.scratch.alloc<uint32_t>(n);
+            tie_hash_kernel<<<(int)std::min<long long>(div_up(g.n, kThreads), (long long)kNumSMs * 16), kThreads, 0,
+                              st>>>(g.n, a.ks_tie, tie);
+            KB_LAUNCH();
+            a.tie = tie;
+            a.all_fit = 2ull * g.maxvw < (unsigned long long)a.bound ? 1 : 0;
+        }
         for (uint32_t s = 0; s < a.S; ++s) {
             a.s = s;
-            // in round 0 every vertex is its own cluster; with no repeated
-            // targets per row nothing needs aggregating
-            a.singletons = (r == 0 && sorted_rows) ? 1 : 0;
             launch_sweep<CLUSTER>(ctx, g, a, b, sweep_bytes(g, 1.0 / a.S));
             PhaseScope ps(ctx, "lp_cluster_admit", 0);
             cluster_decide<<<admit_blocks(), kThreads, 0, st>>>(b.plist, b.hplist, a.hpcount, b.pt, cw, inc, minv,

@@ -17,6 +17,7 @@ struct DevGraph {
     long long m = 0;
     int maxdeg = 0;
     unsigned iso_count = 0, iso_wmax = 0;  // isolated vertices and their largest weight (max_degree fills them)
+    unsigned maxvw = 0xFFFFFFFFu;          // largest node weight (degree_stats fills it; all ones: unknown)
     bool unit_weights = false;  // every edge weight is 1 (lets sweeps skip adjwgt)
     int rows_sorted = -1;       // 1 / 0: rows do / do not list targets strictly increasing; -1 unknown
     const int* xadj = nullptr;

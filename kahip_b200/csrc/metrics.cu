@@ -46,24 +46,28 @@ __global__ void project_kernel(int n, const int* __restrict__ cmap, const int* _
 // out[0] = max degree, out[1] = isolated vertices, out[2] = their largest weight
 __global__ void maxdeg_kernel(int n, const int* __restrict__ xadj, const int* __restrict__ vwgt, int* out) {
     int m = 0;
-    unsigned iso = 0, w = 0;
+    unsigned iso = 0, w = 0, wall = 0;
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
         const int d = xadj[v + 1] - xadj[v];
+        const unsigned wv = (unsigned)vwgt[v];
         m = max(m, d);
+        wall = max(wall, wv);
         if (d == 0) {
             ++iso;
-            w = max(w, (unsigned)vwgt[v]);
+            w = max(w, wv);
         }
     }
     for (int o = 16; o >= 1; o >>= 1) {
         m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
         iso += __shfl_xor_sync(0xffffffffu, iso, o);
         w = max(w, __shfl_xor_sync(0xffffffffu, w, o));
+        wall = max(wall, __shfl_xor_sync(0xffffffffu, wall, o));
     }
     if ((threadIdx.x & 31) == 0) {
         atomicMax(out, m);
         if (iso) atomicAdd(reinterpret_cast<unsigned*>(out + 1), iso);
         if (w) atomicMax(reinterpret_cast<unsigned*>(out + 2), w);
+        if (wall) atomicMax(reinterpret_cast<unsigned*>(out + 3), wall);
     }
 }
 
@@ -172,17 +176,19 @@ void project(Ctx& ctx, int n, const int* cmap, const int* part_coarse, int* part
 
 void degree_stats(Ctx& ctx, DevGraph& g) {
     g.maxdeg = 0;
-    g.iso_count = g.iso_wmax = 0;
+    g.iso_count = g.iso_wmax = g.maxvw = 0;
     if (g.n == 0) return;
-    int* d = ctx.dscalars + 8;  // [8] max degree, [9] isolated count, [10] their max weight
-    KB_CUDA(cudaMemsetAsync(d, 0, 3 * sizeof(int), ctx.stream));
+    // [8] max degree, [9] isolated count, [10] their max weight, [11] max node weight
+    int* d = ctx.dscalars + 8;
+    KB_CUDA(cudaMemsetAsync(d, 0, 4 * sizeof(int), ctx.stream));
     maxdeg_kernel<<<grid_for(g.n, 256), 256, 0, ctx.stream>>>(g.n, g.xadj, g.vwgt, d);
     KB_LAUNCH();
-    KB_CUDA(cudaMemcpyAsync(ctx.pinned + 8, d, 3 * sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    KB_CUDA(cudaMemcpyAsync(ctx.pinned + 8, d, 4 * sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
     KB_CUDA(cudaStreamSynchronize(ctx.stream));
     g.maxdeg = (int)ctx.pinned[8];
     g.iso_count = ctx.pinned[9];
     g.iso_wmax = ctx.pinned[10];
+    g.maxvw = ctx.pinned[11];
 }
 
 int max_degree(Ctx& ctx, const DevGraph& g) {
