@@ -11,11 +11,12 @@
 // Pipeline (all on the device):
 //   1. leader[c] = min member (atomicMin); prefix sum over leader flags
 //      gives coarse ids; cmap gather; coarse node weights (atomicAdd).
-//   2. every fine node merges its neighbours by coarse target in register
-//      slots and writes (cu<<tb|cv, w) entries into its own CSR range of an
-//      m-sized buffer (long rows: the whole warp).
-//   3. the entries move into per-coarse-row buckets (row sizes by atomics,
-//      prefix sum, one atomic reservation per fine node).
+//   2. every coarse row gets a bucket as large as its members' degrees
+//      together (prefix sum); every fine node merges its neighbours by
+//      coarse target in register slots and appends (cv << 32 | w) entries
+//      to its coarse row's bucket, one atomic reservation per slot flush
+//      (long rows: the whole warp).
+//   3. (no separate pass: the buckets are filled by the emission)
 //   4. a warp per coarse row sorts its bucket in shared memory (bitonic),
 //      sums the weights of equal targets and keeps the distinct entries;
 //      rows longer than kSegMax go through a stable LSD radix sort on the
@@ -48,46 +49,42 @@ __global__ void leader_flags(int n, const int* __restrict__ label, const int* __
         flag[v] = mm[label[v]] == v ? 1u : 0u;
 }
 
+// cmap, coarse node weights and each coarse row's bucket capacity (the
+// degrees of its members)
 __global__ void make_cmap(int n, const int* __restrict__ label, const int* __restrict__ mm,
-                          const uint32_t* __restrict__ pos, const int* __restrict__ vwgt, int* cmap,
-                          uint32_t* cvw) {
+                          const uint32_t* __restrict__ pos, const int* __restrict__ vwgt,
+                          const int* __restrict__ xadj, int* cmap, uint32_t* cvw, uint32_t* rowcap) {
     for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
         int c = (int)pos[mm[label[v]]];
         cmap[v] = c;
         atomicAdd(&cvw[c], (uint32_t)vwgt[v]);
+        const uint32_t d = (uint32_t)(xadj[v + 1] - xadj[v]);
+        if (d) atomicAdd(&rowcap[c], d);
     }
 }
 
 // One thread per fine vertex: merges its neighbours by coarse target in
 // kEmitSlots register slots (edges inside its own coarse node are dropped)
-// and writes the (cu<<tb | cv, w) entries into its own CSR range, flushing
-// the slots whenever a new target finds them full -- repeated targets that
-// this leaves are merged by the sort + reduce that follows.
+// and appends the (cv << 32 | w) entries to its coarse row's bucket,
+// flushing the slots whenever a new target finds them full -- repeated
+// targets that this leaves are merged by the per-row sort that follows.
 constexpr int kEmitSlots = 8;
 constexpr int kEmitLaneDeg = 256;  // longer rows are emitted by the whole warp
 
-// Merges the entries [e0, e1) with stride `step` of vertex v's row into
-// kEmitSlots register slots and writes them at positions taken from *pos
-// (a register counter when one lane owns the row, a shared counter when a
-// warp shares it -- atomic then).  Returns nothing; *pos advances.
-template <bool SHARED_POS>
-__device__ __forceinline__ void emit_range(int e0, int e1, int step, uint32_t own, uint64_t hi,
-                                           const int* __restrict__ adjncy, const int* __restrict__ adjwgt,
-                                           const int* __restrict__ cmap, uint64_t* ekey, uint32_t* eval,
-                                           int* pos) {
+__device__ __forceinline__ void flush_slots(int cnt, const uint32_t* st, const uint32_t* sw, uint64_t* dst) {
+#pragma unroll
+    for (int i = 0; i < kEmitSlots; ++i)
+        if (i < cnt) dst[i] = ((uint64_t)st[i] << 32) | sw[i];
+}
+
+// Merges the entries [e0, e1) with stride `step` of a row whose coarse node
+// is `own` into kEmitSlots register slots and appends them to the bucket
+// at rowoff[own] through the row's fill counter.
+__device__ __forceinline__ void emit_range(int e0, int e1, int step, uint32_t own, const int* __restrict__ adjncy,
+                                           const int* __restrict__ adjwgt, const int* __restrict__ cmap,
+                                           const uint32_t* __restrict__ rowoff, uint32_t* fill, uint64_t* bucket) {
     uint32_t st[kEmitSlots], sw[kEmitSlots];
     int used = 0;
-    auto flush = [&](int cnt) {
-        int p = SHARED_POS ? atomicAdd(pos, cnt) : *pos;
-        if (!SHARED_POS) *pos += cnt;
-#pragma unroll
-        for (int i = 0; i < kEmitSlots; ++i)
-            if (i < cnt) {
-                ekey[p] = hi | st[i];
-                eval[p] = sw[i];
-                ++p;
-            }
-    };
     for (int e = e0; e < e1; e += step) {
         const uint32_t t = (uint32_t)cmap[adjncy[e]];
         const uint32_t w = (uint32_t)adjwgt[e];
@@ -98,7 +95,7 @@ __device__ __forceinline__ void emit_range(int e0, int e1, int step, uint32_t ow
             if (i < used && st[i] == t) { sw[i] += w; hit = true; }
         if (hit) continue;
         if (used == kEmitSlots) {
-            flush(kEmitSlots);
+            flush_slots(kEmitSlots, st, sw, bucket + rowoff[own] + atomicAdd(&fill[own], (uint32_t)kEmitSlots));
             used = 0;
         }
 #pragma unroll
@@ -106,32 +103,27 @@ __device__ __forceinline__ void emit_range(int e0, int e1, int step, uint32_t ow
             if (i == used) { st[i] = t; sw[i] = w; }
         ++used;
     }
-    if (used) flush(used);
+    if (used) flush_slots(used, st, sw, bucket + rowoff[own] + atomicAdd(&fill[own], (uint32_t)used));
 }
 
-// Long rows (> kEmitLaneDeg entries) are left to emit_wide; their
-// write cursor wpos[v] starts at the row's first entry.  UNIT: every edge
+// Rows longer than kEmitLaneDeg are left to emit_wide.  UNIT: every edge
 // weight is 1 (adjwgt is not read).  The row entries of the next group of
 // four are loaded while the coarse ids of the current group are gathered.
 template <bool UNIT>
 __global__ void __launch_bounds__(kThreads) emit_kernel(int n, const int* __restrict__ xadj,
                                                         const int* __restrict__ adjncy,
                                                         const int* __restrict__ adjwgt,
-                                                        const int* __restrict__ cmap, uint64_t* ekey,
-                                                        uint32_t* eval, uint32_t* vcount, int* wpos, int tb) {
+                                                        const int* __restrict__ cmap,
+                                                        const uint32_t* __restrict__ rowoff, uint32_t* fill,
+                                                        uint64_t* bucket) {
     for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
         const int v = (int)(base + threadIdx.x);
         if (v >= n) continue;
         const int beg = xadj[v], end = xadj[v + 1];
-        if (end - beg > kEmitLaneDeg) {
-            wpos[v] = beg;
-            continue;
-        }
+        if (end - beg > kEmitLaneDeg) continue;
         const uint32_t own = (uint32_t)cmap[v];
-        const uint64_t hi = (uint64_t)own << tb;
         uint32_t st[kEmitSlots], sw[kEmitSlots];
         int used = 0;
-        int pos = beg;
         int un[4];
         uint32_t wn[4];
 #pragma unroll
@@ -171,12 +163,8 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(int n, const int* __rest
                     if (i < used && st[i] == t[j]) { sw[i] += w[j]; hit = true; }
                 if (hit) continue;
                 if (used == kEmitSlots) {
-#pragma unroll
-                    for (int i = 0; i < kEmitSlots; ++i) {
-                        ekey[pos] = hi | st[i];
-                        eval[pos] = sw[i];
-                        ++pos;
-                    }
+                    flush_slots(kEmitSlots, st, sw,
+                                bucket + rowoff[own] + atomicAdd(&fill[own], (uint32_t)kEmitSlots));
                     used = 0;
                 }
 #pragma unroll
@@ -185,14 +173,7 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(int n, const int* __rest
                 ++used;
             }
         }
-#pragma unroll
-        for (int i = 0; i < kEmitSlots; ++i)
-            if (i < used) {
-                ekey[pos] = hi | st[i];
-                eval[pos] = sw[i];
-                ++pos;
-            }
-        vcount[v] = (uint32_t)(pos - beg);
+        if (used) flush_slots(used, st, sw, bucket + rowoff[own] + atomicAdd(&fill[own], (uint32_t)used));
     }
 }
 
@@ -205,8 +186,8 @@ constexpr int kEmitChunk = 2048;
 
 __global__ void __launch_bounds__(kThreads) emit_wide(int n, long long m, const int* __restrict__ xadj,
                                                       const int* __restrict__ adjncy, const int* __restrict__ adjwgt,
-                                                      const int* __restrict__ cmap, uint64_t* ekey, uint32_t* eval,
-                                                      int* wpos, int tb) {
+                                                      const int* __restrict__ cmap, const uint32_t* __restrict__ rowoff,
+                                                      uint32_t* fill, uint64_t* bucket) {
     const int lane = threadIdx.x & 31;
     const long long chunks = (m + kEmitChunk - 1) / kEmitChunk;
     for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32; c < chunks;
@@ -223,16 +204,11 @@ __global__ void __launch_bounds__(kThreads) emit_wide(int n, long long m, const 
             const int beg = xadj[v], end = xadj[v + 1];
             if (end - beg <= kEmitLaneDeg) continue;
             const int s = (int)std::max<long long>(lo, beg), e = (int)std::min<long long>(hi, end);
-            const uint32_t own = (uint32_t)cmap[v];
-            emit_range<true>(s + lane, e, 32, own, (uint64_t)own << tb, adjncy, adjwgt, cmap, ekey, eval, wpos + v);
+            emit_range(s + lane, e, 32, (uint32_t)cmap[v], adjncy, adjwgt, cmap, rowoff, fill, bucket);
         }
     }
 }
 
-__global__ void wide_counts(int n, const int* __restrict__ xadj, const int* __restrict__ wpos, uint32_t* vcount) {
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
-        if (xadj[v + 1] - xadj[v] > kEmitLaneDeg) vcount[v] = (uint32_t)(wpos[v] - xadj[v]);
-}
 
 // entries of vertex v move from its CSR range to voff[v] in the sort input
 // (one thread per vertex; vertices with many entries are copied by the warp)
@@ -292,49 +268,6 @@ __global__ void reduce_runs(long long E, const uint64_t* __restrict__ K, const u
 // ---- segmented merge: entries bucketed by coarse source row, each row
 // sorted and merged on its own
 
-// rowsz[cmap[v]] += vcount[v]
-__global__ void row_sizes(int n, const int* __restrict__ cmap, const uint32_t* __restrict__ vcount,
-                          uint32_t* rowsz) {
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-        const uint32_t c = vcount[v];
-        if (c) atomicAdd(&rowsz[cmap[v]], c);
-    }
-}
-
-// Moves vertex v's entries to its coarse row's bucket as (cv << 32 | w);
-// vertices with many entries are copied by the warp.  The order inside a
-// bucket depends on the atomics; the per-row sort below removes it.
-__global__ void scatter_rows(int n, const int* __restrict__ xadj, const int* __restrict__ cmap,
-                             const uint32_t* __restrict__ vcount, const uint32_t* __restrict__ rowoff,
-                             uint32_t* rowfill, const uint64_t* __restrict__ ekey,
-                             const uint32_t* __restrict__ eval, uint64_t mask, uint64_t* bucket) {
-    const int lane = threadIdx.x & 31;
-    for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
-        const int v = (int)(base + threadIdx.x);
-        const uint32_t cnt = v < n ? vcount[v] : 0u;
-        long long dst = 0;
-        if (cnt) {
-            const int c = cmap[v];
-            dst = (long long)rowoff[c] + atomicAdd(&rowfill[c], cnt);
-        }
-        const bool wide = cnt > 64;
-        unsigned wm = __ballot_sync(0xffffffffu, wide);
-        while (wm) {
-            const int s = __ffs(wm) - 1;
-            wm &= wm - 1;
-            const int hv = __shfl_sync(0xffffffffu, v, s);
-            const uint32_t hc = __shfl_sync(0xffffffffu, cnt, s);
-            const long long hd = __shfl_sync(0xffffffffu, dst, s);
-            const long long src = xadj[hv];
-            for (uint32_t i = lane; i < hc; i += 32)
-                bucket[hd + i] = ((ekey[src + i] & mask) << 32) | eval[src + i];
-        }
-        if (wide || cnt == 0) continue;
-        const long long src = xadj[v];
-        for (uint32_t i = 0; i < cnt; ++i) bucket[dst + i] = ((ekey[src + i] & mask) << 32) | eval[src + i];
-    }
-}
-
 constexpr int kSegMax = 1024;       // rows up to this many entries merge in shared memory
 constexpr int kMergeWarps = 4;
 
@@ -343,14 +276,14 @@ constexpr int kMergeWarps = 4;
 // the start of the bucket; ucnt[row] = their number.  Longer rows are left
 // for the global path (bigsz[row] = their size).
 __global__ void __launch_bounds__(kMergeWarps * 32) merge_rows(int nc, const uint32_t* __restrict__ rowoff,
-                                                                uint64_t* bucket, uint32_t* ucnt,
-                                                                uint32_t* bigsz) {
+                                                                const uint32_t* __restrict__ fill, uint64_t* bucket,
+                                                                uint32_t* ucnt, uint32_t* bigsz) {
     __shared__ uint64_t buf[kMergeWarps][kSegMax];
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     uint64_t* b = buf[wp];
     for (long long r = (long long)blockIdx.x * kMergeWarps + wp; r < nc; r += (long long)gridDim.x * kMergeWarps) {
         const long long beg = rowoff[r];
-        const int s = (int)(rowoff[r + 1] - beg);
+        const int s = (int)fill[r];
         if (s > kSegMax) {
             if (lane == 0) { bigsz[r] = (uint32_t)s; ucnt[r] = 0; }
             continue;
@@ -358,7 +291,18 @@ __global__ void __launch_bounds__(kMergeWarps * 32) merge_rows(int nc, const uin
         if (lane == 0) bigsz[r] = 0;
         int P = 1;
         while (P < s) P <<= 1;
-        if (P <= 64) {
+        if (P <= 32) {
+            // bitonic sort in registers, one element per lane
+            uint64_t x = lane < s ? bucket[beg + lane] : ~0ull;
+            for (int k = 2; k <= 32; k <<= 1)
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    const uint64_t y = __shfl_xor_sync(0xffffffffu, x, j);
+                    const bool lower = (lane & j) == 0, up = (lane & k) == 0;
+                    x = (lower == up) ? (x < y ? x : y) : (x > y ? x : y);
+                }
+            b[lane] = x;
+            __syncwarp();
+        } else if (P <= 64) {
             // bitonic sort in registers: element i = lane + 32 r, r = 0, 1
             uint64_t x0 = lane < s ? bucket[beg + lane] : ~0ull;
             uint64_t x1 = lane + 32 < s ? bucket[beg + lane + 32] : ~0ull;
@@ -510,55 +454,45 @@ void contract(Ctx& ctx, const DevGraph& g, const int* label, int* cmap, DevGraph
     const int nc = (int)ctx.pinned[0];
     int* cvw = ctx.hier.alloc<int>((size_t)nc);
     int* cxadj = ctx.hier.alloc<int>((size_t)nc + 1);
+    const long long m = g.m;
+    uint32_t* rowcap = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
+    uint32_t* rowoff = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
+    uint32_t* fill = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
     KB_CUDA(cudaMemsetAsync(cvw, 0, sizeof(int) * (size_t)nc, st));
-    make_cmap<<<grid_for(n, 256), 256, 0, st>>>(n, label, mm, pos, g.vwgt, cmap,
-                                                reinterpret_cast<uint32_t*>(cvw));
-    KB_LAUNCH();
+    KB_CUDA(cudaMemsetAsync(rowcap, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
+    KB_CUDA(cudaMemsetAsync(fill, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
+    {
+        PhaseScope ps(ctx, "contract_ids", 16.0 * n);
+        make_cmap<<<grid_for(n, 256), 256, 0, st>>>(n, label, mm, pos, g.vwgt, g.xadj, cmap,
+                                                    reinterpret_cast<uint32_t*>(cvw), rowcap);
+        KB_LAUNCH();
+        // bucket of coarse row c: [rowoff[c], rowoff[c] + its members' degrees)
+        exclusive_scan_u32(rowcap, rowoff, (long long)nc + 1, nullptr, st, ctx.scratch);
+    }
     int tb = 1;
     while ((1LL << tb) < (long long)nc) ++tb;
-    // 2. emission into each vertex's CSR range
-    const long long m = g.m;
-    uint64_t* ekey = ctx.scratch.alloc<uint64_t>((size_t)std::max<long long>(m, 1));
-    uint32_t* eval = ctx.scratch.alloc<uint32_t>((size_t)std::max<long long>(m, 1));
-    uint32_t* vcount = ctx.scratch.alloc<uint32_t>((size_t)n + 1);
-    int* wpos = ctx.scratch.alloc<int>((size_t)n + 1);
+    // 2. emission straight into the coarse rows' buckets (at most m entries)
+    uint64_t* bucket = ctx.scratch.alloc<uint64_t>((size_t)std::max<long long>(m, 1));
     {
         PhaseScope ps(ctx, "contract_emit", (g.unit_weights ? 8.0 : 12.0) * m + 8.0 * n);
         if (g.unit_weights)
-            emit_kernel<true><<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, g.adjncy, g.adjwgt, cmap, ekey,
-                                                                          eval, vcount, wpos, tb);
+            emit_kernel<true><<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, g.adjncy, g.adjwgt, cmap, rowoff,
+                                                                          fill, bucket);
         else
-            emit_kernel<false><<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, g.adjncy, g.adjwgt, cmap, ekey,
-                                                                           eval, vcount, wpos, tb);
+            emit_kernel<false><<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, g.adjncy, g.adjwgt, cmap, rowoff,
+                                                                           fill, bucket);
         KB_LAUNCH();
         if (g.maxdeg > kEmitLaneDeg) {
             const long long chunks = (m + kEmitChunk - 1) / kEmitChunk;
             emit_wide<<<grid_for(32LL * chunks, kThreads), kThreads, 0, st>>>(n, m, g.xadj, g.adjncy, g.adjwgt, cmap,
-                                                                           ekey, eval, wpos, tb);
-            KB_LAUNCH();
-            wide_counts<<<grid_for(n, 256), 256, 0, st>>>(n, g.xadj, wpos, vcount);
+                                                                           rowoff, fill, bucket);
             KB_LAUNCH();
         }
     }
-    // 3. bucket the entries by coarse source row (at most m of them)
-    uint32_t* rowsz = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
-    uint32_t* rowoff = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
     uint32_t* ucnt = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
     uint32_t* bigsz = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
     uint32_t* bigoff = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
-    uint64_t* bucket = ctx.scratch.alloc<uint64_t>((size_t)std::max<long long>(m, 1));
     uint32_t* big = reinterpret_cast<uint32_t*>(ctx.dscalars + 16);  // [16] long-row entries
-    {
-        PhaseScope ps(ctx, "contract_bucket", 8.0 * n + 20.0 * m);
-        KB_CUDA(cudaMemsetAsync(rowsz, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
-        row_sizes<<<grid_for(n, 256), 256, 0, st>>>(n, cmap, vcount, rowsz);
-        KB_LAUNCH();
-        exclusive_scan_u32(rowsz, rowoff, (long long)nc + 1, nullptr, st, ctx.scratch);
-        KB_CUDA(cudaMemsetAsync(rowsz, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
-        scatter_rows<<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, cmap, vcount, rowoff, rowsz, ekey, eval,
-                                                                 (1ull << tb) - 1ull, bucket);
-        KB_LAUNCH();
-    }
     // 4. merge each row: shared-memory sort for rows up to kSegMax entries
     {
         PhaseScope ps(ctx, "contract_merge", 16.0 * m);
@@ -566,7 +500,7 @@ void contract(Ctx& ctx, const DevGraph& g, const int* label, int* cmap, DevGraph
         // ucnt / bigsz have nc + 1 entries (the scans read the last one)
         KB_CUDA(cudaMemsetAsync(ucnt, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
         KB_CUDA(cudaMemsetAsync(bigsz, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
-        merge_rows<<<gb, kMergeWarps * 32, 0, st>>>(nc, rowoff, bucket, ucnt, bigsz);
+        merge_rows<<<gb, kMergeWarps * 32, 0, st>>>(nc, rowoff, fill, bucket, ucnt, bigsz);
         KB_LAUNCH();
         exclusive_scan_u32(bigsz, bigoff, (long long)nc + 1, big, st, ctx.scratch);
     }
