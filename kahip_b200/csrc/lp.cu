@@ -71,6 +71,8 @@ struct SweepArgs {
                                         // strictly increasing targets (clustering round 0)
     const uint32_t* tie;                // singletons: hash32(ks_tie, u) per vertex
     int all_fit;                        // singletons: every neighbour cluster fits (2 max c(v) < bound)
+    int admit_all;                      // CLUSTER: every target takes all its proposers
+                                        // (max c(v) (max degree + 1) < bound): no admission data
     unsigned long long* work;           // [0] vertices, [1] edges
     int* err;                           // set when an invariant breaks
     // BALANCE
@@ -141,8 +143,10 @@ __device__ bool decide_emit(const SweepArgs& a, int v, uint32_t own, uint32_t cv
     if (MODE == CLUSTER) {
         if (id == kEmpty || (uint32_t)(key >> 32) <= conn_own) return false;
         a.pt[v] = (int)id;
-        atomicAdd(&a.inc[id], cv);
-        atomicMin(&a.minv[id], v);
+        if (!a.admit_all) {
+            atomicAdd(&a.inc[id], cv);
+            atomicMin(&a.minv[id], v);
+        }
     } else if (MODE == REFINE) {
         uint32_t base = a.lw[own] <= a.bound ? conn_own : 0u;
         if (id == kEmpty || (uint32_t)(key >> 32) <= base) return false;
@@ -706,14 +710,17 @@ __global__ void cluster_decide(SList pl, const int* hpl, const unsigned* hpc, in
     }
 }
 
+// reset = 0: no admission data was gathered (every proposal is admitted)
 __global__ void cluster_apply(SList pl, const int* hpl, const unsigned* hpc, const int* pt, const int* vwgt,
-                              int* label, uint32_t* cw, uint32_t* inc, int* minv) {
+                              int* label, uint32_t* cw, uint32_t* inc, int* minv, int reset) {
     FOR_EACH_PROPOSAL(pl, hpl, hpc, v) {
         int t = pt[v];
         if (t == -1) continue;
         int b = t >= 0 ? t : -2 - t;
-        inc[b] = 0;
-        minv[b] = INT_MAX;
+        if (reset) {
+            inc[b] = 0;
+            minv[b] = INT_MAX;
+        }
         if (t < 0) continue;
         uint32_t cv = (uint32_t)vwgt[v];
         atomicSub(&cw[label[v]], cv);
@@ -993,6 +1000,10 @@ void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* la
         a.singletons = (r == 0 && sorted_rows) ? 1 : 0;
         a.tie = nullptr;
         a.all_fit = 0;
+        // round 0: a target's proposers are its neighbours, so with
+        // max c(v) (max degree + 1) < bound every target takes them all
+        a.admit_all = (r == 0 && (unsigned long long)g.maxvw * ((unsigned long long)g.maxdeg + 1) <
+                                     (unsigned long long)a.bound) ? 1 : 0;
         if (a.singletons && g.n > 0) {
             uint32_t* tie = ctx.scratch.alloc<uint32_t>(n);
             tie_hash_kernel<<<(int)std::min<long long>(div_up(g.n, kThreads), (long long)kNumSMs * 16), kThreads, 0,
@@ -1005,11 +1016,13 @@ void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* la
             a.s = s;
             launch_sweep<CLUSTER>(ctx, g, a, b, sweep_bytes(g, 1.0 / a.S));
             PhaseScope ps(ctx, "lp_cluster_admit", 0);
-            cluster_decide<<<admit_blocks(), kThreads, 0, st>>>(b.plist, b.hplist, a.hpcount, b.pt, cw, inc, minv,
-                                                                a.bound);
-            KB_LAUNCH();
+            if (!a.admit_all) {
+                cluster_decide<<<admit_blocks(), kThreads, 0, st>>>(b.plist, b.hplist, a.hpcount, b.pt, cw, inc, minv,
+                                                                    a.bound);
+                KB_LAUNCH();
+            }
             cluster_apply<<<admit_blocks(), kThreads, 0, st>>>(b.plist, b.hplist, a.hpcount, b.pt, g.vwgt, label, cw,
-                                                               inc, minv);
+                                                               inc, minv, a.admit_all ? 0 : 1);
             KB_LAUNCH();
         }
     }
