@@ -78,3 +78,19 @@ def test_evolution_does_not_depend_on_workers(N, graphs):
     runs = [N.kaffpae(g, kn, 5, 2, 3, workers=w) for w in (1, 2, 3)]
     for r in runs[1:]:
         assert r[1] == runs[0][1] and np.array_equal(r[2], runs[0][2]) and np.array_equal(r[3], runs[0][3])
+
+
+@pytest.mark.parametrize("gname", ["empty", "single", "isolated", "star", "two_components", "big_star"])
+@pytest.mark.parametrize("k", [2, 8, 100])
+def test_combine_edge_cases(N, O, gname, k):
+    from conftest import csr_from_edges
+    from test_gpu_parity import EDGE_GRAPHS
+    n, edges = EDGE_GRAPHS[gname]
+    g = csr_from_edges(n, edges)
+    pa = O.kaffpa(g, k, 0.03, 1, 0)[1]
+    pb = O.kaffpa(g, k, 0.03, 2, 1)[1]
+    kn_o = O.knobs(g, k, 0.03, 3, 0)
+    kn_d = N.derive_knobs(g["n"], g["vwgt"], k, 0.03, 3, 0)
+    cut_o, part_o, _ = O.kaffpa_combine(g, kn_o, pa, pb)
+    _, cut_d, part_d = N.kaffpa_combine(g, kn_d, pa, pb)
+    assert cut_d == cut_o and np.array_equal(part_d, part_o)

@@ -175,11 +175,12 @@ EDGE_GRAPHS = {
 
 @pytest.mark.parametrize("gname", list(EDGE_GRAPHS))
 @pytest.mark.parametrize("k", [1, 2, 3, 8, 100])
-def test_edge_cases(N, O, gname, k):
+@pytest.mark.parametrize("mode", [0, 1])
+def test_edge_cases(N, O, gname, k, mode):
     n, edges = EDGE_GRAPHS[gname]
     g = csr_from_edges(n, edges)
-    cut_o, part_o, st_o = O.kaffpa(g, k, 0.03, 0, 0)
-    rc, cut_p, part_p = N.kaffpa_ex(g["xadj"], g["adjncy"], k, 0.03, 0, 0)
+    cut_o, part_o, st_o = O.kaffpa(g, k, 0.03, 0, mode)
+    rc, cut_p, part_p = N.kaffpa_ex(g["xadj"], g["adjncy"], k, 0.03, 0, mode)
     assert cut_p == cut_o
     assert np.array_equal(part_p, part_o)
     if n:
