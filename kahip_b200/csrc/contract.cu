@@ -404,6 +404,34 @@ __global__ void reduce_big(long long E, const uint64_t* __restrict__ K, const ui
     }
 }
 
+// Degree statistics of the coarse graph from its row lengths, before the
+// rows are copied: [0] max degree, [1] isolated nodes, [2] their largest
+// weight, [3] largest node weight (what degree_stats computes).
+__global__ void coarse_stats(int nc, const uint32_t* __restrict__ ucnt, const int* __restrict__ cvw, unsigned* out) {
+    unsigned md = 0, iso = 0, wi = 0, wa = 0;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < nc; r += gridDim.x * blockDim.x) {
+        const unsigned d = ucnt[r], w = (unsigned)cvw[r];
+        md = max(md, d);
+        wa = max(wa, w);
+        if (d == 0) {
+            ++iso;
+            wi = max(wi, w);
+        }
+    }
+    for (int o = 16; o >= 1; o >>= 1) {
+        md = max(md, __shfl_xor_sync(0xffffffffu, md, o));
+        iso += __shfl_xor_sync(0xffffffffu, iso, o);
+        wi = max(wi, __shfl_xor_sync(0xffffffffu, wi, o));
+        wa = max(wa, __shfl_xor_sync(0xffffffffu, wa, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (md) atomicMax(out, md);
+        if (iso) atomicAdd(out + 1, iso);
+        if (wi) atomicMax(out + 2, wi);
+        if (wa) atomicMax(out + 3, wa);
+    }
+}
+
 // Warp per row: the distinct entries move from the bucket to the coarse CSR.
 __global__ void copy_rows(int nc, const uint32_t* __restrict__ rowoff, const uint32_t* __restrict__ ucnt,
                           const int* __restrict__ cxadj, const uint64_t* __restrict__ bucket, int* cadj, int* cw) {
@@ -431,6 +459,7 @@ void contract(Ctx& ctx, const DevGraph& g, const int* label, int* cmap, DevGraph
         int* cx = ctx.hier.alloc<int>(1);
         KB_CUDA(cudaMemsetAsync(cx, 0, sizeof(int), st));
         out = DevGraph{};
+        out.maxvw = 0;
         out.xadj = cx;
         *out_xadj = cx;
         *out_adjncy = *out_adjwgt = *out_vwgt = nullptr;
@@ -504,8 +533,24 @@ void contract(Ctx& ctx, const DevGraph& g, const int* label, int* cmap, DevGraph
         KB_LAUNCH();
         exclusive_scan_u32(bigsz, bigoff, (long long)nc + 1, big, st, ctx.scratch);
     }
-    KB_CUDA(cudaMemcpyAsync(ctx.pinned, big, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    KB_CUDA(cudaStreamSynchronize(st));
+    // row lengths -> coarse xadj and the coarse degree statistics, read back
+    // with the long-row count in one synchronisation (redone below in the
+    // rare case of long rows, whose lengths the global path still has to add)
+    unsigned* stats = reinterpret_cast<unsigned*>(ctx.dscalars + 40);  // [40..43]
+    uint32_t* mct = reinterpret_cast<uint32_t*>(ctx.dscalars + 17);    // [17] coarse entries
+    auto rows_and_stats = [&]() {
+        PhaseScope ps(ctx, "contract_rows", 8.0 * nc);
+        exclusive_scan_u32(ucnt, reinterpret_cast<uint32_t*>(cxadj), (long long)nc + 1, mct, st, ctx.scratch);
+        KB_CUDA(cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned), st));
+        coarse_stats<<<grid_for(nc, 256), 256, 0, st>>>(nc, ucnt, cvw, stats);
+        KB_LAUNCH();
+        // pinned[0] long-row entries, [1] coarse entries, [2..5] statistics
+        KB_CUDA(cudaMemcpyAsync(ctx.pinned, big, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        KB_CUDA(cudaMemcpyAsync(ctx.pinned + 1, mct, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        KB_CUDA(cudaMemcpyAsync(ctx.pinned + 2, stats, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        KB_CUDA(cudaStreamSynchronize(st));
+    };
+    rows_and_stats();
     const long long EB = ctx.pinned[0];
     if (EB > 0) {
         // longer rows: global LSD radix sort of their entries, then reduce
@@ -530,15 +575,12 @@ void contract(Ctx& ctx, const DevGraph& g, const int* label, int* cmap, DevGraph
         reduce_big<<<grid_for(EB, 256), 256, 0, st>>>(EB, K, V, uidx, ufirst, rowoff, tb, bucket, ucnt);
         KB_LAUNCH();
         ctx.scratch.release(mk2);
+        rows_and_stats();
     }
-    // 5. row lengths -> coarse xadj, then the rows themselves
-    {
-        PhaseScope ps(ctx, "contract_rows", 4.0 * nc);
-        exclusive_scan_u32(ucnt, reinterpret_cast<uint32_t*>(cxadj), (long long)nc + 1, big, st, ctx.scratch);
-    }
-    KB_CUDA(cudaMemcpyAsync(ctx.pinned, big, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    KB_CUDA(cudaStreamSynchronize(st));
-    const long long mc = (long long)ctx.pinned[0];
+    // 5. the rows themselves
+    const long long mc = (long long)ctx.pinned[1];
+    const int c_maxdeg = (int)ctx.pinned[2];
+    const unsigned c_iso = ctx.pinned[3], c_isow = ctx.pinned[4], c_maxvw = ctx.pinned[5];
     int* cadj = ctx.hier.alloc<int>((size_t)std::max<long long>(mc, 1));
     int* cwgt = ctx.hier.alloc<int>((size_t)std::max<long long>(mc, 1));
     {
@@ -549,6 +591,10 @@ void contract(Ctx& ctx, const DevGraph& g, const int* label, int* cmap, DevGraph
     out = DevGraph{};
     out.n = nc;
     out.m = mc;
+    out.maxdeg = c_maxdeg;
+    out.iso_count = c_iso;
+    out.iso_wmax = c_isow;
+    out.maxvw = c_maxvw;
     out.rows_sorted = 1;  // rows come out sorted by target, without repeats
     out.xadj = cxadj;
     out.adjncy = cadj;

@@ -199,9 +199,9 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
             }
             Level c;
             int *cx, *ca, *cw, *cv;
+            // contraction also fills the coarse graph's degree statistics
             contract(ctx, f, label, lv[L].cmap, c.g, &cx, &ca, &cw, &cv);
             ctx.scratch.release(mk);
-            degree_stats(ctx, c.g);
             if (combine) {
                 int* q1 = ctx.hier.alloc<int>((size_t)std::max(c.g.n, 1));
                 int* q2 = ctx.hier.alloc<int>((size_t)std::max(c.g.n, 1));
