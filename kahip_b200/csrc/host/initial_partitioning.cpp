@@ -178,6 +178,17 @@ public:
         sift_up(pos_[v], key);
         sift_down(pos_[v], key);
     }
+    // after key[v] grew / shrank: one direction suffices
+    void increased(int v, const std::vector<long long>& key) { sift_up(pos_[v], key); }
+    void decreased(int v, const std::vector<long long>& key) { sift_down(pos_[v], key); }
+    // heap of the given nodes (none of them queued), built bottom-up
+    void build(const std::vector<int>& nodes, const std::vector<long long>& key) {
+        for (int v : nodes) {
+            pos_[v] = (int)heap_.size();
+            heap_.push_back(v);
+        }
+        for (int i = (int)heap_.size() / 2 - 1; i >= 0; --i) sift_down(i, key);
+    }
     void clear() {
         for (int v : heap_) pos_[v] = -1;
         heap_.clear();
@@ -286,7 +297,7 @@ void grow_region(const HostGraph& g, int start, uint64_t target0, uint64_t max0,
             int u = g.adjncy[e];
             if (side[u] == 0 || skipped[u]) continue;
             key[u] += 2LL * g.adjwgt[e];
-            if (heap.contains(u)) heap.changed(u, key);
+            if (heap.contains(u)) heap.increased(u, key);
             else heap.push(u, key);
         }
     }
@@ -299,18 +310,20 @@ long long fm_refine(const HostGraph& g, std::vector<char>& side, const Limits& l
     uint64_t w[2] = {0, 0};
     for (int v = 0; v < g.n; ++v) w[(int)side[v]] += (uint64_t)g.vwgt[v];
     thread_local std::vector<char> locked;
-    thread_local std::vector<int> log;
+    thread_local std::vector<int> log, boundary;
     locked.assign(g.n, 0);
     log.clear();
     long long cut = cut_of(g, side);
     for (int pass = 0; pass < passes; ++pass) {
+        boundary.clear();
         for (int v = 0; v < g.n; ++v) {
             long long inside = 0, outside = 0;
             for (int e = g.xadj[v]; e < g.xadj[v + 1]; ++e)
                 (side[g.adjncy[e]] == side[v] ? inside : outside) += g.adjwgt[e];
             key[v] = outside - inside;
-            if (outside > 0) heap.push(v, key);
+            if (outside > 0) boundary.push_back(v);
         }
+        heap.build(boundary, key);
         log.clear();
         size_t best_len = 0;
         int stall = 0;
@@ -329,10 +342,12 @@ long long fm_refine(const HostGraph& g, std::vector<char>& side, const Limits& l
             for (int e = g.xadj[v]; e < g.xadj[v + 1]; ++e) {
                 int u = g.adjncy[e];
                 if (locked[u]) continue;
-                long long d = 2LL * g.adjwgt[e];
-                key[u] += side[u] == to ? -d : d;
-                if (heap.contains(u)) heap.changed(u, key);
-                else heap.push(u, key);
+                const long long d = 2LL * g.adjwgt[e];
+                const bool drop = side[u] == to;
+                key[u] += drop ? -d : d;
+                if (!heap.contains(u)) heap.push(u, key);
+                else if (drop) heap.decreased(u, key);
+                else heap.increased(u, key);
             }
             uint64_t ov = lim.overload(w);
             if (ov < best_ov || (ov == best_ov && cur < best_cut)) {
