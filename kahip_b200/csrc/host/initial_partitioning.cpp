@@ -620,7 +620,15 @@ thread_local int t_spawn_limit = -1;
 void set_ip_thread_limit(int depth) { t_spawn_limit = depth; }
 
 void initial_partition(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
-                       const Knobs& kn, int* part) {
+                       const Knobs& knobs, int* part) {
+    // a dense coarsest graph (average degree > 64: skewed-degree inputs whose
+    // coarsening stalls) gets one growing try and one FM pass per bisection;
+    // its cut hardly depends on them and the FM's cost grows with the degree
+    Knobs kn = knobs;
+    if ((long long)xadj[n] > 64LL * n) {
+        kn.ip_tries = std::min(kn.ip_tries, 1);
+        kn.ip_fm_passes = std::min(kn.ip_fm_passes, 1);
+    }
     HostGraph g;
     g.n = n;
     g.xadj.assign(xadj, xadj + n + 1);

@@ -1303,9 +1303,18 @@ static void rb(const or_graph* g, const int* orig, int k, int offset, const or_k
     sub_free(&R);
 }
 
-void or_initial_partition(const or_graph* g, const or_knobs* kn, int* part) {
+void or_initial_partition(const or_graph* g, const or_knobs* knobs, int* part) {
     /* initial_partitioning.cpp:66-99: several repetitions, keep the best cut */
     const int n = g->n;
+    /* a dense coarsest graph (average degree > 64: skewed-degree inputs whose
+     * coarsening stalls) gets one growing try and one FM pass per bisection;
+     * its cut hardly depends on them and the FM's cost grows with the degree */
+    or_knobs dense = *knobs;
+    if ((long long)g->xadj[n] > 64LL * n) {
+        dense.ip_tries = dense.ip_tries < 1 ? dense.ip_tries : 1;
+        dense.ip_fm_passes = dense.ip_fm_passes < 1 ? dense.ip_fm_passes : 1;
+    }
+    const or_knobs* kn = &dense;
     int* orig = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
     int* cand = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
     for (int v = 0; v < n; ++v) orig[v] = v;

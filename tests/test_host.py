@@ -33,6 +33,27 @@ def test_initial_partitioner_matches_oracle(graphs, gen, k, mode, seed):
     assert a.min() >= 0 and a.max() < k
 
 
+@pytest.mark.parametrize("k,mode", [(8, 0), (16, 1)])
+def test_initial_partitioner_dense_graph_matches_oracle(k, mode):
+    # average degree > 64: one growing try and one FM pass per bisection, in both
+    from conftest import csr_from_edges
+    from kahip_b200 import native
+    rng = np.random.default_rng(k)
+    n = 400
+    edges = set()
+    while len(edges) < 14000:
+        u, v = rng.integers(0, n, 2)
+        if u != v:
+            edges.add((min(u, v), max(u, v)))
+    g = csr_from_edges(n, sorted(edges), weights=list(rng.integers(1, 9, len(edges))))
+    g["vwgt"] = rng.integers(1, 5, n).astype(np.int32)
+    assert g["m"] > 64 * n
+    kn = O.knobs(g, k, 0.03, 1, mode)
+    a = O.initial_partition(g, kn)
+    b = native.initial_partition(g, native.derive_knobs(g["n"], g["vwgt"], k, 0.03, 1, mode))
+    assert np.array_equal(a, b)
+
+
 def test_generators_are_symmetric_and_sorted(graphs):
     for g in (graphs.rgg2d(5000, seed=1), graphs.rgg3d(4000, seed=2), graphs.rmat(12, seed=3),
               graphs.grid2d(50, 40)):
