@@ -601,8 +601,11 @@ void recurse(const Knobs& kn, const HostGraph& g, const std::vector<int>& orig, 
     Bisector bis{kn};
     std::vector<char> side = bis.multilevel(g, t0, lim, (int)(node * 64u + (uint32_t)rep), par);
     std::vector<int> lo, ro;
-    HostGraph L = induced(g, orig, side, 0, lo);
-    HostGraph R = induced(g, orig, side, 1, ro);
+    HostGraph L, R;
+    for_each_index(2, par && g.n > 1024, [&](int h) {
+        if (h == 0) L = induced(g, orig, side, 0, lo);
+        else R = induced(g, orig, side, 1, ro);
+    });
     side.clear();
     side.shrink_to_fit();
     // out[] entries written by the two halves are disjoint
