@@ -210,59 +210,10 @@ __global__ void __launch_bounds__(kThreads) emit_wide(int n, long long m, const 
 }
 
 
-// entries of vertex v move from its CSR range to voff[v] in the sort input
-// (one thread per vertex; vertices with many entries are copied by the warp)
-__global__ void compact_vertices(int n, const int* __restrict__ xadj, const uint32_t* __restrict__ vcount,
-                                 const uint32_t* __restrict__ voff, const uint64_t* __restrict__ ekey,
-                                 const uint32_t* __restrict__ eval, uint64_t* K, uint32_t* V) {
-    const int lane = threadIdx.x & 31;
-    for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
-        const int v = (int)(base + threadIdx.x);
-        const uint32_t cnt = v < n ? vcount[v] : 0u;
-        const bool wide = cnt > 64;
-        unsigned wm = __ballot_sync(0xffffffffu, wide);
-        while (wm) {
-            const int s = __ffs(wm) - 1;
-            wm &= wm - 1;
-            const int hv = __shfl_sync(0xffffffffu, v, s);
-            const uint32_t hc = __shfl_sync(0xffffffffu, cnt, s);
-            const long long src = xadj[hv], dst = voff[hv];
-            for (uint32_t i = lane; i < hc; i += 32) {
-                K[dst + i] = ekey[src + i];
-                V[dst + i] = eval[src + i];
-            }
-        }
-        if (v >= n || wide) continue;
-        const long long src = xadj[v];
-        const long long dst = voff[v];
-        for (uint32_t i = 0; i < cnt; ++i) {
-            K[dst + i] = ekey[src + i];
-            V[dst + i] = eval[src + i];
-        }
-    }
-}
-
 __global__ void head_flags(long long E, const uint64_t* __restrict__ K, uint32_t* h) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < E;
          i += (long long)gridDim.x * blockDim.x)
         h[i] = (i == 0 || K[i] != K[i - 1]) ? 1u : 0u;
-}
-
-__global__ void reduce_runs(long long E, const uint64_t* __restrict__ K, const uint32_t* __restrict__ V,
-                            const uint32_t* __restrict__ uidx, int tb, int* cadj, int* cw,
-                            uint32_t* rowcnt) {
-    const uint64_t mask = (1ull << tb) - 1ull;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < E;
-         i += (long long)gridDim.x * blockDim.x) {
-        uint64_t k = K[i];
-        if (i > 0 && K[i - 1] == k) continue;
-        uint32_t s = V[i];
-        for (long long j = i + 1; j < E && K[j] == k; ++j) s += V[j];
-        uint32_t u = uidx[i];
-        cadj[u] = (int)(k & mask);
-        cw[u] = (int)s;
-        atomicAdd(&rowcnt[k >> tb], 1u);
-    }
 }
 
 // ---- segmented merge: entries bucketed by coarse source row, each row
