@@ -103,29 +103,59 @@ __global__ void init_labels_kernel(int n, const int* __restrict__ vwgt, int* lab
     }
 }
 
+// One pass over the graph, a warp per 32 consecutive vertices: the warp
+// walks the entry range of its vertices in coalesced 32-entry chunks.
+// Flags: 1 target out of range, 2 negative edge weight, 4 negative node
+// weight, 8 xadj not starting at 0 or not monotone (or outside [0, m]), 16
+// some edge weight other than 1, 32 some row not listing its targets in
+// strictly increasing order (not an error; lets the first clustering round
+// skip aggregation).  *wsum = the node weights' sum (32-bit, wrapping as the
+// reference's NodeWeight does).
 __global__ void check_graph_kernel(int n, long long m, const int* __restrict__ xadj,
                                    const int* __restrict__ adjncy, const int* __restrict__ adjwgt,
                                    const int* __restrict__ vwgt, int* flags, unsigned* wsum) {
     int f = 0;
     unsigned w = 0;
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < m;
-         e += (long long)gridDim.x * blockDim.x) {
-        int t = adjncy[e];
-        if (t < 0 || t >= n) f |= 1;
-        const int w = adjwgt[e];
-        if (w < 0) f |= 2;
-        if (w != 1) f |= 16;
-    }
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-        if (vwgt[v] < 0) f |= 4;
-        const int b = xadj[v], e1 = xadj[v + 1];
-        if (e1 < b) f |= 8;
-        w += (unsigned)vwgt[v];
-        // rows listing their targets in strictly increasing order (not an
-        // error; lets the first clustering round skip aggregation)
-        if (!(f & 32) && b >= 0 && e1 <= m)
-            for (int e = b + 1; e < e1; ++e)
-                if (adjncy[e] <= adjncy[e - 1]) { f |= 32; break; }
+    const int lane = threadIdx.x & 31;
+    const long long warps = (long long)gridDim.x * (blockDim.x / 32);
+    for (long long g0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32 * 32; g0 < n; g0 += warps * 32) {
+        const long long v = g0 + lane;
+        const bool in = v < n;
+        long long x0 = 0, x1 = 0;
+        if (in) {
+            x0 = xadj[v];
+            x1 = xadj[v + 1];
+            const int vw = vwgt[v];
+            if (vw < 0) f |= 4;
+            w += (unsigned)vw;
+        }
+        const bool sane = !in || (x0 >= 0 && x0 <= x1 && x1 <= m);
+        if (!__all_sync(0xffffffffu, sane)) {
+            f |= 8;
+            continue;
+        }
+        const int last = (int)min(31LL, (long long)n - 1 - g0);
+        const long long lo = __shfl_sync(0xffffffffu, x0, 0), hi = __shfl_sync(0xffffffffu, x1, last);
+        int carry = 0;
+        for (long long base = lo; base < hi; base += 32) {
+            const long long e = base + lane;
+            const bool ein = e < hi;
+            int t = 0;
+            if (ein) {
+                t = adjncy[e];
+                const int wt = adjwgt[e];
+                if (t < 0 || t >= n) f |= 1;
+                if (wt < 0) f |= 2;
+                if (wt != 1) f |= 16;
+            }
+            // the row starts that fall into this chunk
+            const unsigned bit = (in && x0 >= base && x0 < base + 32) ? 1u << (int)(x0 - base) : 0u;
+            const unsigned starts = __reduce_or_sync(0xffffffffu, bit);
+            const int up = __shfl_up_sync(0xffffffffu, t, 1);
+            const int prev = lane == 0 ? carry : up;
+            if (ein && !((starts >> lane) & 1u) && t <= prev) f |= 32;
+            carry = __shfl_sync(0xffffffffu, t, 31);
+        }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && xadj[0] != 0) f |= 8;
     f = __reduce_or_sync(0xffffffffu, f);
@@ -201,7 +231,7 @@ int check_graph(Ctx& ctx, const DevGraph& g, uint32_t* total_weight) {
     int* d = ctx.dscalars + 2;  // [2] flags, [3] node weight sum
     KB_CUDA(cudaMemsetAsync(d, 0, 2 * sizeof(int), ctx.stream));
     if (g.m > 0 || g.n > 0) {
-        check_graph_kernel<<<grid_for(std::max<long long>(g.m, g.n), 256), 256, 0, ctx.stream>>>(
+        check_graph_kernel<<<grid_for(g.n, 256), 256, 0, ctx.stream>>>(
             g.n, g.m, g.xadj, g.adjncy, g.adjwgt, g.vwgt, d, reinterpret_cast<unsigned*>(d + 1));
         KB_LAUNCH();
     }

@@ -315,3 +315,33 @@ def test_jet_hub_rows(N, O):
         part = (np.arange(n) * k // n).astype(np.int32)
         assert np.array_equal(O.jet_refine(g, kn_o, part, kn_o.upper_bound, 1),
                               N.jet_refine(g, kn_p, part, kn_p.upper_bound, 1))
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_unsorted_rows_with_parallel_entries(N, O, graphs, mode):
+    # rows in arbitrary order, some edges listed twice (both directions): the
+    # device check must see that rows are not strictly increasing, so that
+    # clustering round 0 aggregates repeated targets like the oracle
+    g = graphs.rgg2d(1 << 13, seed=3)
+    rng = np.random.default_rng(1)
+    n = g["n"]
+    src = np.repeat(np.arange(n), np.diff(g["xadj"]))
+    dst = g["adjncy"]
+    upper = src < dst
+    us, vs = src[upper], dst[upper]
+    dup = rng.random(len(us)) < 0.15
+    us = np.concatenate([us, us[dup]])
+    vs = np.concatenate([vs, vs[dup]])
+    ws = rng.integers(1, 5, len(us))
+    a = np.concatenate([us, vs])
+    b = np.concatenate([vs, us])
+    w = np.concatenate([ws, ws])
+    order = np.lexsort((rng.random(len(a)), a))  # by source, random within a row
+    a, b, w = a[order], b[order], w[order]
+    xadj = np.concatenate([[0], np.cumsum(np.bincount(a, minlength=n))]).astype(np.int32)
+    h = {"n": n, "m": len(a), "xadj": xadj, "adjncy": b.astype(np.int32), "adjwgt": w.astype(np.int32),
+         "vwgt": np.ones(n, np.int32)}
+    cut_o, part_o, _ = O.kaffpa(h, 8, 0.03, 0, mode)
+    rc, cut_p, part_p = N.kaffpa_ex(h["xadj"], h["adjncy"], 8, 0.03, 0, mode, vwgt=h["vwgt"], adjwgt=h["adjwgt"])
+    assert cut_p == cut_o
+    assert np.array_equal(part_p, part_o)
