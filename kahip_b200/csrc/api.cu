@@ -23,6 +23,7 @@
 #include "knobs.h"
 #include "learned.cuh"
 #include "match.cuh"
+#include "combine.cuh"
 #include "evolve.cuh"
 #include "partitioner.cuh"
 #include "prims.cuh"
@@ -262,6 +263,8 @@ int run_host_in(Ctx& ctx, int n, const int* vwgt, const int* xadj, const int* ad
                     KB_CUDA(cudaMemcpyAsync(dpar + n, parent_b, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice,
                                             ctx.stream));
                 }
+                if (!parents_in_range(ctx, n, kn.k, dpar, dpar + n))
+                    throw InvalidInput("parent block id out of range");
             }
             double ms_h2d = ms_since(th);
             long long cut = 0;
@@ -344,9 +347,7 @@ int kb200_kaffpa_combine(int n, const int* vwgt, const int* xadj, const int* adj
         if (kn->coarsening < 0 || kn->coarsening > 2) return fail(KB_ERR_INVALID_INPUT, "unknown coarsening");
         if (!edgecut || (n > 0 && (!part || !part_a || !part_b)))
             return fail(KB_ERR_INVALID_INPUT, "edgecut/part/parents is NULL");
-        for (int v = 0; v < n; ++v)
-            if (part_a[v] < 0 || part_a[v] >= kn->k || part_b[v] < 0 || part_b[v] >= kn->k)
-                return fail(KB_ERR_INVALID_INPUT, "parent block id out of range");
+        // parent block ids are range-checked on the device after the upload
         int dev;
         if ((rc = current_device(&dev))) return rc;
         Lease lease(dev);

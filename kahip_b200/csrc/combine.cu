@@ -69,6 +69,14 @@ __global__ void filter_write(int n, const int* __restrict__ xadj, const int* __r
     }
 }
 
+__global__ void parents_check(int n, int k, const int* __restrict__ pa, const int* __restrict__ pb, int* bad) {
+    int f = 0;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x)
+        f |= (pa[v] < 0 || pa[v] >= k || pb[v] < 0 || pb[v] >= k) ? 1 : 0;
+    f = __reduce_or_sync(0xffffffffu, f);
+    if ((threadIdx.x & 31) == 0 && f) atomicOr(bad, 1);
+}
+
 __global__ void parents_down(int n, const int* __restrict__ cmap, const int* __restrict__ p1,
                              const int* __restrict__ p2, int* p1c, int* p2c) {
     for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
@@ -109,6 +117,18 @@ void filter_by_parents(Ctx& ctx, const DevGraph& f, const int* p1, const int* p2
     out.adjncy = fa;
     out.adjwgt = fw;
     degree_stats(ctx, out);
+}
+
+bool parents_in_range(Ctx& ctx, int n, int k, const int* pa, const int* pb) {
+    int* bad = ctx.dscalars + 44;  // [44] out-of-range flag
+    KB_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), ctx.stream));
+    if (n > 0) {
+        parents_check<<<grid_for(n), kThreads, 0, ctx.stream>>>(n, k, pa, pb, bad);
+        KB_LAUNCH();
+    }
+    KB_CUDA(cudaMemcpyAsync(ctx.pinned + 44, bad, sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    KB_CUDA(cudaStreamSynchronize(ctx.stream));
+    return ctx.pinned[44] == 0;
 }
 
 void parents_to_coarse(Ctx& ctx, int n, const int* cmap, const int* p1, const int* p2, int* p1c, int* p2c) {
