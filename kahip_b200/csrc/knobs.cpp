@@ -80,7 +80,10 @@ void derive_knobs_total(int n, uint32_t W, int k, double imbalance, int seed, in
     kn.rating_model = nullptr;
     kn.rating_fallback = 0.0;
     kn.rating_levels = 0;
-    kn.refinement = fast ? 0 : 1;        // eco and the thorough modes refine with Jet
+    // Jet (this library's FM counterpart) wherever the reference runs FM-based
+    // pair refinement: every mode but fast, and fast with k <= 8
+    // (app/configuration.h:108-118 disables quotient-graph refinement above 8)
+    kn.refinement = (fast && k > 8) ? 0 : 1;
     kn.jet_iters = 32;                   // Jet (Gilbert et al. 2023): patience 12, tolerance
     kn.jet_patience = 12;                // 0.25 of the own connection on the finest level,
     kn.jet_c0 = 1;                       // 0.75 on coarser ones

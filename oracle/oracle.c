@@ -113,7 +113,7 @@ void or_derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, 
     o->max_levels = 48;
     o->coarsening = 0;
     o->match_rounds = 16;
-    o->refinement = fast ? 0 : 1;
+    o->refinement = (fast && k > 8) ? 0 : 1; /* configuration.h:108-118: pair refinement up to k = 8 */
     o->jet_iters = 32;
     o->jet_patience = 12;
     o->jet_c0 = 1;

@@ -44,6 +44,7 @@ def test_jet_beats_lp_refinement(graphs):
     for g, k in ((graphs.rgg2d(1 << 15, seed=0), 16), (graphs.rgg3d(1 << 14, seed=1), 8),
                  (graphs.grid2d(150, 150), 32)):
         kn = O.knobs(g, k, 0.03, 0, 0)
+        kn.refinement = 0
         cut_lp, _, st_lp = O.kaffpa_knobs(g, kn)
         kn.refinement = 1
         cut_jet, part, st = O.kaffpa_knobs(g, kn)
