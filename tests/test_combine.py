@@ -91,3 +91,85 @@ def test_evolution_single_member_is_the_plain_partitioner(graphs):
     cut, part, hist = O.kaffpae(g, kn, 1, 2, 1)
     c0, p0, _ = O.kaffpa_knobs(g, kn)
     assert cut == c0 and np.array_equal(part, p0) and list(hist) == [c0] * 3
+
+
+def _evolve_restated(g, kn_base, P, G, W):
+    """The evolution loop restated in Python on top of the oracle's kaffpa and
+    combine (tournament of two hash-drawn members twice, offspring inserted in
+    order: dropped when worse than the worst member, else replacing the most
+    similar member among those not better), an independent check of
+    or_kaffpae's bookkeeping."""
+    n = g["n"]
+    src = np.repeat(np.arange(n), np.diff(g["xadj"]))
+    dst = g["adjncy"]
+    k = kn_base.k
+
+    def obj(p):
+        bw = O.block_weights(g, p, k).astype(np.int64)
+        return (int(np.maximum(bw - kn_base.final_bound, 0).sum()), O.edge_cut(g, p))
+
+    def fitter(objs, a, b):
+        if objs[a] < objs[b]:
+            return a
+        if objs[b] < objs[a]:
+            return b
+        return min(a, b)
+
+    pop, objs = [], []
+    for i in range(P):
+        kn = type(kn_base).from_buffer_copy(kn_base)
+        kn.seed = kn_base.seed + i
+        p = O.kaffpa_knobs(g, kn)[1]
+        pop.append(p)
+        objs.append(obj(p))
+    best = 0
+    for i in range(1, P):
+        best = fitter(objs, best, i)
+    hist = [objs[best][1]]
+    for t in range(G):
+        if P >= 2:
+            offs = []
+            for j in range(W):
+                ks = O.stream(kn_base.seed, 13, t, j)
+                x = [(O.hash32(ks, i) * P) >> 32 for i in range(4)]  # multiply-shift range
+                a = fitter(objs, x[0], x[1])
+                b = fitter(objs, x[2], x[3])
+                if b == a:
+                    b = x[3] if b == x[2] else x[2]
+                if b == a:
+                    b = (a + 1) % P
+                kn = type(kn_base).from_buffer_copy(kn_base)
+                kn.seed = kn_base.seed + P + t * W + j
+                child = O.kaffpa_combine(g, kn, pop[a], pop[b])[1]
+                offs.append((child, obj(child)))
+            for child, oc in offs:
+                worst = 0
+                for i in range(1, P):
+                    if objs[worst] < objs[i]:
+                        worst = i
+                if objs[worst] < oc:
+                    continue
+                pick, pd = -1, 0
+                for i in range(P):
+                    if objs[i] < oc:
+                        continue
+                    d = int(((pop[i][src] != pop[i][dst]) != (child[src] != child[dst])).sum())
+                    if pick < 0 or d < pd:
+                        pick, pd = i, d
+                pop[pick] = child
+                objs[pick] = oc
+        best = 0
+        for i in range(1, P):
+            best = fitter(objs, best, i)
+        hist.append(objs[best][1])
+    return pop[best], hist
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_evolution_matches_python_restatement(graphs, mode):
+    g = graphs.rgg2d(3000, seed=5)
+    kn = O.knobs(g, 4, 0.03, 7, mode)
+    cut, part, hist = O.kaffpae(g, kn, 4, 3, 2)
+    p2, h2 = _evolve_restated(g, kn, 4, 3, 2)
+    assert list(hist) == h2
+    assert np.array_equal(part, p2)
