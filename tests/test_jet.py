@@ -51,3 +51,81 @@ def test_jet_beats_lp_refinement(graphs):
         assert st.balanced
         wins += cut_jet < cut_lp
     assert wins == 3
+
+
+def _jet_restated(g, kn, part, bound, level):
+    """Jet refinement restated in Python (candidate choice with the tie
+    stream, afterburner against higher-priority candidates, moves, the
+    oracle's balance repair when overloaded, best partition by (overload,
+    cut)) -- an independent check of or_jet_refine's bookkeeping."""
+    n, k = g["n"], kn.k
+    xadj, adj, w, vw = g["xadj"], g["adjncy"], g["adjwgt"], g["vwgt"]
+    part = np.array(part, np.int32)
+
+    def quality(p):
+        bw = O.block_weights(g, p, k).astype(np.int64)
+        return int(np.maximum(bw - bound, 0).sum()), O.edge_cut(g, p)
+
+    moved_at = np.full(n, -2)
+    best = part.copy()
+    best_q = quality(part)
+    c4 = kn.jet_c0 if level == 0 else kn.jet_c
+    since = 0
+    for it in range(kn.jet_iters):
+        ks = O.stream(kn.seed, 12, level, it)
+        dest = np.full(n, -1)
+        gain = np.zeros(n, np.int64)
+        for v in range(n):
+            if moved_at[v] == it - 1:
+                continue
+            conn = {}
+            for e in range(xadj[v], xadj[v + 1]):
+                b = int(part[adj[e]])
+                conn[b] = conn.get(b, 0) + int(w[e])
+            own = int(part[v])
+            co = conn.get(own, 0)
+            d, dc = -1, 0
+            for b, c in conn.items():
+                if b == own or c == 0:
+                    continue
+                if d < 0 or c > dc or (c == dc and (O.hash32(ks, b), b) < (O.hash32(ks, d), d)):
+                    d, dc = b, c
+            if d >= 0 and 4 * (dc - co) >= -c4 * co:
+                dest[v], gain[v] = d, dc - co
+        keep = np.zeros(n, bool)
+        for v in np.flatnonzero(dest >= 0):
+            a = 0
+            for e in range(xadj[v], xadj[v + 1]):
+                u = adj[e]
+                bu = part[u]
+                if dest[u] >= 0 and (gain[u] > gain[v] or (gain[u] == gain[v] and u < v)):
+                    bu = dest[u]
+                if bu == dest[v]:
+                    a += int(w[e])
+                elif bu == part[v]:
+                    a -= int(w[e])
+            keep[v] = a >= 0
+        moved = int(keep.sum())
+        part[keep] = dest[keep]
+        moved_at[keep] = it
+        if O.block_weights(g, part, k).max() > bound:
+            part = np.array(O.balance(g, kn, part, bound, level)[0], np.int32)
+        q = quality(part)
+        if q < best_q:
+            best_q, best, since = q, part.copy(), 0
+        else:
+            since += 1
+        if moved == 0 or since >= kn.jet_patience:
+            break
+    return best
+
+
+@pytest.mark.parametrize("which,k,level", [("rgg2d", 4, 0), ("grid", 6, 1), ("rmat", 5, 0)])
+def test_jet_matches_python_restatement(graphs, which, k, level):
+    g = {"rgg2d": lambda: graphs.rgg2d(1500, seed=3), "grid": lambda: graphs.grid2d(40, 30),
+         "rmat": lambda: graphs.rmat(9, seed=4)}[which]()
+    kn = O.knobs(g, k, 0.03, 2, 1)
+    kn.jet_iters = 10
+    part = start_partition(g, k, 11)
+    ref = O.jet_refine(g, kn, part, kn.upper_bound, level=level)
+    assert np.array_equal(ref, _jet_restated(g, kn, part, kn.upper_bound, level))
