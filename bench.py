@@ -420,7 +420,7 @@ def main():
         "bytes_per_launch": bytes_per_launch,
         "ms_per_launch": sweep["ms"] / max(1, sweep["launches"]),
         "share_of_timed_kernels": sweep["ms"] / total_fam_ms,
-        "ge_per_s": (sweep["bytes"] / 12.0 / (sweep["ms"] * 1e-3) / 1e9) if sweep["ms"] else None,
+        "ge_per_s": (sweep_e / args.steps / (sweep["ms"] / args.steps * 1e-3) / 1e9) if sweep["ms"] else None,
     }
 
     line = {

@@ -6,7 +6,7 @@
  * module misc/pymodule/kahip.cpp, the JNI wrapper misc/java_jni_wrapper)
  * link against this library unchanged:
  *   kaffpa             interface/kaHIP_interface.h:30-33  (GPU multilevel path)
- *   kaffpa_balance     interface/kaHIP_interface.h:36-41  (perfectly_balance -> bound ceil(W/k))
+ *   kaffpa_balance     interface/kaHIP_interface.h:36-41  (both flag values: max block <= (1+eps)*ceil(W/k))
  *   kaffpa_balance_NE  interface/kaHIP_interface.h:44-47  (not provided: edgecut = -1)
  *   process_mapping    interface/kaHIP_interface.h:52-58  (not provided: edgecut = qap = -1)
  *   node_separator     interface/kaHIP_interface.h:61-64  (not provided)

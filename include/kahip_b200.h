@@ -227,7 +227,7 @@ int kb200_rating_grad(const kb200_train_graph* graph, const float* params, float
 
 /* Heavy-edge matching of one coarsening level (replaces random_matching.cpp:
  * 20-116 / gpa_matching.cpp:25-129): label[n] out = min(v, mate(v)) or v.
- * rating: NULL = expansion*^2 (edge_ratings.cpp:316-328); else one 32-bit
+ * rating: NULL = expansion*^2 (edge_ratings.cpp:171-183); else one 32-bit
  * rating per directed entry (must be symmetric), larger = match first. */
 int kb200_hem_match(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
                     const kb200_knobs* kn, int level, const uint32_t* rating, int* label);
@@ -273,12 +273,18 @@ int kb200_initial_partition(int n, const int* xadj, const int* adjncy, const int
  * memory owned by another runtime).  All arrays are device pointers on the
  * current device (adjwgt / vwgt may be NULL = unit weights); *d_cut and
  * d_bw[k] are written asynchronously on `stream` (a cudaStream_t, NULL = the
- * default stream); *d_cut = -1 if a block id or target is out of range.
+ * default stream).  xadj must be a valid CSR offset array (xadj[0] = 0,
+ * monotone, xadj[n] <= the length of adjncy): the device cannot see the
+ * length of adjncy.  *d_cut = -1 if a block id is outside [0, k), a row
+ * runs backwards, a target is outside [0, n) or a weight is negative (the
+ * inputs the other entry points reject).
  * Limits: k <= 65536 (larger k returns KB200_ERR_INVALID_INPUT).  Its working
  * memory is one 256 KiB __device__ array held by every GPU that loads the
  * library until exit and shared by all calls: calls that overlap on the GPU
- * race and give wrong results.  The first call on a device looks up that
- * array's address, so make it before any stream capture begins. */
+ * race and give wrong results.  The first call in a CUDA context looks up
+ * that array's address, so make it before any stream capture begins; after
+ * cudaDeviceReset the looked-up address may be stale, so do not call it
+ * again in a process that reset its device. */
 int kb200_edge_cut_noalloc(int n, const int* d_xadj, const int* d_adjncy, const int* d_adjwgt,
                            const int* d_vwgt, const int* d_part, int k, long long* d_cut, uint32_t* d_bw,
                            void* stream);

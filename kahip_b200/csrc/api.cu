@@ -309,6 +309,10 @@ struct PhaseRun {
 };
 
 }  // namespace
+
+// Error reporting shared with the entry points defined in other files.
+int report_error(int code, const char* msg) { return fail(code, msg); }
+void clear_error() { g_last_error.clear(); }
 }  // namespace kb
 
 using namespace kb;
@@ -730,7 +734,7 @@ int kb200_edge_cut(int n, const int* xadj, const int* adjncy, const int* adjwgt,
     return guarded([&]() -> int {
         int rc, dev;
         if ((rc = validate(n, xadj, adjncy, adjwgt, vwgt))) return rc;
-        if (k < 1 || !cut) return fail(KB_ERR_INVALID_INPUT, "invalid arguments");
+        if (k < 1 || !cut || (n > 0 && !part)) return fail(KB_ERR_INVALID_INPUT, "invalid arguments");
         for (int v = 0; v < n; ++v)
             if (part[v] < 0 || part[v] >= k) return fail(KB_ERR_INVALID_INPUT, "block id out of range");
         if ((rc = current_device(&dev))) return rc;
@@ -969,10 +973,14 @@ void kaffpa(int* n, int* vwgt, int* xadj, int* adjcwgt, int* adjncy, int* nparts
 
 void kaffpa_balance(int* n, int* vwgt, int* xadj, int* adjcwgt, int* adjncy, int* nparts, double* imbalance,
                     bool perfectly_balance, bool suppress_output, int seed, int mode, int* edgecut, int* part) {
-    // perfectly_balance asks for max block <= ceil(W/k)
-    // (kaHIP_interface.cpp:120-133); that is the imbalance-0 bound here.
-    double imb = perfectly_balance ? 0.0 : (imbalance ? *imbalance : -1.0);
-    kaffpa(n, vwgt, xadj, adjcwgt, adjncy, nparts, &imb, suppress_output, seed, mode, edgecut, part);
+    // With perfectly_balance the reference partitions with the caller's
+    // epsilon and then runs cycle refinement until every block weighs at
+    // most (1+eps)*ceil(W/k) (kaHIP_interface.cpp:115-129).  That is the
+    // bound U that kaffpa here already meets exactly (the balance repair of
+    // every level guarantees max block <= U), so both values of the flag
+    // partition with the caller's imbalance unchanged.
+    (void)perfectly_balance;
+    kaffpa(n, vwgt, xadj, adjcwgt, adjncy, nparts, imbalance, suppress_output, seed, mode, edgecut, part);
 }
 
 void kaffpa_balance_NE(int* n, int* vwgt, int* xadj, int* adjcwgt, int* adjncy, int* nparts, double* imbalance,

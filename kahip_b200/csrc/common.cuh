@@ -42,6 +42,11 @@ inline void check(cudaError_t e, const char* file, int line) {
 // Number of kernels this library has launched (all threads, all devices).
 extern std::atomic<long long> g_kernel_launches;
 
+// The calling thread's error message (kb200_last_error): report_error sets
+// it and returns `code`; clear_error empties it at the start of a call.
+int report_error(int code, const char* msg);
+void clear_error();
+
 #define KB_CUDA(x) ::kb::check((x), __FILE__, __LINE__)
 #define KB_LAUNCH()                                                          \
     do {                                                                     \

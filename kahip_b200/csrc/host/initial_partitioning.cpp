@@ -379,7 +379,7 @@ long long fm_refine(const HostGraph& g, std::vector<char>& side, const Limits& l
 
 // Matching-based coarsening step: nodes visited in hash order, each
 // unmatched node takes the unmatched neighbour of best expansion*^2 rating
-// (edge_ratings.cpp:316-328), ties to the smaller id.  Leader = min id.
+// (edge_ratings.cpp:171-183), ties to the smaller id.  Leader = min id.
 std::vector<int> heavy_edge_labels(const HostGraph& g, uint64_t ks, uint64_t maxnode) {
     // (hash, id) order by a stable LSD radix sort on the hash (ids start
     // ascending): the same order as sorting the pairs

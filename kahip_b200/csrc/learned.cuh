@@ -1,6 +1,6 @@
 // learned.cuh -- the learned edge rating: a small message-passing network
 // that predicts, per edge, the probability that a partition cuts it; its
-// complement replaces expansion*^2 (edge_ratings.cpp:316-328) as the matching
+// complement replaces expansion*^2 (edge_ratings.cpp:171-183) as the matching
 // rating.  The reference has no learned component; this is new.
 //
 // Network (BF16 weights and activations, FP32 accumulation):

@@ -19,9 +19,18 @@
 //     call's contents; each call clears what it needs before use.  Calls
 //     whose work overlaps on the GPU (different streams, or host threads
 //     issuing concurrently) race on it and give wrong results.
-//   * The first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (with that device current) and caches it; make
-//     that first call before any stream capture is started.
+//   * The first call in a CUDA context looks up the array's device address
+//     with cudaGetSymbolAddress (with that context current) and caches it
+//     under the context's handle; make that first call before any stream
+//     capture is started.  After cudaDeviceReset the cached address is
+//     stale if the driver hands out the same context handle again, so a
+//     process that resets a device must not call this entry point again.
+//   * The graph is trusted as a CSR offset array: xadj[0] = 0, monotone,
+//     and xadj[n] no larger than the length of adjncy.  Rows that run
+//     backwards, block ids outside [0, k), targets outside [0, n) and
+//     negative weights make *d_cut = -1 (the other entry points reject the
+//     same inputs); the kernel cannot see the length of adjncy.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -46,32 +55,50 @@ constexpr size_t kNoAllocScratchBytes = kNoAllocScratchWords * sizeof(unsigned l
 
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoAllocScratchWords];
 
-constexpr int kMaxDevices = 64;
+// Cached device address of the scratch array per CUDA context.
+constexpr int kMaxContexts = 64;
 std::mutex g_addr_mu;
-void* g_addr[kMaxDevices] = {};
+CUcontext g_addr_ctx[kMaxContexts] = {};
+void* g_addr[kMaxContexts] = {};
+int g_addr_used = 0;
 
+// One warp per vertex: the lanes stride over the row (coalesced reads, hub
+// rows spread over 32 lanes).  Accumulates twice the cut, the block
+// weights, and a count of inputs it refuses (bad block id, row running
+// backwards, target out of range, negative weight).
 __global__ void noalloc_cut_kernel(int n, const int* __restrict__ xadj, const int* __restrict__ adjncy,
                                    const int* __restrict__ adjwgt, const int* __restrict__ vwgt,
                                    const int* __restrict__ part, int k, unsigned long long* scratch) {
     unsigned long long* cut2 = scratch;
     unsigned long long* bad = scratch + 1;
     uint32_t* bw = reinterpret_cast<uint32_t*>(scratch + 2);
+    const int lane = threadIdx.x & 31;
+    const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
     unsigned long long c = 0, b = 0;
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    for (long long v = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; v < n; v += warps) {
         const int p = part[v];
-        if (p < 0 || p >= k) { ++b; continue; }  // out-of-range block id: counted, skipped
-        atomicAdd(&bw[p], (uint32_t)(vwgt ? vwgt[v] : 1));
-        for (int e = xadj[v]; e < xadj[v + 1]; ++e) {
+        const int r0 = xadj[v], r1 = xadj[v + 1];
+        if (p < 0 || p >= k || r0 < 0 || r1 < r0) {
+            if (lane == 0) ++b;
+            continue;
+        }
+        if (lane == 0) {
+            const int w = vwgt ? vwgt[v] : 1;
+            if (w < 0) ++b;
+            else atomicAdd(&bw[p], (uint32_t)w);
+        }
+        for (int e = r0 + lane; e < r1; e += 32) {
             const int t = adjncy[e];
-            if (t < 0 || t >= n) { ++b; continue; }
-            if (part[t] != p) c += (unsigned long long)(long long)(adjwgt ? adjwgt[e] : 1);
+            const int w = adjwgt ? adjwgt[e] : 1;
+            if (t < 0 || t >= n || w < 0) { ++b; continue; }
+            if (part[t] != p) c += (unsigned long long)w;
         }
     }
     for (int o = 16; o >= 1; o >>= 1) {
         c += __shfl_xor_sync(0xffffffffu, c, o);
         b += __shfl_xor_sync(0xffffffffu, b, o);
     }
-    if ((threadIdx.x & 31) == 0) {
+    if (lane == 0) {
         if (c) atomicAdd(cut2, c);
         if (b) atomicAdd(bad, b);
     }
@@ -86,19 +113,49 @@ __global__ void noalloc_finish_kernel(int k, const unsigned long long* scratch, 
     if (blockIdx.x == 0 && threadIdx.x == 0) *d_cut = scratch[1] ? -1LL : (long long)(scratch[0] / 2);
 }
 
-// Device address of the scratch array on `dev` (looked up once per device).
-int scratch_address(int dev, unsigned long long** out) {
-    std::lock_guard<std::mutex> lk(g_addr_mu);
-    if (!g_addr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || p == nullptr) {
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+
+// The current CUDA context's handle (nullptr when it cannot be read).
+CUcontext current_context() {
+    static CtxGetCurrentFn fn = []() -> CtxGetCurrentFn {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
             (void)cudaGetLastError();
-            return KB200_ERR_CUDA;
+            return nullptr;
         }
-        g_addr[dev] = p;
+        return reinterpret_cast<CtxGetCurrentFn>(f);
+    }();
+    CUcontext c = nullptr;
+    if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+    return c;
+}
+
+// Device address of the scratch array in the current context, looked up
+// once per context with that context current.
+int scratch_address(unsigned long long** out) {
+    CUcontext ctx = current_context();
+    std::lock_guard<std::mutex> lk(g_addr_mu);
+    if (ctx)
+        for (int i = 0; i < g_addr_used; ++i)
+            if (g_addr_ctx[i] == ctx) {
+                *out = static_cast<unsigned long long*>(g_addr[i]);
+                return KB200_OK;
+            }
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr) {
+        (void)cudaGetLastError();
+        return report_error(KB200_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed");
     }
-    *out = static_cast<unsigned long long*>(g_addr[dev]);
+    if (!ctx) ctx = current_context();  // the lookup made the runtime's context current
+    if (ctx && g_addr_used < kMaxContexts) {
+        g_addr_ctx[g_addr_used] = ctx;
+        g_addr[g_addr_used] = p;
+        ++g_addr_used;
+    }
+    *out = static_cast<unsigned long long*>(p);
     return KB200_OK;
 }
 
@@ -110,36 +167,40 @@ extern "C" {
 
 // Edge cut and block weights of part[] on the current device, all arrays
 // device-resident (adjwgt / vwgt may be NULL = unit weights).  Writes
-// *d_cut (one long long; -1 if a block id or target was out of range) and
-// d_bw[k] asynchronously on `stream`.  Allocates nothing; k <= 65536; see
-// the file comment for the shared scratch array and its limits.
+// *d_cut (one long long; -1 if a block id, row, target or weight was
+// refused) and d_bw[k] asynchronously on `stream`.  Allocates nothing;
+// k <= 65536; see the file comment for the shared scratch array and its
+// limits.
 int kb200_edge_cut_noalloc(int n, const int* d_xadj, const int* d_adjncy, const int* d_adjwgt,
                            const int* d_vwgt, const int* d_part, int k, long long* d_cut, uint32_t* d_bw,
                            void* stream) {
-    if (n < 0 || !d_xadj || (n > 0 && (!d_adjncy || !d_part)) || !d_cut || !d_bw) return KB200_ERR_INVALID_INPUT;
-    if (k < 1 || k > kb::kNoAllocMaxBlocks) return KB200_ERR_INVALID_INPUT;
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kb::kMaxDevices) {
+    kb::clear_error();
+    if (n < 0 || !d_xadj || (n > 0 && (!d_adjncy || !d_part)) || !d_cut || !d_bw)
+        return kb::report_error(KB200_ERR_INVALID_INPUT, "invalid arguments (n < 0 or a NULL array)");
+    if (k < 1 || k > kb::kNoAllocMaxBlocks)
+        return kb::report_error(KB200_ERR_INVALID_INPUT, "k must be in [1, 65536]");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
         (void)cudaGetLastError();
-        return KB200_ERR_NO_DEVICE;
+        return kb::report_error(KB200_ERR_NO_DEVICE, "no CUDA device available (this library has no CPU path)");
     }
     unsigned long long* scratch = nullptr;
-    if (int rc = kb::scratch_address(dev, &scratch)) return rc;
+    if (int rc = kb::scratch_address(&scratch)) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     // clear the two counters and the k block-weight slots this call uses
     if (cudaMemsetAsync(scratch, 0, 2 * sizeof(unsigned long long) + sizeof(uint32_t) * (size_t)k, s) !=
         cudaSuccess) {
         (void)cudaGetLastError();
-        return KB200_ERR_CUDA;
+        return kb::report_error(KB200_ERR_CUDA, "cudaMemsetAsync of the scratch array failed");
     }
     if (n > 0) {
-        int blocks = (int)std::min<long long>(((long long)n + 255) / 256, (long long)kb::kNumSMs * 16);
+        int blocks = (int)std::min<long long>(((long long)n + 7) / 8, (long long)kb::kNumSMs * 8);
         kb::noalloc_cut_kernel<<<blocks, 256, 0, s>>>(n, d_xadj, d_adjncy, d_adjwgt, d_vwgt, d_part, k, scratch);
         kb::g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
     }
     kb::noalloc_finish_kernel<<<(k + 255) / 256, 256, 0, s>>>(k, scratch, d_cut, d_bw);
     kb::g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
-    if (cudaGetLastError() != cudaSuccess) return KB200_ERR_CUDA;
+    if (cudaGetLastError() != cudaSuccess) return kb::report_error(KB200_ERR_CUDA, "kernel launch failed");
     return KB200_OK;
 }
 

@@ -155,7 +155,7 @@ double or_balance_ratio(const or_graph* g, const int* part, int k) {
 }
 
 void or_rate_expansion_star_2(const or_graph* g, double* rating) {
-    /* edge_ratings.cpp:316-328: 1.0*w*w / (c(u)*c(v)), denominator as a
+    /* edge_ratings.cpp:171-183: 1.0*w*w / (c(u)*c(v)), denominator as a
      * 32-bit unsigned product */
     for (int v = 0; v < g->n; ++v) {
         uint32_t cv = (uint32_t)g->vwgt[v];
@@ -1128,7 +1128,7 @@ static int cmp_hv(const void* x, const void* y) {
 }
 
 /* Sequential heavy-edge matching on the expansion*^2 rating
- * (edge_ratings.cpp:316-328, weight bound as random_matching.cpp:85-96):
+ * (edge_ratings.cpp:171-183, weight bound as random_matching.cpp:85-96):
  * nodes in hash order; an unmatched node takes its unmatched neighbour of
  * largest rating (ties: smaller id) with c(u)+c(v) <= maxnode. */
 static void hem(const or_graph* g, uint64_t ks, uint64_t maxnode, int* match) {

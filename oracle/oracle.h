@@ -80,12 +80,12 @@ long long or_edge_cut(const or_graph* g, const int* part);
 void or_block_weights(const or_graph* g, const int* part, int k, uint32_t* bw);
 double or_balance_ratio(const or_graph* g, const int* part, int k);
 
-/* edge_ratings.cpp:316-328 */
+/* edge_ratings.cpp:171-183 */
 void or_rate_expansion_star_2(const or_graph* g, double* rating);
 
 /* Heavy-edge matching of one coarsening level: synchronous locally-dominant
  * rounds on a strict edge order (rating, edge hash, endpoints).  rating_q:
- * NULL = expansion*^2 (edge_ratings.cpp:316-328) computed per entry, else one
+ * NULL = expansion*^2 (edge_ratings.cpp:171-183) computed per entry, else one
  * 32-bit rating per directed entry (symmetric).  Pairs obey
  * c(u)+c(v) <= max_vertex_weight (random_matching.cpp:85-112).
  * label[v] = min(v, mate(v)), or v when unmatched. */

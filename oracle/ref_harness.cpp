@@ -136,7 +136,7 @@ double ref_balance(int n, const int* xadj, const int* adjncy, const int* vwgt,
     return qm.balance(G);
 }
 
-// lib/partition/coarsening/edge_rating/edge_ratings.cpp:316-328
+// lib/partition/coarsening/edge_rating/edge_ratings.cpp:171-183
 void ref_rate_expansion_star_2(int n, const int* xadj, const int* adjncy,
                                const int* vwgt, const int* adjwgt, double* rating) {
     graph_access G;

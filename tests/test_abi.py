@@ -74,6 +74,18 @@ def test_host_validation_before_device():
     assert e.value.code == native.ERR_INVALID_INPUT
 
 
+def test_edge_cut_rejects_null_partition():
+    # checked before any device work, so it needs no GPU
+    from kahip_b200 import native
+    L = native.lib()
+    xadj = np.array([0, 1, 2], np.int32)
+    adj = np.array([1, 0], np.int32)
+    cut = ctypes.c_longlong(5)
+    rc = L.kb200_edge_cut(2, xadj.ctypes.data, adj.ctypes.data, None, None, None, 2, ctypes.byref(cut), None)
+    assert rc == native.ERR_INVALID_INPUT
+    assert b"invalid" in L.kb200_last_error()
+
+
 def test_unsupported_siblings_report_failure():
     from kahip_b200 import native
     L = native.lib()

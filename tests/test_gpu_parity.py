@@ -161,6 +161,35 @@ def test_drop_in_kaffpa_abi(N, O, graphs):
     assert np.array_equal(part, part_o)
 
 
+@pytest.mark.parametrize("perfectly_balance", [False, True])
+def test_drop_in_kaffpa_balance_keeps_epsilon(N, O, graphs, perfectly_balance):
+    """kaffpa_balance keeps the caller's epsilon for either flag value: the
+    reference's perfectly_balance enforces max block <= (1+eps)*ceil(W/k)
+    after partitioning (interface/kaHIP_interface.cpp:115-129), the bound
+    every partition here already meets."""
+    import ctypes
+    g = graphs.rgg2d(1 << 12, seed=2)
+    rng = np.random.default_rng(5)
+    vwgt = rng.integers(1, 4, g["n"]).astype(np.int32)
+    L = N.lib()
+    n = ctypes.c_int(g["n"])
+    k = ctypes.c_int(8)
+    imb = ctypes.c_double(0.03)
+    cut = ctypes.c_int(-7)
+    part = np.zeros(g["n"], np.int32)
+    L.kaffpa_balance.restype = None
+    L.kaffpa_balance(ctypes.byref(n), vwgt.ctypes.data, g["xadj"].ctypes.data, None, g["adjncy"].ctypes.data,
+                     ctypes.byref(k), ctypes.byref(imb), ctypes.c_bool(perfectly_balance), True, 0, 0,
+                     ctypes.byref(cut), part.ctypes.data)
+    gw = dict(g, vwgt=vwgt)
+    cut_o, part_o, _ = O.kaffpa(gw, 8, 0.03, 0, 0)
+    assert cut.value == cut_o
+    assert np.array_equal(part, part_o)
+    W = int(vwgt.sum())
+    bound = int((1 + 0.03) * -(-W // 8))
+    assert O.block_weights(gw, part, 8).max() <= bound
+
+
 EDGE_GRAPHS = {
     "empty": (0, []),
     "single": (1, []),

@@ -11,7 +11,7 @@ import pytest
 
 from conftest import tie_free
 
-REF_EXAMPLES = "/root/reference/examples"
+REF_EXAMPLES = os.path.join(os.environ.get("KAHIP_REFERENCE", "/root/reference"), "examples")
 
 
 @pytest.fixture(scope="module")

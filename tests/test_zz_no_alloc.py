@@ -1,6 +1,7 @@
 """kb200_edge_cut_noalloc: the entry point for callers that must not allocate
 device memory (fixed memory budgets, allocator-free sections, memory owned by
-another runtime) -- checked against the allocating kb200_edge_cut.
+another runtime) -- checked against the CPU oracle's edge cut and block
+weights and against the allocating kb200_edge_cut.
 
 Runs last (file name) so that a stopped-at-first-failure run has already run
 every other test; it also passes alone in a fresh process.
@@ -52,10 +53,14 @@ def test_noalloc_matches_allocating_entry_point(graphs):
         assert rc == 0, native.lib().kb200_last_error()
         return free0, free1
 
+    from oracle import oracle
+
     results = []
     for i in range(3):  # two calls in a row (and a third to watch device memory)
         part = rng.integers(0, k, g["n"]).astype(np.int32)
         free0, free1 = call(part, k, d_bw)
+        assert d_cut.item() == oracle.edge_cut(g, part)
+        assert np.array_equal(d_bw.cpu().numpy().view(np.uint32), oracle.block_weights(g, part, k))
         cut_ref, bw_ref = native.edge_cut(g, part, k)   # the allocating entry point
         assert d_cut.item() == cut_ref
         assert np.array_equal(d_bw.cpu().numpy().view(np.uint32), bw_ref)
@@ -80,3 +85,15 @@ def test_noalloc_matches_allocating_entry_point(graphs):
     bad[7] = 9
     call(bad, 4, torch.zeros(4, dtype=torch.int32, device=dev))
     assert d_cut.item() == -1
+    # a negative edge weight is refused like the other entry points refuse it
+    neg = d["adjwgt"].clone()
+    neg[3] = -5
+    part = rng.integers(0, 4, g["n"]).astype(np.int32)
+    d_part = torch.from_numpy(part).to(dev)
+    rc = fn(g["n"], d["xadj"].data_ptr(), d["adjncy"].data_ptr(), neg.data_ptr(), None, d_part.data_ptr(), 4,
+            d_cut.data_ptr(), d_bw.data_ptr(), stream)
+    torch.cuda.synchronize()
+    assert rc == 0 and d_cut.item() == -1
+    # and the next valid call is unaffected by the refused ones
+    call(part, 4, bw5)
+    assert d_cut.item() == oracle.edge_cut(g, part)
