@@ -12,9 +12,10 @@ Arms
              e2e     = the same through the host C ABI (kb200_kaffpa, pinned
                        host CSR in, part[] out), H2D + D2H inside the timer
   reference  the reference kaffpa() (KaHIP built from its sources into
-             oracle/_ref) on the host cores, one process per core, on a
-             bounded sample of the workload (RGG2D n=2^22, same generator),
-             scaled to the full workload by directed-edge count.
+             oracle/_ref) on the full workload graph, on the host cores:
+             K partitions (one per step, seeds W..W+K-1) run as concurrent
+             single-threaded processes; value = wall / K.  The 1-process
+             latency (seed 0 alone) is reported beside it.
 
 With N > 1 (torchrun), every rank partitions its own replica (weak scaling,
 no collective on the data path); value = max-over-ranks time / (K*N).
@@ -158,52 +159,93 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ reference arm
+#
+# The reference kaffpa() (KaHIP built from its sources into oracle/_ref, its
+# own interface/kaHIP_interface.cpp entry point) partitions the FULL workload
+# graph, in-process, in worker processes that map one shared copy of the CSR.
+# kaffpa is single-threaded, so the host cores run independent partitions
+# (seed = step index) concurrently; each worker times its kaffpa() call alone
+# (the reference CLI's "time spent for partitioning", app/kaffpa.cpp:79,118).
+
+# reference presets: R-MAT uses fastsocial (the reference's LP preset) because
+# reference fast does not finish in reasonable time on it (and misses the
+# balance bound); every other graph uses the arm's own preset
+REF_MODE_FOR_RMAT = 3
+
+
+def ref_mode(args) -> int:
+    return REF_MODE_FOR_RMAT if args.graph == "rmat" else MODES[args.mode]
+
 
 def _ref_worker_init():
     os.environ["KBGEN_THREADS"] = "1"
 
 
-_SAMPLE = {}
+def _ref_full_task(task):
+    """One reference kaffpa() on the shared graph: (ms, cut, peak RSS bytes)."""
+    import resource
 
+    import numpy as np
 
-def _ref_task(args):
-    kind, logn, k, seed, mode = args
     from oracle import oracle
-    g = _SAMPLE.get((kind, logn))
-    if g is None:
-        g = make_graph(kind, logn)
-        _SAMPLE[(kind, logn)] = g
+    gdir, unit, k, seed, mode = task
+    g = {key: np.load(os.path.join(gdir, key + ".npy"), mmap_mode="r") for key in ("xadj", "adjncy", "adjwgt", "vwgt")}
+    g["n"] = len(g["xadj"]) - 1
+    if unit:
+        g["vwgt"] = g["adjwgt"] = None
     t = time.perf_counter()
-    unit = kind != "rmat"
-    cut, _ = oracle.ref_kaffpa(dict(g, vwgt=None, adjwgt=None) if unit else g, k, IMBALANCE, seed, mode)
-    return (time.perf_counter() - t) * 1e3, cut, g["m"]
+    cut, _ = oracle.ref_kaffpa(g, k, IMBALANCE, seed, mode)
+    ms = (time.perf_counter() - t) * 1e3
+    return ms, int(cut), resource.getrusage(resource.RUSAGE_SELF).ru_maxrss * 1024
 
 
-def reference_sample_ms(logn: int, k: int, procs: int, seeds, kind: str = "rgg2d", mode: int = MODE_FAST):
-    """Runs the reference kaffpa on the sample graph in `procs` processes;
-    returns (wall ms, per-run ms list, cuts, m_sample)."""
-    ctx = mp.get_context("spawn")
-    t = time.perf_counter()
-    with ctx.Pool(procs, initializer=_ref_worker_init) as pool:
-        res = pool.map(_ref_task, [(kind, logn, k, s, mode) for s in seeds])
-    wall = (time.perf_counter() - t) * 1e3
-    return wall, [r[0] for r in res], [r[1] for r in res], res[0][2]
+# peak resident bytes of one reference kaffpa process per directed entry
+# (graph_access edges, ratings, coarse levels and the mapped input: 52 B
+# measured on RGG2D n=2^22, fast, k=64), with a margin
+REF_BYTES_PER_ENTRY = 64
 
 
-def host_procs_for_reference():
+def host_procs_for_reference(m_directed: int) -> int:
     n = os.cpu_count() or 1
     try:
         with open("/proc/meminfo") as f:
             avail = next(int(l.split()[1]) for l in f if l.startswith("MemAvailable")) * 1024
-        n = min(n, max(1, int(avail // (3 << 30))))  # ~3 GB per reference process on the 2^22 sample
+        n = min(n, max(1, int(avail // max(1, REF_BYTES_PER_ENTRY * m_directed))))
     except (OSError, StopIteration):
         pass
     return max(1, n)
 
 
-def full_m(kind: str, logn: int) -> int:
-    # the directed entry count of the full workload (generated once; cheap relative to the run)
-    return make_graph(kind, logn)["m"]
+class SharedGraph:
+    """The workload graph written once as .npy files (tmpfs where there is
+    one) for the reference workers to map."""
+
+    def __init__(self, g: dict):
+        import shutil
+        import tempfile
+
+        import numpy as np
+        base = "/dev/shm" if os.path.isdir("/dev/shm") else None
+        need = sum(g[k].nbytes for k in ("xadj", "adjncy", "adjwgt", "vwgt"))
+        if base and shutil.disk_usage(base).free < 2 * need:
+            base = None
+        self.dir = tempfile.mkdtemp(prefix="kb200_ref_", dir=base)
+        for key in ("xadj", "adjncy", "adjwgt", "vwgt"):
+            np.save(os.path.join(self.dir, key + ".npy"), g[key])
+
+    def close(self):
+        import shutil
+        shutil.rmtree(self.dir, ignore_errors=True)
+
+
+def reference_runs(gdir: str, unit: bool, k: int, mode: int, seeds, procs: int):
+    """Runs the reference on `seeds` with `procs` concurrent processes;
+    returns (wall ms, [(ms, cut, rss)])."""
+    ctx = mp.get_context("spawn")
+    t = time.perf_counter()
+    with ctx.Pool(procs, initializer=_ref_worker_init) as pool:
+        res = pool.map(_ref_full_task, [(gdir, unit, k, s, mode) for s in seeds], chunksize=1)
+    return (time.perf_counter() - t) * 1e3, res
 
 
 def run_reference_arm(args, rank):
@@ -214,35 +256,65 @@ def run_reference_arm(args, rank):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libkahip_ref.so was not built "
                           "(reference sources absent when __graft_entry__.build() ran)"}))
         return
-    procs = host_procs_for_reference()
-    m_full = full_m(args.graph, args.logn)
-    sample_logn = GRAPH_KINDS[args.graph][2]
-    step_ms = []
-    cuts = []
-    m_sample = None
-    for step in range(args.warmup + args.steps):
-        seeds = [step * procs + i for i in range(procs)]
-        wall, per, c, m_sample = reference_sample_ms(sample_logn, args.k, procs, seeds, args.graph, MODES[args.mode])
-        if step >= args.warmup:
-            step_ms.append(wall / procs)
-            cuts += c
-    scale = m_full / m_sample
-    value = statistics.mean(step_ms) * scale
-    sample = (f"reference kaffpa {args.mode} (KaHIP built from its sources) on {GRAPH_KINDS[args.graph][0]} "
-              f"n=2^{sample_logn} "
-              f"(m_directed={m_sample}), {procs} concurrent processes (one per core) per step; "
-              f"ms per partition = step wall / {procs}, scaled x{scale:.3f} by directed edges to n=2^{args.logn}")
+    g = make_graph(args.graph, args.logn)
+    m_full = g["m"]
+    unit = args.graph != "rmat"
+    mode = ref_mode(args)
+    procs = host_procs_for_reference(m_full)
+    shared = SharedGraph(g)
+    del g
+    try:
+        # warm-up: seed 0 alone (the 1-process latency and the cut on the
+        # timed workload's own seed), then the other warm-up seeds together
+        _, solo = reference_runs(shared.dir, unit, args.k, mode, [0], 1)
+        if args.warmup > 1:
+            reference_runs(shared.dir, unit, args.k, mode, list(range(1, args.warmup)),
+                           min(procs, args.warmup - 1))
+        # timed: K partitions (seeds W .. W+K-1) in waves of equal size on
+        # the host cores; value = wall / K
+        waves = -(-args.steps // procs)
+        conc = -(-args.steps // waves)
+        wall, res = reference_runs(shared.dir, unit, args.k, mode,
+                                   list(range(args.warmup, args.warmup + args.steps)), conc)
+    finally:
+        shared.close()
+    value = wall / args.steps
+    per = [r[0] for r in res]
+    cuts = [r[1] for r in res]
+    mode_name = {0: "fast", 1: "eco", 3: "fastsocial"}.get(mode, str(mode))
+    sample = (f"full workload: reference kaffpa {mode_name} (KaHIP built from its sources, its kaffpa() entry "
+              f"point, single-threaded) on {GRAPH_KINDS[args.graph][0]} n=2^{args.logn} (m_directed={m_full}); "
+              f"{args.steps} partitions (seeds {args.warmup}..{args.warmup + args.steps - 1}) in {waves} wave(s) "
+              f"of {conc} concurrent processes; ms per partition = wall / {args.steps}")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "ms", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": f"synthetic (seeded {GRAPH_KINDS[args.graph][0]} generator)",
         "config": workload_config(args, m_full),
-        "cpu_baseline": {"value": value, "unit": "ms", "cores": procs, "kind": "reference", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": "ms", "cores": conc, "kind": "reference", "sample": sample,
+                         "latency_1proc": {"value": solo[0][0], "unit": "ms", "cores": 1,
+                                           "sample": f"seed 0 alone, cut {solo[0][1]}"},
+                         "per_partition_ms_under_load": {"mean": statistics.mean(per), "min": min(per),
+                                                         "max": max(per)},
+                         "peak_rss_bytes_per_process": max(r[2] for r in res)},
         "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "reference_cut_sample_mean": statistics.mean(cuts) if cuts else None,
+        "reference_preset": mode_name,
+        "reference_cut_seed0": solo[0][1],
+        "reference_cut_mean": statistics.mean(cuts),
+        "host": host_description(),
     }
     print(json.dumps(line))
+
+
+def host_description() -> dict:
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            model = next((l.split(":", 1)[1].strip() for l in f if l.startswith("model name")), None)
+    except OSError:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count()}
 
 
 def workload_config(args, m):
@@ -447,15 +519,20 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import oracle
         if oracle.ref_available():
-            sample_logn = GRAPH_KINDS[args.graph][2]
-            wall, per, c, m_sample = reference_sample_ms(sample_logn, args.k, 1, [0], args.graph, MODES[args.mode])
-            scale = m / m_sample
+            # the reference kaffpa() on the same full graph, alone on one core
+            mode = ref_mode(args)
+            shared = SharedGraph(g)
+            try:
+                _, res = reference_runs(shared.dir, unit, args.k, mode, [0], 1)
+            finally:
+                shared.close()
+            mode_name = {0: "fast", 1: "eco", 3: "fastsocial"}.get(mode, str(mode))
             line["cpu_baseline"] = {
-                "value": per[0] * scale, "unit": "ms", "cores": 1, "kind": "reference",
-                "sample": (f"one reference kaffpa {args.mode} run (KaHIP built from its sources, single-threaded) on "
-                           f"{GRAPH_KINDS[args.graph][0]} n=2^{sample_logn} (m_directed={m_sample}, "
-                           f"{per[0]:.0f} ms, cut {c[0]}), "
-                           f"scaled x{scale:.3f} by directed edges to n=2^{args.logn}")}
+                "value": res[0][0], "unit": "ms", "cores": 1, "kind": "reference",
+                "sample": (f"full workload: one reference kaffpa {mode_name} run (KaHIP built from its sources, its "
+                           f"kaffpa() entry point, single-threaded) on the same {GRAPH_KINDS[args.graph][0]} "
+                           f"n=2^{args.logn} graph (m_directed={m}), seed 0"),
+                "reference_cut": res[0][1], "host": host_description()}
         else:
             line["cpu_baseline"] = {"value": None, "unit": "ms", "cores": 0, "kind": "reference",
                                     "sample": "unavailable: oracle/_ref not built"}
@@ -672,7 +749,7 @@ def run_many(args, world, rank, dev):
     if rank == 0 and args.workload == "batch" and not args.no_cpu_baseline:
         from oracle import oracle
         if oracle.ref_available():
-            procs = host_procs_for_reference()
+            procs = host_procs_for_reference(max(g["m"] for g in gs))
             sample = min(count, 4 * procs)
             ctx = mp.get_context("spawn")
             t0 = time.perf_counter()

@@ -1,0 +1,100 @@
+"""Bit-exact parity at the benchmark configurations' own sizes.
+
+The CPU oracle's results for RGG2D n=2^24 (k = 16 / 64 / 256, seeds 0-4, fast;
+k = 64 eco), RGG3D n=2^22 (k = 16 / 64 / 256), R-MAT n=2^23 (k = 64 / 256) and
+RGG2D n=2^15 (k = 8 / 64, fast and eco) are committed as digests in
+tests/golden/scale_digests.json (made by tests/golden/make_scale_digests.py:
+minutes of single-threaded oracle time per graph).  Each case regenerates the
+graph with the seeded generator, checks it against the recorded graph hash,
+partitions it on the device through the C ABI (kb200_kaffpa_device) and
+compares the edge cut, the sha256 of part[], the initial partition's cut and
+every level's node count, entry count, cut and heaviest block.  The headline
+configuration also runs through the host ABI (kb200_kaffpa, host buffers in
+and out).  Larger-than-2^15 inputs reach what the small parity cases cannot:
+hub rows through the global-table sweep and the radix-sorted contraction
+rows (R-MAT), multi-block scans and arena sizes of a 2^24-node hierarchy.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+with open(os.path.join(HERE, "golden", "scale_digests.json")) as _f:
+    DIGESTS = json.load(_f)["configs"]
+
+# graph by graph (one device-resident graph at a time), smallest first
+NAMES = sorted(DIGESTS, key=lambda c: (DIGESTS[c]["n"], DIGESTS[c]["graph"], DIGESTS[c]["k"],
+                                       DIGESTS[c]["seed"], DIGESTS[c]["mode"]))
+
+_CACHE = {}
+
+
+def _graph_sha256(g):
+    h = hashlib.sha256()
+    for key in ("xadj", "adjncy", "adjwgt", "vwgt"):
+        h.update(g[key].astype("<i4", copy=False).tobytes())
+    return h.hexdigest()
+
+
+def _device_graph(d):
+    import torch
+
+    from kahip_b200 import graphs
+    key = (d["graph"], d["logn"])
+    if key not in _CACHE:
+        _CACHE.clear()
+        torch.cuda.empty_cache()
+        n = 1 << d["logn"]
+        g = {"rgg2d": lambda: graphs.rgg2d(n, seed=0), "rgg3d": lambda: graphs.rgg3d(n, seed=0),
+             "rmat": lambda: graphs.rmat(d["logn"], seed=0)}[d["graph"]]()
+        assert g["m"] == d["m_directed"]
+        assert _graph_sha256(g) == d["graph_sha256"], "the seeded generator no longer makes the recorded graph"
+        dev = torch.device("cuda", 0)
+        unit = d["graph"] != "rmat"
+        t = {k: torch.from_numpy(g[k]).to(dev) for k in ("xadj", "adjncy", "adjwgt", "vwgt")}
+        _CACHE[key] = (g, t, unit)
+    return _CACHE[key]
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_device_path_matches_oracle_digest(name):
+    import torch
+
+    from kahip_b200 import native
+    assert native.device_count() > 0, "needs a CUDA device"
+    d = DIGESTS[name]
+    g, t, unit = _device_graph(d)
+    n = g["n"]
+    part = torch.empty(n, dtype=torch.int32, device=t["xadj"].device)
+    st = native.Stats()
+    st.collect_level_cuts = 1
+    # unit-weight graphs go in with NULL weights, as the benchmark passes them
+    rc, cut = native.kaffpa_device(n, t["xadj"], t["adjncy"], None if unit else t["adjwgt"],
+                                   None if unit else t["vwgt"], part, d["k"], d["imbalance"], d["seed"],
+                                   d["mode"], stats=st)
+    torch.cuda.synchronize()
+    p = part.cpu().numpy()
+    levels = [[st.level_n[i], st.level_m[i], st.level_cut[i], st.level_maxbw[i]] for i in range(st.levels)]
+    assert levels == d["levels"]
+    assert st.initial_cut == d["initial_cut"]
+    assert cut == d["cut"]
+    assert hashlib.sha256(p.astype("<i4").tobytes()).hexdigest() == d["part_sha256"]
+    bw = np.bincount(p, minlength=d["k"])
+    assert bw.max() == d["max_block"] and bw.max() <= d["bound"]
+
+
+def test_host_abi_matches_oracle_digest_at_the_headline_size():
+    """kb200_kaffpa (host buffers: upload, partition, download) on RGG2D
+    n=2^24, k=64, fast, seed 0."""
+    from kahip_b200 import native
+    d = DIGESTS["rgg2d_2p24_k64_s0_fast"]
+    g, _, _ = _device_graph(d)
+    rc, cut, part = native.kaffpa_ex(g["xadj"], g["adjncy"], d["k"], d["imbalance"], d["seed"], d["mode"])
+    assert cut == d["cut"]
+    assert hashlib.sha256(np.ascontiguousarray(part, np.int32).astype("<i4").tobytes()).hexdigest() == \
+        d["part_sha256"]
