@@ -68,6 +68,9 @@ typedef struct kb200_knobs {
     int jet_iters, jet_patience;  /* Jet: iteration cap, iterations without a better cut */
     int jet_c0, jet_c;         /* Jet: negative-gain tolerance in quarters of the own
                                   connection, finest level / coarser levels */
+    int ip_mode;               /* initial partitioning of the coarsest graph: 1 = on the
+                                  device, every bisection of a recursion depth in one launch
+                                  (default); 0 = the host's multilevel bisection with FM */
 } kb200_knobs;
 
 /* Parameter count of the learned edge rating (kahip_b200/csrc/learned.cuh). */

@@ -1,0 +1,760 @@
+// ip_device.cu -- initial partitioning of the coarsest graph on the device:
+// recursive bisection with every bisection of one recursion depth in one
+// launch, one thread block per block of the current partition.
+//
+// The recursion and its bounds follow graph_partitioner.cpp:110-238: the
+// left half of a block that still splits into kk blocks gets ceil(kk/2) of
+// them, the side targets are in proportion, each side may exceed its target
+// by max((1+eps)^(1/ceil log2 kk) - 1, min(eps, 1%)).  A block is named by
+// its offset o, the first final block id it covers, so part[] holds final
+// block ids once the recursion ends.  A bisection runs `tries` tries and
+// keeps the best by (overload, cut), the first on ties.  A try:
+//   1. start node: s0 = the node of smallest (hash, id); the reached node
+//      farthest from s0 by breadth-first search, then the one farthest from
+//      that (bipartition.cpp:125-146 finds its start by repeated BFS too),
+//      ties to the smaller id;
+//   2. growing: nodes in (BFS distance from the start, id) order, unreached
+//      nodes last; side 0 takes the prefix until it reaches its target, and
+//      the node that crosses the target joins only if side 0 then stays
+//      within its bound (bipartition.cpp:147-222 grows by gain instead);
+//   3. 2-way Jet refinement in synchronous iterations: candidate moves with
+//      a negative-gain tolerance, the afterburner, a balance repair of an
+//      overloaded side by loss classes, the best (overload, cut) kept.
+// The thread block first builds its block's subgraph (members in id order,
+// edges inside the block) from the coarsest graph.  Every step is
+// deterministic: BFS distances, reductions over (key, id) and prefix sums in
+// id order do not depend on the order threads run in.
+#include "ip_device.cuh"
+
+#include <algorithm>
+#include <climits>
+#include <cmath>
+#include <vector>
+
+#include "hash.h"
+
+#include "prims.cuh"
+
+namespace kb {
+
+namespace {
+
+constexpr int kBT = 512;              // threads per bisecting block
+constexpr int kBW = kBT / 32;         // warps
+constexpr int kIpClasses = 256;       // balance repair classes (loss bucket x 8)
+constexpr int kDenseRows = 16;        // average degree from which a warp walks each row
+
+struct IpArgs {
+    int n;
+    const int* xadj;
+    const int* adjncy;
+    const int* adjwgt;
+    const int* vwgt;
+    int* part;        // [reps][n]: current block offset per node
+    int nsplit, reps;
+    const int* split_o;  // [nsplit] offsets of the blocks that split at this depth
+    const int* split_k;  // [nsplit] their block counts
+    const double* split_eb;  // [nsplit] their per-side slack (computed on the host)
+    const int* sidx;     // [k] split index of a block offset, -1 when it does not split
+    unsigned* cnt;       // [reps][nsplit] members
+    unsigned* deg;       // [reps][nsplit] members' degrees
+    unsigned* nbase;     // [reps][nsplit] start of the split's node slots (members + 2 each)
+    unsigned* ebase;     // [reps][nsplit] start of its edge slots
+    long long NS, ES;    // node / edge slots per repetition
+    int* lid;            // [reps][n]
+    int *orig, *lbeg, *ldeg, *dist, *qa, *qb, *moved_at, *cls;  // [reps][NS]
+    int *ladj, *lw;      // [reps][ES]
+    uint8_t *side, *best, *dest, *keep, *won;  // [reps][NS]
+    long long* gain;     // [reps][NS]
+    unsigned long long* layer;  // [reps][NS]
+    int seed, depth, tries, jet_iters, jet_patience, jet_c, bal_iters;
+    double eps;
+    int* err;
+};
+
+struct Acc2 {
+    long long a, b;
+};
+
+__device__ __forceinline__ long long warp_sum_ll(long long x) {
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+// Block-wide reductions; every thread gets the result.  `sh` holds kBW + 1
+// words and is free again when the call returns.
+__device__ unsigned long long block_sum(unsigned long long x, unsigned long long* sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) sh[wid] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < kBW; ++w) t += sh[w];
+        sh[kBW] = t;
+    }
+    __syncthreads();
+    const unsigned long long r = sh[kBW];
+    __syncthreads();
+    return r;
+}
+
+__device__ unsigned long long block_min(unsigned long long x, unsigned long long* sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) x = min(x, __shfl_xor_sync(0xffffffffu, x, o));
+    if (lane == 0) sh[wid] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = ~0ull;
+        for (int w = 0; w < kBW; ++w) t = min(t, sh[w]);
+        sh[kBW] = t;
+    }
+    __syncthreads();
+    const unsigned long long r = sh[kBW];
+    __syncthreads();
+    return r;
+}
+
+__device__ unsigned long long block_max(unsigned long long x, unsigned long long* sh) {
+    return ~block_min(~x, sh);
+}
+
+// Exclusive prefix sum over the block's threads in thread order; *total =
+// the sum.  `sh` as above.
+__device__ unsigned long long block_scan(unsigned long long x, unsigned long long* total, unsigned long long* sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned long long incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) sh[wid] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long run = 0;
+        for (int w = 0; w < kBW; ++w) {
+            const unsigned long long t = sh[w];
+            sh[w] = run;
+            run += t;
+        }
+        sh[kBW] = run;
+    }
+    __syncthreads();
+    const unsigned long long r = sh[wid] + incl - x;
+    *total = sh[kBW];
+    __syncthreads();
+    return r;
+}
+
+// Per-row sums over the local subgraph: entry(i, e, acc) for every entry e
+// of row i, then row(i, acc) once per row (a warp per row when WARP, the
+// warp's lane 0 calling row; a thread per row otherwise).
+template <bool WARP, class F, class G>
+__device__ __forceinline__ void for_rows(int n_o, const int* lbeg, const int* ldeg, F entry, G row) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (WARP) {
+        for (int i = wid; i < n_o; i += kBW) {
+            Acc2 s{0, 0};
+            const int b = lbeg[i], d = ldeg[i];
+            for (int t = lane; t < d; t += 32) entry(i, b + t, s);
+            s.a = warp_sum_ll(s.a);
+            s.b = warp_sum_ll(s.b);
+            if (lane == 0) row(i, s);
+        }
+    } else {
+        for (int i = threadIdx.x; i < n_o; i += kBT) {
+            Acc2 s{0, 0};
+            const int b = lbeg[i], d = ldeg[i];
+            for (int t = 0; t < d; ++t) entry(i, b + t, s);
+            row(i, s);
+        }
+    }
+}
+
+// Breadth-first distances from s (INT_MAX = unreached).
+template <bool WARP>
+__device__ void bfs(int n_o, int s, int* dist, int* qa, int* qb, const int* lbeg, const int* ldeg,
+                    const int* ladj, unsigned* sh_next) {
+    for (int i = threadIdx.x; i < n_o; i += kBT) dist[i] = INT_MAX;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        dist[s] = 0;
+        qa[0] = s;
+    }
+    int cnt = 1, level = 0;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    while (cnt > 0) {
+        if (threadIdx.x == 0) *sh_next = 0;
+        __syncthreads();
+        if (WARP) {
+            for (int f = wid; f < cnt; f += kBW) {
+                const int v = qa[f], b = lbeg[v], d = ldeg[v];
+                for (int t = lane; t < d; t += 32) {
+                    const int u = ladj[b + t];
+                    if (atomicCAS(&dist[u], INT_MAX, level + 1) == INT_MAX) qb[atomicAdd(sh_next, 1u)] = u;
+                }
+            }
+        } else {
+            for (int f = threadIdx.x; f < cnt; f += kBT) {
+                const int v = qa[f], b = lbeg[v], d = ldeg[v];
+                for (int t = 0; t < d; ++t) {
+                    const int u = ladj[b + t];
+                    if (atomicCAS(&dist[u], INT_MAX, level + 1) == INT_MAX) qb[atomicAdd(sh_next, 1u)] = u;
+                }
+            }
+        }
+        __syncthreads();
+        cnt = (int)*sh_next;
+        int* t = qa;
+        qa = qb;
+        qb = t;
+        ++level;
+        __syncthreads();
+    }
+}
+
+// reached node of largest distance, ties to the smaller id
+__device__ int farthest(int n_o, const int* dist, unsigned long long* sh) {
+    unsigned long long best = 0;
+    for (int i = threadIdx.x; i < n_o; i += kBT)
+        if (dist[i] != INT_MAX) {
+            const unsigned long long key = ((unsigned long long)(unsigned)dist[i] << 32) | (0xffffffffu - (unsigned)i);
+            best = max(best, key);
+        }
+    best = block_max(best, sh);
+    return (int)(0xffffffffu - (unsigned)(best & 0xffffffffu));
+}
+
+struct Sub {
+    int n_o;
+    const int *orig, *lbeg, *ldeg, *ladj, *lw;
+    const int* vwgt;  // of the coarsest graph (through orig)
+    __device__ uint32_t c(int i) const { return (uint32_t)vwgt[orig[i]]; }
+};
+
+__device__ void side_weights(const Sub& S, const uint8_t* side, unsigned long long w[2], unsigned long long* sh) {
+    unsigned long long a = 0, b = 0;
+    for (int i = threadIdx.x; i < S.n_o; i += kBT) (side[i] ? b : a) += S.c(i);
+    w[0] = block_sum(a, sh);
+    w[1] = block_sum(b, sh);
+}
+
+__device__ __forceinline__ unsigned long long overload2(const unsigned long long w[2], const unsigned long long mw[2]) {
+    return (w[0] > mw[0] ? w[0] - mw[0] : 0ull) + (w[1] > mw[1] ? w[1] - mw[1] : 0ull);
+}
+
+template <bool WARP>
+__device__ long long cut_of(const Sub& S, const uint8_t* side, unsigned long long* sh) {
+    long long mine = 0;
+    for_rows<WARP>(S.n_o, S.lbeg, S.ldeg,
+                   [&](int i, int e, Acc2& s) { if (side[S.ladj[e]] != side[i]) s.a += S.lw[e]; },
+                   [&](int, const Acc2& s) { mine += s.a; });
+    return (long long)block_sum((unsigned long long)mine, sh) / 2;
+}
+
+__device__ __forceinline__ int loss_bucket_d(long long loss) {
+    if (loss <= 0) return 0;
+    int b = 1;
+    while (b < 31 && (loss >> b) > 0) ++b;
+    return b;
+}
+
+// Moves nodes off side s until it is within mw[s]: classes (log2 bucket of
+// conn(own) - conn(other)) x 8 hashed sub-classes; classes are released in
+// order until their weight covers the excess; released classes move whole
+// while the other side stays within its bound, and in the first class that
+// does not fit, its nodes in id order while the running weight fits.
+template <bool WARP>
+__device__ void balance2(const Sub& S, uint8_t* side, int* cls, int s, const unsigned long long mw[2],
+                         uint64_t ks_cls, int iters, unsigned long long* HS, unsigned long long* sh,
+                         int* sh_int) {
+    for (int it = 0; it < iters; ++it) {
+        unsigned long long w[2];
+        side_weights(S, side, w, sh);
+        if (w[s] <= mw[s]) break;
+        const unsigned long long excess = w[s] - mw[s];
+        const unsigned long long cap = mw[1 - s] > w[1 - s] ? mw[1 - s] - w[1 - s] : 0ull;
+        for (int t = threadIdx.x; t < kIpClasses; t += kBT) HS[t] = 0;
+        __syncthreads();
+        const uint64_t ks = mix64(ks_cls ^ (uint64_t)it);
+        for_rows<WARP>(S.n_o, S.lbeg, S.ldeg,
+                       [&](int i, int e, Acc2& a) {
+                           if (side[S.ladj[e]] == side[i]) a.a += S.lw[e];
+                           else a.b += S.lw[e];
+                       },
+                       [&](int i, const Acc2& a) {
+                           cls[i] = -1;
+                           if (side[i] != s) return;
+                           const int c = loss_bucket_d(a.a - a.b) * 8 + (int)hash_range(hash32(ks, (uint32_t)i), 8u);
+                           cls[i] = c;
+                           atomicAdd(&HS[c], (unsigned long long)S.c(i));
+                       });
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int T = 0;
+            unsigned long long rel = 0;
+            while (T < kIpClasses && rel < excess) rel += HS[T++];
+            int full = 0;
+            unsigned long long used = 0;
+            while (full < T && used + HS[full] <= cap) used += HS[full++];
+            sh_int[0] = T;
+            sh_int[1] = full;
+            HS[kIpClasses] = used;
+        }
+        __syncthreads();
+        const int T = sh_int[0], full = sh_int[1];
+        const unsigned long long used = HS[kIpClasses];
+        unsigned long long moved = 0;
+        // whole classes, then the partial one by id prefix (in chunks of the
+        // block's threads, in id order)
+        unsigned long long run = used;
+        for (int base = 0; base < S.n_o; base += kBT) {
+            const int i = base + threadIdx.x;
+            const int c = i < S.n_o ? cls[i] : -1;
+            if (c >= 0 && c < full) {
+                side[i] = (uint8_t)(1 - s);
+                ++moved;
+            }
+            const bool part_cls = c >= 0 && c == full && full < T;
+            unsigned long long tot;
+            const unsigned long long pre = block_scan(part_cls ? (unsigned long long)S.c(i) : 0ull, &tot, sh);
+            if (part_cls && run + pre + S.c(i) <= cap) {
+                side[i] = (uint8_t)(1 - s);
+                ++moved;
+            }
+            run += tot;
+        }
+        __syncthreads();
+        if (block_sum(moved, sh) == 0) break;
+    }
+}
+
+// 2-way Jet on side[] (best state kept in best[]); returns its cut.
+template <bool WARP>
+__device__ long long jet2(const Sub& S, const IpArgs& a, int r, uint8_t* side, uint8_t* best, uint8_t* dest,
+                          uint8_t* keep, long long* gain, int* moved_at, int* cls, const unsigned long long mw[2],
+                          int bis_level, int bis_round, unsigned long long* HS, unsigned long long* sh,
+                          int* sh_int) {
+    const int n_o = S.n_o;
+    for (int i = threadIdx.x; i < n_o; i += kBT) {
+        moved_at[i] = -2;
+        best[i] = side[i];
+    }
+    __syncthreads();
+    unsigned long long w[2];
+    side_weights(S, side, w, sh);
+    unsigned long long best_ov = overload2(w, mw);
+    long long best_cut = cut_of<WARP>(S, side, sh);
+    const long long c4 = a.jet_c;
+    int since = 0;
+    for (int it = 0; it < a.jet_iters; ++it) {
+        // candidates
+        for_rows<WARP>(n_o, S.lbeg, S.ldeg,
+                       [&](int i, int e, Acc2& s) {
+                           if (side[S.ladj[e]] == side[i]) s.a += S.lw[e];
+                           else s.b += S.lw[e];
+                       },
+                       [&](int i, const Acc2& s) {
+                           dest[i] = 0;
+                           if (moved_at[i] == it - 1 || s.b == 0) return;
+                           const long long gv = s.b - s.a;
+                           if (4 * gv >= -c4 * s.a) {
+                               dest[i] = 1;
+                               gain[i] = gv;
+                           }
+                       });
+        __syncthreads();
+        // afterburner: gain with every higher-priority candidate neighbour moved
+        for_rows<WARP>(n_o, S.lbeg, S.ldeg,
+                       [&](int i, int e, Acc2& s) {
+                           if (!dest[i]) return;
+                           const int u = S.ladj[e];
+                           int su = side[u];
+                           if (dest[u] && (gain[u] > gain[i] || (gain[u] == gain[i] && u < i))) su = 1 - su;
+                           s.a += su != side[i] ? S.lw[e] : -(long long)S.lw[e];
+                       },
+                       [&](int i, const Acc2& s) { keep[i] = dest[i] && s.a >= 0; });
+        __syncthreads();
+        unsigned long long mv = 0;
+        for (int i = threadIdx.x; i < n_o; i += kBT)
+            if (keep[i]) {
+                side[i] ^= 1;
+                moved_at[i] = it;
+                ++mv;
+            }
+        __syncthreads();
+        const unsigned long long moved = block_sum(mv, sh);
+        const uint64_t ks_cls = stream_key(a.seed, TAG_BCLS, bis_level, bis_round * 64 + it);
+        side_weights(S, side, w, sh);
+        for (int s2 = 0; s2 < 2; ++s2)
+            if (w[s2] > mw[s2]) balance2<WARP>(S, side, cls, s2, mw, ks_cls, a.bal_iters, HS, sh, sh_int);
+        side_weights(S, side, w, sh);
+        const unsigned long long ov = overload2(w, mw);
+        const long long cut = cut_of<WARP>(S, side, sh);
+        if (ov < best_ov || (ov == best_ov && cut < best_cut)) {
+            best_ov = ov;
+            best_cut = cut;
+            for (int i = threadIdx.x; i < n_o; i += kBT) best[i] = side[i];
+            since = 0;
+        } else {
+            ++since;
+        }
+        __syncthreads();
+        if (moved == 0 || since >= a.jet_patience) break;
+    }
+    for (int i = threadIdx.x; i < n_o; i += kBT) side[i] = best[i];
+    __syncthreads();
+    return best_cut;
+}
+
+// ---------------------------------------------------------------- kernels
+
+// members and their degrees per (repetition, splitting block)
+__global__ void ip_count(IpArgs a) {
+    const long long total = (long long)a.reps * a.n;
+    for (long long x = (long long)blockIdx.x * blockDim.x + threadIdx.x; x < total;
+         x += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(x / a.n), v = (int)(x % a.n);
+        const int j = a.sidx[a.part[(long long)r * a.n + v]];
+        if (j < 0) continue;
+        atomicAdd(&a.cnt[r * a.nsplit + j], 1u);
+        atomicAdd(&a.deg[r * a.nsplit + j], (unsigned)(a.xadj[v + 1] - a.xadj[v]));
+    }
+}
+
+// node and edge slot bases per (repetition, split): one thread block
+__global__ void ip_bases(IpArgs a) {
+    __shared__ unsigned long long sh[kBW + 1];
+    for (int r = 0; r < a.reps; ++r) {
+        unsigned long long nrun = 0, erun = 0;
+        for (int base = 0; base < a.nsplit; base += kBT) {
+            const int j = base + threadIdx.x;
+            const bool ok = j < a.nsplit;
+            unsigned long long nt, et;
+            const unsigned long long np = block_scan(ok ? a.cnt[r * a.nsplit + j] + 2ull : 0ull, &nt, sh);
+            const unsigned long long ep = block_scan(ok ? (unsigned long long)a.deg[r * a.nsplit + j] : 0ull, &et, sh);
+            if (ok) {
+                a.nbase[r * a.nsplit + j] = (unsigned)(nrun + np);
+                a.ebase[r * a.nsplit + j] = (unsigned)(erun + ep);
+            }
+            nrun += nt;
+            erun += et;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBT) ip_bisect(IpArgs a) {
+    __shared__ unsigned long long sh[kBW + 1];
+    __shared__ unsigned long long HS[kIpClasses + 1];
+    __shared__ unsigned sh_cnt;
+    __shared__ int sh_int[4];
+    const int j = blockIdx.x % a.nsplit, r = blockIdx.x / a.nsplit;
+    const int o = a.split_o[j], kk = a.split_k[j], kl = (kk + 1) / 2;
+    int* part = a.part + (long long)r * a.n;
+    int* lid = a.lid + (long long)r * a.n;
+    const long long nb = (long long)r * a.NS + a.nbase[r * a.nsplit + j];
+    const long long eb = (long long)r * a.ES + a.ebase[r * a.nsplit + j];
+    int* orig = a.orig + nb;
+    int* lbeg = a.lbeg + nb;
+    int* ldeg = a.ldeg + nb;
+    int* ladj = a.ladj + eb;
+    int* lw = a.lw + eb;
+
+    // 1. members in id order -> local ids
+    unsigned long long cnt = 0;
+    for (int base = 0; base < a.n; base += kBT) {
+        const int v = base + threadIdx.x;
+        const bool mem = v < a.n && part[v] == o;
+        unsigned long long tot;
+        const unsigned long long pre = block_scan(mem ? 1ull : 0ull, &tot, sh);
+        if (mem) {
+            lid[v] = (int)(cnt + pre);
+            orig[cnt + pre] = v;
+        }
+        cnt += tot;
+    }
+    const int n_o = (int)cnt;
+    __syncthreads();
+    if (n_o == 0) return;
+    // 2. rows restricted to the block: degrees, then entries (local ids)
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int i = wid; i < n_o; i += kBW) {
+        const int v = orig[i];
+        int d = 0;
+        for (int e = a.xadj[v] + lane; e < a.xadj[v + 1]; e += 32) d += part[a.adjncy[e]] == o;
+        d = __reduce_add_sync(0xffffffffu, d);
+        if (lane == 0) ldeg[i] = d;
+    }
+    __syncthreads();
+    unsigned long long erun = 0;
+    for (int base = 0; base < n_o; base += kBT) {
+        const int i = base + threadIdx.x;
+        unsigned long long tot;
+        const unsigned long long pre = block_scan(i < n_o ? (unsigned long long)ldeg[i] : 0ull, &tot, sh);
+        if (i < n_o) lbeg[i] = (int)(erun + pre);
+        erun += tot;
+    }
+    __syncthreads();
+    for (int i = wid; i < n_o; i += kBW) {
+        const int v = orig[i];
+        int w = lbeg[i];
+        for (int e0 = a.xadj[v]; e0 < a.xadj[v + 1]; e0 += 32) {
+            const int e = e0 + lane;
+            const bool in = e < a.xadj[v + 1] && part[a.adjncy[e]] == o;
+            const unsigned m = __ballot_sync(0xffffffffu, in);
+            if (in) {
+                const int p = w + __popc(m & ((1u << lane) - 1u));
+                ladj[p] = lid[a.adjncy[e]];
+                lw[p] = a.adjwgt[e];
+            }
+            w += __popc(m);
+        }
+    }
+    __syncthreads();
+    const Sub S{n_o, orig, lbeg, ldeg, ladj, lw, a.vwgt};
+    // targets and bounds
+    unsigned long long Wm = 0;
+    for (int i = threadIdx.x; i < n_o; i += kBT) Wm += S.c(i);
+    const unsigned long long W = block_sum(Wm, sh);
+    const unsigned long long t0 = W * (unsigned long long)kl / (unsigned long long)kk, t1 = W - t0;
+    const double eb2 = a.split_eb[j];
+    const unsigned long long mw[2] = {(unsigned long long)((1.0 + eb2) * (double)t0),
+                                      (unsigned long long)((1.0 + eb2) * (double)t1)};
+    const long long ns = (long long)r * a.NS + a.nbase[r * a.nsplit + j];
+    int* dist = a.dist + ns;
+    int* qa = a.qa + ns;
+    int* qb = a.qb + ns;
+    int* moved_at = a.moved_at + ns;
+    int* cls = a.cls + ns;
+    uint8_t* side = a.side + ns;
+    uint8_t* best = a.best + ns;
+    uint8_t* dest = a.dest + ns;
+    uint8_t* keep = a.keep + ns;
+    long long* gain = a.gain + ns;
+    unsigned long long* layer = a.layer + ns;
+    uint8_t* won = a.won + ns;  // the best try's sides
+    const bool warp_rows = erun >= (unsigned long long)kDenseRows * (unsigned long long)n_o;
+    const int bis_level = o, bis_round0 = r * 32 + a.depth;
+    long long best_cut = LLONG_MAX;
+    unsigned long long best_ov = ~0ull;
+    for (int t = 0; t < a.tries; ++t) {
+        const uint64_t ks = stream_key(a.seed, TAG_IP, bis_level, bis_round0 * 64 + t);
+        unsigned long long m0 = ~0ull;
+        for (int i = threadIdx.x; i < n_o; i += kBT)
+            m0 = min(m0, ((unsigned long long)hash32(ks, (uint32_t)i) << 32) | (unsigned)i);
+        const int s0 = (int)(block_min(m0, sh) & 0xffffffffu);
+        if (warp_rows) bfs<true>(n_o, s0, dist, qa, qb, lbeg, ldeg, ladj, &sh_cnt);
+        else bfs<false>(n_o, s0, dist, qa, qb, lbeg, ldeg, ladj, &sh_cnt);
+        const int s1 = farthest(n_o, dist, sh);
+        if (warp_rows) bfs<true>(n_o, s1, dist, qa, qb, lbeg, ldeg, ladj, &sh_cnt);
+        else bfs<false>(n_o, s1, dist, qa, qb, lbeg, ldeg, ladj, &sh_cnt);
+        const int st = farthest(n_o, dist, sh);
+        if (warp_rows) bfs<true>(n_o, st, dist, qa, qb, lbeg, ldeg, ladj, &sh_cnt);
+        else bfs<false>(n_o, st, dist, qa, qb, lbeg, ldeg, ladj, &sh_cnt);
+        // growing by (distance, id): layer weights, the crossing layer, and
+        // the crossing layer's id-order prefix
+        unsigned long long md = 0;
+        for (int i = threadIdx.x; i < n_o; i += kBT)
+            if (dist[i] != INT_MAX) md = max(md, (unsigned long long)dist[i]);
+        const int maxd = (int)block_max(md, sh);
+        const int nl = maxd + 2;
+        for (int l = threadIdx.x; l < nl; l += kBT) layer[l] = 0;
+        __syncthreads();
+        for (int i = threadIdx.x; i < n_o; i += kBT)
+            atomicAdd(&layer[dist[i] == INT_MAX ? maxd + 1 : dist[i]], (unsigned long long)S.c(i));
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long cum = 0;
+            int lc = 0;
+            while (lc < nl && cum + layer[lc] < t0) cum += layer[lc++];
+            sh_int[2] = lc;
+            HS[kIpClasses] = cum;
+        }
+        __syncthreads();
+        const int lc = sh_int[2];
+        unsigned long long run = HS[kIpClasses];
+        __syncthreads();
+        for (int base = 0; base < n_o; base += kBT) {
+            const int i = base + threadIdx.x;
+            int l = INT_MAX;
+            if (i < n_o) {
+                l = dist[i] == INT_MAX ? maxd + 1 : dist[i];
+                side[i] = l < lc ? 0 : 1;
+            }
+            const bool cross = i < n_o && l == lc;
+            unsigned long long tot;
+            const unsigned long long pre = block_scan(cross ? (unsigned long long)S.c(i) : 0ull, &tot, sh);
+            if (cross) {
+                const unsigned long long p = run + pre + S.c(i);
+                if (run + pre < t0 && p <= mw[0]) side[i] = 0;
+            }
+            run += tot;
+        }
+        __syncthreads();
+        const long long c = warp_rows
+                                ? jet2<true>(S, a, r, side, best, dest, keep, gain, moved_at, cls, mw, bis_level,
+                                             bis_round0 * 64 + t, HS, sh, sh_int)
+                                : jet2<false>(S, a, r, side, best, dest, keep, gain, moved_at, cls, mw, bis_level,
+                                              bis_round0 * 64 + t, HS, sh, sh_int);
+        unsigned long long w[2];
+        side_weights(S, side, w, sh);
+        const unsigned long long ov = overload2(w, mw);
+        if (ov < best_ov || (ov == best_ov && c < best_cut)) {
+            best_ov = ov;
+            best_cut = c;
+            for (int i = threadIdx.x; i < n_o; i += kBT) won[i] = side[i];
+        }
+        __syncthreads();
+    }
+    // 3. the winner's side 1 becomes block o + kl
+    for (int i = threadIdx.x; i < n_o; i += kBT)
+        if (won[i]) part[orig[i]] = o + kl;
+}
+
+}  // namespace
+
+void initial_partition_device(Ctx& ctx, const DevGraph& c, const Knobs& kn, int* part) {
+    cudaStream_t st = ctx.stream;
+    const int n = c.n, k = kn.k;
+    if (n == 0) return;
+    const int reps = std::max(kn.ip_reps, 1);
+    int tries = std::max(kn.ip_tries, 1);
+    if (c.m > 64LL * n) tries = std::min(tries, 1);  // dense coarsest graphs: one try
+    // the recursion's shape depends only on k: per depth the (offset, count)
+    // of every block that splits
+    std::vector<std::vector<int>> so, sk;
+    {
+        std::vector<int> kb((size_t)k, 0);
+        kb[0] = k;
+        for (int d = 0; d < 32; ++d) {
+            std::vector<int> o, kk;
+            for (int b = 0; b < k; ++b)
+                if (kb[b] > 1) { o.push_back(b); kk.push_back(kb[b]); }
+            if (o.empty()) break;
+            for (size_t i = 0; i < o.size(); ++i) {
+                const int kl = (kk[i] + 1) / 2;
+                kb[(size_t)o[i]] = kl;
+                kb[(size_t)(o[i] + kl)] = kk[i] - kl;
+            }
+            so.push_back(o);
+            sk.push_back(kk);
+        }
+    }
+    const size_t mk = ctx.scratch.mark();
+    int maxs = 1;
+    for (auto& v : so) maxs = std::max(maxs, (int)v.size());
+    // tables for all depths in one upload: [o | k | sidx] per depth
+    std::vector<int> tab;
+    std::vector<size_t> toff;
+    for (size_t d = 0; d < so.size(); ++d) {
+        toff.push_back(tab.size());
+        tab.insert(tab.end(), so[d].begin(), so[d].end());
+        tab.insert(tab.end(), sk[d].begin(), sk[d].end());
+        std::vector<int> sidx((size_t)k, -1);
+        for (size_t i = 0; i < so[d].size(); ++i) sidx[(size_t)so[d][i]] = (int)i;
+        tab.insert(tab.end(), sidx.begin(), sidx.end());
+    }
+    // per split: the per-side slack max((1+eps)^(1/ceil log2 kk) - 1, min(eps, 1%))
+    const double eps = kn.imbalance > 0 ? kn.imbalance : 0.0;
+    std::vector<double> ebs;
+    for (size_t d = 0; d < so.size(); ++d)
+        for (int kk : sk[d]) {
+            int lg = 0;
+            while ((1 << lg) < kk) ++lg;
+            double eb = std::pow(1.0 + eps, 1.0 / lg) - 1.0;
+            eb = std::max(eb, std::min(eps, 0.01));
+            ebs.push_back(eb);
+        }
+    int* dtab = ctx.scratch.alloc<int>(std::max<size_t>(tab.size(), 1));
+    double* deb = ctx.scratch.alloc<double>(std::max<size_t>(ebs.size(), 1));
+    if (!tab.empty()) KB_CUDA(cudaMemcpyAsync(dtab, tab.data(), sizeof(int) * tab.size(), cudaMemcpyHostToDevice, st));
+    if (!ebs.empty()) KB_CUDA(cudaMemcpyAsync(deb, ebs.data(), sizeof(double) * ebs.size(), cudaMemcpyHostToDevice, st));
+    IpArgs a{};
+    a.n = n;
+    a.xadj = c.xadj;
+    a.adjncy = c.adjncy;
+    a.adjwgt = c.adjwgt;
+    a.vwgt = c.vwgt;
+    a.reps = reps;
+    a.NS = (long long)n + 2LL * maxs;
+    a.ES = std::max<long long>(c.m, 1);
+    a.part = ctx.scratch.alloc<int>((size_t)reps * n);
+    a.cnt = ctx.scratch.alloc<unsigned>((size_t)reps * maxs);
+    a.deg = ctx.scratch.alloc<unsigned>((size_t)reps * maxs);
+    a.nbase = ctx.scratch.alloc<unsigned>((size_t)reps * maxs);
+    a.ebase = ctx.scratch.alloc<unsigned>((size_t)reps * maxs);
+    a.lid = ctx.scratch.alloc<int>((size_t)reps * n);
+    const size_t NSr = (size_t)reps * (size_t)a.NS, ESr = (size_t)reps * (size_t)a.ES;
+    a.orig = ctx.scratch.alloc<int>(NSr);
+    a.lbeg = ctx.scratch.alloc<int>(NSr);
+    a.ldeg = ctx.scratch.alloc<int>(NSr);
+    a.dist = ctx.scratch.alloc<int>(NSr);
+    a.qa = ctx.scratch.alloc<int>(NSr);
+    a.qb = ctx.scratch.alloc<int>(NSr);
+    a.moved_at = ctx.scratch.alloc<int>(NSr);
+    a.cls = ctx.scratch.alloc<int>(NSr);
+    a.ladj = ctx.scratch.alloc<int>(ESr);
+    a.lw = ctx.scratch.alloc<int>(ESr);
+    a.side = ctx.scratch.alloc<uint8_t>(NSr);
+    a.best = ctx.scratch.alloc<uint8_t>(NSr);
+    a.dest = ctx.scratch.alloc<uint8_t>(NSr);
+    a.keep = ctx.scratch.alloc<uint8_t>(NSr);
+    a.won = ctx.scratch.alloc<uint8_t>(NSr);
+    a.gain = ctx.scratch.alloc<long long>(NSr);
+    a.layer = ctx.scratch.alloc<unsigned long long>(NSr);
+    a.seed = kn.seed;
+    a.tries = tries;
+    a.jet_iters = kn.jet_iters;
+    a.jet_patience = kn.jet_patience;
+    a.jet_c = kn.jet_c;
+    a.bal_iters = kn.bal_iters;
+    a.eps = eps;
+    a.err = ctx.dscalars + 60;
+    KB_CUDA(cudaMemsetAsync(a.part, 0, sizeof(int) * (size_t)reps * n, st));
+    {
+        PhaseScope ps(ctx, "initial_device", 0);
+        size_t eoff = 0;
+        for (size_t d = 0; d < so.size(); ++d) {
+            a.depth = (int)d;
+            a.nsplit = (int)so[d].size();
+            a.split_eb = deb + eoff;
+            eoff += (size_t)a.nsplit;
+            a.split_o = dtab + toff[d];
+            a.split_k = a.split_o + a.nsplit;
+            a.sidx = a.split_k + a.nsplit;
+            KB_CUDA(cudaMemsetAsync(a.cnt, 0, sizeof(unsigned) * (size_t)reps * a.nsplit, st));
+            KB_CUDA(cudaMemsetAsync(a.deg, 0, sizeof(unsigned) * (size_t)reps * a.nsplit, st));
+            const long long tot = (long long)reps * n;
+            ip_count<<<(int)std::max<long long>(1, std::min<long long>(div_up(tot, 256), (long long)kNumSMs * 8)), 256, 0,
+                       st>>>(a);
+            KB_LAUNCH();
+            ip_bases<<<1, kBT, 0, st>>>(a);
+            KB_LAUNCH();
+            ip_bisect<<<a.nsplit * reps, kBT, 0, st>>>(a);
+            KB_LAUNCH();
+        }
+    }
+    // the repetition of the smallest cut (the first on ties)
+    int win = 0;
+    if (reps > 1) {
+        uint32_t* bw = ctx.scratch.alloc<uint32_t>((size_t)k);
+        unsigned long long* c2 = reinterpret_cast<unsigned long long*>(ctx.dscalars + 32);
+        long long bestc = LLONG_MAX;
+        for (int r = 0; r < reps; ++r) {
+            block_weights_and_cut(ctx, c, a.part + (size_t)r * n, k, bw, c2);
+            unsigned long long h = 0;
+            KB_CUDA(cudaMemcpyAsync(&h, c2, sizeof(h), cudaMemcpyDeviceToHost, st));
+            KB_CUDA(cudaStreamSynchronize(st));
+            if ((long long)(h / 2) < bestc) { bestc = (long long)(h / 2); win = r; }
+        }
+    }
+    KB_CUDA(cudaMemcpyAsync(part, a.part + (size_t)win * n, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, st));
+    KB_CUDA(cudaStreamSynchronize(st));
+    ctx.scratch.release(mk);
+}
+
+}  // namespace kb

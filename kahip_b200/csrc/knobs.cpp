@@ -88,6 +88,9 @@ void derive_knobs_total(int n, uint32_t W, int k, double imbalance, int seed, in
     kn.jet_patience = 12;                // 0.25 of the own connection on the finest level,
     kn.jet_c0 = 1;                       // 0.75 on coarser ones
     kn.jet_c = 3;
+    // initial partitioning on the device: every bisection of a recursion
+    // depth in one launch (breadth-first growing, 2-way Jet refinement)
+    kn.ip_mode = 1;
 }
 
 }  // namespace kb

@@ -477,11 +477,15 @@ __device__ int packed_members(const SweepArgs& a, int v, int* smap, unsigned lon
         // several equally connected candidates), then the smaller label
         const uint32_t cown = __reduce_add_sync(rmask, (leader && isown) ? sum : 0u);
         const uint32_t maxc = __reduce_max_sync(rmask, cand ? sum : 0u);
+        // (every lane executes each warp intrinsic: none sits behind a
+        // short-circuiting condition)
         bool tie = cand && sum == maxc;
-        const bool multi = tie && __popc(__ballot_sync(0xffffffffu, tie) & rmask) > 1;
+        const unsigned tb = __ballot_sync(0xffffffffu, tie);
+        const bool multi = tie && __popc(tb & rmask) > 1;
         if (__any_sync(0xffffffffu, multi)) {
             const uint32_t h = multi ? (single ? a.tie[l] : hash32(a.ks_tie, l)) : 0xffffffffu;
-            tie = tie && h == __reduce_min_sync(rmask, h);
+            const uint32_t mh = __reduce_min_sync(rmask, h);
+            tie = tie && h == mh;
         }
         const uint32_t id = __reduce_min_sync(rmask, tie ? l : kEmpty);
         // each member reads its results from its row's first lane

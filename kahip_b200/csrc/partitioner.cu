@@ -12,6 +12,7 @@
 #include "combine.cuh"
 #include "contract.cuh"
 #include "host/initial_partitioning.h"
+#include "ip_device.cuh"
 #include "jet.cuh"
 #include "learned.cuh"
 #include "match.cuh"
@@ -229,6 +230,14 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
         const DevGraph& c = lv[L].g;
         if (c.n)
             KB_CUDA(cudaMemcpyAsync(lv[L].part, P1[L], sizeof(int) * (size_t)c.n, cudaMemcpyDeviceToDevice, s));
+        const size_t mk = ctx.scratch.mark();
+        uint32_t* tbw = ctx.scratch.alloc<uint32_t>((size_t)k);
+        initial_cut = read_cut(ctx, c, lv[L].part, k, tbw);
+        ctx.scratch.release(mk);
+    } else if (kn.ip_mode == 1) {
+        // on the device: every bisection of a recursion depth in one launch
+        const DevGraph& c = lv[L].g;
+        initial_partition_device(ctx, c, kn, lv[L].part);
         const size_t mk = ctx.scratch.mark();
         uint32_t* tbw = ctx.scratch.alloc<uint32_t>((size_t)k);
         initial_cut = read_cut(ctx, c, lv[L].part, k, tbw);

@@ -118,6 +118,7 @@ void or_derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, 
     o->jet_patience = 12;
     o->jet_c0 = 1;
     o->jet_c = 3;
+    o->ip_mode = 1;
 }
 
 /* stop_rules.h:64-66: continue coarsening after a level that went from nf to
@@ -1328,6 +1329,313 @@ void or_initial_partition(const or_graph* g, const or_knobs* knobs, int* part) {
     free(cand);
 }
 
+/* ---------------------------- batched recursive bisection (the device's form) */
+
+/* The device runs every bisection of one recursion depth together, one
+ * thread block per block of the current partition, each on the subgraph
+ * its block induces.  The recursion and its bounds are the host form's
+ * (graph_partitioner.cpp:110-238 as restated in rb above): the left half
+ * gets ceil(k/2) blocks, targets in proportion, per-side slack eb.  A
+ * bisection runs `ip_tries` tries and keeps the best by (overload, cut),
+ * the first on ties; a try:
+ *   1. start: s0 = the node of smallest (hash, id); two breadth-first
+ *      searches (bipartition.cpp:125-146) give the reached node farthest
+ *      from s0, then the reached node farthest from that one (ties: smaller
+ *      id), the start;
+ *   2. growing (bipartition.cpp:147-222 grows by gain; here by distance):
+ *      nodes in (BFS distance from the start, id) order, unreached nodes
+ *      last by id; side 0 takes the order's prefix until it reaches t0 --
+ *      the node that crosses t0 joins only if side 0 stays within max0;
+ *   3. 2-way Jet refinement (the synchronous form of or_jet_refine with two
+ *      labels and a bound per side) with a balance repair per side. */
+
+static void bfs_dist(const or_graph* g, int s, int* dist, int* queue) {
+    for (int v = 0; v < g->n; ++v) dist[v] = INT_MAX;
+    int head = 0, tail = 0;
+    dist[s] = 0;
+    queue[tail++] = s;
+    while (head < tail) {
+        const int v = queue[head++];
+        for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) {
+            const int u = g->adjncy[e];
+            if (dist[u] == INT_MAX) { dist[u] = dist[v] + 1; queue[tail++] = u; }
+        }
+    }
+}
+
+/* reached node of largest distance, ties to the smaller id */
+static int farthest_node(const or_graph* g, const int* dist) {
+    int best = 0, bd = -1;
+    for (int v = 0; v < g->n; ++v)
+        if (dist[v] != INT_MAX && dist[v] > bd) { bd = dist[v]; best = v; }
+    return best;
+}
+
+static void grow_bfs(const or_graph* g, const int* dist, uint64_t t0, uint64_t max0, char* side) {
+    const int n = g->n;
+    int maxd = 0;
+    for (int v = 0; v < n; ++v) if (dist[v] != INT_MAX && dist[v] > maxd) maxd = dist[v];
+    /* layer of v: its distance, unreached nodes form layer maxd + 1 */
+    uint64_t* lw = xcalloc((size_t)maxd + 2, sizeof(uint64_t));
+    for (int v = 0; v < n; ++v) lw[dist[v] == INT_MAX ? maxd + 1 : dist[v]] += (uint64_t)g->vwgt[v];
+    uint64_t cum = 0;
+    int lc = 0;
+    while (lc <= maxd + 1 && cum + lw[lc] < t0) cum += lw[lc++];
+    for (int v = 0; v < n; ++v) {
+        const int l = dist[v] == INT_MAX ? maxd + 1 : dist[v];
+        side[v] = l < lc ? 0 : 1;
+    }
+    if (lc <= maxd + 1) {
+        /* the crossing layer in id order: P = inclusive prefix weight */
+        for (int v = 0; v < n; ++v) {
+            const int l = dist[v] == INT_MAX ? maxd + 1 : dist[v];
+            if (l != lc) continue;
+            if (cum >= t0) break;
+            const uint64_t p = cum + (uint64_t)g->vwgt[v];
+            if (p <= max0) side[v] = 0;
+            cum = p;
+        }
+    }
+    free(lw);
+}
+
+static void side_weights(const or_graph* g, const char* side, uint64_t w[2]) {
+    w[0] = w[1] = 0;
+    for (int v = 0; v < g->n; ++v) w[(int)side[v]] += (uint64_t)g->vwgt[v];
+}
+
+/* connection of v to its own side (*co) and to the other side (*cx) */
+static void side_conn(const or_graph* g, const char* side, int v, long long* co, long long* cx) {
+    long long a = 0, b = 0;
+    for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) {
+        if (side[g->adjncy[e]] == side[v]) a += g->adjwgt[e];
+        else b += g->adjwgt[e];
+    }
+    *co = a;
+    *cx = b;
+}
+
+/* Moves nodes off side s until it is within maxw[s] (the balance repair of
+ * or_balance for two labels): every node of s gets a class, log2 bucket of
+ * its loss conn(own) - conn(other) times 8 hashed sub-classes; classes are
+ * released in order until their weight covers the excess; released classes
+ * move in order while the other side stays within its bound, and in the
+ * first class that does not fit whole, its nodes in id order while the
+ * running weight fits. */
+static void balance2(const or_graph* g, char* side, int s, const uint64_t maxw[2], uint64_t ks_cls, int iters) {
+    const int n = g->n;
+    int* cls = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    for (int it = 0; it < iters; ++it) {
+        uint64_t w[2];
+        side_weights(g, side, w);
+        if (w[s] <= maxw[s]) break;
+        const uint64_t excess = w[s] - maxw[s];
+        const uint64_t cap = maxw[1 - s] > w[1 - s] ? maxw[1 - s] - w[1 - s] : 0;
+        uint64_t HS[BAL_CLASSES];
+        memset(HS, 0, sizeof(HS));
+        const uint64_t ks = or_mix64(ks_cls ^ (uint64_t)it);
+        for (int v = 0; v < n; ++v) {
+            cls[v] = -1;
+            if (side[v] != s) continue;
+            long long co, cx;
+            side_conn(g, side, v, &co, &cx);
+            cls[v] = loss_bucket(co - cx) * 8 + (int)or_range(or_hash(ks, (uint32_t)v), 8u);
+            HS[cls[v]] += (uint64_t)g->vwgt[v];
+        }
+        int T = 0;
+        uint64_t rel = 0;
+        while (T < BAL_CLASSES && rel < excess) rel += HS[T++];
+        /* classes [0, full) move whole; class `full` (if < T) moves by id prefix */
+        int full = 0;
+        uint64_t used = 0;
+        while (full < T && used + HS[full] <= cap) used += HS[full++];
+        uint64_t run = used;
+        int moved = 0;
+        for (int v = 0; v < n; ++v) {
+            if (cls[v] < 0) continue;
+            if (cls[v] < full) { side[v] = (char)(1 - s); ++moved; continue; }
+            if (cls[v] == full && full < T) {
+                run += (uint64_t)g->vwgt[v];
+                if (run <= cap) { side[v] = (char)(1 - s); ++moved; }
+            }
+        }
+        if (!moved) break;
+    }
+    free(cls);
+}
+
+/* 2-way Jet refinement with a bound per side (or_jet_refine for two labels,
+ * c4 = jet_c); returns the cut of the best (overload, cut) state kept */
+static long long jet2(const or_graph* g, char* side, const uint64_t maxw[2], const or_knobs* kn, int bis_level,
+                      int bis_round) {
+    const int n = g->n;
+    char* best = xmalloc((size_t)(n ? n : 1));
+    char* dest = xcalloc((size_t)(n ? n : 1), 1);
+    char* keep = xcalloc((size_t)(n ? n : 1), 1);
+    long long* gain = xmalloc(sizeof(long long) * (size_t)(n ? n : 1));
+    int* moved_at = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    for (int v = 0; v < n; ++v) moved_at[v] = -2;
+    memcpy(best, side, (size_t)n);
+    uint64_t w[2];
+    side_weights(g, side, w);
+    uint64_t best_ov = overload2(w, maxw);
+    long long best_cut = cut2(g, side);
+    const int c4 = kn->jet_c;
+    int since = 0;
+    for (int it = 0; it < kn->jet_iters; ++it) {
+        for (int v = 0; v < n; ++v) {
+            dest[v] = 0;
+            if (moved_at[v] == it - 1) continue;
+            long long co, cx;
+            side_conn(g, side, v, &co, &cx);
+            if (cx == 0) continue;
+            const long long gv = cx - co;
+            if (4 * gv >= -(long long)c4 * co) { dest[v] = 1; gain[v] = gv; }
+        }
+        long long moved = 0;
+        for (int v = 0; v < n; ++v) {
+            keep[v] = 0;
+            if (!dest[v]) continue;
+            long long adj = 0;
+            for (int e = g->xadj[v]; e < g->xadj[v + 1]; ++e) {
+                const int u = g->adjncy[e];
+                int su = side[u];
+                if (dest[u] && (gain[u] > gain[v] || (gain[u] == gain[v] && u < v))) su = 1 - su;
+                adj += su != side[v] ? g->adjwgt[e] : -(long long)g->adjwgt[e];
+            }
+            keep[v] = adj >= 0;
+        }
+        for (int v = 0; v < n; ++v) {
+            if (!keep[v]) continue;
+            side[v] = (char)(1 - side[v]);
+            moved_at[v] = it;
+            ++moved;
+        }
+        const uint64_t ks_cls = or_stream(kn->seed, TAG_BCLS, bis_level, bis_round * 64 + it);
+        side_weights(g, side, w);
+        for (int s2 = 0; s2 < 2; ++s2)
+            if (w[s2] > maxw[s2]) balance2(g, side, s2, maxw, ks_cls, kn->bal_iters);
+        side_weights(g, side, w);
+        const uint64_t ov = overload2(w, maxw);
+        const long long cut = cut2(g, side);
+        if (ov < best_ov || (ov == best_ov && cut < best_cut)) {
+            best_ov = ov;
+            best_cut = cut;
+            memcpy(best, side, (size_t)n);
+            since = 0;
+        } else {
+            ++since;
+        }
+        if (moved == 0 || since >= kn->jet_patience) break;
+    }
+    memcpy(side, best, (size_t)n);
+    free(best); free(dest); free(keep); free(gain); free(moved_at);
+    return best_cut;
+}
+
+/* One bisection of the batched form; bis_level / bis_round key its hash
+ * streams (the block's offset, and (repetition, depth)). */
+static void batched_bisect(const or_graph* g, uint64_t t0, const uint64_t maxw[2], const or_knobs* kn,
+                           int bis_level, int bis_round, char* best_side) {
+    const int n = g->n;
+    char* side = xmalloc((size_t)(n ? n : 1));
+    int* dist = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    int* queue = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    long long best_cut = LLONG_MAX;
+    uint64_t best_ov = UINT64_MAX;
+    for (int t = 0; t < kn->ip_tries; ++t) {
+        const uint64_t ks = or_stream(kn->seed, TAG_IP, bis_level, bis_round * 64 + t);
+        int s0 = 0;
+        uint32_t hbest = UINT32_MAX;
+        for (int v = 0; v < n; ++v) {
+            const uint32_t h = or_hash(ks, (uint32_t)v);
+            if (h < hbest) { hbest = h; s0 = v; }
+        }
+        bfs_dist(g, s0, dist, queue);
+        const int s1 = farthest_node(g, dist);
+        bfs_dist(g, s1, dist, queue);
+        const int start = farthest_node(g, dist);
+        bfs_dist(g, start, dist, queue);
+        grow_bfs(g, dist, t0, maxw[0], side);
+        const long long c = jet2(g, side, maxw, kn, bis_level, bis_round * 64 + t);
+        uint64_t w[2];
+        side_weights(g, side, w);
+        const uint64_t ov = overload2(w, maxw);
+        if (ov < best_ov || (ov == best_ov && c < best_cut)) {
+            best_ov = ov;
+            best_cut = c;
+            memcpy(best_side, side, (size_t)n);
+        }
+    }
+    free(side); free(dist); free(queue);
+}
+
+/* Every bisection of a depth sees the partition at the depth's start; a
+ * block is named by its offset o (its first final block id) and still
+ * splits into kb[o] blocks. */
+static void rb_batched(const or_graph* g, const or_knobs* kn, int rep, int* part) {
+    const int n = g->n, k = kn->k;
+    int* kb = xcalloc((size_t)k, sizeof(int));
+    int* kb_next = xcalloc((size_t)k, sizeof(int));
+    kb[0] = k;
+    for (int v = 0; v < n; ++v) part[v] = 0;
+    const double eps = kn->imbalance > 0 ? kn->imbalance : 0.0;
+    int* nid = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    char* all = xcalloc((size_t)(n ? n : 1), 1);
+    for (int depth = 0; depth < 32; ++depth) {
+        int any = 0;
+        memcpy(kb_next, kb, sizeof(int) * (size_t)k);
+        for (int o = 0; o < k; ++o) {
+            if (kb[o] <= 1) continue;
+            any = 1;
+            /* the block's subgraph, ids in increasing order */
+            or_sub S;
+            for (int v = 0; v < n; ++v) all[v] = part[v] == o ? 0 : 1;
+            int* orig = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+            for (int v = 0; v < n; ++v) orig[v] = v;
+            extract(g, orig, all, 0, &S);
+            free(orig);
+            const int kk = kb[o], kl = (kk + 1) / 2;
+            uint64_t W = 0;
+            for (int v = 0; v < S.n; ++v) W += (uint64_t)S.vwgt[v];
+            const uint64_t t0 = W * (uint64_t)kl / (uint64_t)kk, t1 = W - t0;
+            double eb = pow(1.0 + eps, 1.0 / ceil_log2(kk)) - 1.0;
+            const double floor_eb = eps < 0.01 ? eps : 0.01;
+            if (eb < floor_eb) eb = floor_eb;
+            const uint64_t maxw[2] = {(uint64_t)((1.0 + eb) * (double)t0), (uint64_t)((1.0 + eb) * (double)t1)};
+            char* side = xcalloc((size_t)(S.n ? S.n : 1), 1);
+            if (S.n > 0) {
+                or_graph sg = {S.n, S.xadj, S.adjncy, S.adjwgt, S.vwgt};
+                batched_bisect(&sg, t0, maxw, kn, o, rep * 32 + depth, side);
+            }
+            for (int i = 0; i < S.n; ++i)
+                if (side[i]) part[S.orig[i]] = o + kl;
+            kb_next[o] = kl;
+            kb_next[o + kl] = kk - kl;
+            free(side);
+            sub_free(&S);
+        }
+        memcpy(kb, kb_next, sizeof(int) * (size_t)k);
+        if (!any) break;
+    }
+    free(kb); free(kb_next); free(nid); free(all);
+}
+
+void or_initial_partition_batched(const or_graph* g, const or_knobs* knobs, int* part) {
+    const int n = g->n;
+    or_knobs dense = *knobs;
+    if ((long long)g->xadj[n] > 64LL * n) dense.ip_tries = dense.ip_tries < 1 ? dense.ip_tries : 1;
+    const or_knobs* kn = &dense;
+    int* cand = xmalloc(sizeof(int) * (size_t)(n ? n : 1));
+    long long best = LLONG_MAX;
+    for (int rep = 0; rep < kn->ip_reps; ++rep) {
+        rb_batched(g, kn, rep, cand);
+        const long long c = or_edge_cut(g, cand);
+        if (c < best) { best = c; memcpy(part, cand, sizeof(int) * (size_t)n); }
+    }
+    free(cand);
+}
+
 /* ------------------------------------------------------------ full call */
 
 typedef struct {
@@ -1472,7 +1780,8 @@ static int kaffpa_core(int n, const int* vwgt, const int* xadj, const int* adjcw
         }
         memcpy(cpart, P1[L], sizeof(int) * (size_t)lv[L].g.n);
     } else {
-        or_initial_partition(&lv[L].g, &kn, cpart);
+        if (kn.ip_mode == 1) or_initial_partition_batched(&lv[L].g, &kn, cpart);
+        else or_initial_partition(&lv[L].g, &kn, cpart);
     }
     st.initial_cut = or_edge_cut(&lv[L].g, cpart);
     uint32_t* bw = xcalloc((size_t)nparts, sizeof(uint32_t));

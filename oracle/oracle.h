@@ -52,6 +52,8 @@ typedef struct {
     int rating_levels;         /* unused by the oracle */
     int refinement;            /* 0 = LP refinement, 1 = Jet refinement */
     int jet_iters, jet_patience, jet_c0, jet_c;
+    int ip_mode;               /* 0 = multilevel recursive bisection with FM (host form),
+                                  1 = batched recursive bisection (the device's form) */
 } or_knobs;
 
 typedef struct {
@@ -122,6 +124,9 @@ void or_lp_refine_seq(const or_graph* g, int k, uint32_t bound, int rounds, cons
 int or_balance(const or_graph* g, const or_knobs* kn, int level, uint32_t bound, int* part);
 
 /* initial partitioning of a (coarsest) graph into kn->k blocks */
+/* batched recursive bisection: every bisection of a depth together (the
+ * device's initial partitioner) */
+void or_initial_partition_batched(const or_graph* g, const or_knobs* kn, int* part);
 void or_initial_partition(const or_graph* g, const or_knobs* kn, int* part);
 
 /* whole multilevel call, kaffpa() semantics (interface/kaHIP_interface.h:30-33).

@@ -55,9 +55,8 @@ def _device_graph(d):
         assert g["m"] == d["m_directed"]
         assert _graph_sha256(g) == d["graph_sha256"], "the seeded generator no longer makes the recorded graph"
         dev = torch.device("cuda", 0)
-        unit = d["graph"] != "rmat"
         t = {k: torch.from_numpy(g[k]).to(dev) for k in ("xadj", "adjncy", "adjwgt", "vwgt")}
-        _CACHE[key] = (g, t, unit)
+        _CACHE[key] = (g, t)
     return _CACHE[key]
 
 
@@ -68,15 +67,15 @@ def test_device_path_matches_oracle_digest(name):
     from kahip_b200 import native
     assert native.device_count() > 0, "needs a CUDA device"
     d = DIGESTS[name]
-    g, t, unit = _device_graph(d)
+    g, t = _device_graph(d)
     n = g["n"]
     part = torch.empty(n, dtype=torch.int32, device=t["xadj"].device)
     st = native.Stats()
     st.collect_level_cuts = 1
-    # unit-weight graphs go in with NULL weights, as the benchmark passes them
-    rc, cut = native.kaffpa_device(n, t["xadj"], t["adjncy"], None if unit else t["adjwgt"],
-                                   None if unit else t["vwgt"], part, d["k"], d["imbalance"], d["seed"],
-                                   d["mode"], stats=st)
+    # the device entry point takes explicit weights (all ones for the
+    # geometric graphs, which its input check recognises as unit weights)
+    rc, cut = native.kaffpa_device(n, t["xadj"], t["adjncy"], t["adjwgt"], t["vwgt"], part, d["k"],
+                                   d["imbalance"], d["seed"], d["mode"], stats=st)
     torch.cuda.synchronize()
     p = part.cpu().numpy()
     levels = [[st.level_n[i], st.level_m[i], st.level_cut[i], st.level_maxbw[i]] for i in range(st.levels)]
@@ -93,7 +92,7 @@ def test_host_abi_matches_oracle_digest_at_the_headline_size():
     n=2^24, k=64, fast, seed 0."""
     from kahip_b200 import native
     d = DIGESTS["rgg2d_2p24_k64_s0_fast"]
-    g, _, _ = _device_graph(d)
+    g, _ = _device_graph(d)
     rc, cut, part = native.kaffpa_ex(g["xadj"], g["adjncy"], d["k"], d["imbalance"], d["seed"], d["mode"])
     assert cut == d["cut"]
     assert hashlib.sha256(np.ascontiguousarray(part, np.int32).astype("<i4").tobytes()).hexdigest() == \
