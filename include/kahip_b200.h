@@ -269,6 +269,13 @@ int kb200_project(int n, const int* cmap, int nc, const int* part_coarse, int* p
 int kb200_initial_partition(int n, const int* xadj, const int* adjncy, const int* adjwgt,
                             const int* vwgt, const kb200_knobs* kn, int* part);
 
+/* The device initial partitioner (every bisection of a recursion depth in one
+ * launch; initial_partitioning.cpp:39-134 -> graph_partitioner.cpp:110-238 is
+ * the reference's counterpart) on a host graph: uploads it, partitions it
+ * into kn->k blocks and downloads part[n].  kn->ip_mode is ignored. */
+int kb200_initial_partition_device(int n, const int* xadj, const int* adjncy, const int* adjwgt,
+                                   const int* vwgt, const kb200_knobs* kn, int* part);
+
 /* Edge cut and block weights of a device-resident partition, computed
  * without allocating anything.  No counterpart in the reference (which has no
  * device code); it exists for callers that must not call cudaMalloc while

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "contract.cuh"
+#include "ip_device.cuh"
 #include "host/initial_partitioning.h"
 #include "jet.cuh"
 #include "knobs.h"
@@ -774,6 +775,22 @@ int kb200_project(int n, const int* cmap, int nc, const int* part_coarse, int* p
         project(ctx, n, dm, dc, df);
         if (n) KB_CUDA(cudaMemcpyAsync(part_fine, df, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
         KB_CUDA(cudaStreamSynchronize(s));
+        return KB_OK;
+    });
+}
+
+int kb200_initial_partition_device(int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                                   const kb200_knobs* kn, int* part) {
+    g_last_error.clear();
+    return guarded([&]() -> int {
+        int rc, dev;
+        if ((rc = validate(n, xadj, adjncy, adjwgt, vwgt)) || (rc = check_knobs(kn))) return rc;
+        if (n > 0 && !part) return fail(KB_ERR_INVALID_INPUT, "part is NULL");
+        if ((rc = current_device(&dev))) return rc;
+        PhaseRun pr(dev, n, xadj, adjncy, adjwgt, vwgt);
+        initial_partition_device(pr.ctx, pr.up.g, *kn, pr.up.part);
+        if (n) KB_CUDA(cudaMemcpyAsync(part, pr.up.part, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, pr.ctx.stream));
+        KB_CUDA(cudaStreamSynchronize(pr.ctx.stream));
         return KB_OK;
     });
 }

@@ -106,23 +106,9 @@ __device__ __forceinline__ void emit_range(int e0, int e1, int step, uint32_t ow
     if (used) flush_slots(used, st, sw, bucket + rowoff[own] + atomicAdd(&fill[own], (uint32_t)used));
 }
 
-__device__ __forceinline__ unsigned lanemask_le_c() {
-    unsigned m;
-    asm("mov.u32 %0, %%lanemask_le;" : "=r"(m));
-    return m;
-}
-
-// Packed emission: a warp takes 32 consecutive fine vertices; the rows of
-// those with at most 32 entries are laid back to back onto the lanes, as
-// many whole rows per step as fit.  Every lane maps its entry's target to
-// its coarse node, entries inside the row's own coarse node are dropped,
-// equal (coarse row, coarse target) pairs of the step -- also those from
-// different fine vertices of one coarse node -- are merged by match_any and
-// summed, and the merged entries go to their coarse row's bucket with one
-// reservation per coarse row and step.  Rows of 33 .. kEmitLaneDeg entries
-// are emitted by their own lane afterwards (register slots); longer rows are
-// left to emit_wide.  UNIT: every edge weight is 1 (adjwgt is not read on
-// the packed path).
+// Rows longer than kEmitLaneDeg are left to emit_wide.  UNIT: every edge
+// weight is 1 (adjwgt is not read).  The row entries of the next group of
+// four are loaded while the coarse ids of the current group are gathered.
 template <bool UNIT>
 __global__ void __launch_bounds__(kThreads) emit_kernel(int n, const int* __restrict__ xadj,
                                                         const int* __restrict__ adjncy,
@@ -130,65 +116,64 @@ __global__ void __launch_bounds__(kThreads) emit_kernel(int n, const int* __rest
                                                         const int* __restrict__ cmap,
                                                         const uint32_t* __restrict__ rowoff, uint32_t* fill,
                                                         uint64_t* bucket) {
-    __shared__ int smaps[kThreads / 32][32];
-    const int lane = threadIdx.x & 31;
-    int* smap = smaps[threadIdx.x >> 5];
-    const long long warps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w0 * 32 < n; w0 += warps) {
-        const long long vv = w0 * 32 + lane;
-        int beg = 0, deg = 0;
-        uint32_t own = 0;
-        if (vv < n) {
-            beg = xadj[vv];
-            deg = xadj[vv + 1] - beg;
-            own = (uint32_t)cmap[vv];
-        }
-        const int d = deg <= 32 ? deg : 0;
-        int incl = d;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
+        const int v = (int)(base + threadIdx.x);
+        if (v >= n) continue;
+        const int beg = xadj[v], end = xadj[v + 1];
+        if (end - beg > kEmitLaneDeg) continue;
+        const uint32_t own = (uint32_t)cmap[v];
+        uint32_t st[kEmitSlots], sw[kEmitSlots];
+        int used = 0;
+        int un[4];
+        uint32_t wn[4];
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += y;
-        }
-        const int excl = incl - d;
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
-        for (int base = 0, step = 0; base < total && step < 32; ++step) {
-            const bool inb = d > 0 && excl >= base && incl <= base + 32;
-            const unsigned bm = __ballot_sync(0xffffffffu, inb);
-            if (bm == 0) break;  // cannot happen: the next row starts at `base` and fits
-            const int used = __shfl_sync(0xffffffffu, incl, 31 - __clz(bm)) - base;
-            if (inb) smap[excl - base] = lane;
-            const unsigned starts = __reduce_or_sync(0xffffffffu, inb ? 1u << (excl - base) : 0u);
-            __syncwarp();
-            const bool act = lane < used;
-            const int s = 31 - __clz(starts & lanemask_le_c());
-            const int i = act ? smap[s] : lane;
-            const int mb = __shfl_sync(0xffffffffu, beg, i);
-            const uint32_t mown = __shfl_sync(0xffffffffu, own, i);
-            uint32_t t = kEmpty, w = 0;
-            if (act) {
-                const int e = mb + (lane - s);
-                t = (uint32_t)cmap[adjncy[e]];
-                w = UNIT ? 1u : (uint32_t)adjwgt[e];
+        for (int j = 0; j < 4; ++j) {
+            un[j] = -1;
+            wn[j] = 0;
+            if (beg + j < end) {
+                un[j] = adjncy[beg + j];
+                wn[j] = UNIT ? 1u : (uint32_t)adjwgt[beg + j];
             }
-            const bool keep = act && t != mown;
-            const unsigned long long key = keep ? (((unsigned long long)mown << 32) | t) : ~0ull;
-            const unsigned peers = __match_any_sync(0xffffffffu, key);
-            const uint32_t sum = UNIT ? (uint32_t)__popc(peers) : __reduce_add_sync(peers, w);
-            const bool leader = keep && (peers & lanemask_lt()) == 0;
-            // the leaders of one coarse row share one reservation
-            const unsigned lm = __ballot_sync(0xffffffffu, leader);
-            const unsigned rowpeers = __match_any_sync(0xffffffffu, leader ? mown : kEmpty);
-            const unsigned grp = rowpeers & lm;
-            const int first = leader ? __ffs(grp) - 1 : lane;
-            uint32_t resv = 0;
-            if (leader && lane == first) resv = atomicAdd(&fill[mown], (uint32_t)__popc(grp));
-            resv = __shfl_sync(0xffffffffu, resv, first);
-            if (leader) bucket[rowoff[mown] + resv + __popc(grp & lanemask_lt())] = ((uint64_t)t << 32) | sum;
-            base += used;
-            __syncwarp();
         }
-        if (deg > 32 && deg <= kEmitLaneDeg) emit_range(beg, beg + deg, 1, own, adjncy, adjwgt, cmap, rowoff, fill, bucket);
+        for (int e = beg; e < end; e += 4) {
+            int u[4];
+            uint32_t w[4], t[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                u[j] = un[j];
+                w[j] = wn[j];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) t[j] = u[j] >= 0 ? (uint32_t)cmap[u[j]] : kEmpty;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                un[j] = -1;
+                wn[j] = 0;
+                if (e + 4 + j < end) {
+                    un[j] = adjncy[e + 4 + j];
+                    wn[j] = UNIT ? 1u : (uint32_t)adjwgt[e + 4 + j];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (u[j] < 0 || t[j] == own) continue;
+                bool hit = false;
+#pragma unroll
+                for (int i = 0; i < kEmitSlots; ++i)
+                    if (i < used && st[i] == t[j]) { sw[i] += w[j]; hit = true; }
+                if (hit) continue;
+                if (used == kEmitSlots) {
+                    flush_slots(kEmitSlots, st, sw,
+                                bucket + rowoff[own] + atomicAdd(&fill[own], (uint32_t)kEmitSlots));
+                    used = 0;
+                }
+#pragma unroll
+                for (int i = 0; i < kEmitSlots; ++i)
+                    if (i == used) { st[i] = t[j]; sw[i] = w[j]; }
+                ++used;
+            }
+        }
+        if (used) flush_slots(used, st, sw, bucket + rowoff[own] + atomicAdd(&fill[own], (uint32_t)used));
     }
 }
 

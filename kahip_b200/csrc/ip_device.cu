@@ -9,10 +9,9 @@
 // its offset o, the first final block id it covers, so part[] holds final
 // block ids once the recursion ends.  A bisection runs `tries` tries and
 // keeps the best by (overload, cut), the first on ties.  A try:
-//   1. start node: s0 = the node of smallest (hash, id); the reached node
-//      farthest from s0 by breadth-first search, then the one farthest from
-//      that (bipartition.cpp:125-146 finds its start by repeated BFS too),
-//      ties to the smaller id;
+//   1. start node: the reached node farthest from s0 by breadth-first search
+//      (bipartition.cpp:125-146 searches twice), ties to the smaller id,
+//      where s0 is the node of smallest (hash, id);
 //   2. growing: nodes in (BFS distance from the start, id) order, unreached
 //      nodes last; side 0 takes the prefix until it reaches its target, and
 //      the node that crosses the target joins only if side 0 then stays
@@ -20,10 +19,12 @@
 //   3. 2-way Jet refinement in synchronous iterations: candidate moves with
 //      a negative-gain tolerance, the afterburner, a balance repair of an
 //      overloaded side by loss classes, the best (overload, cut) kept.
-// The thread block first builds its block's subgraph (members in id order,
-// edges inside the block) from the coarsest graph.  Every step is
-// deterministic: BFS distances, reductions over (key, id) and prefix sums in
-// id order do not depend on the order threads run in.
+// Per depth: one thread block per splitting block builds its subgraph
+// (members in id order, edges inside the block) from the coarsest graph;
+// one thread block per (block, try) runs the try; one per block keeps the
+// best try and writes the new block ids.  Every step is deterministic: BFS
+// distances, reductions over (key, id) and prefix sums in id order do not
+// depend on the order threads run in.
 #include "ip_device.cuh"
 
 #include <algorithm>
@@ -39,7 +40,7 @@ namespace kb {
 
 namespace {
 
-constexpr int kBT = 512;              // threads per bisecting block
+constexpr int kBT = 256;              // threads per thread block
 constexpr int kBW = kBT / 32;         // warps
 constexpr int kIpClasses = 256;       // balance repair classes (loss bucket x 8)
 constexpr int kDenseRows = 16;        // average degree from which a warp walks each row
@@ -62,11 +63,16 @@ struct IpArgs {
     unsigned* ebase;     // [reps][nsplit] start of its edge slots
     long long NS, ES;    // node / edge slots per repetition
     int* lid;            // [reps][n]
-    int *orig, *lbeg, *ldeg, *dist, *qa, *qb, *moved_at, *cls;  // [reps][NS]
+    int* nsub;           // [reps][nsplit] nodes of each split's subgraph
+    int *orig, *lbeg, *ldeg;  // [reps][NS] subgraphs
     int *ladj, *lw;      // [reps][ES]
-    uint8_t *side, *best, *dest, *keep, *won;  // [reps][NS]
-    long long* gain;     // [reps][NS]
-    unsigned long long* layer;  // [reps][NS]
+    // per (repetition, try): node slots of the try's working state
+    int *dist, *qa, *qb, *moved_at, *cls;  // [reps * tries][NS]
+    uint8_t *side, *best, *dest, *keep;    // [reps * tries][NS]
+    long long* gain;                       // [reps * tries][NS]
+    unsigned long long* layer;             // [reps * tries][NS]
+    unsigned long long* try_ov;            // [reps][nsplit][tries]
+    long long* try_cut;                    // [reps][nsplit][tries]
     int seed, depth, tries, jet_iters, jet_patience, jet_c, bal_iters;
     double eps;
     int* err;
@@ -333,12 +339,52 @@ __device__ void balance2(const Sub& S, uint8_t* side, int* cls, int s, const uns
     }
 }
 
-// 2-way Jet on side[] (best state kept in best[]); returns its cut.
+// Sums of four values over the block; every thread gets them.  `sh` holds
+// 4 * (kBW + 1) words.
+__device__ void block_sum4(unsigned long long v[4], unsigned long long* sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+        if (lane == 0) sh[q * (kBW + 1) + wid] = v[q];
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        unsigned long long t = 0;
+        for (int w = 0; w < kBW; ++w) t += sh[threadIdx.x * (kBW + 1) + w];
+        sh[threadIdx.x * (kBW + 1) + kBW] = t;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = sh[q * (kBW + 1) + kBW];
+    __syncthreads();
+}
+
+// cut and side weights of the current sides, in one reduction
 template <bool WARP>
-__device__ long long jet2(const Sub& S, const IpArgs& a, int r, uint8_t* side, uint8_t* best, uint8_t* dest,
+__device__ void cut_and_weights(const Sub& S, const uint8_t* side, long long* cut, unsigned long long w[2],
+                                unsigned long long* sh4) {
+    unsigned long long v[4] = {0, 0, 0, 0};
+    for_rows<WARP>(S.n_o, S.lbeg, S.ldeg,
+                   [&](int i, int e, Acc2& s) { if (side[S.ladj[e]] != side[i]) s.a += S.lw[e]; },
+                   [&](int i, const Acc2& s) {
+                       v[0] += (unsigned long long)s.a;
+                       v[side[i] ? 2 : 1] += S.c(i);
+                   });
+    block_sum4(v, sh4);
+    *cut = (long long)(v[0] / 2);
+    w[0] = v[1];
+    w[1] = v[2];
+}
+
+// 2-way Jet on side[] (the best state is kept in best[] and left in side[]);
+// returns its cut.
+template <bool WARP>
+__device__ long long jet2(const Sub& S, const IpArgs& a, uint8_t* side, uint8_t* best, uint8_t* dest,
                           uint8_t* keep, long long* gain, int* moved_at, int* cls, const unsigned long long mw[2],
                           int bis_level, int bis_round, unsigned long long* HS, unsigned long long* sh,
-                          int* sh_int) {
+                          unsigned long long* sh4, int* sh_int) {
     const int n_o = S.n_o;
     for (int i = threadIdx.x; i < n_o; i += kBT) {
         moved_at[i] = -2;
@@ -346,9 +392,9 @@ __device__ long long jet2(const Sub& S, const IpArgs& a, int r, uint8_t* side, u
     }
     __syncthreads();
     unsigned long long w[2];
-    side_weights(S, side, w, sh);
+    long long best_cut;
+    cut_and_weights<WARP>(S, side, &best_cut, w, sh4);
     unsigned long long best_ov = overload2(w, mw);
-    long long best_cut = cut_of<WARP>(S, side, sh);
     const long long c4 = a.jet_c;
     int since = 0;
     for (int it = 0; it < a.jet_iters; ++it) {
@@ -379,22 +425,28 @@ __device__ long long jet2(const Sub& S, const IpArgs& a, int r, uint8_t* side, u
                        },
                        [&](int i, const Acc2& s) { keep[i] = dest[i] && s.a >= 0; });
         __syncthreads();
-        unsigned long long mv = 0;
+        // moves; the side weights follow from the moved weight
+        unsigned long long v[4] = {0, 0, 0, 0};  // moves, weight 0 -> 1, weight 1 -> 0
         for (int i = threadIdx.x; i < n_o; i += kBT)
             if (keep[i]) {
+                v[0] += 1;
+                v[side[i] ? 2 : 1] += S.c(i);
                 side[i] ^= 1;
                 moved_at[i] = it;
-                ++mv;
             }
-        __syncthreads();
-        const unsigned long long moved = block_sum(mv, sh);
-        const uint64_t ks_cls = stream_key(a.seed, TAG_BCLS, bis_level, bis_round * 64 + it);
-        side_weights(S, side, w, sh);
-        for (int s2 = 0; s2 < 2; ++s2)
-            if (w[s2] > mw[s2]) balance2<WARP>(S, side, cls, s2, mw, ks_cls, a.bal_iters, HS, sh, sh_int);
-        side_weights(S, side, w, sh);
+        block_sum4(v, sh4);
+        const unsigned long long moved = v[0];
+        w[0] = w[0] - v[1] + v[2];
+        w[1] = w[1] - v[2] + v[1];
+        if (w[0] > mw[0] || w[1] > mw[1]) {
+            const uint64_t ks_cls = stream_key(a.seed, TAG_BCLS, bis_level, bis_round * 64 + it);
+            const unsigned long long w0[2] = {w[0], w[1]};
+            for (int s2 = 0; s2 < 2; ++s2)
+                if (w0[s2] > mw[s2]) balance2<WARP>(S, side, cls, s2, mw, ks_cls, a.bal_iters, HS, sh, sh_int);
+        }
+        long long cut;
+        cut_and_weights<WARP>(S, side, &cut, w, sh4);
         const unsigned long long ov = overload2(w, mw);
-        const long long cut = cut_of<WARP>(S, side, sh);
         if (ov < best_ov || (ov == best_ov && cut < best_cut)) {
             best_ov = ov;
             best_cut = cut;
@@ -447,14 +499,13 @@ __global__ void ip_bases(IpArgs a) {
     }
 }
 
-__global__ void __launch_bounds__(kBT) ip_bisect(IpArgs a) {
+// One thread block per (repetition, split): the split block's subgraph,
+// members in id order, rows restricted to the block, local ids.
+__global__ void __launch_bounds__(kBT) ip_extract(IpArgs a) {
     __shared__ unsigned long long sh[kBW + 1];
-    __shared__ unsigned long long HS[kIpClasses + 1];
-    __shared__ unsigned sh_cnt;
-    __shared__ int sh_int[4];
     const int j = blockIdx.x % a.nsplit, r = blockIdx.x / a.nsplit;
-    const int o = a.split_o[j], kk = a.split_k[j], kl = (kk + 1) / 2;
-    int* part = a.part + (long long)r * a.n;
+    const int o = a.split_o[j];
+    const int* part = a.part + (long long)r * a.n;
     int* lid = a.lid + (long long)r * a.n;
     const long long nb = (long long)r * a.NS + a.nbase[r * a.nsplit + j];
     const long long eb = (long long)r * a.ES + a.ebase[r * a.nsplit + j];
@@ -463,8 +514,6 @@ __global__ void __launch_bounds__(kBT) ip_bisect(IpArgs a) {
     int* ldeg = a.ldeg + nb;
     int* ladj = a.ladj + eb;
     int* lw = a.lw + eb;
-
-    // 1. members in id order -> local ids
     unsigned long long cnt = 0;
     for (int base = 0; base < a.n; base += kBT) {
         const int v = base + threadIdx.x;
@@ -478,9 +527,8 @@ __global__ void __launch_bounds__(kBT) ip_bisect(IpArgs a) {
         cnt += tot;
     }
     const int n_o = (int)cnt;
+    if (threadIdx.x == 0) a.nsub[r * a.nsplit + j] = n_o;
     __syncthreads();
-    if (n_o == 0) return;
-    // 2. rows restricted to the block: degrees, then entries (local ids)
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     for (int i = wid; i < n_o; i += kBW) {
         const int v = orig[i];
@@ -514,17 +562,32 @@ __global__ void __launch_bounds__(kBT) ip_bisect(IpArgs a) {
             w += __popc(m);
         }
     }
-    __syncthreads();
-    const Sub S{n_o, orig, lbeg, ldeg, ladj, lw, a.vwgt};
-    // targets and bounds
-    unsigned long long Wm = 0;
-    for (int i = threadIdx.x; i < n_o; i += kBT) Wm += S.c(i);
-    const unsigned long long W = block_sum(Wm, sh);
-    const unsigned long long t0 = W * (unsigned long long)kl / (unsigned long long)kk, t1 = W - t0;
-    const double eb2 = a.split_eb[j];
-    const unsigned long long mw[2] = {(unsigned long long)((1.0 + eb2) * (double)t0),
-                                      (unsigned long long)((1.0 + eb2) * (double)t1)};
-    const long long ns = (long long)r * a.NS + a.nbase[r * a.nsplit + j];
+}
+
+// One thread block per (repetition, split, try): start node, growing and
+// 2-way Jet; the try's sides stay in its side[] slots, its (overload, cut)
+// in try_ov / try_cut.
+__global__ void __launch_bounds__(kBT) ip_try(IpArgs a) {
+    __shared__ unsigned long long sh[kBW + 1];
+    __shared__ unsigned long long sh4[4 * (kBW + 1)];
+    __shared__ unsigned long long HS[kIpClasses + 1];
+    __shared__ unsigned sh_cnt;
+    __shared__ int sh_int[4];
+    const int t = blockIdx.x % a.tries;
+    const int j = (blockIdx.x / a.tries) % a.nsplit;
+    const int r = blockIdx.x / (a.tries * a.nsplit);
+    const int kk = a.split_k[j], kl = (kk + 1) / 2;
+    const int n_o = a.nsub[r * a.nsplit + j];
+    const long long nb = (long long)r * a.NS + a.nbase[r * a.nsplit + j];
+    const long long eb = (long long)r * a.ES + a.ebase[r * a.nsplit + j];
+    const Sub S{n_o, a.orig + nb, a.lbeg + nb, a.ldeg + nb, a.ladj + eb, a.lw + eb, a.vwgt};
+    const long long res = ((long long)r * a.nsplit + j) * a.tries + t;
+    if (n_o == 0) {
+        if (threadIdx.x == 0) { a.try_ov[res] = 0; a.try_cut[res] = 0; }
+        return;
+    }
+    // working state of this try
+    const long long ns = ((long long)r * a.tries + t) * a.NS + a.nbase[r * a.nsplit + j];
     int* dist = a.dist + ns;
     int* qa = a.qa + ns;
     int* qb = a.qb + ns;
@@ -536,83 +599,97 @@ __global__ void __launch_bounds__(kBT) ip_bisect(IpArgs a) {
     uint8_t* keep = a.keep + ns;
     long long* gain = a.gain + ns;
     unsigned long long* layer = a.layer + ns;
-    uint8_t* won = a.won + ns;  // the best try's sides
-    const bool warp_rows = erun >= (unsigned long long)kDenseRows * (unsigned long long)n_o;
-    const int bis_level = o, bis_round0 = r * 32 + a.depth;
-    long long best_cut = LLONG_MAX;
-    unsigned long long best_ov = ~0ull;
-    for (int t = 0; t < a.tries; ++t) {
-        const uint64_t ks = stream_key(a.seed, TAG_IP, bis_level, bis_round0 * 64 + t);
-        unsigned long long m0 = ~0ull;
-        for (int i = threadIdx.x; i < n_o; i += kBT)
-            m0 = min(m0, ((unsigned long long)hash32(ks, (uint32_t)i) << 32) | (unsigned)i);
-        const int s0 = (int)(block_min(m0, sh) & 0xffffffffu);
-        if (warp_rows) bfs<true>(n_o, s0, dist, qa, qb, lbeg, ldeg, ladj, &sh_cnt);
-        else bfs<false>(n_o, s0, dist, qa, qb, lbeg, ldeg, ladj, &sh_cnt);
-        const int s1 = farthest(n_o, dist, sh);
-        if (warp_rows) bfs<true>(n_o, s1, dist, qa, qb, lbeg, ldeg, ladj, &sh_cnt);
-        else bfs<false>(n_o, s1, dist, qa, qb, lbeg, ldeg, ladj, &sh_cnt);
-        const int st = farthest(n_o, dist, sh);
-        if (warp_rows) bfs<true>(n_o, st, dist, qa, qb, lbeg, ldeg, ladj, &sh_cnt);
-        else bfs<false>(n_o, st, dist, qa, qb, lbeg, ldeg, ladj, &sh_cnt);
-        // growing by (distance, id): layer weights, the crossing layer, and
-        // the crossing layer's id-order prefix
-        unsigned long long md = 0;
-        for (int i = threadIdx.x; i < n_o; i += kBT)
-            if (dist[i] != INT_MAX) md = max(md, (unsigned long long)dist[i]);
-        const int maxd = (int)block_max(md, sh);
-        const int nl = maxd + 2;
-        for (int l = threadIdx.x; l < nl; l += kBT) layer[l] = 0;
-        __syncthreads();
-        for (int i = threadIdx.x; i < n_o; i += kBT)
-            atomicAdd(&layer[dist[i] == INT_MAX ? maxd + 1 : dist[i]], (unsigned long long)S.c(i));
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            unsigned long long cum = 0;
-            int lc = 0;
-            while (lc < nl && cum + layer[lc] < t0) cum += layer[lc++];
-            sh_int[2] = lc;
-            HS[kIpClasses] = cum;
-        }
-        __syncthreads();
-        const int lc = sh_int[2];
-        unsigned long long run = HS[kIpClasses];
-        __syncthreads();
-        for (int base = 0; base < n_o; base += kBT) {
-            const int i = base + threadIdx.x;
-            int l = INT_MAX;
-            if (i < n_o) {
-                l = dist[i] == INT_MAX ? maxd + 1 : dist[i];
-                side[i] = l < lc ? 0 : 1;
-            }
-            const bool cross = i < n_o && l == lc;
-            unsigned long long tot;
-            const unsigned long long pre = block_scan(cross ? (unsigned long long)S.c(i) : 0ull, &tot, sh);
-            if (cross) {
-                const unsigned long long p = run + pre + S.c(i);
-                if (run + pre < t0 && p <= mw[0]) side[i] = 0;
-            }
-            run += tot;
-        }
-        __syncthreads();
-        const long long c = warp_rows
-                                ? jet2<true>(S, a, r, side, best, dest, keep, gain, moved_at, cls, mw, bis_level,
-                                             bis_round0 * 64 + t, HS, sh, sh_int)
-                                : jet2<false>(S, a, r, side, best, dest, keep, gain, moved_at, cls, mw, bis_level,
-                                              bis_round0 * 64 + t, HS, sh, sh_int);
-        unsigned long long w[2];
-        side_weights(S, side, w, sh);
-        const unsigned long long ov = overload2(w, mw);
-        if (ov < best_ov || (ov == best_ov && c < best_cut)) {
-            best_ov = ov;
-            best_cut = c;
-            for (int i = threadIdx.x; i < n_o; i += kBT) won[i] = side[i];
-        }
-        __syncthreads();
-    }
-    // 3. the winner's side 1 becomes block o + kl
+    // targets and bounds
+    unsigned long long Wm = 0;
+    for (int i = threadIdx.x; i < n_o; i += kBT) Wm += S.c(i);
+    const unsigned long long W = block_sum(Wm, sh);
+    const unsigned long long t0 = W * (unsigned long long)kl / (unsigned long long)kk, t1 = W - t0;
+    const double eb2 = a.split_eb[j];
+    const unsigned long long mw[2] = {(unsigned long long)((1.0 + eb2) * (double)t0),
+                                      (unsigned long long)((1.0 + eb2) * (double)t1)};
+    const bool warp_rows = (long long)a.lbeg[nb + n_o - 1] + a.ldeg[nb + n_o - 1] >= (long long)kDenseRows * n_o;
+    const int bis_level = a.split_o[j], bis_round = (r * 32 + a.depth) * 64 + t;
+    // 1. start: farthest from the node of smallest (hash, id)
+    const uint64_t ks = stream_key(a.seed, TAG_IP, bis_level, bis_round);
+    unsigned long long m0 = ~0ull;
     for (int i = threadIdx.x; i < n_o; i += kBT)
-        if (won[i]) part[orig[i]] = o + kl;
+        m0 = min(m0, ((unsigned long long)hash32(ks, (uint32_t)i) << 32) | (unsigned)i);
+    const int s0 = (int)(block_min(m0, sh) & 0xffffffffu);
+    if (warp_rows) bfs<true>(n_o, s0, dist, qa, qb, S.lbeg, S.ldeg, S.ladj, &sh_cnt);
+    else bfs<false>(n_o, s0, dist, qa, qb, S.lbeg, S.ldeg, S.ladj, &sh_cnt);
+    const int st = farthest(n_o, dist, sh);
+    if (warp_rows) bfs<true>(n_o, st, dist, qa, qb, S.lbeg, S.ldeg, S.ladj, &sh_cnt);
+    else bfs<false>(n_o, st, dist, qa, qb, S.lbeg, S.ldeg, S.ladj, &sh_cnt);
+    // 2. growing by (distance, id): layer weights, the crossing layer, and
+    // the crossing layer's id-order prefix
+    unsigned long long md = 0;
+    for (int i = threadIdx.x; i < n_o; i += kBT)
+        if (dist[i] != INT_MAX) md = max(md, (unsigned long long)dist[i]);
+    const int maxd = (int)block_max(md, sh);
+    const int nl = maxd + 2;
+    for (int l = threadIdx.x; l < nl; l += kBT) layer[l] = 0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n_o; i += kBT)
+        atomicAdd(&layer[dist[i] == INT_MAX ? maxd + 1 : dist[i]], (unsigned long long)S.c(i));
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long cum = 0;
+        int lc = 0;
+        while (lc < nl && cum + layer[lc] < t0) cum += layer[lc++];
+        sh_int[2] = lc;
+        HS[kIpClasses] = cum;
+    }
+    __syncthreads();
+    const int lc = sh_int[2];
+    unsigned long long run = HS[kIpClasses];
+    __syncthreads();
+    for (int base = 0; base < n_o; base += kBT) {
+        const int i = base + threadIdx.x;
+        int l = INT_MAX;
+        if (i < n_o) {
+            l = dist[i] == INT_MAX ? maxd + 1 : dist[i];
+            side[i] = l < lc ? 0 : 1;
+        }
+        const bool cross = i < n_o && l == lc;
+        unsigned long long tot;
+        const unsigned long long pre = block_scan(cross ? (unsigned long long)S.c(i) : 0ull, &tot, sh);
+        if (cross) {
+            const unsigned long long p = run + pre + S.c(i);
+            if (run + pre < t0 && p <= mw[0]) side[i] = 0;
+        }
+        run += tot;
+    }
+    __syncthreads();
+    // 3. 2-way Jet
+    const long long c = warp_rows ? jet2<true>(S, a, side, best, dest, keep, gain, moved_at, cls, mw, bis_level,
+                                               bis_round, HS, sh, sh4, sh_int)
+                                  : jet2<false>(S, a, side, best, dest, keep, gain, moved_at, cls, mw, bis_level,
+                                                bis_round, HS, sh, sh4, sh_int);
+    unsigned long long w[2];
+    side_weights(S, side, w, sh);
+    if (threadIdx.x == 0) {
+        a.try_ov[res] = overload2(w, mw);
+        a.try_cut[res] = c;
+    }
+}
+
+// One thread block per (repetition, split): the try of smallest (overload,
+// cut), the first on ties; its side 1 becomes block o + kl.
+__global__ void __launch_bounds__(kBT) ip_select(IpArgs a) {
+    const int j = blockIdx.x % a.nsplit, r = blockIdx.x / a.nsplit;
+    const int o = a.split_o[j], kl = (a.split_k[j] + 1) / 2;
+    const int n_o = a.nsub[r * a.nsplit + j];
+    const long long res = ((long long)r * a.nsplit + j) * a.tries;
+    int b = 0;
+    for (int t = 1; t < a.tries; ++t)
+        if (a.try_ov[res + t] < a.try_ov[res + b] ||
+            (a.try_ov[res + t] == a.try_ov[res + b] && a.try_cut[res + t] < a.try_cut[res + b]))
+            b = t;
+    const long long nb = (long long)r * a.NS + a.nbase[r * a.nsplit + j];
+    const uint8_t* side = a.side + ((long long)r * a.tries + b) * a.NS + a.nbase[r * a.nsplit + j];
+    int* part = a.part + (long long)r * a.n;
+    for (int i = threadIdx.x; i < n_o; i += kBT)
+        if (side[i]) part[a.orig[nb + i]] = o + kl;
 }
 
 }  // namespace
@@ -689,23 +766,26 @@ void initial_partition_device(Ctx& ctx, const DevGraph& c, const Knobs& kn, int*
     a.ebase = ctx.scratch.alloc<unsigned>((size_t)reps * maxs);
     a.lid = ctx.scratch.alloc<int>((size_t)reps * n);
     const size_t NSr = (size_t)reps * (size_t)a.NS, ESr = (size_t)reps * (size_t)a.ES;
+    const size_t NSt = NSr * (size_t)tries;
+    a.nsub = ctx.scratch.alloc<int>((size_t)reps * maxs);
     a.orig = ctx.scratch.alloc<int>(NSr);
     a.lbeg = ctx.scratch.alloc<int>(NSr);
     a.ldeg = ctx.scratch.alloc<int>(NSr);
-    a.dist = ctx.scratch.alloc<int>(NSr);
-    a.qa = ctx.scratch.alloc<int>(NSr);
-    a.qb = ctx.scratch.alloc<int>(NSr);
-    a.moved_at = ctx.scratch.alloc<int>(NSr);
-    a.cls = ctx.scratch.alloc<int>(NSr);
     a.ladj = ctx.scratch.alloc<int>(ESr);
     a.lw = ctx.scratch.alloc<int>(ESr);
-    a.side = ctx.scratch.alloc<uint8_t>(NSr);
-    a.best = ctx.scratch.alloc<uint8_t>(NSr);
-    a.dest = ctx.scratch.alloc<uint8_t>(NSr);
-    a.keep = ctx.scratch.alloc<uint8_t>(NSr);
-    a.won = ctx.scratch.alloc<uint8_t>(NSr);
-    a.gain = ctx.scratch.alloc<long long>(NSr);
-    a.layer = ctx.scratch.alloc<unsigned long long>(NSr);
+    a.dist = ctx.scratch.alloc<int>(NSt);
+    a.qa = ctx.scratch.alloc<int>(NSt);
+    a.qb = ctx.scratch.alloc<int>(NSt);
+    a.moved_at = ctx.scratch.alloc<int>(NSt);
+    a.cls = ctx.scratch.alloc<int>(NSt);
+    a.side = ctx.scratch.alloc<uint8_t>(NSt);
+    a.best = ctx.scratch.alloc<uint8_t>(NSt);
+    a.dest = ctx.scratch.alloc<uint8_t>(NSt);
+    a.keep = ctx.scratch.alloc<uint8_t>(NSt);
+    a.gain = ctx.scratch.alloc<long long>(NSt);
+    a.layer = ctx.scratch.alloc<unsigned long long>(NSt);
+    a.try_ov = ctx.scratch.alloc<unsigned long long>((size_t)reps * maxs * tries);
+    a.try_cut = ctx.scratch.alloc<long long>((size_t)reps * maxs * tries);
     a.seed = kn.seed;
     a.tries = tries;
     a.jet_iters = kn.jet_iters;
@@ -734,7 +814,11 @@ void initial_partition_device(Ctx& ctx, const DevGraph& c, const Knobs& kn, int*
             KB_LAUNCH();
             ip_bases<<<1, kBT, 0, st>>>(a);
             KB_LAUNCH();
-            ip_bisect<<<a.nsplit * reps, kBT, 0, st>>>(a);
+            ip_extract<<<a.nsplit * reps, kBT, 0, st>>>(a);
+            KB_LAUNCH();
+            ip_try<<<a.nsplit * reps * tries, kBT, 0, st>>>(a);
+            KB_LAUNCH();
+            ip_select<<<a.nsplit * reps, kBT, 0, st>>>(a);
             KB_LAUNCH();
         }
     }

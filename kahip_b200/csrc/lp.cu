@@ -371,159 +371,171 @@ __device__ void chunk_process(const SweepArgs& a, WarpTable& T, bool mem, int v,
     }
 }
 
-// ------------------------------------------------------------ packed sweep
+// ------------------------------------------------------ lane-per-vertex sweep
 //
 // The main sweep: a warp takes 32 * kSpan consecutive vertex ids, compacts the
-// members of the sub-round into a per-warp queue, and decides them 32 at a
-// time.  The rows of those 32 members are laid back to back onto the lanes,
-// one row entry per lane, as many whole rows per step as fit into 32 lanes:
-// every lane loads its entry's target and label (coalesced within a row),
-// equal (member, label) pairs are merged with match_any and summed with a
-// warp reduction, and each member's connection to its own label and its best
-// candidate come from reductions over the member's lanes.  Rows longer than
-// 32 entries are queued per warp and decided in the same kernel by
-// chunk_process; rows longer than kWin go to the high-degree list
-// (heavy_kernel).
+// members of the sub-round onto its lanes, and every lane aggregates its own
+// vertex's neighbourhood in kSlots register slots (connection per label; the
+// own label is kept apart), four edges at a time with all loads issued
+// before use.  A vertex whose neighbours carry more distinct labels than
+// slots is queued per warp and decided by chunk_process in the same kernel;
+// one of degree > kWin goes to the high-degree list (heavy_kernel).
 
-constexpr int kSpan = 2;  // chunks of 32 ids per warp task
+constexpr int kSlots = 6;  // 4: ~5 % of RGG rows overflow; 6: 0.6 %, fastest measured
+constexpr int kSpan = 2;  // chunks of 32 ids per warp task (2 measured 3 % faster than 4)
 
-__device__ __forceinline__ unsigned lanemask_le() {
-    unsigned m;
-    asm("mov.u32 %0, %%lanemask_le;" : "=r"(m));
-    return m;
+// r-th set bit (0-based) of mask
+__device__ __forceinline__ int nth_set_bit(unsigned mask, int r) {
+    int lo = 0, hi = 31;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        const unsigned below = mid == 31 ? mask : (mask & ((2u << mid) - 1u));
+        if (__popc(below) > r) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
 }
 
-// Decides the warp's 32 queued members (lane i: member v, or v < 0 for none).
-// Returns per lane: 0 decided (stays), 3 decided (proposes a move), 1 row
-// longer than 32 (chunk_process), 2 row longer than kWin (heavy_kernel).
-// WIDE: labels may reach 2^27 - 1, so (label, member) keys need 64 bits.
-template <int MODE, bool UNIT, bool WIDE>
-__device__ int packed_members(const SweepArgs& a, int v, int* smap, unsigned long long& wv,
-                              unsigned long long& we) {
-    const int lane = threadIdx.x & 31;
-    const bool single = MODE == CLUSTER && a.singletons;
-    int beg = 0, deg = 0;
-    uint32_t own = 0, cv = 0;
-    if (v >= 0) {
-        beg = a.xadj[v];
-        deg = a.xadj[v + 1] - beg;
-        own = (uint32_t)a.lab[v];
-        cv = (uint32_t)a.vwgt[v];
-    }
-    const int d = deg > 32 ? 0 : deg;  // entries this member puts on the lanes
-    int incl = d;
+// 0: decided (stays), 3: decided (proposes a move), 1: too many distinct
+// labels for NS slots, 2: degree above kWin
+template <int MODE, int NS, bool UNIT>
+__device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, unsigned long long& we) {
+    const int beg = a.xadj[v], end = a.xadj[v + 1];
+    if (end - beg > kWin) return 2;
+    const uint32_t own = (uint32_t)a.lab[v];
+    const uint32_t cv = (uint32_t)a.vwgt[v];
+    uint32_t cown = 0;
+    if (MODE == CLUSTER && a.singletons) {
+        // label[u] == u and no target repeats: the connection to cluster u is
+        // exactly w(v,u), so the best candidate is a running maximum; the
+        // tie hashes come precomputed per vertex, and the size test is
+        // skipped when every pair of node weights fits under the bound
+        uint64_t key = 0;
+        uint32_t id = kEmpty;
+        for (int e = beg; e < end; e += 4) {
+            int u[4];
+            uint32_t w[4];
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-    }
-    const int excl = incl - d;
-    const int total = __shfl_sync(0xffffffffu, incl, 31);
-    uint32_t rc = 0, rb = 0, rid = kEmpty;  // per member: own connection, best connection, best label
-    // every step consumes at least one member (so at most 32 steps)
-    for (int base = 0, step = 0; base < total && step < 32; ++step) {
-        // members whose whole row fits into lanes [0, 32) from `base` on; the
-        // first remaining member with entries starts exactly at `base`
-        const bool inb = d > 0 && excl >= base && incl <= base + 32;
-        const unsigned bm = __ballot_sync(0xffffffffu, inb);
-        if (bm == 0) {  // cannot happen; guards the loop bound
-            if (lane == 0) atomicOr(a.err, 2);
-            break;
-        }
-        const int used = __shfl_sync(0xffffffffu, incl, 31 - __clz(bm)) - base;
-        if (inb) smap[excl - base] = lane;
-        const unsigned starts = __reduce_or_sync(0xffffffffu, inb ? 1u << (excl - base) : 0u);
-        __syncwarp();
-        const bool act = lane < used;
-        const int s = 31 - __clz(starts & lanemask_le());  // start lane of this lane's row (lane 0 is one)
-        const int i = act ? smap[s] : lane;                 // the member lane owning it
-        const int mb = __shfl_sync(0xffffffffu, beg, i);
-        const int md = __shfl_sync(0xffffffffu, d, i);
-        const uint32_t mown = __shfl_sync(0xffffffffu, own, i);
-        const uint32_t mcv = __shfl_sync(0xffffffffu, cv, i);
-        uint32_t l = kEmpty, w = 0;
-        if (act) {
-            const int e = mb + (lane - s);
-            const int t = a.adjncy[e];
-            w = UNIT ? 1u : (uint32_t)a.adjwgt[e];
-            l = single ? (uint32_t)t : (uint32_t)a.lab[t];  // round 0: label[u] == u
-        }
-        // reduction mask: the lanes of this lane's row, or all unused lanes
-        const unsigned usedmask = used >= 32 ? 0xffffffffu : ((1u << used) - 1u);
-        const unsigned rmask = act ? ((md == 32 ? 0xffffffffu : ((1u << md) - 1u)) << s) : ~usedmask;
-        // merge equal (member, label) pairs (round 0 has none: rows have
-        // strictly increasing targets)
-        unsigned peers;
-        uint32_t sum;
-        if (single) {
-            peers = 1u << lane;
-            sum = w;
-        } else {
-            if (WIDE) {
-                const unsigned long long key = act ? (((unsigned long long)l << 5) | (unsigned)s) : ~0ull;
-                peers = __match_any_sync(0xffffffffu, key);
-            } else {
-                const uint32_t key = act ? ((l << 5) | (uint32_t)s) : 0xffffffffu;
-                peers = __match_any_sync(0xffffffffu, key);
+            for (int t = 0; t < 4; ++t) {
+                u[t] = -1;
+                w[t] = 0;
+                if (e + t < end) {
+                    u[t] = a.adjncy[e + t];
+                    w[t] = UNIT ? 1u : (uint32_t)a.adjwgt[e + t];
+                }
             }
-            sum = UNIT ? (uint32_t)__popc(peers) : __reduce_add_sync(peers, w);
+            uint32_t h[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) h[t] = u[t] >= 0 ? a.tie[u[t]] : 0u;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                if (u[t] < 0) continue;
+                const uint32_t l = (uint32_t)u[t];
+                if (l == own) { cown += w[t]; continue; }
+                if (a.all_fit ? w[t] > 0 : cand_ok<MODE>(a, l, w[t], cv))
+                    better(key, id, ((uint64_t)w[t] << 32) | (uint32_t)~h[t], l);
+            }
         }
-        const bool leader = act && (peers & lanemask_lt()) == 0;
-        const bool isown = l == mown;
-        const bool cand = leader && !isown &&
-                          ((single && a.all_fit) ? sum > 0 : cand_ok<MODE>(a, l, sum, mcv));
-        // per member: connection to its own label, best candidate connection,
-        // then ties by the smaller tie hash (computed only where a member has
-        // several equally connected candidates), then the smaller label
-        const uint32_t cown = __reduce_add_sync(rmask, (leader && isown) ? sum : 0u);
-        const uint32_t maxc = __reduce_max_sync(rmask, cand ? sum : 0u);
-        // (every lane executes each warp intrinsic: none sits behind a
-        // short-circuiting condition)
-        bool tie = cand && sum == maxc;
-        const unsigned tb = __ballot_sync(0xffffffffu, tie);
-        const bool multi = tie && __popc(tb & rmask) > 1;
-        if (__any_sync(0xffffffffu, multi)) {
-            const uint32_t h = multi ? (single ? a.tie[l] : hash32(a.ks_tie, l)) : 0xffffffffu;
-            const uint32_t mh = __reduce_min_sync(rmask, h);
-            tie = tie && h == mh;
-        }
-        const uint32_t id = __reduce_min_sync(rmask, tie ? l : kEmpty);
-        // each member reads its results from its row's first lane
-        const int src = inb ? excl - base : lane;
-        const uint32_t xc = __shfl_sync(0xffffffffu, cown, src);
-        const uint32_t xm = __shfl_sync(0xffffffffu, maxc, src);
-        const uint32_t xi = __shfl_sync(0xffffffffu, id, src);
-        if (inb) {
-            rc = xc;
-            rb = xm;
-            rid = xi;
-        }
-        base += used;
-        __syncwarp();
+        wv += 1;
+        we += (unsigned long long)(end - beg);
+        return decide_emit<MODE>(a, v, own, cv, cown, key, id) ? 3 : 0;
     }
-    if (v < 0) return 0;
-    if (deg > 32) return deg > kWin ? 2 : 1;
+    // NS register slots (label, connection); a new label enters at slot 0 and
+    // shifts the others up, so slot NS-1 filled means the slots are full
+    uint32_t sl[NS], sc[NS];
+#pragma unroll
+    for (int i = 0; i < NS; ++i) { sl[i] = kEmpty; sc[i] = 0; }
+    bool overflow = false;
+    // software pipeline: the row entries of the next group of four are
+    // loaded while the labels of the current group are gathered
+    int un[4];
+    uint32_t wn[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        un[t] = -1;
+        wn[t] = 0;
+        if (beg + t < end) {
+            un[t] = a.adjncy[beg + t];
+            wn[t] = UNIT ? 1u : (uint32_t)a.adjwgt[beg + t];
+        }
+    }
+    for (int e = beg; e < end && !overflow; e += 4) {
+        int u[4];
+        uint32_t w[4], l[4];
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            u[t] = un[t];
+            w[t] = wn[t];
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) l[t] = u[t] >= 0 ? (uint32_t)a.lab[u[t]] : kEmpty;
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            un[t] = -1;
+            wn[t] = 0;
+            if (e + 4 + t < end) {
+                un[t] = a.adjncy[e + 4 + t];
+                wn[t] = UNIT ? 1u : (uint32_t)a.adjwgt[e + 4 + t];
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            if (u[t] < 0) continue;
+            const uint32_t lt = l[t], wt = w[t];
+            if (lt == own) { cown += wt; continue; }
+            bool hit = false;
+#pragma unroll
+            for (int i = 0; i < NS; ++i) {
+                const bool m = sl[i] == lt;
+                sc[i] += m ? wt : 0u;
+                hit |= m;
+            }
+            if (!hit) {
+                overflow |= sl[NS - 1] != kEmpty;
+#pragma unroll
+                for (int i = NS - 1; i > 0; --i) { sl[i] = sl[i - 1]; sc[i] = sc[i - 1]; }
+                sl[0] = lt;
+                sc[0] = wt;
+            }
+        }
+    }
+    if (overflow) return 1;
     wv += 1;
-    we += (unsigned long long)deg;
+    we += (unsigned long long)(end - beg);
+    // best candidate: largest connection, ties by smaller tie hash, then
+    // smaller label; hashes are computed only for ties
+    uint32_t ok[NS];
+#pragma unroll
+    for (int i = 0; i < NS; ++i) ok[i] = sl[i] != kEmpty && cand_ok<MODE>(a, sl[i], sc[i], cv);
+    uint32_t bc = 0, id = kEmpty;
+#pragma unroll
+    for (int i = 0; i < NS; ++i) {
+        if (!ok[i]) continue;
+        if (id == kEmpty || sc[i] > bc) {
+            bc = sc[i];
+            id = sl[i];
+        } else if (sc[i] == bc) {
+            const uint32_t hi = hash32(a.ks_tie, sl[i]), hb = hash32(a.ks_tie, id);
+            if (hi < hb || (hi == hb && sl[i] < id)) id = sl[i];
+        }
+    }
     // decide_emit reads the connection (upper half) of the key only
-    const uint64_t key = rid == kEmpty ? 0ull : ((uint64_t)rb << 32);
-    return decide_emit<MODE>(a, v, own, cv, rc, key, rid) ? 3 : 0;
+    const uint64_t key = id == kEmpty ? 0ull : ((uint64_t)bc << 32);
+    return decide_emit<MODE>(a, v, own, cv, cown, key, id) ? 3 : 0;
 }
 
 
-template <int MODE, bool UNIT, bool WIDE>
-__global__ void __launch_bounds__(kThreads, 4) sweep_kernel(SweepArgs a) {
+template <int MODE, bool UNIT>
+__global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
     static_assert(kTab == 256, "slot64 assumes 256 slots");
     // per-warp queue of members still to be processed, so that every pass
     // over the lanes is full, and of vertices that overflowed the slots
     __shared__ int queue[kWarpsPerBlock][32 * kSpan + 32];
     __shared__ int oqueue[kWarpsPerBlock][64];
-    __shared__ int smaps[kWarpsPerBlock][32];
     __shared__ WarpTable tabs[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
     int* q = queue[threadIdx.x >> 5];
     int* oq = oqueue[threadIdx.x >> 5];
-    int* smap = smaps[threadIdx.x >> 5];
     WarpTable& T = tabs[threadIdx.x >> 5];
     for (int i = lane; i < kTab; i += 32) { T.key[i] = kEmpty64; T.val[i] = 0; }
     if (lane == 0) T.nused = 0;
@@ -544,7 +556,8 @@ __global__ void __launch_bounds__(kThreads, 4) sweep_kernel(SweepArgs a) {
         chunk_process<MODE>(a, T, mem, v, wv, we, wo);
     };
     auto pass = [&](int v) {
-        const int status = packed_members<MODE, UNIT, WIDE>(a, v, smap, wv, we);
+        int status = 0;
+        if (v >= 0) status = lane_vertex<MODE, kSlots, UNIT>(a, v, wv, we);
         const unsigned om = __ballot_sync(0xffffffffu, status == 1);
         if (status == 1) oq[oqn + __popc(om & lanemask_lt())] = v;
         oqn += __popc(om);
@@ -902,15 +915,8 @@ void launch_sweep(Ctx& ctx, const DevGraph& g, SweepArgs a, const SweepBuffers& 
     KB_CUDA(cudaMemsetAsync(b.counters, 0, sizeof(unsigned) * kCntMoved, ctx.stream));
     {
         PhaseScope ps(ctx, family(MODE, 0), bytes);
-        // (label << 5 | member lane) keys fit 32 bits while labels < 2^27 - 1
-        const bool wide = g.n >= (1 << 27) - 1;
-        if (g.unit_weights) {
-            if (wide) sweep_kernel<MODE, true, true><<<b.lblocks, kThreads, 0, ctx.stream>>>(a);
-            else sweep_kernel<MODE, true, false><<<b.lblocks, kThreads, 0, ctx.stream>>>(a);
-        } else {
-            if (wide) sweep_kernel<MODE, false, true><<<b.lblocks, kThreads, 0, ctx.stream>>>(a);
-            else sweep_kernel<MODE, false, false><<<b.lblocks, kThreads, 0, ctx.stream>>>(a);
-        }
+        if (g.unit_weights) lane_kernel<MODE, true><<<b.lblocks, kThreads, 0, ctx.stream>>>(a);
+        else lane_kernel<MODE, false><<<b.lblocks, kThreads, 0, ctx.stream>>>(a);
         KB_LAUNCH();
     }
     if (b.gcap > 0) {

@@ -104,6 +104,7 @@ EXPORTS = [
     "kb200_read_metis", "kb200_read_bgf", "kb200_write_partition", "kb200_free", "kb200_io_error",
     "kb200_lp_cluster", "kb200_contract", "kb200_jet_refine",
     "kb200_lp_refine", "kb200_balance", "kb200_edge_cut", "kb200_project", "kb200_initial_partition",
+    "kb200_initial_partition_device",
     "kb200_last_error", "kb200_kernel_launches", "kb200_device_count", "kb200_edge_cut_noalloc",
     # reference-compatible ABI (include/kaHIP_interface.h)
     "kaffpa", "kaffpa_balance", "kaffpa_balance_NE", "process_mapping", "node_separator", "reduced_nd",
@@ -153,6 +154,7 @@ def lib():
         L.kb200_edge_cut.argtypes = [i, vp, vp, vp, vp, vp, i, c_ll_p, vp]
         L.kb200_project.argtypes = [i, vp, i, vp, vp]
         L.kb200_initial_partition.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), vp]
+        L.kb200_initial_partition_device.argtypes = [i, vp, vp, vp, vp, ctypes.POINTER(Knobs), vp]
         L.kb200_last_error.restype = ctypes.c_char_p
         L.kb200_last_error.argtypes = []
         L.kb200_device_count.argtypes = []
@@ -161,6 +163,9 @@ def lib():
         L.kaffpa.argtypes = [c_int_p, vp, vp, vp, vp, c_int_p, ctypes.POINTER(d), ctypes.c_bool, i, i,
                              c_int_p, vp]
         L.kaffpa.restype = None
+        L.kaffpa_balance.argtypes = [c_int_p, vp, vp, vp, vp, c_int_p, ctypes.POINTER(d), ctypes.c_bool,
+                                     ctypes.c_bool, i, i, c_int_p, vp]
+        L.kaffpa_balance.restype = None
         _LIB = L
     return _LIB
 
@@ -333,6 +338,15 @@ def initial_partition(g: dict, kn: Knobs) -> np.ndarray:
     p = np.empty(g["n"], np.int32)
     _check(lib().kb200_initial_partition(g["n"], _ptr(g["xadj"]), _ptr(g["adjncy"]), _ptr(g["adjwgt"]),
                                          _ptr(g["vwgt"]), ctypes.byref(kn), _ptr(p)))
+    return p
+
+
+def initial_partition_device(g: dict, kn: Knobs) -> np.ndarray:
+    """The device initial partitioner (every bisection of a recursion depth
+    in one launch) on a host graph."""
+    p = np.empty(g["n"], np.int32)
+    _check(lib().kb200_initial_partition_device(g["n"], _ptr(g["xadj"]), _ptr(g["adjncy"]), _ptr(g["adjwgt"]),
+                                                _ptr(g["vwgt"]), ctypes.byref(kn), _ptr(p)))
     return p
 
 

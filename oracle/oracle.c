@@ -1338,10 +1338,9 @@ void or_initial_partition(const or_graph* g, const or_knobs* knobs, int* part) {
  * gets ceil(k/2) blocks, targets in proportion, per-side slack eb.  A
  * bisection runs `ip_tries` tries and keeps the best by (overload, cut),
  * the first on ties; a try:
- *   1. start: s0 = the node of smallest (hash, id); two breadth-first
- *      searches (bipartition.cpp:125-146) give the reached node farthest
- *      from s0, then the reached node farthest from that one (ties: smaller
- *      id), the start;
+ *   1. start: the reached node farthest from s0 by breadth-first search
+ *      (bipartition.cpp:125-146 searches twice), ties to the smaller id,
+ *      where s0 is the node of smallest (hash, id);
  *   2. growing (bipartition.cpp:147-222 grows by gain; here by distance):
  *      nodes in (BFS distance from the start, id) order, unreached nodes
  *      last by id; side 0 takes the order's prefix until it reaches t0 --
@@ -1552,8 +1551,6 @@ static void batched_bisect(const or_graph* g, uint64_t t0, const uint64_t maxw[2
             if (h < hbest) { hbest = h; s0 = v; }
         }
         bfs_dist(g, s0, dist, queue);
-        const int s1 = farthest_node(g, dist);
-        bfs_dist(g, s1, dist, queue);
         const int start = farthest_node(g, dist);
         bfs_dist(g, start, dist, queue);
         grow_bfs(g, dist, t0, maxw[0], side);

@@ -222,6 +222,13 @@ def initial_partition(g: dict, kn: Knobs) -> np.ndarray:
     return p
 
 
+def initial_partition_batched(g: dict, kn: Knobs) -> np.ndarray:
+    """The batched recursive bisection (the device's initial partitioner)."""
+    p = np.empty(g["n"], np.int32)
+    lib().or_initial_partition_batched(G(g).ref, ctypes.byref(kn), _p(p))
+    return p
+
+
 def kaffpa(g: dict, k: int, imbalance=0.03, seed=0, mode=0, unit_weights=False):
     """Returns (edgecut, part, stats)."""
     part = np.empty(g["n"], np.int32)

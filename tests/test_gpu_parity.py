@@ -177,7 +177,6 @@ def test_drop_in_kaffpa_balance_keeps_epsilon(N, O, graphs, perfectly_balance):
     imb = ctypes.c_double(0.03)
     cut = ctypes.c_int(-7)
     part = np.zeros(g["n"], np.int32)
-    L.kaffpa_balance.restype = None
     L.kaffpa_balance(ctypes.byref(n), vwgt.ctypes.data, g["xadj"].ctypes.data, None, g["adjncy"].ctypes.data,
                      ctypes.byref(k), ctypes.byref(imb), ctypes.c_bool(perfectly_balance), True, 0, 0,
                      ctypes.byref(cut), part.ctypes.data)
@@ -188,6 +187,51 @@ def test_drop_in_kaffpa_balance_keeps_epsilon(N, O, graphs, perfectly_balance):
     W = int(vwgt.sum())
     bound = int((1 + 0.03) * -(-W // 8))
     assert O.block_weights(gw, part, 8).max() <= bound
+
+
+@pytest.mark.parametrize("gen,k,mode,seed", [("rgg2d", 8, 0, 0), ("rgg2d", 64, 0, 0), ("rgg2d", 64, 1, 5),
+                                             ("rgg3d", 13, 1, 2), ("rmat", 16, 0, 1), ("grid", 2, 0, 1),
+                                             ("rgg2d", 256, 0, 3), ("grid", 7, 1, 4)])
+def test_device_initial_partitioner_matches_oracle(N, O, graphs, gen, k, mode, seed):
+    """The device's batched recursive bisection on a coarsest-like graph (one
+    level of oracle LP clustering) against its oracle restatement."""
+    g = {"rgg2d": lambda: graphs.rgg2d(1 << 15, seed=seed), "rgg3d": lambda: graphs.rgg3d(1 << 14, seed=seed),
+         "rmat": lambda: graphs.rmat(13, seed=seed), "grid": lambda: graphs.grid2d(120, 100)}[gen]()
+    kn = O.knobs(g, k, 0.03, seed, mode)
+    c, _ = O.contract(g, O.lp_cluster(g, kn, 0))
+    a = O.initial_partition_batched(c, kn)
+    b = N.initial_partition_device(c, N.derive_knobs(g["n"], g["vwgt"], k, 0.03, seed, mode))
+    assert np.array_equal(a, b)
+    assert a.min() >= 0 and a.max() < k
+
+
+@pytest.mark.parametrize("k,mode", [(8, 0), (16, 1)])
+def test_device_initial_partitioner_dense_graph(N, O, k, mode):
+    # average degree > 64: one try per bisection, rows walked by whole warps
+    rng = np.random.default_rng(k)
+    n = 400
+    edges = set()
+    while len(edges) < 14000:
+        u, v = rng.integers(0, n, 2)
+        if u != v:
+            edges.add((min(u, v), max(u, v)))
+    g = csr_from_edges(n, sorted(edges), weights=list(rng.integers(1, 9, len(edges))))
+    g["vwgt"] = rng.integers(1, 5, n).astype(np.int32)
+    kn = O.knobs(g, k, 0.03, 1, mode)
+    a = O.initial_partition_batched(g, kn)
+    b = N.initial_partition_device(g, N.derive_knobs(g["n"], g["vwgt"], k, 0.03, 1, mode))
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("gname", ["single", "isolated", "path", "star", "two_components"])
+@pytest.mark.parametrize("k", [2, 3, 8, 100])
+def test_device_initial_partitioner_edge_cases(N, O, gname, k):
+    n, edges = EDGE_GRAPHS[gname]
+    g = csr_from_edges(n, edges)
+    kn = O.knobs(g, k, 0.03, 0, 0)
+    a = O.initial_partition_batched(g, kn)
+    b = N.initial_partition_device(g, N.derive_knobs(g["n"], g["vwgt"], k, 0.03, 0, 0))
+    assert np.array_equal(a, b)
 
 
 EDGE_GRAPHS = {
