@@ -220,26 +220,34 @@ __global__ void head_flags(long long E, const uint64_t* __restrict__ K, uint32_t
 // sorted and merged on its own
 
 constexpr int kSegMax = 1024;       // rows up to this many entries merge in shared memory
-constexpr int kMergeWarps = 4;
+constexpr int kSegSmall = 64;       // rows up to this many entries sort in registers
+constexpr int kMergeWarps = 4;      // warps per block of the shared-memory merge
+constexpr int kMergeWarpsSmall = 8; // warps per block of the register merge
 
-// Warp per coarse row: sorts the row's bucket (bitonic, in shared memory),
-// sums the weights of equal targets and writes the distinct entries back to
-// the start of the bucket; ucnt[row] = their number.  Longer rows are left
-// for the global path (bigsz[row] = their size).
-__global__ void __launch_bounds__(kMergeWarps * 32) merge_rows(int nc, const uint32_t* __restrict__ rowoff,
-                                                                const uint32_t* __restrict__ fill, uint64_t* bucket,
-                                                                uint32_t* ucnt, uint32_t* bigsz) {
-    __shared__ uint64_t buf[kMergeWarps][kSegMax];
+// Warp per coarse row: sorts the row's bucket (bitonic), sums the weights of
+// equal targets and writes the distinct entries back to the start of the
+// bucket; ucnt[row] = their number.  LARGE = false takes the rows of at
+// most kSegSmall entries (sorted in registers, a 512-byte staging buffer
+// per warp, so many warps fit on an SM); LARGE = true the rows of up to
+// kSegMax entries (sorted in an 8 KiB shared buffer per warp) and marks the
+// longer ones for the global path (bigsz[row] = their size).
+template <bool LARGE>
+__global__ void __launch_bounds__((LARGE ? kMergeWarps : kMergeWarpsSmall) * 32)
+    merge_rows(int nc, const uint32_t* __restrict__ rowoff, const uint32_t* __restrict__ fill, uint64_t* bucket,
+               uint32_t* ucnt, uint32_t* bigsz) {
+    constexpr int W = LARGE ? kMergeWarps : kMergeWarpsSmall;
+    constexpr int CAP = LARGE ? kSegMax : kSegSmall;
+    __shared__ uint64_t buf[W][CAP];
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     uint64_t* b = buf[wp];
-    for (long long r = (long long)blockIdx.x * kMergeWarps + wp; r < nc; r += (long long)gridDim.x * kMergeWarps) {
+    for (long long r = (long long)blockIdx.x * W + wp; r < nc; r += (long long)gridDim.x * W) {
         const long long beg = rowoff[r];
         const int s = (int)fill[r];
-        if (s > kSegMax) {
+        if (LARGE && s > kSegMax) {
             if (lane == 0) { bigsz[r] = (uint32_t)s; ucnt[r] = 0; }
             continue;
         }
-        if (lane == 0) bigsz[r] = 0;
+        if ((s <= kSegSmall) == LARGE) continue;  // the other kernel's row
         int P = 1;
         while (P < s) P <<= 1;
         if (P <= 32) {
@@ -275,7 +283,7 @@ __global__ void __launch_bounds__(kMergeWarps * 32) merge_rows(int nc, const uin
             b[lane] = x0;
             b[lane + 32] = x1;
             __syncwarp();
-        } else {
+        } else if (LARGE) {
             for (int i = lane; i < P; i += 32) b[i] = i < s ? bucket[beg + i] : ~0ull;
             __syncwarp();
             for (int k = 2; k <= P; k <<= 1)
@@ -476,12 +484,17 @@ void contract(Ctx& ctx, const DevGraph& g, const int* label, int* cmap, DevGraph
     // 4. merge each row: shared-memory sort for rows up to kSegMax entries
     {
         PhaseScope ps(ctx, "contract_merge", 16.0 * m);
-        const int gb = (int)std::max<long long>(1, std::min<long long>(div_up(nc, kMergeWarps), (long long)kNumSMs * 16));
         // ucnt / bigsz have nc + 1 entries (the scans read the last one)
         KB_CUDA(cudaMemsetAsync(ucnt, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
         KB_CUDA(cudaMemsetAsync(bigsz, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
-        merge_rows<<<gb, kMergeWarps * 32, 0, st>>>(nc, rowoff, fill, bucket, ucnt, bigsz);
+        const int gs = (int)std::max<long long>(1, std::min<long long>(div_up(nc, kMergeWarpsSmall), (long long)kNumSMs * 16));
+        merge_rows<false><<<gs, kMergeWarpsSmall * 32, 0, st>>>(nc, rowoff, fill, bucket, ucnt, bigsz);
         KB_LAUNCH();
+        if (g.maxdeg > 0) {
+            const int gb = (int)std::max<long long>(1, std::min<long long>(div_up(nc, kMergeWarps), (long long)kNumSMs * 7));
+            merge_rows<true><<<gb, kMergeWarps * 32, 0, st>>>(nc, rowoff, fill, bucket, ucnt, bigsz);
+            KB_LAUNCH();
+        }
         exclusive_scan_u32(bigsz, bigoff, (long long)nc + 1, big, st, ctx.scratch);
     }
     // row lengths -> coarse xadj and the coarse degree statistics, read back

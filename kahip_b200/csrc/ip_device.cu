@@ -44,6 +44,8 @@ constexpr int kBT = 256;              // threads per thread block
 constexpr int kBW = kBT / 32;         // warps
 constexpr int kIpClasses = 256;       // balance repair classes (loss bucket x 8)
 constexpr int kDenseRows = 16;        // average degree from which a warp walks each row
+constexpr int kIpSmemPerNode = 56;    // shared-memory bytes per node of a try's working state
+constexpr int kIpSmem = 200 * 1024;   // dynamic shared memory of the try kernel
 
 struct IpArgs {
     int n;
@@ -64,7 +66,7 @@ struct IpArgs {
     long long NS, ES;    // node / edge slots per repetition
     int* lid;            // [reps][n]
     int* nsub;           // [reps][nsplit] nodes of each split's subgraph
-    int *orig, *lbeg, *ldeg;  // [reps][NS] subgraphs
+    int *orig, *lbeg, *ldeg, *lcw;  // [reps][NS] subgraphs (lcw: node weights)
     int *ladj, *lw;      // [reps][ES]
     // per (repetition, try): node slots of the try's working state
     int *dist, *qa, *qb, *moved_at, *cls;  // [reps * tries][NS]
@@ -75,6 +77,7 @@ struct IpArgs {
     long long* try_cut;                    // [reps][nsplit][tries]
     int seed, depth, tries, jet_iters, jet_patience, jet_c, bal_iters;
     double eps;
+    int smem_bytes;      // dynamic shared memory of ip_try
     int* err;
 };
 
@@ -235,11 +238,15 @@ __device__ int farthest(int n_o, const int* dist, unsigned long long* sh) {
     return (int)(0xffffffffu - (unsigned)(best & 0xffffffffu));
 }
 
+// A bisection's subgraph in local ids: row starts and lengths, entries and
+// their weights, node weights.
 struct Sub {
     int n_o;
-    const int *orig, *lbeg, *ldeg, *ladj, *lw;
-    const int* vwgt;  // of the coarsest graph (through orig)
-    __device__ uint32_t c(int i) const { return (uint32_t)vwgt[orig[i]]; }
+    const int *lbeg, *ldeg;
+    const int* __restrict__ ladj;
+    const int* __restrict__ lw;
+    const int* cw;
+    __device__ uint32_t c(int i) const { return (uint32_t)cw[i]; }
 };
 
 __device__ void side_weights(const Sub& S, const uint8_t* side, unsigned long long w[2], unsigned long long* sh) {
@@ -523,6 +530,7 @@ __global__ void __launch_bounds__(kBT) ip_extract(IpArgs a) {
         if (mem) {
             lid[v] = (int)(cnt + pre);
             orig[cnt + pre] = v;
+            a.lcw[nb + cnt + pre] = a.vwgt[v];
         }
         cnt += tot;
     }
@@ -530,8 +538,18 @@ __global__ void __launch_bounds__(kBT) ip_extract(IpArgs a) {
     if (threadIdx.x == 0) a.nsub[r * a.nsplit + j] = n_o;
     __syncthreads();
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    // rows of up to 32 entries by their own thread, longer rows by a warp
+    for (int i = threadIdx.x; i < n_o; i += kBT) {
+        const int v = orig[i];
+        const int e0 = a.xadj[v], e1 = a.xadj[v + 1];
+        if (e1 - e0 > 32) continue;
+        int d = 0;
+        for (int e = e0; e < e1; ++e) d += part[a.adjncy[e]] == o;
+        ldeg[i] = d;
+    }
     for (int i = wid; i < n_o; i += kBW) {
         const int v = orig[i];
+        if (a.xadj[v + 1] - a.xadj[v] <= 32) continue;
         int d = 0;
         for (int e = a.xadj[v] + lane; e < a.xadj[v + 1]; e += 32) d += part[a.adjncy[e]] == o;
         d = __reduce_add_sync(0xffffffffu, d);
@@ -547,8 +565,22 @@ __global__ void __launch_bounds__(kBT) ip_extract(IpArgs a) {
         erun += tot;
     }
     __syncthreads();
+    for (int i = threadIdx.x; i < n_o; i += kBT) {
+        const int v = orig[i];
+        const int e0 = a.xadj[v], e1 = a.xadj[v + 1];
+        if (e1 - e0 > 32) continue;
+        int w = lbeg[i];
+        for (int e = e0; e < e1; ++e) {
+            const int u = a.adjncy[e];
+            if (part[u] != o) continue;
+            ladj[w] = lid[u];
+            lw[w] = a.adjwgt[e];
+            ++w;
+        }
+    }
     for (int i = wid; i < n_o; i += kBW) {
         const int v = orig[i];
+        if (a.xadj[v + 1] - a.xadj[v] <= 32) continue;
         int w = lbeg[i];
         for (int e0 = a.xadj[v]; e0 < a.xadj[v + 1]; e0 += 32) {
             const int e = e0 + lane;
@@ -573,6 +605,7 @@ __global__ void __launch_bounds__(kBT) ip_try(IpArgs a) {
     __shared__ unsigned long long HS[kIpClasses + 1];
     __shared__ unsigned sh_cnt;
     __shared__ int sh_int[4];
+    extern __shared__ __align__(16) unsigned char dyn[];
     const int t = blockIdx.x % a.tries;
     const int j = (blockIdx.x / a.tries) % a.nsplit;
     const int r = blockIdx.x / (a.tries * a.nsplit);
@@ -580,25 +613,60 @@ __global__ void __launch_bounds__(kBT) ip_try(IpArgs a) {
     const int n_o = a.nsub[r * a.nsplit + j];
     const long long nb = (long long)r * a.NS + a.nbase[r * a.nsplit + j];
     const long long eb = (long long)r * a.ES + a.ebase[r * a.nsplit + j];
-    const Sub S{n_o, a.orig + nb, a.lbeg + nb, a.ldeg + nb, a.ladj + eb, a.lw + eb, a.vwgt};
     const long long res = ((long long)r * a.nsplit + j) * a.tries + t;
     if (n_o == 0) {
         if (threadIdx.x == 0) { a.try_ov[res] = 0; a.try_cut[res] = 0; }
         return;
     }
-    // working state of this try
+    // working state of this try: in shared memory when it fits (kIpSmemPerNode
+    // bytes per node), else in its global slots
     const long long ns = ((long long)r * a.tries + t) * a.NS + a.nbase[r * a.nsplit + j];
-    int* dist = a.dist + ns;
-    int* qa = a.qa + ns;
-    int* qb = a.qb + ns;
-    int* moved_at = a.moved_at + ns;
-    int* cls = a.cls + ns;
-    uint8_t* side = a.side + ns;
-    uint8_t* best = a.best + ns;
-    uint8_t* dest = a.dest + ns;
-    uint8_t* keep = a.keep + ns;
-    long long* gain = a.gain + ns;
-    unsigned long long* layer = a.layer + ns;
+    uint8_t* gside = a.side + ns;
+    const bool in_smem = (long long)(n_o + 2) * kIpSmemPerNode + 64 <= (long long)a.smem_bytes;
+    long long* gain;
+    unsigned long long* layer;
+    int *dist, *qa, *qb, *moved_at, *cls, *lbeg, *ldeg, *cw;
+    uint8_t *side, *best, *dest, *keep;
+    if (in_smem) {
+        const size_t N = (size_t)n_o + 2;
+        unsigned char* p = dyn;
+        gain = reinterpret_cast<long long*>(p); p += 8 * N;
+        layer = reinterpret_cast<unsigned long long*>(p); p += 8 * N;
+        dist = reinterpret_cast<int*>(p); p += 4 * N;
+        qa = reinterpret_cast<int*>(p); p += 4 * N;
+        qb = reinterpret_cast<int*>(p); p += 4 * N;
+        moved_at = reinterpret_cast<int*>(p); p += 4 * N;
+        cls = reinterpret_cast<int*>(p); p += 4 * N;
+        lbeg = reinterpret_cast<int*>(p); p += 4 * N;
+        ldeg = reinterpret_cast<int*>(p); p += 4 * N;
+        cw = reinterpret_cast<int*>(p); p += 4 * N;
+        side = p; p += N;
+        best = p; p += N;
+        dest = p; p += N;
+        keep = p; p += N;
+        for (int i = threadIdx.x; i < n_o; i += kBT) {
+            lbeg[i] = a.lbeg[nb + i];
+            ldeg[i] = a.ldeg[nb + i];
+            cw[i] = a.lcw[nb + i];
+        }
+        __syncthreads();
+    } else {
+        gain = a.gain + ns;
+        layer = a.layer + ns;
+        dist = a.dist + ns;
+        qa = a.qa + ns;
+        qb = a.qb + ns;
+        moved_at = a.moved_at + ns;
+        cls = a.cls + ns;
+        lbeg = a.lbeg + nb;
+        ldeg = a.ldeg + nb;
+        cw = a.lcw + nb;
+        side = gside;
+        best = a.best + ns;
+        dest = a.dest + ns;
+        keep = a.keep + ns;
+    }
+    const Sub S{n_o, lbeg, ldeg, a.ladj + eb, a.lw + eb, cw};
     // targets and bounds
     unsigned long long Wm = 0;
     for (int i = threadIdx.x; i < n_o; i += kBT) Wm += S.c(i);
@@ -671,6 +739,8 @@ __global__ void __launch_bounds__(kBT) ip_try(IpArgs a) {
         a.try_ov[res] = overload2(w, mw);
         a.try_cut[res] = c;
     }
+    if (in_smem)
+        for (int i = threadIdx.x; i < n_o; i += kBT) gside[i] = side[i];
 }
 
 // One thread block per (repetition, split): the try of smallest (overload,
@@ -771,6 +841,7 @@ void initial_partition_device(Ctx& ctx, const DevGraph& c, const Knobs& kn, int*
     a.orig = ctx.scratch.alloc<int>(NSr);
     a.lbeg = ctx.scratch.alloc<int>(NSr);
     a.ldeg = ctx.scratch.alloc<int>(NSr);
+    a.lcw = ctx.scratch.alloc<int>(NSr);
     a.ladj = ctx.scratch.alloc<int>(ESr);
     a.lw = ctx.scratch.alloc<int>(ESr);
     a.dist = ctx.scratch.alloc<int>(NSt);
@@ -793,6 +864,12 @@ void initial_partition_device(Ctx& ctx, const DevGraph& c, const Knobs& kn, int*
     a.jet_c = kn.jet_c;
     a.bal_iters = kn.bal_iters;
     a.eps = eps;
+    a.smem_bytes = kIpSmem;
+    static bool smem_set[64] = {};
+    if (!smem_set[ctx.device & 63]) {
+        KB_CUDA(cudaFuncSetAttribute(ip_try, cudaFuncAttributeMaxDynamicSharedMemorySize, kIpSmem));
+        smem_set[ctx.device & 63] = true;
+    }
     a.err = ctx.dscalars + 60;
     KB_CUDA(cudaMemsetAsync(a.part, 0, sizeof(int) * (size_t)reps * n, st));
     {
@@ -816,7 +893,7 @@ void initial_partition_device(Ctx& ctx, const DevGraph& c, const Knobs& kn, int*
             KB_LAUNCH();
             ip_extract<<<a.nsplit * reps, kBT, 0, st>>>(a);
             KB_LAUNCH();
-            ip_try<<<a.nsplit * reps * tries, kBT, 0, st>>>(a);
+            ip_try<<<a.nsplit * reps * tries, kBT, kIpSmem, st>>>(a);
             KB_LAUNCH();
             ip_select<<<a.nsplit * reps, kBT, 0, st>>>(a);
             KB_LAUNCH();
