@@ -137,24 +137,38 @@ __global__ void check_graph_kernel(int n, long long m, const int* __restrict__ x
         const int last = (int)min(31LL, (long long)n - 1 - g0);
         const long long lo = __shfl_sync(0xffffffffu, x0, 0), hi = __shfl_sync(0xffffffffu, x1, last);
         int carry = 0;
-        for (long long base = lo; base < hi; base += 32) {
-            const long long e = base + lane;
-            const bool ein = e < hi;
-            int t = 0;
-            if (ein) {
-                t = adjncy[e];
-                const int wt = adjwgt[e];
-                if (t < 0 || t >= n) f |= 1;
-                if (wt < 0) f |= 2;
-                if (wt != 1) f |= 16;
+        // four chunks of 32 entries in flight per step (latency-bound otherwise)
+        for (long long base0 = lo; base0 < hi; base0 += 128) {
+            int tt[4], ww[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const long long e = base0 + 32 * c + lane;
+                tt[c] = 0;
+                ww[c] = 1;
+                if (e < hi) {
+                    tt[c] = adjncy[e];
+                    ww[c] = adjwgt[e];
+                }
             }
-            // the row starts that fall into this chunk
-            const unsigned bit = (in && x0 >= base && x0 < base + 32) ? 1u << (int)(x0 - base) : 0u;
-            const unsigned starts = __reduce_or_sync(0xffffffffu, bit);
-            const int up = __shfl_up_sync(0xffffffffu, t, 1);
-            const int prev = lane == 0 ? carry : up;
-            if (ein && !((starts >> lane) & 1u) && t <= prev) f |= 32;
-            carry = __shfl_sync(0xffffffffu, t, 31);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const long long base = base0 + 32 * c;
+                if (base >= hi) break;  // warp-uniform
+                const bool ein = base + lane < hi;
+                const int t = tt[c];
+                if (ein) {
+                    if (t < 0 || t >= n) f |= 1;
+                    if (ww[c] < 0) f |= 2;
+                    if (ww[c] != 1) f |= 16;
+                }
+                // the row starts that fall into this chunk
+                const unsigned bit = (in && x0 >= base && x0 < base + 32) ? 1u << (int)(x0 - base) : 0u;
+                const unsigned starts = __reduce_or_sync(0xffffffffu, bit);
+                const int up = __shfl_up_sync(0xffffffffu, t, 1);
+                const int prev = lane == 0 ? carry : up;
+                if (ein && !((starts >> lane) & 1u) && t <= prev) f |= 32;
+                carry = __shfl_sync(0xffffffffu, t, 31);
+            }
         }
     }
     if (blockIdx.x == 0 && threadIdx.x == 0 && xadj[0] != 0) f |= 8;
