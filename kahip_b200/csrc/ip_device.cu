@@ -40,11 +40,12 @@ namespace kb {
 
 namespace {
 
-constexpr int kBT = 256;              // threads per thread block
-constexpr int kBW = kBT / 32;         // warps
+constexpr int kBT = 256;              // threads per block of the small kernels
+constexpr int kMaxBW = 32;            // warps per block at most (reduction buffers)
+constexpr int kTryMaxBT = 512;        // threads per block of ip_try at most
 constexpr int kIpClasses = 256;       // balance repair classes (loss bucket x 8)
 constexpr int kDenseRows = 16;        // average degree from which a warp walks each row
-constexpr int kIpSmemPerNode = 56;    // shared-memory bytes per node of a try's working state
+constexpr int kIpSmemPerNode = 36;    // shared-memory bytes per node of a try's working state
 constexpr int kIpSmem = 200 * 1024;   // dynamic shared memory of the try kernel
 
 struct IpArgs {
@@ -91,7 +92,7 @@ __device__ __forceinline__ long long warp_sum_ll(long long x) {
     return x;
 }
 
-// Block-wide reductions; every thread gets the result.  `sh` holds kBW + 1
+// Block-wide reductions; every thread gets the result.  `sh` holds kMaxBW + 1
 // words and is free again when the call returns.
 __device__ unsigned long long block_sum(unsigned long long x, unsigned long long* sh) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -101,11 +102,11 @@ __device__ unsigned long long block_sum(unsigned long long x, unsigned long long
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned long long t = 0;
-        for (int w = 0; w < kBW; ++w) t += sh[w];
-        sh[kBW] = t;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+        sh[kMaxBW] = t;
     }
     __syncthreads();
-    const unsigned long long r = sh[kBW];
+    const unsigned long long r = sh[kMaxBW];
     __syncthreads();
     return r;
 }
@@ -118,11 +119,11 @@ __device__ unsigned long long block_min(unsigned long long x, unsigned long long
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned long long t = ~0ull;
-        for (int w = 0; w < kBW; ++w) t = min(t, sh[w]);
-        sh[kBW] = t;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t = min(t, sh[w]);
+        sh[kMaxBW] = t;
     }
     __syncthreads();
-    const unsigned long long r = sh[kBW];
+    const unsigned long long r = sh[kMaxBW];
     __syncthreads();
     return r;
 }
@@ -145,16 +146,16 @@ __device__ unsigned long long block_scan(unsigned long long x, unsigned long lon
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned long long run = 0;
-        for (int w = 0; w < kBW; ++w) {
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
             const unsigned long long t = sh[w];
             sh[w] = run;
             run += t;
         }
-        sh[kBW] = run;
+        sh[kMaxBW] = run;
     }
     __syncthreads();
     const unsigned long long r = sh[wid] + incl - x;
-    *total = sh[kBW];
+    *total = sh[kMaxBW];
     __syncthreads();
     return r;
 }
@@ -166,7 +167,7 @@ template <bool WARP, class F, class G>
 __device__ __forceinline__ void for_rows(int n_o, const int* lbeg, const int* ldeg, F entry, G row) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (WARP) {
-        for (int i = wid; i < n_o; i += kBW) {
+        for (int i = wid; i < n_o; i += (int)(blockDim.x >> 5)) {
             Acc2 s{0, 0};
             const int b = lbeg[i], d = ldeg[i];
             for (int t = lane; t < d; t += 32) entry(i, b + t, s);
@@ -175,10 +176,17 @@ __device__ __forceinline__ void for_rows(int n_o, const int* lbeg, const int* ld
             if (lane == 0) row(i, s);
         }
     } else {
-        for (int i = threadIdx.x; i < n_o; i += kBT) {
+        for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) {
             Acc2 s{0, 0};
             const int b = lbeg[i], d = ldeg[i];
-            for (int t = 0; t < d; ++t) entry(i, b + t, s);
+            int t = 0;
+            for (; t + 4 <= d; t += 4) {  // four independent entries in flight
+                entry(i, b + t, s);
+                entry(i, b + t + 1, s);
+                entry(i, b + t + 2, s);
+                entry(i, b + t + 3, s);
+            }
+            for (; t < d; ++t) entry(i, b + t, s);
             row(i, s);
         }
     }
@@ -188,7 +196,7 @@ __device__ __forceinline__ void for_rows(int n_o, const int* lbeg, const int* ld
 template <bool WARP>
 __device__ void bfs(int n_o, int s, int* dist, int* qa, int* qb, const int* lbeg, const int* ldeg,
                     const int* ladj, unsigned* sh_next) {
-    for (int i = threadIdx.x; i < n_o; i += kBT) dist[i] = INT_MAX;
+    for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) dist[i] = INT_MAX;
     __syncthreads();
     if (threadIdx.x == 0) {
         dist[s] = 0;
@@ -200,7 +208,7 @@ __device__ void bfs(int n_o, int s, int* dist, int* qa, int* qb, const int* lbeg
         if (threadIdx.x == 0) *sh_next = 0;
         __syncthreads();
         if (WARP) {
-            for (int f = wid; f < cnt; f += kBW) {
+            for (int f = wid; f < cnt; f += (int)(blockDim.x >> 5)) {
                 const int v = qa[f], b = lbeg[v], d = ldeg[v];
                 for (int t = lane; t < d; t += 32) {
                     const int u = ladj[b + t];
@@ -208,7 +216,7 @@ __device__ void bfs(int n_o, int s, int* dist, int* qa, int* qb, const int* lbeg
                 }
             }
         } else {
-            for (int f = threadIdx.x; f < cnt; f += kBT) {
+            for (int f = threadIdx.x; f < cnt; f += (int)blockDim.x) {
                 const int v = qa[f], b = lbeg[v], d = ldeg[v];
                 for (int t = 0; t < d; ++t) {
                     const int u = ladj[b + t];
@@ -229,7 +237,7 @@ __device__ void bfs(int n_o, int s, int* dist, int* qa, int* qb, const int* lbeg
 // reached node of largest distance, ties to the smaller id
 __device__ int farthest(int n_o, const int* dist, unsigned long long* sh) {
     unsigned long long best = 0;
-    for (int i = threadIdx.x; i < n_o; i += kBT)
+    for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x)
         if (dist[i] != INT_MAX) {
             const unsigned long long key = ((unsigned long long)(unsigned)dist[i] << 32) | (0xffffffffu - (unsigned)i);
             best = max(best, key);
@@ -251,7 +259,7 @@ struct Sub {
 
 __device__ void side_weights(const Sub& S, const uint8_t* side, unsigned long long w[2], unsigned long long* sh) {
     unsigned long long a = 0, b = 0;
-    for (int i = threadIdx.x; i < S.n_o; i += kBT) (side[i] ? b : a) += S.c(i);
+    for (int i = threadIdx.x; i < S.n_o; i += (int)blockDim.x) (side[i] ? b : a) += S.c(i);
     w[0] = block_sum(a, sh);
     w[1] = block_sum(b, sh);
 }
@@ -291,7 +299,7 @@ __device__ void balance2(const Sub& S, uint8_t* side, int* cls, int s, const uns
         if (w[s] <= mw[s]) break;
         const unsigned long long excess = w[s] - mw[s];
         const unsigned long long cap = mw[1 - s] > w[1 - s] ? mw[1 - s] - w[1 - s] : 0ull;
-        for (int t = threadIdx.x; t < kIpClasses; t += kBT) HS[t] = 0;
+        for (int t = threadIdx.x; t < kIpClasses; t += (int)blockDim.x) HS[t] = 0;
         __syncthreads();
         const uint64_t ks = mix64(ks_cls ^ (uint64_t)it);
         for_rows<WARP>(S.n_o, S.lbeg, S.ldeg,
@@ -325,7 +333,7 @@ __device__ void balance2(const Sub& S, uint8_t* side, int* cls, int s, const uns
         // whole classes, then the partial one by id prefix (in chunks of the
         // block's threads, in id order)
         unsigned long long run = used;
-        for (int base = 0; base < S.n_o; base += kBT) {
+        for (int base = 0; base < S.n_o; base += (int)blockDim.x) {
             const int i = base + threadIdx.x;
             const int c = i < S.n_o ? cls[i] : -1;
             if (c >= 0 && c < full) {
@@ -347,24 +355,24 @@ __device__ void balance2(const Sub& S, uint8_t* side, int* cls, int s, const uns
 }
 
 // Sums of four values over the block; every thread gets them.  `sh` holds
-// 4 * (kBW + 1) words.
+// 4 * (kMaxBW + 1) words.
 __device__ void block_sum4(unsigned long long v[4], unsigned long long* sh) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
 #pragma unroll
         for (int o = 16; o >= 1; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
-        if (lane == 0) sh[q * (kBW + 1) + wid] = v[q];
+        if (lane == 0) sh[q * (kMaxBW + 1) + wid] = v[q];
     }
     __syncthreads();
     if (threadIdx.x < 4) {
         unsigned long long t = 0;
-        for (int w = 0; w < kBW; ++w) t += sh[threadIdx.x * (kBW + 1) + w];
-        sh[threadIdx.x * (kBW + 1) + kBW] = t;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[threadIdx.x * (kMaxBW + 1) + w];
+        sh[threadIdx.x * (kMaxBW + 1) + kMaxBW] = t;
     }
     __syncthreads();
 #pragma unroll
-    for (int q = 0; q < 4; ++q) v[q] = sh[q * (kBW + 1) + kBW];
+    for (int q = 0; q < 4; ++q) v[q] = sh[q * (kMaxBW + 1) + kMaxBW];
     __syncthreads();
 }
 
@@ -393,7 +401,7 @@ __device__ long long jet2(const Sub& S, const IpArgs& a, uint8_t* side, uint8_t*
                           int bis_level, int bis_round, unsigned long long* HS, unsigned long long* sh,
                           unsigned long long* sh4, int* sh_int) {
     const int n_o = S.n_o;
-    for (int i = threadIdx.x; i < n_o; i += kBT) {
+    for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) {
         moved_at[i] = -2;
         best[i] = side[i];
     }
@@ -434,7 +442,7 @@ __device__ long long jet2(const Sub& S, const IpArgs& a, uint8_t* side, uint8_t*
         __syncthreads();
         // moves; the side weights follow from the moved weight
         unsigned long long v[4] = {0, 0, 0, 0};  // moves, weight 0 -> 1, weight 1 -> 0
-        for (int i = threadIdx.x; i < n_o; i += kBT)
+        for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x)
             if (keep[i]) {
                 v[0] += 1;
                 v[side[i] ? 2 : 1] += S.c(i);
@@ -457,7 +465,7 @@ __device__ long long jet2(const Sub& S, const IpArgs& a, uint8_t* side, uint8_t*
         if (ov < best_ov || (ov == best_ov && cut < best_cut)) {
             best_ov = ov;
             best_cut = cut;
-            for (int i = threadIdx.x; i < n_o; i += kBT) best[i] = side[i];
+            for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) best[i] = side[i];
             since = 0;
         } else {
             ++since;
@@ -465,7 +473,7 @@ __device__ long long jet2(const Sub& S, const IpArgs& a, uint8_t* side, uint8_t*
         __syncthreads();
         if (moved == 0 || since >= a.jet_patience) break;
     }
-    for (int i = threadIdx.x; i < n_o; i += kBT) side[i] = best[i];
+    for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) side[i] = best[i];
     __syncthreads();
     return best_cut;
 }
@@ -487,10 +495,10 @@ __global__ void ip_count(IpArgs a) {
 
 // node and edge slot bases per (repetition, split): one thread block
 __global__ void ip_bases(IpArgs a) {
-    __shared__ unsigned long long sh[kBW + 1];
+    __shared__ unsigned long long sh[kMaxBW + 1];
     for (int r = 0; r < a.reps; ++r) {
         unsigned long long nrun = 0, erun = 0;
-        for (int base = 0; base < a.nsplit; base += kBT) {
+        for (int base = 0; base < a.nsplit; base += (int)blockDim.x) {
             const int j = base + threadIdx.x;
             const bool ok = j < a.nsplit;
             unsigned long long nt, et;
@@ -509,7 +517,7 @@ __global__ void ip_bases(IpArgs a) {
 // One thread block per (repetition, split): the split block's subgraph,
 // members in id order, rows restricted to the block, local ids.
 __global__ void __launch_bounds__(kBT) ip_extract(IpArgs a) {
-    __shared__ unsigned long long sh[kBW + 1];
+    __shared__ unsigned long long sh[kMaxBW + 1];
     const int j = blockIdx.x % a.nsplit, r = blockIdx.x / a.nsplit;
     const int o = a.split_o[j];
     const int* part = a.part + (long long)r * a.n;
@@ -521,25 +529,47 @@ __global__ void __launch_bounds__(kBT) ip_extract(IpArgs a) {
     int* ldeg = a.ldeg + nb;
     int* ladj = a.ladj + eb;
     int* lw = a.lw + eb;
-    unsigned long long cnt = 0;
-    for (int base = 0; base < a.n; base += kBT) {
-        const int v = base + threadIdx.x;
-        const bool mem = v < a.n && part[v] == o;
-        unsigned long long tot;
-        const unsigned long long pre = block_scan(mem ? 1ull : 0ull, &tot, sh);
-        if (mem) {
-            lid[v] = (int)(cnt + pre);
-            orig[cnt + pre] = v;
-            a.lcw[nb + cnt + pre] = a.vwgt[v];
-        }
-        cnt += tot;
-    }
-    const int n_o = (int)cnt;
-    if (threadIdx.x == 0) a.nsub[r * a.nsplit + j] = n_o;
-    __syncthreads();
+    // members in id order: every warp counts the members of its own range
+    // of ids, then writes them behind the ranges before it
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nwarps = (int)(blockDim.x >> 5);
+    const int seg = (a.n + nwarps - 1) / nwarps;
+    const int lo = wid * seg, hi = min(a.n, lo + seg);
+    unsigned mine = 0;
+    for (int base = lo; base < hi; base += 32) {
+        const int v = base + lane;
+        mine += __popc(__ballot_sync(0xffffffffu, v < hi && part[v] == o));
+    }
+    if (lane == 0) sh[wid] = mine;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long run = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+            const unsigned long long t = sh[w];
+            sh[w] = run;
+            run += t;
+        }
+        sh[kMaxBW] = run;
+    }
+    __syncthreads();
+    unsigned long long cnt = sh[wid];
+    for (int base = lo; base < hi; base += 32) {
+        const int v = base + lane;
+        const bool mem = v < hi && part[v] == o;
+        const unsigned m = __ballot_sync(0xffffffffu, mem);
+        if (mem) {
+            const unsigned long long idx = cnt + __popc(m & ((1u << lane) - 1u));
+            lid[v] = (int)idx;
+            orig[idx] = v;
+            a.lcw[nb + idx] = a.vwgt[v];
+        }
+        cnt += __popc(m);
+    }
+    const int n_o = (int)sh[kMaxBW];
+    __syncthreads();
+    if (threadIdx.x == 0) a.nsub[r * a.nsplit + j] = n_o;
     // rows of up to 32 entries by their own thread, longer rows by a warp
-    for (int i = threadIdx.x; i < n_o; i += kBT) {
+    for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) {
         const int v = orig[i];
         const int e0 = a.xadj[v], e1 = a.xadj[v + 1];
         if (e1 - e0 > 32) continue;
@@ -547,7 +577,7 @@ __global__ void __launch_bounds__(kBT) ip_extract(IpArgs a) {
         for (int e = e0; e < e1; ++e) d += part[a.adjncy[e]] == o;
         ldeg[i] = d;
     }
-    for (int i = wid; i < n_o; i += kBW) {
+    for (int i = wid; i < n_o; i += (int)(blockDim.x >> 5)) {
         const int v = orig[i];
         if (a.xadj[v + 1] - a.xadj[v] <= 32) continue;
         int d = 0;
@@ -557,7 +587,7 @@ __global__ void __launch_bounds__(kBT) ip_extract(IpArgs a) {
     }
     __syncthreads();
     unsigned long long erun = 0;
-    for (int base = 0; base < n_o; base += kBT) {
+    for (int base = 0; base < n_o; base += (int)blockDim.x) {
         const int i = base + threadIdx.x;
         unsigned long long tot;
         const unsigned long long pre = block_scan(i < n_o ? (unsigned long long)ldeg[i] : 0ull, &tot, sh);
@@ -565,7 +595,7 @@ __global__ void __launch_bounds__(kBT) ip_extract(IpArgs a) {
         erun += tot;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < n_o; i += kBT) {
+    for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) {
         const int v = orig[i];
         const int e0 = a.xadj[v], e1 = a.xadj[v + 1];
         if (e1 - e0 > 32) continue;
@@ -578,7 +608,7 @@ __global__ void __launch_bounds__(kBT) ip_extract(IpArgs a) {
             ++w;
         }
     }
-    for (int i = wid; i < n_o; i += kBW) {
+    for (int i = wid; i < n_o; i += (int)(blockDim.x >> 5)) {
         const int v = orig[i];
         if (a.xadj[v + 1] - a.xadj[v] <= 32) continue;
         int w = lbeg[i];
@@ -599,9 +629,9 @@ __global__ void __launch_bounds__(kBT) ip_extract(IpArgs a) {
 // One thread block per (repetition, split, try): start node, growing and
 // 2-way Jet; the try's sides stay in its side[] slots, its (overload, cut)
 // in try_ov / try_cut.
-__global__ void __launch_bounds__(kBT) ip_try(IpArgs a) {
-    __shared__ unsigned long long sh[kBW + 1];
-    __shared__ unsigned long long sh4[4 * (kBW + 1)];
+__global__ void __launch_bounds__(kTryMaxBT) ip_try(IpArgs a) {
+    __shared__ unsigned long long sh[kMaxBW + 1];
+    __shared__ unsigned long long sh4[4 * (kMaxBW + 1)];
     __shared__ unsigned long long HS[kIpClasses + 1];
     __shared__ unsigned sh_cnt;
     __shared__ int sh_int[4];
@@ -618,36 +648,58 @@ __global__ void __launch_bounds__(kBT) ip_try(IpArgs a) {
         if (threadIdx.x == 0) { a.try_ov[res] = 0; a.try_cut[res] = 0; }
         return;
     }
-    // working state of this try: in shared memory when it fits (kIpSmemPerNode
-    // bytes per node), else in its global slots
+    // working state of this try: in shared memory when it fits
+    // (kIpSmemPerNode bytes per node; buffers whose lives do not overlap
+    // share storage), the subgraph's entries too when they also fit; else
+    // in its global slots
     const long long ns = ((long long)r * a.tries + t) * a.NS + a.nbase[r * a.nsplit + j];
     uint8_t* gside = a.side + ns;
-    const bool in_smem = (long long)(n_o + 2) * kIpSmemPerNode + 64 <= (long long)a.smem_bytes;
+    const long long E_o = (long long)a.lbeg[nb + n_o - 1] + a.ldeg[nb + n_o - 1];
+    const long long need_state = (long long)(n_o + 2) * kIpSmemPerNode + 256;
+    const bool in_smem = need_state <= (long long)a.smem_bytes;
+    const bool csr_smem = in_smem && need_state + 8 * E_o + 64 <= (long long)a.smem_bytes;
     long long* gain;
     unsigned long long* layer;
     int *dist, *qa, *qb, *moved_at, *cls, *lbeg, *ldeg, *cw;
+    const int* ladj = a.ladj + eb;
+    const int* lw = a.lw + eb;
     uint8_t *side, *best, *dest, *keep;
     if (in_smem) {
         const size_t N = (size_t)n_o + 2;
         unsigned char* p = dyn;
-        gain = reinterpret_cast<long long*>(p); p += 8 * N;
-        layer = reinterpret_cast<unsigned long long*>(p); p += 8 * N;
-        dist = reinterpret_cast<int*>(p); p += 4 * N;
-        qa = reinterpret_cast<int*>(p); p += 4 * N;
-        qb = reinterpret_cast<int*>(p); p += 4 * N;
-        moved_at = reinterpret_cast<int*>(p); p += 4 * N;
-        cls = reinterpret_cast<int*>(p); p += 4 * N;
+        gain = reinterpret_cast<long long*>(p);  // growing's layer weights, then Jet's gains
+        layer = reinterpret_cast<unsigned long long*>(p);
+        p += 8 * N;
+        dist = reinterpret_cast<int*>(p);  // distances, then Jet's best / dest / keep bytes
+        best = p;
+        dest = p + N;
+        keep = p + 2 * N;
+        p += 4 * N;
+        qa = reinterpret_cast<int*>(p);  // a BFS queue, then Jet's move iterations
+        moved_at = qa;
+        p += 4 * N;
+        qb = reinterpret_cast<int*>(p);  // the other BFS queue, then balance classes
+        cls = qb;
+        p += 4 * N;
         lbeg = reinterpret_cast<int*>(p); p += 4 * N;
         ldeg = reinterpret_cast<int*>(p); p += 4 * N;
         cw = reinterpret_cast<int*>(p); p += 4 * N;
-        side = p; p += N;
-        best = p; p += N;
-        dest = p; p += N;
-        keep = p; p += N;
-        for (int i = threadIdx.x; i < n_o; i += kBT) {
+        side = p;
+        p += (N + 15) & ~(size_t)15;
+        for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) {
             lbeg[i] = a.lbeg[nb + i];
             ldeg[i] = a.ldeg[nb + i];
             cw[i] = a.lcw[nb + i];
+        }
+        if (csr_smem) {
+            int* sa = reinterpret_cast<int*>(p);
+            int* sw = sa + E_o;
+            for (long long e = threadIdx.x; e < E_o; e += blockDim.x) {
+                sa[e] = a.ladj[eb + e];
+                sw[e] = a.lw[eb + e];
+            }
+            ladj = sa;
+            lw = sw;
         }
         __syncthreads();
     } else {
@@ -666,21 +718,21 @@ __global__ void __launch_bounds__(kBT) ip_try(IpArgs a) {
         dest = a.dest + ns;
         keep = a.keep + ns;
     }
-    const Sub S{n_o, lbeg, ldeg, a.ladj + eb, a.lw + eb, cw};
+    const Sub S{n_o, lbeg, ldeg, ladj, lw, cw};
     // targets and bounds
     unsigned long long Wm = 0;
-    for (int i = threadIdx.x; i < n_o; i += kBT) Wm += S.c(i);
+    for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) Wm += S.c(i);
     const unsigned long long W = block_sum(Wm, sh);
     const unsigned long long t0 = W * (unsigned long long)kl / (unsigned long long)kk, t1 = W - t0;
     const double eb2 = a.split_eb[j];
     const unsigned long long mw[2] = {(unsigned long long)((1.0 + eb2) * (double)t0),
                                       (unsigned long long)((1.0 + eb2) * (double)t1)};
-    const bool warp_rows = (long long)a.lbeg[nb + n_o - 1] + a.ldeg[nb + n_o - 1] >= (long long)kDenseRows * n_o;
+    const bool warp_rows = E_o >= (long long)kDenseRows * n_o;
     const int bis_level = a.split_o[j], bis_round = (r * 32 + a.depth) * 64 + t;
     // 1. start: farthest from the node of smallest (hash, id)
     const uint64_t ks = stream_key(a.seed, TAG_IP, bis_level, bis_round);
     unsigned long long m0 = ~0ull;
-    for (int i = threadIdx.x; i < n_o; i += kBT)
+    for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x)
         m0 = min(m0, ((unsigned long long)hash32(ks, (uint32_t)i) << 32) | (unsigned)i);
     const int s0 = (int)(block_min(m0, sh) & 0xffffffffu);
     if (warp_rows) bfs<true>(n_o, s0, dist, qa, qb, S.lbeg, S.ldeg, S.ladj, &sh_cnt);
@@ -691,13 +743,13 @@ __global__ void __launch_bounds__(kBT) ip_try(IpArgs a) {
     // 2. growing by (distance, id): layer weights, the crossing layer, and
     // the crossing layer's id-order prefix
     unsigned long long md = 0;
-    for (int i = threadIdx.x; i < n_o; i += kBT)
+    for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x)
         if (dist[i] != INT_MAX) md = max(md, (unsigned long long)dist[i]);
     const int maxd = (int)block_max(md, sh);
     const int nl = maxd + 2;
-    for (int l = threadIdx.x; l < nl; l += kBT) layer[l] = 0;
+    for (int l = threadIdx.x; l < nl; l += (int)blockDim.x) layer[l] = 0;
     __syncthreads();
-    for (int i = threadIdx.x; i < n_o; i += kBT)
+    for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x)
         atomicAdd(&layer[dist[i] == INT_MAX ? maxd + 1 : dist[i]], (unsigned long long)S.c(i));
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -711,7 +763,7 @@ __global__ void __launch_bounds__(kBT) ip_try(IpArgs a) {
     const int lc = sh_int[2];
     unsigned long long run = HS[kIpClasses];
     __syncthreads();
-    for (int base = 0; base < n_o; base += kBT) {
+    for (int base = 0; base < n_o; base += (int)blockDim.x) {
         const int i = base + threadIdx.x;
         int l = INT_MAX;
         if (i < n_o) {
@@ -740,7 +792,7 @@ __global__ void __launch_bounds__(kBT) ip_try(IpArgs a) {
         a.try_cut[res] = c;
     }
     if (in_smem)
-        for (int i = threadIdx.x; i < n_o; i += kBT) gside[i] = side[i];
+        for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) gside[i] = side[i];
 }
 
 // One thread block per (repetition, split): the try of smallest (overload,
@@ -758,7 +810,7 @@ __global__ void __launch_bounds__(kBT) ip_select(IpArgs a) {
     const long long nb = (long long)r * a.NS + a.nbase[r * a.nsplit + j];
     const uint8_t* side = a.side + ((long long)r * a.tries + b) * a.NS + a.nbase[r * a.nsplit + j];
     int* part = a.part + (long long)r * a.n;
-    for (int i = threadIdx.x; i < n_o; i += kBT)
+    for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x)
         if (side[i]) part[a.orig[nb + i]] = o + kl;
 }
 
@@ -893,7 +945,15 @@ void initial_partition_device(Ctx& ctx, const DevGraph& c, const Knobs& kn, int*
             KB_LAUNCH();
             ip_extract<<<a.nsplit * reps, kBT, 0, st>>>(a);
             KB_LAUNCH();
-            ip_try<<<a.nsplit * reps * tries, kBT, kIpSmem, st>>>(a);
+            // threads and shared memory per try from the expected subgraph
+            // size at this depth (a larger subgraph falls back to global
+            // memory for what does not fit)
+            const double share = 1.1 / (double)(1LL << std::min<size_t>(d, 40));
+            const long long n_est = (long long)(share * n) + 2, m_est = (long long)(share * (double)c.m);
+            const int bt = n_est > 2048 ? kTryMaxBT : (n_est > 512 ? 256 : 128);
+            const long long want = n_est * kIpSmemPerNode + 8 * m_est + 512;
+            a.smem_bytes = (int)std::min<long long>(kIpSmem, (want + 1023) & ~1023LL);
+            ip_try<<<a.nsplit * reps * tries, bt, a.smem_bytes, st>>>(a);
             KB_LAUNCH();
             ip_select<<<a.nsplit * reps, kBT, 0, st>>>(a);
             KB_LAUNCH();

@@ -383,9 +383,6 @@ __device__ void chunk_process(const SweepArgs& a, WarpTable& T, bool mem, int v,
 
 constexpr int kSlots = 6;  // 4: ~5 % of RGG rows overflow; 6: 0.6 %, fastest measured
 constexpr int kSpan = 2;  // chunks of 32 ids per warp task (2 measured 3 % faster than 4)
-constexpr int kDegClasses = 4;  // member queues by row length: <= 8, <= 16, <= 24, longer
-
-__device__ __forceinline__ int deg_class(int d) { return d <= 8 ? 0 : d <= 16 ? 1 : d <= 24 ? 2 : 3; }
 
 // r-th set bit (0-based) of mask
 __device__ __forceinline__ int nth_set_bit(unsigned mask, int r) {
@@ -531,19 +528,19 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
 template <int MODE, bool UNIT>
 __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
     static_assert(kTab == 256, "slot64 assumes 256 slots");
-    // per-warp queues of members still to be processed, one per degree class
-    // (a pass takes 32 members of one class, so its lanes walk rows of
-    // similar length), and of vertices that overflowed the slots
-    __shared__ int queue[kWarpsPerBlock][kDegClasses][32 * kSpan + 32];
+    // per-warp queue of members still to be processed, so that every pass
+    // over the lanes is full, and of vertices that overflowed the slots
+    __shared__ int queue[kWarpsPerBlock][32 * kSpan + 32];
     __shared__ int oqueue[kWarpsPerBlock][64];
     __shared__ WarpTable tabs[kWarpsPerBlock];
     const int lane = threadIdx.x & 31;
+    int* q = queue[threadIdx.x >> 5];
     int* oq = oqueue[threadIdx.x >> 5];
     WarpTable& T = tabs[threadIdx.x >> 5];
     for (int i = lane; i < kTab; i += 32) { T.key[i] = kEmpty64; T.val[i] = 0; }
     if (lane == 0) T.nused = 0;
     __syncwarp();
-    int qn[kDegClasses] = {}, oqn = 0;  // warp-uniform
+    int qn = 0, oqn = 0;  // warp-uniform
     unsigned long long wv = 0, we = 0, wo = 0;
     const long long span = 32LL * kSpan;
     const long long ntasks = ((long long)a.n + span - 1) / span;
@@ -576,33 +573,21 @@ __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
             const long long vv = base + c * 32 + lane;
             const bool valid = vv < a.n;
             const bool mem = valid && member<MODE>(a, (int)vv);
-            int dc = 0;
-            if (mem) dc = deg_class(a.xadj[vv + 1] - a.xadj[vv]);
-#pragma unroll
-            for (int d = 0; d < kDegClasses; ++d) {
-                const bool in = mem && dc == d;
-                const unsigned m = __ballot_sync(0xffffffffu, in);
-                if (in) queue[threadIdx.x >> 5][d][qn[d] + __popc(m & lanemask_lt())] = (int)vv;
-                qn[d] += __popc(m);
-            }
+            const unsigned m = __ballot_sync(0xffffffffu, mem);
+            if (mem) q[qn + __popc(m & lanemask_lt())] = (int)vv;
+            qn += __popc(m);
         }
         __syncwarp();
-#pragma unroll
-        for (int d = 0; d < kDegClasses; ++d) {
-            int* q = queue[threadIdx.x >> 5][d];
-            while (qn[d] >= 32) {
-                const int v = q[lane];
-                __syncwarp();
-                for (int i = lane; i + 32 < qn[d]; i += 32) q[i] = q[i + 32];
-                __syncwarp();
-                qn[d] -= 32;
-                pass(v);
-            }
+        while (qn >= 32) {
+            const int v = q[lane];
+            __syncwarp();
+            for (int i = lane; i + 32 < qn; i += 32) q[i] = q[i + 32];
+            __syncwarp();
+            qn -= 32;
+            pass(v);
         }
     }
-#pragma unroll
-    for (int d = 0; d < kDegClasses; ++d)
-        if (qn[d] > 0) pass(lane < qn[d] ? queue[threadIdx.x >> 5][d][lane] : -1);
+    if (qn > 0) pass(lane < qn ? q[lane] : -1);
     while (oqn > 0) overflow_pass();
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) {
