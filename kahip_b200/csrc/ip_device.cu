@@ -289,13 +289,70 @@ __device__ __forceinline__ int loss_bucket_d(long long loss) {
 // order until their weight covers the excess; released classes move whole
 // while the other side stays within its bound, and in the first class that
 // does not fit, its nodes in id order while the running weight fits.
+__device__ void block_sum4(unsigned long long v[4], unsigned long long* sh);
+
+// Release threshold T (classes [0, T) cover the excess) and the whole classes
+// that fit the other side, [0, full), with their weight `used`, from the
+// class weights HS[0 .. kIpClasses): warp 0, eight classes per lane.
+__device__ void class_thresholds(const unsigned long long* HS, unsigned long long excess, unsigned long long cap,
+                                 int* T_out, int* full_out, unsigned long long* used_out) {
+    const int L = threadIdx.x;  // warp 0 only
+    unsigned long long h[8], sum = 0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        h[q] = HS[L * 8 + q];
+        sum += h[q];
+    }
+    unsigned long long incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (L >= o) incl += y;
+    }
+    const unsigned long long excl = incl - sum;
+    // T = the first t with (weight of classes before t) >= excess, else kIpClasses
+    int myT = kIpClasses, myF = kIpClasses;
+    unsigned long long run = excl;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        if (myT == kIpClasses && run >= excess) myT = L * 8 + q;
+        if (myF == kIpClasses && run + h[q] > cap) myF = L * 8 + q;
+        run += h[q];
+    }
+    const int T = (int)__reduce_min_sync(0xffffffffu, (unsigned)myT);
+    const int full = min(T, (int)__reduce_min_sync(0xffffffffu, (unsigned)myF));
+    // used = weight of the classes before `full`
+    unsigned long long u = 0;
+    const bool owner = full < kIpClasses ? (full >> 3) == L : L == 31;
+    if (owner) {
+        if (full < kIpClasses) {
+            u = excl;
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                if (L * 8 + q < full) u += h[q];
+        } else {
+            u = incl;
+        }
+    }
+    const unsigned long long used = __shfl_sync(0xffffffffu, u, full < kIpClasses ? (full >> 3) : 31);
+    if (L == 0) {
+        *T_out = T;
+        *full_out = full;
+        *used_out = used;
+    }
+}
+
+// Moves nodes off side s until it is within mw[s]: classes (log2 bucket of
+// conn(own) - conn(other)) x 8 hashed sub-classes; classes are released in
+// order until their weight covers the excess; released classes move whole
+// while the other side stays within its bound, and in the first class that
+// does not fit, its nodes in id order while the running weight fits.  w[]
+// (the side weights, exact on entry) is kept up to date.
 template <bool WARP>
 __device__ void balance2(const Sub& S, uint8_t* side, int* cls, int s, const unsigned long long mw[2],
-                         uint64_t ks_cls, int iters, unsigned long long* HS, unsigned long long* sh,
-                         int* sh_int) {
+                         unsigned long long w[2], uint64_t ks_cls, int iters, unsigned long long* HS,
+                         unsigned long long* sh, unsigned long long* sh4, int* sh_int) {
     for (int it = 0; it < iters; ++it) {
-        unsigned long long w[2];
-        side_weights(S, side, w, sh);
         if (w[s] <= mw[s]) break;
         const unsigned long long excess = w[s] - mw[s];
         const unsigned long long cap = mw[1 - s] > w[1 - s] ? mw[1 - s] - w[1 - s] : 0ull;
@@ -315,42 +372,47 @@ __device__ void balance2(const Sub& S, uint8_t* side, int* cls, int s, const uns
                            atomicAdd(&HS[c], (unsigned long long)S.c(i));
                        });
         __syncthreads();
-        if (threadIdx.x == 0) {
-            int T = 0;
-            unsigned long long rel = 0;
-            while (T < kIpClasses && rel < excess) rel += HS[T++];
-            int full = 0;
-            unsigned long long used = 0;
-            while (full < T && used + HS[full] <= cap) used += HS[full++];
-            sh_int[0] = T;
-            sh_int[1] = full;
-            HS[kIpClasses] = used;
-        }
+        if (threadIdx.x < 32) class_thresholds(HS, excess, cap, &sh_int[0], &sh_int[1], &HS[kIpClasses]);
         __syncthreads();
         const int T = sh_int[0], full = sh_int[1];
         const unsigned long long used = HS[kIpClasses];
-        unsigned long long moved = 0;
+        unsigned long long mv[4] = {0, 0, 0, 0};  // moves, moved weight
         // whole classes, then the partial one by id prefix (in chunks of the
         // block's threads, in id order)
-        unsigned long long run = used;
-        for (int base = 0; base < S.n_o; base += (int)blockDim.x) {
-            const int i = base + threadIdx.x;
-            const int c = i < S.n_o ? cls[i] : -1;
-            if (c >= 0 && c < full) {
-                side[i] = (uint8_t)(1 - s);
-                ++moved;
+        if (full < T) {
+            unsigned long long run = used;
+            for (int base = 0; base < S.n_o; base += (int)blockDim.x) {
+                const int i = base + threadIdx.x;
+                const int c = i < S.n_o ? cls[i] : -1;
+                if (c >= 0 && c < full) {
+                    side[i] = (uint8_t)(1 - s);
+                    mv[0] += 1;
+                    mv[1] += S.c(i);
+                }
+                const bool part_cls = c == full;
+                unsigned long long tot;
+                const unsigned long long pre = block_scan(part_cls ? (unsigned long long)S.c(i) : 0ull, &tot, sh);
+                if (part_cls && run + pre + S.c(i) <= cap) {
+                    side[i] = (uint8_t)(1 - s);
+                    mv[0] += 1;
+                    mv[1] += S.c(i);
+                }
+                run += tot;
             }
-            const bool part_cls = c >= 0 && c == full && full < T;
-            unsigned long long tot;
-            const unsigned long long pre = block_scan(part_cls ? (unsigned long long)S.c(i) : 0ull, &tot, sh);
-            if (part_cls && run + pre + S.c(i) <= cap) {
-                side[i] = (uint8_t)(1 - s);
-                ++moved;
+        } else {
+            for (int i = threadIdx.x; i < S.n_o; i += (int)blockDim.x) {
+                const int c = cls[i];
+                if (c >= 0 && c < full) {
+                    side[i] = (uint8_t)(1 - s);
+                    mv[0] += 1;
+                    mv[1] += S.c(i);
+                }
             }
-            run += tot;
         }
-        __syncthreads();
-        if (block_sum(moved, sh) == 0) break;
+        block_sum4(mv, sh4);
+        w[s] -= mv[1];
+        w[1 - s] += mv[1];
+        if (mv[0] == 0) break;
     }
 }
 
@@ -394,32 +456,50 @@ __device__ void cut_and_weights(const Sub& S, const uint8_t* side, long long* cu
 }
 
 // 2-way Jet on side[] (the best state is kept in best[] and left in side[]);
-// returns its cut.
+// returns its cut.  The cut and side weights of the state an iteration
+// leaves are summed in the next iteration's candidate pass, which reads
+// every row anyway; the best-state bookkeeping of iteration it - 1 runs
+// there, before iteration it moves anything (the same order as evaluating
+// at the end of iteration it - 1).
 template <bool WARP>
 __device__ long long jet2(const Sub& S, const IpArgs& a, uint8_t* side, uint8_t* best, uint8_t* dest,
                           uint8_t* keep, long long* gain, int* moved_at, int* cls, const unsigned long long mw[2],
                           int bis_level, int bis_round, unsigned long long* HS, unsigned long long* sh,
                           unsigned long long* sh4, int* sh_int) {
     const int n_o = S.n_o;
-    for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) {
-        moved_at[i] = -2;
-        best[i] = side[i];
-    }
+    for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) moved_at[i] = -2;
     __syncthreads();
-    unsigned long long w[2];
-    long long best_cut;
-    cut_and_weights<WARP>(S, side, &best_cut, w, sh4);
-    unsigned long long best_ov = overload2(w, mw);
+    unsigned long long best_ov = 0, moved_prev = 0;
+    long long best_cut = 0;
     const long long c4 = a.jet_c;
     int since = 0;
-    for (int it = 0; it < a.jet_iters; ++it) {
-        // candidates
+    bool done = false;
+    // one state evaluation: best tracking, then the stopping rule
+    auto evaluate = [&](long long cut, const unsigned long long w[2], bool first) -> bool {
+        const unsigned long long ov = overload2(w, mw);
+        if (first || ov < best_ov || (ov == best_ov && cut < best_cut)) {
+            best_ov = ov;
+            best_cut = cut;
+            for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) best[i] = side[i];
+            since = 0;
+        } else {
+            ++since;
+        }
+        __syncthreads();
+        return !first && (moved_prev == 0 || since >= a.jet_patience);
+    };
+    int it = 0;
+    for (; it < a.jet_iters; ++it) {
+        // candidates, and the cut and weights of the current state
+        unsigned long long v[4] = {0, 0, 0, 0};
         for_rows<WARP>(n_o, S.lbeg, S.ldeg,
                        [&](int i, int e, Acc2& s) {
                            if (side[S.ladj[e]] == side[i]) s.a += S.lw[e];
                            else s.b += S.lw[e];
                        },
                        [&](int i, const Acc2& s) {
+                           v[0] += (unsigned long long)s.b;
+                           v[side[i] ? 2 : 1] += S.c(i);
                            dest[i] = 0;
                            if (moved_at[i] == it - 1 || s.b == 0) return;
                            const long long gv = s.b - s.a;
@@ -428,7 +508,12 @@ __device__ long long jet2(const Sub& S, const IpArgs& a, uint8_t* side, uint8_t*
                                gain[i] = gv;
                            }
                        });
-        __syncthreads();
+        block_sum4(v, sh4);
+        unsigned long long w[2] = {v[1], v[2]};
+        if (evaluate((long long)(v[0] / 2), w, it == 0)) {
+            done = true;
+            break;
+        }
         // afterburner: gain with every higher-priority candidate neighbour moved
         for_rows<WARP>(n_o, S.lbeg, S.ldeg,
                        [&](int i, int e, Acc2& s) {
@@ -441,37 +526,31 @@ __device__ long long jet2(const Sub& S, const IpArgs& a, uint8_t* side, uint8_t*
                        [&](int i, const Acc2& s) { keep[i] = dest[i] && s.a >= 0; });
         __syncthreads();
         // moves; the side weights follow from the moved weight
-        unsigned long long v[4] = {0, 0, 0, 0};  // moves, weight 0 -> 1, weight 1 -> 0
+        unsigned long long m[4] = {0, 0, 0, 0};  // moves, weight 0 -> 1, weight 1 -> 0
         for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x)
             if (keep[i]) {
-                v[0] += 1;
-                v[side[i] ? 2 : 1] += S.c(i);
+                m[0] += 1;
+                m[side[i] ? 2 : 1] += S.c(i);
                 side[i] ^= 1;
                 moved_at[i] = it;
             }
-        block_sum4(v, sh4);
-        const unsigned long long moved = v[0];
-        w[0] = w[0] - v[1] + v[2];
-        w[1] = w[1] - v[2] + v[1];
+        block_sum4(m, sh4);
+        moved_prev = m[0];
+        w[0] = w[0] - m[1] + m[2];
+        w[1] = w[1] - m[2] + m[1];
         if (w[0] > mw[0] || w[1] > mw[1]) {
             const uint64_t ks_cls = stream_key(a.seed, TAG_BCLS, bis_level, bis_round * 64 + it);
-            const unsigned long long w0[2] = {w[0], w[1]};
+            const bool over[2] = {w[0] > mw[0], w[1] > mw[1]};
             for (int s2 = 0; s2 < 2; ++s2)
-                if (w0[s2] > mw[s2]) balance2<WARP>(S, side, cls, s2, mw, ks_cls, a.bal_iters, HS, sh, sh_int);
+                if (over[s2]) balance2<WARP>(S, side, cls, s2, mw, w, ks_cls, a.bal_iters, HS, sh, sh4, sh_int);
         }
+    }
+    if (!done) {
+        // the state the last iteration left (or the start, without iterations)
         long long cut;
+        unsigned long long w[2];
         cut_and_weights<WARP>(S, side, &cut, w, sh4);
-        const unsigned long long ov = overload2(w, mw);
-        if (ov < best_ov || (ov == best_ov && cut < best_cut)) {
-            best_ov = ov;
-            best_cut = cut;
-            for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) best[i] = side[i];
-            since = 0;
-        } else {
-            ++since;
-        }
-        __syncthreads();
-        if (moved == 0 || since >= a.jet_patience) break;
+        evaluate(cut, w, it == 0);
     }
     for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) side[i] = best[i];
     __syncthreads();
