@@ -595,7 +595,7 @@ __global__ void ip_bases(IpArgs a) {
 
 // One thread block per (repetition, split): the split block's subgraph,
 // members in id order, rows restricted to the block, local ids.
-__global__ void __launch_bounds__(kBT) ip_extract(IpArgs a) {
+__global__ void __launch_bounds__(kTryMaxBT) ip_extract(IpArgs a) {
     __shared__ unsigned long long sh[kMaxBW + 1];
     const int j = blockIdx.x % a.nsplit, r = blockIdx.x / a.nsplit;
     const int o = a.split_o[j];
@@ -652,8 +652,12 @@ __global__ void __launch_bounds__(kBT) ip_extract(IpArgs a) {
         const int v = orig[i];
         const int e0 = a.xadj[v], e1 = a.xadj[v + 1];
         if (e1 - e0 > 32) continue;
-        int d = 0;
-        for (int e = e0; e < e1; ++e) d += part[a.adjncy[e]] == o;
+        int d = 0, e = e0;
+        for (; e + 4 <= e1; e += 4) {  // four independent gathers in flight
+            const int u0 = a.adjncy[e], u1 = a.adjncy[e + 1], u2 = a.adjncy[e + 2], u3 = a.adjncy[e + 3];
+            d += (part[u0] == o) + (part[u1] == o) + (part[u2] == o) + (part[u3] == o);
+        }
+        for (; e < e1; ++e) d += part[a.adjncy[e]] == o;
         ldeg[i] = d;
     }
     for (int i = wid; i < n_o; i += (int)(blockDim.x >> 5)) {
@@ -678,8 +682,25 @@ __global__ void __launch_bounds__(kBT) ip_extract(IpArgs a) {
         const int v = orig[i];
         const int e0 = a.xadj[v], e1 = a.xadj[v + 1];
         if (e1 - e0 > 32) continue;
-        int w = lbeg[i];
-        for (int e = e0; e < e1; ++e) {
+        int w = lbeg[i], e = e0;
+        for (; e + 4 <= e1; e += 4) {  // four independent gathers in flight
+            int u[4], pu[4], wt[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) u[q] = a.adjncy[e + q];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                pu[q] = part[u[q]];
+                wt[q] = a.adjwgt[e + q];
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+                if (pu[q] == o) {
+                    ladj[w] = lid[u[q]];
+                    lw[w] = wt[q];
+                    ++w;
+                }
+        }
+        for (; e < e1; ++e) {
             const int u = a.adjncy[e];
             if (part[u] != o) continue;
             ladj[w] = lid[u];
@@ -1022,7 +1043,7 @@ void initial_partition_device(Ctx& ctx, const DevGraph& c, const Knobs& kn, int*
             KB_LAUNCH();
             ip_bases<<<1, kBT, 0, st>>>(a);
             KB_LAUNCH();
-            ip_extract<<<a.nsplit * reps, kBT, 0, st>>>(a);
+            ip_extract<<<a.nsplit * reps, kTryMaxBT, 0, st>>>(a);
             KB_LAUNCH();
             // threads and shared memory per try from the expected subgraph
             // size at this depth (a larger subgraph falls back to global
