@@ -1050,9 +1050,9 @@ void initial_partition_device(Ctx& ctx, const DevGraph& c, const Knobs& kn, int*
             // memory for what does not fit)
             const double share = 1.1 / (double)(1LL << std::min<size_t>(d, 40));
             const long long n_est = (long long)(share * n) + 2, m_est = (long long)(share * (double)c.m);
-            // (small subgraphs: one or two warps, whose barriers and
-            // reductions cost little)
-            const int bt = n_est > 2048 ? kTryMaxBT : (n_est > 512 ? 256 : (n_est > 128 ? 64 : 32));
+            // (fewer threads on small subgraphs measured slower: a try's
+            // passes run longer per thread than its barriers cost)
+            const int bt = n_est > 2048 ? kTryMaxBT : 256;
             const long long want = n_est * kIpSmemPerNode + 8 * m_est + 512;
             a.smem_bytes = (int)std::min<long long>(kIpSmem, (want + 1023) & ~1023LL);
             ip_try<<<a.nsplit * reps * tries, bt, a.smem_bytes, st>>>(a);
