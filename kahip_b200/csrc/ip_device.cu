@@ -1053,7 +1053,9 @@ void initial_partition_device(Ctx& ctx, const DevGraph& c, const Knobs& kn, int*
             // (fewer threads on small subgraphs measured slower: a try's
             // passes run longer per thread than its barriers cost)
             const int bt = n_est > 2048 ? kTryMaxBT : 256;
-            const long long want = n_est * kIpSmemPerNode + 8 * m_est + 512;
+            // (the rows only when they fit beside the working state)
+            const long long state = n_est * kIpSmemPerNode + 512;
+            const long long want = state + 8 * m_est <= kIpSmem ? state + 8 * m_est : state;
             a.smem_bytes = (int)std::min<long long>(kIpSmem, (want + 1023) & ~1023LL);
             ip_try<<<a.nsplit * reps * tries, bt, a.smem_bytes, st>>>(a);
             KB_LAUNCH();
