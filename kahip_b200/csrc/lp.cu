@@ -1054,7 +1054,6 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
     a.H = H;
     a.minvP = minvP;
     unsigned* moved = b.counters + kCntMoved;
-    cudaEvent_t round_done[2] = {ctx.ev(), ctx.ev()};
     for (int r = 0; r < kn.ref_rounds; ++r) {
         a.active = act;
         a.ks_sub = stream_key(kn.seed, TAG_RSUB, level, r);
@@ -1074,21 +1073,13 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
             KB_LAUNCH();
         }
         std::swap(act, nact);
-        // The host learns a round's move count one round late: round r + 1
-        // is already queued when it reads round r's, so the device does not
-        // idle on the read.  A round after a round without moves has no
-        // active vertex and changes nothing, so results are those of
-        // stopping right after the first round without moves.
-        KB_CUDA(cudaMemcpyAsync(ctx.pinned + 48 + (r & 1), moved, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-        KB_CUDA(cudaEventRecord(round_done[r & 1], st));
-        if (r >= 1) {
-            KB_CUDA(cudaEventSynchronize(round_done[(r - 1) & 1]));
-            if (ctx.pinned[48 + ((r - 1) & 1)] == 0) break;
-        }
+        // (reading the count one round late, with the next round already
+        // queued, measured slower: the queued round after the last one costs
+        // more than the synchronisation it hides)
+        KB_CUDA(cudaMemcpyAsync(ctx.pinned, moved, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        KB_CUDA(cudaStreamSynchronize(st));
+        if (ctx.pinned[0] == 0) break;
     }
-    KB_CUDA(cudaStreamSynchronize(st));
-    ctx.ev_free.push_back(round_done[0]);
-    ctx.ev_free.push_back(round_done[1]);
     ctx.scratch.release(mk);
 }
 
