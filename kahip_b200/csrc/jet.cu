@@ -219,7 +219,8 @@ __device__ __forceinline__ long long afterburn_sum(const JetArgs& A, int v, int 
     return adj;
 }
 
-__global__ void __launch_bounds__(kThreads) jet_afterburn(JetArgs A, uint8_t* keep) {
+__global__ void __launch_bounds__(kThreads) jet_afterburn(JetArgs A, uint8_t* keep, const int* stop) {
+    if (*stop) return;  // the loop ended at this iteration's evaluation
     const int lane = threadIdx.x & 31;
     for (long long base = (long long)blockIdx.x * kThreads; base < A.n; base += (long long)gridDim.x * kThreads) {
         const int v = (int)(base + threadIdx.x);
@@ -244,7 +245,8 @@ __global__ void __launch_bounds__(kThreads) jet_afterburn(JetArgs A, uint8_t* ke
 }
 
 __global__ void jet_apply(int n, int it, const uint8_t* keep, const int* dest, const int* vwgt, int* part,
-                          int* moved_at, uint32_t* bw, unsigned* moved) {
+                          int* moved_at, uint32_t* bw, unsigned* moved, const int* stop) {
+    if (*stop) return;
     unsigned c = 0;
     for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < n; v += (long long)gridDim.x * blockDim.x) {
         if (!keep[v]) continue;
@@ -258,6 +260,64 @@ __global__ void jet_apply(int n, int it, const uint8_t* keep, const int* dest, c
 #pragma unroll
     for (int off = 16; off; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(moved, c);
+}
+
+// The loop's state on the device, so that the host reads it once per
+// iteration: the best (overload, cut) so far, iterations since it improved,
+// whether the current partition is the best one, and whether the loop ended.
+struct JetCtl {
+    unsigned long long best_ov;
+    long long best_cut;
+    int since, stop, part_is_best, pad;
+};
+
+// Judges the partition the previous iteration left (cut2 summed by this
+// iteration's choose kernels, bw current): best tracking, then the stopping
+// rule (a move-less iteration, jet_patience iterations without a better
+// partition, or the iteration cap).  One block.
+__global__ void jet_track(JetCtl* c, const uint32_t* bw, int k, uint32_t bound, const unsigned long long* cut2,
+                          const unsigned* moved, int it, int iters, int patience) {
+    __shared__ unsigned long long red[32];
+    if (c->stop) return;
+    unsigned long long ov = 0;
+    for (int b = threadIdx.x; b < k; b += blockDim.x)
+        if (bw[b] > bound) ov += bw[b] - bound;
+#pragma unroll
+    for (int off = 16; off; off >>= 1) ov += __shfl_xor_sync(0xffffffffu, ov, off);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = ov;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) ov += red[w];
+        const long long cut = (long long)(*cut2 / 2);
+        if (it == 0 || ov < c->best_ov || (ov == c->best_ov && cut < c->best_cut)) {
+            c->best_ov = ov;
+            c->best_cut = cut;
+            c->part_is_best = 1;
+            c->since = 0;
+        } else {
+            c->part_is_best = 0;
+            ++c->since;
+        }
+        c->stop = ((it > 0 && (*moved == 0 || c->since >= patience)) || it == iters) ? 1 : 0;
+    }
+}
+
+// best <- part (and the block weights) when the loop goes on from a new best
+__global__ void jet_save(const JetCtl* c, int n, int k, const int* part, const uint32_t* bw, int* best,
+                         uint32_t* best_bw) {
+    if (c->stop || !c->part_is_best) return;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        best[i] = part[i];
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < k; b += gridDim.x * blockDim.x) best_bw[b] = bw[b];
+}
+
+// part <- best when the loop ended away from its best partition
+__global__ void jet_restore(const JetCtl* c, int n, int k, int* part, uint32_t* bw, const int* best,
+                            const uint32_t* best_bw) {
+    if (c->part_is_best) return;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        part[i] = best[i];
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < k; b += gridDim.x * blockDim.x) bw[b] = best_bw[b];
 }
 
 __global__ void fill_i32_kernel(int n, int v, int* p) {
@@ -305,13 +365,13 @@ void jet_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_
     A.nwide = ctr;
     A.cut2 = cut2;
     // bw holds the block weights of part on entry (the callers keep it
-    // current) and stays current: jet_apply and balance() update it
-    std::vector<uint32_t> hbw((size_t)k);
-    uint64_t best_ov = 0;
-    long long best_cut = 0;
-    bool part_is_best = false;  // best[] is stale while the current partition is the best one
-    unsigned moved = 0;
-    int since = 0;
+    // current) and stays current: jet_apply and balance() update it.  The
+    // best-state bookkeeping and the stopping rule run on the device
+    // (jet_track); the host reads the stop flag once per iteration, in the
+    // synchronisation that balance() needs anyway.
+    JetCtl* ctl = reinterpret_cast<JetCtl*>(ctx.scratch.alloc<unsigned long long>(4));
+    KB_CUDA(cudaMemsetAsync(ctl, 0, sizeof(JetCtl), s));
+    const int* stop = &ctl->stop;
     for (int it = 0;; ++it) {
         // cut of the partition left by the previous iteration (the input at it = 0)
         KB_CUDA(cudaMemsetAsync(cut2, 0, sizeof(unsigned long long), s));
@@ -327,47 +387,26 @@ void jet_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_
         } else {
             block_weights_and_cut(ctx, g, part, k, bw, cut2);
         }
-        unsigned long long c2 = 0;
-        KB_CUDA(cudaMemcpyAsync(&c2, cut2, sizeof(c2), cudaMemcpyDeviceToHost, s));
-        KB_CUDA(cudaMemcpyAsync(hbw.data(), bw, sizeof(uint32_t) * (size_t)k, cudaMemcpyDeviceToHost, s));
-        KB_CUDA(cudaStreamSynchronize(s));
-        uint64_t ov = 0;
-        for (uint32_t x : hbw) if (x > bound) ov += x - bound;
-        const long long cut = (long long)(c2 / 2);
-        if (it == 0 || ov < best_ov || (ov == best_ov && cut < best_cut)) {
-            best_ov = ov;
-            best_cut = cut;
-            part_is_best = true;
-            since = 0;
-        } else {
-            ++since;
-        }
-        if (it > 0 && (moved == 0 || since >= kn.jet_patience)) break;
-        if (it == kn.jet_iters) break;
-        if (part_is_best) {
-            KB_CUDA(cudaMemcpyAsync(best, part, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
-            KB_CUDA(cudaMemcpyAsync(best_bw, bw, sizeof(uint32_t) * (size_t)k, cudaMemcpyDeviceToDevice, s));
-            part_is_best = false;
-        }
         {
             PhaseScope ps(ctx, "jet_afterburn", 0);
-            jet_afterburn<<<grid_for(n), kThreads, 0, s>>>(A, keep);
+            jet_track<<<1, 256, 0, s>>>(ctl, bw, k, bound, cut2, ctr + 1, it, kn.jet_iters, kn.jet_patience);
+            KB_LAUNCH();
+            jet_save<<<grid_for(n), kThreads, 0, s>>>(ctl, n, k, part, bw, best, best_bw);
+            KB_LAUNCH();
+            jet_afterburn<<<grid_for(n), kThreads, 0, s>>>(A, keep, stop);
             KB_LAUNCH();
             KB_CUDA(cudaMemsetAsync(ctr + 1, 0, sizeof(unsigned), s));
-            jet_apply<<<grid_for(n), kThreads, 0, s>>>(n, it, keep, dest, g.vwgt, part, moved_at, bw, ctr + 1);
+            jet_apply<<<grid_for(n), kThreads, 0, s>>>(n, it, keep, dest, g.vwgt, part, moved_at, bw, ctr + 1, stop);
             KB_LAUNCH();
         }
-        KB_CUDA(cudaMemcpyAsync(&moved, ctr + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-        KB_CUDA(cudaMemcpyAsync(hbw.data(), bw, sizeof(uint32_t) * (size_t)k, cudaMemcpyDeviceToHost, s));
-        KB_CUDA(cudaStreamSynchronize(s));
-        uint32_t mx = 0;
-        for (uint32_t x : hbw) mx = std::max(mx, x);
-        if (mx > bound) balance(ctx, g, kn, level, bound, part, bw);
+        KB_CUDA(cudaMemcpyAsync(ctx.pinned + 50, stop, sizeof(int), cudaMemcpyDeviceToHost, s));
+        // repairs an overloaded partition (nothing once the loop has ended);
+        // synchronises, so the stop flag is on the host afterwards
+        balance(ctx, g, kn, level, bound, part, bw, stop);
+        if (ctx.pinned[50]) break;
     }
-    if (!part_is_best) {
-        KB_CUDA(cudaMemcpyAsync(part, best, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, s));
-        KB_CUDA(cudaMemcpyAsync(bw, best_bw, sizeof(uint32_t) * (size_t)k, cudaMemcpyDeviceToDevice, s));
-    }
+    jet_restore<<<grid_for(n), kThreads, 0, s>>>(ctl, n, k, part, bw, best, best_bw);
+    KB_LAUNCH();
     ctx.scratch.release(mk);
 }
 

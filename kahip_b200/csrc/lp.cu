@@ -812,8 +812,16 @@ __global__ void balance_release(SList pl, const int* hpl, const unsigned* hpc, c
 }
 
 // lightest block (ties: smaller id) and whether any block exceeds bound
+// (skip != nullptr and *skip != 0: report no overload, the caller is done)
 __global__ void block_scan_kernel(const uint32_t* bw, int k, uint32_t bound, int* lightest,
-                                  int* over) {
+                                  int* over, const int* skip) {
+    if (skip && *skip) {
+        if (threadIdx.x == 0) {
+            *lightest = 0;
+            *over = 0;
+        }
+        return;
+    }
     __shared__ unsigned long long best[32];
     __shared__ int ov[32];
     unsigned long long mine = ~0ull;
@@ -1086,15 +1094,25 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
 // ------------------------------------------------------------------ balance
 
 bool balance(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t bound, int* part,
-             uint32_t* bw) {
+             uint32_t* bw, const int* skip) {
     const size_t mk = ctx.scratch.mark();
     cudaStream_t st = ctx.stream;
     const int k = kn.k, P = kn.ref_classes;
+    int* flags = ctx.scratch.alloc<int>(2);  // [0] lightest, [1] over
+    // the first check before any set-up: most calls find every block within
+    // the bound
+    block_scan_kernel<<<1, 1024, 0, st>>>(bw, k, bound, flags, flags + 1, skip);
+    KB_LAUNCH();
+    KB_CUDA(cudaMemcpyAsync(ctx.pinned, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    KB_CUDA(cudaStreamSynchronize(st));
+    if (ctx.pinned[0] == 0) {
+        ctx.scratch.release(mk);
+        return true;
+    }
     uint32_t* H = ctx.scratch.alloc<uint32_t>((size_t)k * P);
     int* minvP = ctx.scratch.alloc<int>((size_t)k * P);
     uint32_t* HS = ctx.scratch.alloc<uint32_t>((size_t)k * kBalClasses);
     int* thr = ctx.scratch.alloc<int>((size_t)k);
-    int* flags = ctx.scratch.alloc<int>(2);  // [0] lightest, [1] over
     SweepBuffers b = make_buffers(ctx, g);
     fill_u32(H, (long long)k * P, 0u, st);
     fill_i32(minvP, (long long)k * P, INT_MAX, st);
@@ -1107,11 +1125,13 @@ bool balance(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t b
     a.lightest = flags;
     bool ok = false;
     for (int it = 0; it < kn.bal_iters; ++it) {
-        block_scan_kernel<<<1, 1024, 0, st>>>(bw, k, bound, flags, flags + 1);
-        KB_LAUNCH();
-        KB_CUDA(cudaMemcpyAsync(ctx.pinned, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
-        KB_CUDA(cudaStreamSynchronize(st));
-        if (ctx.pinned[0] == 0) { ok = true; break; }
+        if (it > 0) {  // iteration 0's check ran above
+            block_scan_kernel<<<1, 1024, 0, st>>>(bw, k, bound, flags, flags + 1, nullptr);
+            KB_LAUNCH();
+            KB_CUDA(cudaMemcpyAsync(ctx.pinned, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+            KB_CUDA(cudaStreamSynchronize(st));
+            if (ctx.pinned[0] == 0) { ok = true; break; }
+        }
         PhaseScope ps(ctx, "balance", 0);
         a.ks_tie = stream_key(kn.seed, TAG_BTIE, level, it);
         a.ks_sub = stream_key(kn.seed, TAG_BCLS, level, it);  // release class stream
@@ -1131,7 +1151,7 @@ bool balance(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t b
         KB_LAUNCH();
     }
     if (!ok) {
-        block_scan_kernel<<<1, 1024, 0, st>>>(bw, k, bound, flags, flags + 1);
+        block_scan_kernel<<<1, 1024, 0, st>>>(bw, k, bound, flags, flags + 1, nullptr);
         KB_LAUNCH();
         KB_CUDA(cudaMemcpyAsync(ctx.pinned, flags + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
         KB_CUDA(cudaStreamSynchronize(st));

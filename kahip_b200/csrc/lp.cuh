@@ -38,9 +38,11 @@ void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* la
 void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t bound, int* part,
                uint32_t* bw);
 
-// Exact balance repair; returns true if every block ends <= bound.
+// Exact balance repair; returns true if every block ends <= bound.  skip
+// (device, optional): when *skip != 0 the call does nothing (a caller whose
+// own loop already ended on the device).
 bool balance(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t bound, int* part,
-             uint32_t* bw);
+             uint32_t* bw, const int* skip = nullptr);
 
 // Block weights (bw[k] zeroed and filled) and, when cut != nullptr, the edge
 // cut (device uint64, sum over directed entries / 2 applied by the caller).
