@@ -816,11 +816,15 @@ int kb200_initial_partition(int n, const int* xadj, const int* adjncy, const int
 // graphs instead.  Every item's result is the one a single call with the same
 // arguments returns.
 
+// Default worker count: 8 (at most the host's cores).  With the initial
+// partitioning on the device a worker spends its time queueing kernels; on
+// a 512-graph batch (16-core host) 8 workers gave 296-308 partitions/s,
+// 4 / 6 / 12 / 16 / 24 gave 151-194 / 205-266 / 192-194 / 125-168 / 158-170.
 static int batch_workers(int requested, int count) {
     if (requested > 0) return std::min(requested, std::max(count, 1));
     unsigned hc = std::thread::hardware_concurrency();
-    int w = (int)std::max(4u, std::min(32u, hc ? hc : 8u));
-    return std::min(w, std::max(count, 1));
+    int w = (int)std::min(8u, hc ? hc : 8u);
+    return std::max(1, std::min(w, std::max(count, 1)));
 }
 
 int kb200_kaffpa_batch(kb200_batch_item* items, int count, int workers, kb200_batch_report* report) {
