@@ -729,7 +729,8 @@ __global__ void __launch_bounds__(kTryMaxBT) ip_extract(IpArgs a) {
 // One thread block per (repetition, split, try): start node, growing and
 // 2-way Jet; the try's sides stay in its side[] slots, its (overload, cut)
 // in try_ov / try_cut.
-__global__ void __launch_bounds__(kTryMaxBT) ip_try(IpArgs a) {
+template <int MAXBT>
+__global__ void __launch_bounds__(MAXBT) ip_try(IpArgs a) {
     __shared__ unsigned long long sh[kMaxBW + 1];
     __shared__ unsigned long long sh4[4 * (kMaxBW + 1)];
     __shared__ unsigned long long HS[kIpClasses + 1];
@@ -1019,7 +1020,8 @@ void initial_partition_device(Ctx& ctx, const DevGraph& c, const Knobs& kn, int*
     a.smem_bytes = kIpSmem;
     static bool smem_set[64] = {};
     if (!smem_set[ctx.device & 63]) {
-        KB_CUDA(cudaFuncSetAttribute(ip_try, cudaFuncAttributeMaxDynamicSharedMemorySize, kIpSmem));
+        KB_CUDA(cudaFuncSetAttribute(ip_try<kTryMaxBT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kIpSmem));
+        KB_CUDA(cudaFuncSetAttribute(ip_try<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, kIpSmem));
         smem_set[ctx.device & 63] = true;
     }
     a.err = ctx.dscalars + 60;
@@ -1052,12 +1054,16 @@ void initial_partition_device(Ctx& ctx, const DevGraph& c, const Knobs& kn, int*
             const long long n_est = (long long)(share * n) + 2, m_est = (long long)(share * (double)c.m);
             // (fewer threads on small subgraphs measured slower: a try's
             // passes run longer per thread than its barriers cost)
-            const int bt = n_est > 2048 ? kTryMaxBT : 256;
             // (the rows only when they fit beside the working state)
             const long long state = n_est * kIpSmemPerNode + 512;
             const long long want = state + 8 * m_est <= kIpSmem ? state + 8 * m_est : state;
             a.smem_bytes = (int)std::min<long long>(kIpSmem, (want + 1023) & ~1023LL);
-            ip_try<<<a.nsplit * reps * tries, bt, a.smem_bytes, st>>>(a);
+            if (n_est > 8192) {  // large subgraphs: a whole SM's threads per try
+                ip_try<1024><<<a.nsplit * reps * tries, 1024, a.smem_bytes, st>>>(a);
+            } else {
+                const int bt = n_est > 2048 ? kTryMaxBT : 256;
+                ip_try<kTryMaxBT><<<a.nsplit * reps * tries, bt, a.smem_bytes, st>>>(a);
+            }
             KB_LAUNCH();
             ip_select<<<a.nsplit * reps, kBT, 0, st>>>(a);
             KB_LAUNCH();
