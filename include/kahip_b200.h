@@ -87,11 +87,12 @@ typedef struct kb200_stats {
     int balanced;                  /* final max block weight <= final_bound */
     /* inputs to the report */
     int collect_level_cuts;        /* in: 1 = compute the cut at every level */
-    int timing;                    /* in: 1 = time kernel families with CUDA events */
+    int timing;                    /* in: 1 = time every kernel family with CUDA events,
+                                      2 = only the LP clustering sweep (lp_cluster_sweep) */
     /* timings (milliseconds) */
     double ms_total;               /* wall time of the call on the host */
     double ms_h2d, ms_coarsen, ms_initial, ms_uncoarsen, ms_d2h;
-    /* kernel families (timing == 1): device ms, algorithmic bytes, launches */
+    /* kernel families (timing 1 or 2): device ms, algorithmic bytes, launches */
     int nfamilies;
     char family_name[32][24];
     double family_ms[32];

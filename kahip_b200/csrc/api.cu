@@ -202,7 +202,7 @@ void fill_stats_families(Ctx& ctx, kb200_stats* st) {
 }
 
 void begin_stats(Ctx& ctx, kb200_stats* st) {
-    ctx.timing = st && st->timing;
+    ctx.timing = st ? std::max(0, std::min(2, st->timing)) : 0;
     ctx.reset_stats();
 }
 
@@ -302,7 +302,7 @@ struct PhaseRun {
     PhaseRun(int dev, int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt)
         : lease(dev), ctx(*lease.ctx) {
         reserve_for(ctx, n, xadj[n], true, 1.0);
-        ctx.timing = false;
+        ctx.timing = 0;
         ctx.reset_stats();
         up = upload(ctx, n, xadj, adjncy, adjwgt, vwgt);
         check_uploaded(ctx, up.g);
@@ -390,7 +390,7 @@ int kb200_kaffpae(int n, const int* vwgt, const int* xadj, const int* adjcwgt, c
             try {
                 // the main context holds the graph; the workers reserve their own arenas
                 reserve_for(ctx, n, m, true, attempt == 0 ? 1.0 : 2.0 * attempt);
-                ctx.timing = false;
+                ctx.timing = 0;
                 ctx.reset_stats();
                 Upload up = upload(ctx, n, xadj, adjncy, adjcwgt, vwgt);
                 check_uploaded(ctx, up.g);
@@ -604,7 +604,7 @@ int kb200_rating_train(const kb200_train_graph* graphs, int count, int steps, fl
         Lease lease(dev);
         Ctx& ctx = *lease.ctx;
         reserve_train(ctx, graphs, count);
-        ctx.timing = false;
+        ctx.timing = 0;
         ctx.reset_stats();
         TrainUpload tu;
         if ((rc = upload_train(ctx, graphs, count, tu))) return rc;
@@ -626,7 +626,7 @@ int kb200_rating_grad(const kb200_train_graph* graph, const float* params, float
         Lease lease(dev);
         Ctx& ctx = *lease.ctx;
         reserve_train(ctx, graph, 1);
-        ctx.timing = false;
+        ctx.timing = 0;
         ctx.reset_stats();
         TrainUpload tu;
         if ((rc = upload_train(ctx, graph, 1, tu))) return rc;

@@ -79,12 +79,16 @@ struct Ctx {
     int* dscalars = nullptr;               // 64 ints
     unsigned long long* work = nullptr;    // [0] swept vertices, [1] swept edges
     uint32_t* pinned = nullptr;            // 64 words, page-locked
-    // timing
-    bool timing = false;
+    // timing: 0 off, 1 every kernel family, 2 only the LP clustering sweep
+    int timing = 0;
     std::vector<PhaseTimer> phases;
     struct Pending { int phase; cudaEvent_t a, b; double bytes; };
     std::vector<cudaEvent_t> ev_free;
     std::vector<Pending> pending;
+    // trace: with KB200_TRACE=<file> set, every timed span is appended to the
+    // file as "family start_ms end_ms" relative to the call's first event
+    const char* trace_path = nullptr;
+    cudaEvent_t origin = nullptr;
 
     ~Ctx();
     void init(int dev, cudaStream_t s);
@@ -103,10 +107,13 @@ struct PhaseScope {
     cudaEvent_t a = nullptr;
     double bytes;
     PhaseScope(Ctx& c_, const char* name, double b) : c(c_), id(-1), bytes(b) {
-        if (c.timing) { id = c.phase_id(name); c.begin(id, a); }
+        if (c.timing == 1 || (c.timing == 2 && std::strcmp(name, "lp_cluster_sweep") == 0)) {
+            id = c.phase_id(name);
+            c.begin(id, a);
+        }
     }
     ~PhaseScope() {
-        if (c.timing && id >= 0) c.end(id, a, bytes);
+        if (id >= 0) c.end(id, a, bytes);
     }
 };
 

@@ -49,17 +49,270 @@ __global__ void leader_flags(int n, const int* __restrict__ label, const int* __
         flag[v] = mm[label[v]] == v ? 1u : 0u;
 }
 
-// cmap, coarse node weights and each coarse row's bucket capacity (the
-// degrees of its members)
+// cmap, coarse node weights, each coarse row's bucket capacity (the degrees
+// of its members) and, when msize is given, each coarse node's member count.
+// Consecutive fine nodes often share a coarse node: the lanes of a warp with
+// equal coarse ids add their shares together and one of them does the atomics.
 __global__ void make_cmap(int n, const int* __restrict__ label, const int* __restrict__ mm,
                           const uint32_t* __restrict__ pos, const int* __restrict__ vwgt,
-                          const int* __restrict__ xadj, int* cmap, uint32_t* cvw, uint32_t* rowcap) {
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-        int c = (int)pos[mm[label[v]]];
-        cmap[v] = c;
-        atomicAdd(&cvw[c], (uint32_t)vwgt[v]);
-        const uint32_t d = (uint32_t)(xadj[v + 1] - xadj[v]);
-        if (d) atomicAdd(&rowcap[c], d);
+                          const int* __restrict__ xadj, int* cmap, uint32_t* cvw, uint32_t* rowcap,
+                          uint32_t* msize) {
+    const int lane = threadIdx.x & 31;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
+        const int v = (int)(base + threadIdx.x);
+        const bool ok = v < n;
+        int c = -1;
+        uint32_t w = 0, d = 0;
+        if (ok) {
+            c = (int)pos[mm[label[v]]];
+            cmap[v] = c;
+            w = (uint32_t)vwgt[v];
+            d = (uint32_t)(xadj[v + 1] - xadj[v]);
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, c);
+        const uint32_t sw = __reduce_add_sync(peers, w);
+        const uint32_t sd = __reduce_add_sync(peers, d);
+        if (ok && lane == __ffs(peers) - 1) {
+            atomicAdd(&cvw[c], sw);
+            if (sd) atomicAdd(&rowcap[c], sd);
+            if (msize) atomicAdd(&msize[c], (uint32_t)__popc(peers));
+        }
+    }
+}
+
+// Member rows: the rows (xadj[v], degree) of the fine nodes bucketed by
+// coarse id; mrow[mbeg[c] .. mbeg[c + 1]) are the rows of c's members, in
+// no particular order.
+__global__ void scatter_members(int n, const int* __restrict__ cmap, const int* __restrict__ xadj,
+                                const uint32_t* __restrict__ mbeg, uint32_t* mfill, int2* mrow) {
+    const int lane = threadIdx.x & 31;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
+        const int v = (int)(base + threadIdx.x);
+        const bool ok = v < n;
+        const int c = ok ? cmap[v] : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, c);
+        const int leader = __ffs(peers) - 1;
+        uint32_t at = 0;
+        if (ok && lane == leader) at = atomicAdd(&mfill[c], (uint32_t)__popc(peers));
+        at = __shfl_sync(0xffffffffu, at, leader);
+        if (ok) {
+            const int b = xadj[v];
+            mrow[mbeg[c] + at + __popc(peers & lanemask_lt())] = make_int2(b, xadj[v + 1] - b);
+        }
+    }
+}
+
+// ---- gather contraction: a warp per coarse node walks the rows of all its
+// members back to back (32 entries per batch, kGatherWin batches loaded
+// together), drops the entries inside the node, adds the others into the
+// warp's shared-memory table (shared-memory atomics; a key is inserted by
+// compare-and-swap once), then sorts the distinct targets and writes them to
+// the node's bucket.  Nodes with more than kGatherMaxDistinct distinct targets, or more
+// than kGatherMaxEntries member entries, are flagged (sel) for the emission
+// path below.
+constexpr int kGatherWarps = 8;
+constexpr int kGatherTab = 256;                  // table slots per warp
+constexpr int kGatherMaxDistinct = kGatherTab / 2;
+constexpr int kGatherList = kGatherMaxDistinct + 32;  // a batch may add 32 past the limit
+constexpr int kGatherSort = 256;                 // sort buffer (power of two >= kGatherList)
+constexpr int kGatherWin = 4;
+constexpr int kGatherBlocksPerSM = 6;
+constexpr long long kGatherMaxEntries = 8192;
+
+__device__ __forceinline__ uint32_t gather_slot(uint32_t key) {
+    return (key * 0x9E3779B1u) >> 24;  // kGatherTab == 256
+}
+
+template <bool UNIT>
+__global__ void __launch_bounds__(kGatherWarps * 32, kGatherBlocksPerSM) gather_rows(
+    int nc, const uint32_t* __restrict__ mbeg, const int2* __restrict__ mrow, const int* __restrict__ adjncy,
+    const int* __restrict__ adjwgt, const int* __restrict__ cmap, const uint32_t* __restrict__ rowoff,
+    uint64_t* bucket, uint32_t* ucnt, uint8_t* sel, unsigned* nsel) {
+    static_assert(kGatherTab == 256 && kGatherSort >= kGatherList, "table layout");
+    __shared__ uint32_t tk[kGatherWarps][kGatherTab];
+    __shared__ uint32_t tv[kGatherWarps][kGatherTab];
+    __shared__ uint64_t sb[kGatherWarps][kGatherSort];  // used slots, then the sorted entries
+    __shared__ unsigned tcount[kGatherWarps];
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    volatile uint32_t* K = tk[wp];
+    uint32_t* V = tv[wp];
+    uint64_t* B = sb[wp];
+    for (int i = lane; i < kGatherTab; i += 32) {
+        K[i] = kEmpty;
+        V[i] = 0;
+    }
+    if (lane == 0) tcount[wp] = 0;
+    __syncwarp();
+    const long long nwarps = (long long)gridDim.x * kGatherWarps;
+    long long cc = (long long)blockIdx.x * kGatherWarps + wp;
+    // the next node's member range and row capacity are loaded one node ahead
+    uint32_t nm0 = 0, nm1 = 0, nr0 = 0, nr1 = 0;
+    if (cc < nc) {
+        nm0 = mbeg[cc];
+        nm1 = mbeg[cc + 1];
+        nr0 = rowoff[cc];
+        nr1 = rowoff[cc + 1];
+    }
+    for (; cc < nc; cc += nwarps) {
+        const int c = (int)cc;
+        const uint32_t m0 = nm0, m1 = nm1, r0 = nr0, r1 = nr1;
+        if (cc + nwarps < nc) {
+            nm0 = mbeg[cc + nwarps];
+            nm1 = mbeg[cc + nwarps + 1];
+            nr0 = rowoff[cc + nwarps];
+            nr1 = rowoff[cc + nwarps + 1];
+        }
+        if ((long long)r1 - r0 > kGatherMaxEntries) {
+            if (lane == 0) {
+                sel[c] = 1;
+                atomicAdd(nsel, 1u);
+            }
+            continue;
+        }
+        bool over = false;
+        for (uint32_t mb = m0; mb < m1 && !over; mb += 32) {
+            int beg = 0, deg = 0;
+            if (mb + lane < m1) {
+                const int2 r = mrow[mb + lane];
+                beg = r.x;
+                deg = r.y;
+            }
+            int incl = deg;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int off = incl - deg;
+            const int E = __shfl_sync(0xffffffffu, incl, 31);
+            for (int q0 = 0; q0 < E && !over; q0 += 32 * kGatherWin) {
+                int tg[kGatherWin];
+                uint32_t wg[kGatherWin];
+#pragma unroll
+                for (int b = 0; b < kGatherWin; ++b) {
+                    const int q = q0 + b * 32 + lane;
+                    // owner: the largest lane o with off[o] <= q (its degree is > 0)
+                    int o = 0;
+#pragma unroll
+                    for (int step = 16; step >= 1; step >>= 1) {
+                        const int oc = __shfl_sync(0xffffffffu, off, o + step);
+                        if (oc <= q) o += step;
+                    }
+                    const int ob = __shfl_sync(0xffffffffu, beg, o);
+                    const int oo = __shfl_sync(0xffffffffu, off, o);
+                    tg[b] = -1;
+                    wg[b] = 0;
+                    if (q < E) {
+                        const int e = ob + (q - oo);
+                        tg[b] = adjncy[e];
+                        wg[b] = UNIT ? 1u : (uint32_t)adjwgt[e];
+                    }
+                }
+#pragma unroll
+                for (int b = 0; b < kGatherWin; ++b)
+                    if (tg[b] >= 0) tg[b] = cmap[tg[b]];
+                bool full = false;
+#pragma unroll
+                for (int b = 0; b < kGatherWin; ++b) {
+                    if (tg[b] < 0 || tg[b] == c) continue;
+                    // a new key goes in only while fewer than kGatherMaxDistinct are
+                    // (at most 31 other lanes pass that test together), so the table
+                    // never holds kGatherList keys and the probe ends
+                    const uint32_t key = (uint32_t)tg[b];
+                    uint32_t sl = gather_slot(key);
+                    for (int probe = 0; probe < kGatherTab; ++probe) {
+                        const uint32_t cur = K[sl];
+                        if (cur == key) {
+                            atomicAdd(&V[sl], wg[b]);
+                            break;
+                        }
+                        if (cur == kEmpty) {
+                            if (*(volatile unsigned*)&tcount[wp] >= (unsigned)kGatherMaxDistinct) {
+                                full = true;
+                                break;
+                            }
+                            const uint32_t prev = atomicCAS(const_cast<uint32_t*>(&K[sl]), kEmpty, key);
+                            if (prev == kEmpty) {
+                                B[atomicAdd(&tcount[wp], 1u)] = sl;
+                                atomicAdd(&V[sl], wg[b]);
+                                break;
+                            }
+                            if (prev == key) {
+                                atomicAdd(&V[sl], wg[b]);
+                                break;
+                            }
+                        }
+                        sl = (sl + 1) & (kGatherTab - 1);
+                    }
+                }
+                if (__any_sync(0xffffffffu, full)) over = true;
+            }
+        }
+        __syncwarp();
+        const int d = (int)tcount[wp];
+        if (over) {
+            for (int i = lane; i < d; i += 32) {
+                const uint32_t sl = (uint32_t)B[i];
+                K[sl] = kEmpty;
+                V[sl] = 0;
+            }
+            if (lane == 0) {
+                sel[c] = 1;
+                atomicAdd(nsel, 1u);
+                tcount[wp] = 0;
+            }
+            __syncwarp();
+            continue;
+        }
+        // entries (target << 32 | weight); the table is cleared behind them
+        if (d <= 32) {
+            uint64_t x = ~0ull;
+            if (lane < d) {
+                const uint32_t sl = (uint32_t)B[lane];
+                x = ((uint64_t)K[sl] << 32) | V[sl];
+                K[sl] = kEmpty;
+                V[sl] = 0;
+            }
+            for (int k = 2; k <= 32; k <<= 1)
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    const uint64_t y = __shfl_xor_sync(0xffffffffu, x, j);
+                    const bool lower = (lane & j) == 0, up = (lane & k) == 0;
+                    x = (lower == up) ? (x < y ? x : y) : (x > y ? x : y);
+                }
+            if (lane < d) bucket[(long long)r0 + lane] = x;
+        } else {
+            int P = 64;
+            while (P < d) P <<= 1;
+            for (int i = lane; i < d; i += 32) {
+                const uint32_t sl = (uint32_t)B[i];
+                B[i] = ((uint64_t)K[sl] << 32) | V[sl];
+                K[sl] = kEmpty;
+                V[sl] = 0;
+            }
+            for (int i = d + lane; i < P; i += 32) B[i] = ~0ull;
+            __syncwarp();
+            for (int k = 2; k <= P; k <<= 1)
+                for (int j = k >> 1; j > 0; j >>= 1) {
+                    for (int i = lane; i < P; i += 32) {
+                        const int l = i ^ j;
+                        if (l > i) {
+                            const uint64_t x = B[i], y = B[l];
+                            const bool up = (i & k) == 0;
+                            if ((x > y) == up) {
+                                B[i] = y;
+                                B[l] = x;
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
+            for (int i = lane; i < d; i += 32) bucket[(long long)r0 + i] = B[i];
+        }
+        if (lane == 0) {
+            ucnt[c] = (uint32_t)d;
+            tcount[wp] = 0;
+        }
+        __syncwarp();
     }
 }
 
@@ -109,19 +362,24 @@ __device__ __forceinline__ void emit_range(int e0, int e1, int step, uint32_t ow
 // Rows longer than kEmitLaneDeg are left to emit_wide.  UNIT: every edge
 // weight is 1 (adjwgt is not read).  The row entries of the next group of
 // four are loaded while the coarse ids of the current group are gathered.
+// With sel, only the fine nodes of flagged coarse nodes are emitted, and
+// nothing at all when *nsel is 0.
 template <bool UNIT>
 __global__ void __launch_bounds__(kThreads) emit_kernel(int n, const int* __restrict__ xadj,
                                                         const int* __restrict__ adjncy,
                                                         const int* __restrict__ adjwgt,
                                                         const int* __restrict__ cmap,
                                                         const uint32_t* __restrict__ rowoff, uint32_t* fill,
-                                                        uint64_t* bucket) {
+                                                        uint64_t* bucket, const uint8_t* __restrict__ sel,
+                                                        const unsigned* __restrict__ nsel) {
+    if (nsel && *nsel == 0u) return;
     for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
         const int v = (int)(base + threadIdx.x);
         if (v >= n) continue;
+        const uint32_t own = (uint32_t)cmap[v];
+        if (sel && !sel[own]) continue;
         const int beg = xadj[v], end = xadj[v + 1];
         if (end - beg > kEmitLaneDeg) continue;
-        const uint32_t own = (uint32_t)cmap[v];
         uint32_t st[kEmitSlots], sw[kEmitSlots];
         int used = 0;
         int un[4];
@@ -187,7 +445,9 @@ constexpr int kEmitChunk = 2048;
 __global__ void __launch_bounds__(kThreads) emit_wide(int n, long long m, const int* __restrict__ xadj,
                                                       const int* __restrict__ adjncy, const int* __restrict__ adjwgt,
                                                       const int* __restrict__ cmap, const uint32_t* __restrict__ rowoff,
-                                                      uint32_t* fill, uint64_t* bucket) {
+                                                      uint32_t* fill, uint64_t* bucket, const uint8_t* __restrict__ sel,
+                                                      const unsigned* __restrict__ nsel) {
+    if (nsel && *nsel == 0u) return;
     const int lane = threadIdx.x & 31;
     const long long chunks = (m + kEmitChunk - 1) / kEmitChunk;
     for (long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32; c < chunks;
@@ -203,8 +463,10 @@ __global__ void __launch_bounds__(kThreads) emit_wide(int n, long long m, const 
         for (int v = a; v < n && xadj[v] < hi; ++v) {
             const int beg = xadj[v], end = xadj[v + 1];
             if (end - beg <= kEmitLaneDeg) continue;
+            const uint32_t own = (uint32_t)cmap[v];
+            if (sel && !sel[own]) continue;
             const int s = (int)std::max<long long>(lo, beg), e = (int)std::min<long long>(hi, end);
-            emit_range(s + lane, e, 32, (uint32_t)cmap[v], adjncy, adjwgt, cmap, rowoff, fill, bucket);
+            emit_range(s + lane, e, 32, own, adjncy, adjwgt, cmap, rowoff, fill, bucket);
         }
     }
 }
@@ -230,17 +492,20 @@ constexpr int kMergeWarpsSmall = 8; // warps per block of the register merge
 // most kSegSmall entries (sorted in registers, a 512-byte staging buffer
 // per warp, so many warps fit on an SM); LARGE = true the rows of up to
 // kSegMax entries (sorted in an 8 KiB shared buffer per warp) and marks the
-// longer ones for the global path (bigsz[row] = their size).
+// longer ones for the global path (bigsz[row] = their size).  With sel, only
+// the flagged rows (none when *nsel is 0).
 template <bool LARGE>
 __global__ void __launch_bounds__((LARGE ? kMergeWarps : kMergeWarpsSmall) * 32)
     merge_rows(int nc, const uint32_t* __restrict__ rowoff, const uint32_t* __restrict__ fill, uint64_t* bucket,
-               uint32_t* ucnt, uint32_t* bigsz) {
+               uint32_t* ucnt, uint32_t* bigsz, const uint8_t* __restrict__ sel, const unsigned* __restrict__ nsel) {
     constexpr int W = LARGE ? kMergeWarps : kMergeWarpsSmall;
     constexpr int CAP = LARGE ? kSegMax : kSegSmall;
     __shared__ uint64_t buf[W][CAP];
+    if (nsel && *nsel == 0u) return;
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     uint64_t* b = buf[wp];
     for (long long r = (long long)blockIdx.x * W + wp; r < nc; r += (long long)gridDim.x * W) {
+        if (sel && !sel[r]) continue;  // a row of the gather path
         const long long beg = rowoff[r];
         const int s = (int)fill[r];
         if (LARGE && s > kSegMax) {
@@ -449,50 +714,87 @@ void contract(Ctx& ctx, const DevGraph& g, const int* label, int* cmap, DevGraph
     KB_CUDA(cudaMemsetAsync(cvw, 0, sizeof(int) * (size_t)nc, st));
     KB_CUDA(cudaMemsetAsync(rowcap, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
     KB_CUDA(cudaMemsetAsync(fill, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
+    // clusterings (several members per coarse node on average) take the
+    // gather path; matchings (at most two) the emission path
+    const bool gather = (long long)n * 2 >= (long long)nc * 5;
+    uint32_t* msize = nullptr;
+    if (gather) {
+        msize = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
+        KB_CUDA(cudaMemsetAsync(msize, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
+    }
     {
         PhaseScope ps(ctx, "contract_ids", 16.0 * n);
         make_cmap<<<grid_for(n, 256), 256, 0, st>>>(n, label, mm, pos, g.vwgt, g.xadj, cmap,
-                                                    reinterpret_cast<uint32_t*>(cvw), rowcap);
+                                                    reinterpret_cast<uint32_t*>(cvw), rowcap, msize);
         KB_LAUNCH();
         // bucket of coarse row c: [rowoff[c], rowoff[c] + its members' degrees)
         exclusive_scan_u32(rowcap, rowoff, (long long)nc + 1, nullptr, st, ctx.scratch);
     }
     int tb = 1;
     while ((1LL << tb) < (long long)nc) ++tb;
-    // 2. emission straight into the coarse rows' buckets (at most m entries)
     uint64_t* bucket = ctx.scratch.alloc<uint64_t>((size_t)std::max<long long>(m, 1));
-    {
-        PhaseScope ps(ctx, "contract_emit", (g.unit_weights ? 8.0 : 12.0) * m + 8.0 * n);
-        if (g.unit_weights)
-            emit_kernel<true><<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, g.adjncy, g.adjwgt, cmap, rowoff,
-                                                                          fill, bucket);
-        else
-            emit_kernel<false><<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, g.adjncy, g.adjwgt, cmap, rowoff,
-                                                                           fill, bucket);
-        KB_LAUNCH();
-        if (g.maxdeg > kEmitLaneDeg) {
-            const long long chunks = (m + kEmitChunk - 1) / kEmitChunk;
-            emit_wide<<<grid_for(32LL * chunks, kThreads), kThreads, 0, st>>>(n, m, g.xadj, g.adjncy, g.adjwgt, cmap,
-                                                                           rowoff, fill, bucket);
-            KB_LAUNCH();
-        }
-    }
     uint32_t* ucnt = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
     uint32_t* bigsz = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
     uint32_t* bigoff = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
     uint32_t* big = reinterpret_cast<uint32_t*>(ctx.dscalars + 16);  // [16] long-row entries
+    // ucnt / bigsz have nc + 1 entries (the scans read the last one)
+    KB_CUDA(cudaMemsetAsync(ucnt, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
+    KB_CUDA(cudaMemsetAsync(bigsz, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
+    // 2a. gather path: member lists, then a warp per coarse node; the nodes it
+    // flags go through the emission path, which then skips all others
+    uint8_t* sel = nullptr;
+    unsigned* nsel = nullptr;
+    if (gather) {
+        uint32_t* mbeg = ctx.scratch.alloc<uint32_t>((size_t)nc + 1);
+        uint32_t* mfill = ctx.scratch.alloc<uint32_t>((size_t)nc);
+        int2* mrow = ctx.scratch.alloc<int2>((size_t)n);
+        sel = ctx.scratch.alloc<uint8_t>((size_t)nc);
+        nsel = reinterpret_cast<unsigned*>(ctx.dscalars + 18);  // [18] flagged nodes
+        KB_CUDA(cudaMemsetAsync(mfill, 0, sizeof(uint32_t) * (size_t)nc, st));
+        KB_CUDA(cudaMemsetAsync(sel, 0, (size_t)nc, st));
+        KB_CUDA(cudaMemsetAsync(nsel, 0, sizeof(unsigned), st));
+        {
+            PhaseScope ps(ctx, "contract_ids", 12.0 * n);
+            exclusive_scan_u32(msize, mbeg, (long long)nc + 1, nullptr, st, ctx.scratch);
+            scatter_members<<<grid_for(n, 256), 256, 0, st>>>(n, cmap, g.xadj, mbeg, mfill, mrow);
+            KB_LAUNCH();
+        }
+        PhaseScope ps(ctx, "contract_gather", (g.unit_weights ? 8.0 : 12.0) * m + 16.0 * n);
+        const int gg = (int)std::max<long long>(1, std::min<long long>(div_up(nc, kGatherWarps), (long long)kNumSMs * kGatherBlocksPerSM));
+        if (g.unit_weights)
+            gather_rows<true><<<gg, kGatherWarps * 32, 0, st>>>(nc, mbeg, mrow, g.adjncy, g.adjwgt, cmap, rowoff,
+                                                                bucket, ucnt, sel, nsel);
+        else
+            gather_rows<false><<<gg, kGatherWarps * 32, 0, st>>>(nc, mbeg, mrow, g.adjncy, g.adjwgt, cmap, rowoff,
+                                                                 bucket, ucnt, sel, nsel);
+        KB_LAUNCH();
+    }
+    // 2b. emission straight into the coarse rows' buckets (at most m entries)
+    {
+        PhaseScope ps(ctx, "contract_emit", gather ? 0.0 : (g.unit_weights ? 8.0 : 12.0) * m + 8.0 * n);
+        if (g.unit_weights)
+            emit_kernel<true><<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, g.adjncy, g.adjwgt, cmap, rowoff,
+                                                                          fill, bucket, sel, nsel);
+        else
+            emit_kernel<false><<<grid_for(n, kThreads), kThreads, 0, st>>>(n, g.xadj, g.adjncy, g.adjwgt, cmap, rowoff,
+                                                                           fill, bucket, sel, nsel);
+        KB_LAUNCH();
+        if (g.maxdeg > kEmitLaneDeg) {
+            const long long chunks = (m + kEmitChunk - 1) / kEmitChunk;
+            emit_wide<<<grid_for(32LL * chunks, kThreads), kThreads, 0, st>>>(n, m, g.xadj, g.adjncy, g.adjwgt, cmap,
+                                                                           rowoff, fill, bucket, sel, nsel);
+            KB_LAUNCH();
+        }
+    }
     // 4. merge each row: shared-memory sort for rows up to kSegMax entries
     {
-        PhaseScope ps(ctx, "contract_merge", 16.0 * m);
-        // ucnt / bigsz have nc + 1 entries (the scans read the last one)
-        KB_CUDA(cudaMemsetAsync(ucnt, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
-        KB_CUDA(cudaMemsetAsync(bigsz, 0, sizeof(uint32_t) * ((size_t)nc + 1), st));
+        PhaseScope ps(ctx, "contract_merge", gather ? 0.0 : 16.0 * m);
         const int gs = (int)std::max<long long>(1, std::min<long long>(div_up(nc, kMergeWarpsSmall), (long long)kNumSMs * 16));
-        merge_rows<false><<<gs, kMergeWarpsSmall * 32, 0, st>>>(nc, rowoff, fill, bucket, ucnt, bigsz);
+        merge_rows<false><<<gs, kMergeWarpsSmall * 32, 0, st>>>(nc, rowoff, fill, bucket, ucnt, bigsz, sel, nsel);
         KB_LAUNCH();
         if (g.maxdeg > 0) {
             const int gb = (int)std::max<long long>(1, std::min<long long>(div_up(nc, kMergeWarps), (long long)kNumSMs * 7));
-            merge_rows<true><<<gb, kMergeWarps * 32, 0, st>>>(nc, rowoff, fill, bucket, ucnt, bigsz);
+            merge_rows<true><<<gb, kMergeWarps * 32, 0, st>>>(nc, rowoff, fill, bucket, ucnt, bigsz, sel, nsel);
             KB_LAUNCH();
         }
         exclusive_scan_u32(bigsz, bigoff, (long long)nc + 1, big, st, ctx.scratch);

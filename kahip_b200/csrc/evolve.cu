@@ -104,7 +104,7 @@ void run_tasks(const std::vector<Ctx*>& workers, const DevGraph& g0, int count, 
                 for (int attempt = 0;; ++attempt) {
                     try {
                         reserve_for(c, g0.n, g0.m, false, (attempt == 0 ? 1.0 : 2.0 * attempt) * 1.5);
-                        c.timing = false;
+                        c.timing = 0;
                         c.reset_stats();
                         f(c, i);
                         break;

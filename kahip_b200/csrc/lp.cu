@@ -73,6 +73,7 @@ struct SweepArgs {
     int all_fit;                        // singletons: every neighbour cluster fits (2 max c(v) < bound)
     int admit_all;                      // CLUSTER: every target takes all its proposers
                                         // (max c(v) (max degree + 1) < bound): no admission data
+    int stash;                          // host: sweep with lane_vertex's label stash
     unsigned long long* work;           // [0] vertices, [1] edges
     int* err;                           // set when an invariant breaks
     // BALANCE
@@ -210,9 +211,20 @@ constexpr int kTab = 2 * kWin;            // table slots per warp (load <= 1/2)
 constexpr unsigned long long kEmpty64 = ~0ull;
 constexpr int kWarpsPerBlock = kThreads / 32;
 
+// Labels (and weights) that lane_vertex stashes per lane: column `lane` of a
+// row-major [kStash][32] array, so that lanes never share a bank.  The stash
+// overlays the chunk table, which chunk_process clears before each use.
+constexpr int kStashUnit = 24;  // unit edge weights: labels only
+constexpr int kStashWgt = 12;   // labels, then weights
+
 struct WarpTable {
-    unsigned long long key[kTab];  // (member lane << 32) | label
-    uint32_t val[kTab];
+    union {
+        struct {
+            unsigned long long key[kTab];  // (member lane << 32) | label
+            uint32_t val[kTab];
+        };
+        uint32_t stash[3 * kTab];
+    };
     uint16_t used[kWin];           // slots filled in the current window
     unsigned long long bkey[32];   // per member: best candidate key
     uint32_t bid[32];              // per member: best candidate label
@@ -235,8 +247,8 @@ __device__ __forceinline__ uint32_t slot64(unsigned long long k) {
 // found with shared-memory atomicMax / atomicMin.  Used for the vertices
 // whose neighbours carry more distinct labels than the lane path's slots.
 template <int MODE>
-__device__ void chunk_process(const SweepArgs& a, WarpTable& T, bool mem, int v, unsigned long long& wv,
-                              unsigned long long& we, unsigned long long& wo) {
+__device__ void chunk_process(const SweepArgs& a, WarpTable& T, bool mem, int v, unsigned& wv, unsigned& we,
+                              unsigned& wo) {
     const int lane = threadIdx.x & 31;
     int beg = 0, deg = 0;
     bool heavy = false;
@@ -249,7 +261,7 @@ __device__ void chunk_process(const SweepArgs& a, WarpTable& T, bool mem, int v,
             heavy = true;
         } else {
             wv += 1;
-            we += (unsigned long long)deg;
+            we += (unsigned)deg;
             wo += 1;
         }
         T.own[lane] = (uint32_t)a.lab[v];
@@ -266,6 +278,12 @@ __device__ void chunk_process(const SweepArgs& a, WarpTable& T, bool mem, int v,
     const int off = incl - deg;
     const unsigned lightmask = __ballot_sync(0xffffffffu, light);
     if (!lightmask) return;
+    // the table doubles as lane_vertex's stash: clear it before use
+    for (int i = lane; i < kTab; i += 32) {
+        T.key[i] = kEmpty64;
+        T.val[i] = 0;
+    }
+    __syncwarp();
     int wstart = __ffs(lightmask) - 1;
     while (wstart < 32) {
         // window: lanes [wstart, wend) whose edges fit into kWin slots
@@ -398,8 +416,8 @@ __device__ __forceinline__ int nth_set_bit(unsigned mask, int r) {
 
 // 0: decided (stays), 3: decided (proposes a move), 1: too many distinct
 // labels for NS slots, 2: degree above kWin
-template <int MODE, int NS, bool UNIT>
-__device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, unsigned long long& we) {
+template <int MODE, int NS, bool UNIT, bool STASH>
+__device__ int lane_vertex(const SweepArgs& a, int v, uint32_t* st, unsigned& wv, unsigned& we) {
     const int beg = a.xadj[v], end = a.xadj[v + 1];
     if (end - beg > kWin) return 2;
     const uint32_t own = (uint32_t)a.lab[v];
@@ -437,7 +455,7 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
             }
         }
         wv += 1;
-        we += (unsigned long long)(end - beg);
+        we += (unsigned)(end - beg);
         return decide_emit<MODE>(a, v, own, cv, cown, key, id) ? 3 : 0;
     }
     // NS register slots (label, connection); a new label enters at slot 0 and
@@ -446,6 +464,36 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
 #pragma unroll
     for (int i = 0; i < NS; ++i) { sl[i] = kEmpty; sc[i] = 0; }
     bool overflow = false;
+    auto add_label = [&](uint32_t lt, uint32_t wt) {
+        bool hit = false;
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+            const bool m = sl[j] == lt;
+            sc[j] += m ? wt : 0u;
+            hit |= m;
+        }
+        if (!hit) {
+            overflow |= sl[NS - 1] != kEmpty;
+#pragma unroll
+            for (int j = NS - 1; j > 0; --j) { sl[j] = sl[j - 1]; sc[j] = sc[j - 1]; }
+            sl[0] = lt;
+            sc[0] = wt;
+        }
+    };
+    // STASH: two passes -- the gather pass adds entries of the own label to
+    // cown and stashes the others in shared memory, the slot pass merges the
+    // stash into the slots.  Once most entries carry the own label the slot
+    // search then runs over far fewer entries than the row has (without the
+    // stash every lane's slot search runs whenever one lane of the warp needs
+    // it).
+    constexpr int kStash = UNIT ? kStashUnit : kStashWgt;
+    uint32_t* const stl = st;
+    uint32_t* const stw = st + kStashWgt * 32;  // weights (not UNIT)
+    int ns = 0;
+    auto slot_pass = [&]() {
+        for (int i = 0; i < ns && !overflow; ++i) add_label(stl[i * 32], UNIT ? 1u : stw[i * 32]);
+        ns = 0;
+    };
     // software pipeline: the row entries of the next group of four are
     // loaded while the labels of the current group are gathered
     int un[4];
@@ -480,28 +528,23 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
         }
 #pragma unroll
         for (int t = 0; t < 4; ++t) {
-            if (u[t] < 0) continue;
-            const uint32_t lt = l[t], wt = w[t];
-            if (lt == own) { cown += wt; continue; }
-            bool hit = false;
-#pragma unroll
-            for (int i = 0; i < NS; ++i) {
-                const bool m = sl[i] == lt;
-                sc[i] += m ? wt : 0u;
-                hit |= m;
-            }
-            if (!hit) {
-                overflow |= sl[NS - 1] != kEmpty;
-#pragma unroll
-                for (int i = NS - 1; i > 0; --i) { sl[i] = sl[i - 1]; sc[i] = sc[i - 1]; }
-                sl[0] = lt;
-                sc[0] = wt;
+            if (l[t] == kEmpty) continue;  // past the row's end (labels are < n)
+            if (l[t] == own) {
+                cown += w[t];
+            } else if (STASH) {
+                stl[ns * 32] = l[t];
+                if (!UNIT) stw[ns * 32] = w[t];
+                ++ns;
+            } else {
+                add_label(l[t], w[t]);
             }
         }
+        if (STASH && ns > kStash - 4) slot_pass();  // room for the next group of four
     }
+    if (STASH) slot_pass();
     if (overflow) return 1;
     wv += 1;
-    we += (unsigned long long)(end - beg);
+    we += (unsigned)(end - beg);
     // best candidate: largest connection, ties by smaller tie hash, then
     // smaller label; hashes are computed only for ties
     uint32_t ok[NS];
@@ -525,7 +568,7 @@ __device__ int lane_vertex(const SweepArgs& a, int v, unsigned long long& wv, un
 }
 
 
-template <int MODE, bool UNIT>
+template <int MODE, bool UNIT, bool STASH>
 __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
     static_assert(kTab == 256, "slot64 assumes 256 slots");
     // per-warp queue of members still to be processed, so that every pass
@@ -537,11 +580,11 @@ __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
     int* q = queue[threadIdx.x >> 5];
     int* oq = oqueue[threadIdx.x >> 5];
     WarpTable& T = tabs[threadIdx.x >> 5];
-    for (int i = lane; i < kTab; i += 32) { T.key[i] = kEmpty64; T.val[i] = 0; }
     if (lane == 0) T.nused = 0;
     __syncwarp();
     int qn = 0, oqn = 0;  // warp-uniform
-    unsigned long long wv = 0, we = 0, wo = 0;
+    // per-lane work counts (32 bits: a lane never sees more than m < 2^31 entries)
+    unsigned wv = 0, we = 0, wo = 0;
     const long long span = 32LL * kSpan;
     const long long ntasks = ((long long)a.n + span - 1) / span;
     const long long warp = ((long long)blockIdx.x * kThreads + threadIdx.x) / 32;
@@ -557,7 +600,7 @@ __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
     };
     auto pass = [&](int v) {
         int status = 0;
-        if (v >= 0) status = lane_vertex<MODE, kSlots, UNIT>(a, v, wv, we);
+        if (v >= 0) status = lane_vertex<MODE, kSlots, UNIT, STASH>(a, v, T.stash + lane, wv, we);
         const unsigned om = __ballot_sync(0xffffffffu, status == 1);
         if (status == 1) oq[oqn + __popc(om & lanemask_lt())] = v;
         oqn += __popc(om);
@@ -596,9 +639,9 @@ __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
         wo += __shfl_xor_sync(0xffffffffu, wo, o);
     }
     if (lane == 0 && (wv | we)) {
-        atomicAdd(&a.work[0], wv);
-        atomicAdd(&a.work[1], we);
-        if (wo) atomicAdd(&a.work[2], wo);
+        atomicAdd(&a.work[0], (unsigned long long)wv);
+        atomicAdd(&a.work[1], (unsigned long long)we);
+        if (wo) atomicAdd(&a.work[2], (unsigned long long)wo);
     }
 }
 
@@ -923,8 +966,13 @@ void launch_sweep(Ctx& ctx, const DevGraph& g, SweepArgs a, const SweepBuffers& 
     KB_CUDA(cudaMemsetAsync(b.counters, 0, sizeof(unsigned) * kCntMoved, ctx.stream));
     {
         PhaseScope ps(ctx, family(MODE, 0), bytes);
-        if (g.unit_weights) lane_kernel<MODE, true><<<b.lblocks, kThreads, 0, ctx.stream>>>(a);
-        else lane_kernel<MODE, false><<<b.lblocks, kThreads, 0, ctx.stream>>>(a);
+        if (a.stash) {
+            if (g.unit_weights) lane_kernel<MODE, true, true><<<b.lblocks, kThreads, 0, ctx.stream>>>(a);
+            else lane_kernel<MODE, false, true><<<b.lblocks, kThreads, 0, ctx.stream>>>(a);
+        } else {
+            if (g.unit_weights) lane_kernel<MODE, true, false><<<b.lblocks, kThreads, 0, ctx.stream>>>(a);
+            else lane_kernel<MODE, false, false><<<b.lblocks, kThreads, 0, ctx.stream>>>(a);
+        }
         KB_LAUNCH();
     }
     if (b.gcap > 0) {
@@ -1006,6 +1054,9 @@ void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* la
         // in round 0 every vertex is its own cluster; with no repeated
         // targets per row nothing needs aggregating
         a.singletons = (r == 0 && sorted_rows) ? 1 : 0;
+        // from round 2 on most neighbours share the vertex's cluster: the
+        // stash measured faster there, slower in round 1
+        a.stash = r >= 2 ? 1 : 0;
         a.tie = nullptr;
         a.all_fit = 0;
         // round 0: a target's proposers are its neighbours, so with
@@ -1061,6 +1112,7 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
     a.P = P;
     a.H = H;
     a.minvP = minvP;
+    a.stash = 1;  // most neighbours lie in the vertex's own block
     unsigned* moved = b.counters + kCntMoved;
     for (int r = 0; r < kn.ref_rounds; ++r) {
         a.active = act;
@@ -1123,6 +1175,7 @@ bool balance(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t b
     a.P = P;
     a.HS = HS;
     a.lightest = flags;
+    a.stash = 1;
     bool ok = false;
     for (int it = 0; it < kn.bal_iters; ++it) {
         if (it > 0) {  // iteration 0's check ran above

@@ -6,6 +6,8 @@
 #include "partitioner.cuh"
 
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
 
@@ -26,6 +28,7 @@ Ctx::~Ctx() {
     if (device >= 0) cudaSetDevice(device);
     for (auto& p : pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
     for (auto e : ev_free) cudaEventDestroy(e);
+    if (origin) cudaEventDestroy(origin);
     if (pinned) cudaFreeHost(pinned);
     if (dscalars) cudaFree(dscalars);
     hier.free_all();
@@ -83,9 +86,16 @@ void Ctx::end(int phase, cudaEvent_t a, double bytes) {
 }
 
 void Ctx::collect() {
+    FILE* tf = (trace_path && origin && !pending.empty()) ? std::fopen(trace_path, "a") : nullptr;
     for (auto& p : pending) {
         float ms = 0;
         KB_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+        if (tf) {
+            float t0 = 0, t1 = 0;
+            KB_CUDA(cudaEventElapsedTime(&t0, origin, p.a));
+            KB_CUDA(cudaEventElapsedTime(&t1, origin, p.b));
+            std::fprintf(tf, "%s %.4f %.4f\n", phases[p.phase].name.c_str(), t0, t1);
+        }
         phases[p.phase].ms += ms;
         phases[p.phase].bytes += p.bytes;
         phases[p.phase].launches += 1;
@@ -93,10 +103,22 @@ void Ctx::collect() {
         ev_free.push_back(p.b);
     }
     pending.clear();
+    if (tf) std::fclose(tf);
 }
 
 void Ctx::reset_stats() {
     phases.clear();
+    if (timing) {
+        trace_path = std::getenv("KB200_TRACE");
+        if (trace_path) {
+            if (!origin) KB_CUDA(cudaEventCreate(&origin));
+            KB_CUDA(cudaEventRecord(origin, stream));
+            if (FILE* tf = std::fopen(trace_path, "a")) {
+                std::fprintf(tf, "# call\n");
+                std::fclose(tf);
+            }
+        }
+    }
     if (work) KB_CUDA(cudaMemsetAsync(work, 0, 4 * sizeof(unsigned long long), stream));
     if (dscalars) KB_CUDA(cudaMemsetAsync(dscalars + 60, 0, sizeof(int), stream));
 }
