@@ -71,6 +71,8 @@ typedef struct kb200_knobs {
     int ip_mode;               /* initial partitioning of the coarsest graph: 1 = on the
                                   device, every bisection of a recursion depth in one launch
                                   (default); 0 = the host's multilevel bisection with FM */
+    int ip_jet_iters, ip_jet_patience;  /* ip_mode 1: the 2-way Jet of every bisection try:
+                                  iteration cap, iterations without a better state */
 } kb200_knobs;
 
 /* Parameter count of the learned edge rating (kahip_b200/csrc/learned.cuh). */

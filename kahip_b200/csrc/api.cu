@@ -214,7 +214,7 @@ int check_knobs(const kb200_knobs* kn) {
     if (kn->k < 1 || kn->lpc_subrounds < 1 || kn->ref_subrounds < 1 || kn->ref_classes < 1 ||
         kn->coarsening < 0 || kn->coarsening > 2 || kn->max_levels < 1 || kn->max_levels > 64 ||
         kn->refinement < 0 || kn->refinement > 1 || kn->jet_iters < 0 || kn->jet_patience < 1 ||
-        kn->ip_mode < 0 || kn->ip_mode > 1)
+        kn->ip_mode < 0 || kn->ip_mode > 1 || kn->ip_jet_iters < 0 || kn->ip_jet_patience < 1)
         return fail(KB_ERR_INVALID_INPUT, "invalid knobs");
     return KB_OK;
 }

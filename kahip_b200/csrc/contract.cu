@@ -38,9 +38,17 @@ int grid_for(long long n, int threads) {
     return (int)std::max<long long>(1, std::min<long long>(div_up(n, threads), (long long)kNumSMs * 16));
 }
 
+// mm[c] = the smallest member of cluster c.  Lanes of a warp with the same
+// label take one atomic: the lowest of them holds the group's smallest id.
 __global__ void leader_min(int n, const int* __restrict__ label, int* mm) {
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
-        atomicMin(&mm[label[v]], v);
+    const int lane = threadIdx.x & 31;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
+        const int v = (int)(base + threadIdx.x);
+        const bool ok = v < n;
+        const int l = ok ? label[v] : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, l);
+        if (ok && lane == __ffs(peers) - 1) atomicMin(&mm[l], v);
+    }
 }
 
 __global__ void leader_flags(int n, const int* __restrict__ label, const int* __restrict__ mm,

@@ -46,6 +46,8 @@ constexpr int kTryMaxBT = 512;        // threads per block of ip_try at most
 constexpr int kIpClasses = 256;       // balance repair classes (loss bucket x 8)
 constexpr int kDenseRows = 16;        // average degree from which a warp walks each row
 constexpr int kIpSmemPerNode = 36;    // shared-memory bytes per node of a try's working state
+constexpr int kIpSmemLean = 22;       // ... without row starts, lengths and node weights
+constexpr int kIpSmemBfs = 12;        // breadth-first distances and queues only
 constexpr int kIpSmem = 200 * 1024;   // dynamic shared memory of the try kernel
 
 struct IpArgs {
@@ -192,46 +194,62 @@ __device__ __forceinline__ void for_rows(int n_o, const int* lbeg, const int* ld
     }
 }
 
-// Breadth-first distances from s (INT_MAX = unreached).
+// Breadth-first distances from s (INT_MAX = unreached).  One barrier per
+// level: level L counts its next frontier in sh_next[L % 3], and thread 0
+// clears sh_next[(L + 1) % 3] during level L -- every thread read that
+// counter before the barrier of level L - 1.
+__device__ __forceinline__ void bfs_visit(int u, int next, int* dist, int* qb, unsigned* cnt) {
+    if (atomicCAS(&dist[u], INT_MAX, next) == INT_MAX) qb[atomicAdd(cnt, 1u)] = u;
+}
+
 template <bool WARP>
 __device__ void bfs(int n_o, int s, int* dist, int* qa, int* qb, const int* lbeg, const int* ldeg,
                     const int* ladj, unsigned* sh_next) {
     for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) dist[i] = INT_MAX;
+    if (threadIdx.x == 0) {
+        sh_next[0] = 0;
+        sh_next[1] = 0;
+        sh_next[2] = 0;
+    }
     __syncthreads();
     if (threadIdx.x == 0) {
         dist[s] = 0;
         qa[0] = s;
     }
+    __syncthreads();
     int cnt = 1, level = 0;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     while (cnt > 0) {
-        if (threadIdx.x == 0) *sh_next = 0;
-        __syncthreads();
+        unsigned* nx = sh_next + level % 3;
+        const int next = level + 1;
         if (WARP) {
             for (int f = wid; f < cnt; f += (int)(blockDim.x >> 5)) {
                 const int v = qa[f], b = lbeg[v], d = ldeg[v];
-                for (int t = lane; t < d; t += 32) {
-                    const int u = ladj[b + t];
-                    if (atomicCAS(&dist[u], INT_MAX, level + 1) == INT_MAX) qb[atomicAdd(sh_next, 1u)] = u;
-                }
+                for (int t = lane; t < d; t += 32) bfs_visit(ladj[b + t], next, dist, qb, nx);
             }
         } else {
             for (int f = threadIdx.x; f < cnt; f += (int)blockDim.x) {
                 const int v = qa[f], b = lbeg[v], d = ldeg[v];
-                for (int t = 0; t < d; ++t) {
-                    const int u = ladj[b + t];
-                    if (atomicCAS(&dist[u], INT_MAX, level + 1) == INT_MAX) qb[atomicAdd(sh_next, 1u)] = u;
+                int t = 0;
+                for (; t + 4 <= d; t += 4) {  // four row entries loaded together
+                    const int u0 = ladj[b + t], u1 = ladj[b + t + 1], u2 = ladj[b + t + 2], u3 = ladj[b + t + 3];
+                    bfs_visit(u0, next, dist, qb, nx);
+                    bfs_visit(u1, next, dist, qb, nx);
+                    bfs_visit(u2, next, dist, qb, nx);
+                    bfs_visit(u3, next, dist, qb, nx);
                 }
+                for (; t < d; ++t) bfs_visit(ladj[b + t], next, dist, qb, nx);
             }
         }
+        if (threadIdx.x == 0) sh_next[(level + 1) % 3] = 0;
         __syncthreads();
-        cnt = (int)*sh_next;
-        int* t = qa;
+        cnt = (int)*nx;
+        int* tq = qa;
         qa = qb;
-        qb = t;
+        qb = tq;
         ++level;
-        __syncthreads();
     }
+    __syncthreads();
 }
 
 // reached node of largest distance, ties to the smaller id
@@ -438,6 +456,34 @@ __device__ void block_sum4(unsigned long long v[4], unsigned long long* sh) {
     __syncthreads();
 }
 
+// Sums of four values over the block with one barrier: warp sums go into one
+// of three rotating shared accumulators; call c clears the accumulator of
+// call c + 1, which every thread last read before the barrier of call c - 1.
+// Every thread of the block makes the same calls in the same order.
+struct Red4 {
+    unsigned long long (*acc)[4];  // [3][4], zero before the first call
+    int ph;
+};
+
+__device__ void red4(unsigned long long v[4], Red4& r) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    unsigned long long* b = r.acc[r.ph];
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (v[q]) atomicAdd(&b[q], v[q]);
+    const int nx = r.ph == 2 ? 0 : r.ph + 1;
+    if (threadIdx.x < 4) r.acc[nx][threadIdx.x] = 0;
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = b[q];
+    r.ph = nx;
+}
+
 // cut and side weights of the current sides, in one reduction
 template <bool WARP>
 __device__ void cut_and_weights(const Sub& S, const uint8_t* side, long long* cut, unsigned long long w[2],
@@ -466,15 +512,24 @@ __device__ long long jet2(const Sub& S, const IpArgs& a, uint8_t* side, uint8_t*
                           uint8_t* keep, long long* gain, int* moved_at, int* cls, const unsigned long long mw[2],
                           int bis_level, int bis_round, unsigned long long* HS, unsigned long long* sh,
                           unsigned long long* sh4, int* sh_int) {
+    __shared__ unsigned long long racc[3][4];
     const int n_o = S.n_o;
     for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) moved_at[i] = -2;
+    if (threadIdx.x < 12) racc[threadIdx.x / 4][threadIdx.x % 4] = 0;
     __syncthreads();
+    Red4 red{racc, 0};
+    // the sides alternate between two buffers: the afterburner reads the
+    // current one and writes the moved state into the other (keep[])
+    uint8_t* const side0 = side;
+    uint8_t* nside = keep;
     unsigned long long best_ov = 0, moved_prev = 0;
     long long best_cut = 0;
     const long long c4 = a.jet_c;
     int since = 0;
     bool done = false;
-    // one state evaluation: best tracking, then the stopping rule
+    // one state evaluation: best tracking, then the stopping rule (each
+    // thread copies its own nodes, which no other thread writes before the
+    // copy is read at the end)
     auto evaluate = [&](long long cut, const unsigned long long w[2], bool first) -> bool {
         const unsigned long long ov = overload2(w, mw);
         if (first || ov < best_ov || (ov == best_ov && cut < best_cut)) {
@@ -485,7 +540,6 @@ __device__ long long jet2(const Sub& S, const IpArgs& a, uint8_t* side, uint8_t*
         } else {
             ++since;
         }
-        __syncthreads();
         return !first && (moved_prev == 0 || since >= a.jet_patience);
     };
     int it = 0;
@@ -508,13 +562,16 @@ __device__ long long jet2(const Sub& S, const IpArgs& a, uint8_t* side, uint8_t*
                                gain[i] = gv;
                            }
                        });
-        block_sum4(v, sh4);
+        red4(v, red);
         unsigned long long w[2] = {v[1], v[2]};
         if (evaluate((long long)(v[0] / 2), w, it == 0)) {
             done = true;
             break;
         }
-        // afterburner: gain with every higher-priority candidate neighbour moved
+        // afterburner (gain with every higher-priority candidate neighbour
+        // moved) and the moves it keeps, into the other side buffer; the side
+        // weights follow from the moved weight
+        unsigned long long m[4] = {0, 0, 0, 0};  // moves, weight 0 -> 1, weight 1 -> 0
         for_rows<WARP>(n_o, S.lbeg, S.ldeg,
                        [&](int i, int e, Acc2& s) {
                            if (!dest[i]) return;
@@ -523,18 +580,23 @@ __device__ long long jet2(const Sub& S, const IpArgs& a, uint8_t* side, uint8_t*
                            if (dest[u] && (gain[u] > gain[i] || (gain[u] == gain[i] && u < i))) su = 1 - su;
                            s.a += su != side[i] ? S.lw[e] : -(long long)S.lw[e];
                        },
-                       [&](int i, const Acc2& s) { keep[i] = dest[i] && s.a >= 0; });
-        __syncthreads();
-        // moves; the side weights follow from the moved weight
-        unsigned long long m[4] = {0, 0, 0, 0};  // moves, weight 0 -> 1, weight 1 -> 0
-        for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x)
-            if (keep[i]) {
-                m[0] += 1;
-                m[side[i] ? 2 : 1] += S.c(i);
-                side[i] ^= 1;
-                moved_at[i] = it;
-            }
-        block_sum4(m, sh4);
+                       [&](int i, const Acc2& s) {
+                           const uint8_t si = side[i];
+                           if (dest[i] && s.a >= 0) {
+                               m[0] += 1;
+                               m[si ? 2 : 1] += S.c(i);
+                               nside[i] = (uint8_t)(si ^ 1);
+                               moved_at[i] = it;
+                           } else {
+                               nside[i] = si;
+                           }
+                       });
+        red4(m, red);
+        {
+            uint8_t* tsd = side;
+            side = nside;
+            nside = tsd;
+        }
         moved_prev = m[0];
         w[0] = w[0] - m[1] + m[2];
         w[1] = w[1] - m[2] + m[1];
@@ -552,7 +614,8 @@ __device__ long long jet2(const Sub& S, const IpArgs& a, uint8_t* side, uint8_t*
         cut_and_weights<WARP>(S, side, &cut, w, sh4);
         evaluate(cut, w, it == 0);
     }
-    for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) side[i] = best[i];
+    __syncthreads();
+    for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) side0[i] = best[i];
     __syncthreads();
     return best_cut;
 }
@@ -734,7 +797,7 @@ __global__ void __launch_bounds__(MAXBT) ip_try(IpArgs a) {
     __shared__ unsigned long long sh[kMaxBW + 1];
     __shared__ unsigned long long sh4[4 * (kMaxBW + 1)];
     __shared__ unsigned long long HS[kIpClasses + 1];
-    __shared__ unsigned sh_cnt;
+    __shared__ unsigned sh_cnt[3];
     __shared__ int sh_int[4];
     extern __shared__ __align__(16) unsigned char dyn[];
     const int t = blockIdx.x % a.tries;
@@ -749,24 +812,42 @@ __global__ void __launch_bounds__(MAXBT) ip_try(IpArgs a) {
         if (threadIdx.x == 0) { a.try_ov[res] = 0; a.try_cut[res] = 0; }
         return;
     }
-    // working state of this try: in shared memory when it fits
-    // (kIpSmemPerNode bytes per node; buffers whose lives do not overlap
-    // share storage), the subgraph's entries too when they also fit; else
-    // in its global slots
+    // working state of this try, by what fits in shared memory:
+    //   full  kIpSmemPerNode bytes per node (buffers whose lives do not
+    //         overlap share storage), the subgraph's entries too when they
+    //         also fit;
+    //   lean  the same without the row starts, lengths and node weights
+    //         (read from global memory);
+    //   bfs   only the breadth-first distances and queues;
+    //   none  everything in the try's global slots.
     const long long ns = ((long long)r * a.tries + t) * a.NS + a.nbase[r * a.nsplit + j];
     uint8_t* gside = a.side + ns;
     const long long E_o = (long long)a.lbeg[nb + n_o - 1] + a.ldeg[nb + n_o - 1];
-    const long long need_state = (long long)(n_o + 2) * kIpSmemPerNode + 256;
-    const bool in_smem = need_state <= (long long)a.smem_bytes;
-    const bool csr_smem = in_smem && need_state + 8 * E_o + 64 <= (long long)a.smem_bytes;
-    long long* gain;
-    unsigned long long* layer;
-    int *dist, *qa, *qb, *moved_at, *cls, *lbeg, *ldeg, *cw;
+    const long long N2 = (long long)n_o + 2;
+    const long long need_full = N2 * kIpSmemPerNode + 256;
+    const bool full = need_full <= (long long)a.smem_bytes;
+    const bool lean = !full && N2 * kIpSmemLean + 256 <= (long long)a.smem_bytes;
+    const bool bfs_smem = !full && !lean && N2 * kIpSmemBfs + 256 <= (long long)a.smem_bytes;
+    const bool in_smem = full || lean;  // side[] lives in shared memory
+    const bool csr_smem = full && need_full + 8 * E_o + 64 <= (long long)a.smem_bytes;
+    long long* gain = a.gain + ns;
+    unsigned long long* layer = a.layer + ns;
+    int* dist = a.dist + ns;
+    int* qa = a.qa + ns;
+    int* qb = a.qb + ns;
+    int* moved_at = a.moved_at + ns;
+    int* cls = a.cls + ns;
+    const int* lbeg = a.lbeg + nb;
+    const int* ldeg = a.ldeg + nb;
+    const int* cw = a.lcw + nb;
     const int* ladj = a.ladj + eb;
     const int* lw = a.lw + eb;
-    uint8_t *side, *best, *dest, *keep;
+    uint8_t* side = gside;
+    uint8_t* best = a.best + ns;
+    uint8_t* dest = a.dest + ns;
+    uint8_t* keep = a.keep + ns;
     if (in_smem) {
-        const size_t N = (size_t)n_o + 2;
+        const size_t N = (size_t)N2;
         unsigned char* p = dyn;
         gain = reinterpret_cast<long long*>(p);  // growing's layer weights, then Jet's gains
         layer = reinterpret_cast<unsigned long long*>(p);
@@ -782,15 +863,20 @@ __global__ void __launch_bounds__(MAXBT) ip_try(IpArgs a) {
         qb = reinterpret_cast<int*>(p);  // the other BFS queue, then balance classes
         cls = qb;
         p += 4 * N;
-        lbeg = reinterpret_cast<int*>(p); p += 4 * N;
-        ldeg = reinterpret_cast<int*>(p); p += 4 * N;
-        cw = reinterpret_cast<int*>(p); p += 4 * N;
         side = p;
         p += (N + 15) & ~(size_t)15;
-        for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) {
-            lbeg[i] = a.lbeg[nb + i];
-            ldeg[i] = a.ldeg[nb + i];
-            cw[i] = a.lcw[nb + i];
+        if (full) {
+            int* sbeg = reinterpret_cast<int*>(p); p += 4 * N;
+            int* sdeg = reinterpret_cast<int*>(p); p += 4 * N;
+            int* scw = reinterpret_cast<int*>(p); p += 4 * N;
+            for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) {
+                sbeg[i] = a.lbeg[nb + i];
+                sdeg[i] = a.ldeg[nb + i];
+                scw[i] = a.lcw[nb + i];
+            }
+            lbeg = sbeg;
+            ldeg = sdeg;
+            cw = scw;
         }
         if (csr_smem) {
             int* sa = reinterpret_cast<int*>(p);
@@ -803,21 +889,11 @@ __global__ void __launch_bounds__(MAXBT) ip_try(IpArgs a) {
             lw = sw;
         }
         __syncthreads();
-    } else {
-        gain = a.gain + ns;
-        layer = a.layer + ns;
-        dist = a.dist + ns;
-        qa = a.qa + ns;
-        qb = a.qb + ns;
-        moved_at = a.moved_at + ns;
-        cls = a.cls + ns;
-        lbeg = a.lbeg + nb;
-        ldeg = a.ldeg + nb;
-        cw = a.lcw + nb;
-        side = gside;
-        best = a.best + ns;
-        dest = a.dest + ns;
-        keep = a.keep + ns;
+    } else if (bfs_smem) {
+        const size_t N = (size_t)N2;
+        dist = reinterpret_cast<int*>(dyn);
+        qa = dist + N;
+        qb = qa + N;
     }
     const Sub S{n_o, lbeg, ldeg, ladj, lw, cw};
     // targets and bounds
@@ -836,11 +912,11 @@ __global__ void __launch_bounds__(MAXBT) ip_try(IpArgs a) {
     for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x)
         m0 = min(m0, ((unsigned long long)hash32(ks, (uint32_t)i) << 32) | (unsigned)i);
     const int s0 = (int)(block_min(m0, sh) & 0xffffffffu);
-    if (warp_rows) bfs<true>(n_o, s0, dist, qa, qb, S.lbeg, S.ldeg, S.ladj, &sh_cnt);
-    else bfs<false>(n_o, s0, dist, qa, qb, S.lbeg, S.ldeg, S.ladj, &sh_cnt);
+    if (warp_rows) bfs<true>(n_o, s0, dist, qa, qb, S.lbeg, S.ldeg, S.ladj, sh_cnt);
+    else bfs<false>(n_o, s0, dist, qa, qb, S.lbeg, S.ldeg, S.ladj, sh_cnt);
     const int st = farthest(n_o, dist, sh);
-    if (warp_rows) bfs<true>(n_o, st, dist, qa, qb, S.lbeg, S.ldeg, S.ladj, &sh_cnt);
-    else bfs<false>(n_o, st, dist, qa, qb, S.lbeg, S.ldeg, S.ladj, &sh_cnt);
+    if (warp_rows) bfs<true>(n_o, st, dist, qa, qb, S.lbeg, S.ldeg, S.ladj, sh_cnt);
+    else bfs<false>(n_o, st, dist, qa, qb, S.lbeg, S.ldeg, S.ladj, sh_cnt);
     // 2. growing by (distance, id): layer weights, the crossing layer, and
     // the crossing layer's id-order prefix
     unsigned long long md = 0;
@@ -1012,8 +1088,8 @@ void initial_partition_device(Ctx& ctx, const DevGraph& c, const Knobs& kn, int*
     a.try_cut = ctx.scratch.alloc<long long>((size_t)reps * maxs * tries);
     a.seed = kn.seed;
     a.tries = tries;
-    a.jet_iters = kn.jet_iters;
-    a.jet_patience = kn.jet_patience;
+    a.jet_iters = kn.ip_jet_iters;
+    a.jet_patience = kn.ip_jet_patience;
     a.jet_c = kn.jet_c;
     a.bal_iters = kn.bal_iters;
     a.eps = eps;

@@ -91,6 +91,13 @@ void derive_knobs_total(int n, uint32_t W, int k, double imbalance, int seed, in
     // initial partitioning on the device: every bisection of a recursion
     // depth in one launch (breadth-first growing, 2-way Jet refinement)
     kn.ip_mode = 1;
+    // the bisection tries' 2-way Jet: 20 iterations, patience 8 (against 32 /
+    // 12, on the oracle: final cut +0.04 % in geometric mean over RGG2D 2^15 /
+    // 2^17, RGG3D 2^16, R-MAT 2^15 at k = 16 / 64 / 256, seeds 0-3, and
+    // +0.00 % over RGG2D 2^21, RGG3D 2^20, k = 16 / 64 / 256, seeds 0-4;
+    // 16 / 6 gave +0.09 % and +0.31 %)
+    kn.ip_jet_iters = 20;
+    kn.ip_jet_patience = 8;
 }
 
 }  // namespace kb

@@ -8,7 +8,10 @@ namespace kb {
 namespace {
 
 // One thread per vertex, block-local histogram of block weights when k fits
-// into shared memory, warp-then-block reduction of the cut.
+// into shared memory, warp-then-block reduction of the cut.  The row is read
+// four entries at a time (all loads issued before the block ids are
+// compared); UNIT: every edge weight is 1 (adjwgt is not read).
+template <bool UNIT>
 __global__ void cut_bw_kernel(int n, const int* __restrict__ xadj, const int* __restrict__ adjncy,
                               const int* __restrict__ adjwgt, const int* __restrict__ vwgt,
                               const int* __restrict__ part, int k, uint32_t* bw,
@@ -18,13 +21,39 @@ __global__ void cut_bw_kernel(int n, const int* __restrict__ xadj, const int* __
         for (int b = threadIdx.x; b < k; b += blockDim.x) hist[b] = 0;
     __syncthreads();
     unsigned long long c = 0;
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-        int p = part[v];
-        if (use_smem) atomicAdd(&hist[p], (uint32_t)vwgt[v]);
-        else atomicAdd(&bw[p], (uint32_t)vwgt[v]);
+    const int lane = threadIdx.x & 31;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
+        const int v = (int)(base + threadIdx.x);
+        const bool ok = v < n;
+        const int p = ok ? part[v] : -1;
+        // neighbouring vertices mostly share a block: one atomic per block
+        // id present in the warp
+        const unsigned peers = __match_any_sync(0xffffffffu, p);
+        const uint32_t wsum = __reduce_add_sync(peers, ok ? (uint32_t)vwgt[v] : 0u);
+        if (ok && lane == __ffs(peers) - 1) {
+            if (use_smem) atomicAdd(&hist[p], wsum);
+            else atomicAdd(&bw[p], wsum);
+        }
+        if (!ok) continue;
         if (cut2) {
-            for (int e = xadj[v]; e < xadj[v + 1]; ++e)
-                if (part[adjncy[e]] != p) c += (unsigned long long)(long long)adjwgt[e];
+            const int beg = xadj[v], end = xadj[v + 1];
+            int e = beg;
+            for (; e + 4 <= end; e += 4) {
+                int u[4];
+                long long w[4];
+#pragma unroll
+                for (int t = 0; t < 4; ++t) {
+                    u[t] = adjncy[e + t];
+                    w[t] = UNIT ? 1 : (long long)adjwgt[e + t];
+                }
+#pragma unroll
+                for (int t = 0; t < 4; ++t) u[t] = part[u[t]];
+#pragma unroll
+                for (int t = 0; t < 4; ++t)
+                    if (u[t] != p) c += (unsigned long long)w[t];
+            }
+            for (; e < end; ++e)
+                if (part[adjncy[e]] != p) c += UNIT ? 1ull : (unsigned long long)(long long)adjwgt[e];
         }
     }
     __syncthreads();
@@ -205,9 +234,13 @@ void block_weights_and_cut(Ctx& ctx, const DevGraph& g, const int* part, int k, 
     int use_smem = k <= 12288;
     size_t smem = use_smem ? sizeof(uint32_t) * (size_t)k : 0;
     PhaseScope ps(ctx, cut2 ? "cut_and_weights" : "block_weights",
-                  cut2 ? 12.0 * g.m + 12.0 * g.n : 8.0 * g.n);
-    cut_bw_kernel<<<grid_for(g.n, 256), 256, smem, st>>>(g.n, g.xadj, g.adjncy, g.adjwgt, g.vwgt, part, k,
-                                                         bw, cut2, use_smem);
+                  cut2 ? (g.unit_weights ? 8.0 : 12.0) * g.m + 12.0 * g.n : 8.0 * g.n);
+    if (g.unit_weights)
+        cut_bw_kernel<true><<<grid_for(g.n, 256), 256, smem, st>>>(g.n, g.xadj, g.adjncy, g.adjwgt, g.vwgt, part, k,
+                                                                   bw, cut2, use_smem);
+    else
+        cut_bw_kernel<false><<<grid_for(g.n, 256), 256, smem, st>>>(g.n, g.xadj, g.adjncy, g.adjwgt, g.vwgt, part,
+                                                                    k, bw, cut2, use_smem);
     KB_LAUNCH();
 }
 

@@ -119,6 +119,8 @@ void or_derive_knobs(int n, const int* vwgt, int k, double imbalance, int seed, 
     o->jet_c0 = 1;
     o->jet_c = 3;
     o->ip_mode = 1;
+    o->ip_jet_iters = 20;
+    o->ip_jet_patience = 8;
 }
 
 /* stop_rules.h:64-66: continue coarsening after a level that went from nf to
@@ -1464,7 +1466,8 @@ static void balance2(const or_graph* g, char* side, int s, const uint64_t maxw[2
 }
 
 /* 2-way Jet refinement with a bound per side (or_jet_refine for two labels,
- * c4 = jet_c); returns the cut of the best (overload, cut) state kept */
+ * c4 = jet_c, at most ip_jet_iters iterations, patience ip_jet_patience);
+ * returns the cut of the best (overload, cut) state kept */
 static long long jet2(const or_graph* g, char* side, const uint64_t maxw[2], const or_knobs* kn, int bis_level,
                       int bis_round) {
     const int n = g->n;
@@ -1481,7 +1484,7 @@ static long long jet2(const or_graph* g, char* side, const uint64_t maxw[2], con
     long long best_cut = cut2(g, side);
     const int c4 = kn->jet_c;
     int since = 0;
-    for (int it = 0; it < kn->jet_iters; ++it) {
+    for (int it = 0; it < kn->ip_jet_iters; ++it) {
         for (int v = 0; v < n; ++v) {
             dest[v] = 0;
             if (moved_at[v] == it - 1) continue;
@@ -1525,7 +1528,7 @@ static long long jet2(const or_graph* g, char* side, const uint64_t maxw[2], con
         } else {
             ++since;
         }
-        if (moved == 0 || since >= kn->jet_patience) break;
+        if (moved == 0 || since >= kn->ip_jet_patience) break;
     }
     memcpy(side, best, (size_t)n);
     free(best); free(dest); free(keep); free(gain); free(moved_at);

@@ -54,6 +54,7 @@ typedef struct {
     int jet_iters, jet_patience, jet_c0, jet_c;
     int ip_mode;               /* 0 = multilevel recursive bisection with FM (host form),
                                   1 = batched recursive bisection (the device's form) */
+    int ip_jet_iters, ip_jet_patience;  /* ip_mode 1: 2-way Jet per bisection try */
 } or_knobs;
 
 typedef struct {

@@ -36,7 +36,8 @@ class Knobs(ctypes.Structure):
                 ("match_rounds", ctypes.c_int), ("rating_model", ctypes.c_void_p),
                 ("rating_fallback", ctypes.c_double), ("rating_levels", ctypes.c_int),
                 ("refinement", ctypes.c_int), ("jet_iters", ctypes.c_int), ("jet_patience", ctypes.c_int),
-                ("jet_c0", ctypes.c_int), ("jet_c", ctypes.c_int), ("ip_mode", ctypes.c_int)]
+                ("jet_c0", ctypes.c_int), ("jet_c", ctypes.c_int), ("ip_mode", ctypes.c_int),
+                ("ip_jet_iters", ctypes.c_int), ("ip_jet_patience", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
