@@ -73,6 +73,11 @@ struct SweepArgs {
     int all_fit;                        // singletons: every neighbour cluster fits (2 max c(v) < bound)
     int admit_all;                      // CLUSTER: every target takes all its proposers
                                         // (max c(v) (max degree + 1) < bound): no admission data
+    int fuse_apply;                     // singletons + all_fit + admit_all, no row above kWin:
+                                        // moves are applied in the sweep (nothing reads labels
+                                        // or cluster weights of others in that round)
+    int* label_w;                       // fuse_apply: labels, written by their own vertex
+    uint32_t* cw_w;                     // fuse_apply: cluster weights
     int stash;                          // host: sweep with lane_vertex's label stash
     unsigned long long* work;           // [0] vertices, [1] edges
     int* err;                           // set when an invariant breaks
@@ -420,9 +425,43 @@ template <int MODE, int NS, bool UNIT, bool STASH>
 __device__ int lane_vertex(const SweepArgs& a, int v, uint32_t* st, unsigned& wv, unsigned& we) {
     const int beg = a.xadj[v], end = a.xadj[v + 1];
     if (end - beg > kWin) return 2;
-    const uint32_t own = (uint32_t)a.lab[v];
+    // clustering round 0 (singletons): every label is its own vertex id
+    const uint32_t own = (MODE == CLUSTER && a.singletons) ? (uint32_t)v : (uint32_t)a.lab[v];
     const uint32_t cv = (uint32_t)a.vwgt[v];
     uint32_t cown = 0;
+    if (MODE == CLUSTER && a.singletons && UNIT && a.all_fit) {
+        // unit weights: every neighbour cluster has connection 1, so the best
+        // is the neighbour of smallest (tie hash, id) -- one 64-bit minimum
+        // per entry
+        uint64_t bk = ~0ull;
+        for (int e = beg; e < end; e += 4) {
+            int u[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) u[t] = e + t < end ? a.adjncy[e + t] : -1;
+            uint32_t h[4];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) h[t] = u[t] >= 0 ? a.tie[u[t]] : 0u;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                if (u[t] < 0) continue;
+                if ((uint32_t)u[t] == own) { cown += 1; continue; }
+                const uint64_t k = ((uint64_t)h[t] << 32) | (uint32_t)u[t];
+                bk = k < bk ? k : bk;
+            }
+        }
+        wv += 1;
+        we += (unsigned)(end - beg);
+        const uint32_t id = bk == ~0ull ? kEmpty : (uint32_t)bk;
+        if (a.fuse_apply) {
+            if (id == kEmpty || 1u <= cown) return 0;
+            a.label_w[v] = (int)id;
+            atomicSub(&a.cw_w[own], cv);
+            atomicAdd(&a.cw_w[id], cv);
+            return 0;
+        }
+        const uint64_t key = id == kEmpty ? 0ull : (1ull << 32);
+        return decide_emit<MODE>(a, v, own, cv, cown, key, id) ? 3 : 0;
+    }
     if (MODE == CLUSTER && a.singletons) {
         // label[u] == u and no target repeats: the connection to cluster u is
         // exactly w(v,u), so the best candidate is a running maximum; the
@@ -1071,9 +1110,15 @@ void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* la
             a.tie = tie;
             a.all_fit = 2ull * g.maxvw < (unsigned long long)a.bound ? 1 : 0;
         }
+        // unit weights, every target fitting and taking all its proposers and
+        // no row for the high-degree kernel: the sweep applies the moves itself
+        a.fuse_apply = (a.singletons && a.all_fit && a.admit_all && g.unit_weights && g.maxdeg <= kWin) ? 1 : 0;
+        a.label_w = label;
+        a.cw_w = cw;
         for (uint32_t s = 0; s < a.S; ++s) {
             a.s = s;
             launch_sweep<CLUSTER>(ctx, g, a, b, sweep_bytes(g, 1.0 / a.S));
+            if (a.fuse_apply) continue;
             PhaseScope ps(ctx, "lp_cluster_admit", 0);
             if (!a.admit_all) {
                 cluster_decide<<<admit_blocks(), kThreads, 0, st>>>(b.plist, b.hplist, a.hpcount, b.pt, cw, inc, minv,
