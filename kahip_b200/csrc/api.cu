@@ -182,6 +182,111 @@ Upload upload(Ctx& ctx, int n, const int* xadj, const int* adjncy, const int* ad
     return u;
 }
 
+// upload + the device check, overlapped: the copy stream brings xadj, the
+// node weights and then adjncy (and adjwgt) in kUploadChunks pieces of equal
+// entry counts; the work stream fills unit weights meanwhile and checks every
+// vertex range as soon as the pieces holding its rows have landed.  Throws
+// InvalidInput like check_uploaded.
+// Whether host memory p is page-locked (registered or cudaHostAlloc'd).
+bool is_pinned(const void* p) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+}
+
+constexpr int kUploadChunks = 8;
+
+Upload upload_checked(Ctx& ctx, int n, const int* xadj, const int* adjncy, const int* adjwgt, const int* vwgt,
+                      uint32_t* total_weight) {
+    Upload u;
+    const long long m = xadj[n];
+    cudaStream_t s = ctx.stream, cs = ctx.copies();
+    int* dx = ctx.hier.alloc<int>((size_t)n + 1);
+    int* da = ctx.hier.alloc<int>((size_t)std::max<long long>(m, 1));
+    int* dw = ctx.hier.alloc<int>((size_t)std::max<long long>(m, 1));
+    int* dv = ctx.hier.alloc<int>((size_t)std::max(n, 1));
+    u.part = ctx.hier.alloc<int>((size_t)std::max(n, 1));
+    u.g.n = n;
+    u.g.m = m;
+    u.g.xadj = dx;
+    u.g.adjncy = da;
+    u.g.adjwgt = dw;
+    u.g.vwgt = dv;
+    std::vector<cudaEvent_t> evs;
+    auto mark = [&](cudaStream_t st) {
+        cudaEvent_t e;
+        KB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        KB_CUDA(cudaEventRecord(e, st));
+        evs.push_back(e);
+        return e;
+    };
+    struct Free {
+        std::vector<cudaEvent_t>& e;
+        ~Free() { for (auto x : e) cudaEventDestroy(x); }
+    } free_evs{evs};
+    // the copy stream starts after everything queued on the work stream
+    KB_CUDA(cudaStreamWaitEvent(cs, mark(s), 0));
+    KB_CUDA(cudaMemcpyAsync(dx, xadj, sizeof(int) * ((size_t)n + 1), cudaMemcpyHostToDevice, cs));
+    if (vwgt && n) KB_CUDA(cudaMemcpyAsync(dv, vwgt, sizeof(int) * (size_t)n, cudaMemcpyHostToDevice, cs));
+    const cudaEvent_t e_rows = mark(cs);
+    const int C = m > 0 ? kUploadChunks : 0;
+    std::vector<cudaEvent_t> e_chunk((size_t)C);
+    auto chunk_lo = [&](int c) { return m * c / std::max(C, 1); };
+    for (int c = 0; c < C; ++c) {
+        const long long lo = chunk_lo(c), hi = chunk_lo(c + 1);
+        if (hi > lo) {
+            KB_CUDA(cudaMemcpyAsync(da + lo, adjncy + lo, sizeof(int) * (size_t)(hi - lo), cudaMemcpyHostToDevice, cs));
+            if (adjwgt)
+                KB_CUDA(cudaMemcpyAsync(dw + lo, adjwgt + lo, sizeof(int) * (size_t)(hi - lo), cudaMemcpyHostToDevice,
+                                        cs));
+        }
+        e_chunk[(size_t)c] = mark(cs);
+    }
+    // work stream: unit weights, then the checks behind the pieces
+    if (!adjwgt) fill_i32(dw, m, 1, s);
+    if (!vwgt) fill_i32(dv, n, 1, s);
+    check_graph_begin(ctx);
+    KB_CUDA(cudaStreamWaitEvent(s, e_rows, 0));
+    if (C == 0) {
+        if (n > 0) check_graph_range(ctx, u.g, 0, n, !adjwgt);
+    } else {
+        // vertex ranges of about m / C entries each (host xadj; a broken xadj
+        // is caught by the check itself, and then every piece has landed)
+        int v0 = 0;
+        for (int c = 0; c < C; ++c) {
+            int v1 = n;
+            if (c + 1 < C) {
+                const long long target = chunk_lo(c + 1);
+                v1 = (int)(std::lower_bound(xadj, xadj + n + 1, (int)std::min<long long>(target, INT_MAX)) - xadj);
+                v1 = std::max(v0, std::min(v1, n));
+            }
+            // the pieces that hold entries [xadj[v0], xadj[v1]) (all of them
+            // if those values are out of order or range)
+            const long long e1 = xadj[v1];
+            int need = C - 1;
+            if (e1 >= 0 && e1 <= m && xadj[v0] <= e1) {
+                need = 0;
+                while (need + 1 < C && chunk_lo(need + 1) < e1) ++need;
+            }
+            KB_CUDA(cudaStreamWaitEvent(s, e_chunk[(size_t)need], 0));
+            if (v1 > v0 || (c == 0 && n == 0)) check_graph_range(ctx, u.g, v0, v1, !adjwgt);
+            v0 = v1;
+        }
+    }
+    KB_CUDA(cudaStreamWaitEvent(s, mark(cs), 0));
+    const int flags = check_graph_end(ctx, total_weight);
+    u.g.unit_weights = (flags & 16) == 0;
+    u.g.rows_sorted = (flags & 32) ? 0 : 1;
+    if (flags & 1) throw InvalidInput("adjncy entry out of range");
+    if (flags & 2) throw InvalidInput("negative edge weight");
+    if (flags & 4) throw InvalidInput("negative node weight");
+    if (flags & 8) throw InvalidInput("xadj does not start at 0 or is not monotone");
+    return u;
+}
+
 void fill_stats_families(Ctx& ctx, kb200_stats* st) {
     if (!st) return;
     ctx.collect();
@@ -253,9 +358,8 @@ int run_host_in(Ctx& ctx, int n, const int* vwgt, const int* xadj, const int* ad
             reserve_for(ctx, n, m, true, (attempt == 0 ? 1.0 : 2.0 * attempt) * (comb ? 1.5 : 1.0));
             begin_stats(ctx, st);
             auto th = clk::now();
-            Upload up = upload(ctx, n, xadj, adjncy, adjcwgt, vwgt);
             uint32_t W = 0;
-            check_uploaded(ctx, up.g, &W);
+            Upload up = upload_checked(ctx, n, xadj, adjncy, adjcwgt, vwgt, &W);
             if (derive_on_device) derive_knobs_total(n, W, kn_in.k, kn_in.imbalance, kn_in.seed, kn_in.mode, kn);
             int* dpar = nullptr;
             if (comb) {
@@ -270,10 +374,15 @@ int run_host_in(Ctx& ctx, int n, const int* vwgt, const int* xadj, const int* ad
             }
             double ms_h2d = ms_since(th);
             long long cut = 0;
+            // the result straight from the last refinement into a page-locked
+            // caller buffer (overlapped with the final cut); else copied here
+            bool host_done = false;
+            int* early = (!comb && is_pinned(part)) ? part : nullptr;
             int r = comb ? combine(ctx, up.g, kn, dpar, dpar + n, up.part, &cut, st)
-                         : partition(ctx, up.g, kn, up.part, &cut, st);
+                         : partition(ctx, up.g, kn, up.part, &cut, st, early, &host_done);
             auto td = clk::now();
-            if (n) KB_CUDA(cudaMemcpyAsync(part, up.part, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, ctx.stream));
+            if (n && !host_done)
+                KB_CUDA(cudaMemcpyAsync(part, up.part, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, ctx.stream));
             KB_CUDA(cudaStreamSynchronize(ctx.stream));
             *edgecut = cut;
             if (st) {

@@ -73,6 +73,8 @@ struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaStream_t copy_stream = nullptr;  // host <-> device copies beside the work (created on first use)
+    cudaStream_t copies();
     Arena hier;     // graph hierarchy (lives for the whole call)
     Arena scratch;  // per-phase scratch (mark/release)
     // small device scalars (counters, flags) and their pinned host mirror

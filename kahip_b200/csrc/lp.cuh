@@ -64,6 +64,12 @@ void degree_stats(Ctx& ctx, DevGraph& g);
 // row does not list its targets in strictly increasing order (not an error).  Also returns the node weight sum (32-bit, as the reference's
 // NodeWeight accumulates it).  Synchronises the stream.
 int check_graph(Ctx& ctx, const DevGraph& g, uint32_t* total_weight = nullptr);
+// The same check in parts: begin (clears the flags), any number of vertex
+// ranges (unit_known: every edge weight is 1, adjwgt is not read), end
+// (synchronises and returns the flags).
+void check_graph_begin(Ctx& ctx);
+void check_graph_range(Ctx& ctx, const DevGraph& g, int v_lo, int v_hi, bool unit_known);
+int check_graph_end(Ctx& ctx, uint32_t* total_weight);
 
 // true if every row lists its targets in strictly increasing order
 // (synchronises the stream)

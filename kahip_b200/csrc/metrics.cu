@@ -142,14 +142,15 @@ __global__ void init_labels_kernel(int n, const int* __restrict__ vwgt, int* lab
 // reference's NodeWeight does).
 __global__ void check_graph_kernel(int n, long long m, const int* __restrict__ xadj,
                                    const int* __restrict__ adjncy, const int* __restrict__ adjwgt,
-                                   const int* __restrict__ vwgt, int* flags, unsigned* wsum) {
+                                   const int* __restrict__ vwgt, int* flags, unsigned* wsum, int v_lo, int v_hi) {
     int f = 0;
     unsigned w = 0;
     const int lane = threadIdx.x & 31;
     const long long warps = (long long)gridDim.x * (blockDim.x / 32);
-    for (long long g0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32 * 32; g0 < n; g0 += warps * 32) {
+    for (long long g0 = v_lo + ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32 * 32; g0 < v_hi;
+         g0 += warps * 32) {
         const long long v = g0 + lane;
-        const bool in = v < n;
+        const bool in = v < v_hi;
         long long x0 = 0, x1 = 0;
         if (in) {
             x0 = xadj[v];
@@ -163,7 +164,7 @@ __global__ void check_graph_kernel(int n, long long m, const int* __restrict__ x
             f |= 8;
             continue;
         }
-        const int last = (int)min(31LL, (long long)n - 1 - g0);
+        const int last = (int)min(31LL, (long long)v_hi - 1 - g0);
         const long long lo = __shfl_sync(0xffffffffu, x0, 0), hi = __shfl_sync(0xffffffffu, x1, last);
         int carry = 0;
         // four chunks of 32 entries in flight per step (latency-bound otherwise)
@@ -176,7 +177,7 @@ __global__ void check_graph_kernel(int n, long long m, const int* __restrict__ x
                 ww[c] = 1;
                 if (e < hi) {
                     tt[c] = adjncy[e];
-                    ww[c] = adjwgt[e];
+                    if (adjwgt) ww[c] = adjwgt[e];  // null: unit weights, known on the host
                 }
             }
 #pragma unroll
@@ -200,7 +201,7 @@ __global__ void check_graph_kernel(int n, long long m, const int* __restrict__ x
             }
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0 && xadj[0] != 0) f |= 8;
+    if (v_lo == 0 && blockIdx.x == 0 && threadIdx.x == 0 && xadj[0] != 0) f |= 8;
     f = __reduce_or_sync(0xffffffffu, f);
     w = __reduce_add_sync(0xffffffffu, w);
     if ((threadIdx.x & 31) == 0) {
@@ -274,18 +275,30 @@ int max_degree(Ctx& ctx, const DevGraph& g) {
     return h.maxdeg;
 }
 
-int check_graph(Ctx& ctx, const DevGraph& g, uint32_t* total_weight) {
-    int* d = ctx.dscalars + 2;  // [2] flags, [3] node weight sum
-    KB_CUDA(cudaMemsetAsync(d, 0, 2 * sizeof(int), ctx.stream));
-    if (g.m > 0 || g.n > 0) {
-        check_graph_kernel<<<grid_for(g.n, 256), 256, 0, ctx.stream>>>(
-            g.n, g.m, g.xadj, g.adjncy, g.adjwgt, g.vwgt, d, reinterpret_cast<unsigned*>(d + 1));
-        KB_LAUNCH();
-    }
-    KB_CUDA(cudaMemcpyAsync(ctx.pinned + 2, d, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+void check_graph_begin(Ctx& ctx) {
+    KB_CUDA(cudaMemsetAsync(ctx.dscalars + 2, 0, 2 * sizeof(int), ctx.stream));  // [2] flags, [3] weight sum
+}
+
+void check_graph_range(Ctx& ctx, const DevGraph& g, int v_lo, int v_hi, bool unit_known) {
+    if (v_hi <= v_lo && !(v_lo == 0 && g.n == 0)) return;
+    int* d = ctx.dscalars + 2;
+    check_graph_kernel<<<grid_for((long long)std::max(v_hi - v_lo, 1), 256), 256, 0, ctx.stream>>>(
+        g.n, g.m, g.xadj, g.adjncy, unit_known ? nullptr : g.adjwgt, g.vwgt, d, reinterpret_cast<unsigned*>(d + 1),
+        v_lo, v_hi);
+    KB_LAUNCH();
+}
+
+int check_graph_end(Ctx& ctx, uint32_t* total_weight) {
+    KB_CUDA(cudaMemcpyAsync(ctx.pinned + 2, ctx.dscalars + 2, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
     KB_CUDA(cudaStreamSynchronize(ctx.stream));
     if (total_weight) *total_weight = ctx.pinned[3];
     return (int)ctx.pinned[2];
+}
+
+int check_graph(Ctx& ctx, const DevGraph& g, uint32_t* total_weight) {
+    check_graph_begin(ctx);
+    if (g.m > 0 || g.n > 0) check_graph_range(ctx, g, 0, g.n, false);
+    return check_graph_end(ctx, total_weight);
 }
 
 bool rows_strictly_increasing(Ctx& ctx, const DevGraph& g) {

@@ -29,6 +29,7 @@ Ctx::~Ctx() {
     for (auto& p : pending) { cudaEventDestroy(p.a); cudaEventDestroy(p.b); }
     for (auto e : ev_free) cudaEventDestroy(e);
     if (origin) cudaEventDestroy(origin);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
     if (pinned) cudaFreeHost(pinned);
     if (dscalars) cudaFree(dscalars);
     hier.free_all();
@@ -67,6 +68,11 @@ cudaEvent_t Ctx::ev() {
     cudaEvent_t e;
     KB_CUDA(cudaEventCreate(&e));
     return e;
+}
+
+cudaStream_t Ctx::copies() {
+    if (!copy_stream) KB_CUDA(cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking));
+    return copy_stream;
 }
 
 void Ctx::begin(int phase, cudaEvent_t& a) {
@@ -171,7 +177,8 @@ void reserve_for(Ctx& ctx, int n, long long m, bool copy_input, double factor) {
 // one; the coarsening then runs on the edges inside both parents' blocks and
 // the coarsest graph takes p1 instead of an initial partitioning.
 static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_part, long long* edgecut,
-                          kb200_stats* st, const int* p1 = nullptr, const int* p2 = nullptr) {
+                          kb200_stats* st, const int* p1 = nullptr, const int* p2 = nullptr,
+                          int* host_part = nullptr) {
     const int k = kn.k;
     const bool collect = st && st->collect_level_cuts;
     const bool combine = p1 != nullptr;
@@ -298,6 +305,16 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
         bool ok = balance(ctx, g, kn, l, bound, lv[l].part, bw);
         if (kn.refinement == 1) jet_refine(ctx, g, kn, l, bound, lv[l].part, bw);
         else lp_refine(ctx, g, kn, l, bound, lv[l].part, bw);
+        if (l == 0 && host_part && g.n) {
+            // the final partition goes to the host on the copy stream while the
+            // cut and block weights are computed
+            cudaEvent_t done = ctx.ev();
+            KB_CUDA(cudaEventRecord(done, s));
+            KB_CUDA(cudaStreamWaitEvent(ctx.copies(), done, 0));
+            KB_CUDA(cudaMemcpyAsync(host_part, lv[0].part, sizeof(int) * (size_t)g.n, cudaMemcpyDeviceToHost,
+                                    ctx.copies()));
+            ctx.ev_free.push_back(done);
+        }
         if (l == 0) balanced = ok;
         if (collect || l == 0) {
             long long c = read_cut(ctx, g, lv[l].part, k, bw);
@@ -307,6 +324,7 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
         }
     }
     KB_CUDA(cudaStreamSynchronize(s));
+    if (host_part) KB_CUDA(cudaStreamSynchronize(ctx.copies()));
     double ms_uncoarsen = ms_since(t2);
 
     {
@@ -371,10 +389,14 @@ int combine(Ctx& ctx, const DevGraph& g0, const Knobs& kn, const int* pa, const 
 }
 
 int partition(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_part, long long* edgecut,
-              kb200_stats* st) {
+              kb200_stats* st, int* host_part, bool* host_done) {
     if (st) st->rating_fallback_used = 0;
-    if (!(kn.coarsening == 2 && kn.rating_model && kn.rating_fallback > 0))
-        return partition_once(ctx, g0, kn, d_part, edgecut, st);
+    if (host_done) *host_done = false;
+    if (!(kn.coarsening == 2 && kn.rating_model && kn.rating_fallback > 0)) {
+        const int r = partition_once(ctx, g0, kn, d_part, edgecut, st, nullptr, nullptr, host_part);
+        if (host_done) *host_done = host_part != nullptr;
+        return r;
+    }
     // learned rating with a guard: the expansion*^2 matching runs too, and
     // its partition is kept when the learned one cuts more than
     // rating_fallback times as much
