@@ -19,11 +19,15 @@
 #include "lp.cuh"
 #include "prims.cuh"
 
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <climits>
 #include <vector>
 
 namespace kb {
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -53,7 +57,9 @@ struct SweepArgs {
     const int* __restrict__ vwgt;
     const int* __restrict__ lab;        // cluster id or block id per vertex
     const uint32_t* __restrict__ lw;    // weight per label (cluster / block)
-    const uint8_t* __restrict__ active; // REFINE: vertex may move this round
+    const uint8_t* __restrict__ active; // REFINE: vertex may move this round (null: every vertex)
+    const int* vlist;                   // REFINE: sweep only these vertices (null: ids 0 .. n-1)
+    const unsigned* vcount;             // their number
     uint32_t bound;
     uint32_t S, s;                      // sub-rounds, this sub-round
     uint64_t ks_sub, ks_tie, ks_prio;
@@ -204,7 +210,7 @@ __device__ __forceinline__ void append_striped(bool pred, int v, const SList& L)
 template <int MODE>
 __device__ __forceinline__ bool member(const SweepArgs& a, int v) {
     if (MODE == BALANCE) return a.lw[a.lab[v]] > a.bound;
-    if (MODE == REFINE && !a.active[v]) return false;
+    if (MODE == REFINE && a.active && !a.active[v]) return false;
     return hash_range(hash32(a.ks_sub, (uint32_t)v), a.S) == a.s;
 }
 
@@ -625,7 +631,9 @@ __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
     // per-lane work counts (32 bits: a lane never sees more than m < 2^31 entries)
     unsigned wv = 0, we = 0, wo = 0;
     const long long span = 32LL * kSpan;
-    const long long ntasks = ((long long)a.n + span - 1) / span;
+    // the swept items: vertex ids 0 .. n-1, or the entries of vlist
+    const long long nitems = a.vlist ? (long long)*a.vcount : (long long)a.n;
+    const long long ntasks = (nitems + span - 1) / span;
     const long long warp = ((long long)blockIdx.x * kThreads + threadIdx.x) / 32;
     const long long nwarps = (long long)gridDim.x * kThreads / 32;
     auto overflow_pass = [&]() {
@@ -653,10 +661,11 @@ __global__ void __launch_bounds__(kThreads, 4) lane_kernel(SweepArgs a) {
 #pragma unroll
         for (int c = 0; c < kSpan; ++c) {
             const long long vv = base + c * 32 + lane;
-            const bool valid = vv < a.n;
-            const bool mem = valid && member<MODE>(a, (int)vv);
+            const bool valid = vv < nitems;
+            const int v = valid ? (a.vlist ? a.vlist[vv] : (int)vv) : 0;
+            const bool mem = valid && member<MODE>(a, v);
             const unsigned m = __ballot_sync(0xffffffffu, mem);
-            if (mem) q[qn + __popc(m & lanemask_lt())] = (int)vv;
+            if (mem) q[qn + __popc(m & lanemask_lt())] = v;
             qn += __popc(m);
         }
         __syncwarp();
@@ -839,9 +848,21 @@ __global__ void class_decide(SList pl, const int* hpl, const unsigned* hpc, int*
     }
 }
 
+// The vertices a refinement round sweeps next: the neighbours of the ones it
+// moves, as flags (a round that moves many vertices) or as a list in which
+// each is listed once (the first thread to raise its stamp to this round's
+// tag appends it; appends are aggregated over the coalesced lanes).
+struct NextActive {
+    uint8_t* flags;   // non-null: flags[u] = 1
+    uint32_t* stamp;  // per vertex: the tag of the last round that listed it
+    uint32_t tag;     // this round's tag, larger than every earlier one
+    int* list;        // null (and no flags): nothing is kept
+    unsigned* count;
+};
+
 __global__ void class_apply(SList pl, const int* hpl, const unsigned* hpc, const int* pt, const int* pc,
                             const int* xadj, const int* adjncy, const int* vwgt, int* part, uint32_t* bw,
-                            uint32_t* H, int* minvP, int P, uint8_t* next_active, unsigned* moved) {
+                            uint32_t* H, int* minvP, int P, NextActive na, unsigned* moved) {
     unsigned mv = 0;
     FOR_EACH_PROPOSAL(pl, hpl, hpc, v) {
         int t = pt[v];
@@ -857,8 +878,19 @@ __global__ void class_apply(SList pl, const int* hpl, const unsigned* hpc, const
         atomicAdd(&bw[t], cv);
         part[v] = t;
         ++mv;
-        if (next_active)
-            for (int e = xadj[v]; e < xadj[v + 1]; ++e) next_active[adjncy[e]] = 1;
+        if (na.flags)
+            for (int e = xadj[v]; e < xadj[v + 1]; ++e) na.flags[adjncy[e]] = 1;
+        else if (na.list)
+            for (int e = xadj[v]; e < xadj[v + 1]; ++e) {
+                const int u = adjncy[e];
+                if (atomicMax(&na.stamp[u], na.tag) < na.tag) {
+                    cg::coalesced_group g = cg::coalesced_threads();
+                    unsigned at = 0;
+                    if (g.thread_rank() == 0) at = atomicAdd(na.count, g.size());
+                    at = g.shfl(at, 0);
+                    na.list[at + g.thread_rank()] = u;
+                }
+            }
     }
     mv = __reduce_add_sync(0xffffffffu, mv);
     if ((threadIdx.x & 31) == 0 && mv) atomicAdd(moved, mv);
@@ -1143,12 +1175,18 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
     const int k = kn.k, P = kn.ref_classes;
     uint32_t* H = ctx.scratch.alloc<uint32_t>((size_t)k * P);
     int* minvP = ctx.scratch.alloc<int>((size_t)k * P);
-    uint8_t* act = ctx.scratch.alloc<uint8_t>((size_t)g.n);
-    uint8_t* nact = ctx.scratch.alloc<uint8_t>((size_t)g.n);
+    // round 0 sweeps every vertex; round r > 0 the neighbours of the vertices
+    // round r - 1 moved: as flags over all ids after round 0 (which moves
+    // many), as a list after later rounds (no pass over all ids)
+    uint8_t* flags = ctx.scratch.alloc<uint8_t>((size_t)g.n);
+    uint32_t* stamp = ctx.scratch.alloc<uint32_t>((size_t)g.n);
+    int* alist[2] = {ctx.scratch.alloc<int>((size_t)g.n), ctx.scratch.alloc<int>((size_t)g.n)};
+    unsigned* acount = ctx.scratch.alloc<unsigned>(2);
     SweepBuffers b = make_buffers(ctx, g);
     fill_u32(H, (long long)k * P, 0u, st);
     fill_i32(minvP, (long long)k * P, INT_MAX, st);
-    fill_u8(act, g.n, 1, st);
+    fill_u32(stamp, g.n, 0u, st);
+    fill_u8(flags, g.n, 0, st);
     SweepArgs a = base_args(g, b);
     a.lab = part;
     a.lw = bw;
@@ -1160,11 +1198,15 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
     a.stash = 1;  // most neighbours lie in the vertex's own block
     unsigned* moved = b.counters + kCntMoved;
     for (int r = 0; r < kn.ref_rounds; ++r) {
-        a.active = act;
+        a.active = r == 1 ? flags : nullptr;
+        a.vlist = r >= 2 ? alist[r & 1] : nullptr;
+        a.vcount = acount + (r & 1);
+        const NextActive na{r == 0 ? flags : nullptr, stamp, (uint32_t)r + 1u, alist[(r + 1) & 1],
+                            acount + ((r + 1) & 1)};
         a.ks_sub = stream_key(kn.seed, TAG_RSUB, level, r);
         a.ks_tie = stream_key(kn.seed, TAG_RTIE, level, r);
         a.ks_prio = stream_key(kn.seed, TAG_RPRIO, level, r);
-        fill_u8(nact, g.n, 0, st);
+        KB_CUDA(cudaMemsetAsync(na.count, 0, sizeof(unsigned), st));
         KB_CUDA(cudaMemsetAsync(moved, 0, sizeof(unsigned), st));
         for (uint32_t s = 0; s < a.S; ++s) {
             a.s = s;
@@ -1174,10 +1216,9 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
                                                               H, minvP, P, bound, 1);
             KB_LAUNCH();
             class_apply<<<admit_blocks(), kThreads, 0, st>>>(b.plist, b.hplist, a.hpcount, b.pt, b.pc, g.xadj,
-                                                             g.adjncy, g.vwgt, part, bw, H, minvP, P, nact, moved);
+                                                             g.adjncy, g.vwgt, part, bw, H, minvP, P, na, moved);
             KB_LAUNCH();
         }
-        std::swap(act, nact);
         // (reading the count one round late, with the next round already
         // queued, measured slower: the queued round after the last one costs
         // more than the synchronisation it hides)
@@ -1245,7 +1286,7 @@ bool balance(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t b
                                                           minvP, P, bound, 0);
         KB_LAUNCH();
         class_apply<<<admit_blocks(), kThreads, 0, st>>>(b.plist, b.hplist, a.hpcount, b.pt, b.pc, g.xadj, g.adjncy,
-                                                         g.vwgt, part, bw, H, minvP, P, nullptr, b.counters + kCntMoved);
+                                                         g.vwgt, part, bw, H, minvP, P, NextActive{}, b.counters + kCntMoved);
         KB_LAUNCH();
     }
     if (!ok) {
