@@ -172,7 +172,14 @@ __device__ __forceinline__ void for_rows(int n_o, const int* lbeg, const int* ld
         for (int i = wid; i < n_o; i += (int)(blockDim.x >> 5)) {
             Acc2 s{0, 0};
             const int b = lbeg[i], d = ldeg[i];
-            for (int t = lane; t < d; t += 32) entry(i, b + t, s);
+            int t = lane;
+            for (; t + 96 < d; t += 128) {  // four entries per lane in flight
+                entry(i, b + t, s);
+                entry(i, b + t + 32, s);
+                entry(i, b + t + 64, s);
+                entry(i, b + t + 96, s);
+            }
+            for (; t < d; t += 32) entry(i, b + t, s);
             s.a = warp_sum_ll(s.a);
             s.b = warp_sum_ll(s.b);
             if (lane == 0) row(i, s);
@@ -726,8 +733,13 @@ __global__ void __launch_bounds__(kTryMaxBT) ip_extract(IpArgs a) {
     for (int i = wid; i < n_o; i += (int)(blockDim.x >> 5)) {
         const int v = orig[i];
         if (a.xadj[v + 1] - a.xadj[v] <= 32) continue;
-        int d = 0;
-        for (int e = a.xadj[v] + lane; e < a.xadj[v + 1]; e += 32) d += part[a.adjncy[e]] == o;
+        const int e1 = a.xadj[v + 1];
+        int d = 0, e = a.xadj[v] + lane;
+        for (; e + 96 < e1; e += 128) {  // four gathers per lane in flight
+            const int u0 = a.adjncy[e], u1 = a.adjncy[e + 32], u2 = a.adjncy[e + 64], u3 = a.adjncy[e + 96];
+            d += (part[u0] == o) + (part[u1] == o) + (part[u2] == o) + (part[u3] == o);
+        }
+        for (; e < e1; e += 32) d += part[a.adjncy[e]] == o;
         d = __reduce_add_sync(0xffffffffu, d);
         if (lane == 0) ldeg[i] = d;
     }
@@ -775,16 +787,29 @@ __global__ void __launch_bounds__(kTryMaxBT) ip_extract(IpArgs a) {
         const int v = orig[i];
         if (a.xadj[v + 1] - a.xadj[v] <= 32) continue;
         int w = lbeg[i];
-        for (int e0 = a.xadj[v]; e0 < a.xadj[v + 1]; e0 += 32) {
-            const int e = e0 + lane;
-            const bool in = e < a.xadj[v + 1] && part[a.adjncy[e]] == o;
-            const unsigned m = __ballot_sync(0xffffffffu, in);
-            if (in) {
-                const int p = w + __popc(m & ((1u << lane) - 1u));
-                ladj[p] = lid[a.adjncy[e]];
-                lw[p] = a.adjwgt[e];
+        const int e1 = a.xadj[v + 1];
+        // four 32-entry chunks loaded together, then written in order
+        for (int c0 = a.xadj[v]; c0 < e1; c0 += 128) {
+            int u[4], pu[4], wt[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int e = c0 + 32 * q + lane;
+                u[q] = e < e1 ? a.adjncy[e] : -1;
+                wt[q] = e < e1 ? a.adjwgt[e] : 0;
             }
-            w += __popc(m);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) pu[q] = u[q] >= 0 ? part[u[q]] : -1;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const bool in = u[q] >= 0 && pu[q] == o;
+                const unsigned m = __ballot_sync(0xffffffffu, in);
+                if (in) {
+                    const int p = w + __popc(m & ((1u << lane) - 1u));
+                    ladj[p] = lid[u[q]];
+                    lw[p] = wt[q];
+                }
+                w += __popc(m);
+            }
         }
     }
 }
@@ -1134,7 +1159,8 @@ void initial_partition_device(Ctx& ctx, const DevGraph& c, const Knobs& kn, int*
             const long long state = n_est * kIpSmemPerNode + 512;
             const long long want = state + 8 * m_est <= kIpSmem ? state + 8 * m_est : state;
             a.smem_bytes = (int)std::min<long long>(kIpSmem, (want + 1023) & ~1023LL);
-            if (n_est > 8192) {  // large subgraphs: a whole SM's threads per try
+            // large or dense subgraphs: a whole SM's threads per try
+            if (n_est > 8192 || (m_est >= 65536 && m_est >= (long long)kDenseRows * n_est)) {
                 ip_try<1024><<<a.nsplit * reps * tries, 1024, a.smem_bytes, st>>>(a);
             } else {
                 const int bt = n_est > 2048 ? kTryMaxBT : 256;

@@ -858,7 +858,32 @@ struct NextActive {
     uint32_t tag;     // this round's tag, larger than every earlier one
     int* list;        // null (and no flags): nothing is kept
     unsigned* count;
+    int* hubs;        // non-null: moved vertices of degree > kHubMark are listed
+    unsigned* nhubs;  // here instead, for mark_hubs (a warp per vertex)
 };
+
+// (a thread marks at most this many neighbours itself: in list mode every
+// mark waits for its atomic's result)
+constexpr int kHubMark = 32;
+
+// Marks (or lists) the neighbours of one moved vertex, row entries
+// [e0, e1), by the threads t, t + nt, ...
+__device__ __forceinline__ void mark_row(const NextActive& na, const int* adjncy, int e0, int e1, int t, int nt) {
+    if (na.flags) {
+        for (int e = e0 + t; e < e1; e += nt) na.flags[adjncy[e]] = 1;
+    } else if (na.list) {
+        for (int e = e0 + t; e < e1; e += nt) {
+            const int u = adjncy[e];
+            if (atomicMax(&na.stamp[u], na.tag) < na.tag) {
+                cg::coalesced_group g = cg::coalesced_threads();
+                unsigned at = 0;
+                if (g.thread_rank() == 0) at = atomicAdd(na.count, g.size());
+                at = g.shfl(at, 0);
+                na.list[at + g.thread_rank()] = u;
+            }
+        }
+    }
+}
 
 __global__ void class_apply(SList pl, const int* hpl, const unsigned* hpc, const int* pt, const int* pc,
                             const int* xadj, const int* adjncy, const int* vwgt, int* part, uint32_t* bw,
@@ -878,22 +903,25 @@ __global__ void class_apply(SList pl, const int* hpl, const unsigned* hpc, const
         atomicAdd(&bw[t], cv);
         part[v] = t;
         ++mv;
-        if (na.flags)
-            for (int e = xadj[v]; e < xadj[v + 1]; ++e) na.flags[adjncy[e]] = 1;
-        else if (na.list)
-            for (int e = xadj[v]; e < xadj[v + 1]; ++e) {
-                const int u = adjncy[e];
-                if (atomicMax(&na.stamp[u], na.tag) < na.tag) {
-                    cg::coalesced_group g = cg::coalesced_threads();
-                    unsigned at = 0;
-                    if (g.thread_rank() == 0) at = atomicAdd(na.count, g.size());
-                    at = g.shfl(at, 0);
-                    na.list[at + g.thread_rank()] = u;
-                }
-            }
+        if (!na.flags && !na.list) continue;
+        // a longer row is marked by a whole warp later (mark_hubs), not by
+        // this one thread
+        const int e0 = xadj[v], e1 = xadj[v + 1];
+        if (na.hubs && e1 - e0 > kHubMark) na.hubs[atomicAdd(na.nhubs, 1u)] = v;
+        else mark_row(na, adjncy, e0, e1, 0, 1);
     }
     mv = __reduce_add_sync(0xffffffffu, mv);
     if ((threadIdx.x & 31) == 0 && mv) atomicAdd(moved, mv);
+}
+
+// the neighbours of the listed moved vertices with long rows, a warp each
+__global__ void mark_hubs(NextActive na, const int* xadj, const int* adjncy) {
+    const unsigned n = *na.nhubs;
+    const unsigned w = (blockIdx.x * blockDim.x + threadIdx.x) / 32, nw = gridDim.x * blockDim.x / 32;
+    for (unsigned i = w; i < n; i += nw) {
+        const int v = na.hubs[i];
+        mark_row(na, adjncy, xadj[v], xadj[v + 1], (int)(threadIdx.x & 31), 32);
+    }
 }
 
 // Balance: per overloaded block, the release threshold class.
@@ -1168,7 +1196,7 @@ void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* la
 // --------------------------------------------------------------- refinement
 
 void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t bound, int* part,
-               uint32_t* bw) {
+               uint32_t* bw, const uint8_t* active0) {
     if (g.n == 0) return;
     const size_t mk = ctx.scratch.mark();
     cudaStream_t st = ctx.stream;
@@ -1182,6 +1210,11 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
     uint32_t* stamp = ctx.scratch.alloc<uint32_t>((size_t)g.n);
     int* alist[2] = {ctx.scratch.alloc<int>((size_t)g.n), ctx.scratch.alloc<int>((size_t)g.n)};
     unsigned* acount = ctx.scratch.alloc<unsigned>(2);
+    // moved vertices of degree > kHubMark mark their neighbours a warp each
+    // (levels with rows of more than 128 entries; elsewhere the few such
+    // rows cost less than the extra launches)
+    int* hubs = g.maxdeg > 128 ? ctx.scratch.alloc<int>((size_t)g.n) : nullptr;
+    unsigned* nhubs = hubs ? ctx.scratch.alloc<unsigned>(1) : nullptr;
     SweepBuffers b = make_buffers(ctx, g);
     fill_u32(H, (long long)k * P, 0u, st);
     fill_i32(minvP, (long long)k * P, INT_MAX, st);
@@ -1198,11 +1231,11 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
     a.stash = 1;  // most neighbours lie in the vertex's own block
     unsigned* moved = b.counters + kCntMoved;
     for (int r = 0; r < kn.ref_rounds; ++r) {
-        a.active = r == 1 ? flags : nullptr;
+        a.active = r == 0 ? active0 : r == 1 ? flags : nullptr;
         a.vlist = r >= 2 ? alist[r & 1] : nullptr;
         a.vcount = acount + (r & 1);
         const NextActive na{r == 0 ? flags : nullptr, stamp, (uint32_t)r + 1u, alist[(r + 1) & 1],
-                            acount + ((r + 1) & 1)};
+                            acount + ((r + 1) & 1), hubs, nhubs};
         a.ks_sub = stream_key(kn.seed, TAG_RSUB, level, r);
         a.ks_tie = stream_key(kn.seed, TAG_RTIE, level, r);
         a.ks_prio = stream_key(kn.seed, TAG_RPRIO, level, r);
@@ -1215,9 +1248,14 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
             class_decide<<<admit_blocks(), kThreads, 0, st>>>(b.plist, b.hplist, a.hpcount, b.pt, b.pc, g.vwgt, bw,
                                                               H, minvP, P, bound, 1);
             KB_LAUNCH();
+            if (hubs) KB_CUDA(cudaMemsetAsync(nhubs, 0, sizeof(unsigned), st));
             class_apply<<<admit_blocks(), kThreads, 0, st>>>(b.plist, b.hplist, a.hpcount, b.pt, b.pc, g.xadj,
                                                              g.adjncy, g.vwgt, part, bw, H, minvP, P, na, moved);
             KB_LAUNCH();
+            if (hubs) {
+                mark_hubs<<<4 * kNumSMs, kThreads, 0, st>>>(na, g.xadj, g.adjncy);
+                KB_LAUNCH();
+            }
         }
         // (reading the count one round late, with the next round already
         // queued, measured slower: the queued round after the last one costs
@@ -1232,7 +1270,8 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
 // ------------------------------------------------------------------ balance
 
 bool balance(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t bound, int* part,
-             uint32_t* bw, const int* skip) {
+             uint32_t* bw, const int* skip, bool* moved) {
+    if (moved) *moved = false;
     const size_t mk = ctx.scratch.mark();
     cudaStream_t st = ctx.stream;
     const int k = kn.k, P = kn.ref_classes;
@@ -1247,6 +1286,7 @@ bool balance(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t b
         ctx.scratch.release(mk);
         return true;
     }
+    if (moved) *moved = true;
     uint32_t* H = ctx.scratch.alloc<uint32_t>((size_t)k * P);
     int* minvP = ctx.scratch.alloc<int>((size_t)k * P);
     uint32_t* HS = ctx.scratch.alloc<uint32_t>((size_t)k * kBalClasses);

@@ -35,22 +35,30 @@ struct SweepWork {
 void lp_cluster(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, int* label);
 
 // LP refinement at one level; part[n] in/out, bw[k] in/out (device).
+// active0 (device, optional): the vertices the first round sweeps (flags);
+// it must hold every vertex with a neighbour in another block -- the others
+// cannot propose a move, so leaving them out changes nothing.  Null: all.
 void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t bound, int* part,
-               uint32_t* bw);
+               uint32_t* bw, const uint8_t* active0 = nullptr);
 
 // Exact balance repair; returns true if every block ends <= bound.  skip
 // (device, optional): when *skip != 0 the call does nothing (a caller whose
-// own loop already ended on the device).
+// own loop already ended on the device).  *moved (optional) tells whether
+// the repair ran (and may have moved vertices).
 bool balance(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t bound, int* part,
-             uint32_t* bw, const int* skip = nullptr);
+             uint32_t* bw, const int* skip = nullptr, bool* moved = nullptr);
 
 // Block weights (bw[k] zeroed and filled) and, when cut != nullptr, the edge
 // cut (device uint64, sum over directed entries / 2 applied by the caller).
 void block_weights_and_cut(Ctx& ctx, const DevGraph& g, const int* part, int k, uint32_t* bw,
                            unsigned long long* cut2);
 
-// part_fine[v] = part_coarse[cmap[v]]
-void project(Ctx& ctx, int n, const int* cmap, const int* part_coarse, int* part_fine);
+// part_fine[v] = part_coarse[cmap[v]]; with cb and fb also fb[v] = cb[cmap[v]]
+void project(Ctx& ctx, int n, const int* cmap, const int* part_coarse, int* part_fine,
+             const uint8_t* cb = nullptr, uint8_t* fb = nullptr);
+
+// out[v] = 1 when v has a neighbour in another block of part (device)
+void boundary_flags(Ctx& ctx, const DevGraph& g, const int* part, uint8_t* out);
 
 // max degree of g (device reduction + readback)
 int max_degree(Ctx& ctx, const DevGraph& g);

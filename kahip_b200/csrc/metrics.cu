@@ -67,9 +67,29 @@ __global__ void cut_bw_kernel(int n, const int* __restrict__ xadj, const int* __
 }
 
 __global__ void project_kernel(int n, const int* __restrict__ cmap, const int* __restrict__ pc,
-                               int* __restrict__ pf) {
-    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x)
-        pf[v] = pc[cmap[v]];
+                               int* __restrict__ pf, const uint8_t* __restrict__ cb, uint8_t* __restrict__ fb) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const int c = cmap[v];
+        pf[v] = pc[c];
+        if (fb) fb[v] = cb[c];
+    }
+}
+
+// out[v] = 1 when a neighbour of v lies in another block (rows read four
+// entries at a time, stopping at the first such neighbour)
+__global__ void boundary_kernel(int n, const int* __restrict__ xadj, const int* __restrict__ adjncy,
+                                const int* __restrict__ part, uint8_t* __restrict__ out) {
+    for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+        const int p = part[v], e1 = xadj[v + 1];
+        int e = xadj[v];
+        bool b = false;
+        for (; !b && e + 4 <= e1; e += 4) {
+            const int u0 = adjncy[e], u1 = adjncy[e + 1], u2 = adjncy[e + 2], u3 = adjncy[e + 3];
+            b = (part[u0] != p) | (part[u1] != p) | (part[u2] != p) | (part[u3] != p);
+        }
+        for (; !b && e < e1; ++e) b = part[adjncy[e]] != p;
+        out[v] = b ? 1 : 0;
+    }
 }
 
 // out[0] = max degree, out[1] = isolated vertices, out[2] = their largest weight
@@ -245,10 +265,18 @@ void block_weights_and_cut(Ctx& ctx, const DevGraph& g, const int* part, int k, 
     KB_LAUNCH();
 }
 
-void project(Ctx& ctx, int n, const int* cmap, const int* part_coarse, int* part_fine) {
+void project(Ctx& ctx, int n, const int* cmap, const int* part_coarse, int* part_fine, const uint8_t* cb,
+             uint8_t* fb) {
     if (n == 0) return;
     PhaseScope ps(ctx, "project", 12.0 * n);
-    project_kernel<<<grid_for(n, 256), 256, 0, ctx.stream>>>(n, cmap, part_coarse, part_fine);
+    project_kernel<<<grid_for(n, 256), 256, 0, ctx.stream>>>(n, cmap, part_coarse, part_fine, cb, fb);
+    KB_LAUNCH();
+}
+
+void boundary_flags(Ctx& ctx, const DevGraph& g, const int* part, uint8_t* out) {
+    if (g.n == 0) return;
+    PhaseScope ps(ctx, "boundary", 8.0 * g.m + 9.0 * g.n);
+    boundary_kernel<<<grid_for(g.n, 256), 256, 0, ctx.stream>>>(g.n, g.xadj, g.adjncy, part, out);
     KB_LAUNCH();
 }
 

@@ -297,14 +297,34 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
     std::vector<uint32_t> hbw;
     bool balanced = true;
     long long final_cut = 0;
+    // LP refinement: a vertex can only move if it has a neighbour in another
+    // block, and then so does its coarse node one level up -- the first
+    // round sweeps only vertices whose coarse node was on the boundary after
+    // that level's refinement (all of them again when the balance repair ran)
+    const size_t mkb = ctx.scratch.mark();
+    uint8_t* bflag[2] = {nullptr, nullptr};
+    if (kn.refinement == 0 && L > 0) {
+        bflag[0] = ctx.scratch.alloc<uint8_t>((size_t)std::max(lv[0].g.n, 1));
+        bflag[1] = ctx.scratch.alloc<uint8_t>((size_t)std::max(lv[0].g.n, 1));
+    }
+    const uint8_t* cb = nullptr;  // boundary flags of level l + 1
     for (int l = L; l >= 0; --l) {
         const DevGraph& g = lv[l].g;
-        if (l < L) project(ctx, g.n, lv[l].cmap, lv[l + 1].part, lv[l].part);
+        uint8_t* act0 = cb ? bflag[l & 1] : nullptr;
+        if (l < L) project(ctx, g.n, lv[l].cmap, lv[l + 1].part, lv[l].part, cb, act0);
         const uint32_t bound = l == 0 ? kn.final_bound : kn.upper_bound;
         block_weights_and_cut(ctx, g, lv[l].part, k, bw, nullptr);
-        bool ok = balance(ctx, g, kn, l, bound, lv[l].part, bw);
+        bool repaired = false;
+        bool ok = balance(ctx, g, kn, l, bound, lv[l].part, bw, nullptr, &repaired);
         if (kn.refinement == 1) jet_refine(ctx, g, kn, l, bound, lv[l].part, bw);
-        else lp_refine(ctx, g, kn, l, bound, lv[l].part, bw);
+        else lp_refine(ctx, g, kn, l, bound, lv[l].part, bw, repaired ? nullptr : act0);
+        // (level l's own flags replace its first-round set, which is no
+        // longer needed; level l - 1 projects them into the other buffer)
+        cb = nullptr;
+        if (bflag[0] && l > 0) {
+            boundary_flags(ctx, g, lv[l].part, bflag[l & 1]);
+            cb = bflag[l & 1];
+        }
         if (l == 0 && host_part && g.n) {
             // the final partition goes to the host on the copy stream while the
             // cut and block weights are computed
@@ -323,6 +343,7 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
             if (st && l < 64) { st->level_cut[l] = c; st->level_maxbw[l] = mx; }
         }
     }
+    ctx.scratch.release(mkb);
     KB_CUDA(cudaStreamSynchronize(s));
     if (host_part) KB_CUDA(cudaStreamSynchronize(ctx.copies()));
     double ms_uncoarsen = ms_since(t2);
