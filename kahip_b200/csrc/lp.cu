@@ -1203,10 +1203,11 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
     const int k = kn.k, P = kn.ref_classes;
     uint32_t* H = ctx.scratch.alloc<uint32_t>((size_t)k * P);
     int* minvP = ctx.scratch.alloc<int>((size_t)k * P);
-    // round 0 sweeps every vertex; round r > 0 the neighbours of the vertices
-    // round r - 1 moved: as flags over all ids after round 0 (which moves
-    // many), as a list after later rounds (no pass over all ids)
-    uint8_t* flags = ctx.scratch.alloc<uint8_t>((size_t)g.n);
+    // round 0 sweeps every vertex (or active0); round r > 0 the neighbours of
+    // the vertices round r - 1 moved: as flags over all ids when many moved
+    // (round 0, or a round after one that moved more than n / 64), else as a
+    // list (no pass over all ids; every listing waits for an atomic)
+    uint8_t* flagbuf[2] = {ctx.scratch.alloc<uint8_t>((size_t)g.n), ctx.scratch.alloc<uint8_t>((size_t)g.n)};
     uint32_t* stamp = ctx.scratch.alloc<uint32_t>((size_t)g.n);
     int* alist[2] = {ctx.scratch.alloc<int>((size_t)g.n), ctx.scratch.alloc<int>((size_t)g.n)};
     unsigned* acount = ctx.scratch.alloc<unsigned>(2);
@@ -1219,7 +1220,6 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
     fill_u32(H, (long long)k * P, 0u, st);
     fill_i32(minvP, (long long)k * P, INT_MAX, st);
     fill_u32(stamp, g.n, 0u, st);
-    fill_u8(flags, g.n, 0, st);
     SweepArgs a = base_args(g, b);
     a.lab = part;
     a.lw = bw;
@@ -1230,11 +1230,16 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
     a.minvP = minvP;
     a.stash = 1;  // most neighbours lie in the vertex's own block
     unsigned* moved = b.counters + kCntMoved;
+    bool flags_in = false;               // this round's set came as flags
+    unsigned long long moved_prev = ~0ull;  // moves of the round before
     for (int r = 0; r < kn.ref_rounds; ++r) {
-        a.active = r == 0 ? active0 : r == 1 ? flags : nullptr;
-        a.vlist = r >= 2 ? alist[r & 1] : nullptr;
+        a.active = r == 0 ? active0 : flags_in ? flagbuf[r & 1] : nullptr;
+        a.vlist = r > 0 && !flags_in ? alist[r & 1] : nullptr;
         a.vcount = acount + (r & 1);
-        const NextActive na{r == 0 ? flags : nullptr, stamp, (uint32_t)r + 1u, alist[(r + 1) & 1],
+        const bool flags_out = moved_prev == ~0ull || moved_prev * 64 > (unsigned long long)g.n;
+        uint8_t* fo = flagbuf[(r + 1) & 1];
+        if (flags_out) fill_u8(fo, g.n, 0, st);
+        const NextActive na{flags_out ? fo : nullptr, stamp, (uint32_t)r + 1u, alist[(r + 1) & 1],
                             acount + ((r + 1) & 1), hubs, nhubs};
         a.ks_sub = stream_key(kn.seed, TAG_RSUB, level, r);
         a.ks_tie = stream_key(kn.seed, TAG_RTIE, level, r);
@@ -1263,6 +1268,8 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
         KB_CUDA(cudaMemcpyAsync(ctx.pinned, moved, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
         KB_CUDA(cudaStreamSynchronize(st));
         if (ctx.pinned[0] == 0) break;
+        moved_prev = ctx.pinned[0];
+        flags_in = flags_out;
     }
     ctx.scratch.release(mk);
 }
