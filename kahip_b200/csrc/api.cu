@@ -121,7 +121,7 @@ struct InvalidInput : std::runtime_error {
 };
 
 void check_uploaded(Ctx& ctx, DevGraph& g, uint32_t* total_weight = nullptr) {
-    int flags = check_graph(ctx, g, total_weight);
+    int flags = check_graph(ctx, g, total_weight, &g);
     g.unit_weights = (flags & 16) == 0;
     g.rows_sorted = (flags & 32) ? 0 : 1;
     if (flags & 1) throw InvalidInput("adjncy entry out of range");
@@ -277,7 +277,7 @@ Upload upload_checked(Ctx& ctx, int n, const int* xadj, const int* adjncy, const
         }
     }
     KB_CUDA(cudaStreamWaitEvent(s, mark(cs), 0));
-    const int flags = check_graph_end(ctx, total_weight);
+    const int flags = check_graph_end(ctx, total_weight, &u.g);
     u.g.unit_weights = (flags & 16) == 0;
     u.g.rows_sorted = (flags & 32) ? 0 : 1;
     if (flags & 1) throw InvalidInput("adjncy entry out of range");

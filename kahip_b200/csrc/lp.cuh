@@ -20,6 +20,7 @@ struct DevGraph {
     unsigned maxvw = 0xFFFFFFFFu;          // largest node weight (degree_stats fills it; all ones: unknown)
     bool unit_weights = false;  // every edge weight is 1 (lets sweeps skip adjwgt)
     int rows_sorted = -1;       // 1 / 0: rows do / do not list targets strictly increasing; -1 unknown
+    bool stats_known = false;   // maxdeg, iso_count, iso_wmax and maxvw are filled (the input check did it)
     const int* xadj = nullptr;
     const int* adjncy = nullptr;
     const int* adjwgt = nullptr;
@@ -71,13 +72,14 @@ void degree_stats(Ctx& ctx, DevGraph& g);
 // monotone, 16 = some edge weight differs from 1 (not an error), 32 = some
 // row does not list its targets in strictly increasing order (not an error).  Also returns the node weight sum (32-bit, as the reference's
 // NodeWeight accumulates it).  Synchronises the stream.
-int check_graph(Ctx& ctx, const DevGraph& g, uint32_t* total_weight = nullptr);
+// stats (optional): receives the degree statistics of degree_stats as well.
+int check_graph(Ctx& ctx, const DevGraph& g, uint32_t* total_weight = nullptr, DevGraph* stats = nullptr);
 // The same check in parts: begin (clears the flags), any number of vertex
 // ranges (unit_known: every edge weight is 1, adjwgt is not read), end
 // (synchronises and returns the flags).
 void check_graph_begin(Ctx& ctx);
 void check_graph_range(Ctx& ctx, const DevGraph& g, int v_lo, int v_hi, bool unit_known);
-int check_graph_end(Ctx& ctx, uint32_t* total_weight);
+int check_graph_end(Ctx& ctx, uint32_t* total_weight, DevGraph* stats = nullptr);
 
 // true if every row lists its targets in strictly increasing order
 // (synchronises the stream)

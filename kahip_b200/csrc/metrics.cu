@@ -162,9 +162,13 @@ __global__ void init_labels_kernel(int n, const int* __restrict__ vwgt, int* lab
 // reference's NodeWeight does).
 __global__ void check_graph_kernel(int n, long long m, const int* __restrict__ xadj,
                                    const int* __restrict__ adjncy, const int* __restrict__ adjwgt,
-                                   const int* __restrict__ vwgt, int* flags, unsigned* wsum, int v_lo, int v_hi) {
+                                   const int* __restrict__ vwgt, int* flags, unsigned* wsum, int v_lo, int v_hi,
+                                   unsigned* ds) {
     int f = 0;
     unsigned w = 0;
+    // degree statistics (what degree_stats computes): [0] max degree,
+    // [1] isolated nodes, [2] their largest weight, [3] largest node weight
+    unsigned md = 0, iso = 0, wi = 0, wa = 0;
     const int lane = threadIdx.x & 31;
     const long long warps = (long long)gridDim.x * (blockDim.x / 32);
     for (long long g0 = v_lo + ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32 * 32; g0 < v_hi;
@@ -178,6 +182,13 @@ __global__ void check_graph_kernel(int n, long long m, const int* __restrict__ x
             const int vw = vwgt[v];
             if (vw < 0) f |= 4;
             w += (unsigned)vw;
+            const unsigned d = x0 >= 0 && x1 >= x0 ? (unsigned)min(x1 - x0, (long long)INT_MAX) : 0u;
+            md = max(md, d);
+            wa = max(wa, (unsigned)vw);
+            if (d == 0) {
+                ++iso;
+                wi = max(wi, (unsigned)vw);
+            }
         }
         const bool sane = !in || (x0 >= 0 && x0 <= x1 && x1 <= m);
         if (!__all_sync(0xffffffffu, sane)) {
@@ -224,9 +235,17 @@ __global__ void check_graph_kernel(int n, long long m, const int* __restrict__ x
     if (v_lo == 0 && blockIdx.x == 0 && threadIdx.x == 0 && xadj[0] != 0) f |= 8;
     f = __reduce_or_sync(0xffffffffu, f);
     w = __reduce_add_sync(0xffffffffu, w);
+    md = __reduce_max_sync(0xffffffffu, md);
+    iso = __reduce_add_sync(0xffffffffu, iso);
+    wi = __reduce_max_sync(0xffffffffu, wi);
+    wa = __reduce_max_sync(0xffffffffu, wa);
     if ((threadIdx.x & 31) == 0) {
         if (f) atomicOr(flags, f);
         if (w) atomicAdd(wsum, w);
+        if (md) atomicMax(ds, md);
+        if (iso) atomicAdd(ds + 1, iso);
+        if (wi) atomicMax(ds + 2, wi);
+        if (wa) atomicMax(ds + 3, wa);
     }
 }
 
@@ -305,6 +324,7 @@ int max_degree(Ctx& ctx, const DevGraph& g) {
 
 void check_graph_begin(Ctx& ctx) {
     KB_CUDA(cudaMemsetAsync(ctx.dscalars + 2, 0, 2 * sizeof(int), ctx.stream));  // [2] flags, [3] weight sum
+    KB_CUDA(cudaMemsetAsync(ctx.dscalars + 8, 0, 4 * sizeof(int), ctx.stream));  // [8..11] degree statistics
 }
 
 void check_graph_range(Ctx& ctx, const DevGraph& g, int v_lo, int v_hi, bool unit_known) {
@@ -312,21 +332,29 @@ void check_graph_range(Ctx& ctx, const DevGraph& g, int v_lo, int v_hi, bool uni
     int* d = ctx.dscalars + 2;
     check_graph_kernel<<<grid_for((long long)std::max(v_hi - v_lo, 1), 256), 256, 0, ctx.stream>>>(
         g.n, g.m, g.xadj, g.adjncy, unit_known ? nullptr : g.adjwgt, g.vwgt, d, reinterpret_cast<unsigned*>(d + 1),
-        v_lo, v_hi);
+        v_lo, v_hi, reinterpret_cast<unsigned*>(ctx.dscalars + 8));
     KB_LAUNCH();
 }
 
-int check_graph_end(Ctx& ctx, uint32_t* total_weight) {
+int check_graph_end(Ctx& ctx, uint32_t* total_weight, DevGraph* stats) {
     KB_CUDA(cudaMemcpyAsync(ctx.pinned + 2, ctx.dscalars + 2, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    KB_CUDA(cudaMemcpyAsync(ctx.pinned + 8, ctx.dscalars + 8, 4 * sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
     KB_CUDA(cudaStreamSynchronize(ctx.stream));
     if (total_weight) *total_weight = ctx.pinned[3];
+    if (stats) {
+        stats->maxdeg = (int)ctx.pinned[8];
+        stats->iso_count = ctx.pinned[9];
+        stats->iso_wmax = ctx.pinned[10];
+        stats->maxvw = ctx.pinned[11];
+        stats->stats_known = true;
+    }
     return (int)ctx.pinned[2];
 }
 
-int check_graph(Ctx& ctx, const DevGraph& g, uint32_t* total_weight) {
+int check_graph(Ctx& ctx, const DevGraph& g, uint32_t* total_weight, DevGraph* stats) {
     check_graph_begin(ctx);
     if (g.m > 0 || g.n > 0) check_graph_range(ctx, g, 0, g.n, false);
-    return check_graph_end(ctx, total_weight);
+    return check_graph_end(ctx, total_weight, stats);
 }
 
 bool rows_strictly_increasing(Ctx& ctx, const DevGraph& g) {

@@ -186,7 +186,7 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
     std::vector<Level> lv;
     std::vector<const int*> P1{p1}, P2{p2};
     lv.push_back(Level{g0, nullptr, d_part});
-    degree_stats(ctx, lv[0].g);
+    if (!lv[0].g.stats_known) degree_stats(ctx, lv[0].g);
     // learned rating: the model's parameters, once per call
     float* d_model = nullptr;
     if (kn.coarsening == 2 && kn.rating_model) {
@@ -308,6 +308,11 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
         bflag[1] = ctx.scratch.alloc<uint8_t>((size_t)std::max(lv[0].g.n, 1));
     }
     const uint8_t* cb = nullptr;  // boundary flags of level l + 1
+    // LP refinement never lets a block exceed the bound it refines under, and
+    // projection keeps block weights: after a level that ended within its
+    // bound, the next level under the same bound needs no balance check
+    bool within = false;
+    uint32_t within_bound = 0;
     for (int l = L; l >= 0; --l) {
         const DevGraph& g = lv[l].g;
         uint8_t* act0 = cb ? bflag[l & 1] : nullptr;
@@ -315,7 +320,10 @@ static int partition_once(Ctx& ctx, const DevGraph& g0, const Knobs& kn, int* d_
         const uint32_t bound = l == 0 ? kn.final_bound : kn.upper_bound;
         block_weights_and_cut(ctx, g, lv[l].part, k, bw, nullptr);
         bool repaired = false;
-        bool ok = balance(ctx, g, kn, l, bound, lv[l].part, bw, nullptr, &repaired);
+        const bool ok = (within && bound == within_bound) ? true
+                                                         : balance(ctx, g, kn, l, bound, lv[l].part, bw, nullptr, &repaired);
+        within = ok && kn.refinement == 0;
+        within_bound = bound;
         if (kn.refinement == 1) jet_refine(ctx, g, kn, l, bound, lv[l].part, bw);
         else lp_refine(ctx, g, kn, l, bound, lv[l].part, bw, repaired ? nullptr : act0);
         // (level l's own flags replace its first-round set, which is no
