@@ -704,13 +704,20 @@ constexpr int kSmemTab = 4096;
 // `which`: 0 = every listed vertex, 1 = only those whose table fits in
 // shared memory, 2 = only the others (the two kinds can run as separate
 // launches with different grids; the decisions do not depend on the order).
+// The shared-memory table (stab slots, a power of two, keys then values) is
+// dynamic shared memory: kSmemTab slots in the many-block launches, more in
+// the launch of the longest rows, whose rows up to stab / 2 entries then
+// stay out of the global table.
 template <int MODE, int BT>
-__global__ void __launch_bounds__(BT) heavy_kernel(SweepArgs a, uint32_t* gtk, uint32_t* gtv, int gcap, int which) {
+__global__ void __launch_bounds__(BT) heavy_kernel(SweepArgs a, uint32_t* gtk, uint32_t* gtv, int gcap, int which,
+                                                   int stab) {
     __shared__ uint64_t sk[BT / 32];
     __shared__ uint32_t sid[BT / 32];
     __shared__ uint32_t sco;
-    __shared__ uint32_t stk[kSmemTab], stv[kSmemTab];
-    for (int s = threadIdx.x; s < kSmemTab; s += BT) {
+    extern __shared__ uint32_t htab[];
+    uint32_t* stk = htab;
+    uint32_t* stv = htab + stab;
+    for (int s = threadIdx.x; s < stab; s += BT) {
         stk[s] = kEmpty;
         stv[s] = 0;
     }
@@ -730,8 +737,8 @@ __global__ void __launch_bounds__(BT) heavy_kernel(SweepArgs a, uint32_t* gtk, u
         int cap = 256;
         while (cap < 2 * (end - beg) && cap < gcap) cap <<= 1;
         if ((which == 1 && cap > kSmemTab) || (which == 2 && cap <= kSmemTab)) continue;
-        uint32_t* tk = cap <= kSmemTab ? stk : gk;
-        uint32_t* tv = cap <= kSmemTab ? stv : gv;
+        uint32_t* tk = cap <= stab ? stk : gk;
+        uint32_t* tv = cap <= stab ? stv : gv;
         if (threadIdx.x == 0) {
             sco = 0;
             atomicAdd(&a.work[0], 1ull);
@@ -1060,6 +1067,24 @@ const char* family(int mode, int part) {
     return names[mode][part];
 }
 
+// Shared-memory slots of the longest rows' launch: rows up to kBigTab / 2
+// entries aggregate in shared memory (128 KiB of the block's), longer ones in
+// the global table.  The launch needs the larger dynamic shared memory
+// allowed once per device; without it the launch keeps kSmemTab slots.
+constexpr int kBigTab = 16384;
+
+template <int MODE>
+bool big_tab_ok() {
+    static int state[64];  // per device: 0 unknown, 1 allowed, -1 refused
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+    if (state[dev] == 0)
+        state[dev] = cudaFuncSetAttribute(heavy_kernel<MODE, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          8 * kBigTab) == cudaSuccess ? 1 : -1;
+    if (state[dev] < 0) (void)cudaGetLastError();
+    return state[dev] > 0;
+}
+
 template <int MODE>
 void launch_sweep(Ctx& ctx, const DevGraph& g, SweepArgs a, const SweepBuffers& b, double bytes) {
     KB_CUDA(cudaMemsetAsync(b.counters, 0, sizeof(unsigned) * kCntMoved, ctx.stream));
@@ -1077,14 +1102,17 @@ void launch_sweep(Ctx& ctx, const DevGraph& g, SweepArgs a, const SweepBuffers& 
     if (b.gcap > 0) {
         PhaseScope ps(ctx, family(MODE, 2), 0);
         if (b.gcap <= kSmemTab) {
-            heavy_kernel<MODE, kThreads><<<b.hblocks, kThreads, 0, ctx.stream>>>(a, nullptr, nullptr, b.gcap, 0);
+            heavy_kernel<MODE, kThreads><<<b.hblocks, kThreads, 8 * kSmemTab, ctx.stream>>>(a, nullptr, nullptr, b.gcap,
+                                                                                           0, kSmemTab);
             KB_LAUNCH();
         } else {
             // rows that fit the shared tables on many blocks, the longest
             // rows on the blocks that own a global table
-            heavy_kernel<MODE, kThreads><<<8 * kNumSMs, kThreads, 0, ctx.stream>>>(a, nullptr, nullptr, b.gcap, 1);
+            heavy_kernel<MODE, kThreads><<<8 * kNumSMs, kThreads, 8 * kSmemTab, ctx.stream>>>(a, nullptr, nullptr,
+                                                                                              b.gcap, 1, kSmemTab);
             KB_LAUNCH();
-            heavy_kernel<MODE, 1024><<<b.hblocks, 1024, 0, ctx.stream>>>(a, b.gtk, b.gtv, b.gcap, 2);
+            const int tab = big_tab_ok<MODE>() ? kBigTab : kSmemTab;
+            heavy_kernel<MODE, 1024><<<b.hblocks, 1024, 8 * tab, ctx.stream>>>(a, b.gtk, b.gtv, b.gcap, 2, tab);
             KB_LAUNCH();
         }
     }
