@@ -165,21 +165,50 @@ __device__ unsigned long long block_scan(unsigned long long x, unsigned long lon
 // Per-row sums over the local subgraph: entry(i, e, acc) for every entry e
 // of row i, then row(i, acc) once per row (a warp per row when WARP, the
 // warp's lane 0 calling row; a thread per row otherwise).
-template <bool WARP, class F, class G>
-__device__ __forceinline__ void for_rows(int n_o, const int* lbeg, const int* ldeg, F entry, G row) {
+// every row by default; take(i) false: row i's entries are not read (row(i)
+// still runs, with zero sums)
+struct AllRows {
+    __device__ bool operator()(int) const { return true; }
+};
+
+template <bool WARP, class F, class G, class Q = AllRows>
+__device__ __forceinline__ void for_rows(int n_o, const int* lbeg, const int* ldeg, const int* __restrict__ ladj,
+                                         const int* __restrict__ lw, bool vec, F entry, G row, Q take = Q()) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (WARP) {
         for (int i = wid; i < n_o; i += (int)(blockDim.x >> 5)) {
             Acc2 s{0, 0};
-            const int b = lbeg[i], d = ldeg[i];
-            int t = lane;
-            for (; t + 96 < d; t += 128) {  // four entries per lane in flight
-                entry(i, b + t, s);
-                entry(i, b + t + 32, s);
-                entry(i, b + t + 64, s);
-                entry(i, b + t + 96, s);
+            const int b = lbeg[i], d = take(i) ? ldeg[i] : 0;
+            if (vec && d >= 64) {
+                // 16-byte loads of four entries (and weights) per lane, from
+                // the 16-byte boundary at or before the row start; entries
+                // outside the row are skipped (rows in global memory only:
+                // the first load may start up to three entries before the
+                // row, the last end up to three after it, inside the arrays'
+                // allocation)
+                const int e1 = b + d;
+                const int a0 = b - (int)(((uintptr_t)(ladj + b) >> 2) & 3);
+                for (int c = a0 + 4 * lane; c < e1; c += 128) {
+                    const int4 u4 = *reinterpret_cast<const int4*>(ladj + c);
+                    const int4 w4 = *reinterpret_cast<const int4*>(lw + c);
+                    if (c >= b) entry(i, u4.x, w4.x, s);
+                    if (c + 1 >= b && c + 1 < e1) entry(i, u4.y, w4.y, s);
+                    if (c + 2 >= b && c + 2 < e1) entry(i, u4.z, w4.z, s);
+                    if (c + 3 >= b && c + 3 < e1) entry(i, u4.w, w4.w, s);
+                }
+            } else {
+                int t = lane;
+                for (; t + 96 < d; t += 128) {  // four entries per lane in flight
+                    const int e = b + t;
+                    const int u0 = ladj[e], u1 = ladj[e + 32], u2 = ladj[e + 64], u3 = ladj[e + 96];
+                    const int w0 = lw[e], w1 = lw[e + 32], w2 = lw[e + 64], w3 = lw[e + 96];
+                    entry(i, u0, w0, s);
+                    entry(i, u1, w1, s);
+                    entry(i, u2, w2, s);
+                    entry(i, u3, w3, s);
+                }
+                for (; t < d; t += 32) entry(i, ladj[b + t], lw[b + t], s);
             }
-            for (; t < d; t += 32) entry(i, b + t, s);
             s.a = warp_sum_ll(s.a);
             s.b = warp_sum_ll(s.b);
             if (lane == 0) row(i, s);
@@ -187,15 +216,18 @@ __device__ __forceinline__ void for_rows(int n_o, const int* lbeg, const int* ld
     } else {
         for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) {
             Acc2 s{0, 0};
-            const int b = lbeg[i], d = ldeg[i];
+            const int b = lbeg[i], d = take(i) ? ldeg[i] : 0;
             int t = 0;
             for (; t + 4 <= d; t += 4) {  // four independent entries in flight
-                entry(i, b + t, s);
-                entry(i, b + t + 1, s);
-                entry(i, b + t + 2, s);
-                entry(i, b + t + 3, s);
+                const int e = b + t;
+                const int u0 = ladj[e], u1 = ladj[e + 1], u2 = ladj[e + 2], u3 = ladj[e + 3];
+                const int w0 = lw[e], w1 = lw[e + 1], w2 = lw[e + 2], w3 = lw[e + 3];
+                entry(i, u0, w0, s);
+                entry(i, u1, w1, s);
+                entry(i, u2, w2, s);
+                entry(i, u3, w3, s);
             }
-            for (; t < d; ++t) entry(i, b + t, s);
+            for (; t < d; ++t) entry(i, ladj[b + t], lw[b + t], s);
             row(i, s);
         }
     }
@@ -279,6 +311,7 @@ struct Sub {
     const int* __restrict__ ladj;
     const int* __restrict__ lw;
     const int* cw;
+    bool vec;  // rows in global memory, ladj and lw 16-byte aligned alike: 16-byte row loads
     __device__ uint32_t c(int i) const { return (uint32_t)cw[i]; }
 };
 
@@ -296,8 +329,8 @@ __device__ __forceinline__ unsigned long long overload2(const unsigned long long
 template <bool WARP>
 __device__ long long cut_of(const Sub& S, const uint8_t* side, unsigned long long* sh) {
     long long mine = 0;
-    for_rows<WARP>(S.n_o, S.lbeg, S.ldeg,
-                   [&](int i, int e, Acc2& s) { if (side[S.ladj[e]] != side[i]) s.a += S.lw[e]; },
+    for_rows<WARP>(S.n_o, S.lbeg, S.ldeg, S.ladj, S.lw, S.vec,
+                   [&](int i, int u, int w, Acc2& s) { if (side[u] != side[i]) s.a += w; },
                    [&](int, const Acc2& s) { mine += s.a; });
     return (long long)block_sum((unsigned long long)mine, sh) / 2;
 }
@@ -384,10 +417,10 @@ __device__ void balance2(const Sub& S, uint8_t* side, int* cls, int s, const uns
         for (int t = threadIdx.x; t < kIpClasses; t += (int)blockDim.x) HS[t] = 0;
         __syncthreads();
         const uint64_t ks = mix64(ks_cls ^ (uint64_t)it);
-        for_rows<WARP>(S.n_o, S.lbeg, S.ldeg,
-                       [&](int i, int e, Acc2& a) {
-                           if (side[S.ladj[e]] == side[i]) a.a += S.lw[e];
-                           else a.b += S.lw[e];
+        for_rows<WARP>(S.n_o, S.lbeg, S.ldeg, S.ladj, S.lw, S.vec,
+                       [&](int i, int u, int w, Acc2& a) {
+                           if (side[u] == side[i]) a.a += w;
+                           else a.b += w;
                        },
                        [&](int i, const Acc2& a) {
                            cls[i] = -1;
@@ -496,8 +529,8 @@ template <bool WARP>
 __device__ void cut_and_weights(const Sub& S, const uint8_t* side, long long* cut, unsigned long long w[2],
                                 unsigned long long* sh4) {
     unsigned long long v[4] = {0, 0, 0, 0};
-    for_rows<WARP>(S.n_o, S.lbeg, S.ldeg,
-                   [&](int i, int e, Acc2& s) { if (side[S.ladj[e]] != side[i]) s.a += S.lw[e]; },
+    for_rows<WARP>(S.n_o, S.lbeg, S.ldeg, S.ladj, S.lw, S.vec,
+                   [&](int i, int u, int w, Acc2& s) { if (side[u] != side[i]) s.a += w; },
                    [&](int i, const Acc2& s) {
                        v[0] += (unsigned long long)s.a;
                        v[side[i] ? 2 : 1] += S.c(i);
@@ -553,10 +586,10 @@ __device__ long long jet2(const Sub& S, const IpArgs& a, uint8_t* side, uint8_t*
     for (; it < a.jet_iters; ++it) {
         // candidates, and the cut and weights of the current state
         unsigned long long v[4] = {0, 0, 0, 0};
-        for_rows<WARP>(n_o, S.lbeg, S.ldeg,
-                       [&](int i, int e, Acc2& s) {
-                           if (side[S.ladj[e]] == side[i]) s.a += S.lw[e];
-                           else s.b += S.lw[e];
+        for_rows<WARP>(n_o, S.lbeg, S.ldeg, S.ladj, S.lw, S.vec,
+                       [&](int i, int u, int w, Acc2& s) {
+                           if (side[u] == side[i]) s.a += w;
+                           else s.b += w;
                        },
                        [&](int i, const Acc2& s) {
                            v[0] += (unsigned long long)s.b;
@@ -579,13 +612,11 @@ __device__ long long jet2(const Sub& S, const IpArgs& a, uint8_t* side, uint8_t*
         // moved) and the moves it keeps, into the other side buffer; the side
         // weights follow from the moved weight
         unsigned long long m[4] = {0, 0, 0, 0};  // moves, weight 0 -> 1, weight 1 -> 0
-        for_rows<WARP>(n_o, S.lbeg, S.ldeg,
-                       [&](int i, int e, Acc2& s) {
-                           if (!dest[i]) return;
-                           const int u = S.ladj[e];
+        for_rows<WARP>(n_o, S.lbeg, S.ldeg, S.ladj, S.lw, S.vec,
+                       [&](int i, int u, int w, Acc2& s) {
                            int su = side[u];
                            if (dest[u] && (gain[u] > gain[i] || (gain[u] == gain[i] && u < i))) su = 1 - su;
-                           s.a += su != side[i] ? S.lw[e] : -(long long)S.lw[e];
+                           s.a += su != side[i] ? w : -(long long)w;
                        },
                        [&](int i, const Acc2& s) {
                            const uint8_t si = side[i];
@@ -597,7 +628,8 @@ __device__ long long jet2(const Sub& S, const IpArgs& a, uint8_t* side, uint8_t*
                            } else {
                                nside[i] = si;
                            }
-                       });
+                       },
+                       [&](int i) { return dest[i] != 0; });
         red4(m, red);
         {
             uint8_t* tsd = side;
@@ -920,7 +952,8 @@ __global__ void __launch_bounds__(MAXBT) ip_try(IpArgs a) {
         qa = dist + N;
         qb = qa + N;
     }
-    const Sub S{n_o, lbeg, ldeg, ladj, lw, cw};
+    const bool vec = !csr_smem && (((uintptr_t)a.ladj | (uintptr_t)a.lw) & 15) == 0;
+    const Sub S{n_o, lbeg, ldeg, ladj, lw, cw, vec};
     // targets and bounds
     unsigned long long Wm = 0;
     for (int i = threadIdx.x; i < n_o; i += (int)blockDim.x) Wm += S.c(i);
