@@ -1257,10 +1257,18 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
     a.H = H;
     a.minvP = minvP;
     a.stash = 1;  // most neighbours lie in the vertex's own block
-    unsigned* moved = b.counters + kCntMoved;
+    // Small levels read each round's move count one round late: round r + 1
+    // is queued before the host waits for round r's count (a round after one
+    // without moves sweeps an empty set), so the GPU is not idle while the
+    // host reads it.  On large levels the extra round costs more than the
+    // wait (measured).
+    const bool late = g.n <= (1 << 18);
+    unsigned* moved_r = ctx.scratch.alloc<unsigned>(2);
+    cudaEvent_t counted[2] = {ctx.ev(), ctx.ev()};
     bool flags_in = false;               // this round's set came as flags
-    unsigned long long moved_prev = ~0ull;  // moves of the round before
+    unsigned long long moved_prev = ~0ull;  // latest move count known to the host
     for (int r = 0; r < kn.ref_rounds; ++r) {
+        unsigned* moved = moved_r + (r & 1);
         a.active = r == 0 ? active0 : flags_in ? flagbuf[r & 1] : nullptr;
         a.vlist = r > 0 && !flags_in ? alist[r & 1] : nullptr;
         a.vcount = acount + (r & 1);
@@ -1293,12 +1301,24 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
         // (reading the count one round late, with the next round already
         // queued, measured slower: the queued round after the last one costs
         // more than the synchronisation it hides)
-        KB_CUDA(cudaMemcpyAsync(ctx.pinned, moved, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-        KB_CUDA(cudaStreamSynchronize(st));
-        if (ctx.pinned[0] == 0) break;
-        moved_prev = ctx.pinned[0];
+        KB_CUDA(cudaMemcpyAsync(ctx.pinned + 20 + (r & 1), moved, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
         flags_in = flags_out;
+        if (!late) {
+            KB_CUDA(cudaStreamSynchronize(st));
+            if (ctx.pinned[20 + (r & 1)] == 0) break;
+            moved_prev = ctx.pinned[20 + (r & 1)];
+            continue;
+        }
+        KB_CUDA(cudaEventRecord(counted[r & 1], st));
+        if (r > 0) {
+            KB_CUDA(cudaEventSynchronize(counted[(r - 1) & 1]));
+            const unsigned mp = ctx.pinned[20 + ((r - 1) & 1)];
+            if (mp == 0) break;  // round r (queued) has nothing to sweep
+            moved_prev = mp;
+        }
     }
+    ctx.ev_free.push_back(counted[0]);
+    ctx.ev_free.push_back(counted[1]);
     ctx.scratch.release(mk);
 }
 
