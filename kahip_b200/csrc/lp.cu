@@ -1298,9 +1298,10 @@ void lp_refine(Ctx& ctx, const DevGraph& g, const Knobs& kn, int level, uint32_t
                 KB_LAUNCH();
             }
         }
-        // (reading the count one round late, with the next round already
-        // queued, measured slower: the queued round after the last one costs
-        // more than the synchronisation it hides)
+        // large levels wait for this round's count before queueing the next
+        // (read one round late there, the queued round after the last one
+        // cost more than the synchronisation it hid); small levels read it
+        // one round late
         KB_CUDA(cudaMemcpyAsync(ctx.pinned + 20 + (r & 1), moved, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
         flags_in = flags_out;
         if (!late) {
