@@ -999,8 +999,6 @@ __global__ void block_scan_kernel(const uint32_t* bw, int k, uint32_t bound, int
 
 // ------------------------------------------------------------- host helpers
 
-int sweep_blocks() { return kNumSMs * 5; }  // 48 registers, 32 KB shared: 5 blocks per SM
-
 struct SweepBuffers {
     int *pt, *pc;
     unsigned* counters;  // [0, kStripes) unused, [kStripes, 2 kStripes) proposals,
@@ -1030,6 +1028,8 @@ SweepBuffers make_buffers(Ctx& ctx, const DevGraph& g) {
     b.counters = A.alloc<unsigned>(2 * kStripes + 8);
     // stripe capacities from the producers' warp counts and per-warp work
     const long long tasks = (n + 32 * kSpan - 1) / (32 * kSpan);
+    // one wave: 64 registers and 37 KB of shared memory per 256-thread
+    // block leave room for 4 blocks per SM
     b.lblocks = (int)std::max<long long>(1, std::min<long long>(div_up(tasks, kWarpsPerBlock), kNumSMs * 4LL));
     const long long wl = (long long)b.lblocks * kWarpsPerBlock;
     const long long cap_l = ((wl + kStripes - 1) / kStripes) * ((tasks + wl - 1) / wl) * 32 * kSpan;
